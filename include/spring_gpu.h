@@ -1,0 +1,170 @@
+/*
+ * spring_gpu.h — C ABI of the B200 phonon-scattering library (libspring_b200.so).
+ *
+ * Replaces the hot path of SPRING's kappa.x / kappa_iter.x / LineWidth.x:
+ * the per-q0 loop body of src/Kappa/Src/main.f90:552-715 and the kappa
+ * stage main.f90:734-751.  A Fortran host binds these entry points with
+ * iso_c_binding interfaces (bind(C), explicit-shape dummies, value scalars).
+ *
+ * Conventions
+ *  - Every call returns an int status (SPRING_OK == 0); spring_last_error()
+ *    gives the message of the last failure on that context.  Nothing throws.
+ *  - Arrays are the reference's Fortran arrays, column-major, passed as plain
+ *    pointers; the shape of each is written in Fortran order next to it.
+ *  - Indices that cross the ABI (q-point / grid / quartet numbers) are 1-based.
+ *  - complex(c_double_complex) arrays are interleaved (re, im) doubles.
+ *  - The host keeps ownership of its arrays: the library copies inputs into
+ *    device memory it owns and copies results back before returning.
+ *  - Output pointers documented as optional may be NULL: the result then stays
+ *    resident on the device for the next call (e.g. linewidths -> kappa).
+ *  - A context is used by one host thread at a time.
+ *  - Units are the reference's (src/Kappa/Src/constants.f90): omega in rad/ps,
+ *    force constants in eV/A^n, masses in amu, kappa in W/m/K.
+ */
+#ifndef SPRING_GPU_H
+#define SPRING_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct spring_ctx spring_ctx;
+
+/* status codes */
+#define SPRING_OK 0
+#define SPRING_ERR_ARG 1         /* invalid argument (NULL, size, range) */
+#define SPRING_ERR_STATE 2       /* a required input has not been set */
+#define SPRING_ERR_CUDA 3        /* CUDA runtime error (message has the CUDA text) */
+#define SPRING_ERR_ALLOC 4       /* device allocation failed */
+#define SPRING_ERR_UNSUPPORTED 5 /* valid request this build does not handle */
+#define SPRING_ERR_INJECTED 6    /* failure injected by spring_debug_inject_fault */
+
+/* delta-function schemes */
+#define SPRING_DELTA_GAUSS 0 /* Gaussian smearing, ThirdOrder_m.f90:442-543 */
+#define SPRING_DELTA_TETRA 1 /* linear tetrahedron, ThirdOrder_m.f90:169-275 */
+
+/* arithmetic of the V3/V4 contractions (deltas, rates and kappa stay FP64) */
+#define SPRING_FP64 0
+
+typedef struct {
+    int nbasis;  /* Nb: atoms in the unit cell (Ndof = 3*Nb), at most 8 */
+    int mesh[3]; /* q-mesh (AnhInfo qmesh) */
+    int n_temps; /* number of temperatures evaluated together (>= 1) */
+    int device;  /* CUDA device ordinal; -1 = the calling thread's current device */
+} spring_dims;
+
+/* ---- context ---------------------------------------------------------- */
+int spring_ctx_create(spring_ctx** ctx, const spring_dims* dims);
+int spring_ctx_destroy(spring_ctx* ctx);
+const char* spring_last_error(const spring_ctx* ctx);
+/* Use the caller's CUDA stream (cudaStream_t) for all work; NULL restores the
+ * context's own stream. */
+int spring_set_stream(spring_ctx* ctx, void* cuda_stream);
+int spring_synchronize(spring_ctx* ctx);
+/* Number of launches of this library's kernels since the context was created. */
+int spring_kernel_launches(const spring_ctx* ctx, long long* count);
+
+/* ---- crystal and force constants (L1/L2 inputs) ------------------------ */
+/* cell%init_data, src/Kappa/Src/unit_mod.f90:64-209: latvec(3,3) columns are
+ * the lattice vectors (A); mass(Nb) per basis atom (amu).  Computes the cell
+ * volume and the reciprocal vectors G like the reference. */
+int spring_set_crystal(spring_ctx* ctx, const double* latvec, const double* mass);
+
+/* FC2type%set_FC2, src/Kappa/Src/FC2_mod.f90:46-65:
+ * atm_num(Nb), atm_indx(4,na2,Nb) = (cell R1,R2,R3, basis index), fc2(1,3,3,na2,Nb). */
+int spring_set_fc2(spring_ctx* ctx, int na2, const int* atm_num, const int* atm_indx, const double* fc2);
+
+/* FC3type%set_FC3, src/Kappa/Src/FC3_mod.f90:49-94: atm_indx(4,na3,Nb),
+ * fc3(3,3,3,na3,na3,Nb) = (gamma,beta,alpha,N2,N1,mu). */
+int spring_set_fc3(spring_ctx* ctx, int na3, const int* atm_num, const int* atm_indx, const double* fc3);
+
+/* ---- mesh and irreducible q-points (L3) -------------------------------- */
+/* q_tetrahedron%make_tetrahedron, src/Kappa/Src/TetrahedronQ_m.f90:56-221.
+ * zero_centered = 1 folds to [-N/2+1, N/2] (kappa.x), 0 keeps [0, N) (LineWidth.x).
+ * Outputs (optional): q_pnt_int(3,Nq), q_pnt(3,Nq), tetrahedrons(4,6*Nq). */
+int spring_make_mesh(spring_ctx* ctx, const int* shift, int zero_centered, int* q_pnt_int, double* q_pnt,
+                     int* tetrahedrons);
+
+/* q_tetrahedron%FindIrrQ, TetrahedronQ_m.f90:224-331 (spglib's
+ * spg_get_ir_reciprocal_mesh for a Gamma-centred mesh, then unique_sort and
+ * FindPositionAndMultiplicity).  rotations(3,3,nrot) is the integer array
+ * spg_get_symmetry fills (src/Kappa/Src/Symmetry_m.f90:84): its memory is
+ * spglib's row-major W with x' = W x on fractional coordinates (the reference
+ * transposes it to build Rxyz, :92-97).  Outputs: *nq0, irr_q_pnt_int(3,Nq)
+ * (first nq0 columns used), pos(Nq) (1-based), multiplicity(Nq) (first nq0). */
+int spring_find_irr_q(spring_ctx* ctx, int nrot, const int* rotations, int time_rev, int* nq0,
+                      int* irr_q_pnt_int, int* pos, int* multiplicity);
+
+/* ---- harmonic phonons (L4) -------------------------------------------- */
+/* Phon%set_Phon_mp + get_phonon, src/Kappa/Src/phonon_mod.f90:156-313 and
+ * DynaMat_mod.f90:486-709, for the grid and the irreducible set, every
+ * temperature, on the device (batched FP64 Hermitian eigensolver).
+ * temps(n_temps) in K; freq_cut is the -omegacut value (stored, not used on this path). */
+int spring_compute_phonons(spring_ctx* ctx, const double* temps, double freq_cut);
+
+/* Load phonons computed by the host (e.g. with LAPACK zheevd) instead.
+ * which = 0: the Nq grid points; which = 1: the Nq0 irreducible points.
+ * evec(2,Ndof,Ndof,n) interleaved complex Evec(row,s,q); omega(Ndof,n);
+ * onebyomega(Ndof,n); nbe(Ndof,n,n_temps); grp_vel(3,Ndof,n).  temps(n_temps). */
+int spring_set_phonons(spring_ctx* ctx, int which, const double* temps, const double* evec, const double* omega,
+                       const double* onebyomega, const double* nbe, const double* grp_vel);
+/* Copy the device phonons back (any pointer may be NULL). */
+int spring_get_phonons(spring_ctx* ctx, int which, double* evec, double* omega, double* onebyomega, double* nbe,
+                       double* grp_vel);
+
+/* ---- enumeration (L5) -------------------------------------------------- */
+/* MomentumConsrv3rd, src/Kappa/Src/QuasiMomentumConsrv3rd_m.f90:13-158, for
+ * q0 = irreducible point i0 (1-based), without the count assertions
+ * (:148-153).  Allq1q2(4,Nq), q1q2_permuted(2,Nq) (first counts[0] columns),
+ * counts = (pairs, total_count).  Outputs are bit-identical to the reference
+ * algorithm's, on every mesh. */
+int spring_enumerate3(spring_ctx* ctx, int i0, int* Allq1q2, int* q1q2_permuted, int* counts);
+
+/* ---- three-phonon scattering ------------------------------------------ */
+/* ScatterProbAllq1, src/Kappa/Src/ThirdOrder_m.f90:41-166: the W3 of every
+ * grid q1 for q0 = i0; sctrq1(Ndof,Ndof,Ndof,Nq) = (s2,s1,s0,q1). */
+int spring_scatter_w3(spring_ctx* ctx, int i0, double* sctrq1);
+
+/* The 3-phonon linewidth of irreducible points i0_first .. i0_first+n_q0-1
+ * at every temperature: V3 -> W -> delta sum, fused on the device.
+ *   delta_mode SPRING_DELTA_TETRA: CalculateLwTetrahedron (ThirdOrder_m.f90:169-275);
+ *   delta_mode SPRING_DELTA_GAUSS: CalculateLinewidth (ThirdOrder_m.f90:442-543),
+ *     sigma in rad/ps (2 cm^-1 = 0.37673 rad/ps), branch start reset per q1.
+ * pol3(2,3): Polarization3rd (Helper_m.f90:310-353) or NULL for all branches.
+ * lw(Ndof,n_q0,n_temps) and p3_q0(Ndof,n_q0) are optional outputs; the
+ * linewidth is also added to the context's resident LW_Allq0 (main.f90:584). */
+int spring_linewidth3(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol3,
+                      double* lw, double* p3_q0);
+
+/* Isotope scattering rate, CalculateIsoW + CalculateIsoLwTetra
+ * (src/Kappa/Src/IsotopicScatter.f90:36-168); Gaussian form uses
+ * delta(omega0 - omega1).  g2(Nb) mass variance.  rate(Ndof,n_q0,n_temps)
+ * optional; 0.5*rate is added to the resident LW_Allq0 (main.f90:604). */
+int spring_linewidth_iso(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const double* g2,
+                         double* rate);
+
+/* Zero / read / replace the resident LW_Allq0(Ndof,Nq0,n_temps). */
+int spring_reset_linewidths(spring_ctx* ctx);
+int spring_get_linewidths(spring_ctx* ctx, double* lw_all);
+int spring_set_linewidths(spring_ctx* ctx, const double* lw_all);
+
+/* ---- thermal conductivity --------------------------------------------- */
+/* RTA kappa per temperature, kappa(9,n_temps) in kron_prod order.
+ *   symm = 1: GrVelKronProdSymm + kappa_noIter_symm (VelocityKronProd_symm.f90:34-91,
+ *             ThermalConductivity.f90:167-292); Rxyz(3,3,nsym) Cartesian rotations.
+ *   symm = 0: kappa_noIter over the full grid (ThermalConductivity.f90:36-164).
+ * s_range(2): branch window (min/max of Polarization3rd/4th first column) or NULL.
+ * mode_k(9,Ndof,n_temps) optional (ModeResolvedKappa). Uses the resident LW_Allq0. */
+int spring_kappa_rta(spring_ctx* ctx, int symm, int nsym, const double* Rxyz, const int* s_range, double* kappa,
+                     double* mode_k);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* Make the n-th (1-based) subsequent device allocation (kind 0), host<->device
+ * copy (kind 1) or kernel launch (kind 2) report failure without performing
+ * it; n = 0 disarms.  For testing callers' error paths. */
+int spring_debug_inject_fault(spring_ctx* ctx, int kind, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SPRING_GPU_H */

@@ -1,0 +1,332 @@
+"""Oracle driver — TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper around ``oracle/_build/liboracle.so`` (the C++ FP64
+restatement) plus the orchestration of ``kappa.x``'s driver loop
+(``src/Kappa/Src/main.f90:552-766``) on top of it.  Used by tests/, by the
+CPU-baseline leg of bench.py and by ``__graft_entry__.smoke`` as the checker;
+the product never imports it.
+
+Parity status: unpinned against reference outputs (the reference Fortran
+cannot be built here and ships no golden vectors for this path); pinned by the
+reference's in-code invariants and the known-answer tests in tests/.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+from . import constants as C
+from . import phonons as P
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+c128p = np.ctypeslib.ndpointer(dtype=np.complex128, flags="C_CONTIGUOUS")
+i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+def build() -> str:
+    """Compile the oracle (``make -C oracle``) and return the library path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return os.path.join(_HERE, "_build", "liboracle.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "_build", "liboracle.so")
+        if not os.path.exists(path):
+            path = build()
+        L = ct.CDLL(path)
+        L.orc_make_tetrahedron.argtypes = [i32p, i32p, f64p, ct.c_int, i32p, f64p, i32p]
+        L.orc_make_tetrahedron.restype = ct.c_int
+        L.orc_irr_q.argtypes = [i32p, ct.c_int, i32p, ct.c_int, i32p, i32p, i32p, i32p, i32p]
+        L.orc_irr_q.restype = ct.c_int
+        L.orc_momentum3.argtypes = [i32p, i32p, i32p, i32p, i32p, i32p]
+        L.orc_momentum3.restype = None
+        L.orc_momentum4.argtypes = [i32p, i32p, i32p, i32p, i32p, ct.c_longlong, i64p]
+        L.orc_momentum4.restype = ct.c_int
+        L.orc_scatter_w3.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, ct.c_int, f64p, i32p,
+                                     i32p, c128p, f64p, c128p, f64p, ct.c_int, i32p, f64p]
+        L.orc_scatter_w3.restype = None
+        L.orc_find_g_iver.argtypes = [ct.c_double, f64p, f64p, ct.c_int, f64p, f64p, f64p, f64p, i32p]
+        L.orc_find_g_iver.restype = ct.c_int
+        L.orc_lw3_tetra.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, f64p, i32p, i32p, i32p, f64p, f64p, f64p]
+        L.orc_lw3_tetra.restype = None
+        L.orc_lw3_gauss.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, f64p, i32p, i32p, i32p, ct.c_double,
+                                    f64p, f64p]
+        L.orc_lw3_gauss.restype = None
+        L.orc_iso_w.argtypes = [ct.c_int, ct.c_int, c128p, f64p, c128p, f64p, f64p]
+        L.orc_iso_w.restype = None
+        L.orc_iso_lw_tetra.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, i32p, f64p]
+        L.orc_iso_lw_tetra.restype = None
+        L.orc_iso_lw_gauss.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, ct.c_double, f64p]
+        L.orc_iso_lw_gauss.restype = None
+        L.orc_velkron_symm.argtypes = [ct.c_int, ct.c_int, f64p, ct.c_int, f64p, i32p, f64p]
+        L.orc_velkron_symm.restype = None
+        L.orc_kappa_symm.argtypes = [ct.c_int, ct.c_int, ct.c_int, i32p, f64p, f64p, f64p, f64p, ct.c_int,
+                                     ct.c_int, ct.c_double, ct.c_double, ct.c_double, f64p, ct.c_void_p]
+        L.orc_kappa_symm.restype = None
+        L.orc_kappa_full.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, f64p, ct.c_int, ct.c_int,
+                                     ct.c_double, ct.c_double, ct.c_double, f64p]
+        L.orc_kappa_full.restype = None
+        L.orc_num_threads.restype = ct.c_int
+        _LIB = L
+    return _LIB
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+# ----------------------------------------------------------------------------- mesh
+def make_tetrahedron(mesh, G, shift=(0, 0, 0), zero_centered=True):
+    mesh = _i(mesh)
+    nq = int(np.prod(mesh))
+    qi = np.zeros((nq, 3), np.int32)
+    qf = np.zeros((nq, 3), np.float64)
+    tet = np.zeros((6 * nq, 4), np.int32)
+    rc = lib().orc_make_tetrahedron(mesh, _i(shift), _f(np.asarray(G).T), int(zero_centered), qi, qf, tet)
+    if rc != 0:
+        raise ValueError("make_tetrahedron: vertex outside the grid")
+    return qi, qf, tet
+
+
+def irr_q(mesh, W, q_pnt_int, time_rev=0):
+    mesh = _i(mesh)
+    nq = int(np.prod(mesh))
+    mp = np.zeros(nq, np.int32)
+    irr = np.zeros((nq, 3), np.int32)
+    pos = np.zeros(nq, np.int32)
+    mult = np.zeros(nq, np.int32)
+    n = lib().orc_irr_q(mesh, len(W), _i(W), int(time_rev), _i(q_pnt_int), mp, irr, pos, mult)
+    return dict(map=mp, irr_q_pnt_int=irr[:n].copy(), pos=pos, multiplicity=mult[:n].copy())
+
+
+# ----------------------------------------------------------------------------- enumeration
+def momentum3(mesh, q_pnt_int, q0_int):
+    nq = int(np.prod(mesh))
+    A = np.zeros((nq, 4), np.int32)
+    Pm = np.zeros((nq, 2), np.int32)
+    cnt = np.zeros(2, np.int32)
+    lib().orc_momentum3(_i(mesh), _i(q_pnt_int), _i(q0_int), A, Pm, cnt)
+    return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
+
+
+def momentum4(mesh, q_pnt_int, q0_int, cap=None):
+    nq = int(np.prod(mesh))
+    if cap is None:
+        cap = nq * nq
+    A = np.zeros((nq, nq, 3), np.int32)
+    Pm = np.zeros((cap, 3), np.int32)
+    cnt = np.zeros(2, np.int64)
+    rc = lib().orc_momentum4(_i(mesh), _i(q_pnt_int), _i(q0_int), A, Pm, int(cap), cnt)
+    if rc != 0:
+        raise ValueError("momentum4: capacity exceeded")
+    return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
+
+
+# ----------------------------------------------------------------------------- V3 / W
+def fc3_derived(cr):
+    """basisTyp(Na3,Nb) and atmPosR(3,Na3,Nb) of ``set_FC3`` (``src/Kappa/Src/FC3_mod.f90:49-94``)."""
+    idx = cr.fc3_atm_indx
+    btyp = _i(idx[:, :, 3])
+    pos = np.einsum("ij,mnj->mni", cr.latvec, idx[:, :, :3].astype(np.float64))
+    return btyp, _f(pos)
+
+
+def scatter_w3(cr, q_pnt, q_pnt_int, q0_int, evec0, oneby0, evec, oneby, q1q2_perm):
+    nb = cr.nbasis
+    ndof = 3 * nb
+    nq = q_pnt.shape[0]
+    btyp, posr = fc3_derived(cr)
+    out = np.zeros((nq, ndof, ndof, ndof), np.float64)
+    lib().orc_scatter_w3(nb, cr.fc3.shape[1], _i(cr.fc3_atm_num), btyp, posr, _f(cr.fc3),
+                         _f(1.0 / np.sqrt(cr.mass)), nq, _f(q_pnt), _i(q_pnt_int), _i(q0_int), _c(evec0),
+                         _f(oneby0), _c(evec), _f(oneby), len(q1q2_perm), _i(q1q2_perm), out)
+    return out   # [q1][s0][s1][s2] == Fortran Sctrq1(s2,s1,s0,q1)
+
+
+def find_g_iver(Mqs, M, F, strict=False):
+    g = np.zeros(1)
+    I = np.zeros(4)
+    Ms = np.zeros(4)
+    Fs = np.zeros(4)
+    perm = np.zeros(4, np.int32)
+    e = lib().orc_find_g_iver(float(Mqs), _f(M), _f(F), int(strict), g, I, Ms, Fs, perm)
+    return bool(e), float(g[0]), I, Ms, Fs, perm
+
+
+def lw3_tetra(omega0, omega, nbe, sctr, tetra, Allq1q2, pol=None):
+    ndof = omega.shape[1]
+    nq = omega.shape[0]
+    if pol is None:
+        pol = np.array([[1, ndof]] * 3, np.int32)
+    lw = np.zeros(ndof)
+    p3q = np.zeros(ndof)
+    p3 = np.zeros(1)
+    lib().orc_lw3_tetra(ndof, nq, _f(omega0), _f(omega), _f(nbe), _f(sctr), _i(tetra), _i(Allq1q2), _i(pol),
+                        lw, p3q, p3)
+    return lw, p3q, float(p3[0])
+
+
+def lw3_gauss(omega0, omega, nbe, sctr, Allq1q2, q_pnt_int, sigma, pol=None):
+    ndof = omega.shape[1]
+    nq = omega.shape[0]
+    if pol is None:
+        pol = np.array([[1, ndof]] * 3, np.int32)
+    lw = np.zeros(ndof)
+    p3q = np.zeros(ndof)
+    lib().orc_lw3_gauss(ndof, nq, _f(omega0), _f(omega), _f(nbe), _f(sctr), _i(Allq1q2), _i(q_pnt_int),
+                        _i(pol), float(sigma), lw, p3q)
+    return lw, p3q
+
+
+def iso_w(nb, evec0, omega0, evec, g2):
+    nq = evec.shape[0]
+    ndof = 3 * nb
+    out = np.zeros((nq, ndof, ndof))
+    lib().orc_iso_w(nb, nq, _c(evec0), _f(omega0), _c(evec), _f(g2), out)
+    return out    # [q1][s0][s1] == Fortran W_iso(s1,s0,q1)
+
+
+def iso_lw_tetra(omega0, omega, w_iso, tetra):
+    ndof = omega.shape[1]
+    lw = np.zeros(ndof)
+    lib().orc_iso_lw_tetra(ndof, omega.shape[0], _f(omega0), _f(omega), _f(w_iso), _i(tetra), lw)
+    return lw
+
+
+def iso_lw_gauss(omega0, omega, w_iso, sigma):
+    ndof = omega.shape[1]
+    lw = np.zeros(ndof)
+    lib().orc_iso_lw_gauss(ndof, omega.shape[0], _f(omega0), _f(omega), _f(w_iso), float(sigma), lw)
+    return lw
+
+
+# ----------------------------------------------------------------------------- kappa
+def velkron_symm(grp_vel0, Rxyz, mult):
+    nq0, ndof = grp_vel0.shape[:2]
+    out = np.zeros((nq0, ndof, 9))
+    # Rxyz(3,3,Nsym) column-major == C array [ns][col][row]
+    R = _f(np.transpose(np.asarray(Rxyz), (0, 2, 1)))
+    lib().orc_velkron_symm(ndof, nq0, _f(grp_vel0), len(Rxyz), R, _i(mult), out)
+    return out
+
+
+def kappa_symm(nq, irr_int, omega0, nbe0, lw, krn, vol, T, s_first=1, s_last=None, mode=False):
+    nq0, ndof = omega0.shape
+    if s_last is None:
+        s_last = ndof
+    kap = np.zeros(9)
+    mk = np.zeros((ndof, 9)) if mode else None
+    lib().orc_kappa_symm(ndof, nq, nq0, _i(irr_int), _f(omega0), _f(nbe0), _f(lw), _f(krn), s_first, s_last,
+                         vol, T, C.kW_m_k, kap, mk.ctypes.data if mode else None)
+    return (kap, mk) if mode else kap
+
+
+def kappa_full(q_pnt_int, pos, omega, nbe, grp_vel, lw, vol, T, s_first=1, s_last=None):
+    nq, ndof = omega.shape
+    if s_last is None:
+        s_last = ndof
+    kap = np.zeros(9)
+    lib().orc_kappa_full(ndof, nq, _i(q_pnt_int), _i(pos), _f(omega), _f(nbe), _f(grp_vel), _f(lw), s_first,
+                         s_last, vol, T, C.kW_m_k, kap)
+    return kap
+
+
+# ----------------------------------------------------------------------------- pipeline
+class Setup:
+    """Mesh, irreducible set and phonons for one crystal / mesh / temperature list."""
+
+    def __init__(self, cr, mesh, temps, W=None, Rxyz=None):
+        from spring_b200 import synthetic as S
+        self.cr = cr
+        self.mesh = np.array(mesh, np.int32)
+        self.temps = np.atleast_1d(np.asarray(temps, np.float64))
+        self.nq = int(np.prod(self.mesh))
+        self.q_pnt_int, self.q_pnt, self.tetra = make_tetrahedron(self.mesh, cr.G)
+        if W is None:
+            W, Rxyz = S.point_group(cr)
+        self.W, self.Rxyz = W, Rxyz
+        ir = irr_q(self.mesh, W, self.q_pnt_int)
+        self.irr_int = ir["irr_q_pnt_int"]
+        self.pos = ir["pos"]
+        self.mult = ir["multiplicity"]
+        self.nq0 = self.irr_int.shape[0]
+        Ru = cr.G / self.mesh[None, :]
+        self.irr_q = (Ru @ self.irr_int.T.astype(np.float64)).T
+        args = (cr.latvec, cr.mass, cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
+        self.ph0 = P.get_phonon(*args, self.irr_q, self.temps)
+        self.ph = P.get_phonon(*args, self.q_pnt, self.temps)
+
+
+def linewidth3_q0(st: Setup, i0, delta="gauss", sigma=0.3767, it=0, pol=None, with_w=False):
+    """One pass of the q0 loop body (``main.f90:560-587``) for q0 = i0 (0-based)."""
+    A, perm, cnt = momentum3(st.mesh, st.q_pnt_int, st.irr_int[i0])
+    sctr = scatter_w3(st.cr, st.q_pnt, st.q_pnt_int, st.irr_int[i0], st.ph0["evec"][i0],
+                      st.ph0["onebyomega"][i0], st.ph["evec"], st.ph["onebyomega"], perm)
+    om0 = st.ph0["omega"][i0]
+    if delta == "gauss":
+        lw, p3q = lw3_gauss(om0, st.ph["omega"], st.ph["nbe"][it], sctr, A, st.q_pnt_int, sigma, pol)
+        p3 = float(p3q.sum())
+    else:
+        lw, p3q, p3 = lw3_tetra(om0, st.ph["omega"], st.ph["nbe"][it], sctr, st.tetra, A, pol)
+    out = dict(lw=lw, p3_q0=p3q, p3=p3, npairs=cnt[0])
+    if with_w:
+        out["sctr"] = sctr
+        out["Allq1q2"] = A
+        out["perm"] = perm
+    return out
+
+
+def linewidth3_all(st: Setup, delta="gauss", sigma=0.3767, q0_list=None, isotope=None):
+    """Linewidths (nT, Nq0, Ndof) of the 3-phonon (+isotope) path for the given q0s."""
+    nT = len(st.temps)
+    ndof = st.cr.ndof
+    q0_list = range(st.nq0) if q0_list is None else q0_list
+    lw = np.zeros((nT, st.nq0, ndof))
+    for i0 in q0_list:
+        A, perm, cnt = momentum3(st.mesh, st.q_pnt_int, st.irr_int[i0])
+        sctr = scatter_w3(st.cr, st.q_pnt, st.q_pnt_int, st.irr_int[i0], st.ph0["evec"][i0],
+                          st.ph0["onebyomega"][i0], st.ph["evec"], st.ph["onebyomega"], perm)
+        om0 = st.ph0["omega"][i0]
+        for it in range(nT):
+            if delta == "gauss":
+                l3, _ = lw3_gauss(om0, st.ph["omega"], st.ph["nbe"][it], sctr, A, st.q_pnt_int, sigma)
+            else:
+                l3, _, _ = lw3_tetra(om0, st.ph["omega"], st.ph["nbe"][it], sctr, st.tetra, A)
+            lw[it, i0] = l3
+        if isotope is not None:
+            wi = iso_w(st.cr.nbasis, st.ph0["evec"][i0], om0, st.ph["evec"], isotope)
+            li = (iso_lw_gauss(om0, st.ph["omega"], wi, sigma) if delta == "gauss"
+                  else iso_lw_tetra(om0, st.ph["omega"], wi, st.tetra))
+            lw[:, i0] += 0.5 * li
+    return lw
+
+
+def kappa_rta(st: Setup, lw, symm=True):
+    """RTA kappa (nT, 9) from linewidths (nT, Nq0, Ndof)."""
+    out = []
+    for it, T in enumerate(st.temps):
+        if symm:
+            krn = velkron_symm(st.ph0["grp_vel"], st.Rxyz, st.mult)
+            out.append(kappa_symm(st.nq, st.irr_int, st.ph0["omega"], st.ph0["nbe"][it], lw[it], krn,
+                                  st.cr.vol, T))
+        else:
+            out.append(kappa_full(st.q_pnt_int, st.pos, st.ph["omega"], st.ph["nbe"][it], st.ph["grp_vel"],
+                                  lw[it], st.cr.vol, T))
+    return np.array(out)

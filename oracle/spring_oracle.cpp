@@ -1,0 +1,736 @@
+// Oracle — TEST INFRASTRUCTURE ONLY.  A CPU FP64 restatement of the SPRING
+// phonon-scattering path, written loop-for-loop after the reference Fortran so
+// that the GPU library can be checked against it.  Only tests/, bench.py's CPU
+// baseline leg and __graft_entry__.smoke() load this library; the product
+// (spring_b200) never does.
+//
+// Parity status: the reference Fortran cannot be compiled in this environment
+// (no Fortran compiler, no HDF5, no spglib), and the reference ships no golden
+// vectors for this path.  The restatement is pinned by the reference's own
+// in-code invariants (count identities on odd meshes, sum of tetrahedron
+// weights, FindIrrQ grid identity) and by known-answer tests in tests/.
+//
+// Array conventions: every array is the flat memory of the reference's Fortran
+// array (column-major); comments give the Fortran shape.  Indices stored in
+// arrays are 1-based like the reference's.
+#include <cmath>
+#include <complex>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef std::complex<double> cplx;
+
+namespace {
+
+const double PI = 4.0 * std::atan(1.0);
+const double Onebysqrt2PI = 1.0 / std::sqrt(2.0 * PI);
+const double zero_prec = 5.0e-5;
+const double OnebySix = 0.16666666666666666;
+const double Sctr3THz2 = 1.054571817 * (1.60217733 * 1.60217733) *
+                         (6.02214076 * 6.02214076 * 6.02214076) * 1000000.0 * PI * 0.0625;
+
+inline int imod(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+// dot_product(modulo(v, mesh), mesh_mul) + 1   (1-based grid index)
+inline int grid_index(const int v[3], const int mesh[3]) {
+    return imod(v[0], mesh[0]) + mesh[0] * imod(v[1], mesh[1]) +
+           mesh[0] * mesh[1] * imod(v[2], mesh[2]) + 1;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---------------------------------------------------------------------------
+// make_tetrahedron  (src/Kappa/Src/TetrahedronQ_m.f90:56-221, fold_indx
+// src/Kappa/Src/IndxChng_mod.f90:85-107, MapAwayFromBZboundary :110-135)
+//   q_pnt_int(3,Nq) int, q_pnt(3,Nq) f64, tetrahedrons(4,6*Nq) int (1-based)
+//   G: 3x3 column-major, G(:,i) is reciprocal vector i.
+// Returns 0, or -1 when a vertex maps outside the grid (the reference stops).
+int orc_make_tetrahedron(const int* mesh, const int* shift, const double* G, int zero_centered,
+                         int* q_pnt_int, double* q_pnt, int* tetrahedrons) {
+    const int box[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 0, 1}, {0, 1, 1},
+                           {1, 0, 1}, {1, 1, 1}, {1, 1, 0}, {0, 1, 0}};
+    const int nq = mesh[0] * mesh[1] * mesh[2];
+    std::vector<char> uniq(nq, 1);
+    double Ru[3][3];  // Recp_cell_unit(:, i) = G(:, i)/mesh(i)
+    for (int i = 0; i < 3; ++i)
+        for (int r = 0; r < 3; ++r) Ru[r][i] = G[r + 3 * i] / double(mesh[i]);
+    int tcount = 0;
+    for (int iz = 0; iz < mesh[2]; ++iz)
+        for (int iy = 0; iy < mesh[1]; ++iy)
+            for (int ix = 0; ix < mesh[0]; ++ix) {
+                int indx[3] = {ix, iy, iz}, vt[3];
+                for (int d = 0; d < 3; ++d) {
+                    vt[d] = indx[d];
+                    if (zero_centered && vt[d] > mesh[d] / 2) vt[d] -= mesh[d];
+                }
+                int bt[8];
+                for (int v = 0; v < 8; ++v) {
+                    int vert[3], vf[3];
+                    for (int d = 0; d < 3; ++d) vert[d] = box[v][d] + vt[d];
+                    for (int d = 0; d < 3; ++d) {
+                        vf[d] = vert[d];
+                        if (zero_centered) {
+                            if (vf[d] > mesh[d] / 2) vf[d] -= mesh[d];
+                        } else {
+                            if (vf[d] == mesh[d]) vf[d] -= mesh[d];
+                            else if (vf[d] > mesh[d]) return -1;
+                        }
+                    }
+                    int g = grid_index(vf, mesh);
+                    if (g > nq) return -1;
+                    bt[v] = g;
+                    if (uniq[g - 1]) {
+                        for (int d = 0; d < 3; ++d) q_pnt_int[3 * (g - 1) + d] = vf[d];
+                        for (int r = 0; r < 3; ++r) {
+                            double s = 0.0;
+                            for (int c = 0; c < 3; ++c) s += Ru[r][c] * (double(vf[c]) + double(shift[c]) * 0.5);
+                            q_pnt[3 * (g - 1) + r] = s;
+                        }
+                        uniq[g - 1] = 0;
+                    }
+                }
+                const int pat[6][4] = {{0, 1, 2, 3}, {2, 3, 4, 1}, {5, 3, 4, 1},
+                                       {5, 3, 6, 1}, {6, 3, 7, 1}, {0, 3, 7, 1}};
+                for (int t = 0; t < 6; ++t)
+                    for (int v = 0; v < 4; ++v) tetrahedrons[4 * (tcount + t) + v] = bt[pat[t][v]];
+                tcount += 6;
+            }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Irreducible q-points.  Restates spglib 1.16.5 spg_get_ir_reciprocal_mesh
+// (called at src/Kappa/Src/TetrahedronQ_m.f90:261) for a Gamma-centred mesh:
+// every grid point maps to the smallest grid index in its orbit under the
+// reciprocal rotations W^T (and -W^T when time_rev != 0).  Then unique_sort
+// (Helper_m.f90:510-545) and FindPositionAndMultiplicity (:548-594).
+//   rot: nrot integer 3x3 matrices W, row-major (x' = W x on fractional coords)
+//   map_out(Nq) 0-based representative; irr(3,Nq0) addresses; pos(Nq) 1-based;
+//   mult(Nq0).  Returns Nq0.
+int orc_irr_q(const int* mesh, int nrot, const int* rot, int time_rev,
+              const int* q_pnt_int, int* map_out, int* irr_q_pnt_int, int* pos, int* mult) {
+    const int nq = mesh[0] * mesh[1] * mesh[2];
+    std::vector<int> map(nq);
+    for (int i = 0; i < nq; ++i) {
+        const int* a = q_pnt_int + 3 * i;
+        int best = i;
+        for (int s = 0; s < nrot; ++s) {
+            const int* W = rot + 9 * s;
+            for (int sg = 0; sg < (time_rev ? 2 : 1); ++sg) {
+                int b[3];
+                for (int r = 0; r < 3; ++r) {
+                    // (W^T a)_r = sum_c W[c][r] a_c
+                    b[r] = W[0 * 3 + r] * a[0] + W[1 * 3 + r] * a[1] + W[2 * 3 + r] * a[2];
+                    if (sg) b[r] = -b[r];
+                }
+                int g = grid_index(b, mesh) - 1;
+                if (g < best) best = g;
+            }
+        }
+        map[i] = best;
+    }
+    // unique_sort: ascending distinct representatives
+    std::vector<int> uniq(map);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    const int nirr = int(uniq.size());
+    for (int k = 0; k < nirr; ++k) {
+        mult[k] = 0;
+        for (int d = 0; d < 3; ++d) irr_q_pnt_int[3 * k + d] = q_pnt_int[3 * uniq[k] + d];
+    }
+    for (int i = 0; i < nq; ++i) {
+        map_out[i] = map[i];
+        int k = int(std::lower_bound(uniq.begin(), uniq.end(), map[i]) - uniq.begin());
+        pos[i] = k + 1;
+        mult[k] += 1;
+    }
+    return nirr;
+}
+
+// ---------------------------------------------------------------------------
+// MomentumConsrv3rd (src/Kappa/Src/QuasiMomentumConsrv3rd_m.f90:13-158),
+// CheckIfWithinBZ (:161-173), Permutation3rd (:176-240).  The count
+// assertions (:148-153) are not applied; counts are returned instead.
+//   q_pnt_int(3,Nq); Allq1q2(4,Nq); q1q2_permuted(2,Nq) (first npairs used)
+//   counts[0] = q1q2_count (pairs), counts[1] = total_count.
+void orc_momentum3(const int* mesh, const int* q_pnt_int, const int* q0_int, int* Allq1q2,
+                   int* q1q2_permuted, int* counts) {
+    const int nq = mesh[0] * mesh[1] * mesh[2];
+    const int sgn[3] = {0, 1, -1};
+    int G[27][3];
+    int gc = 0;
+    for (int c3 = 0; c3 < 3; ++c3)
+        for (int c2 = 0; c2 < 3; ++c2)
+            for (int c1 = 0; c1 < 3; ++c1) {
+                G[gc][0] = sgn[c1] * mesh[0];
+                G[gc][1] = sgn[c2] * mesh[1];
+                G[gc][2] = sgn[c3] * mesh[2];
+                ++gc;
+            }
+    const int bound[3] = {mesh[0] / 2, mesh[1] / 2, mesh[2] / 2};
+    std::vector<char> covered(nq, 0);
+    std::memset(Allq1q2, 0, sizeof(int) * 4 * nq);
+    int cnt = 0, total = 0;
+    for (int i1 = 1; i1 <= nq; ++i1) {
+        const int* q1 = q_pnt_int + 3 * (i1 - 1);
+        int g1 = grid_index(q1, mesh);
+        if (covered[g1 - 1]) continue;
+        bool found = false;
+        int q2[3], g2 = 0;
+        for (int iG = 0; iG < 27; ++iG) {
+            for (int d = 0; d < 3; ++d) q2[d] = G[iG][d] - (q0_int[d] + q1[d]);
+            g2 = grid_index(q2, mesh);
+            bool within = true;
+            for (int d = 0; d < 3; ++d)
+                if (q2[d] > bound[d] || q2[d] < -bound[d]) within = false;
+            if (within && g2 <= nq && g2 >= 1) { found = true; break; }
+        }
+        if (!found) continue;  // reference prints a warning
+        ++cnt;
+        int* a = Allq1q2 + 4 * (g1 - 1);
+        a[0] = 1; a[1] = cnt; a[2] = g1; a[3] = g2;
+        covered[g1 - 1] = 1;
+        ++total;
+        q1q2_permuted[2 * (cnt - 1)] = g1;
+        q1q2_permuted[2 * (cnt - 1) + 1] = g2;
+        // Permutation3rd: per = (2,1); flagged when the swapped integer vectors differ
+        bool differ = (q1[0] != q2[0]) || (q1[1] != q2[1]) || (q1[2] != q2[2]);
+        if (differ) {
+            int* b = Allq1q2 + 4 * (g2 - 1);
+            b[0] = 0; b[1] = cnt; b[2] = g2; b[3] = g1;
+            covered[g2 - 1] = 1;
+            ++total;
+        }
+    }
+    counts[0] = cnt;
+    counts[1] = total;
+}
+
+// ---------------------------------------------------------------------------
+// MomentumConsrv4th (src/Kappa/Src/QuasiMomentumConsrv4th_m.f90:32-206) and
+// Permutation4th (:224-312).  Allq1q2q3(3,Nq,Nq) Fortran = flat
+// [q1][q2][3]; q1q2q3_permuted(3, cap).  Count assertions (:190-200) are not
+// applied.  counts[0] = q1q2q3_count, counts[1] = total_count.
+// Returns -1 when more than `cap` quartets would be written.
+int orc_momentum4(const int* mesh, const int* q_pnt_int, const int* q0_int, int* Allq1q2q3,
+                  int* q1q2q3_permuted, long long cap, long long* counts) {
+    const int nq = mesh[0] * mesh[1] * mesh[2];
+    const int sgn[3] = {0, 1, -1};
+    int G[27][3];
+    int gc = 0;
+    for (int c3 = 0; c3 < 3; ++c3)
+        for (int c2 = 0; c2 < 3; ++c2)
+            for (int c1 = 0; c1 < 3; ++c1) {
+                G[gc][0] = sgn[c1] * mesh[0];
+                G[gc][1] = sgn[c2] * mesh[1];
+                G[gc][2] = sgn[c3] * mesh[2];
+                ++gc;
+            }
+    const int bound[3] = {mesh[0] / 2, mesh[1] / 2, mesh[2] / 2};
+    const int per[5][3] = {{0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
+    std::vector<char> covered((size_t)nq * nq, 0);   // AlreadyCovered(q2, q1) -> [q1][q2]
+    long long cnt = 0, total = 0;
+    for (int i1 = 1; i1 <= nq; ++i1) {
+        const int* q1 = q_pnt_int + 3 * (i1 - 1);
+        int g1 = grid_index(q1, mesh);
+        for (int i2 = 1; i2 <= nq; ++i2) {
+            const int* q2 = q_pnt_int + 3 * (i2 - 1);
+            int g2 = grid_index(q2, mesh);
+            if (covered[(size_t)(g1 - 1) * nq + (g2 - 1)]) continue;
+            bool found = false;
+            int q3[3], g3 = 0;
+            for (int iG = 0; iG < 27; ++iG) {
+                for (int d = 0; d < 3; ++d) q3[d] = G[iG][d] - (q0_int[d] + q1[d] + q2[d]);
+                g3 = grid_index(q3, mesh);
+                bool within = true;
+                for (int d = 0; d < 3; ++d)
+                    if (q3[d] > bound[d] || q3[d] < -bound[d]) within = false;
+                if (within && g3 <= nq && g3 >= 1) { found = true; break; }
+            }
+            if (!found) continue;
+            if (cnt >= cap) return -1;
+            ++cnt;
+            int* a = Allq1q2q3 + 3 * ((size_t)(g1 - 1) * nq + (g2 - 1));
+            a[0] = 0; a[1] = (int)cnt; a[2] = g3;
+            covered[(size_t)(g1 - 1) * nq + (g2 - 1)] = 1;
+            ++total;
+            q1q2q3_permuted[3 * (cnt - 1)] = g1;
+            q1q2q3_permuted[3 * (cnt - 1) + 1] = g2;
+            q1q2q3_permuted[3 * (cnt - 1) + 2] = g3;
+            // Permutation4th
+            const int* ini[3] = {q1, q2, q3};
+            const int gi[3] = {g1, g2, g3};
+            int pg[5][3];
+            for (int pp = 0; pp < 5; ++pp) {
+                for (int k = 0; k < 3; ++k) pg[pp][k] = gi[per[pp][k]];
+                bool nonew = true;
+                for (int k = 0; k < 3; ++k)
+                    for (int d = 0; d < 3; ++d)
+                        if (ini[per[pp][k]][d] != ini[k][d]) nonew = false;
+                for (int qq = 0; qq < pp; ++qq)
+                    nonew = nonew || (pg[pp][0] == pg[qq][0] && pg[pp][1] == pg[qq][1] && pg[pp][2] == pg[qq][2]);
+                if (!nonew) {
+                    int* b = Allq1q2q3 + 3 * ((size_t)(pg[pp][0] - 1) * nq + (pg[pp][1] - 1));
+                    b[0] = pp + 1; b[1] = (int)cnt; b[2] = pg[pp][2];
+                    covered[(size_t)(pg[pp][0] - 1) * nq + (pg[pp][1] - 1)] = 1;
+                    ++total;
+                }
+            }
+        }
+    }
+    counts[0] = cnt;
+    counts[1] = total;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// ScatterProbAllq1 (src/Kappa/Src/ThirdOrder_m.f90:41-166) with ScatterMatEl
+// (:278-386, the reference's 9-deep loop order) and ScatterProbability
+// (:389-439).
+//   fc3: fC(3,3,3,Na3,Na3,Nb); atm_num(Nb); basis_typ(Na3,Nb) 1-based;
+//   atm_pos_r(3,Na3,Nb); onebysqrtmass(Nb);
+//   q_pnt(3,Nq); q_pnt_int(3,Nq); q0_int(3);
+//   evec0(Ndof,Ndof) = Evec(:,:,i0) of the q0 set; oneby0(Ndof);
+//   evec(Ndof,Ndof,Nq), oneby(Ndof,Nq) of the grid;
+//   q1q2_permuted(2,npairs);  Sctrq1(Ndof,Ndof,Ndof,Nq) output (zeroed here).
+void orc_scatter_w3(int nb, int na3, const int* atm_num, const int* basis_typ,
+                    const double* atm_pos_r, const double* fc3, const double* onebysqrtmass,
+                    int nq, const double* q_pnt, const int* q_pnt_int, const int* q0_int,
+                    const double* evec0_ri, const double* oneby0, const double* evec_ri,
+                    const double* oneby, int npairs, const int* q1q2_permuted, double* sctr) {
+    const int ndof = 3 * nb;
+    const size_t n3 = (size_t)ndof * ndof * ndof;
+    const cplx* evec0 = reinterpret_cast<const cplx*>(evec0_ri);
+    const cplx* evec = reinterpret_cast<const cplx*>(evec_ri);
+    std::memset(sctr, 0, sizeof(double) * n3 * nq);
+    const double mfac = Sctr3THz2 / double(nq);
+    const bool g0 = q0_int[0] == 0 && q0_int[1] == 0 && q0_int[2] == 0;
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int ip = 0; ip < npairs; ++ip) {
+        const int g1 = q1q2_permuted[2 * ip], g2 = q1q2_permuted[2 * ip + 1];
+        const int* q1i = q_pnt_int + 3 * (g1 - 1);
+        const int* q2i = q_pnt_int + 3 * (g2 - 1);
+        const double* q1 = q_pnt + 3 * (g1 - 1);
+        const double* q2 = q_pnt + 3 * (g2 - 1);
+        const cplx* e1 = evec + (size_t)(g1 - 1) * ndof * ndof;
+        const cplx* e2 = evec + (size_t)(g2 - 1) * ndof * ndof;
+        int strt[3] = {1, 1, 1};
+        if (g0) strt[0] = 4;
+        if (q1i[0] == 0 && q1i[1] == 0 && q1i[2] == 0) strt[1] = 4;
+        if (q2i[0] == 0 && q2i[1] == 0 && q2i[2] == 0) strt[2] = 4;
+        std::vector<cplx> phi(n3, cplx(0.0, 0.0));  // Phi_ss1s2(s2,s1,s)
+        for (int mu = 1; mu <= nb; ++mu) {
+            const int natm = atm_num[mu - 1];
+            for (int N1 = 1; N1 <= natm; ++N1) {
+                const int nu = basis_typ[(N1 - 1) + na3 * (mu - 1)];
+                const double* R1 = atm_pos_r + 3 * ((N1 - 1) + na3 * (mu - 1));
+                const double qr1 = q1[0] * R1[0] + q1[1] * R1[1] + q1[2] * R1[2];
+                const cplx ex1(std::cos(qr1), std::sin(qr1));
+                for (int N2 = 1; N2 <= natm; ++N2) {
+                    const int eta = basis_typ[(N2 - 1) + na3 * (mu - 1)];
+                    const double* R2 = atm_pos_r + 3 * ((N2 - 1) + na3 * (mu - 1));
+                    const double qr2 = q2[0] * R2[0] + q2[1] * R2[1] + q2[2] * R2[2];
+                    const cplx ex2(std::cos(qr2), std::sin(qr2));
+                    const double mass_fac = onebysqrtmass[mu - 1] * onebysqrtmass[nu - 1] * onebysqrtmass[eta - 1];
+                    const cplx exm = ex1 * ex2 * mass_fac;
+                    for (int al = 1; al <= 3; ++al) {
+                        const int r0 = 3 * (mu - 1) + al;
+                        for (int s = strt[0]; s <= ndof; ++s) {
+                            const cplx w0 = evec0[(r0 - 1) + ndof * (s - 1)];
+                            for (int be = 1; be <= 3; ++be) {
+                                const int r1 = 3 * (nu - 1) + be;
+                                for (int s1 = strt[1]; s1 <= ndof; ++s1) {
+                                    const cplx w1 = e1[(r1 - 1) + ndof * (s1 - 1)];
+                                    for (int ga = 1; ga <= 3; ++ga) {
+                                        const int r2 = 3 * (eta - 1) + ga;
+                                        const size_t fi = (size_t)(ga - 1) + 3 * ((be - 1) + 3 * ((al - 1) +
+                                                          3 * ((N2 - 1) + (size_t)na3 * ((N1 - 1) + (size_t)na3 * (mu - 1)))));
+                                        const cplx pm = fc3[fi] * exm;
+                                        for (int s2 = strt[2]; s2 <= ndof; ++s2) {
+                                            const cplx w2 = e2[(r2 - 1) + ndof * (s2 - 1)];
+                                            phi[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s - 1))] += pm * w0 * w1 * w2;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        // ScatterProbability
+        const double* o0 = oneby0;
+        const double* o1 = oneby + (size_t)(g1 - 1) * ndof;
+        const double* o2 = oneby + (size_t)(g2 - 1) * ndof;
+        double* W1 = sctr + (size_t)(g1 - 1) * n3;
+        double* W2 = sctr + (size_t)(g2 - 1) * n3;
+        std::vector<double> Wp(n3, 0.0), Wd(n3, 0.0);
+        for (int s = strt[0]; s <= ndof; ++s)
+            for (int s1 = strt[1]; s1 <= ndof; ++s1)
+                for (int s2 = strt[2]; s2 <= ndof; ++s2) {
+                    const cplx p = phi[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s - 1))];
+                    const double abs2 = p.real() * p.real() + p.imag() * p.imag();
+                    const double el = abs2 * (o0[s - 1] * o1[s1 - 1] * o2[s2 - 1]);
+                    Wd[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s - 1))] = el * mfac;
+                    Wp[(s1 - 1) + ndof * ((s2 - 1) + (size_t)ndof * (s - 1))] = el * mfac;
+                }
+        std::memcpy(W1, Wd.data(), sizeof(double) * n3);
+        if (g1 != g2) std::memcpy(W2, Wp.data(), sizeof(double) * n3);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// my_sort (src/Kappa/Src/TetrahedronIntegration_m.f90:18-90): ascending sort
+// of the four vertex energies (dlasrt 'I'); equal values take the original
+// vertices in their original order (first uncovered match).
+static void my_sort(double* om, double* F, int* v1, int* v2) {
+    double omc[4], Fc[4];
+    int v1c[4], v2c[4];
+    for (int i = 0; i < 4; ++i) { omc[i] = om[i]; Fc[i] = F[i]; v1c[i] = v1[i]; v2c[i] = v2[i]; }
+    std::sort(om, om + 4);
+    bool covered[4] = {false, false, false, false};
+    for (int ii = 0; ii < 4; ++ii) {
+        int act = -1;
+        for (int k = 0; k < 4; ++k)
+            if (!covered[k] && omc[k] == om[ii]) { act = k; break; }
+        covered[act] = true;
+        v1[ii] = v1c[act]; v2[ii] = v2c[act]; F[ii] = Fc[act];
+    }
+}
+
+// FindgAndIver (TetrahedronIntegration_m.f90:93-218).  `strict` selects the
+// case bounds of the LineWidth/kappa_iter copies (strict '<'/'>' at every
+// bound, src/LineWidth/Src/TetrahedronIntegration_m.f90:113,133,169);
+// kappa.x uses the non-strict form.
+static bool find_g_iver(double Mqs, double* g, double* I, double* M, double* F, int* v1, int* v2,
+                        int strict) {
+    my_sort(M, F, v1, v2);
+    bool c1, c2, c3;
+    if (!strict) {
+        c1 = (Mqs >= M[0]) && (Mqs < M[1]);
+        c2 = (Mqs >= M[1]) && (Mqs < M[2]);
+        c3 = (Mqs >= M[2]) && (Mqs <= M[3]);
+    } else {
+        c1 = (Mqs > M[0]) && (Mqs < M[1]);
+        c2 = (Mqs > M[1]) && (Mqs < M[2]);
+        c3 = (Mqs > M[2]) && (Mqs < M[3]);
+    }
+    if (c1) {
+        *g = (3.0 * ((Mqs - M[0]) * (Mqs - M[0]))) / ((M[1] - M[0]) * (M[2] - M[0]) * (M[3] - M[0]));
+        I[0] = (((Mqs - M[1]) / (M[0] - M[1])) + ((Mqs - M[2]) / (M[0] - M[2])) +
+                ((Mqs - M[3]) / (M[0] - M[3]))) / 3.0;
+        for (int v = 1; v < 4; ++v) I[v] = ((Mqs - M[0]) / (M[v] - M[0])) / 3.0;
+        return true;
+    } else if (c2) {
+        const double gg = (3.0 / ((M[1] - M[2]) * (M[3] - M[0]))) *
+                          ((((Mqs - M[0]) * (Mqs - M[2])) / (M[2] - M[0])) -
+                           (((Mqs - M[1]) * (Mqs - M[3])) / (M[1] - M[3])));
+        *g = gg;
+        const double den = gg * (M[3] - M[0]);
+        I[0] = (((Mqs - M[3]) / (M[0] - M[3])) / 3.0) +
+               ((((Mqs - M[2]) / (M[0] - M[2])) * ((Mqs - M[0]) / (M[2] - M[0])) *
+                 ((Mqs - M[2]) / (M[1] - M[2]))) / den);
+        const double t1 = (Mqs - M[3]) / (M[1] - M[3]);
+        I[1] = (((Mqs - M[2]) / (M[1] - M[2])) / 3.0) + (((t1 * t1) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
+        const double t2 = (Mqs - M[0]) / (M[2] - M[0]);
+        I[2] = (((Mqs - M[1]) / (M[2] - M[1])) / 3.0) + (((t2 * t2) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
+        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) / 3.0) +
+               ((((Mqs - M[1]) / (M[3] - M[1])) * ((Mqs - M[3]) / (M[1] - M[3])) *
+                 ((Mqs - M[1]) / (M[2] - M[1]))) / den);
+        return true;
+    } else if (c3) {
+        *g = (3.0 * ((Mqs - M[3]) * (Mqs - M[3]))) / ((M[3] - M[0]) * (M[3] - M[1]) * (M[3] - M[2]));
+        for (int v = 0; v < 3; ++v) I[v] = ((Mqs - M[3]) / (M[v] - M[3])) / 3.0;
+        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) + ((Mqs - M[1]) / (M[3] - M[1])) +
+                ((Mqs - M[2]) / (M[3] - M[2]))) / 3.0;
+        return true;
+    }
+    *g = 0.0;
+    for (int v = 0; v < 4; ++v) I[v] = 0.0;
+    return false;
+}
+
+static double iver_x_fver(const double* I, const double* F, bool enter) {
+    double s = 0.0;
+    if (enter)
+        for (int v = 0; v < 4; ++v) s += I[v] * F[v];
+    return OnebySix * s;
+}
+
+// Exposed for known-answer tests of the tetrahedron weights.
+int orc_find_g_iver(double Mqs, const double* M_in, const double* F_in, int strict, double* g_out,
+                    double* I_out, double* M_sorted, double* F_sorted, int* perm) {
+    double M[4], F[4];
+    int v1[4] = {1, 2, 3, 4}, v2[4] = {1, 2, 3, 4};
+    for (int i = 0; i < 4; ++i) { M[i] = M_in[i]; F[i] = F_in[i]; }
+    bool e = find_g_iver(Mqs, g_out, I_out, M, F, v1, v2, strict);
+    for (int i = 0; i < 4; ++i) { M_sorted[i] = M[i]; F_sorted[i] = F[i]; perm[i] = v1[i]; }
+    return e ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// CalculateLwTetrahedron (src/Kappa/Src/ThirdOrder_m.f90:169-275) with
+// FindFandOmegaAtVertices (TetrahedronIntegration_m.f90:259-295).
+//   omega0(Ndof) of q0; omega(Ndof,Nq), nbe(Ndof,Nq) of the grid (one T);
+//   sctr(Ndof,Ndof,Ndof,Nq); tetra(4,6Nq); Allq1q2(4,Nq); pol(2,3) 1-based.
+//   lw(Ndof), P3_q0(Ndof), *P3.
+void orc_lw3_tetra(int ndof, int nq, const double* omega0, const double* omega, const double* nbe,
+                   const double* sctr, const int* tetra, const int* Allq1q2, const int* pol,
+                   double* lw, double* P3_q0, double* P3) {
+    const size_t n3 = (size_t)ndof * ndof * ndof;
+    const int ntet = 6 * nq;
+    for (int s = 0; s < ndof; ++s) { lw[s] = 0.0; P3_q0[s] = 0.0; }
+    std::vector<double> p3s(ndof, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s0 = pol[0]; s0 <= pol[1]; ++s0) {
+        const double Mqs = omega0[s0 - 1];
+        double lws = 0.0, p3 = 0.0;
+        for (int nT = 0; nT < ntet; ++nT) {
+            int tv1[4], tv2[4];
+            for (int v = 0; v < 4; ++v) {
+                tv1[v] = tetra[4 * nT + v];
+                tv2[v] = Allq1q2[4 * (tv1[v] - 1) + 3];
+            }
+            for (int s1 = pol[2]; s1 <= pol[3]; ++s1)
+                for (int s2 = pol[4]; s2 <= pol[5]; ++s2) {
+                    double F1[4], F2[4], F3[4], M1[4], M2[4], M3[4];
+                    for (int v = 0; v < 4; ++v) {
+                        const int a = tv1[v] - 1, b = tv2[v] - 1;
+                        const double W = sctr[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s0 - 1)) + n3 * a];
+                        const double n1 = nbe[(s1 - 1) + (size_t)ndof * a];
+                        const double n2 = nbe[(s2 - 1) + (size_t)ndof * b];
+                        F1[v] = W * (n1 + n2 + 1.0);
+                        F2[v] = W * (n1 - n2);
+                        const double o1 = omega[(s1 - 1) + (size_t)ndof * a];
+                        const double o2 = omega[(s2 - 1) + (size_t)ndof * b];
+                        M1[v] = o1 + o2;
+                        M2[v] = o2 - o1;
+                        M3[v] = o1 - o2;
+                    }
+                    for (int v = 0; v < 4; ++v) F3[v] = F2[v];
+                    double g, I[4];
+                    int a1[4], a2[4];
+                    bool e;
+                    std::memcpy(a1, tv1, sizeof a1); std::memcpy(a2, tv2, sizeof a2);
+                    e = find_g_iver(Mqs, &g, I, M1, F1, a1, a2, 0);
+                    lws += g * iver_x_fver(I, F1, e); p3 += g;
+                    std::memcpy(a1, tv1, sizeof a1); std::memcpy(a2, tv2, sizeof a2);
+                    e = find_g_iver(Mqs, &g, I, M2, F2, a1, a2, 0);
+                    lws += g * iver_x_fver(I, F2, e); p3 += g;
+                    std::memcpy(a1, tv1, sizeof a1); std::memcpy(a2, tv2, sizeof a2);
+                    e = find_g_iver(Mqs, &g, I, M3, F3, a1, a2, 0);
+                    lws -= g * iver_x_fver(I, F3, e); p3 += g;
+                }
+        }
+        lw[s0 - 1] = lws;
+        P3_q0[s0 - 1] = p3;
+    }
+    double t = 0.0;
+    for (int s = 0; s < ndof; ++s) t += P3_q0[s];
+    *P3 = t;
+}
+
+// ---------------------------------------------------------------------------
+// Gaussian linewidth: CalculateLinewidth (src/Kappa/Src/ThirdOrder_m.f90:442-543)
+// with the branch start reset per q1 (the reference leaves strt(2)/strt(3) at 4
+// after the first Gamma point, :483,500,509; W is zero for Gamma acoustic modes
+// anyway, :413-437) and the polarisation window of CalculateLwTetrahedron.
+//   Also returns the Gaussian phase space P3_q0(s0) = sum (d1+d2+d3).
+void orc_lw3_gauss(int ndof, int nq, const double* omega0, const double* omega, const double* nbe,
+                   const double* sctr, const int* Allq1q2, const int* q_pnt_int, const int* pol,
+                   double sigma, double* lw, double* P3_q0) {
+    const size_t n3 = (size_t)ndof * ndof * ndof;
+    const double os = 1.0 / sigma, os2 = os * os;
+    for (int s = 0; s < ndof; ++s) { lw[s] = 0.0; P3_q0[s] = 0.0; }
+    for (int q1 = 0; q1 < nq; ++q1) {
+        const int q2 = Allq1q2[4 * q1 + 3] - 1;
+        const int* a = q_pnt_int + 3 * q1;
+        const int* b = q_pnt_int + 3 * q2;
+        const int st1 = (a[0] == 0 && a[1] == 0 && a[2] == 0) ? 4 : 1;
+        const int st2 = (b[0] == 0 && b[1] == 0 && b[2] == 0) ? 4 : 1;
+        for (int s0 = pol[0]; s0 <= pol[1]; ++s0) {
+            double acc = 0.0, ps = 0.0;
+            for (int s1 = std::max(st1, pol[2]); s1 <= pol[3]; ++s1)
+                for (int s2 = std::max(st2, pol[4]); s2 <= pol[5]; ++s2) {
+                    const double o0 = omega0[s0 - 1];
+                    const double o1 = omega[(s1 - 1) + (size_t)ndof * q1];
+                    const double o2 = omega[(s2 - 1) + (size_t)ndof * q2];
+                    const double n1 = nbe[(s1 - 1) + (size_t)ndof * q1];
+                    const double n2 = nbe[(s2 - 1) + (size_t)ndof * q2];
+                    const double d1 = o0 - o1 - o2, d2 = o0 + o1 - o2, d3 = o0 - o1 + o2;
+                    const double e1 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d1 * d1));
+                    const double e2 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d2 * d2));
+                    const double e3 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d3 * d3));
+                    const double W = sctr[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s0 - 1)) + n3 * q1];
+                    acc += W * (((n1 + n2 + 1.0) * e1) + ((n1 - n2) * (e2 - e3)));
+                    ps += e1 + e2 + e3;
+                }
+            lw[s0 - 1] += acc;
+            P3_q0[s0 - 1] += ps;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// CalculateIsoW (src/Kappa/Src/IsotopicScatter.f90:36-94):
+//   W_iso(Ndof,Ndof,Nq) = (s1, s0, q1)
+void orc_iso_w(int nb, int nq, const double* evec0_ri, const double* omega0, const double* evec_ri,
+               const double* g2iso, double* w_iso) {
+    const int ndof = 3 * nb;
+    const cplx* e0 = reinterpret_cast<const cplx*>(evec0_ri);
+    const cplx* ev = reinterpret_cast<const cplx*>(evec_ri);
+#pragma omp parallel for
+    for (int q1 = 0; q1 < nq; ++q1)
+        for (int s0 = 0; s0 < ndof; ++s0) {
+            const double M = omega0[s0];
+            for (int s1 = 0; s1 < ndof; ++s1) {
+                double acc = 0.0;
+                for (int b = 0; b < nb; ++b) {
+                    cplx d(0.0, 0.0);
+                    for (int c = 0; c < 3; ++c)
+                        d += std::conj(ev[(3 * b + c) + ndof * s1 + (size_t)ndof * ndof * q1]) * e0[(3 * b + c) + ndof * s0];
+                    acc += g2iso[b] * (d.real() * d.real() + d.imag() * d.imag());
+                }
+                w_iso[s1 + ndof * s0 + (size_t)ndof * ndof * q1] = acc * PI * (M * M) * 0.5 / double(nq);
+            }
+        }
+}
+
+// CalculateIsoLwTetra (IsotopicScatter.f90:97-168): NaN g / I set to zero.
+void orc_iso_lw_tetra(int ndof, int nq, const double* omega0, const double* omega, const double* w_iso,
+                      const int* tetra, double* lw) {
+    const int ntet = 6 * nq;
+#pragma omp parallel for
+    for (int s0 = 0; s0 < ndof; ++s0) {
+        const double Mqs = omega0[s0];
+        double acc = 0.0;
+        for (int nT = 0; nT < ntet; ++nT) {
+            const int* tv = tetra + 4 * nT;
+            for (int s1 = 0; s1 < ndof; ++s1) {
+                double F[4], M[4], I[4], g;
+                int a1[4], a2[4];
+                for (int v = 0; v < 4; ++v) {
+                    const int q = tv[v] - 1;
+                    F[v] = w_iso[s1 + ndof * s0 + (size_t)ndof * ndof * q];
+                    M[v] = omega[s1 + (size_t)ndof * q];
+                    a1[v] = a2[v] = tv[v];
+                }
+                bool e = find_g_iver(Mqs, &g, I, M, F, a1, a2, 0);
+                for (int v = 0; v < 4; ++v) if (std::isnan(I[v])) I[v] = 0.0;
+                if (std::isnan(g)) g = 0.0;
+                acc += g * iver_x_fver(I, F, e);
+            }
+        }
+        lw[s0] = acc;
+    }
+}
+
+// Gaussian isotope scattering rate: sum_q1,s1 W_iso delta(omega0 - omega1)
+// (build-side Gaussian form of CalculateIsoLwTetra; same units).
+void orc_iso_lw_gauss(int ndof, int nq, const double* omega0, const double* omega, const double* w_iso,
+                      double sigma, double* lw) {
+    const double os = 1.0 / sigma, os2 = os * os;
+    for (int s0 = 0; s0 < ndof; ++s0) {
+        double acc = 0.0;
+        for (int q = 0; q < nq; ++q)
+            for (int s1 = 0; s1 < ndof; ++s1) {
+                const double d = omega0[s0] - omega[s1 + (size_t)ndof * q];
+                acc += w_iso[s1 + ndof * s0 + (size_t)ndof * ndof * q] * os * Onebysqrt2PI * std::exp(-0.5 * os2 * d * d);
+            }
+        lw[s0] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// GrVelKronProdSymm (src/Kappa/Src/VelocityKronProd_symm.f90:34-91)
+//   grp_vel(3,Ndof,Nq0); Rxyz(3,3,Nsym) column-major; mult(Nq0);
+//   out KrnGrpVelSym(9,Ndof,Nq0) in kron_prod order (Helper_m.f90:670-697).
+void orc_velkron_symm(int ndof, int nq0, const double* grp_vel, int nsym, const double* Rxyz,
+                      const int* mult, double* krn) {
+    for (int q = 0; q < nq0; ++q) {
+        const double p = 1.0 / double(nsym / mult[q]);
+        for (int s = 0; s < ndof; ++s) {
+            const double* vg = grp_vel + 3 * (s + (size_t)ndof * q);
+            double acc[9] = {0};
+            for (int ns = 0; ns < nsym; ++ns) {
+                const double* R = Rxyz + 9 * ns;
+                double rv[3];
+                for (int i = 0; i < 3; ++i) rv[i] = R[i] * vg[0] + R[i + 3] * vg[1] + R[i + 6] * vg[2];
+                for (int i = 0; i < 3; ++i)
+                    for (int j = 0; j < 3; ++j) acc[3 * i + j] += rv[i] * rv[j];
+            }
+            for (int k = 0; k < 9; ++k) krn[k + 9 * (s + (size_t)ndof * q)] = acc[k] * p;
+        }
+    }
+}
+
+// kappa_noIter_symm (src/Kappa/Src/ThermalConductivity.f90:167-292):
+//   sum over irreducible q0 with symmetrised v (x) v.  mode_k(9,Ndof) optional.
+void orc_kappa_symm(int ndof, int nq, int nq0, const int* irr_q_pnt_int, const double* omega0,
+                    const double* nbe0, const double* lw, const double* krn, int s_first, int s_last,
+                    double vol, double T, double kw_m_k, double* kappa, double* mode_k) {
+    const double f1 = kw_m_k / ((T * T) * vol);
+    const double f2 = f1 / double(nq);
+    for (int k = 0; k < 9; ++k) kappa[k] = 0.0;
+    if (mode_k) for (int k = 0; k < 9 * ndof; ++k) mode_k[k] = 0.0;
+    for (int q = 0; q < nq0; ++q) {
+        const int* a = irr_q_pnt_int + 3 * q;
+        int strt = s_first;
+        if (a[0] == 0 && a[1] == 0 && a[2] == 0) strt = 4;
+        for (int s = strt; s <= s_last; ++s) {
+            const double om = omega0[(s - 1) + (size_t)ndof * q];
+            const double n = nbe0[(s - 1) + (size_t)ndof * q];
+            const double tau = 0.5 / lw[(s - 1) + (size_t)ndof * q];
+            const double pre = (om * om) * n * (n + 1.0) * tau;
+            for (int k = 0; k < 9; ++k) {
+                const double kq = pre * krn[k + 9 * ((s - 1) + (size_t)ndof * q)];
+                kappa[k] += kq;
+                if (mode_k) mode_k[k + 9 * (s - 1)] += kq;
+            }
+        }
+    }
+    for (int k = 0; k < 9; ++k) kappa[k] *= f2;
+    if (mode_k) for (int k = 0; k < 9 * ndof; ++k) mode_k[k] *= f2;
+}
+
+// kappa_noIter (ThermalConductivity.f90:36-164): full grid, v (x) v per q.
+void orc_kappa_full(int ndof, int nq, const int* q_pnt_int, const int* pos, const double* omega,
+                    const double* nbe, const double* grp_vel, const double* lw, int s_first, int s_last,
+                    double vol, double T, double kw_m_k, double* kappa) {
+    const double f1 = kw_m_k / ((T * T) * vol);
+    const double f2 = f1 / double(nq);
+    for (int k = 0; k < 9; ++k) kappa[k] = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        const int* a = q_pnt_int + 3 * q;
+        int strt = s_first;
+        if (a[0] == 0 && a[1] == 0 && a[2] == 0) strt = 4;
+        const int ip = pos[q] - 1;
+        for (int s = strt; s <= s_last; ++s) {
+            const double om = omega[(s - 1) + (size_t)ndof * q];
+            const double n = nbe[(s - 1) + (size_t)ndof * q];
+            const double* v = grp_vel + 3 * ((s - 1) + (size_t)ndof * q);
+            const double tau = 0.5 / lw[(s - 1) + (size_t)ndof * ip];
+            const double pre = (om * om) * n * (n + 1.0) * tau;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) kappa[3 * i + j] += pre * v[i] * v[j];
+        }
+    }
+    for (int k = 0; k < 9; ++k) kappa[k] *= f2;
+}
+
+int orc_num_threads() {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

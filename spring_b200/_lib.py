@@ -1,0 +1,82 @@
+"""ctypes binding of libspring_b200.so (the C ABI declared in include/spring_gpu.h).
+
+There is no fallback: if the library is missing or cannot be loaded, importing
+the bindings raises.  Build it with ``python -m spring_b200.build``.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libspring_b200.so")
+
+SPRING_OK = 0
+SPRING_ERR_ARG = 1
+SPRING_ERR_STATE = 2
+SPRING_ERR_CUDA = 3
+SPRING_ERR_ALLOC = 4
+SPRING_ERR_UNSUPPORTED = 5
+SPRING_ERR_INJECTED = 6
+SPRING_DELTA_GAUSS = 0
+SPRING_DELTA_TETRA = 1
+
+
+class spring_dims(ct.Structure):
+    _fields_ = [("nbasis", ct.c_int), ("mesh", ct.c_int * 3), ("n_temps", ct.c_int), ("device", ct.c_int)]
+
+
+P = ct.c_void_p
+I = ct.c_int
+D = ct.c_double
+
+# name -> argtypes (every function returns int unless listed in _RESTYPE)
+SIGNATURES = {
+    "spring_ctx_create": [ct.POINTER(P), ct.POINTER(spring_dims)],
+    "spring_ctx_destroy": [P],
+    "spring_last_error": [P],
+    "spring_set_stream": [P, P],
+    "spring_synchronize": [P],
+    "spring_kernel_launches": [P, P],
+    "spring_set_crystal": [P, P, P],
+    "spring_set_fc2": [P, I, P, P, P],
+    "spring_set_fc3": [P, I, P, P, P],
+    "spring_make_mesh": [P, P, I, P, P, P],
+    "spring_find_irr_q": [P, I, P, I, P, P, P, P],
+    "spring_compute_phonons": [P, P, D],
+    "spring_set_phonons": [P, I, P, P, P, P, P, P],
+    "spring_get_phonons": [P, I, P, P, P, P, P],
+    "spring_enumerate3": [P, I, P, P, P],
+    "spring_scatter_w3": [P, I, P],
+    "spring_linewidth3": [P, I, I, I, D, P, P, P],
+    "spring_linewidth_iso": [P, I, I, I, D, P, P],
+    "spring_reset_linewidths": [P],
+    "spring_get_linewidths": [P, P],
+    "spring_set_linewidths": [P, P],
+    "spring_kappa_rta": [P, I, I, P, P, P, P],
+    "spring_debug_inject_fault": [P, I, I],
+}
+_RESTYPE = {"spring_last_error": ct.c_char_p}
+
+_lib = None
+
+
+def load():
+    """Load the library once; raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m spring_b200.build` "
+                          "(there is no CPU fallback)")
+    lib = ct.CDLL(LIB_PATH)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPE.get(name, ct.c_int)
+    _lib = lib
+    return lib
+
+
+def exported_symbols() -> list[str]:
+    return list(SIGNATURES)

@@ -1,0 +1,237 @@
+"""Host-side interface of the B200 path, mirroring SPRING's kappa.x procedures.
+
+Each method of :class:`Context` wraps one C-ABI entry point of
+``libspring_b200.so`` and names the reference procedure it replaces.  Arrays
+are numpy arrays whose memory is the reference's Fortran array (C-order with
+the Fortran axes reversed), e.g. ``Allq1q2(4,Nq)`` is returned as shape
+``(Nq, 4)``.  Indices crossing the boundary are 1-based like the reference's.
+Errors raise :class:`SpringError` with the library's message.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+
+from . import _lib as L
+
+
+class SpringError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"spring error {code}: {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(ct.c_void_p)
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class Context:
+    """One ``spring_ctx``: a crystal, a q-mesh and a list of temperatures on one GPU."""
+
+    def __init__(self, nbasis: int, mesh, n_temps: int = 1, device: int = -1):
+        self._lib = L.load()
+        d = L.spring_dims()
+        d.nbasis = int(nbasis)
+        for k in range(3):
+            d.mesh[k] = int(mesh[k])
+        d.n_temps = int(n_temps)
+        d.device = int(device)
+        h = ct.c_void_p()
+        rc = self._lib.spring_ctx_create(ct.byref(h), ct.byref(d))
+        if rc != 0:
+            raise SpringError(rc, "spring_ctx_create failed")
+        self._h = h
+        self.nbasis = int(nbasis)
+        self.ndof = 3 * self.nbasis
+        self.mesh = tuple(int(m) for m in mesh)
+        self.nq = int(np.prod(self.mesh))
+        self.n_temps = int(n_temps)
+        self.nq0 = None
+
+    # -- plumbing
+    def _call(self, name, *args):
+        rc = getattr(self._lib, name)(self._h, *args)
+        if rc != 0:
+            msg = self._lib.spring_last_error(self._h)
+            raise SpringError(rc, (msg or b"").decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.spring_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        self._call("spring_set_stream", ct.c_void_p(stream_ptr) if stream_ptr else None)
+
+    def synchronize(self):
+        self._call("spring_synchronize")
+
+    def kernel_launches(self) -> int:
+        n = ct.c_longlong()
+        self._call("spring_kernel_launches", ct.byref(n))
+        return int(n.value)
+
+    def inject_fault(self, kind: int, n: int):
+        self._call("spring_debug_inject_fault", int(kind), int(n))
+
+    # -- cell%init_data / FC readers
+    def set_crystal(self, latvec, mass):
+        lat = _c(np.asarray(latvec).T, np.float64)  # Fortran latvec(3,3): columns are vectors
+        self._call("spring_set_crystal", _ptr(lat), _ptr(_c(mass, np.float64)))
+
+    def set_fc2(self, atm_num, atm_indx, fc2):
+        na = int(np.asarray(atm_indx).shape[1])
+        self._call("spring_set_fc2", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),
+                   _ptr(_c(fc2, np.float64)))
+
+    def set_fc3(self, atm_num, atm_indx, fc3):
+        na = int(np.asarray(atm_indx).shape[1])
+        self._call("spring_set_fc3", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),
+                   _ptr(_c(fc3, np.float64)))
+
+    # -- q_tetrahedron
+    def make_mesh(self, shift=(0, 0, 0), zero_centered=True, want=True):
+        sh = _c(shift, np.int32)
+        if not want:
+            self._call("spring_make_mesh", _ptr(sh), int(zero_centered), None, None, None)
+            return None
+        qi = np.zeros((self.nq, 3), np.int32)
+        qf = np.zeros((self.nq, 3), np.float64)
+        tet = np.zeros((6 * self.nq, 4), np.int32)
+        self._call("spring_make_mesh", _ptr(sh), int(zero_centered), _ptr(qi), _ptr(qf), _ptr(tet))
+        return qi, qf, tet
+
+    def find_irr_q(self, rotations, time_rev=0):
+        rot = _c(rotations, np.int32)  # (nrot, 3, 3) row-major W
+        nq0 = ct.c_int()
+        irr = np.zeros((self.nq, 3), np.int32)
+        pos = np.zeros(self.nq, np.int32)
+        mult = np.zeros(self.nq, np.int32)
+        self._call("spring_find_irr_q", int(rot.shape[0]), _ptr(rot), int(time_rev), ct.byref(nq0), _ptr(irr),
+                   _ptr(pos), _ptr(mult))
+        self.nq0 = int(nq0.value)
+        return dict(irr_q_pnt_int=irr[: self.nq0].copy(), pos=pos, multiplicity=mult[: self.nq0].copy())
+
+    # -- Phon
+    def compute_phonons(self, temps, freq_cut=2.56789e-5):
+        self._call("spring_compute_phonons", _ptr(_c(temps, np.float64)), float(freq_cut))
+
+    def set_phonons(self, which: int, temps, ph: dict):
+        self._call("spring_set_phonons", int(which), _ptr(_c(temps, np.float64)), _ptr(_c(ph["evec"], np.complex128)),
+                   _ptr(_c(ph["omega"], np.float64)), _ptr(_c(ph["onebyomega"], np.float64)),
+                   _ptr(_c(ph["nbe"], np.float64)), _ptr(_c(ph["grp_vel"], np.float64)))
+
+    def get_phonons(self, which: int) -> dict:
+        n = self.nq if which == 0 else self.nq0
+        nd = self.ndof
+        out = dict(evec=np.zeros((n, nd, nd), np.complex128), omega=np.zeros((n, nd)), onebyomega=np.zeros((n, nd)),
+                   nbe=np.zeros((self.n_temps, n, nd)), grp_vel=np.zeros((n, nd, 3)))
+        self._call("spring_get_phonons", int(which), _ptr(out["evec"]), _ptr(out["omega"]), _ptr(out["onebyomega"]),
+                   _ptr(out["nbe"]), _ptr(out["grp_vel"]))
+        return out
+
+    # -- MomentumConsrv3rd
+    def enumerate3(self, i0: int):
+        A = np.zeros((self.nq, 4), np.int32)
+        Pm = np.zeros((self.nq, 2), np.int32)
+        cnt = np.zeros(2, np.int32)
+        self._call("spring_enumerate3", int(i0), _ptr(A), _ptr(Pm), _ptr(cnt))
+        return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
+
+    # -- ScatterProbAllq1
+    def scatter_w3(self, i0: int):
+        nd = self.ndof
+        out = np.zeros((self.nq, nd, nd, nd))
+        self._call("spring_scatter_w3", int(i0), _ptr(out))
+        return out
+
+    # -- linewidths
+    def linewidth3(self, i0_first: int, n_q0: int, delta: str = "gauss", sigma: float = 0.3767, pol3=None,
+                   want=True):
+        mode = L.SPRING_DELTA_GAUSS if delta == "gauss" else L.SPRING_DELTA_TETRA
+        pol = None if pol3 is None else _c(pol3, np.int32)
+        if not want:
+            self._call("spring_linewidth3", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), None, None)
+            return None
+        lw = np.zeros((self.n_temps, n_q0, self.ndof))
+        p3 = np.zeros((n_q0, self.ndof))
+        self._call("spring_linewidth3", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), _ptr(lw), _ptr(p3))
+        return lw, p3
+
+    def linewidth_iso(self, i0_first: int, n_q0: int, g2, delta: str = "gauss", sigma: float = 0.3767, want=True):
+        mode = L.SPRING_DELTA_GAUSS if delta == "gauss" else L.SPRING_DELTA_TETRA
+        g = _c(g2, np.float64)
+        if not want:
+            self._call("spring_linewidth_iso", int(i0_first), int(n_q0), mode, float(sigma), _ptr(g), None)
+            return None
+        rate = np.zeros((self.n_temps, n_q0, self.ndof))
+        self._call("spring_linewidth_iso", int(i0_first), int(n_q0), mode, float(sigma), _ptr(g), _ptr(rate))
+        return rate
+
+    def reset_linewidths(self):
+        self._call("spring_reset_linewidths")
+
+    def get_linewidths(self):
+        out = np.zeros((self.n_temps, self.nq0, self.ndof))
+        self._call("spring_get_linewidths", _ptr(out))
+        return out
+
+    def set_linewidths(self, lw):
+        self._call("spring_set_linewidths", _ptr(_c(lw, np.float64)))
+
+    # -- kappa_noIter(_symm)
+    def kappa_rta(self, Rxyz=None, symm=True, s_range=None, mode=False):
+        R = None
+        nsym = 0
+        if symm:
+            R = _c(np.transpose(np.asarray(Rxyz), (0, 2, 1)), np.float64)  # Rxyz(3,3,Nsym) column-major
+            nsym = R.shape[0]
+        sr = None if s_range is None else _c(s_range, np.int32)
+        kap = np.zeros((self.n_temps, 9))
+        mk = np.zeros((self.n_temps, self.ndof, 9)) if mode else None
+        self._call("spring_kappa_rta", int(bool(symm)), nsym, _ptr(R), _ptr(sr), _ptr(kap), _ptr(mk))
+        return (kap, mk) if mode else kap
+
+
+def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True):
+    """A ready context for a :class:`spring_b200.synthetic.Crystal`.
+
+    ``phonons="device"`` computes them with the device eigensolver; a dict
+    ``{"grid": ph, "irr": ph}`` loads host-computed ones instead.
+    Returns ``(ctx, info)`` where ``info`` holds the mesh and irreducible set.
+    """
+    from . import synthetic as S
+    temps = np.atleast_1d(np.asarray(temps, np.float64))
+    ctx = Context(cr.nbasis, mesh, len(temps))
+    ctx.set_crystal(cr.latvec, cr.mass)
+    ctx.set_fc2(cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
+    if with_fc3:
+        ctx.set_fc3(cr.fc3_atm_num, cr.fc3_atm_indx, cr.fc3)
+    qi, qf, tet = ctx.make_mesh()
+    if W is None:
+        W, Rxyz = S.point_group(cr)
+    irr = ctx.find_irr_q(W)
+    if isinstance(phonons, dict):
+        ctx.set_phonons(0, temps, phonons["grid"])
+        ctx.set_phonons(1, temps, phonons["irr"])
+    else:
+        ctx.compute_phonons(temps)
+    info = dict(q_pnt_int=qi, q_pnt=qf, tetra=tet, W=W, Rxyz=Rxyz, temps=temps, **irr)
+    return ctx, info

@@ -1,0 +1,653 @@
+// C-ABI entry points of libspring_b200.so: context, inputs, orchestration.
+// Kernels live in k_*.cu; this file validates arguments, owns device memory
+// and sequences the launches on the context's stream.
+#include <cstdarg>
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include <new>
+
+#include "spring_internal.cuh"
+
+using namespace spring;
+
+namespace spring {
+
+HostConst host_constants() {
+    HostConst k;
+    const double pi = 4.0 * std::atan(1.0);
+    k.wTHz = std::sqrt(1.60217733 * 6.02214076 * 10.0) * 10.0;
+    k.vg_ms = k.wTHz * 100.0;
+    k.BEConv = std::sqrt(1.60217733 * 6.02214076 * 10.0) * 6.582119569 * 100.0 / 8.617333262;
+    k.Sctr3THz2 = 1.054571817 * (1.60217733 * 1.60217733) * (6.02214076 * 6.02214076 * 6.02214076) * 1000000.0 *
+                  pi * 0.0625;
+    const double hb = 1.054571817 * 1.602176565;
+    const double na = 6.022140857;
+    k.Sctr4THz2 = 0.125 * pi * (hb * hb) * (na * na * na * na) * 1000000.0;
+    k.kW_m_k = (1.054571817 * 1.054571817) * 0.001 / 1.380649;
+    return k;
+}
+
+int fail(spring_ctx* c, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+int cuda_fail(spring_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, SPRING_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+static bool injected(spring_ctx* c, int kind) {
+    if (c->inject_kind != kind || c->inject_n <= 0) return false;
+    c->inject_seen[kind] += 1;
+    if (c->inject_seen[kind] == c->inject_n) {
+        c->inject_kind = -1;
+        return true;
+    }
+    return false;
+}
+
+int dalloc_bytes(spring_ctx* c, void** p, size_t bytes, const char* what) {
+    if (injected(c, 0)) return fail(c, SPRING_ERR_INJECTED, "%s: injected allocation failure", what);
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(c, SPRING_ERR_ALLOC, "%s: cudaMalloc(%zu bytes) failed: %s", what, bytes, cudaGetErrorString(e));
+    }
+    return SPRING_OK;
+}
+
+int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
+    if (injected(c, 1)) return fail(c, SPRING_ERR_INJECTED, "%s: injected copy failure", what);
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
+    if (injected(c, 1)) return fail(c, SPRING_ERR_INJECTED, "%s: injected copy failure", what);
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+int zero(spring_ctx* c, void* dst, size_t bytes, const char* what) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, c->stream);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+bool launch_injected(spring_ctx* c) { return injected(c, 2); }
+
+int launch_check(spring_ctx* c, const char* what) {
+    c->launches += 1;
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+}  // namespace spring
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+#define CTX_ENTER(ctx)                                                     \
+    if (!(ctx)) return SPRING_ERR_ARG;                                      \
+    DeviceGuard _guard((ctx)->device);                                      \
+    (ctx)->err.clear()
+
+int need(spring_ctx* c, bool ok, const char* what) {
+    return ok ? SPRING_OK : fail(c, SPRING_ERR_STATE, "%s has not been set", what);
+}
+
+void free_phonons(Phonons& p) {
+    dfree(p.evec); dfree(p.omega); dfree(p.oneby); dfree(p.nbe); dfree(p.vel);
+    p.set = false;
+}
+
+int alloc_phonons(spring_ctx* c, Phonons& p, int n) {
+    p.n = n;
+    const size_t nd = c->ndof;
+    SPRING_CHECK(dalloc(c, p.evec, (size_t)n * nd * nd, "phonon eigenvectors"));
+    SPRING_CHECK(dalloc(c, p.omega, (size_t)n * nd, "phonon omega"));
+    SPRING_CHECK(dalloc(c, p.oneby, (size_t)n * nd, "phonon 1/omega"));
+    SPRING_CHECK(dalloc(c, p.nbe, (size_t)c->nT * n * nd, "phonon nBE"));
+    SPRING_CHECK(dalloc(c, p.vel, (size_t)n * nd * 3, "phonon velocity"));
+    return SPRING_OK;
+}
+
+int set_temps(spring_ctx* c, const double* temps) {
+    if (!temps) return fail(c, SPRING_ERR_ARG, "temps is NULL");
+    for (int i = 0; i < c->nT; ++i)
+        if (!(temps[i] > 0.0)) return fail(c, SPRING_ERR_ARG, "temperature %d is not positive", i + 1);
+    c->temps.assign(temps, temps + c->nT);
+    SPRING_CHECK(dalloc(c, c->d_temps, c->nT, "temperatures"));
+    return h2d(c, c->d_temps.p, temps, sizeof(double) * c->nT, "temperatures");
+}
+
+Pol make_pol(spring_ctx* c, const int* pol3) {
+    Pol p;
+    for (int k = 0; k < 3; ++k) {
+        p.lo[k] = pol3 ? pol3[2 * k] - 1 : 0;
+        p.hi[k] = pol3 ? pol3[2 * k + 1] - 1 : c->ndof - 1;
+    }
+    return p;
+}
+
+int check_pol(spring_ctx* c, const int* pol3) {
+    if (!pol3) return SPRING_OK;
+    for (int k = 0; k < 3; ++k)
+        if (pol3[2 * k] < 1 || pol3[2 * k + 1] > c->ndof || pol3[2 * k] > pol3[2 * k + 1])
+            return fail(c, SPRING_ERR_ARG, "pol3 column %d out of range [1,%d]", k + 1, c->ndof);
+    return SPRING_OK;
+}
+
+int check_q0_range(spring_ctx* c, int i0_first, int n_q0) {
+    if (!c->irr_set) return fail(c, SPRING_ERR_STATE, "irreducible q-points have not been set");
+    if (n_q0 < 0 || i0_first < 1 || i0_first + n_q0 - 1 > c->nq0)
+        return fail(c, SPRING_ERR_ARG, "q0 range [%d, %d] outside [1, %d]", i0_first, i0_first + n_q0 - 1, c->nq0);
+    return SPRING_OK;
+}
+
+// Copy a [T][q0 range][s] device slab to the Fortran array out(Ndof, n_q0, nT).
+int copy_lw_out(spring_ctx* c, const double* d_src, int q0_first, int n_q0, double* out) {
+    if (!out) return SPRING_OK;
+    for (int t = 0; t < c->nT; ++t)
+        SPRING_CHECK(d2h(c, out + (size_t)t * n_q0 * c->ndof, d_src + ((size_t)t * c->nq0 + q0_first) * c->ndof,
+                         sizeof(double) * n_q0 * c->ndof, "linewidth output"));
+    return SPRING_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int spring_ctx_create(spring_ctx** out, const spring_dims* d) {
+    if (!out || !d) return SPRING_ERR_ARG;
+    *out = nullptr;
+    if (d->nbasis < 1 || d->nbasis > MAX_NB) return SPRING_ERR_ARG;
+    if (d->mesh[0] < 1 || d->mesh[1] < 1 || d->mesh[2] < 1 || d->n_temps < 1) return SPRING_ERR_ARG;
+    long long nq = (long long)d->mesh[0] * d->mesh[1] * d->mesh[2];
+    if (nq > (1LL << 24)) return SPRING_ERR_ARG;
+    spring_ctx* c = new (std::nothrow) spring_ctx();
+    if (!c) return SPRING_ERR_ALLOC;
+    if (d->device >= 0) {
+        c->device = d->device;
+    } else if (cudaGetDevice(&c->device) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return SPRING_ERR_CUDA;
+    }
+    DeviceGuard g(c->device);
+    c->nb = d->nbasis;
+    c->ndof = 3 * d->nbasis;
+    for (int k = 0; k < 3; ++k) c->mesh[k] = d->mesh[k];
+    c->nq = (int)nq;
+    c->nT = d->n_temps;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return SPRING_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    *out = c;
+    return SPRING_OK;
+}
+
+int spring_ctx_destroy(spring_ctx* c) {
+    if (!c) return SPRING_ERR_ARG;
+    {
+        DeviceGuard g(c->device);
+        cudaStreamSynchronize(c->stream);
+        dfree(c->d_mass_rs); dfree(c->d_fc2); dfree(c->d_fc2_idx); dfree(c->d_fc2_num);
+        dfree(c->d_fc3t); dfree(c->d_fc3_posr); dfree(c->d_fc3_btyp);
+        dfree(c->d_qint); dfree(c->d_qpnt); dfree(c->d_tetra);
+        dfree(c->d_irr_int); dfree(c->d_irr_q); dfree(c->d_mult); dfree(c->d_pos); dfree(c->d_temps);
+        free_phonons(c->ph_grid); free_phonons(c->ph_irr);
+        dfree(c->d_partner); dfree(c->d_pairoff); dfree(c->d_pairs); dfree(c->d_pair_q0); dfree(c->d_pairpos);
+        dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
+        dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
+        if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    }
+    delete c;
+    return SPRING_OK;
+}
+
+const char* spring_last_error(const spring_ctx* c) { return c ? c->err.c_str() : "NULL context"; }
+
+int spring_set_stream(spring_ctx* c, void* s) {
+    CTX_ENTER(c);
+    c->stream = s ? (cudaStream_t)s : c->own_stream;
+    return SPRING_OK;
+}
+
+int spring_synchronize(spring_ctx* c) {
+    CTX_ENTER(c);
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, "synchronize");
+}
+
+int spring_kernel_launches(const spring_ctx* c, long long* count) {
+    if (!c || !count) return SPRING_ERR_ARG;
+    *count = c->launches;
+    return SPRING_OK;
+}
+
+int spring_debug_inject_fault(spring_ctx* c, int kind, int n) {
+    CTX_ENTER(c);
+    if (kind < 0 || kind > 2 || n < 0) return fail(c, SPRING_ERR_ARG, "kind must be 0..2 and n >= 0");
+    c->inject_kind = n > 0 ? kind : -1;
+    c->inject_n = n;
+    for (int k = 0; k < 3; ++k) c->inject_seen[k] = 0;
+    return SPRING_OK;
+}
+
+int spring_set_crystal(spring_ctx* c, const double* latvec, const double* mass) {
+    CTX_ENTER(c);
+    if (!latvec || !mass) return fail(c, SPRING_ERR_ARG, "latvec/mass is NULL");
+    std::memcpy(c->latvec, latvec, sizeof c->latvec);
+    const double* a = c->latvec;  // a[r + 3*i] = component r of vector i
+    auto cross = [](const double* x, const double* y, double* o) {
+        o[0] = x[1] * y[2] - x[2] * y[1];
+        o[1] = x[2] * y[0] - x[0] * y[2];
+        o[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    double cr[3];
+    cross(a + 3, a + 6, cr);
+    c->vol = std::fabs(a[0] * cr[0] + a[1] * cr[1] + a[2] * cr[2]);
+    if (!(c->vol > 0.0)) return fail(c, SPRING_ERR_ARG, "lattice vectors are degenerate");
+    for (int i = 0; i < 3; ++i) {
+        int i2 = (i + 1) % 3, i3 = (i + 2) % 3;
+        cross(a + 3 * i2, a + 3 * i3, cr);
+        for (int r = 0; r < 3; ++r) c->G[r + 3 * i] = cr[r] * 2.0 * (4.0 * std::atan(1.0)) / c->vol;
+    }
+    c->mass.assign(mass, mass + c->nb);
+    std::vector<double> rs(c->nb);
+    for (int i = 0; i < c->nb; ++i) {
+        if (!(mass[i] > 0.0)) return fail(c, SPRING_ERR_ARG, "mass %d is not positive", i + 1);
+        rs[i] = 1.0 / std::sqrt(mass[i]);
+    }
+    SPRING_CHECK(dalloc(c, c->d_mass_rs, c->nb, "masses"));
+    SPRING_CHECK(h2d(c, c->d_mass_rs.p, rs.data(), sizeof(double) * c->nb, "masses"));
+    c->crystal_set = true;
+    return SPRING_OK;
+}
+
+int spring_set_fc2(spring_ctx* c, int na2, const int* num, const int* idx, const double* fc) {
+    CTX_ENTER(c);
+    if (!num || !idx || !fc || na2 < 1) return fail(c, SPRING_ERR_ARG, "FC2 arrays are NULL or na2 < 1");
+    for (int mu = 0; mu < c->nb; ++mu) {
+        if (num[mu] < 0 || num[mu] > na2) return fail(c, SPRING_ERR_ARG, "FC2 atm_num(%d) out of range", mu + 1);
+        for (int n = 0; n < num[mu]; ++n) {
+            int b = idx[4 * (n + (size_t)na2 * mu) + 3];
+            if (b < 1 || b > c->nb) return fail(c, SPRING_ERR_ARG, "FC2 atm_indx basis out of range");
+        }
+    }
+    c->na2 = na2;
+    SPRING_CHECK(dalloc(c, c->d_fc2, (size_t)c->nb * na2 * 9, "FC2"));
+    SPRING_CHECK(dalloc(c, c->d_fc2_idx, (size_t)c->nb * na2 * 4, "FC2 index"));
+    SPRING_CHECK(dalloc(c, c->d_fc2_num, c->nb, "FC2 counts"));
+    SPRING_CHECK(h2d(c, c->d_fc2.p, fc, sizeof(double) * c->nb * na2 * 9, "FC2"));
+    SPRING_CHECK(h2d(c, c->d_fc2_idx.p, idx, sizeof(int) * c->nb * na2 * 4, "FC2 index"));
+    SPRING_CHECK(h2d(c, c->d_fc2_num.p, num, sizeof(int) * c->nb, "FC2 counts"));
+    SPRING_CHECK(spring_synchronize(c));
+    c->fc2_set = true;
+    return SPRING_OK;
+}
+
+int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const double* fc) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->crystal_set, "crystal"));
+    if (!num || !idx || !fc || na3 < 1 || na3 > 16) return fail(c, SPRING_ERR_ARG, "FC3 arrays are NULL or na3 not in 1..16");
+    const int nb = c->nb;
+    // kernel layout: [mu][k2 = N2*3+gamma][r = (N1*3+alpha)*3+beta], zero padded beyond atm_num
+    const int K = 3 * na3, R = 9 * na3;
+    std::vector<double> t((size_t)nb * K * R, 0.0), posr((size_t)nb * na3 * 3, 0.0);
+    std::vector<int> btyp((size_t)nb * na3, 0);
+    for (int mu = 0; mu < nb; ++mu) {
+        if (num[mu] < 0 || num[mu] > na3) return fail(c, SPRING_ERR_ARG, "FC3 atm_num(%d) out of range", mu + 1);
+        for (int n = 0; n < num[mu]; ++n) {
+            const int* e = idx + 4 * (n + (size_t)na3 * mu);
+            if (e[3] < 1 || e[3] > nb) return fail(c, SPRING_ERR_ARG, "FC3 atm_indx basis out of range");
+            btyp[(size_t)mu * na3 + n] = e[3] - 1;
+            for (int r = 0; r < 3; ++r)  // atmPosR = latvec * cell (FC3_mod.f90:84)
+                posr[((size_t)mu * na3 + n) * 3 + r] =
+                    c->latvec[r] * e[0] + c->latvec[r + 3] * e[1] + c->latvec[r + 6] * e[2];
+        }
+        for (int n1 = 0; n1 < num[mu]; ++n1)
+            for (int n2 = 0; n2 < num[mu]; ++n2)
+                for (int al = 0; al < 3; ++al)
+                    for (int be = 0; be < 3; ++be)
+                        for (int ga = 0; ga < 3; ++ga) {
+                            // Fortran fC(ga,be,al,N2,N1,mu)
+                            size_t fi = ga + 3 * (be + 3 * (al + 3 * (n2 + (size_t)na3 * (n1 + (size_t)na3 * mu))));
+                            int k2 = n2 * 3 + ga, r = (n1 * 3 + al) * 3 + be;
+                            t[((size_t)mu * K + k2) * R + r] = fc[fi];
+                        }
+    }
+    c->na3 = na3;
+    SPRING_CHECK(dalloc(c, c->d_fc3t, t.size(), "FC3"));
+    SPRING_CHECK(dalloc(c, c->d_fc3_posr, posr.size(), "FC3 positions"));
+    SPRING_CHECK(dalloc(c, c->d_fc3_btyp, btyp.size(), "FC3 basis"));
+    SPRING_CHECK(h2d(c, c->d_fc3t.p, t.data(), sizeof(double) * t.size(), "FC3"));
+    SPRING_CHECK(h2d(c, c->d_fc3_posr.p, posr.data(), sizeof(double) * posr.size(), "FC3 positions"));
+    SPRING_CHECK(h2d(c, c->d_fc3_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC3 basis"));
+    SPRING_CHECK(spring_synchronize(c));
+    c->fc3_set = true;
+    return SPRING_OK;
+}
+
+int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_pnt_int, double* q_pnt,
+                     int* tetrahedrons) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->crystal_set, "crystal"));
+    int sh[3] = {0, 0, 0};
+    if (shift) for (int k = 0; k < 3; ++k) sh[k] = shift[k];
+    const size_t nq = c->nq;
+    SPRING_CHECK(dalloc(c, c->d_qint, nq * 3, "q_pnt_int"));
+    SPRING_CHECK(dalloc(c, c->d_qpnt, nq * 3, "q_pnt"));
+    SPRING_CHECK(dalloc(c, c->d_tetra, nq * 24, "tetrahedrons"));
+    SPRING_CHECK(run_make_mesh(c, sh, zero_centered));
+    if (q_pnt_int) SPRING_CHECK(d2h(c, q_pnt_int, c->d_qint.p, sizeof(int) * nq * 3, "q_pnt_int"));
+    if (q_pnt) SPRING_CHECK(d2h(c, q_pnt, c->d_qpnt.p, sizeof(double) * nq * 3, "q_pnt"));
+    if (tetrahedrons) {
+        std::vector<int> t(nq * 24);
+        SPRING_CHECK(d2h(c, t.data(), c->d_tetra.p, sizeof(int) * nq * 24, "tetrahedrons"));
+        for (size_t i = 0; i < t.size(); ++i) tetrahedrons[i] = t[i] + 1;
+    }
+    SPRING_CHECK(spring_synchronize(c));
+    c->mesh_set = true;
+    c->enum3_done = false;
+    return SPRING_OK;
+}
+
+static int install_irr(spring_ctx* c, int nq0, const int* irr_int, const int* pos, const int* mult) {
+    c->nq0 = nq0;
+    c->h_irr_int.assign(irr_int, irr_int + 3 * nq0);
+    c->h_pos.assign(pos, pos + c->nq);
+    c->h_mult.assign(mult, mult + nq0);
+    std::vector<double> q((size_t)nq0 * 3);
+    for (int i = 0; i < nq0; ++i)
+        for (int r = 0; r < 3; ++r) {
+            double s = 0.0;  // Recp_cell_unit * irr (TetrahedronQ_m.f90:304)
+            for (int k = 0; k < 3; ++k) s += (c->G[r + 3 * k] / c->mesh[k]) * double(irr_int[3 * i + k]);
+            q[3 * i + r] = s;
+        }
+    SPRING_CHECK(dalloc(c, c->d_irr_int, (size_t)nq0 * 3, "irreducible q"));
+    SPRING_CHECK(dalloc(c, c->d_irr_q, (size_t)nq0 * 3, "irreducible q"));
+    SPRING_CHECK(dalloc(c, c->d_mult, nq0, "multiplicity"));
+    SPRING_CHECK(h2d(c, c->d_irr_int.p, irr_int, sizeof(int) * nq0 * 3, "irreducible q"));
+    SPRING_CHECK(h2d(c, c->d_irr_q.p, q.data(), sizeof(double) * nq0 * 3, "irreducible q"));
+    SPRING_CHECK(h2d(c, c->d_mult.p, mult, sizeof(int) * nq0, "multiplicity"));
+    SPRING_CHECK(dalloc(c, c->d_pos, c->nq, "pos"));
+    SPRING_CHECK(h2d(c, c->d_pos.p, pos, sizeof(int) * c->nq, "pos"));
+    SPRING_CHECK(dalloc(c, c->d_lw_all, (size_t)c->nT * nq0 * c->ndof, "LW_Allq0"));
+    SPRING_CHECK(zero(c, c->d_lw_all.p, sizeof(double) * c->nT * nq0 * c->ndof, "LW_Allq0"));
+    SPRING_CHECK(spring_synchronize(c));
+    c->irr_set = true;
+    c->enum3_done = false;
+    free_phonons(c->ph_irr);
+    return SPRING_OK;
+}
+
+int spring_find_irr_q(spring_ctx* c, int nrot, const int* rot, int time_rev, int* nq0_out, int* irr_q_pnt_int,
+                      int* pos, int* multiplicity) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    if (nrot < 1 || nrot > 192 || !rot) return fail(c, SPRING_ERR_ARG, "rotations: need 1..192 matrices");
+    DBuf<int> d_rot, d_map;
+    int rc = dalloc(c, d_rot, (size_t)nrot * 9, "rotations");
+    if (rc == SPRING_OK) rc = dalloc(c, d_map, c->nq, "irreducible map");
+    if (rc == SPRING_OK) rc = h2d(c, d_rot.p, rot, sizeof(int) * 9 * nrot, "rotations");
+    if (rc == SPRING_OK) rc = run_irr_map(c, d_rot.p, nrot, time_rev, d_map.p);
+    std::vector<int> map(c->nq), qint((size_t)c->nq * 3);
+    if (rc == SPRING_OK) rc = d2h(c, map.data(), d_map.p, sizeof(int) * c->nq, "irreducible map");
+    if (rc == SPRING_OK) rc = d2h(c, qint.data(), c->d_qint.p, sizeof(int) * c->nq * 3, "q_pnt_int");
+    dfree(d_rot);
+    dfree(d_map);
+    if (rc != SPRING_OK) return rc;
+    // unique_sort + FindPositionAndMultiplicity (Helper_m.f90:510-594)
+    std::vector<int> uniq(map);
+    std::sort(uniq.begin(), uniq.end());
+    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
+    const int nq0 = (int)uniq.size();
+    std::vector<int> irr((size_t)nq0 * 3), ps(c->nq), mu(nq0, 0);
+    for (int k = 0; k < nq0; ++k)
+        for (int d = 0; d < 3; ++d) irr[3 * k + d] = qint[3 * (size_t)uniq[k] + d];
+    for (int i = 0; i < c->nq; ++i) {
+        int k = (int)(std::lower_bound(uniq.begin(), uniq.end(), map[i]) - uniq.begin());
+        ps[i] = k + 1;
+        mu[k] += 1;
+    }
+    SPRING_CHECK(install_irr(c, nq0, irr.data(), ps.data(), mu.data()));
+    if (nq0_out) *nq0_out = nq0;
+    if (irr_q_pnt_int) std::memcpy(irr_q_pnt_int, irr.data(), sizeof(int) * irr.size());
+    if (pos) std::memcpy(pos, ps.data(), sizeof(int) * ps.size());
+    if (multiplicity) std::memcpy(multiplicity, mu.data(), sizeof(int) * mu.size());
+    return SPRING_OK;
+}
+
+int spring_compute_phonons(spring_ctx* c, const double* temps, double freq_cut) {
+    CTX_ENTER(c);
+    (void)freq_cut;
+    SPRING_CHECK(need(c, c->fc2_set, "FC2"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    SPRING_CHECK(set_temps(c, temps));
+    SPRING_CHECK(alloc_phonons(c, c->ph_grid, c->nq));
+    SPRING_CHECK(alloc_phonons(c, c->ph_irr, c->nq0));
+    SPRING_CHECK(run_phonons(c, c->ph_grid, c->d_qpnt.p, c->nq));
+    SPRING_CHECK(run_phonons(c, c->ph_irr, c->d_irr_q.p, c->nq0));
+    c->ph_grid.set = c->ph_irr.set = true;
+    return SPRING_OK;
+}
+
+int spring_set_phonons(spring_ctx* c, int which, const double* temps, const double* evec, const double* omega,
+                       const double* oneby, const double* nbe, const double* vel) {
+    CTX_ENTER(c);
+    if (which != 0 && which != 1) return fail(c, SPRING_ERR_ARG, "which must be 0 (grid) or 1 (irreducible)");
+    if (!evec || !omega || !oneby || !nbe || !vel) return fail(c, SPRING_ERR_ARG, "phonon arrays are NULL");
+    if (which == 1) SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    SPRING_CHECK(set_temps(c, temps));
+    Phonons& p = which == 0 ? c->ph_grid : c->ph_irr;
+    const int n = which == 0 ? c->nq : c->nq0;
+    SPRING_CHECK(alloc_phonons(c, p, n));
+    const size_t nd = c->ndof;
+    SPRING_CHECK(h2d(c, p.evec.p, evec, sizeof(double2) * n * nd * nd, "eigenvectors"));
+    SPRING_CHECK(h2d(c, p.omega.p, omega, sizeof(double) * n * nd, "omega"));
+    SPRING_CHECK(h2d(c, p.oneby.p, oneby, sizeof(double) * n * nd, "1/omega"));
+    SPRING_CHECK(h2d(c, p.nbe.p, nbe, sizeof(double) * c->nT * n * nd, "nBE"));
+    SPRING_CHECK(h2d(c, p.vel.p, vel, sizeof(double) * n * nd * 3, "group velocity"));
+    SPRING_CHECK(spring_synchronize(c));
+    p.set = true;
+    return SPRING_OK;
+}
+
+int spring_get_phonons(spring_ctx* c, int which, double* evec, double* omega, double* oneby, double* nbe,
+                       double* vel) {
+    CTX_ENTER(c);
+    if (which != 0 && which != 1) return fail(c, SPRING_ERR_ARG, "which must be 0 or 1");
+    Phonons& p = which == 0 ? c->ph_grid : c->ph_irr;
+    SPRING_CHECK(need(c, p.set, "phonons"));
+    const size_t nd = c->ndof, n = p.n;
+    if (evec) SPRING_CHECK(d2h(c, evec, p.evec.p, sizeof(double2) * n * nd * nd, "eigenvectors"));
+    if (omega) SPRING_CHECK(d2h(c, omega, p.omega.p, sizeof(double) * n * nd, "omega"));
+    if (oneby) SPRING_CHECK(d2h(c, oneby, p.oneby.p, sizeof(double) * n * nd, "1/omega"));
+    if (nbe) SPRING_CHECK(d2h(c, nbe, p.nbe.p, sizeof(double) * c->nT * n * nd, "nBE"));
+    if (vel) SPRING_CHECK(d2h(c, vel, p.vel.p, sizeof(double) * n * nd * 3, "group velocity"));
+    return SPRING_OK;
+}
+
+int spring_enumerate3(spring_ctx* c, int i0, int* allq1q2, int* perm, int* counts) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0, 1));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    DBuf<int> a, p, n;
+    int rc = dalloc(c, a, (size_t)c->nq * 4, "Allq1q2");
+    if (rc == SPRING_OK) rc = dalloc(c, p, (size_t)c->nq * 2, "q1q2_permuted");
+    if (rc == SPRING_OK) rc = dalloc(c, n, 2, "counts");
+    if (rc == SPRING_OK) rc = run_enumerate3_fortran(c, i0 - 1, a.p, p.p, n.p);
+    int hc[2] = {0, 0};
+    if (rc == SPRING_OK) rc = d2h(c, hc, n.p, sizeof hc, "counts");
+    if (rc == SPRING_OK && allq1q2) rc = d2h(c, allq1q2, a.p, sizeof(int) * 4 * c->nq, "Allq1q2");
+    if (rc == SPRING_OK && perm) rc = d2h(c, perm, p.p, sizeof(int) * 2 * hc[0], "q1q2_permuted");
+    if (rc == SPRING_OK && counts) { counts[0] = hc[0]; counts[1] = hc[1]; }
+    dfree(a); dfree(p); dfree(n);
+    return rc;
+}
+
+static int ensure_enum3(spring_ctx* c) {
+    if (c->enum3_done) return SPRING_OK;
+    SPRING_CHECK(run_enumerate3(c));
+    c->enum3_done = true;
+    return SPRING_OK;
+}
+
+static int ready3(spring_ctx* c) {
+    SPRING_CHECK(need(c, c->fc3_set, "FC3"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    SPRING_CHECK(need(c, c->ph_irr.set, "irreducible-point phonons"));
+    return SPRING_OK;
+}
+
+// Number of q0 whose W grids fit the tetrahedron W buffer (keeps it around L2 size).
+static int w_slots(spring_ctx* c, int n_q0) {
+    const size_t slot = (size_t)c->nq * c->ndof * c->ndof * c->ndof * sizeof(double);
+    size_t budget = (size_t)96 << 20;
+    int s = (int)std::max<size_t>(1, budget / slot);
+    return std::min(s, std::max(n_q0, 1));
+}
+
+int spring_scatter_w3(spring_ctx* c, int i0, double* sctr) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0, 1));
+    SPRING_CHECK(ready3(c));
+    SPRING_CHECK(ensure_enum3(c));
+    const size_t n = (size_t)c->nq * c->ndof * c->ndof * c->ndof;
+    SPRING_CHECK(dalloc(c, c->d_w, n, "W buffer"));
+    SPRING_CHECK(run_v3_wgrid(c, i0 - 1, 1, c->d_w.p));
+    if (sctr) SPRING_CHECK(d2h(c, sctr, c->d_w.p, sizeof(double) * n, "Sctrq1"));
+    return SPRING_OK;
+}
+
+int spring_linewidth3(spring_ctx* c, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol3,
+                      double* lw, double* p3_q0) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0_first, n_q0));
+    SPRING_CHECK(ready3(c));
+    SPRING_CHECK(check_pol(c, pol3));
+    if (delta_mode != SPRING_DELTA_GAUSS && delta_mode != SPRING_DELTA_TETRA)
+        return fail(c, SPRING_ERR_ARG, "delta_mode must be SPRING_DELTA_GAUSS or SPRING_DELTA_TETRA");
+    if (delta_mode == SPRING_DELTA_GAUSS && !(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    if (n_q0 == 0) return SPRING_OK;
+    SPRING_CHECK(ensure_enum3(c));
+    const Pol pol = make_pol(c, pol3);
+    const int q0 = i0_first - 1;
+    const size_t nl = (size_t)c->nT * c->nq0 * c->ndof;
+    SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
+    SPRING_CHECK(dalloc(c, c->d_p3, (size_t)c->nq0 * c->ndof, "phase-space scratch"));
+    SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
+    SPRING_CHECK(zero(c, c->d_p3.p, sizeof(double) * c->nq0 * c->ndof, "phase-space scratch"));
+    if (delta_mode == SPRING_DELTA_GAUSS) {
+        SPRING_CHECK(run_v3_gauss(c, q0, n_q0, sigma, pol, c->d_lw_tmp.p, c->d_p3.p));
+    } else {
+        const int slots = w_slots(c, n_q0);
+        const size_t slot = (size_t)c->nq * c->ndof * c->ndof * c->ndof;
+        SPRING_CHECK(dalloc(c, c->d_w, slot * slots, "W buffer"));
+        for (int b = 0; b < n_q0; b += slots) {
+            const int nb = std::min(slots, n_q0 - b);
+            SPRING_CHECK(run_v3_wgrid(c, q0 + b, nb, c->d_w.p));
+            SPRING_CHECK(run_tetra3(c, q0 + b, nb, c->d_w.p, pol, c->d_lw_tmp.p, c->d_p3.p));
+        }
+    }
+    // LW_Allq0 += lw (third order: weight 1, main.f90:584)
+    SPRING_CHECK(run_axpy_lw(c, 1.0, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
+    SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, lw));
+    if (p3_q0)
+        SPRING_CHECK(d2h(c, p3_q0, c->d_p3.p + (size_t)q0 * c->ndof, sizeof(double) * n_q0 * c->ndof, "P3_q0"));
+    return SPRING_OK;
+}
+
+int spring_linewidth_iso(spring_ctx* c, int i0_first, int n_q0, int delta_mode, double sigma, const double* g2,
+                         double* rate) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0_first, n_q0));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set && c->ph_irr.set, "phonons"));
+    if (!g2) return fail(c, SPRING_ERR_ARG, "g2 is NULL");
+    if (delta_mode != SPRING_DELTA_GAUSS && delta_mode != SPRING_DELTA_TETRA)
+        return fail(c, SPRING_ERR_ARG, "delta_mode must be SPRING_DELTA_GAUSS or SPRING_DELTA_TETRA");
+    if (delta_mode == SPRING_DELTA_GAUSS && !(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    if (n_q0 == 0) return SPRING_OK;
+    const int q0 = i0_first - 1;
+    const size_t nl = (size_t)c->nT * c->nq0 * c->ndof;
+    SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
+    SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
+    SPRING_CHECK(run_iso(c, q0, n_q0, delta_mode, sigma, g2, c->d_lw_tmp.p));
+    SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
+    SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
+    return SPRING_OK;
+}
+
+int spring_reset_linewidths(spring_ctx* c) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    return zero(c, c->d_lw_all.p, sizeof(double) * c->nT * c->nq0 * c->ndof, "LW_Allq0");
+}
+
+int spring_get_linewidths(spring_ctx* c, double* out) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    if (!out) return fail(c, SPRING_ERR_ARG, "output is NULL");
+    return d2h(c, out, c->d_lw_all.p, sizeof(double) * c->nT * c->nq0 * c->ndof, "LW_Allq0");
+}
+
+int spring_set_linewidths(spring_ctx* c, const double* in) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    if (!in) return fail(c, SPRING_ERR_ARG, "input is NULL");
+    SPRING_CHECK(h2d(c, c->d_lw_all.p, in, sizeof(double) * c->nT * c->nq0 * c->ndof, "LW_Allq0"));
+    return spring_synchronize(c);
+}
+
+int spring_kappa_rta(spring_ctx* c, int symm, int nsym, const double* rxyz, const int* s_range, double* kappa,
+                     double* mode_k) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    SPRING_CHECK(need(c, c->ph_irr.set, "irreducible-point phonons"));
+    if (!symm) SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    if (symm && (nsym < 1 || !rxyz)) return fail(c, SPRING_ERR_ARG, "symmetrised kappa needs Rxyz");
+    int lo = 1, hi = c->ndof;
+    if (s_range) { lo = s_range[0]; hi = s_range[1]; }
+    if (lo < 1 || hi > c->ndof || lo > hi) return fail(c, SPRING_ERR_ARG, "s_range out of range");
+    SPRING_CHECK(dalloc(c, c->d_kappa, (size_t)c->nT * 9 * (1 + c->ndof), "kappa"));
+    if (symm) {
+        SPRING_CHECK(dalloc(c, c->d_rxyz, (size_t)nsym * 9, "Rxyz"));
+        SPRING_CHECK(h2d(c, c->d_rxyz.p, rxyz, sizeof(double) * 9 * nsym, "Rxyz"));
+    }
+    double* dk = c->d_kappa.p;
+    double* dm = c->d_kappa.p + (size_t)c->nT * 9;
+    SPRING_CHECK(run_kappa_rta(c, symm, nsym, c->d_rxyz.p, lo - 1, hi - 1, dk, dm));
+    if (kappa) SPRING_CHECK(d2h(c, kappa, dk, sizeof(double) * 9 * c->nT, "kappa"));
+    if (mode_k) SPRING_CHECK(d2h(c, mode_k, dm, sizeof(double) * 9 * c->ndof * c->nT, "mode kappa"));
+    return SPRING_OK;
+}
+
+}  // extern "C"
