@@ -1,0 +1,374 @@
+#!/usr/bin/env python
+"""Throughput of the 3-phonon scattering path on B200: one JSON line on stdout.
+
+Workload (BASELINE config "3-phonon at 24x24x24, T = 100/300/700 K" on the
+rocksalt crystal of config 1): fcc rocksalt 2-atom cell, seeded spring-model
+FC2 and FC3, 24^3 Gamma-centred mesh (13824 q, 413 irreducible q0), Gaussian
+smearing sigma = 2 cm^-1.  One step = the whole path for all temperatures:
+device phonons for the grid and the irreducible set, pair enumeration for every
+q0, V3 -> W -> Gaussian delta sum for every pair, RTA kappa (symmetrised).
+
+metric: 3-phonon scattering evaluations per second, one evaluation = one mode
+triple (s0,s1,s2) of one enumerated pair (sum over q0 of npairs * Ndof^3 per
+step; the three temperatures reuse the same V3).
+
+--impl reference times the CPU restatement of the reference (the oracle; the
+Fortran reference cannot be built on this image) on a bounded sample of the
+same workload, with all host threads.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MESH = 24
+TEMPS = [100.0, 300.0, 700.0]
+SIGMA = 0.3767          # 2 cm^-1 in rad/ps
+DELTA = "gauss"
+WORKLOAD = "rocksalt2-fcc-24x24x24-3ph-gauss-T100/300/700"
+METRIC = "3ph scattering evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mesh", type=int, default=MESH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def algorithmic_flops_per_pair(ndof, na3_counts):
+    """V3 in the factored form: phase-weighted FC sum 4*27*sum_mu Na3^2, three
+    eigenvector contractions 3*8*Ndof^4, |Phi|^2 scaling 3*Ndof^3."""
+    return 4 * 27 * int(np.sum(np.asarray(na3_counts) ** 2)) + 3 * 8 * ndof ** 4 + 3 * ndof ** 3
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (200 ms period)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for r in csv.reader(fh):
+                if len(r) >= 9:
+                    rows.append([x.strip() for x in r])
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        load = [s for s in sm if s > 0.5 * smax] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+
+
+def fp64_peak_tflops(torch):
+    """Measured FP64 ceiling of this GPU in this run: cuBLAS DGEMM 8192^3, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 0.0
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_baseline(cr, mesh, temps, ph_grid, ph_irr, irr_int, sample, threads_note):
+    """The oracle (CPU restatement of the reference loops) on a sample of q0: enumeration,
+    naive V3 (ScatterMatEl loop order) and the Gaussian sum at every temperature."""
+    from oracle import driver as D
+    qi, qf, _ = D.make_tetrahedron(mesh, cr.G)
+    evals = 0
+    t0 = time.perf_counter()
+    for i0 in sample:
+        A, perm, cnt = D.momentum3(mesh, qi, irr_int[i0])
+        sctr = D.scatter_w3(cr, qf, qi, irr_int[i0], ph_irr["evec"][i0], ph_irr["onebyomega"][i0], ph_grid["evec"],
+                            ph_grid["onebyomega"], perm)
+        for it in range(len(temps)):
+            D.lw3_gauss(ph_irr["omega"][i0], ph_grid["omega"], ph_grid["nbe"][it], sctr, A, qi, SIGMA)
+        evals += cnt[0] * cr.ndof ** 3
+    dt = time.perf_counter() - t0
+    return evals / dt, dt, D.lib().orc_num_threads()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import driver as D
+    from oracle import phonons as P
+    from spring_b200 import synthetic as S
+    cr = S.build("rocksalt2")
+    mesh = (args.mesh,) * 3
+    qi, qf, _ = D.make_tetrahedron(mesh, cr.G)
+    W, _ = S.point_group(cr)
+    ir = D.irr_q(mesh, W, qi)
+    irr = ir["irr_q_pnt_int"]
+    irq = ((cr.G / np.array(mesh)[None, :]) @ irr.T.astype(float)).T
+    args_ph = (cr.latvec, cr.mass, cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
+    ph_grid = P.get_phonon(*args_ph, qf, TEMPS)
+    ph_irr = P.get_phonon(*args_ph, irq, TEMPS)
+    nq0 = irr.shape[0]
+    order = [(7 * k + 1) % nq0 for k in range(args.steps + args.warmup)]
+    for k in range(args.warmup):
+        cpu_baseline(cr, mesh, TEMPS, ph_grid, ph_irr, irr, [order[k]], "")
+    evals, secs = 0, 0.0
+    threads = 1
+    for k in range(args.steps):
+        i0 = order[args.warmup + k]
+        v, dt, threads = cpu_baseline(cr, mesh, TEMPS, ph_grid, ph_irr, irr, [i0], "")
+        evals += v * dt
+        secs += dt
+    value = evals / secs
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "mesh": list(mesh), "temperatures": TEMPS, "sigma_rad_ps": SIGMA,
+                       "sample": "one irreducible q0 per step"},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads, "kind": "port",
+                             "sample": f"{args.steps} of {nq0} irreducible q0 (one per step): enumeration, V3 in "
+                                       "the reference loop order, Gaussian sum at 3 T; phonons excluded"},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def partition(counts, world, rank):
+    """Contiguous q0 block of this rank, balanced by pair count (DistributeQpoints balanced by cost)."""
+    c = np.cumsum(counts)
+    tot = c[-1]
+    lo = 0 if rank == 0 else int(np.searchsorted(c, tot * rank / world, side="right"))
+    hi = len(counts) if rank == world - 1 else int(np.searchsorted(c, tot * (rank + 1) / world, side="right"))
+    return lo, hi
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from spring_b200 import synthetic as S
+    from spring_b200.api import Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(device=dev)
+
+    cr = S.build("rocksalt2")
+    W, Rxyz = S.point_group(cr)
+    mesh = (args.mesh,) * 3
+    ctx = Context(cr.nbasis, mesh, len(TEMPS), device=local)
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_crystal(cr.latvec, cr.mass)
+    ctx.set_fc2(cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
+    ctx.set_fc3(cr.fc3_atm_num, cr.fc3_atm_indx, cr.fc3)
+    ctx.make_mesh(want=False)
+    irr = ctx.find_irr_q(W)
+    nq0 = ctx.nq0
+    ctx.compute_phonons(TEMPS)
+    counts = np.array([ctx.enumerate3(i + 1)[2][0] for i in range(nq0)])
+    lo, hi = partition(counts, world, rank)
+    my_pairs = int(counts[lo:hi].sum())
+    evals_total = int(counts.sum()) * cr.ndof ** 3
+    flops_pair = algorithmic_flops_per_pair(cr.ndof, cr.fc3_atm_num)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    kap_dev = torch.zeros(len(TEMPS), 9, dtype=torch.float64, device=dev)
+
+    def step():
+        ctx.compute_phonons(TEMPS)
+        ctx.prepare3()
+        ctx.reset_linewidths()
+        if hi > lo:
+            ctx.linewidth3(lo + 1, hi - lo, delta=DELTA, sigma=SIGMA, want=False)
+        if world > 1:
+            lw = torch.from_numpy(ctx.get_linewidths()).to(dev)
+            dist.all_reduce(lw)
+            ctx.set_linewidths(lw.cpu().numpy())
+        ctx.kappa_rta(Rxyz, want=False)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        clocks = Clocks(local)
+        clocks.start()
+        ctx.set_profiling(True)
+        l0 = ctx.kernel_launches()
+        times = []
+        for _ in range(args.steps):
+            flush.zero_()           # L2 flush, outside the timed events
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            e1.synchronize()
+            times.append(e0.elapsed_time(e1))
+        torch.cuda.synchronize()
+        launches = ctx.kernel_launches() - l0
+        v3_ms, v3_n = ctx.kernel_time("k_v3")
+        ctx.set_profiling(False)
+        clk = clocks.stop()
+        ms = float(np.sum(times)) / args.steps
+        if world > 1:
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+            dist.barrier()
+
+        # end to end through the public API: host inputs, pinned, copied every step
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+        h_lat, h_mass = pin(cr.latvec), pin(cr.mass)
+        h_f2 = (pin(cr.fc2_atm_num), pin(cr.fc2_atm_indx), pin(cr.fc2))
+        h_f3 = (pin(cr.fc3_atm_num), pin(cr.fc3_atm_indx), pin(cr.fc3))
+        h_W = pin(W)
+        h_lw = pin(np.zeros((len(TEMPS), max(hi - lo, 1), cr.ndof)))
+        h_kap = pin(np.zeros((len(TEMPS), 9)))
+        nq = int(np.prod(mesh))
+        h2d = (h_lat.nbytes + h_mass.nbytes + sum(a.nbytes for a in h_f2) + sum(a.nbytes for a in h_f3) + h_W.nbytes
+               + 8 * len(TEMPS))
+        d2h = (4 * nq + 12 * nq          # irreducible map and grid addresses (find_irr_q)
+               + 8 + 4 * (nq0 + 1)       # pair count and offsets (prepare3)
+               + h_lw.nbytes + h_kap.nbytes)
+
+        def step_e2e():
+            ctx.set_crystal(h_lat, h_mass)
+            ctx.set_fc2(*h_f2)
+            ctx.set_fc3(*h_f3)
+            ctx.make_mesh(want=False)
+            ctx.find_irr_q(h_W)
+            ctx.compute_phonons(TEMPS)
+            ctx.prepare3()
+            ctx.reset_linewidths()
+            if hi > lo:
+                ctx.linewidth3(lo + 1, hi - lo, delta=DELTA, sigma=SIGMA, out=h_lw)
+            if world > 1:
+                lw = torch.zeros(len(TEMPS), nq0, cr.ndof, dtype=torch.float64)
+                lw[:, lo:hi] = torch.from_numpy(h_lw[:, : hi - lo])
+                lw = lw.to(dev)
+                dist.all_reduce(lw)
+                ctx.set_linewidths(lw.cpu().numpy())
+            ctx.kappa_rta(Rxyz, out=h_kap)
+
+        for _ in range(max(1, args.warmup)):
+            step_e2e()
+        torch.cuda.synchronize()
+        et = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step_e2e()
+            e1.record(stream)
+            e1.synchronize()
+            et.append(e0.elapsed_time(e1))
+        e2e_ms = float(np.mean(et))
+        if world > 1:
+            t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_ms = float(t.item())
+
+    peak = fp64_peak_tflops(torch) if rank == 0 else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ph_grid, ph_irr = ctx.get_phonons(0), ctx.get_phonons(1)
+        sample = [1, nq0 // 2, nq0 - 1]
+        v, dt, thr = cpu_baseline(cr, mesh, TEMPS, ph_grid, ph_irr, irr["irr_q_pnt_int"], sample, "")
+        cpu = {"value": v, "unit": "evals/s", "cores": thr, "kind": "port",
+               "sample": f"{len(sample)} of {nq0} irreducible q0: enumeration, V3 in the reference loop order, "
+                         f"Gaussian sum at 3 T; phonons excluded ({dt:.1f} s)"}
+    if rank == 0:
+        value = evals_total / (ms * 1e-3)
+        v3_per_launch = v3_ms / max(v3_n, 1)
+        achieved = flops_pair * my_pairs / (v3_per_launch * 1e-3) / 1e12 if v3_n else None
+        line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "mesh": list(mesh), "irreducible_q0": nq0,
+                           "pairs": int(counts.sum()), "temperatures": TEMPS, "sigma_rad_ps": SIGMA,
+                           "delta": DELTA, "parallelism": f"q0-partition x{world}",
+                           "l2": "256 MiB buffer written between timed steps, outside the events"},
+                "roofline": {"kernel": "k_v3<gauss>", "bound": "fp64", "achieved": achieved, "peak": peak,
+                             "unit": "TFLOP/s", "frac": (achieved / peak) if (achieved and peak) else None,
+                             "traffic": None, "algorithmic_flops_per_pair": flops_pair,
+                             "kernel_ms_per_launch": v3_per_launch,
+                             "kernel_share_of_step": v3_per_launch / ms,
+                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run "
+                                            "(MEASURED_PEAKS.json holds no FP64 figure)"},
+                "cpu_baseline": cpu,
+                "e2e": {"value": evals_total / (e2e_ms * 1e-3), "unit": "evals/s", "ms_per_step": e2e_ms,
+                        "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+                "gpu_launches": int(launches),
+                "clocks": clk}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -120,6 +120,11 @@ int spring_get_phonons(spring_ctx* ctx, int which, double* evec, double* omega, 
  * algorithm's, on every mesh. */
 int spring_enumerate3(spring_ctx* ctx, int i0, int* Allq1q2, int* q1q2_permuted, int* counts);
 
+/* Enumerate the pairs of every irreducible q0 on the device (the same lists as
+ * spring_enumerate3, kept resident for the scattering calls).  The scattering
+ * calls run it on first use; calling it again recomputes it. */
+int spring_prepare3(spring_ctx* ctx);
+
 /* ---- three-phonon scattering ------------------------------------------ */
 /* ScatterProbAllq1, src/Kappa/Src/ThirdOrder_m.f90:41-166: the W3 of every
  * grid q1 for q0 = i0; sctrq1(Ndof,Ndof,Ndof,Nq) = (s2,s1,s0,q1). */
@@ -158,7 +163,20 @@ int spring_set_linewidths(spring_ctx* ctx, const double* lw_all);
 int spring_kappa_rta(spring_ctx* ctx, int symm, int nsym, const double* Rxyz, const int* s_range, double* kappa,
                      double* mode_k);
 
+/* ---- options ----------------------------------------------------------- */
+/* SPRING_OPT_GENERIC_V3 = 1: always use the any-cell V3 kernel (default 0 picks the
+ * two-atom specialisation when the cell fits it; both give the same W). */
+#define SPRING_OPT_GENERIC_V3 1
+int spring_set_option(spring_ctx* ctx, int option, int value);
+
 /* ---- diagnostics ------------------------------------------------------- */
+/* Record CUDA events around every kernel launch (on = 1) or stop (on = 0);
+ * turning it on clears earlier records. */
+int spring_set_profiling(spring_ctx* ctx, int on);
+/* Device time (ms) and launch count of the recorded launches whose kernel
+ * name starts with `prefix` (e.g. "k_v3"); synchronizes the stream. */
+int spring_kernel_time(spring_ctx* ctx, const char* prefix, double* ms, long long* launches);
+
 /* Make the n-th (1-based) subsequent device allocation (kind 0), host<->device
  * copy (kind 1) or kernel launch (kind 2) report failure without performing
  * it; n = 0 disarms.  For testing callers' error paths. */

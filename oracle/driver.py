@@ -75,6 +75,10 @@ def lib():
         L.orc_kappa_full.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, f64p, ct.c_int, ct.c_int,
                                      ct.c_double, ct.c_double, ct.c_double, f64p]
         L.orc_kappa_full.restype = None
+        L.orc_bte_iter.argtypes = [ct.c_int, ct.c_int, i32p, ct.c_int, i32p, i32p, i32p, i32p, i32p, f64p, f64p,
+                                   f64p, f64p, i32p, ct.c_double, ct.c_double, ct.c_double, ct.c_int, f64p, f64p,
+                                   f64p, f64p]
+        L.orc_bte_iter.restype = ct.c_int
         L.orc_num_threads.restype = ct.c_int
         _LIB = L
     return _LIB
@@ -330,3 +334,50 @@ def kappa_rta(st: Setup, lw, symm=True):
             out.append(kappa_full(st.q_pnt_int, st.pos, st.ph["omega"], st.ph["nbe"][it], st.ph["grp_vel"],
                                   lw[it], st.cr.vol, T))
     return np.array(out)
+
+
+# ----------------------------------------------------------------------------- iterative BTE
+def time_reversal_set(mesh, q_pnt_int):
+    """Irreducible set under q ~ -q (kappa_iter.x, Irr_q_point_m.f90:216-335) with the smaller grid
+    index as representative.  Returns (irr_grid, pos_tr, sgn_tr, neg, deg)."""
+    mesh = np.asarray(mesh)
+    neg_int = -np.asarray(q_pnt_int)
+    m = np.mod(neg_int, mesh[None, :])
+    neg = (m[:, 0] + mesh[0] * (m[:, 1] + mesh[1] * m[:, 2])).astype(np.int32)
+    g = np.arange(len(q_pnt_int))
+    rep = np.minimum(g, neg)
+    irr_grid = np.unique(rep).astype(np.int32)
+    pos = np.searchsorted(irr_grid, rep).astype(np.int32)
+    sgn = np.where(g == rep, 1, -1).astype(np.int32)
+    deg = np.bincount(pos, minlength=len(irr_grid)).astype(np.int32)
+    return irr_grid, pos, sgn, neg, deg
+
+
+def partner_map(mesh, q_pnt_int, q0_int):
+    """kappa.x's partner p(q1) = grid(-q0 - q1) (0-based)."""
+    mesh = np.asarray(mesh)
+    m = np.mod(-(np.asarray(q0_int)[None, :] + np.asarray(q_pnt_int)), mesh[None, :])
+    return (m[:, 0] + mesh[0] * (m[:, 1] + mesh[1] * m[:, 2])).astype(np.int32)
+
+
+def bte_iter(st: Setup, it=0, eps_k=1e-6, max_iter=1000):
+    """kappa_iter.x on the grid phonons of ``st`` at temperature index ``it``."""
+    irr_grid, pos, sgn, neg, deg = time_reversal_set(st.mesh, st.q_pnt_int)
+    nirr = len(irr_grid)
+    nd = st.cr.ndof
+    sctr = np.zeros((nirr, st.nq, nd, nd, nd))
+    part = np.zeros((nirr, st.nq), np.int32)
+    for i, g0 in enumerate(irr_grid):
+        q0 = st.q_pnt_int[g0]
+        A, perm, _ = momentum3(st.mesh, st.q_pnt_int, q0)
+        sctr[i] = scatter_w3(st.cr, st.q_pnt, st.q_pnt_int, q0, st.ph["evec"][g0], st.ph["onebyomega"][g0],
+                             st.ph["evec"], st.ph["onebyomega"], perm)
+        part[i] = partner_map(st.mesh, st.q_pnt_int, q0)
+    inv_tau = np.zeros((nirr, nd))
+    F = np.zeros((nirr, nd, 3))
+    krta = np.zeros(9)
+    kap = np.zeros(9)
+    iters = lib().orc_bte_iter(nd, st.nq, _i(st.tetra), nirr, irr_grid, pos, sgn, neg, part, _f(sctr),
+                               _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _f(st.ph["grp_vel"]), deg,
+                               float(st.temps[it]), st.cr.vol, eps_k, max_iter, inv_tau, F, krta, kap)
+    return dict(kappa=kap, kappa_rta=krta, inv_tau=inv_tau, F=F, iters=iters, irr_grid=irr_grid, deg=deg)

@@ -549,13 +549,16 @@ void orc_lw3_gauss(int ndof, int nq, const double* omega0, const double* omega, 
     const size_t n3 = (size_t)ndof * ndof * ndof;
     const double os = 1.0 / sigma, os2 = os * os;
     for (int s = 0; s < ndof; ++s) { lw[s] = 0.0; P3_q0[s] = 0.0; }
+    // s0 outermost (parallel): for each s0 the q1 accumulation order is the reference's
+#pragma omp parallel for schedule(static, 1)
+    for (int s0 = pol[0]; s0 <= pol[1]; ++s0)
     for (int q1 = 0; q1 < nq; ++q1) {
         const int q2 = Allq1q2[4 * q1 + 3] - 1;
         const int* a = q_pnt_int + 3 * q1;
         const int* b = q_pnt_int + 3 * q2;
         const int st1 = (a[0] == 0 && a[1] == 0 && a[2] == 0) ? 4 : 1;
         const int st2 = (b[0] == 0 && b[1] == 0 && b[2] == 0) ? 4 : 1;
-        for (int s0 = pol[0]; s0 <= pol[1]; ++s0) {
+        {
             double acc = 0.0, ps = 0.0;
             for (int s1 = std::max(st1, pol[2]); s1 <= pol[3]; ++s1)
                 for (int s2 = std::max(st2, pol[4]); s2 <= pol[5]; ++s2) {
@@ -723,6 +726,167 @@ void orc_kappa_full(int ndof, int nq, const int* q_pnt_int, const int* pos, cons
         }
     }
     for (int k = 0; k < 9; ++k) kappa[k] *= f2;
+}
+
+// ---------------------------------------------------------------------------
+// Iterative BTE of kappa_iter.x (src/Kappa/Src_iterative):
+//   TetrahedronWplus/Wminus (Quasi_momentum_consrv.f90:701-1208) -> 1/tau,
+//   CreateFzero (HelperSubroutines.f90:118-185), TetrahedronIterPlus/Minus
+//   (TetrahedronDeltaSum.f90:22-607), multiplyTaudFnew (:188-232), kappa (:277-347),
+//   loop main.f90:295-361 (stop when max|dkappa| < eps_k or after max_iter).
+// Irreducible set: time reversal only (q ~ -q), as Irr_q_point_m.f90:216-335.
+// The W of each vertex is taken from kappa.x's Sctrq1 of the same q0 (both
+// orientations of every pair are stored there), times 4: kappa_iter's
+// Sctr3THz2 carries pi/4 where kappa.x's carries pi/16 (constants.f90:53-54).
+// Vertex structure, in grid indices (0-based here):
+//   plus  channel: vertex x, partner ConsrvPlus%q2indx = -p(x), M = w(-p(x),s2) - w(x,s1),
+//                  W+ = 4 W3(q0; x s1; p(x) s2) (n(x,s1) - n(p(x),s2)),
+//                  dF += (F(-p(x),s2) - F(x,s1)) terms;
+//   minus channel: vertex v, partner u = q0 - v, M = w(v,s1) + w(u,s2),
+//                  W- = 4 W3(q0; -v s1; p(-v) s2) (1 + n(-v,s1) + n(p(-v),s2)),
+//                  dF += 0.5 (F(v,s1) + F(u,s2)) terms;
+// where p(x) = grid(-q0 - x) is kappa.x's partner.  Strict case bounds, and a
+// vertex set only counts when |sum(I) - 1| < zero_prec.
+//   n_irr irreducible points: irr_grid[i] grid index of the representative,
+//   pos_tr[q] irreducible index of grid point q, sgn_tr[q] = +1 (representative) / -1;
+//   neg[q] grid index of -q; partner[i][q] = p(q) for q0 = irr i;
+//   sctr[i][q][s0][s1][s2] kappa.x W3; omega[q][s], nbe[q][s] (one T), vel[q][s][3];
+//   deg[i] number of grid points of irreducible point i.
+// Outputs inv_tau[i][s], F[i][s][3], kappa_rta[9] (iteration 0), kappa[9]; returns iterations.
+int orc_bte_iter(int ndof, int nq, const int* tetra, int n_irr, const int* irr_grid, const int* pos_tr,
+                 const int* sgn_tr, const int* neg, const int* partner, const double* sctr, const double* omega,
+                 const double* nbe, const double* vel, const int* deg, double T, double vol, double eps_k,
+                 int max_iter, double* inv_tau, double* F, double* kappa_rta, double* kappa) {
+    const int n = ndof;
+    const size_t n3 = (size_t)n * n * n;
+    const int ntet = 6 * nq;
+    const double FunitE = 1.054571817 / 1.380649;
+    const double kW_mK = 1.054571817 * 0.001;
+    const double mfac_k = 1.0 / (double(nq) * vol);
+    std::vector<double> F0((size_t)n_irr * n * 3, 0.0), dF((size_t)n_irr * n * 3, 0.0);
+    auto Fat = [&](const double* Fv, int q, int s, int k) { return sgn_tr[q] * Fv[((size_t)pos_tr[q] * n + s) * 3 + k]; };
+
+    // one pass over both channels; mode 0 accumulates 1/tau, mode 1 accumulates dF from Fv
+    auto pass = [&](int mode, const double* Fv) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            const int* p = partner + (size_t)i * nq;
+            const double* W3 = sctr + (size_t)i * nq * n3;
+            for (int nT = 0; nT < ntet; ++nT) {
+                int v1[4];
+                for (int v = 0; v < 4; ++v) v1[v] = tetra[4 * nT + v] - 1;
+                for (int s = 0; s < n; ++s) {
+                    const double Mqs = omega[(size_t)g0 * n + s];
+                    for (int s1 = 0; s1 < n; ++s1)
+                        for (int s2 = 0; s2 < n; ++s2)
+                            for (int ch = 0; ch < 2; ++ch) {
+                                double M[4], Fdummy[4];
+                                int a1[4], a2[4];
+                                for (int v = 0; v < 4; ++v) {
+                                    const int x = v1[v];
+                                    if (ch == 0) {  // plus
+                                        const int q2 = neg[p[x]];
+                                        M[v] = omega[(size_t)q2 * n + s2] - omega[(size_t)x * n + s1];
+                                        a2[v] = q2;
+                                    } else {        // minus
+                                        const int u = neg[p[neg[x]]];
+                                        M[v] = omega[(size_t)x * n + s1] + omega[(size_t)u * n + s2];
+                                        a2[v] = u;
+                                    }
+                                    a1[v] = x;
+                                    Fdummy[v] = 0.0;
+                                }
+                                double g, I[4];
+                                const bool e = find_g_iver(Mqs, &g, I, M, Fdummy, a1, a2, 1);
+                                if (!e) continue;
+                                const double sI = I[0] + I[1] + I[2] + I[3];
+                                if (!(std::fabs(sI - 1.0) < zero_prec)) continue;
+                                double tv = 0.0, tf[3] = {0.0, 0.0, 0.0};
+                                for (int v = 0; v < 4; ++v) {
+                                    const int x = a1[v];
+                                    double Wv;
+                                    if (ch == 0) {
+                                        const double w3 = 4.0 * W3[(size_t)x * n3 + ((size_t)s * n + s1) * n + s2];
+                                        Wv = w3 * (nbe[(size_t)x * n + s1] - nbe[(size_t)p[x] * n + s2]);
+                                    } else {
+                                        const int y = neg[x];
+                                        const double w3 = 4.0 * W3[(size_t)y * n3 + ((size_t)s * n + s1) * n + s2];
+                                        Wv = w3 * (1.0 + nbe[(size_t)y * n + s1] + nbe[(size_t)p[y] * n + s2]);
+                                    }
+                                    if (mode == 0) {
+                                        tv += I[v] * Wv;
+                                    } else {
+                                        for (int k = 0; k < 3; ++k) {
+                                            const double f1 = Fat(Fv, x, s1, k), f2 = Fat(Fv, a2[v], s2, k);
+                                            tf[k] += (I[v] * Wv) * (ch == 0 ? (f2 - f1) : (f2 + f1));
+                                        }
+                                    }
+                                }
+                                const double pre = ch == 0 ? OnebySix * g : 0.5 * OnebySix * g;
+                                if (mode == 0) inv_tau[(size_t)i * n + s] += pre * tv;
+                                else
+                                    for (int k = 0; k < 3; ++k) dF[((size_t)i * n + s) * 3 + k] += pre * tf[k];
+                            }
+                }
+            }
+        }
+    };
+    auto kappa_of = [&](const double* Fv, double* out) {
+        for (int k = 0; k < 9; ++k) out[k] = 0.0;
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            const bool gamma = g0 == 0;
+            for (int s = gamma ? 3 : 0; s < n; ++s) {
+                const double w = omega[(size_t)g0 * n + s], nq_ = nbe[(size_t)g0 * n + s];
+                const double* v = vel + ((size_t)g0 * n + s) * 3;
+                const double* f = Fv + ((size_t)i * n + s) * 3;
+                const double pre = double(deg[i]) * w * nq_ * (nq_ + 1.0);
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) out[3 * a + b] += pre * (v[a] * f[b]);
+            }
+        }
+        for (int k = 0; k < 9; ++k) out[k] = kW_mK * mfac_k * out[k];
+    };
+
+    for (size_t k = 0; k < (size_t)n_irr * n; ++k) inv_tau[k] = 0.0;
+    pass(0, nullptr);
+    for (int i = 0; i < n_irr; ++i) {
+        const int g0 = irr_grid[i];
+        for (int s = (g0 == 0 ? 3 : 0); s < n; ++s) {
+            const double it = inv_tau[(size_t)i * n + s];
+            if (std::fabs(it) > zero_prec)
+                for (int k = 0; k < 3; ++k)
+                    F0[((size_t)i * n + s) * 3 + k] =
+                        FunitE * omega[(size_t)g0 * n + s] * vel[((size_t)g0 * n + s) * 3 + k] / (it * (T * T));
+        }
+    }
+    std::vector<double> Fc(F0);
+    kappa_of(Fc.data(), kappa_rta);
+    double kold[9];
+    for (int k = 0; k < 9; ++k) kold[k] = kappa_rta[k];
+    int iter = 0;
+    for (;;) {
+        ++iter;
+        std::fill(dF.begin(), dF.end(), 0.0);
+        pass(1, Fc.data());
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            for (int s = (g0 == 0 ? 3 : 0); s < n; ++s) {
+                const double it = inv_tau[(size_t)i * n + s];
+                if (std::fabs(it) > zero_prec)
+                    for (int k = 0; k < 3; ++k) dF[((size_t)i * n + s) * 3 + k] /= it;
+            }
+        }
+        for (size_t k = 0; k < Fc.size(); ++k) Fc[k] = F0[k] + dF[k];
+        kappa_of(Fc.data(), kappa);
+        double acc = 0.0;
+        for (int k = 0; k < 9; ++k) acc = std::max(acc, std::fabs(kappa[k] - kold[k]));
+        if (acc < eps_k || iter > max_iter) break;
+        for (int k = 0; k < 9; ++k) kold[k] = kappa[k];
+    }
+    std::memcpy(F, Fc.data(), sizeof(double) * Fc.size());
+    return iter;
 }
 
 int orc_num_threads() {

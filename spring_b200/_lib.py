@@ -47,6 +47,10 @@ SIGNATURES = {
     "spring_set_phonons": [P, I, P, P, P, P, P, P],
     "spring_get_phonons": [P, I, P, P, P, P, P],
     "spring_enumerate3": [P, I, P, P, P],
+    "spring_prepare3": [P],
+    "spring_set_profiling": [P, I],
+    "spring_set_option": [P, I, I],
+    "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_scatter_w3": [P, I, P],
     "spring_linewidth3": [P, I, I, I, D, P, P, P],
     "spring_linewidth_iso": [P, I, I, I, D, P, P],

@@ -91,6 +91,26 @@ class Context:
     def inject_fault(self, kind: int, n: int):
         self._call("spring_debug_inject_fault", int(kind), int(n))
 
+    def set_option(self, option: int, value: int):
+        self._call("spring_set_option", int(option), int(value))
+
+    def use_generic_v3(self, on: bool = True):
+        """Force the any-cell V3 kernel instead of the two-atom specialisation."""
+        self.set_option(1, int(bool(on)))
+
+    def set_profiling(self, on: bool):
+        self._call("spring_set_profiling", int(bool(on)))
+
+    def kernel_time(self, prefix: str):
+        """(device ms, launches) of the recorded launches whose kernel name starts with ``prefix``."""
+        ms = ct.c_double()
+        n = ct.c_longlong()
+        self._call("spring_kernel_time", prefix.encode(), ct.byref(ms), ct.byref(n))
+        return float(ms.value), int(n.value)
+
+    def prepare3(self):
+        self._call("spring_prepare3")
+
     # -- cell%init_data / FC readers
     def set_crystal(self, latvec, mass):
         lat = _c(np.asarray(latvec).T, np.float64)  # Fortran latvec(3,3): columns are vectors
@@ -164,9 +184,15 @@ class Context:
 
     # -- linewidths
     def linewidth3(self, i0_first: int, n_q0: int, delta: str = "gauss", sigma: float = 0.3767, pol3=None,
-                   want=True):
+                   want=True, out=None):
+        """``want=False``: results stay on the device; ``out``: a caller-owned (nT, n_q0, Ndof) float64
+        array (e.g. pinned) that receives the linewidths, without the phase space."""
         mode = L.SPRING_DELTA_GAUSS if delta == "gauss" else L.SPRING_DELTA_TETRA
         pol = None if pol3 is None else _c(pol3, np.int32)
+        if out is not None:
+            assert out.dtype == np.float64 and out.flags.c_contiguous and out.shape == (self.n_temps, n_q0, self.ndof)
+            self._call("spring_linewidth3", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), _ptr(out), None)
+            return out
         if not want:
             self._call("spring_linewidth3", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), None, None)
             return None
@@ -197,14 +223,17 @@ class Context:
         self._call("spring_set_linewidths", _ptr(_c(lw, np.float64)))
 
     # -- kappa_noIter(_symm)
-    def kappa_rta(self, Rxyz=None, symm=True, s_range=None, mode=False):
+    def kappa_rta(self, Rxyz=None, symm=True, s_range=None, mode=False, want=True, out=None):
         R = None
         nsym = 0
         if symm:
             R = _c(np.transpose(np.asarray(Rxyz), (0, 2, 1)), np.float64)  # Rxyz(3,3,Nsym) column-major
             nsym = R.shape[0]
         sr = None if s_range is None else _c(s_range, np.int32)
-        kap = np.zeros((self.n_temps, 9))
+        if not want:
+            self._call("spring_kappa_rta", int(bool(symm)), nsym, _ptr(R), _ptr(sr), None, None)
+            return None
+        kap = np.zeros((self.n_temps, 9)) if out is None else out
         mk = np.zeros((self.n_temps, self.ndof, 9)) if mode else None
         self._call("spring_kappa_rta", int(bool(symm)), nsym, _ptr(R), _ptr(sr), _ptr(kap), _ptr(mk))
         return (kap, mk) if mode else kap

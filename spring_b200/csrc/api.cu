@@ -81,12 +81,39 @@ int zero(spring_ctx* c, void* dst, size_t bytes, const char* what) {
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
 }
 
-bool launch_injected(spring_ctx* c) { return injected(c, 2); }
+bool launch_injected(spring_ctx* c) {
+    if (injected(c, 2)) return true;
+    if (c->profiling && !c->prof_pending) {
+        if (cudaEventCreate(&c->prof_pending) == cudaSuccess) cudaEventRecord(c->prof_pending, c->stream);
+        else c->prof_pending = nullptr;
+    }
+    return false;
+}
 
 int launch_check(spring_ctx* c, const char* what) {
     c->launches += 1;
     cudaError_t e = cudaGetLastError();
+    if (c->profiling && c->prof_pending) {
+        cudaEvent_t stop;
+        if (cudaEventCreate(&stop) == cudaSuccess) {
+            cudaEventRecord(stop, c->stream);
+            c->prof.push_back({what, c->prof_pending, stop});
+        } else {
+            cudaEventDestroy(c->prof_pending);
+        }
+        c->prof_pending = nullptr;
+    }
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+void clear_profile(spring_ctx* c) {
+    for (auto& r : c->prof) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    c->prof.clear();
+    if (c->prof_pending) cudaEventDestroy(c->prof_pending);
+    c->prof_pending = nullptr;
 }
 
 }  // namespace spring
@@ -215,12 +242,15 @@ int spring_ctx_destroy(spring_ctx* c) {
     {
         DeviceGuard g(c->device);
         cudaStreamSynchronize(c->stream);
+        clear_profile(c);
         dfree(c->d_mass_rs); dfree(c->d_fc2); dfree(c->d_fc2_idx); dfree(c->d_fc2_num);
-        dfree(c->d_fc3t); dfree(c->d_fc3_posr); dfree(c->d_fc3_btyp);
+        dfree(c->d_fc3); dfree(c->d_fc3_off); dfree(c->d_fc3_posr); dfree(c->d_fc3_btyp);
         dfree(c->d_qint); dfree(c->d_qpnt); dfree(c->d_tetra);
         dfree(c->d_irr_int); dfree(c->d_irr_q); dfree(c->d_mult); dfree(c->d_pos); dfree(c->d_temps);
         free_phonons(c->ph_grid); free_phonons(c->ph_irr);
-        dfree(c->d_partner); dfree(c->d_pairoff); dfree(c->d_pairs); dfree(c->d_pair_q0); dfree(c->d_pairpos);
+        free_pairs(c->ps_irr); free_pairs(c->ps_tr);
+        dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
+        dfree(c->d_neg); dfree(c->d_wtr);
         dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -247,6 +277,52 @@ int spring_kernel_launches(const spring_ctx* c, long long* count) {
     if (!c || !count) return SPRING_ERR_ARG;
     *count = c->launches;
     return SPRING_OK;
+}
+
+int spring_set_option(spring_ctx* c, int option, int value) {
+    CTX_ENTER(c);
+    switch (option) {
+        case SPRING_OPT_GENERIC_V3: c->force_generic_v3 = value != 0; return SPRING_OK;
+        default: return fail(c, SPRING_ERR_ARG, "unknown option %d", option);
+    }
+}
+
+int spring_set_profiling(spring_ctx* c, int on) {
+    CTX_ENTER(c);
+    cudaStreamSynchronize(c->stream);
+    clear_profile(c);
+    c->profiling = on != 0;
+    return SPRING_OK;
+}
+
+int spring_kernel_time(spring_ctx* c, const char* prefix, double* ms, long long* count) {
+    CTX_ENTER(c);
+    if (!prefix || !ms) return fail(c, SPRING_ERR_ARG, "prefix/ms is NULL");
+    cudaError_t e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, "kernel_time");
+    double tot = 0.0;
+    long long n = 0;
+    const size_t lp = std::strlen(prefix);
+    for (auto& r : c->prof) {
+        if (r.name.compare(0, lp, prefix) != 0) continue;
+        float t = 0.f;
+        if (cudaEventElapsedTime(&t, r.start, r.stop) == cudaSuccess) {
+            tot += t;
+            ++n;
+        }
+    }
+    *ms = tot;
+    if (count) *count = n;
+    return SPRING_OK;
+}
+
+int spring_prepare3(spring_ctx* c) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
+    c->ps_irr.n0 = c->nq0;
+    c->ps_irr.q0_int = c->d_irr_int.p;
+    return run_enumerate3(c, c->ps_irr);
 }
 
 int spring_debug_inject_fault(spring_ctx* c, int kind, int n) {
@@ -317,35 +393,48 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     if (!num || !idx || !fc || na3 < 1 || na3 > 16) return fail(c, SPRING_ERR_ARG, "FC3 arrays are NULL or na3 not in 1..16");
     const int nb = c->nb;
     // kernel layout: [mu][k2 = N2*3+gamma][r = (N1*3+alpha)*3+beta], zero padded beyond atm_num
-    const int K = 3 * na3, R = 9 * na3;
-    std::vector<double> t((size_t)nb * K * R, 0.0), posr((size_t)nb * na3 * 3, 0.0);
-    std::vector<int> btyp((size_t)nb * na3, 0);
+    // Device layout [mu][N1][N2][alpha][beta][gamma] (the Fortran memory order), zero beyond
+    // atm_num, with the neighbour slots of each mu reordered so that slots of the same basis
+    // atom are contiguous (stable); off[mu][nu] .. off[mu][nu+1] are the slots of basis nu.
+    // Only the order of the sums over N1/N2 changes.
+    std::vector<double> t((size_t)nb * na3 * na3 * 27, 0.0), posr((size_t)nb * na3 * 3, 0.0);
+    std::vector<int> btyp((size_t)nb * na3, 0), off((size_t)nb * (nb + 1), 0);
     for (int mu = 0; mu < nb; ++mu) {
         if (num[mu] < 0 || num[mu] > na3) return fail(c, SPRING_ERR_ARG, "FC3 atm_num(%d) out of range", mu + 1);
-        for (int n = 0; n < num[mu]; ++n) {
+        std::vector<int> order;  // new slot -> original slot
+        for (int nu = 0; nu < nb; ++nu) {
+            off[(size_t)mu * (nb + 1) + nu] = (int)order.size();
+            for (int n = 0; n < num[mu]; ++n) {
+                const int* e = idx + 4 * (n + (size_t)na3 * mu);
+                if (e[3] < 1 || e[3] > nb) return fail(c, SPRING_ERR_ARG, "FC3 atm_indx basis out of range");
+                if (e[3] - 1 == nu) order.push_back(n);
+            }
+        }
+        off[(size_t)mu * (nb + 1) + nb] = (int)order.size();
+        for (int k = 0; k < num[mu]; ++k) {
+            const int n = order[k];
             const int* e = idx + 4 * (n + (size_t)na3 * mu);
-            if (e[3] < 1 || e[3] > nb) return fail(c, SPRING_ERR_ARG, "FC3 atm_indx basis out of range");
-            btyp[(size_t)mu * na3 + n] = e[3] - 1;
+            btyp[(size_t)mu * na3 + k] = e[3] - 1;
             for (int r = 0; r < 3; ++r)  // atmPosR = latvec * cell (FC3_mod.f90:84)
-                posr[((size_t)mu * na3 + n) * 3 + r] =
+                posr[((size_t)mu * na3 + k) * 3 + r] =
                     c->latvec[r] * e[0] + c->latvec[r + 3] * e[1] + c->latvec[r + 6] * e[2];
         }
-        for (int n1 = 0; n1 < num[mu]; ++n1)
-            for (int n2 = 0; n2 < num[mu]; ++n2)
-                for (int al = 0; al < 3; ++al)
-                    for (int be = 0; be < 3; ++be)
-                        for (int ga = 0; ga < 3; ++ga) {
-                            // Fortran fC(ga,be,al,N2,N1,mu)
-                            size_t fi = ga + 3 * (be + 3 * (al + 3 * (n2 + (size_t)na3 * (n1 + (size_t)na3 * mu))));
-                            int k2 = n2 * 3 + ga, r = (n1 * 3 + al) * 3 + be;
-                            t[((size_t)mu * K + k2) * R + r] = fc[fi];
-                        }
+        for (int k1 = 0; k1 < num[mu]; ++k1)
+            for (int k2 = 0; k2 < num[mu]; ++k2)
+                for (int abc = 0; abc < 27; ++abc) {
+                    // Fortran fC(ga,be,al,N2,N1,mu): abc = (al*3+be)*3+ga is the fastest index
+                    const int n1 = order[k1], n2 = order[k2];
+                    t[((size_t)(mu * na3 + k1) * na3 + k2) * 27 + abc] =
+                        fc[((size_t)(mu * na3 + n1) * na3 + n2) * 27 + abc];
+                }
     }
     c->na3 = na3;
-    SPRING_CHECK(dalloc(c, c->d_fc3t, t.size(), "FC3"));
+    SPRING_CHECK(dalloc(c, c->d_fc3_off, off.size(), "FC3 slot offsets"));
+    SPRING_CHECK(h2d(c, c->d_fc3_off.p, off.data(), sizeof(int) * off.size(), "FC3 slot offsets"));
+    SPRING_CHECK(dalloc(c, c->d_fc3, t.size(), "FC3"));
     SPRING_CHECK(dalloc(c, c->d_fc3_posr, posr.size(), "FC3 positions"));
     SPRING_CHECK(dalloc(c, c->d_fc3_btyp, btyp.size(), "FC3 basis"));
-    SPRING_CHECK(h2d(c, c->d_fc3t.p, t.data(), sizeof(double) * t.size(), "FC3"));
+    SPRING_CHECK(h2d(c, c->d_fc3.p, t.data(), sizeof(double) * t.size(), "FC3"));
     SPRING_CHECK(h2d(c, c->d_fc3_posr.p, posr.data(), sizeof(double) * posr.size(), "FC3 positions"));
     SPRING_CHECK(h2d(c, c->d_fc3_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC3 basis"));
     SPRING_CHECK(spring_synchronize(c));
@@ -373,7 +462,9 @@ int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_
     }
     SPRING_CHECK(spring_synchronize(c));
     c->mesh_set = true;
-    c->enum3_done = false;
+    c->ps_irr.done = false;
+    c->ps_tr.done = false;
+    c->ntr = 0;
     return SPRING_OK;
 }
 
@@ -401,7 +492,9 @@ static int install_irr(spring_ctx* c, int nq0, const int* irr_int, const int* po
     SPRING_CHECK(zero(c, c->d_lw_all.p, sizeof(double) * c->nT * nq0 * c->ndof, "LW_Allq0"));
     SPRING_CHECK(spring_synchronize(c));
     c->irr_set = true;
-    c->enum3_done = false;
+    c->ps_irr.done = false;
+    c->ps_irr.n0 = nq0;
+    c->ps_irr.q0_int = c->d_irr_int.p;
     free_phonons(c->ph_irr);
     return SPRING_OK;
 }
@@ -513,10 +606,10 @@ int spring_enumerate3(spring_ctx* c, int i0, int* allq1q2, int* perm, int* count
 }
 
 static int ensure_enum3(spring_ctx* c) {
-    if (c->enum3_done) return SPRING_OK;
-    SPRING_CHECK(run_enumerate3(c));
-    c->enum3_done = true;
-    return SPRING_OK;
+    if (c->ps_irr.done) return SPRING_OK;
+    c->ps_irr.n0 = c->nq0;
+    c->ps_irr.q0_int = c->d_irr_int.p;
+    return run_enumerate3(c, c->ps_irr);
 }
 
 static int ready3(spring_ctx* c) {
@@ -542,7 +635,7 @@ int spring_scatter_w3(spring_ctx* c, int i0, double* sctr) {
     SPRING_CHECK(ensure_enum3(c));
     const size_t n = (size_t)c->nq * c->ndof * c->ndof * c->ndof;
     SPRING_CHECK(dalloc(c, c->d_w, n, "W buffer"));
-    SPRING_CHECK(run_v3_wgrid(c, i0 - 1, 1, c->d_w.p));
+    SPRING_CHECK(run_v3_wgrid(c, c->ps_irr, irr_view(c), i0 - 1, 1, c->d_w.p));
     if (sctr) SPRING_CHECK(d2h(c, sctr, c->d_w.p, sizeof(double) * n, "Sctrq1"));
     return SPRING_OK;
 }
@@ -573,7 +666,7 @@ int spring_linewidth3(spring_ctx* c, int i0_first, int n_q0, int delta_mode, dou
         SPRING_CHECK(dalloc(c, c->d_w, slot * slots, "W buffer"));
         for (int b = 0; b < n_q0; b += slots) {
             const int nb = std::min(slots, n_q0 - b);
-            SPRING_CHECK(run_v3_wgrid(c, q0 + b, nb, c->d_w.p));
+            SPRING_CHECK(run_v3_wgrid(c, c->ps_irr, irr_view(c), q0 + b, nb, c->d_w.p));
             SPRING_CHECK(run_tetra3(c, q0 + b, nb, c->d_w.p, pol, c->d_lw_tmp.p, c->d_p3.p));
         }
     }

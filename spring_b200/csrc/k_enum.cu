@@ -109,62 +109,56 @@ int run_exclusive_scan(spring_ctx* c, const int* d_in, int* d_out, int n) {
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, "exclusive scan");
 }
 
-int run_enumerate3(spring_ctx* c) {
-    const long long total = (long long)c->nq0 * c->nq;
+int run_enumerate3(spring_ctx* c, PairSet& ps) {
+    ps.done = false;
+    const long long total = (long long)ps.n0 * c->nq;
     if (total > 0x7fffffffLL) return fail(c, SPRING_ERR_UNSUPPORTED, "Nq0 * Nq exceeds 2^31");
-    DBuf<int> rep, pos;
-    SPRING_CHECK(dalloc(c, c->d_partner, total, "partner map"));
+    DBuf<int> rep;
+    SPRING_CHECK(dalloc(c, ps.partner, total, "partner map"));
     int rc = dalloc(c, rep, total, "representative flags");
-    if (rc == SPRING_OK) rc = dalloc(c, pos, total, "pair positions");
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pairpos, total, "pair positions");
     const int threads = 256;
     const int blocks = (int)std::min<long long>((total + threads - 1) / threads, 148LL * 32);
     if (rc == SPRING_OK && launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
     if (rc == SPRING_OK) {
-        k_enum3_flags<<<blocks, threads, 0, c->stream>>>(c->nq, c->nq0, c->mesh[0], c->mesh[1], c->mesh[2],
-                                                         c->d_irr_int.p, c->d_qint.p, c->d_partner.p, rep.p);
+        k_enum3_flags<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, c->mesh[0], c->mesh[1], c->mesh[2],
+                                                         ps.q0_int, c->d_qint.p, ps.partner.p, rep.p);
         rc = launch_check(c, "k_enum3_flags");
     }
-    if (rc == SPRING_OK) rc = run_exclusive_scan(c, rep.p, pos.p, (int)total);
+    if (rc == SPRING_OK) rc = run_exclusive_scan(c, rep.p, ps.pairpos.p, (int)total);
     int last[2] = {0, 0};
-    if (rc == SPRING_OK) rc = d2h(c, &last[0], pos.p + total - 1, sizeof(int), "pair count");
+    if (rc == SPRING_OK) rc = d2h(c, &last[0], ps.pairpos.p + total - 1, sizeof(int), "pair count");
     if (rc == SPRING_OK) rc = d2h(c, &last[1], rep.p + total - 1, sizeof(int), "pair count");
     const int npairs = last[0] + last[1];
-    if (rc == SPRING_OK) rc = dalloc(c, c->d_pairs, npairs, "pair list");
-    if (rc == SPRING_OK) rc = dalloc(c, c->d_pair_q0, npairs, "pair list");
-    if (rc == SPRING_OK) rc = dalloc(c, c->d_pairoff, c->nq0 + 1, "pair offsets");
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pairs, npairs, "pair list");
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, npairs, "pair list");
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pairoff, ps.n0 + 1, "pair offsets");
+    if (rc == SPRING_OK && launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
     if (rc == SPRING_OK) {
-        k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, c->nq0, c->d_partner.p, rep.p, pos.p, c->d_pairs.p,
-                                                         c->d_pair_q0.p, c->d_pairoff.p);
+        k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, ps.partner.p, rep.p, ps.pairpos.p, ps.pairs.p,
+                                                         ps.pair_q0.p, ps.pairoff.p);
         rc = launch_check(c, "k_enum3_pairs");
     }
     if (rc == SPRING_OK) {
-        c->h_pairoff.assign(c->nq0 + 1, 0);
-        rc = d2h(c, c->h_pairoff.data(), c->d_pairoff.p, sizeof(int) * (c->nq0 + 1), "pair offsets");
-    }
-    // keep the positions of every (q0, q1) for the Fortran-layout output
-    if (rc == SPRING_OK) {
-        dfree(c->d_pairpos);
-        c->d_pairpos = pos;
-        pos = DBuf<int>();
+        ps.h_pairoff.assign(ps.n0 + 1, 0);
+        rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
     }
     dfree(rep);
-    dfree(pos);
+    if (rc == SPRING_OK) ps.done = true;
     return rc;
 }
 
 int run_enumerate3_fortran(spring_ctx* c, int q0, int* d_allq1q2, int* d_perm, int* d_counts) {
-    if (!c->enum3_done) {
-        SPRING_CHECK(run_enumerate3(c));
-        c->enum3_done = true;
-    }
-    const int* p = c->d_pairpos.p + (size_t)q0 * c->nq;
-    const int base = c->h_pairoff[q0];
+    PairSet& ps = c->ps_irr;
+    if (!ps.done) SPRING_CHECK(run_enumerate3(c, ps));
+    const int* p = ps.pairpos.p + (size_t)q0 * c->nq;
+    const int base = ps.h_pairoff[q0];
     SPRING_CHECK(zero(c, d_counts, 2 * sizeof(int), "counts"));
     const int threads = 256, blocks = (c->nq + threads - 1) / threads;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
     k_enum3_fortran<<<blocks, threads, 0, c->stream>>>(c->nq, c->mesh[0], c->mesh[1], c->mesh[2],
-                                                       c->d_irr_int.p + 3 * q0, c->d_qint.p,
-                                                       c->d_partner.p + (size_t)q0 * c->nq, p, base, d_allq1q2, d_perm,
+                                                       ps.q0_int + 3 * q0, c->d_qint.p,
+                                                       ps.partner.p + (size_t)q0 * c->nq, p, base, d_allq1q2, d_perm,
                                                        d_counts);
     return launch_check(c, "k_enum3_fortran");
 }

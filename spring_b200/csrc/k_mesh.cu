@@ -120,6 +120,7 @@ int run_make_mesh(spring_ctx* c, const int shift[3], int zc) {
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "make_mesh: injected launch failure");
     k_grid_points<<<blocks, threads, 0, c->stream>>>(a, c->d_qint.p, c->d_qpnt.p);
     SPRING_CHECK(launch_check(c, "k_grid_points"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "make_mesh: injected launch failure");
     k_tetrahedra<<<blocks, threads, 0, c->stream>>>(a, reinterpret_cast<int4*>(c->d_tetra.p));
     return launch_check(c, "k_tetrahedra");
 }

@@ -346,7 +346,7 @@ int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const P
         a.s0n = std::min(NS0, pol.hi[0] - s0a + 1);
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "tetra3: injected launch failure");
         const int4* tet = reinterpret_cast<const int4*>(c->d_tetra.p);
-        const int* part = c->d_partner.p;
+        const int* part = c->ps_irr.partner.p;
         if (c->nT == 1) {
             k_tetra3<1><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, c->ph_irr.omega.p, c->ph_grid.omega.p,
                                                           c->ph_grid.nbe.p, d_lw, d_p3);
@@ -383,6 +383,7 @@ int run_iso(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma,
                                                    c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_grid.evec.p, c->d_wiso.p);
         rc = launch_check(c, "k_iso_w");
         if (rc != SPRING_OK) break;
+        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "iso: injected launch failure"); break; }
         if (delta_mode == SPRING_DELTA_TETRA) {
             const long long items = 6LL * c->nq * c->ndof;
             dim3 grid(grid_x(items, threads, ns), ns);

@@ -5,25 +5,30 @@
 // linewidth CalculateLinewidth (:442-543).
 //
 // The reference evaluates Phi(s2,s1,s) in a 9-deep loop (~Na3^2*27*Ndof^3
-// complex MACs per pair).  Here the sum is factored into three contractions
-// per basis atom mu (FC3 is real, phases are per neighbour slot):
-//   E1[N1 b][s1] = e^{i q1.R_N1} m_nu^-1/2 e1(nu b, s1)        (nu = basis of N1)
-//   E2[N2 c][s2] = e^{i q2.R_N2} m_eta^-1/2 e2(eta c, s2)
-//   Y[(N1 a) b][s2] = sum_{N2 c} FC3(c,b,a,N2,N1,mu) E2[N2 c][s2]   (real x complex GEMM, K = 3 Na3)
-//   Z[a][s1][s2]    = sum_{N1 b} E1[N1 b][s1] Y[(N1 a) b][s2]
-//   Phi[s0][s1][s2] += sum_a m_mu^-1/2 e0(mu a, s0) Z[a][s1][s2]
+// complex MACs per pair).  Here the sum is regrouped: the neighbour phases
+// depend on the neighbour slot while the eigenvectors depend only on its basis
+// atom, so the phases are folded into the force constants first,
+//   D_mu[a][nu b][eta c] = sum_{N1 in nu, N2 in eta} FC3(c,b,a,N2,N1,mu)
+//                          e^{i q1.R_N1} e^{i q2.R_N2} m_nu^-1/2 m_eta^-1/2,
+// and the eigenvectors enter through three Ndof^4 contractions:
+//   T1[a][nu b][s2] = sum_{eta c} D_mu[a][nu b][eta c] e2(eta c, s2)
+//   T2[a][s1][s2]   = sum_{nu b}  e1(nu b, s1) T1[a][nu b][s2]
+//   Phi[s0][s1][s2] += sum_a m_mu^-1/2 e0(mu a, s0) T2[a][s1][s2]
+// 4*27*sum_mu Na3^2 + 3*8*Ndof^4 flops per pair (41.7 kflop for the 2-atom cell).
 // W = |Phi|^2 (1/w0)(1/w1)(1/w2) Sctr3THz2/Nq, zero for Gamma acoustic modes.
 //
-// One CTA handles one (pair, block of s0) work item, so that Phi fits in shared
-// memory for Ndof up to 24.  Two epilogues:
+// One CTA handles one (pair, block of s0) work item, so that every tensor fits
+// in shared memory up to Ndof = 24.  Two epilogues:
 //   GAUSS: the pair's contribution to Gamma(q0,s0) for every temperature, fused
 //          (W never leaves the SM).  The reference sums over every grid q1; the
 //          q2-side term of a pair equals its q1-side term exactly (swap s1<->s2),
-//          so each pair is weighted by 2 (1 when q1 == q2).
+//          so each pair is weighted by 2 (1 when q1 == q2).  exp() is skipped
+//          where it underflows to 0 (argument below -745.2), which leaves every
+//          sum bit-identical to evaluating it.
 //   WGRID: W for q1 and its s1<->s2 transpose for q2, i.e. the reference's
 //          Sctrq1(s2,s1,s0,q) for every grid q, for the tetrahedron integration.
-// Roofline: FP64 FMA pipe (about 110 kflop per pair for Ndof 6), plus FP64 exp
-// in the GAUSS epilogue (3 per mode triple).
+// Roofline: FP64 FMA pipe; inputs per pair are two eigenvector sets (2 Ndof^2
+// complex, L2-resident), outputs a few atomics (GAUSS) or 2 Ndof^3 doubles (WGRID).
 #include "spring_internal.cuh"
 
 namespace spring {
@@ -42,32 +47,41 @@ struct V3Args {
     int pol_lo[3], pol_hi[3];
 };
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+constexpr double EXP_UNDERFLOW = 745.2;  // exp(-x) == 0 in FP64 for x above this
+
+__device__ __forceinline__ void cfma(double2& acc, double2 a, double2 b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
 }
 
 template <int EPI>
 __global__ void __launch_bounds__(128) k_v3(V3Args a, const int2* __restrict__ pairs, const int* __restrict__ pair_q0,
-                                            const double* __restrict__ fc3t, const double* __restrict__ posr,
+                                            const double* __restrict__ fc3, const double* __restrict__ posr,
                                             const int* __restrict__ btyp, const double* __restrict__ mrs,
                                             const double* __restrict__ qpnt, const int* __restrict__ irr_int,
+                                            const int* __restrict__ q0_grid,
                                             const double2* __restrict__ ev0, const double* __restrict__ om0,
                                             const double* __restrict__ ob0, const double2* __restrict__ evg,
                                             const double* __restrict__ omg, const double* __restrict__ obg,
                                             const double* __restrict__ nbeg, double* __restrict__ out_lw,
                                             double* __restrict__ out_p3, double* __restrict__ out_w) {
-    extern __shared__ double smem_d[];
-    const int n = a.n, K = 3 * a.na, R = 9 * a.na;
+    extern __shared__ double2 smem2[];
+    const int n = a.n, na = a.na, nn = n * n;
     const int sb = a.sb;
-    double* sFC = smem_d;                                  // [K][R] (padded to an even count)
-    double2* sE1 = reinterpret_cast<double2*>(sFC + ((K * R + 1) & ~1));  // [K][n]
-    double2* sE2 = sE1 + K * n;                            // [K][n]
-    double2* sY = sE2 + K * n;                             // [R][n]
-    double2* sZ = sY + R * n;                              // [3][n][n]
-    double2* sPhi = sZ + 3 * n * n;                        // [sb][n][n]
-    double2* sP1 = sPhi + sb * n * n;                      // [na]
-    double2* sP2 = sP1 + a.na;                             // [na]
-    double* sLw = reinterpret_cast<double*>(sP2 + a.na);  // [nT][sb] + [sb]
+    double2* sE0 = smem2;              // [s][row]
+    double2* sE1 = sE0 + nn;
+    double2* sE2 = sE1 + nn;
+    double2* sD = sE2 + nn;            // [a][nu b][eta c]
+    double2* sT1 = sD + 3 * nn;        // [a][nu b][s2]
+    double2* sT2 = sT1 + 3 * nn;       // [a][s1][s2]
+    double2* sPhi = sT2 + 3 * nn;      // [s0 - s0b][s1][s2]
+    double2* sPP = sPhi + sb * nn;     // [N1][N2] phase products with masses
+    double2* sP = sPP + na * na;       // [2][na] phases of q1 and q2
+    double* sFC = reinterpret_cast<double*>(sP + 2 * na);  // [N1][N2][27]
+    double* sLw = sFC + ((na * na * 27 + 1) & ~1);         // [nT + 1][sb]
+    int* sBt = reinterpret_cast<int*>(sLw + (a.nT + 1) * sb + 1);  // [na]
 
     const int tid = threadIdx.x, nt = blockDim.x;
     const int work = blockIdx.x;
@@ -76,84 +90,88 @@ __global__ void __launch_bounds__(128) k_v3(V3Args a, const int2* __restrict__ p
     const int2 pq = pairs[pr];
     const int g1 = pq.x, g2 = pq.y;
     const int q0 = pair_q0[pr];
-    const double q1x = qpnt[3 * g1], q1y = qpnt[3 * g1 + 1], q1z = qpnt[3 * g1 + 2];
-    const double q2x = qpnt[3 * g2], q2y = qpnt[3 * g2 + 1], q2z = qpnt[3 * g2 + 2];
-    const double2* e0 = ev0 + (size_t)q0 * n * n;   // [s][row]
-    const double2* e1 = evg + (size_t)g1 * n * n;
-    const double2* e2 = evg + (size_t)g2 * n * n;
-    const int nphi = min(sb, n - s0b) * n * n;  // the last s0 block may be partial
+    const int p0 = q0_grid ? q0_grid[q0] : q0;  // row of the q0 phonons
+    const int nphi = min(sb, n - s0b) * nn;  // the last s0 block may be partial
 
+    for (int i = tid; i < nn; i += nt) {
+        sE0[i] = ev0[(size_t)p0 * nn + i];
+        sE1[i] = evg[(size_t)g1 * nn + i];
+        sE2[i] = evg[(size_t)g2 * nn + i];
+    }
     for (int i = tid; i < nphi; i += nt) sPhi[i] = make_double2(0.0, 0.0);
 
     for (int mu = 0; mu < a.nb; ++mu) {
-        // stage FC3 of mu and the neighbour phases
-        const double* f = fc3t + (size_t)mu * K * R;
-        for (int i = tid; i < K * R; i += nt) sFC[i] = f[i];
-        for (int i = tid; i < 2 * a.na; i += nt) {
-            const int N = i % a.na;
-            const double* Rv = posr + ((size_t)mu * a.na + N) * 3;
-            const double qr = i < a.na ? (q1x * Rv[0] + q1y * Rv[1] + q1z * Rv[2])
-                                       : (q2x * Rv[0] + q2y * Rv[1] + q2z * Rv[2]);
+        // (a) stage FC3 of mu, basis of each neighbour slot, and the neighbour phases
+        const double* f = fc3 + (size_t)mu * na * na * 27;
+        for (int i = tid; i < na * na * 27; i += nt) sFC[i] = f[i];
+        for (int i = tid; i < na; i += nt) sBt[i] = btyp[mu * na + i];
+        for (int i = tid; i < 2 * na; i += nt) {
+            const int N = i % na;
+            const int g = i < na ? g1 : g2;
+            const double* Rv = posr + ((size_t)mu * na + N) * 3;
+            const double qr = qpnt[3 * g] * Rv[0] + qpnt[3 * g + 1] * Rv[1] + qpnt[3 * g + 2] * Rv[2];
             double sn, cs;
             sincos(qr, &sn, &cs);
-            (i < a.na ? sP1 : sP2)[N] = make_double2(cs, sn);
+            sP[i] = make_double2(cs, sn);
         }
         __syncthreads();
-        // E1, E2: [k = N*3 + b][s]
-        for (int i = tid; i < 2 * K * n; i += nt) {
-            const int which = i / (K * n), j = i % (K * n);
-            const int k = j / n, s = j % n;
-            const int N = k / 3, b = k % 3;
-            const int nu = btyp[mu * a.na + N];
-            const double2 ph = (which ? sP2 : sP1)[N];
-            const double2 ev = (which ? e2 : e1)[s * n + 3 * nu + b];
-            const double m = mrs[nu];
-            (which ? sE2 : sE1)[j] = make_double2(m * (ph.x * ev.x - ph.y * ev.y), m * (ph.x * ev.y + ph.y * ev.x));
+        // (b) phase products with the neighbour masses
+        for (int i = tid; i < na * na; i += nt) {
+            const int N1 = i / na, N2 = i % na;
+            const double2 p1 = sP[N1], p2 = sP[na + N2];
+            const double m = mrs[sBt[N1]] * mrs[sBt[N2]];
+            sPP[i] = make_double2(m * (p1.x * p2.x - p1.y * p2.y), m * (p1.x * p2.y + p1.y * p2.x));
         }
         __syncthreads();
-        // Y[r][s2] = sum_k FC[k][r] E2[k][s2]
-        for (int o = tid; o < R * n; o += nt) {
-            const int r = o / n, s2 = o % n;
-            double yr = 0.0, yi = 0.0;
-            for (int k = 0; k < K; ++k) {
-                const double fv = sFC[k * R + r];
-                const double2 e = sE2[k * n + s2];
-                yr = fma(fv, e.x, yr);
-                yi = fma(fv, e.y, yi);
-            }
-            sY[o] = make_double2(yr, yi);
-        }
-        __syncthreads();
-        // Z[al][s1][s2] = sum_{N1, b} E1[N1*3+b][s1] Y[(N1*3+al)*3+b][s2]
-        for (int o = tid; o < 3 * n * n; o += nt) {
-            const int al = o / (n * n), s1 = (o / n) % n, s2 = o % n;
-            double zr = 0.0, zi = 0.0;
-            for (int N1 = 0; N1 < a.na; ++N1)
-                for (int b = 0; b < 3; ++b) {
-                    const double2 x = sE1[(N1 * 3 + b) * n + s1];
-                    const double2 y = sY[((N1 * 3 + al) * 3 + b) * n + s2];
-                    zr = fma(x.x, y.x, zr);
-                    zr = fma(-x.y, y.y, zr);
-                    zi = fma(x.x, y.y, zi);
-                    zi = fma(x.y, y.x, zi);
+        // (c) D[a][nu b][eta c] = sum over slots of basis nu / eta of FC * phase
+        for (int o = tid; o < 3 * nn; o += nt) {
+            const int al = o / nn, r = (o / n) % n, cidx = o % n;
+            const int nu = r / 3, be = r % 3, eta = cidx / 3, ga = cidx % 3;
+            const int abc = (al * 3 + be) * 3 + ga;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int N1 = 0; N1 < na; ++N1) {
+                if (sBt[N1] != nu) continue;
+                for (int N2 = 0; N2 < na; ++N2) {
+                    if (sBt[N2] != eta) continue;
+                    const double fv = sFC[(N1 * na + N2) * 27 + abc];
+                    const double2 pp = sPP[N1 * na + N2];
+                    acc.x = fma(fv, pp.x, acc.x);
+                    acc.y = fma(fv, pp.y, acc.y);
                 }
-            sZ[o] = make_double2(zr, zi);
+            }
+            sD[o] = acc;
         }
         __syncthreads();
-        // Phi[s0][s1][s2] += sum_al m_mu^-1/2 e0(3 mu + al, s0) Z[al][s1][s2]
+        // (d) T1[a][r][s2] = sum_c D[a][r][c] e2(c, s2)
+        for (int o = tid; o < 3 * nn; o += nt) {
+            const int ar = o / n, s2 = o % n;
+            const double2* drow = sD + ar * n;
+            const double2* e2 = sE2 + s2 * n;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k]);
+            sT1[o] = acc;
+        }
+        __syncthreads();
+        // (e) T2[a][s1][s2] = sum_r e1(r, s1) T1[a][r][s2]
+        for (int o = tid; o < 3 * nn; o += nt) {
+            const int al = o / nn, s1 = (o / n) % n, s2 = o % n;
+            const double2* e1 = sE1 + s1 * n;
+            const double2* t1 = sT1 + al * nn + s2;
+            double2 acc = make_double2(0.0, 0.0);
+            for (int k = 0; k < n; ++k) cfma(acc, e1[k], t1[k * n]);
+            sT2[o] = acc;
+        }
+        __syncthreads();
+        // (f) Phi[s0][s1][s2] += sum_a m_mu^-1/2 e0(mu a, s0) T2[a][s1][s2]
         const double mm = mrs[mu];
         for (int o = tid; o < nphi; o += nt) {
-            const int s0 = s0b + o / (n * n), r12 = o % (n * n);
+            const int s0 = s0b + o / nn, r12 = o % nn;
             double2 acc = sPhi[o];
             for (int al = 0; al < 3; ++al) {
-                double2 w = e0[s0 * n + 3 * mu + al];
+                double2 w = sE0[s0 * n + 3 * mu + al];
                 w.x *= mm;
                 w.y *= mm;
-                const double2 z = sZ[al * n * n + r12];
-                acc.x = fma(w.x, z.x, acc.x);
-                acc.x = fma(-w.y, z.y, acc.x);
-                acc.y = fma(w.x, z.y, acc.y);
-                acc.y = fma(w.y, z.x, acc.y);
+                cfma(acc, w, sT2[al * nn + r12]);
             }
             sPhi[o] = acc;
         }
@@ -168,37 +186,42 @@ __global__ void __launch_bounds__(128) k_v3(V3Args a, const int2* __restrict__ p
         __syncthreads();
     }
     for (int o = tid; o < nphi; o += nt) {
-        const int s0 = s0b + o / (n * n), s1 = (o / n) % n, s2 = o % n;
+        const int s0 = s0b + o / nn, s1 = (o / n) % n, s2 = o % n;
         double W = 0.0;
         if (!((gq0 && s0 < 3) || (gq1 && s1 < 3) || (gq2 && s2 < 3))) {
             const double2 p = sPhi[o];
             const double abs2 = p.x * p.x + p.y * p.y;
-            W = abs2 * (ob0[(size_t)q0 * n + s0] * obg[(size_t)g1 * n + s1] * obg[(size_t)g2 * n + s2]) * a.mfac;
+            W = abs2 * (ob0[(size_t)p0 * n + s0] * obg[(size_t)g1 * n + s1] * obg[(size_t)g2 * n + s2]) * a.mfac;
         }
         if (EPI == 1) {
             const int slot = q0 - a.q0_first;
-            const size_t n3 = (size_t)n * n * n;
+            const size_t n3 = (size_t)n * nn;
             out_w[((size_t)slot * a.nq + g1) * n3 + (s0 * n + s1) * n + s2] = W;
             if (g1 != g2) out_w[((size_t)slot * a.nq + g2) * n3 + (s0 * n + s2) * n + s1] = W;
         } else {
             if (s0 < a.pol_lo[0] || s0 > a.pol_hi[0] || s1 < a.pol_lo[1] || s1 > a.pol_hi[1] || s2 < a.pol_lo[2] ||
                 s2 > a.pol_hi[2] || (gq1 && s1 < 3) || (gq2 && s2 < 3))
                 continue;
-            const double w0 = om0[(size_t)q0 * n + s0];
+            const double w0 = om0[(size_t)p0 * n + s0];
             const double w1 = omg[(size_t)g1 * n + s1];
             const double w2 = omg[(size_t)g2 * n + s2];
             const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
             const double pre = a.onebysigma * ONEBYSQRT2PI;
-            const double e1v = pre * exp(-0.5 * a.onebysigma2 * (d1 * d1));
-            const double e2v = pre * exp(-0.5 * a.onebysigma2 * (d2 * d2));
-            const double e3v = pre * exp(-0.5 * a.onebysigma2 * (d3 * d3));
+            const double x1 = 0.5 * a.onebysigma2 * (d1 * d1);
+            const double x2 = 0.5 * a.onebysigma2 * (d2 * d2);
+            const double x3 = 0.5 * a.onebysigma2 * (d3 * d3);
+            const double e1v = x1 < EXP_UNDERFLOW ? pre * exp(-x1) : 0.0;
+            const double e2v = x2 < EXP_UNDERFLOW ? pre * exp(-x2) : 0.0;
+            const double e3v = x3 < EXP_UNDERFLOW ? pre * exp(-x3) : 0.0;
+            const double esum = e1v + e2v + e3v;
+            if (esum == 0.0) continue;
             for (int t = 0; t < a.nT; ++t) {
                 const double n1 = nbeg[((size_t)t * a.nq + g1) * n + s1];
                 const double n2 = nbeg[((size_t)t * a.nq + g2) * n + s2];
                 const double v = W * (((n1 + n2 + 1.0) * e1v) + ((n1 - n2) * (e2v - e3v)));
                 atomicAdd(&sLw[t * sb + (s0 - s0b)], v);
             }
-            atomicAdd(&sLw[a.nT * sb + (s0 - s0b)], e1v + e2v + e3v);
+            atomicAdd(&sLw[a.nT * sb + (s0 - s0b)], esum);
         }
     }
     if (EPI == 0) {
@@ -206,7 +229,7 @@ __global__ void __launch_bounds__(128) k_v3(V3Args a, const int2* __restrict__ p
         const double mult = g1 != g2 ? 2.0 : 1.0;
         for (int i = tid; i < (a.nT + 1) * sb; i += nt) {
             const int t = i / sb, s0 = s0b + i % sb;
-            if (s0 >= n) continue;
+            if (s0 >= n || sLw[i] == 0.0) continue;
             if (t < a.nT)
                 atomicAdd(&out_lw[((size_t)t * a.nq0 + q0) * n + s0], mult * sLw[i]);
             else
@@ -216,9 +239,9 @@ __global__ void __launch_bounds__(128) k_v3(V3Args a, const int2* __restrict__ p
 }
 
 size_t v3_smem(int n, int na, int sb, int nT) {
-    const int K = 3 * na, R = 9 * na;
-    return sizeof(double) * ((K * R + 1) & ~1) + sizeof(double2) * (2 * K * n + R * n + 3 * n * n + sb * n * n + 2 * na) +
-           sizeof(double) * (nT + 1) * sb;
+    const int nn = n * n;
+    return sizeof(double2) * (3 * nn + 9 * nn + sb * nn + na * na + 2 * na) +
+           sizeof(double) * (((na * na * 27 + 1) & ~1) + (nT + 1) * sb + 1) + sizeof(int) * na + 16;
 }
 
 int v3_block(int n) {
@@ -227,18 +250,19 @@ int v3_block(int n) {
 }
 
 template <int EPI>
-int launch_v3(spring_ctx* c, int q0_first, int n_q0, V3Args a, double* lw, double* p3, double* w) {
+int launch_v3(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, V3Args a, double* lw,
+              double* p3, double* w) {
     a.nb = c->nb;
     a.n = c->ndof;
     a.na = c->na3;
     a.nq = c->nq;
-    a.nq0 = c->nq0;
+    a.nq0 = ps.n0;
     a.nT = c->nT;
     a.q0_first = q0_first;
     a.sb = v3_block(c->ndof);
     a.nsb = (c->ndof + a.sb - 1) / a.sb;
     a.mfac = host_constants().Sctr3THz2 / double(c->nq);
-    const int p0 = c->h_pairoff[q0_first], p1 = c->h_pairoff[q0_first + n_q0];
+    const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
     a.pair_first = p0;
     const size_t smem = v3_smem(a.n, a.na, a.sb, a.nT);
     if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "V3 tile needs %zu bytes of shared memory", smem);
@@ -248,15 +272,24 @@ int launch_v3(spring_ctx* c, int q0_first, int n_q0, V3Args a, double* lw, doubl
     if (items > 0x7fffffffLL) return fail(c, SPRING_ERR_UNSUPPORTED, "too many V3 work items");
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3: injected launch failure");
     k_v3<EPI><<<(unsigned)items, 128, smem, c->stream>>>(
-        a, c->d_pairs.p, c->d_pair_q0.p, c->d_fc3t.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p,
-        c->d_irr_int.p, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->ph_grid.evec.p, c->ph_grid.omega.p,
-        c->ph_grid.oneby.p, c->ph_grid.nbe.p, lw, p3, w);
+        a, ps.pairs.p, ps.pair_q0.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p,
+        v.q0_int, v.q0_grid, v.evec, v.omega, v.oneby, c->ph_grid.evec.p, c->ph_grid.omega.p, c->ph_grid.oneby.p,
+        c->ph_grid.nbe.p, lw, p3, w);
     return launch_check(c, EPI == 0 ? "k_v3<gauss>" : "k_v3<wgrid>");
 }
 
 }  // namespace
 
+Q0View irr_view(spring_ctx* c) {
+    return Q0View{c->d_irr_int.p, nullptr, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p};
+}
+
 int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3) {
+    bool handled = false;
+    if (!c->force_generic_v3)
+        SPRING_CHECK(launch_v3s(c, c->ps_irr, irr_view(c), q0_first, n_q0, 0, sigma, &pol, d_lw, d_p3, nullptr,
+                                &handled));
+    if (handled) return SPRING_OK;
     V3Args a{};
     a.onebysigma = 1.0 / sigma;
     a.onebysigma2 = a.onebysigma * a.onebysigma;
@@ -264,12 +297,16 @@ int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol&
         a.pol_lo[k] = pol.lo[k];
         a.pol_hi[k] = pol.hi[k];
     }
-    return launch_v3<0>(c, q0_first, n_q0, a, d_lw, d_p3, nullptr);
+    return launch_v3<0>(c, c->ps_irr, irr_view(c), q0_first, n_q0, a, d_lw, d_p3, nullptr);
 }
 
-int run_v3_wgrid(spring_ctx* c, int q0_first, int n_q0, double* d_w) {
+int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, double* d_w) {
+    bool handled = false;
+    if (!c->force_generic_v3)
+        SPRING_CHECK(launch_v3s(c, ps, v, q0_first, n_q0, 1, 0.0, nullptr, nullptr, nullptr, d_w, &handled));
+    if (handled) return SPRING_OK;
     V3Args a{};
-    return launch_v3<1>(c, q0_first, n_q0, a, nullptr, nullptr, d_w);
+    return launch_v3<1>(c, ps, v, q0_first, n_q0, a, nullptr, nullptr, d_w);
 }
 
 }  // namespace spring

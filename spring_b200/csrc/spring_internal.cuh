@@ -32,6 +32,30 @@ struct DBuf {
     size_t n = 0;
 };
 
+// Momentum-conserving pairs of every q0 of one set of q0 points (the point-group
+// irreducible set of kappa.x, or the time-reversal set of kappa_iter.x).
+struct PairSet {
+    int n0 = 0;
+    const int* q0_int = nullptr;  // [n0][3] device, not owned
+    const int* q0_grid = nullptr; // [n0] grid index of each q0 (device) or null
+    DBuf<int> partner;            // [q0][q1] partner grid index (0-based)
+    DBuf<int> pairoff;            // [n0 + 1]
+    DBuf<int2> pairs;             // (g1, g2) 0-based, grouped by q0
+    DBuf<int> pair_q0;            // q0 of each pair
+    DBuf<int> pairpos;            // [q0][q1] exclusive-scan position of each representative
+    std::vector<int> h_pairoff;
+    bool done = false;
+};
+
+// The q0 side of the V3 kernel: integer q0 vectors and the phonons of each q0.
+struct Q0View {
+    const int* q0_int;      // [n0][3]
+    const int* q0_grid;     // null: phonons indexed by q0; else by q0_grid[q0]
+    const double2* evec;
+    const double* omega;
+    const double* oneby;
+};
+
 struct Phonons {
     int n = 0;                       // number of q points
     DBuf<double2> evec;              // [q][s][row]  (Fortran Evec(row,s,q))
@@ -54,6 +78,16 @@ struct spring_ctx {
     std::string err;
     long long launches = 0;
     int precision = SPRING_FP64;
+    bool force_generic_v3 = false;  // spring_set_option(SPRING_OPT_GENERIC_V3): use the any-cell V3 kernel
+
+    // per-launch CUDA-event records (spring_set_profiling)
+    struct ProfRec {
+        std::string name;
+        cudaEvent_t start, stop;
+    };
+    bool profiling = false;
+    std::vector<ProfRec> prof;
+    cudaEvent_t prof_pending = nullptr;
 
     // fault injection
     int inject_kind = -1;
@@ -72,12 +106,13 @@ struct spring_ctx {
     spring::DBuf<int> d_fc2_idx;     // [mu][N][4]
     spring::DBuf<int> d_fc2_num;
 
-    // FC3: kernel layout [mu][N2*3+gamma][(N1*3+alpha)*3+beta]  (zero padded to na3)
+    // FC3: [mu][N1][N2][alpha][beta][gamma] (Fortran memory order), zero beyond atm_num
     bool fc3_set = false;
     int na3 = 0;
-    spring::DBuf<double> d_fc3t;
+    spring::DBuf<double> d_fc3;
     spring::DBuf<double> d_fc3_posr;  // [mu][N][3]  Cartesian cell vector
     spring::DBuf<int> d_fc3_btyp;     // [mu][N] 0-based basis index
+    spring::DBuf<int> d_fc3_off;      // [mu][nb+1] first slot of each basis atom (slots grouped by basis)
 
     // mesh
     bool mesh_set = false;
@@ -96,14 +131,17 @@ struct spring_ctx {
     spring::DBuf<double> d_temps;
     spring::Phonons ph_grid, ph_irr;
 
-    // 3-phonon enumeration, all irreducible points
-    bool enum3_done = false;
-    spring::DBuf<int> d_partner;   // [q0][q1] partner grid index (0-based)
-    spring::DBuf<int> d_pairoff;   // [nq0+1]
-    spring::DBuf<int2> d_pairs;    // (g1, g2) 0-based
-    spring::DBuf<int> d_pair_q0;   // q0 of each pair
-    spring::DBuf<int> d_pairpos;   // [q0][q1] exclusive-scan position of each representative
-    std::vector<int> h_pairoff;
+    // 3-phonon pairs of the irreducible set and of the time-reversal set
+    spring::PairSet ps_irr, ps_tr;
+    // time-reversal set (kappa_iter.x): representatives, their F slots and signs
+    int ntr = 0;
+    spring::DBuf<int> d_tr_int;    // [ntr][3]
+    spring::DBuf<int> d_tr_grid;   // [ntr] grid index
+    spring::DBuf<int> d_tr_pos;    // [q] slot of each grid point
+    spring::DBuf<int> d_tr_sgn;    // [q] +1 representative, -1 its inverse
+    spring::DBuf<int> d_tr_deg;    // [ntr]
+    spring::DBuf<int> d_neg;       // [q] grid index of -q
+    spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
 
     // scratch
     spring::DBuf<int> d_scan_tmp;
@@ -140,10 +178,18 @@ void dfree(DBuf<T>& b) {
     b.p = nullptr;
     b.n = 0;
 }
+inline void free_pairs(PairSet& s) {
+    dfree(s.partner); dfree(s.pairoff); dfree(s.pairs); dfree(s.pair_q0); dfree(s.pairpos);
+    s.h_pairoff.clear();
+    s.done = false;
+}
 int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what);
-int launch_check(spring_ctx* c, const char* what);  // counts launches, checks cudaGetLastError
+// Every kernel launch site calls launch_injected() first (fault injection and,
+// when profiling, the start event) and launch_check() right after the launch
+// (error check, launch count, stop event named after the kernel).
+int launch_check(spring_ctx* c, const char* what);
 bool launch_injected(spring_ctx* c);
 
 // ---- kernels (host launchers), each defined in its own .cu -------------------
@@ -153,13 +199,19 @@ int run_irr_map(spring_ctx* c, const int* d_rot, int nrot, int time_rev, int* d_
 // k_phonon.cu
 int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int n);
 // k_enum.cu
-int run_enumerate3(spring_ctx* c);
+int run_enumerate3(spring_ctx* c, PairSet& ps);
 int run_enumerate3_fortran(spring_ctx* c, int i0, int* d_allq1q2, int* d_perm, int* d_counts);
 int run_exclusive_scan(spring_ctx* c, const int* d_in, int* d_out, int n);
 // k_v3.cu
 struct Pol { int lo[3], hi[3]; };
+Q0View irr_view(spring_ctx* c);
 int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3);
-int run_v3_wgrid(spring_ctx* c, int q0_first, int n_q0, double* d_w);
+int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, double* d_w);
+// k_v3s.cu: specialised V3 for two-atom cells; *handled is false when the cell does not fit it
+int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
+               const Pol* pol, double* lw, double* p3, double* w, bool* handled);
+// k_bte.cu
+int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters);
 // k_tetra.cu
 int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const Pol& pol, double* d_lw, double* d_p3);
 int run_iso(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const double* g2, double* d_rate);
