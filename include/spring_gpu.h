@@ -163,6 +163,14 @@ int spring_set_linewidths(spring_ctx* ctx, const double* lw_all);
 int spring_kappa_rta(spring_ctx* ctx, int symm, int nsym, const double* Rxyz, const int* s_range, double* kappa,
                      double* mode_k);
 
+/* Iterative (non-RTA) kappa of kappa_iter.x (src/Kappa/Src_iterative/main.f90:219-361):
+ * time-reversal irreducible set, tetrahedron 1/tau and F0 (CreateFzero), then
+ * F <- F0 + tau * sum(...) until max|kappa_new - kappa_old| < eps_k or more than
+ * max_iter iterations (MAX_ITER = 1000 in the reference), for every temperature.
+ * Uses the grid phonons and FC3.  kappa(9,n_temps), kappa_rta(9,n_temps) (iteration
+ * 0) and iters(n_temps) are outputs (NULL allowed). */
+int spring_kappa_iter(spring_ctx* ctx, double eps_k, int max_iter, double* kappa, double* kappa_rta, int* iters);
+
 /* ---- options ----------------------------------------------------------- */
 /* SPRING_OPT_GENERIC_V3 = 1: always use the any-cell V3 kernel (default 0 picks the
  * two-atom specialisation when the cell fits it; both give the same W). */

@@ -50,6 +50,7 @@ SIGNATURES = {
     "spring_prepare3": [P],
     "spring_set_profiling": [P, I],
     "spring_set_option": [P, I, I],
+    "spring_kappa_iter": [P, D, I, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_scatter_w3": [P, I, P],
     "spring_linewidth3": [P, I, I, I, D, P, P, P],

@@ -239,6 +239,16 @@ class Context:
         return (kap, mk) if mode else kap
 
 
+    # -- kappa_iter.x
+    def kappa_iter(self, eps_k: float = 1e-6, max_iter: int = 1000):
+        """Iterative kappa per temperature: dict(kappa (nT,9), kappa_rta (nT,9), iters (nT,))."""
+        kap = np.zeros((self.n_temps, 9))
+        k0 = np.zeros((self.n_temps, 9))
+        it = np.zeros(self.n_temps, np.int32)
+        self._call("spring_kappa_iter", float(eps_k), int(max_iter), _ptr(kap), _ptr(k0), _ptr(it))
+        return dict(kappa=kap, kappa_rta=k0, iters=it)
+
+
 def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True):
     """A ready context for a :class:`spring_b200.synthetic.Crystal`.
 

@@ -279,6 +279,15 @@ int spring_kernel_launches(const spring_ctx* c, long long* count) {
     return SPRING_OK;
 }
 
+int spring_kappa_iter(spring_ctx* c, double eps_k, int max_iter, double* kappa, double* kappa_rta, int* iters) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->fc3_set, "FC3"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    if (!(eps_k > 0.0) || max_iter < 0) return fail(c, SPRING_ERR_ARG, "eps_k must be > 0 and max_iter >= 0");
+    return run_bte(c, eps_k, max_iter, kappa, kappa_rta, iters);
+}
+
 int spring_set_option(spring_ctx* c, int option, int value) {
     CTX_ENTER(c);
     switch (option) {
@@ -439,6 +448,7 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc3_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC3 basis"));
     SPRING_CHECK(spring_synchronize(c));
     c->fc3_set = true;
+    dfree(c->d_wtr);  // cached W grids depend on FC3
     return SPRING_OK;
 }
 
@@ -548,6 +558,7 @@ int spring_compute_phonons(spring_ctx* c, const double* temps, double freq_cut) 
     SPRING_CHECK(run_phonons(c, c->ph_grid, c->d_qpnt.p, c->nq));
     SPRING_CHECK(run_phonons(c, c->ph_irr, c->d_irr_q.p, c->nq0));
     c->ph_grid.set = c->ph_irr.set = true;
+    dfree(c->d_wtr);  // cached W grids depend on the phonons
     return SPRING_OK;
 }
 
@@ -569,6 +580,7 @@ int spring_set_phonons(spring_ctx* c, int which, const double* temps, const doub
     SPRING_CHECK(h2d(c, p.vel.p, vel, sizeof(double) * n * nd * 3, "group velocity"));
     SPRING_CHECK(spring_synchronize(c));
     p.set = true;
+    if (which == 0) dfree(c->d_wtr);  // cached W grids depend on the grid phonons
     return SPRING_OK;
 }
 

@@ -1,0 +1,435 @@
+// Iterative (non-RTA) Boltzmann transport of kappa_iter.x on the device.
+//
+// Reference (src/Kappa/Src_iterative): the time-reversal irreducible set
+// (Irr_q_point_m.f90:216-335), W+ = W (n1 - n2) and W- = W (1 + n1 + n2) per
+// pair (Quasi_momentum_consrv.f90:567-621, Sctr3THz2 with pi/4), 1/tau from the
+// tetrahedron sums TetrahedronWplus / TetrahedronWminus (:701-1208, strict case
+// bounds, a vertex set counts only when |sum I - 1| < 5e-5), CreateFzero,
+// TetrahedronIterPlus / Minus (TetrahedronDeltaSum.f90:22-607), multiplyTaudFnew,
+// kappa (HelperSubroutines.f90:118-347) and the loop of main.f90:295-361.
+//
+// Representatives of the time-reversal pairs {q, -q} are the smaller grid
+// index (the reference takes the first one met while building tetrahedra);
+// F(-q) = -F(q).  The W of a vertex comes from kappa.x's W grid of the same q0,
+// which stores both orientations of every pair; 4 W there is kappa_iter's W.
+//   plus  channel, vertex x:  partner -p(x),  M = w(-p(x),s2) - w(x,s1),
+//                             W+ = 4 W3(q0; x s1; p(x) s2) (n(x,s1) - n(p(x),s2)),
+//                             dF term (F(-p(x),s2) - F(x,s1));
+//   minus channel, vertex v:  partner u = -p(-v), M = w(v,s1) + w(u,s2),
+//                             W- = 4 W3(q0; -v s1; p(-v) s2) (1 + n(-v,s1) + n(p(-v),s2)),
+//                             dF term 0.5 (F(u,s2) + F(v,s1));
+// with p(x) = grid(-q0 - x).  One thread per (q0, tetrahedron, s1, s2) sorts each
+// channel's vertex energies once (stable) and loops over s0.  The W grids of
+// every q0 are computed once and kept in HBM when they fit a 40 GB budget, and
+// otherwise recomputed batch by batch on every pass.
+// Roofline: FP64 ALU (divisions of the tetrahedron weights), like k_tetra3.
+#include <algorithm>
+#include <cmath>
+
+#include "spring_internal.cuh"
+
+namespace spring {
+namespace {
+
+constexpr int NS0 = 6;
+constexpr double ZERO_PREC = 5.0e-5;
+constexpr double FUNIT_E = 1.054571817 / 1.380649;  // FunitE_11m_K (Src_iterative/constants.f90:56)
+constexpr double KW_MK = 1.054571817 * 0.001;       // kW_mK (:58)
+
+__device__ __forceinline__ void sort4(const double* M, int* p) {
+    p[0] = 0; p[1] = 1; p[2] = 2; p[3] = 3;
+#define SWP(i, j)                                                                           \
+    {                                                                                       \
+        const double a_ = M[p[i]], b_ = M[p[j]];                                            \
+        if (b_ < a_ || (b_ == a_ && p[j] < p[i])) { int t_ = p[i]; p[i] = p[j]; p[j] = t_; } \
+    }
+    SWP(0, 1) SWP(2, 3) SWP(0, 2) SWP(1, 3) SWP(1, 2)
+#undef SWP
+}
+
+// FindgAndIver with the strict bounds of kappa_iter (Quasi_momentum_consrv.f90:811-867).
+__device__ __forceinline__ bool g_iver_strict(double Mqs, const double* M, double& g, double* I) {
+    if ((Mqs > M[0]) && (Mqs < M[1])) {
+        g = (3.0 * ((Mqs - M[0]) * (Mqs - M[0]))) / ((M[1] - M[0]) * (M[2] - M[0]) * (M[3] - M[0]));
+        I[0] = (((Mqs - M[1]) / (M[0] - M[1])) + ((Mqs - M[2]) / (M[0] - M[2])) + ((Mqs - M[3]) / (M[0] - M[3]))) / 3.0;
+        for (int v = 1; v < 4; ++v) I[v] = ((Mqs - M[0]) / (M[v] - M[0])) / 3.0;
+        return true;
+    }
+    if ((Mqs > M[1]) && (Mqs < M[2])) {
+        g = (3.0 / ((M[1] - M[2]) * (M[3] - M[0]))) *
+            ((((Mqs - M[0]) * (Mqs - M[2])) / (M[2] - M[0])) - (((Mqs - M[1]) * (Mqs - M[3])) / (M[1] - M[3])));
+        const double den = g * (M[3] - M[0]);
+        I[0] = (((Mqs - M[3]) / (M[0] - M[3])) / 3.0) +
+               ((((Mqs - M[2]) / (M[0] - M[2])) * ((Mqs - M[0]) / (M[2] - M[0])) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
+        const double t1 = (Mqs - M[3]) / (M[1] - M[3]);
+        I[1] = (((Mqs - M[2]) / (M[1] - M[2])) / 3.0) + (((t1 * t1) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
+        const double t2 = (Mqs - M[0]) / (M[2] - M[0]);
+        I[2] = (((Mqs - M[1]) / (M[2] - M[1])) / 3.0) + (((t2 * t2) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
+        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) / 3.0) +
+               ((((Mqs - M[1]) / (M[3] - M[1])) * ((Mqs - M[3]) / (M[1] - M[3])) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
+        return true;
+    }
+    if ((Mqs > M[2]) && (Mqs < M[3])) {
+        g = (3.0 * ((Mqs - M[3]) * (Mqs - M[3]))) / ((M[3] - M[0]) * (M[3] - M[1]) * (M[3] - M[2]));
+        for (int v = 0; v < 3; ++v) I[v] = ((Mqs - M[3]) / (M[v] - M[3])) / 3.0;
+        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) + ((Mqs - M[1]) / (M[3] - M[1])) + ((Mqs - M[2]) / (M[3] - M[2]))) / 3.0;
+        return true;
+    }
+    g = 0.0;
+    return false;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+struct PassArgs {
+    int n, nq, ntet, q0_first, s0a, s0n;
+    const int* tr_grid;   // [ntr]
+    const int* tr_pos;    // [nq]
+    const int* tr_sgn;    // [nq]
+    const int* neg;       // [nq]
+    const int* partner;   // [ntr][nq]
+    const double* wgrid;  // [slot][nq][n^3] for q0_first ..
+    const double* omega;  // [nq][n]
+    const double* nbe;    // [nq][n] at this temperature
+    const double* F;      // [ntr][n][3] (MODE 1)
+    double* out;          // MODE 0: inv_tau [ntr][n]; MODE 1: dF [ntr][n][3]
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_bte_pass(PassArgs a, const int4* __restrict__ tet) {
+    constexpr int NC = MODE == 0 ? 1 : 3;
+    __shared__ double sacc[NS0 * 3];
+    const int slot = blockIdx.y;
+    const int q0 = a.q0_first + slot;
+    const int n = a.n;
+    const size_t n3 = (size_t)n * n * n;
+    const int g0 = a.tr_grid[q0];
+    const int* p = a.partner + (size_t)q0 * a.nq;
+    const double* W3 = a.wgrid + (size_t)slot * a.nq * n3;
+    for (int i = threadIdx.x; i < NS0 * 3; i += blockDim.x) sacc[i] = 0.0;
+    __syncthreads();
+    double acc[NS0][NC];
+#pragma unroll
+    for (int s = 0; s < NS0; ++s)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) acc[s][k] = 0.0;
+
+    const long long items = (long long)a.ntet * n * n;
+    for (long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x; it < items;
+         it += (long long)gridDim.x * blockDim.x) {
+        const int s2 = (int)(it % n), s1 = (int)((it / n) % n), t = (int)(it / ((long long)n * n));
+        const int4 tv = tet[t];
+        const int x[4] = {tv.x, tv.y, tv.z, tv.w};
+#pragma unroll
+        for (int ch = 0; ch < 2; ++ch) {
+            int part[4], wrow[4];
+            double M[4], Wf[4];  // Wf: the occupation factor; W3 is read per s0
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                if (ch == 0) {
+                    const int px = p[x[v]];
+                    part[v] = a.neg[px];
+                    wrow[v] = x[v];
+                    M[v] = a.omega[(size_t)part[v] * n + s2] - a.omega[(size_t)x[v] * n + s1];
+                    Wf[v] = a.nbe[(size_t)x[v] * n + s1] - a.nbe[(size_t)px * n + s2];
+                } else {
+                    const int y = a.neg[x[v]];
+                    const int py = p[y];
+                    part[v] = a.neg[py];
+                    wrow[v] = y;
+                    M[v] = a.omega[(size_t)x[v] * n + s1] + a.omega[(size_t)part[v] * n + s2];
+                    Wf[v] = 1.0 + a.nbe[(size_t)y * n + s1] + a.nbe[(size_t)py * n + s2];
+                }
+            }
+            int pm[4];
+            sort4(M, pm);
+            double S[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) S[v] = M[pm[v]];
+            // F terms per vertex (MODE 1): plus F(part,s2) - F(x,s1); minus F(part,s2) + F(x,s1)
+            double Fc[4][NC];
+            if (MODE == 1) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int xv = x[pm[v]], pv = part[pm[v]];
+                    const double sx = a.tr_sgn[xv], sp = a.tr_sgn[pv];
+                    const double* f1 = a.F + ((size_t)a.tr_pos[xv] * n + s1) * 3;
+                    const double* f2 = a.F + ((size_t)a.tr_pos[pv] * n + s2) * 3;
+#pragma unroll
+                    for (int k = 0; k < NC; ++k)
+                        Fc[v][k] = ch == 0 ? (sp * f2[k] - sx * f1[k]) : (sp * f2[k] + sx * f1[k]);
+                }
+            }
+#pragma unroll
+            for (int si = 0; si < NS0; ++si) {
+                if (si >= a.s0n) break;
+                const int s0 = a.s0a + si;
+                const double Mqs = a.omega[(size_t)g0 * n + s0];
+                double g, I[4];
+                if (!g_iver_strict(Mqs, S, g, I)) continue;
+                if (!(fabs(I[0] + I[1] + I[2] + I[3] - 1.0) < ZERO_PREC)) continue;
+                const double pre = ch == 0 ? ONEBYSIX * g : 0.5 * ONEBYSIX * g;
+                double tv[NC];
+#pragma unroll
+                for (int k = 0; k < NC; ++k) tv[k] = 0.0;
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    const int q = pm[v];
+                    const double Wv = 4.0 * W3[(size_t)wrow[q] * n3 + (s0 * n + s1) * n + s2] * Wf[q];
+                    if (MODE == 0) {
+                        tv[0] += I[v] * Wv;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < NC; ++k) tv[k] += (I[v] * Wv) * Fc[v][k];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < NC; ++k) acc[si][k] += pre * tv[k];
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < NS0; ++s)
+#pragma unroll
+        for (int k = 0; k < NC; ++k) {
+            const double v = warp_sum(acc[s][k]);
+            if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&sacc[s * 3 + k], v);
+        }
+    __syncthreads();
+    for (int i = threadIdx.x; i < NS0 * NC; i += blockDim.x) {
+        const int s = i / NC, k = i % NC;
+        if (s >= a.s0n || sacc[s * 3 + k] == 0.0) continue;
+        const int s0 = a.s0a + s;
+        if (MODE == 0) atomicAdd(&a.out[(size_t)q0 * n + s0], sacc[s * 3]);
+        else atomicAdd(&a.out[((size_t)q0 * n + s0) * 3 + k], sacc[s * 3 + k]);
+    }
+}
+
+// F0 = FunitE w v / (1/tau T^2) where |1/tau| > zero_prec (CreateFzero).
+__global__ void k_bte_f0(int ntr, int n, const int* tr_grid, const double* omega, const double* vel,
+                         const double* inv_tau, double T, double* F0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntr * n; i += gridDim.x * blockDim.x) {
+        const int q = i / n, s = i % n, g0 = tr_grid[q];
+        const double it = inv_tau[i];
+        for (int k = 0; k < 3; ++k) {
+            double f = 0.0;
+            if (!(g0 == 0 && s < 3) && fabs(it) > ZERO_PREC)
+                f = FUNIT_E * omega[(size_t)g0 * n + s] * vel[((size_t)g0 * n + s) * 3 + k] / (it * (T * T));
+            F0[(size_t)i * 3 + k] = f;
+        }
+    }
+}
+
+// multiplyTaudFnew then F = F0 + dF.
+__global__ void k_bte_update(int ntr, int n, const int* tr_grid, const double* inv_tau, const double* F0,
+                             double* dF, double* F) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntr * n; i += gridDim.x * blockDim.x) {
+        const int q = i / n, s = i % n;
+        const double it = inv_tau[i];
+        const bool scale = !(tr_grid[q] == 0 && s < 3) && fabs(it) > ZERO_PREC;
+        for (int k = 0; k < 3; ++k) {
+            double d = dF[(size_t)i * 3 + k];
+            if (scale) d /= it;
+            F[(size_t)i * 3 + k] = F0[(size_t)i * 3 + k] + d;
+        }
+    }
+}
+
+// kappa = kW_mK / (Nq V) sum_{q, s} deg w n (n+1) v (x) F   (one CTA, tree reduction)
+__global__ void __launch_bounds__(256) k_bte_kappa(int ntr, int n, int nq, double vol, const int* tr_grid,
+                                                   const int* deg, const double* omega, const double* nbe,
+                                                   const double* vel, const double* F, double* kappa) {
+    __shared__ double red[256][9];
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < ntr * n; i += blockDim.x) {
+        const int q = i / n, s = i % n, g0 = tr_grid[q];
+        if (g0 == 0 && s < 3) continue;
+        const double w = omega[(size_t)g0 * n + s], nb = nbe[(size_t)g0 * n + s];
+        const double pre = double(deg[q]) * w * nb * (nb + 1.0);
+        const double* v = vel + ((size_t)g0 * n + s) * 3;
+        const double* f = F + (size_t)i * 3;
+        for (int x = 0; x < 3; ++x)
+            for (int y = 0; y < 3; ++y) acc[3 * x + y] += pre * (v[x] * f[y]);
+    }
+    for (int k = 0; k < 9; ++k) red[threadIdx.x][k] = acc[k];
+    __syncthreads();
+    for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int k = 0; k < 9; ++k) red[threadIdx.x][k] += red[threadIdx.x + h][k];
+        __syncthreads();
+    }
+    if (threadIdx.x < 9) kappa[threadIdx.x] = KW_MK * (1.0 / (double(nq) * vol)) * red[0][threadIdx.x];
+}
+
+int grid_x(long long items, int threads, int slots) {
+    long long want = (items + (long long)threads * 4 - 1) / ((long long)threads * 4);
+    long long cap = (148LL * 16 + slots - 1) / slots;
+    if (want > cap) want = cap;
+    return (int)(want < 1 ? 1 : want);
+}
+
+// Time-reversal set on the host from the grid addresses.
+int build_tr_set(spring_ctx* c) {
+    const int nq = c->nq;
+    std::vector<int> qint((size_t)nq * 3);
+    SPRING_CHECK(d2h(c, qint.data(), c->d_qint.p, sizeof(int) * qint.size(), "grid addresses"));
+    auto gidx = [&](int x, int y, int z) {
+        auto m = [](int a, int n) { int r = a % n; return r < 0 ? r + n : r; };
+        return m(x, c->mesh[0]) + c->mesh[0] * (m(y, c->mesh[1]) + c->mesh[1] * m(z, c->mesh[2]));
+    };
+    std::vector<int> neg(nq), rep(nq);
+    for (int q = 0; q < nq; ++q) {
+        neg[q] = gidx(-qint[3 * q], -qint[3 * q + 1], -qint[3 * q + 2]);
+        rep[q] = std::min(q, neg[q]);
+    }
+    std::vector<int> grid;
+    for (int q = 0; q < nq; ++q)
+        if (rep[q] == q) grid.push_back(q);
+    const int ntr = (int)grid.size();
+    std::vector<int> slot(nq, -1), pos(nq), sgn(nq), deg(ntr, 0), tint((size_t)ntr * 3);
+    for (int i = 0; i < ntr; ++i) {
+        slot[grid[i]] = i;
+        for (int d = 0; d < 3; ++d) tint[3 * i + d] = qint[3 * grid[i] + d];
+    }
+    for (int q = 0; q < nq; ++q) {
+        pos[q] = slot[rep[q]];
+        sgn[q] = q == rep[q] ? 1 : -1;
+        deg[pos[q]] += 1;
+    }
+    SPRING_CHECK(dalloc(c, c->d_tr_int, tint.size(), "time-reversal set"));
+    SPRING_CHECK(dalloc(c, c->d_tr_grid, ntr, "time-reversal set"));
+    SPRING_CHECK(dalloc(c, c->d_tr_pos, nq, "time-reversal set"));
+    SPRING_CHECK(dalloc(c, c->d_tr_sgn, nq, "time-reversal set"));
+    SPRING_CHECK(dalloc(c, c->d_tr_deg, ntr, "time-reversal set"));
+    SPRING_CHECK(dalloc(c, c->d_neg, nq, "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_tr_int.p, tint.data(), sizeof(int) * tint.size(), "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_tr_grid.p, grid.data(), sizeof(int) * ntr, "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_tr_pos.p, pos.data(), sizeof(int) * nq, "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_tr_sgn.p, sgn.data(), sizeof(int) * nq, "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_tr_deg.p, deg.data(), sizeof(int) * ntr, "time-reversal set"));
+    SPRING_CHECK(h2d(c, c->d_neg.p, neg.data(), sizeof(int) * nq, "time-reversal set"));
+    c->ntr = ntr;
+    c->ps_tr.n0 = ntr;
+    c->ps_tr.q0_int = c->d_tr_int.p;
+    c->ps_tr.q0_grid = c->d_tr_grid.p;
+    c->ps_tr.done = false;
+    dfree(c->d_wtr);
+    return SPRING_OK;
+}
+
+}  // namespace
+
+int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters) {
+    if (c->ntr == 0) SPRING_CHECK(build_tr_set(c));
+    if (!c->ps_tr.done) SPRING_CHECK(run_enumerate3(c, c->ps_tr));
+    const int n = c->ndof, ntr = c->ntr, nq = c->nq;
+    const size_t slot = (size_t)nq * n * n * n;
+    const Q0View view{c->d_tr_int.p, c->d_tr_grid.p, c->ph_grid.evec.p, c->ph_grid.omega.p, c->ph_grid.oneby.p};
+    // W grids: all of them resident when they fit the budget, else batches recomputed per pass
+    const size_t budget = (size_t)40 << 30;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const bool cache_all = slot * ntr * sizeof(double) <= std::min(budget, free_b / 2);
+    int batch = ntr;
+    if (cache_all) {
+        if (!c->d_wtr.p || c->d_wtr.n < slot * ntr) {
+            SPRING_CHECK(dalloc(c, c->d_wtr, slot * ntr, "time-reversal W grids"));
+            SPRING_CHECK(run_v3_wgrid(c, c->ps_tr, view, 0, ntr, c->d_wtr.p));
+        }
+    } else {
+        batch = (int)std::max<size_t>(1, ((size_t)96 << 20) / (slot * sizeof(double)));
+        batch = std::min(batch, ntr);
+        SPRING_CHECK(dalloc(c, c->d_w, slot * batch, "W buffer"));
+    }
+    DBuf<double> inv_tau, F0, F, dF, kap;
+    int rc = dalloc(c, inv_tau, (size_t)ntr * n, "1/tau");
+    if (rc == SPRING_OK) rc = dalloc(c, F0, (size_t)ntr * n * 3, "F0");
+    if (rc == SPRING_OK) rc = dalloc(c, F, (size_t)ntr * n * 3, "F");
+    if (rc == SPRING_OK) rc = dalloc(c, dF, (size_t)ntr * n * 3, "dF");
+    if (rc == SPRING_OK) rc = dalloc(c, kap, 9, "kappa");
+
+    auto pass = [&](int mode, int T) -> int {
+        PassArgs pa;
+        pa.n = n;
+        pa.nq = nq;
+        pa.ntet = 6 * nq;
+        pa.tr_grid = c->d_tr_grid.p;
+        pa.tr_pos = c->d_tr_pos.p;
+        pa.tr_sgn = c->d_tr_sgn.p;
+        pa.neg = c->d_neg.p;
+        pa.partner = c->ps_tr.partner.p;
+        pa.omega = c->ph_grid.omega.p;
+        pa.nbe = c->ph_grid.nbe.p + (size_t)T * nq * n;
+        pa.F = F.p;
+        pa.out = mode == 0 ? inv_tau.p : dF.p;
+        const long long items = (long long)pa.ntet * n * n;
+        for (int b = 0; b < ntr; b += batch) {
+            const int nb = std::min(batch, ntr - b);
+            if (!cache_all) SPRING_CHECK(run_v3_wgrid(c, c->ps_tr, view, b, nb, c->d_w.p));
+            pa.q0_first = b;
+            pa.wgrid = cache_all ? c->d_wtr.p + slot * b : c->d_w.p;
+            dim3 grid(grid_x(items, 128, nb), nb);
+            for (int s0a = 0; s0a < n; s0a += NS0) {
+                pa.s0a = s0a;
+                pa.s0n = std::min(NS0, n - s0a);
+                if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure");
+                if (mode == 0) k_bte_pass<0><<<grid, 128, 0, c->stream>>>(pa, reinterpret_cast<const int4*>(c->d_tetra.p));
+                else k_bte_pass<1><<<grid, 128, 0, c->stream>>>(pa, reinterpret_cast<const int4*>(c->d_tetra.p));
+                SPRING_CHECK(launch_check(c, mode == 0 ? "k_bte_pass<tau>" : "k_bte_pass<dF>"));
+            }
+        }
+        return SPRING_OK;
+    };
+    auto kappa_of = [&](int T, const double* Fv, double* out9) -> int {
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure");
+        k_bte_kappa<<<1, 256, 0, c->stream>>>(ntr, n, nq, c->vol, c->d_tr_grid.p, c->d_tr_deg.p, c->ph_grid.omega.p,
+                                              c->ph_grid.nbe.p + (size_t)T * nq * n, c->ph_grid.vel.p, Fv, kap.p);
+        SPRING_CHECK(launch_check(c, "k_bte_kappa"));
+        return d2h(c, out9, kap.p, sizeof(double) * 9, "kappa");
+    };
+    const int threads = 256, blocks = std::max(1, std::min((ntr * n + threads - 1) / threads, 148 * 8));
+    for (int T = 0; rc == SPRING_OK && T < c->nT; ++T) {
+        rc = zero(c, inv_tau.p, sizeof(double) * ntr * n, "1/tau");
+        if (rc == SPRING_OK) rc = pass(0, T);
+        if (rc == SPRING_OK && !launch_injected(c)) {
+            k_bte_f0<<<blocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, c->ph_grid.omega.p, c->ph_grid.vel.p,
+                                                        inv_tau.p, c->temps[T], F0.p);
+            rc = launch_check(c, "k_bte_f0");
+        }
+        if (rc == SPRING_OK)
+            rc = cudaMemcpyAsync(F.p, F0.p, sizeof(double) * ntr * n * 3, cudaMemcpyDeviceToDevice, c->stream) ==
+                         cudaSuccess ? SPRING_OK : fail(c, SPRING_ERR_CUDA, "F copy");
+        double k0[9], kold[9], knew[9];
+        if (rc == SPRING_OK) rc = kappa_of(T, F.p, k0);
+        if (rc != SPRING_OK) break;
+        std::copy(k0, k0 + 9, kold);
+        std::copy(k0, k0 + 9, knew);
+        int iter = 0;
+        for (;;) {
+            ++iter;
+            rc = zero(c, dF.p, sizeof(double) * ntr * n * 3, "dF");
+            if (rc == SPRING_OK) rc = pass(1, T);
+            if (rc == SPRING_OK && !launch_injected(c)) {
+                k_bte_update<<<blocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, inv_tau.p, F0.p, dF.p, F.p);
+                rc = launch_check(c, "k_bte_update");
+            }
+            if (rc == SPRING_OK) rc = kappa_of(T, F.p, knew);
+            if (rc != SPRING_OK) break;
+            double d = 0.0;
+            for (int k = 0; k < 9; ++k) d = std::max(d, std::fabs(knew[k] - kold[k]));
+            if (d < eps_k || iter > max_iter) break;
+            std::copy(knew, knew + 9, kold);
+        }
+        if (rc != SPRING_OK) break;
+        if (h_kappa) std::copy(knew, knew + 9, h_kappa + 9 * T);
+        if (h_kappa_rta) std::copy(k0, k0 + 9, h_kappa_rta + 9 * T);
+        if (h_iters) h_iters[T] = iter;
+    }
+    dfree(inv_tau); dfree(F0); dfree(F); dfree(dF); dfree(kap);
+    return rc;
+}
+
+}  // namespace spring

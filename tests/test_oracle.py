@@ -204,6 +204,19 @@ def test_kappa_cubic_isotropy(setup5):
     assert abs(np.trace(full.reshape(3, 3)) / 3 - kap[0]) < 0.05 * kap[0]
 
 
+def test_bte_iteration0_is_full_grid_rta(cr):
+    """kappa_iter's 1/tau equals twice kappa.x's linewidth per mode, and its iteration-0 kappa
+    equals kappa.x's full-grid RTA kappa, when both use every grid point (identity symmetry)."""
+    N = 4
+    st = D.Setup(cr, (N, N, N), [300.0], W=np.eye(3, dtype=np.int32)[None], Rxyz=np.eye(3)[None])
+    r = D.bte_iter(st)
+    lw = D.linewidth3_all(st, "tetra")
+    np.testing.assert_allclose(r["inv_tau"], 2.0 * lw[0][r["irr_grid"]], rtol=1e-10, atol=1e-16)
+    kf = D.kappa_rta(st, lw, symm=False)[0]
+    np.testing.assert_allclose(r["kappa_rta"], kf, rtol=1e-10, atol=1e-10 * np.abs(kf).max())
+    assert r["iters"] > 1 and r["kappa"][0] > r["kappa_rta"][0]
+
+
 def test_constants():
     assert abs(C.wTHz - 98.22693) < 1e-4
     assert abs(0.3767 - 2 * 2 * np.pi * 2.99792458e-2) < 2e-4   # 2 cm^-1 in rad/ps
