@@ -141,6 +141,22 @@ int spring_scatter_w3(spring_ctx* ctx, int i0, double* sctrq1);
 int spring_linewidth3(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol3,
                       double* lw, double* p3_q0);
 
+/* No counterpart in the reference.  The tetrahedron 3-phonon linewidth of one
+ * irreducible point i0 (1-based) for callers that must not have the library
+ * call cudaMalloc: hosts whose device memory belongs to another allocator, or
+ * pipelines that cannot take the synchronisation cudaMalloc/cudaFree may imply.
+ * Allocates nothing: its scratch is a fixed 16 MiB device array inside the
+ * library (held by every GPU that loads it, until exit).  Limit:
+ * Nq*Ndof^3 + (n_temps+1)*Nq0*Ndof <= 2^21 doubles (a 2-atom cell up to about
+ * 21^3 q-points); larger meshes get SPRING_ERR_UNSUPPORTED.
+ * Needs the inputs loaded and spring_prepare3 called beforehand.  d_lw (Ndof x
+ * n_temps) and d_p3 (Ndof) are caller-owned DEVICE buffers; the context's
+ * resident LW_Allq0 is not touched.  pol3 as in spring_linewidth3 (or NULL).
+ * The first call on a device looks the array's address up; make it before any
+ * stream capture.  All calls share the array: calls whose GPU work overlaps race
+ * and must be serialised by the caller. */
+int spring_linewidth3_tetra_noalloc(spring_ctx* ctx, int i0, const int* pol3, double* d_lw, double* d_p3);
+
 /* Isotope scattering rate, CalculateIsoW + CalculateIsoLwTetra
  * (src/Kappa/Src/IsotopicScatter.f90:36-168); Gaussian form uses
  * delta(omega0 - omega1).  g2(Nb) mass variance.  rate(Ndof,n_q0,n_temps)

@@ -55,6 +55,7 @@ SIGNATURES = {
     "spring_scatter_w3": [P, I, P],
     "spring_linewidth3": [P, I, I, I, D, P, P, P],
     "spring_linewidth_iso": [P, I, I, I, D, P, P],
+    "spring_linewidth3_tetra_noalloc": [P, I, P, P, P],
     "spring_reset_linewidths": [P],
     "spring_get_linewidths": [P, P],
     "spring_set_linewidths": [P, P],
