@@ -78,6 +78,10 @@ int spring_set_fc2(spring_ctx* ctx, int na2, const int* atm_num, const int* atm_
  * fc3(3,3,3,na3,na3,Nb) = (gamma,beta,alpha,N2,N1,mu). */
 int spring_set_fc3(spring_ctx* ctx, int na3, const int* atm_num, const int* atm_indx, const double* fc3);
 
+/* FC4type%set_FC4, src/Kappa/Src/FC4_mod.f90:46-97: atm_indx(4,na4,Nb),
+ * fc4(3,3,3,3,na4,na4,na4,Nb) = (delta,gamma,beta,alpha,N3,N2,N1,mu). */
+int spring_set_fc4(spring_ctx* ctx, int na4, const int* atm_num, const int* atm_indx, const double* fc4);
+
 /* ---- mesh and irreducible q-points (L3) -------------------------------- */
 /* q_tetrahedron%make_tetrahedron, src/Kappa/Src/TetrahedronQ_m.f90:56-221.
  * zero_centered = 1 folds to [-N/2+1, N/2] (kappa.x), 0 keeps [0, N) (LineWidth.x).
@@ -163,6 +167,30 @@ int spring_linewidth3_tetra_noalloc(spring_ctx* ctx, int i0, const int* pol3, do
  * optional; 0.5*rate is added to the resident LW_Allq0 (main.f90:604). */
 int spring_linewidth_iso(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const double* g2,
                          double* rate);
+
+/* ---- four-phonon scattering ------------------------------------------- */
+/* MomentumConsrv4th + Permutation4th, src/Kappa/Src/QuasiMomentumConsrv4th_m.f90:32-312,
+ * for q0 = i0 (1-based): Allq1q2q3(3,Nq,Nq) = (permutation type, quartet
+ * number, q3 grid index) of every ordered (q1, q2); q1q2q3_permuted(3,cap) the
+ * grid indices of each quartet.  counts = (q1q2q3_count, total_count).  Both
+ * arrays optional; more than cap quartets with a non-NULL q1q2q3_permuted is
+ * SPRING_ERR_ARG.  Bit-identical to the reference algorithm on every mesh. */
+int spring_enumerate4(spring_ctx* ctx, int i0, int* Allq1q2q3, int* q1q2q3_permuted, long long cap,
+                      long long* counts);
+
+/* The 4-phonon scattering rate of irreducible points i0_first .. +n_q0-1, every
+ * temperature: quartets -> V4 -> W4 -> delta sum on the device.
+ *   delta_mode SPRING_DELTA_TETRA: ScatterProbq1q2_per (FourthOrder_m.f90:286-473)
+ *     + TetrahedronIntegration4th (Tetrahedron4th_sep.f90:37-425), every W read
+ *     through the stored quartet with the reference's permutation of branches;
+ *     holds one q0's quartet W (Nq^2/6 x Ndof^4 doubles) on the device.
+ *   delta_mode SPRING_DELTA_GAUSS: the same three channels with
+ *     delta(omega0 - M), W of each ordering from its quartet (build-side form).
+ * Two-atom cells, na4 <= 8, n_temps <= 9.  pol4(2,4): Polarization4th or NULL.
+ * rate(Ndof,n_q0,n_temps) optional; 0.5*rate is added to the resident LW_Allq0
+ * (main.f90:661). */
+int spring_linewidth4(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol4,
+                      double* rate);
 
 /* Zero / read / replace the resident LW_Allq0(Ndof,Nq0,n_temps). */
 int spring_reset_linewidths(spring_ctx* ctx);

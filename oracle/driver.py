@@ -381,3 +381,88 @@ def bte_iter(st: Setup, it=0, eps_k=1e-6, max_iter=1000):
                                _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _f(st.ph["grp_vel"]), deg,
                                float(st.temps[it]), st.cr.vol, eps_k, max_iter, inv_tau, F, krta, kap)
     return dict(kappa=kap, kappa_rta=krta, inv_tau=inv_tau, F=F, iters=iters, irr_grid=irr_grid, deg=deg)
+
+
+# ----------------------------------------------------------------------------- four-phonon
+def _l4():
+    L = lib()
+    if not hasattr(L, "_w4_set"):
+        L.orc_w4_naive.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, ct.c_int, f64p, f64p, f64p, i32p,
+                                   c128p, f64p, c128p, f64p, c128p, f64p, c128p, f64p, f64p]
+        L.orc_w4_naive.restype = None
+        L.orc_w4_factored.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, ct.c_int, f64p, i32p, i32p,
+                                      c128p, f64p, c128p, f64p, ct.c_longlong, i32p, f64p]
+        L.orc_w4_factored.restype = None
+        L.orc_lw4_tetra.argtypes = [ct.c_int, ct.c_int, i32p, f64p, f64p, f64p, f64p, i32p, i32p, f64p, i32p, f64p]
+        L.orc_lw4_tetra.restype = None
+        L.orc_lw4_gauss.argtypes = [ct.c_int, ct.c_int, i32p, f64p, f64p, f64p, f64p, i32p, f64p, i32p, ct.c_double,
+                                    f64p]
+        L.orc_lw4_gauss.restype = None
+        L._w4_set = True
+    return L
+
+
+def fc4_derived(cr):
+    idx = cr.fc4_atm_indx
+    return _i(idx[:, :, 3]), _f(np.einsum("ij,mnj->mni", cr.latvec, idx[:, :, :3].astype(np.float64)))
+
+
+def w4_naive(cr, nq, q1, q2, q3, q0chk, e0, o0, e1, o1, e2, o2, e3, o3):
+    """ScatterMatEl4 + ScatterProbability4 in the reference loop order, one quartet."""
+    nd = cr.ndof
+    btyp, posr = fc4_derived(cr)
+    W = np.zeros((nd, nd, nd, nd))
+    _l4().orc_w4_naive(cr.nbasis, cr.fc4.shape[1], _i(cr.fc4_atm_num), btyp, posr, _f(cr.fc4),
+                       _f(1.0 / np.sqrt(cr.mass)), nq, _f(q1), _f(q2), _f(q3), _i(q0chk), _c(e0), _f(o0), _c(e1),
+                       _f(o1), _c(e2), _f(o2), _c(e3), _f(o3), W)
+    return W
+
+
+def w4_factored(st, i0, quartets, q0_from_grid=None):
+    """W4 [quartet][s0][s1][s2][s3] for 1-based grid quartets (q1, q2, q3) of q0 = irreducible i0."""
+    cr = st.cr
+    nd = cr.ndof
+    btyp, posr = fc4_derived(cr)
+    quartets = _i(quartets)
+    out = np.zeros((len(quartets), nd, nd, nd, nd))
+    _l4().orc_w4_factored(cr.nbasis, cr.fc4.shape[1], _i(cr.fc4_atm_num), btyp, posr, _f(cr.fc4),
+                          _f(1.0 / np.sqrt(cr.mass)), st.nq, _f(st.q_pnt), _i(st.q_pnt_int), _i(st.irr_int[i0]),
+                          _c(st.ph0["evec"][i0]), _f(st.ph0["onebyomega"][i0]), _c(st.ph["evec"]),
+                          _f(st.ph["onebyomega"]), len(quartets), quartets, out)
+    return out
+
+
+def lw4_tetra(st, i0, it=0, pol=None):
+    """Four-phonon scattering rate of q0 = irreducible i0 (TetrahedronIntegration4th)."""
+    nd = st.cr.ndof
+    if pol is None:
+        pol = np.array([[1, nd]] * 4, np.int32)
+    A, perm, cnt = momentum4(st.mesh, st.q_pnt_int, st.irr_int[i0])
+    Wq = w4_factored(st, i0, perm)
+    rate = np.zeros(nd)
+    _l4().orc_lw4_tetra(nd, st.nq, _i(st.irr_int[i0]), _f(st.ph0["omega"][i0]), _f(st.ph0["nbe"][it][i0]),
+                        _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _i(st.tetra), _i(A), _f(Wq), _i(pol), rate)
+    return rate, dict(Allq1q2q3=A, perm=perm, counts=cnt)
+
+
+def q3_map(st, q0_int):
+    """grid index (0-based) of q3 = -q0 - q1 - q2 for every ordered (q1, q2)."""
+    mesh = st.mesh
+    s = -(np.asarray(q0_int)[None, None, :] + st.q_pnt_int[:, None, :] + st.q_pnt_int[None, :, :])
+    m = np.mod(s, mesh[None, None, :])
+    return (m[..., 0] + mesh[0] * (m[..., 1] + mesh[1] * m[..., 2])).astype(np.int32)
+
+
+def lw4_gauss(st, i0, it=0, sigma=0.3767, pol=None):
+    """Gaussian four-phonon scattering rate of q0 = irreducible i0 (build-side extension)."""
+    nd = st.cr.ndof
+    if pol is None:
+        pol = np.array([[1, nd]] * 4, np.int32)
+    q3 = q3_map(st, st.irr_int[i0])
+    g = np.arange(st.nq, dtype=np.int32)
+    quart = np.stack([np.repeat(g, st.nq), np.tile(g, st.nq), q3.ravel()], axis=1) + 1
+    W4 = w4_factored(st, i0, quart)
+    rate = np.zeros(nd)
+    _l4().orc_lw4_gauss(nd, st.nq, _i(st.irr_int[i0]), _f(st.ph0["omega"][i0]), _f(st.ph0["nbe"][it][i0]),
+                        _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _i(q3), _f(W4), _i(pol), float(sigma), rate)
+    return rate

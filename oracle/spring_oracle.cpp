@@ -729,6 +729,298 @@ void orc_kappa_full(int ndof, int nq, const int* q_pnt_int, const int* pos, cons
 }
 
 // ---------------------------------------------------------------------------
+// Four-phonon matrix elements.
+// ScatterMatEl4 (src/Kappa/Src/FourthOrder_m.f90:286-422) in the reference loop
+// order, for one quartet: Phi(s3,s2,s1,s) = sum FC4(d,c,b,a,N3,N2,N1,mu)
+// e^{i q1.R1} e^{i q2.R2} e^{i q3.R3} m^-1/2(mu,nu,eta,ro) e0(mu a,s) e1(nu b,s1) e2(eta c,s2) e3(ro d,s3),
+// then ScatterProbability4 (:425-473): W = |Phi|^2 (1/w0)(1/w1)(1/w2)(1/w3) Sctr4THz2/Nq^2.
+//   fc4(3,3,3,3,Na4,Na4,Na4,Nb); e*(Ndof,Ndof) [s][row] memory; q0chk = Gamma flags of q0..q3.
+//   out W[s0][s1][s2][s3] (== Fortran W(s3,s2,s1,s0)).
+static const double Sctr4THz2 = 0.125 * PI * ((1.054571817 * 1.602176565) * (1.054571817 * 1.602176565)) *
+                                (6.022140857 * 6.022140857 * 6.022140857 * 6.022140857) * 1000000.0;
+
+void orc_w4_naive(int nb, int na4, const int* atm_num, const int* basis_typ, const double* atm_pos_r,
+                  const double* fc4, const double* onebysqrtmass, int nq, const double* q1, const double* q2,
+                  const double* q3, const int* q0chk, const double* e0_ri, const double* o0, const double* e1_ri,
+                  const double* o1, const double* e2_ri, const double* o2, const double* e3_ri, const double* o3,
+                  double* W) {
+    const int n = 3 * nb;
+    const cplx* e0 = reinterpret_cast<const cplx*>(e0_ri);
+    const cplx* e1 = reinterpret_cast<const cplx*>(e1_ri);
+    const cplx* e2 = reinterpret_cast<const cplx*>(e2_ri);
+    const cplx* e3 = reinterpret_cast<const cplx*>(e3_ri);
+    const size_t n4 = (size_t)n * n * n * n;
+    std::vector<cplx> phi(n4, cplx(0.0, 0.0));
+    int strt[4];
+    for (int k = 0; k < 4; ++k) strt[k] = q0chk[k] ? 3 : 0;
+    for (int mu = 0; mu < nb; ++mu)
+        for (int N1 = 0; N1 < atm_num[mu]; ++N1) {
+            const int nu = basis_typ[N1 + na4 * mu] - 1;
+            const double* R1 = atm_pos_r + 3 * (N1 + na4 * mu);
+            const double a1 = q1[0] * R1[0] + q1[1] * R1[1] + q1[2] * R1[2];
+            const cplx x1(std::cos(a1), std::sin(a1));
+            for (int N2 = 0; N2 < atm_num[mu]; ++N2) {
+                const int eta = basis_typ[N2 + na4 * mu] - 1;
+                const double* R2 = atm_pos_r + 3 * (N2 + na4 * mu);
+                const double a2 = q2[0] * R2[0] + q2[1] * R2[1] + q2[2] * R2[2];
+                const cplx x2(std::cos(a2), std::sin(a2));
+                for (int N3 = 0; N3 < atm_num[mu]; ++N3) {
+                    const int ro = basis_typ[N3 + na4 * mu] - 1;
+                    const double* R3 = atm_pos_r + 3 * (N3 + na4 * mu);
+                    const double a3 = q3[0] * R3[0] + q3[1] * R3[1] + q3[2] * R3[2];
+                    const cplx x3(std::cos(a3), std::sin(a3));
+                    const double mf = onebysqrtmass[mu] * onebysqrtmass[nu] * onebysqrtmass[eta] * onebysqrtmass[ro];
+                    const cplx em = mf * x1 * x2 * x3;
+                    for (int al = 0; al < 3; ++al)
+                        for (int s = strt[0]; s < n; ++s) {
+                            const cplx w0 = e0[(3 * mu + al) + n * s];
+                            for (int be = 0; be < 3; ++be)
+                                for (int s1 = strt[1]; s1 < n; ++s1) {
+                                    const cplx w1 = e1[(3 * nu + be) + n * s1];
+                                    for (int ga = 0; ga < 3; ++ga)
+                                        for (int s2 = strt[2]; s2 < n; ++s2) {
+                                            const cplx w2 = e2[(3 * eta + ga) + n * s2];
+                                            for (int de = 0; de < 3; ++de) {
+                                                const size_t fi = de + 3 * (ga + 3 * (be + 3 * (al + 3 * (N3 + (size_t)na4 * (N2 + (size_t)na4 * (N1 + (size_t)na4 * mu))))));
+                                                const cplx pm = fc4[fi] * em;
+                                                for (int s3 = strt[3]; s3 < n; ++s3)
+                                                    phi[((s * n + s1) * n + s2) * (size_t)n + s3] += pm * w0 * w1 * w2 * e3[(3 * ro + de) + n * s3];
+                                            }
+                                        }
+                                }
+                        }
+                }
+            }
+        }
+    const double mfac = Sctr4THz2 / (double(nq) * double(nq));
+    for (int s = 0; s < n; ++s)
+        for (int s1 = 0; s1 < n; ++s1)
+            for (int s2 = 0; s2 < n; ++s2)
+                for (int s3 = 0; s3 < n; ++s3) {
+                    const size_t k = ((s * n + s1) * n + s2) * (size_t)n + s3;
+                    const bool z = s < strt[0] || s1 < strt[1] || s2 < strt[2] || s3 < strt[3];
+                    const double a2 = phi[k].real() * phi[k].real() + phi[k].imag() * phi[k].imag();
+                    W[k] = z ? 0.0 : (a2 * (o0[s] * o1[s1] * o2[s2] * o3[s3])) * mfac;
+                }
+}
+
+// The same W for many quartets with the sum regrouped (phases folded into FC4 per basis
+// block, then four eigenvector contractions); OpenMP over quartets.
+//   quartets(3,nquart) 1-based grid indices; q_pnt(3,Nq), q_pnt_int(3,Nq); q0 float/int;
+//   evec grid (Ndof,Ndof,Nq), oneby grid; out W [quartet][s0][s1][s2][s3].
+void orc_w4_factored(int nb, int na4, const int* atm_num, const int* basis_typ, const double* atm_pos_r,
+                     const double* fc4, const double* onebysqrtmass, int nq, const double* q_pnt, const int* q_pnt_int,
+                     const int* q0_int, const double* e0_ri, const double* o0, const double* evec_ri,
+                     const double* oneby, long long nquart, const int* quart, double* Wout) {
+    const int n = 3 * nb;
+    const size_t n4 = (size_t)n * n * n * n;
+    const cplx* e0 = reinterpret_cast<const cplx*>(e0_ri);
+    const cplx* ev = reinterpret_cast<const cplx*>(evec_ri);
+    const double mfac = Sctr4THz2 / (double(nq) * double(nq));
+    const bool g0 = q0_int[0] == 0 && q0_int[1] == 0 && q0_int[2] == 0;
+#pragma omp parallel
+    {
+        std::vector<cplx> D((size_t)3 * n * n * n), T1((size_t)3 * n * n * n), T2((size_t)3 * n * n * n),
+            T3((size_t)3 * n * n * n), phi(n4);
+#pragma omp for schedule(dynamic, 16)
+        for (long long iq = 0; iq < nquart; ++iq) {
+            const int g[3] = {quart[3 * iq] - 1, quart[3 * iq + 1] - 1, quart[3 * iq + 2] - 1};
+            std::fill(phi.begin(), phi.end(), cplx(0.0, 0.0));
+            for (int mu = 0; mu < nb; ++mu) {
+                std::fill(D.begin(), D.end(), cplx(0.0, 0.0));
+                std::vector<cplx> P[3];
+                for (int k = 0; k < 3; ++k) {
+                    P[k].resize(atm_num[mu]);
+                    const double* q = q_pnt + 3 * g[k];
+                    for (int N = 0; N < atm_num[mu]; ++N) {
+                        const double* R = atm_pos_r + 3 * (N + na4 * mu);
+                        const double a = q[0] * R[0] + q[1] * R[1] + q[2] * R[2];
+                        const int b = basis_typ[N + na4 * mu] - 1;
+                        P[k][N] = onebysqrtmass[b] * cplx(std::cos(a), std::sin(a));
+                    }
+                }
+                // D[a][nu b][eta c][ro d]
+                for (int N1 = 0; N1 < atm_num[mu]; ++N1)
+                    for (int N2 = 0; N2 < atm_num[mu]; ++N2)
+                        for (int N3 = 0; N3 < atm_num[mu]; ++N3) {
+                            const int nu = basis_typ[N1 + na4 * mu] - 1, eta = basis_typ[N2 + na4 * mu] - 1,
+                                      ro = basis_typ[N3 + na4 * mu] - 1;
+                            const cplx ph = P[0][N1] * P[1][N2] * P[2][N3];
+                            const double* f = fc4 + 81 * (N3 + (size_t)na4 * (N2 + (size_t)na4 * (N1 + (size_t)na4 * mu)));
+                            for (int al = 0; al < 3; ++al)
+                                for (int be = 0; be < 3; ++be)
+                                    for (int ga = 0; ga < 3; ++ga)
+                                        for (int de = 0; de < 3; ++de)
+                                            D[((al * n + 3 * nu + be) * n + 3 * eta + ga) * n + 3 * ro + de] +=
+                                                f[((al * 3 + be) * 3 + ga) * 3 + de] * ph;
+                        }
+                const cplx* e1 = ev + (size_t)g[0] * n * n;
+                const cplx* e2 = ev + (size_t)g[1] * n * n;
+                const cplx* e3 = ev + (size_t)g[2] * n * n;
+                const size_t R3 = (size_t)3 * n * n;  // rows (a, nu b, eta c)
+                for (size_t r = 0; r < R3; ++r)
+                    for (int s3 = 0; s3 < n; ++s3) {
+                        cplx acc(0.0, 0.0);
+                        for (int k = 0; k < n; ++k) acc += D[r * n + k] * e3[k + n * s3];
+                        T1[r * n + s3] = acc;
+                    }
+                // T2[a][nu b][s2][s3] = sum_{eta c} e2(eta c, s2) T1[a][nu b][eta c][s3]
+                for (int ab = 0; ab < 3 * n; ++ab)
+                    for (int s2 = 0; s2 < n; ++s2)
+                        for (int s3 = 0; s3 < n; ++s3) {
+                            cplx acc(0.0, 0.0);
+                            for (int k = 0; k < n; ++k) acc += e2[k + n * s2] * T1[((size_t)ab * n + k) * n + s3];
+                            T2[((size_t)ab * n + s2) * n + s3] = acc;
+                        }
+                // T3[a][s1][s2][s3] = sum_{nu b} e1(nu b, s1) T2[a][nu b][s2][s3]
+                for (int a = 0; a < 3; ++a)
+                    for (int s1 = 0; s1 < n; ++s1)
+                        for (int s23 = 0; s23 < n * n; ++s23) {
+                            cplx acc(0.0, 0.0);
+                            for (int k = 0; k < n; ++k) acc += e1[k + n * s1] * T2[((size_t)a * n + k) * n * n + s23];
+                            T3[((size_t)a * n + s1) * n * n + s23] = acc;
+                        }
+                for (int s = 0; s < n; ++s)
+                    for (int a = 0; a < 3; ++a) {
+                        const cplx w = onebysqrtmass[mu] * e0[(3 * mu + a) + n * s];
+                        for (int k = 0; k < n * n * n; ++k) phi[(size_t)s * n * n * n + k] += w * T3[(size_t)a * n * n * n + k];
+                    }
+            }
+            const bool gq[3] = {g[0] == 0, g[1] == 0, g[2] == 0};
+            double* W = Wout + (size_t)iq * n4;
+            const double* o1 = oneby + (size_t)g[0] * n;
+            const double* o2 = oneby + (size_t)g[1] * n;
+            const double* o3 = oneby + (size_t)g[2] * n;
+            for (int s = 0; s < n; ++s)
+                for (int s1 = 0; s1 < n; ++s1)
+                    for (int s2 = 0; s2 < n; ++s2)
+                        for (int s3 = 0; s3 < n; ++s3) {
+                            const size_t k = ((s * n + s1) * n + s2) * (size_t)n + s3;
+                            const bool z = (g0 && s < 3) || (gq[0] && s1 < 3) || (gq[1] && s2 < 3) || (gq[2] && s3 < 3);
+                            const double a2 = phi[k].real() * phi[k].real() + phi[k].imag() * phi[k].imag();
+                            W[k] = z ? 0.0 : (a2 * (o0[s] * o1[s1] * o2[s2] * o3[s3])) * mfac;
+                        }
+        }
+    }
+}
+
+// TetrahedronIntegration4th / SumOverPolarization / FindFandOmegaVer_4th
+// (src/Kappa/Src/Tetrahedron4th_sep.f90:37-425), one q0: for every q1 of the grid
+// and every tetrahedron of q2, the vertices' q3, quartet number and permutation
+// type come from Allq1q2q3 (as written by MomentumConsrv4th) and the W of a vertex
+// is read from the stored quartet W with the reference's mode permutation
+// (after_perm = before_perm(per(:, type))).  Three channels (1/6, 1/2, 1/2) with
+// F divided by n0; NaN weights set to zero.
+//   Allq1q2q3 [q1][q2][3]; Wq [quartet][s0][s1][s2][s3]; pol(2,4) 1-based;
+//   omega0/nbe0 of q0 (Ndof); omega/nbe grid [q][s]; out rate(Ndof).
+void orc_lw4_tetra(int ndof, int nq, const int* q0_int, const double* omega0, const double* nbe0, const double* omega,
+                   const double* nbe, const int* tetra, const int* Allq1q2q3, const double* Wq, const int* pol,
+                   double* rate) {
+    const int n = ndof;
+    const size_t n4 = (size_t)n * n * n * n;
+    const int ntet = 6 * nq;
+    const int per[5][3] = {{1, 3, 2}, {2, 1, 3}, {2, 3, 1}, {3, 1, 2}, {3, 2, 1}};
+    const bool g0 = q0_int[0] == 0 && q0_int[1] == 0 && q0_int[2] == 0;
+    const int s0a = g0 ? 4 : pol[0];
+    std::vector<double> acc((size_t)n, 0.0);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s0 = s0a; s0 <= pol[1]; ++s0) {
+        const double Mq0 = omega0[s0 - 1], n0 = nbe0[s0 - 1];
+        double lw = 0.0;
+        for (int q1 = 0; q1 < nq; ++q1) {
+            for (int t = 0; t < ntet; ++t) {
+                int v2[4], v3[4], typ[4], pos[4];
+                for (int v = 0; v < 4; ++v) {
+                    v2[v] = tetra[4 * t + v] - 1;
+                    const int* e = Allq1q2q3 + 3 * ((size_t)q1 * nq + v2[v]);
+                    typ[v] = e[0];
+                    pos[v] = e[1] - 1;
+                    v3[v] = e[2] - 1;
+                }
+                for (int s1 = pol[2]; s1 <= pol[3]; ++s1) {
+                    const double M1s = omega[(size_t)q1 * n + s1 - 1], nq1 = nbe[(size_t)q1 * n + s1 - 1];
+                    for (int s2 = pol[4]; s2 <= pol[5]; ++s2)
+                        for (int s3 = pol[6]; s3 <= pol[7]; ++s3) {
+                            double F1[4], F2[4], F3[4], M1[4], M2[4], M3[4];
+                            const int before[3] = {s1, s2, s3};
+                            for (int v = 0; v < 4; ++v) {
+                                int after[3];
+                                for (int k = 0; k < 3; ++k) after[k] = typ[v] == 0 ? before[k] : before[per[typ[v] - 1][k] - 1];
+                                const double W = Wq[(size_t)pos[v] * n4 + (((size_t)(s0 - 1) * n + (after[0] - 1)) * n + (after[1] - 1)) * n + (after[2] - 1)];
+                                const double n2 = nbe[(size_t)v2[v] * n + s2 - 1], n3 = nbe[(size_t)v3[v] * n + s3 - 1];
+                                const double w2 = omega[(size_t)v2[v] * n + s2 - 1], w3 = omega[(size_t)v3[v] * n + s3 - 1];
+                                F1[v] = W * (nq1 * n2 * n3 / n0);
+                                M1[v] = (M1s + w2 + w3);
+                                F2[v] = W * ((1.0 + nq1) * n2 * n3 / n0);
+                                M2[v] = (w2 + w3 - M1s);
+                                F3[v] = W * ((1.0 + nq1) * (1.0 + n2) * n3 / n0);
+                                M3[v] = (w3 - M1s - w2);
+                            }
+                            double g, I[4];
+                            int a1[4] = {0, 1, 2, 3}, a2[4] = {0, 1, 2, 3};
+                            const double wts[3] = {OnebySix, 0.5, 0.5};
+                            double* Fs[3] = {F1, F2, F3};
+                            double* Ms[3] = {M1, M2, M3};
+                            for (int ch = 0; ch < 3; ++ch) {
+                                for (int v = 0; v < 4; ++v) { a1[v] = v; a2[v] = v; }
+                                const bool e = find_g_iver(Mq0, &g, I, Ms[ch], Fs[ch], a1, a2, 0);
+                                for (int v = 0; v < 4; ++v) if (std::isnan(I[v])) I[v] = 0.0;
+                                if (std::isnan(g)) g = 0.0;
+                                lw += wts[ch] * g * iver_x_fver(I, Fs[ch], e);
+                            }
+                        }
+                }
+            }
+        }
+        acc[s0 - 1] = lw;
+    }
+    for (int s = 0; s < n; ++s) rate[s] = acc[s];
+}
+
+// Gaussian form of the same rate (a build-side extension: the reference has only the
+// tetrahedron form): sum over every grid (q1, q2) with q3 from the conservation law,
+//   (1/6) F1 d(w0 - M1) + (1/2) F2 d(w0 - M2) + (1/2) F3 d(w0 - M3),
+// with W computed directly for each ordered (q1, q2, q3) (no stored permutation).
+//   W4 [q1][q2][s0][s1][s2][s3] for this q0 (from orc_w4_factored on every ordered pair).
+void orc_lw4_gauss(int ndof, int nq, const int* q0_int, const double* omega0, const double* nbe0, const double* omega,
+                   const double* nbe, const int* q3_of, const double* W4, const int* pol, double sigma, double* rate) {
+    const int n = ndof;
+    const size_t n4 = (size_t)n * n * n * n;
+    const double os = 1.0 / sigma, os2 = os * os;
+    const bool g0 = q0_int[0] == 0 && q0_int[1] == 0 && q0_int[2] == 0;
+    const int s0a = g0 ? 4 : pol[0];
+    for (int s = 0; s < n; ++s) rate[s] = 0.0;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s0 = s0a; s0 <= pol[1]; ++s0) {
+        const double w0 = omega0[s0 - 1], n0 = nbe0[s0 - 1];
+        double lw = 0.0;
+        for (int q1 = 0; q1 < nq; ++q1)
+            for (int q2 = 0; q2 < nq; ++q2) {
+                const int q3 = q3_of[(size_t)q1 * nq + q2];
+                const double* W = W4 + ((size_t)q1 * nq + q2) * n4;
+                for (int s1 = pol[2]; s1 <= pol[3]; ++s1) {
+                    const double w1 = omega[(size_t)q1 * n + s1 - 1], n1 = nbe[(size_t)q1 * n + s1 - 1];
+                    for (int s2 = pol[4]; s2 <= pol[5]; ++s2) {
+                        const double w2 = omega[(size_t)q2 * n + s2 - 1], n2 = nbe[(size_t)q2 * n + s2 - 1];
+                        for (int s3 = pol[6]; s3 <= pol[7]; ++s3) {
+                            const double w3 = omega[(size_t)q3 * n + s3 - 1], n3 = nbe[(size_t)q3 * n + s3 - 1];
+                            const double Wv = W[(((size_t)(s0 - 1) * n + s1 - 1) * n + s2 - 1) * n + s3 - 1];
+                            const double d1 = w0 - (w1 + w2 + w3), d2 = w0 - (w2 + w3 - w1), d3 = w0 - (w3 - w1 - w2);
+                            const double e1 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d1 * d1));
+                            const double e2 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d2 * d2));
+                            const double e3 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d3 * d3));
+                            lw += OnebySix * (Wv * (n1 * n2 * n3 / n0)) * e1 +
+                                  0.5 * (Wv * ((1.0 + n1) * n2 * n3 / n0)) * e2 +
+                                  0.5 * (Wv * ((1.0 + n1) * (1.0 + n2) * n3 / n0)) * e3;
+                        }
+                    }
+                }
+            }
+        rate[s0 - 1] = lw;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Iterative BTE of kappa_iter.x (src/Kappa/Src_iterative):
 //   TetrahedronWplus/Wminus (Quasi_momentum_consrv.f90:701-1208) -> 1/tau,
 //   CreateFzero (HelperSubroutines.f90:118-185), TetrahedronIterPlus/Minus

@@ -41,6 +41,7 @@ SIGNATURES = {
     "spring_set_crystal": [P, P, P],
     "spring_set_fc2": [P, I, P, P, P],
     "spring_set_fc3": [P, I, P, P, P],
+    "spring_set_fc4": [P, I, P, P, P],
     "spring_make_mesh": [P, P, I, P, P, P],
     "spring_find_irr_q": [P, I, P, I, P, P, P, P],
     "spring_compute_phonons": [P, P, D],
@@ -56,6 +57,8 @@ SIGNATURES = {
     "spring_linewidth3": [P, I, I, I, D, P, P, P],
     "spring_linewidth_iso": [P, I, I, I, D, P, P],
     "spring_linewidth3_tetra_noalloc": [P, I, P, P, P],
+    "spring_enumerate4": [P, I, P, P, ct.c_longlong, P],
+    "spring_linewidth4": [P, I, I, I, D, P, P],
     "spring_reset_linewidths": [P],
     "spring_get_linewidths": [P, P],
     "spring_set_linewidths": [P, P],

@@ -126,6 +126,11 @@ class Context:
         self._call("spring_set_fc3", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),
                    _ptr(_c(fc3, np.float64)))
 
+    def set_fc4(self, atm_num, atm_indx, fc4):
+        na = int(np.asarray(atm_indx).shape[1])
+        self._call("spring_set_fc4", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),
+                   _ptr(_c(fc4, np.float64)))
+
     # -- q_tetrahedron
     def make_mesh(self, shift=(0, 0, 0), zero_centered=True, want=True):
         sh = _c(shift, np.int32)
@@ -175,6 +180,16 @@ class Context:
         self._call("spring_enumerate3", int(i0), _ptr(A), _ptr(Pm), _ptr(cnt))
         return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
 
+    # -- MomentumConsrv4th
+    def enumerate4(self, i0: int, cap=None):
+        """Allq1q2q3 [q1][q2][3], q1q2q3_permuted [quartet][3] (1-based) and (count, total_count)."""
+        A = np.zeros((self.nq, self.nq, 3), np.int32)
+        cap = self.nq * self.nq if cap is None else int(cap)
+        Pm = np.zeros((max(cap, 1), 3), np.int32)
+        cnt = np.zeros(2, np.int64)
+        self._call("spring_enumerate4", int(i0), _ptr(A), _ptr(Pm), cap, _ptr(cnt))
+        return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
+
     # -- ScatterProbAllq1
     def scatter_w3(self, i0: int):
         nd = self.ndof
@@ -209,6 +224,18 @@ class Context:
             return None
         rate = np.zeros((self.n_temps, n_q0, self.ndof))
         self._call("spring_linewidth_iso", int(i0_first), int(n_q0), mode, float(sigma), _ptr(g), _ptr(rate))
+        return rate
+
+    def linewidth4(self, i0_first: int, n_q0: int, delta: str = "tetra", sigma: float = 0.3767, pol4=None,
+                   want=True):
+        """Four-phonon scattering rate (nT, n_q0, Ndof); 0.5 x rate joins the resident linewidths."""
+        mode = L.SPRING_DELTA_GAUSS if delta == "gauss" else L.SPRING_DELTA_TETRA
+        pol = None if pol4 is None else _c(pol4, np.int32)
+        if not want:
+            self._call("spring_linewidth4", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), None)
+            return None
+        rate = np.zeros((self.n_temps, n_q0, self.ndof))
+        self._call("spring_linewidth4", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), _ptr(rate))
         return rate
 
     def reset_linewidths(self):
@@ -249,7 +276,7 @@ class Context:
         return dict(kappa=kap, kappa_rta=k0, iters=it)
 
 
-def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True):
+def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True, with_fc4=False):
     """A ready context for a :class:`spring_b200.synthetic.Crystal`.
 
     ``phonons="device"`` computes them with the device eigensolver; a dict
@@ -263,6 +290,8 @@ def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=
     ctx.set_fc2(cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
     if with_fc3:
         ctx.set_fc3(cr.fc3_atm_num, cr.fc3_atm_indx, cr.fc3)
+    if with_fc4:
+        ctx.set_fc4(cr.fc4_atm_num, cr.fc4_atm_indx, cr.fc4)
     qi, qf, tet = ctx.make_mesh()
     if W is None:
         W, Rxyz = S.point_group(cr)

@@ -244,6 +244,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         cudaStreamSynchronize(c->stream);
         clear_profile(c);
         dfree(c->d_mass_rs); dfree(c->d_fc2); dfree(c->d_fc2_idx); dfree(c->d_fc2_num);
+        dfree(c->d_fc4); dfree(c->d_fc4_posr); dfree(c->d_fc4_btyp); dfree(c->d_fc4_off);
         dfree(c->d_fc3); dfree(c->d_fc3_off); dfree(c->d_fc3_posr); dfree(c->d_fc3_btyp);
         dfree(c->d_qint); dfree(c->d_qpnt); dfree(c->d_tetra);
         dfree(c->d_irr_int); dfree(c->d_irr_q); dfree(c->d_mult); dfree(c->d_pos); dfree(c->d_temps);
@@ -449,6 +450,55 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     SPRING_CHECK(spring_synchronize(c));
     c->fc3_set = true;
     dfree(c->d_wtr);  // cached W grids depend on FC3
+    return SPRING_OK;
+}
+
+int spring_set_fc4(spring_ctx* c, int na4, const int* num, const int* idx, const double* fc) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->crystal_set, "crystal"));
+    if (!num || !idx || !fc || na4 < 1 || na4 > 16) return fail(c, SPRING_ERR_ARG, "FC4 arrays are NULL or na4 not in 1..16");
+    const int nb = c->nb;
+    const size_t blk = 81;
+    std::vector<double> t((size_t)nb * na4 * na4 * na4 * blk, 0.0), posr((size_t)nb * na4 * 3, 0.0);
+    std::vector<int> btyp((size_t)nb * na4, 0), off((size_t)nb * (nb + 1), 0);
+    for (int mu = 0; mu < nb; ++mu) {
+        if (num[mu] < 0 || num[mu] > na4) return fail(c, SPRING_ERR_ARG, "FC4 atm_num(%d) out of range", mu + 1);
+        std::vector<int> order;  // slots grouped by basis atom (stable), as for FC3
+        for (int nu = 0; nu < nb; ++nu) {
+            off[(size_t)mu * (nb + 1) + nu] = (int)order.size();
+            for (int n = 0; n < num[mu]; ++n) {
+                const int* e = idx + 4 * (n + (size_t)na4 * mu);
+                if (e[3] < 1 || e[3] > nb) return fail(c, SPRING_ERR_ARG, "FC4 atm_indx basis out of range");
+                if (e[3] - 1 == nu) order.push_back(n);
+            }
+        }
+        off[(size_t)mu * (nb + 1) + nb] = (int)order.size();
+        for (int k = 0; k < num[mu]; ++k) {
+            const int* e = idx + 4 * (order[k] + (size_t)na4 * mu);
+            btyp[(size_t)mu * na4 + k] = e[3] - 1;
+            for (int r = 0; r < 3; ++r)  // atmPosR = latvec * cell (FC4_mod.f90:74-93)
+                posr[((size_t)mu * na4 + k) * 3 + r] =
+                    c->latvec[r] * e[0] + c->latvec[r + 3] * e[1] + c->latvec[r + 6] * e[2];
+        }
+        for (int k1 = 0; k1 < num[mu]; ++k1)
+            for (int k2 = 0; k2 < num[mu]; ++k2)
+                for (int k3 = 0; k3 < num[mu]; ++k3) {
+                    const size_t dst = (((size_t)(mu * na4 + k1) * na4 + k2) * na4 + k3) * blk;
+                    const size_t src = (((size_t)(mu * na4 + order[k1]) * na4 + order[k2]) * na4 + order[k3]) * blk;
+                    for (size_t x = 0; x < blk; ++x) t[dst + x] = fc[src + x];
+                }
+    }
+    c->na4 = na4;
+    SPRING_CHECK(dalloc(c, c->d_fc4, t.size(), "FC4"));
+    SPRING_CHECK(dalloc(c, c->d_fc4_posr, posr.size(), "FC4 positions"));
+    SPRING_CHECK(dalloc(c, c->d_fc4_btyp, btyp.size(), "FC4 basis"));
+    SPRING_CHECK(dalloc(c, c->d_fc4_off, off.size(), "FC4 slot offsets"));
+    SPRING_CHECK(h2d(c, c->d_fc4.p, t.data(), sizeof(double) * t.size(), "FC4"));
+    SPRING_CHECK(h2d(c, c->d_fc4_posr.p, posr.data(), sizeof(double) * posr.size(), "FC4 positions"));
+    SPRING_CHECK(h2d(c, c->d_fc4_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC4 basis"));
+    SPRING_CHECK(h2d(c, c->d_fc4_off.p, off.data(), sizeof(int) * off.size(), "FC4 slot offsets"));
+    SPRING_CHECK(spring_synchronize(c));
+    c->fc4_set = true;
     return SPRING_OK;
 }
 
@@ -706,6 +756,53 @@ int spring_linewidth_iso(spring_ctx* c, int i0_first, int n_q0, int delta_mode, 
     SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
     SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
     SPRING_CHECK(run_iso(c, q0, n_q0, delta_mode, sigma, g2, c->d_lw_tmp.p));
+    SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
+    SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
+    return SPRING_OK;
+}
+
+int spring_enumerate4(spring_ctx* c, int i0, int* allq1q2q3, int* perm, long long cap, long long* counts) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0, 1));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    if (perm && cap < 0) return fail(c, SPRING_ERR_ARG, "cap must be >= 0");
+    const size_t cells = (size_t)c->nq * c->nq;
+    DBuf<int> a, p;
+    long long hc[2] = {0, 0};
+    int rc = SPRING_OK;
+    if (allq1q2q3) rc = dalloc(c, a, cells * 3, "Allq1q2q3");
+    if (rc == SPRING_OK && perm) rc = dalloc(c, p, (size_t)std::max<long long>(cap, 1) * 3, "q1q2q3_permuted");
+    if (rc == SPRING_OK) rc = run_enumerate4_fortran(c, i0 - 1, a.p, p.p, cap, hc);
+    if (rc == SPRING_OK && perm && hc[0] > cap)
+        rc = fail(c, SPRING_ERR_ARG, "%lld quartets exceed cap = %lld", hc[0], cap);
+    if (rc == SPRING_OK && allq1q2q3) rc = d2h(c, allq1q2q3, a.p, sizeof(int) * 3 * cells, "Allq1q2q3");
+    if (rc == SPRING_OK && perm) rc = d2h(c, perm, p.p, sizeof(int) * 3 * (size_t)hc[0], "q1q2q3_permuted");
+    if (rc == SPRING_OK && counts) { counts[0] = hc[0]; counts[1] = hc[1]; }
+    dfree(a); dfree(p);
+    return rc;
+}
+
+int spring_linewidth4(spring_ctx* c, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol4,
+                      double* rate) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0_first, n_q0));
+    SPRING_CHECK(need(c, c->fc4_set, "FC4"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    SPRING_CHECK(need(c, c->ph_irr.set, "irreducible-point phonons"));
+    if (delta_mode != SPRING_DELTA_GAUSS && delta_mode != SPRING_DELTA_TETRA)
+        return fail(c, SPRING_ERR_ARG, "delta_mode must be SPRING_DELTA_GAUSS or SPRING_DELTA_TETRA");
+    if (delta_mode == SPRING_DELTA_GAUSS && !(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    if (pol4)
+        for (int k = 0; k < 4; ++k)
+            if (pol4[2 * k] < 1 || pol4[2 * k + 1] > c->ndof || pol4[2 * k] > pol4[2 * k + 1])
+                return fail(c, SPRING_ERR_ARG, "pol4 column %d outside 1..Ndof", k + 1);
+    if (n_q0 == 0) return SPRING_OK;
+    const int q0 = i0_first - 1;
+    const size_t nl = (size_t)c->nT * c->nq0 * c->ndof;
+    SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
+    SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
+    SPRING_CHECK(run_lw4(c, q0, n_q0, delta_mode, sigma, pol4, c->d_lw_tmp.p));
     SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
     SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
     return SPRING_OK;

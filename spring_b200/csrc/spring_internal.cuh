@@ -114,6 +114,14 @@ struct spring_ctx {
     spring::DBuf<int> d_fc3_btyp;     // [mu][N] 0-based basis index
     spring::DBuf<int> d_fc3_off;      // [mu][nb+1] first slot of each basis atom (slots grouped by basis)
 
+    // FC4: [mu][N1][N2][N3][a][b][c][d] (Fortran memory order), slots grouped by basis like FC3
+    bool fc4_set = false;
+    int na4 = 0;
+    spring::DBuf<double> d_fc4;
+    spring::DBuf<double> d_fc4_posr;  // [mu][N][3]
+    spring::DBuf<int> d_fc4_btyp;     // [mu][N]
+    spring::DBuf<int> d_fc4_off;      // [mu][nb+1]
+
     // mesh
     bool mesh_set = false;
     spring::DBuf<int> d_qint;      // [q][3]
@@ -210,6 +218,9 @@ int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first
 // k_v3s.cu: specialised V3 for two-atom cells; *handled is false when the cell does not fit it
 int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
                const Pol* pol, double* lw, double* p3, double* w, bool* handled);
+// k_4ph.cu
+int run_enumerate4_fortran(spring_ctx* c, int q0, int* d_all, int* d_perm, long long cap, long long* h_counts);
+int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const int* pol4, double* d_rate);
 // k_bte.cu
 int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters);
 // k_tetra.cu
