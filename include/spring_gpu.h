@@ -192,6 +192,29 @@ int spring_enumerate4(spring_ctx* ctx, int i0, int* Allq1q2q3, int* q1q2q3_permu
 int spring_linewidth4(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol4,
                       double* rate);
 
+/* ---- LineWidth.x path mode ------------------------------------------- */
+/* q_points_highsymm, src/LineWidth/Src/CreateMesh_mod.f90:85-172: path points
+ * from q_high_sym(4,n_nodes) (fractional node, points on the segment ending at
+ * it).  *n_rows = points written (the reference allocates sum(q_high_sym(4,:))
+ * rows and fills this many); qpoints(3,*) Cartesian, dist(*) and
+ * zero_centered(*) (1 when the segment uses the zero-centred q1 mesh) may be
+ * NULL (then only *n_rows is returned). */
+int spring_path_qpoints(spring_ctx* ctx, int n_nodes, const double* q_high_sym, int* n_rows, double* qpoints,
+                        double* dist, int* zero_centered);
+
+/* Linewidth at off-grid q0 points, the q0 loop of src/LineWidth/Src/main.f90:297-389:
+ * ScatterProbAllq1 (Linewidth_m.f90:48-231: q2 = G - q0 - q1 found inside the
+ * zone in fractional coordinates, phonons of every q2 on the device) and
+ *   SPRING_DELTA_TETRA: CalculateLwTetrahedron (Linewidth_m.f90:326-417), or
+ *   SPRING_DELTA_GAUSS: CalculateLinewidth (:234-323, branch start reset per q1).
+ * q0(3,n_q0) Cartesian, zero_centered(n_q0) from spring_path_qpoints.  Needs
+ * FC2, FC3, a zero-centred mesh and its grid phonons; non-zero-centred segments
+ * take their q1 vectors from the [0, N) mesh and the phonons of the same grid
+ * points.  lw(Ndof,n_q0,n_temps) and omega_q0(Ndof,n_q0) are optional outputs;
+ * the resident LW_Allq0 is not touched. */
+int spring_linewidth_path(spring_ctx* ctx, int n_q0, const double* q0, const int* zero_centered, int delta_mode,
+                          double sigma, double* lw, double* omega_q0);
+
 /* Zero / read / replace the resident LW_Allq0(Ndof,Nq0,n_temps). */
 int spring_reset_linewidths(spring_ctx* ctx);
 int spring_get_linewidths(spring_ctx* ctx, double* lw_all);

@@ -466,3 +466,109 @@ def lw4_gauss(st, i0, it=0, sigma=0.3767, pol=None):
     _l4().orc_lw4_gauss(nd, st.nq, _i(st.irr_int[i0]), _f(st.ph0["omega"][i0]), _f(st.ph0["nbe"][it][i0]),
                         _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _i(q3), _f(W4), _i(pol), float(sigma), rate)
     return rate
+
+
+# ----------------------------------------------------------------------------- LineWidth.x path mode
+def path_points(G, q_high_sym):
+    """q_points_highsymm (src/LineWidth/Src/CreateMesh_mod.f90:85-172): (qpoints, dist, zero_centered)."""
+    qhs = np.asarray(q_high_sym, np.float64)  # (n_nodes, 4)
+    G = np.asarray(G, np.float64)
+    qs, ds, zs = [], [], []
+    sd = dist = 0.0
+    for nd in range(len(qhs) - 1):
+        a, b = qhs[nd, :3], qhs[nd + 1, :3]
+        npt = int(qhs[nd + 1, 3])
+        zc = bool(np.any(a < 0.0) or np.any(b < 0.0) or np.all(np.abs(a) <= 0.5) or np.all(np.abs(b) <= 0.5))
+        s = np.array([G[r, 0] * a[0] + G[r, 1] * a[1] + G[r, 2] * a[2] for r in range(3)])
+        e = np.array([G[r, 0] * b[0] + G[r, 1] * b[1] + G[r, 2] * b[2] for r in range(3)])
+        d = e - s
+        vlen = np.sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2])
+        vh = d / vlen
+        step = vlen / npt if npt != 0 else 0.0
+        for ii in range(1, npt + 1):
+            dist = sd + ii * step
+            qs.append(s + (ii * step) * vh)
+            ds.append(dist)
+            zs.append(zc)
+        sd = dist
+    return np.array(qs).reshape(-1, 3), np.array(ds), np.array(zs, bool)
+
+
+def _lpath():
+    L = lib()
+    if not hasattr(L, "_path_set"):
+        L.orc_w3_path.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, f64p, f64p, ct.c_int, ct.c_int, f64p, f64p,
+                                  i32p, c128p, f64p, c128p, f64p, c128p, f64p, f64p]
+        L.orc_w3_path.restype = None
+        L.orc_lw_path_tetra.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, f64p, f64p, f64p, i32p, f64p]
+        L.orc_lw_path_tetra.restype = None
+        L.orc_lw_path_gauss.argtypes = [ct.c_int, ct.c_int, f64p, f64p, f64p, f64p, f64p, f64p, i32p, i32p,
+                                        ct.c_double, f64p]
+        L.orc_lw_path_gauss.restype = None
+        L._path_set = True
+    return L
+
+
+def find_q2(G, q0, q1s, zero_centered):
+    """q2 = G - (q0 + q1) for the first G of (0,1,-1,2,-2)^3 (first component fastest) inside the zone,
+    tested in fractional coordinates from LAPACK's LU solve (ScatterProbAllq1 / CheckIfWithinBZ,
+    Linewidth_m.f90:115-185, 458-497).  Returns (q2 (n, 3), exists (n,))."""
+    import scipy.linalg as sl
+    G = np.asarray(G, np.float64)
+    lu = sl.lu_factor(G)
+    sgn = [0, 1, -1, 2, -2]
+    n = len(q1s)
+    q2 = np.zeros((n, 3))
+    found = np.zeros(n, bool)
+    base = np.asarray(q0)[None, :] + np.asarray(q1s)
+    for c3 in sgn:
+        for c2 in sgn:
+            for c1 in sgn:
+                idx = np.array([c1, c2, c3], np.float64)
+                gv = np.array([G[r, 0] * idx[0] + G[r, 1] * idx[1] + G[r, 2] * idx[2] for r in range(3)])
+                t = gv[None, :] - base
+                x = sl.lu_solve(lu, t.T).T
+                if zero_centered:
+                    inside = np.all(np.abs(x) <= 0.5, axis=1)
+                else:
+                    inside = np.all(x >= 0.0, axis=1) & np.all(x <= 1.0, axis=1)
+                take = inside & ~found
+                q2[take] = t[take]
+                found |= take
+    return q2, found
+
+
+def linewidth_path(st: Setup, q0, zero_centered, delta="tetra", sigma=0.3767, it=0, q0_phonons=None):
+    """LineWidth.x linewidth at one off-grid q0 (Cartesian), one temperature: ScatterProbAllq1 +
+    CalculateLwTetrahedron / CalculateLinewidth.  The q1 mesh is the setup's grid; non-zero-centred
+    segments use the [0, N) vectors of the same grid points and their phonons."""
+    cr = st.cr
+    nd = cr.ndof
+    args = (cr.latvec, cr.mass, cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2)
+    ph0 = q0_phonons if q0_phonons is not None else P.get_phonon(*args, np.asarray(q0)[None, :], st.temps)
+    if zero_centered:
+        q1s = st.q_pnt
+    else:
+        _, q1s, _ = make_tetrahedron(st.mesh, st.cr.G, zero_centered=False)
+    q2, ex = find_q2(st.cr.G, q0, q1s, zero_centered)
+    ph2 = P.get_phonon(*args, q2, st.temps)
+    ph2["omega"][~ex] = 0.0
+    ph2["nbe"][:, ~ex] = 0.0
+    q0chk = np.stack([np.full(st.nq, np.all(np.abs(q0) < C.zero_prec)),
+                      np.all(st.q_pnt_int == 0, axis=1),
+                      np.all(np.abs(q2) < C.zero_prec, axis=1)], axis=1).astype(np.int32)
+    btyp, posr = fc3_derived(cr)
+    W = np.zeros((st.nq, nd, nd, nd))
+    _lpath().orc_w3_path(cr.nbasis, cr.fc3.shape[1], _i(cr.fc3_atm_num), btyp, posr, _f(cr.fc3), _f(cr.mass),
+                         st.nq, st.nq, _f(q1s), _f(q2), _i(q0chk), _c(ph0["evec"][0]), _f(ph0["omega"][0]),
+                         _c(st.ph["evec"]), _f(st.ph["omega"]), _c(ph2["evec"]), _f(ph2["omega"]), W)
+    W[~ex] = 0.0
+    lw = np.zeros(nd)
+    if delta == "tetra":
+        _lpath().orc_lw_path_tetra(nd, st.nq, _f(ph0["omega"][0]), _f(st.ph["omega"]), _f(st.ph["nbe"][it]),
+                                   _f(ph2["omega"]), _f(ph2["nbe"][it]), _f(W), _i(st.tetra), lw)
+    else:
+        _lpath().orc_lw_path_gauss(nd, st.nq, _f(ph0["omega"][0]), _f(st.ph["omega"]), _f(st.ph["nbe"][it]),
+                                   _f(ph2["omega"]), _f(ph2["nbe"][it]), _f(W), _i(ex.astype(np.int32)),
+                                   _i(st.q_pnt_int), float(sigma), lw)
+    return lw, dict(omega0=ph0["omega"][0], q2=q2, exists=ex, W=W)

@@ -1189,4 +1189,166 @@ int orc_num_threads() {
 #endif
 }
 
+
+// ---------------------------------------------------------------------------
+// LineWidth.x path mode (src/LineWidth/Src/Linewidth_m.f90).
+// ScatterMatEl (:500-591) + ScatterProbability (:594-657) for explicit
+// (q1, q2) vectors: the 9-deep loop in the reference order, then
+// W(s2,s1,s) = |Phi|^2 / (w0 w1 w2 Nq) * Sctr3THz2, zero below mode 4 where
+// q0chk(k) is set.  q1v, q2v (n, 3); q0chk (n, 3) 0/1; e0 (Ndof x Ndof,
+// Evec(row,s)); e1, e2 (n, Ndof x Ndof); w0 (Ndof); w1, w2 (n, Ndof);
+// out W [pair][s0][s1][s2].
+void orc_w3_path(int nb, int na3, const int* atm_num, const int* basis_typ, const double* atm_pos_r, const double* fc3,
+                 const double* mass, int nq, int npairs, const double* q1v, const double* q2v, const int* q0chk,
+                 const double* e0_ri, const double* w0, const double* e1_ri, const double* w1, const double* e2_ri,
+                 const double* w2, double* Wout) {
+    const int ndof = 3 * nb;
+    const size_t n2 = (size_t)ndof * ndof, n3 = n2 * ndof;
+    const cplx* evec0 = reinterpret_cast<const cplx*>(e0_ri);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int ip = 0; ip < npairs; ++ip) {
+        const double* q1 = q1v + 3 * ip;
+        const double* q2 = q2v + 3 * ip;
+        const cplx* e1 = reinterpret_cast<const cplx*>(e1_ri) + ip * n2;
+        const cplx* e2 = reinterpret_cast<const cplx*>(e2_ri) + ip * n2;
+        int strt[3];
+        for (int k = 0; k < 3; ++k) strt[k] = q0chk[3 * ip + k] ? 4 : 1;
+        std::vector<cplx> phi(n3, cplx(0.0, 0.0));  // Phi_ss1s2(s2,s1,s)
+        for (int mu = 1; mu <= nb; ++mu) {
+            const int natm = atm_num[mu - 1];
+            for (int N1 = 1; N1 <= natm; ++N1) {
+                const int nu = basis_typ[(N1 - 1) + na3 * (mu - 1)];
+                const double* R1 = atm_pos_r + 3 * ((N1 - 1) + na3 * (mu - 1));
+                const double qr1 = q1[0] * R1[0] + q1[1] * R1[1] + q1[2] * R1[2];
+                const cplx ex1(std::cos(qr1), std::sin(qr1));
+                for (int N2 = 1; N2 <= natm; ++N2) {
+                    const int eta = basis_typ[(N2 - 1) + na3 * (mu - 1)];
+                    const double* R2 = atm_pos_r + 3 * ((N2 - 1) + na3 * (mu - 1));
+                    const double qr2 = q2[0] * R2[0] + q2[1] * R2[1] + q2[2] * R2[2];
+                    const cplx ex2(std::cos(qr2), std::sin(qr2));
+                    const double mass_fac = 1.0 / std::sqrt(mass[mu - 1] * mass[nu - 1] * mass[eta - 1]);
+                    const cplx exm = ex1 * ex2 * mass_fac;
+                    for (int al = 1; al <= 3; ++al) {
+                        const int r0 = 3 * (mu - 1) + al;
+                        for (int s = strt[0]; s <= ndof; ++s) {
+                            const cplx ww0 = evec0[(r0 - 1) + ndof * (s - 1)];
+                            for (int be = 1; be <= 3; ++be) {
+                                const int r1 = 3 * (nu - 1) + be;
+                                for (int s1 = strt[1]; s1 <= ndof; ++s1) {
+                                    const cplx ww1 = e1[(r1 - 1) + ndof * (s1 - 1)];
+                                    for (int ga = 1; ga <= 3; ++ga) {
+                                        const int r2 = 3 * (eta - 1) + ga;
+                                        const size_t fi = (size_t)(ga - 1) + 3 * ((be - 1) + 3 * ((al - 1) +
+                                                          3 * ((N2 - 1) + (size_t)na3 * ((N1 - 1) + (size_t)na3 * (mu - 1)))));
+                                        const cplx pm = fc3[fi] * exm;
+                                        for (int s2 = strt[2]; s2 <= ndof; ++s2) {
+                                            const cplx ww2 = e2[(r2 - 1) + ndof * (s2 - 1)];
+                                            phi[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s - 1))] += pm * ww0 * ww1 * ww2;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        double* W = Wout + (size_t)ip * n3;
+        std::memset(W, 0, sizeof(double) * n3);
+        const double* o1 = w1 + (size_t)ip * ndof;
+        const double* o2 = w2 + (size_t)ip * ndof;
+        for (int s = strt[0]; s <= ndof; ++s)
+            for (int s1 = strt[1]; s1 <= ndof; ++s1)
+                for (int s2 = strt[2]; s2 <= ndof; ++s2) {
+                    const cplx p = phi[(s2 - 1) + ndof * ((s1 - 1) + (size_t)ndof * (s - 1))];
+                    const double abs2 = p.real() * p.real() + p.imag() * p.imag();
+                    const double el = abs2 / (w0[s - 1] * o1[s1 - 1] * o2[s2 - 1] * double(nq));
+                    W[((size_t)(s - 1) * ndof + (s1 - 1)) * ndof + (s2 - 1)] = el * Sctr3THz2;
+                }
+    }
+}
+
+// CalculateLwTetrahedron of LineWidth.x (Linewidth_m.f90:326-417) with
+// FindFandOmegaAtVertices (src/LineWidth/Src/TetrahedronIntegration_m.f90:257-293):
+// the q2 phonons of vertex q1 come from its own table; strict case bounds.
+//   omega0 (Ndof); omega1/nbe1 grid [q][s]; omega2/nbe2 [q1][s]; W [q1][s0][s1][s2];
+//   tetra (6Nq, 4) 1-based; out lw (Ndof).
+void orc_lw_path_tetra(int ndof, int nq, const double* omega0, const double* omega1, const double* nbe1,
+                       const double* omega2, const double* nbe2, const double* W, const int* tetra, double* lw) {
+    const int n = ndof;
+    const size_t n3 = (size_t)n * n * n;
+    const int ntet = 6 * nq;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s0 = 1; s0 <= n; ++s0) {
+        const double Mq0s = omega0[s0 - 1];
+        double acc = 0.0;
+        for (int t = 0; t < ntet; ++t) {
+            int tv[4];
+            for (int v = 0; v < 4; ++v) tv[v] = tetra[4 * t + v] - 1;
+            for (int s1 = 1; s1 <= n; ++s1)
+                for (int s2 = 1; s2 <= n; ++s2) {
+                    double F1[4], F2[4], F3[4], M1[4], M2[4], M3[4];
+                    for (int v = 0; v < 4; ++v) {
+                        const int q = tv[v];
+                        const double Wv = W[(size_t)q * n3 + ((size_t)(s0 - 1) * n + (s1 - 1)) * n + (s2 - 1)];
+                        const double n1 = nbe1[(size_t)q * n + s1 - 1], n2 = nbe2[(size_t)q * n + s2 - 1];
+                        const double o1 = omega1[(size_t)q * n + s1 - 1], o2 = omega2[(size_t)q * n + s2 - 1];
+                        F1[v] = Wv * (n1 + n2 + 1.0);
+                        F2[v] = Wv * (n1 - n2);
+                        M1[v] = o1 + o2;
+                        M2[v] = o2 - o1;
+                        M3[v] = o1 - o2;
+                    }
+                    for (int v = 0; v < 4; ++v) F3[v] = F2[v];
+                    double g, I[4];
+                    int a1[4], a2[4];
+                    for (int v = 0; v < 4; ++v) { a1[v] = v; a2[v] = v; }
+                    bool e = find_g_iver(Mq0s, &g, I, M1, F1, a1, a2, 1);
+                    acc += g * iver_x_fver(I, F1, e);
+                    for (int v = 0; v < 4; ++v) { a1[v] = v; a2[v] = v; }
+                    e = find_g_iver(Mq0s, &g, I, M2, F2, a1, a2, 1);
+                    acc += g * iver_x_fver(I, F2, e);
+                    for (int v = 0; v < 4; ++v) { a1[v] = v; a2[v] = v; }
+                    e = find_g_iver(Mq0s, &g, I, M3, F3, a1, a2, 1);
+                    acc -= g * iver_x_fver(I, F3, e);
+                }
+        }
+        lw[s0 - 1] = acc;
+    }
+}
+
+// CalculateLinewidth of LineWidth.x (Linewidth_m.f90:234-323) with the branch
+// start reset for every q1 (the reference keeps strt(2)/strt(3) at 4 once set).
+//   exists [q1]; q_pnt_int (Nq, 3); the rest as orc_lw_path_tetra.
+void orc_lw_path_gauss(int ndof, int nq, const double* omega0, const double* omega1, const double* nbe1,
+                       const double* omega2, const double* nbe2, const double* W, const int* exists,
+                       const int* q_pnt_int, double sigma, double* lw) {
+    const int n = ndof;
+    const size_t n3 = (size_t)n * n * n;
+    const double os = 1.0 / sigma, os2 = os * os;
+    for (int s = 0; s < n; ++s) lw[s] = 0.0;
+    for (int q1 = 0; q1 < nq; ++q1) {
+        if (!exists[q1]) continue;
+        const int* qi = q_pnt_int + 3 * q1;
+        const int st1 = (qi[0] == 0 && qi[1] == 0 && qi[2] == 0) ? 4 : 1;
+        const double* o2 = omega2 + (size_t)q1 * n;
+        const int st2 = (std::fabs(o2[0]) < zero_prec && std::fabs(o2[1]) < zero_prec && std::fabs(o2[2]) < zero_prec) ? 4 : 1;
+        for (int s0 = 1; s0 <= n; ++s0) {
+            double t = 0.0;
+            for (int s1 = st1; s1 <= n; ++s1)
+                for (int s2 = st2; s2 <= n; ++s2) {
+                    const double w1 = omega1[(size_t)q1 * n + s1 - 1], w2 = o2[s2 - 1];
+                    const double n1 = nbe1[(size_t)q1 * n + s1 - 1], n2 = nbe2[(size_t)q1 * n + s2 - 1];
+                    const double d1 = omega0[s0 - 1] - w1 - w2, d2 = omega0[s0 - 1] + w1 - w2, d3 = omega0[s0 - 1] - w1 + w2;
+                    const double e1 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d1 * d1));
+                    const double e2 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d2 * d2));
+                    const double e3 = os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d3 * d3));
+                    t += W[(size_t)q1 * n3 + ((size_t)(s0 - 1) * n + (s1 - 1)) * n + (s2 - 1)] *
+                         (((n1 + n2 + 1.0) * e1) + ((n1 - n2) * (e2 - e3)));
+                }
+            lw[s0 - 1] += t;
+        }
+    }
+}
+
 }  // extern "C"

@@ -238,6 +238,29 @@ class Context:
         self._call("spring_linewidth4", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), _ptr(rate))
         return rate
 
+    # -- LineWidth.x path mode
+    def path_qpoints(self, q_high_sym):
+        """q_points_highsymm: (qpoints (n, 3) Cartesian, dist (n,), zero_centered (n,) bool)."""
+        qhs = _c(q_high_sym, np.float64)  # (n_nodes, 4): fractional node, point count
+        n_rows = ct.c_int()
+        self._call("spring_path_qpoints", int(qhs.shape[0]), _ptr(qhs), ct.byref(n_rows), None, None, None)
+        n = int(n_rows.value)
+        q = np.zeros((max(n, 1), 3))
+        d = np.zeros(max(n, 1))
+        z = np.zeros(max(n, 1), np.int32)
+        self._call("spring_path_qpoints", int(qhs.shape[0]), _ptr(qhs), ct.byref(n_rows), _ptr(q), _ptr(d), _ptr(z))
+        return q[:n], d[:n], z[:n].astype(bool)
+
+    def linewidth_path(self, q0, zero_centered, delta: str = "tetra", sigma: float = 0.3767):
+        """Linewidths (nT, n_q0, Ndof) and frequencies (n_q0, Ndof) at off-grid q0 points."""
+        q = _c(q0, np.float64).reshape(-1, 3)
+        z = _c(zero_centered, np.int32)
+        mode = L.SPRING_DELTA_GAUSS if delta == "gauss" else L.SPRING_DELTA_TETRA
+        lw = np.zeros((self.n_temps, q.shape[0], self.ndof))
+        om = np.zeros((q.shape[0], self.ndof))
+        self._call("spring_linewidth_path", int(q.shape[0]), _ptr(q), _ptr(z), mode, float(sigma), _ptr(lw), _ptr(om))
+        return lw, om
+
     def reset_linewidths(self):
         self._call("spring_reset_linewidths")
 

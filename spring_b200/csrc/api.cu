@@ -106,6 +106,22 @@ int launch_check(spring_ctx* c, const char* what) {
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
 }
 
+void free_phonons(Phonons& p) {
+    dfree(p.evec); dfree(p.omega); dfree(p.oneby); dfree(p.nbe); dfree(p.vel);
+    p.set = false;
+}
+
+int alloc_phonons(spring_ctx* c, Phonons& p, int n) {
+    p.n = n;
+    const size_t nd = c->ndof;
+    SPRING_CHECK(dalloc(c, p.evec, (size_t)n * nd * nd, "phonon eigenvectors"));
+    SPRING_CHECK(dalloc(c, p.omega, (size_t)n * nd, "phonon omega"));
+    SPRING_CHECK(dalloc(c, p.oneby, (size_t)n * nd, "phonon 1/omega"));
+    SPRING_CHECK(dalloc(c, p.nbe, (size_t)c->nT * n * nd, "phonon nBE"));
+    SPRING_CHECK(dalloc(c, p.vel, (size_t)n * nd * 3, "phonon velocity"));
+    return SPRING_OK;
+}
+
 void clear_profile(spring_ctx* c) {
     for (auto& r : c->prof) {
         cudaEventDestroy(r.start);
@@ -140,22 +156,6 @@ struct DeviceGuard {
 
 int need(spring_ctx* c, bool ok, const char* what) {
     return ok ? SPRING_OK : fail(c, SPRING_ERR_STATE, "%s has not been set", what);
-}
-
-void free_phonons(Phonons& p) {
-    dfree(p.evec); dfree(p.omega); dfree(p.oneby); dfree(p.nbe); dfree(p.vel);
-    p.set = false;
-}
-
-int alloc_phonons(spring_ctx* c, Phonons& p, int n) {
-    p.n = n;
-    const size_t nd = c->ndof;
-    SPRING_CHECK(dalloc(c, p.evec, (size_t)n * nd * nd, "phonon eigenvectors"));
-    SPRING_CHECK(dalloc(c, p.omega, (size_t)n * nd, "phonon omega"));
-    SPRING_CHECK(dalloc(c, p.oneby, (size_t)n * nd, "phonon 1/omega"));
-    SPRING_CHECK(dalloc(c, p.nbe, (size_t)c->nT * n * nd, "phonon nBE"));
-    SPRING_CHECK(dalloc(c, p.vel, (size_t)n * nd * 3, "phonon velocity"));
-    return SPRING_OK;
 }
 
 int set_temps(spring_ctx* c, const double* temps) {
@@ -522,6 +522,8 @@ int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_
     }
     SPRING_CHECK(spring_synchronize(c));
     c->mesh_set = true;
+    c->mesh_zc = zero_centered != 0;
+    for (int k = 0; k < 3; ++k) c->mesh_shift[k] = sh[k];
     c->ps_irr.done = false;
     c->ps_tr.done = false;
     c->ntr = 0;
@@ -805,6 +807,37 @@ int spring_linewidth4(spring_ctx* c, int i0_first, int n_q0, int delta_mode, dou
     SPRING_CHECK(run_lw4(c, q0, n_q0, delta_mode, sigma, pol4, c->d_lw_tmp.p));
     SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
     SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
+    return SPRING_OK;
+}
+
+int spring_path_qpoints(spring_ctx* c, int n_nodes, const double* q_high_sym, int* n_rows, double* qpoints,
+                        double* dist, int* zero_centered) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->crystal_set, "crystal"));
+    if (n_nodes < 1 || !q_high_sym || !n_rows) return fail(c, SPRING_ERR_ARG, "n_nodes < 1 or NULL q_high_sym / n_rows");
+    for (int k = 0; k < n_nodes; ++k)
+        if (!(q_high_sym[4 * k + 3] >= 0.0)) return fail(c, SPRING_ERR_ARG, "negative point count at node %d", k + 1);
+    *n_rows = path_points(c->G, n_nodes, q_high_sym, qpoints, dist, zero_centered);
+    return SPRING_OK;
+}
+
+int spring_linewidth_path(spring_ctx* c, int n_q0, const double* q0, const int* zero_centered, int delta_mode,
+                          double sigma, double* lw, double* omega_q0) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->fc2_set, "FC2"));
+    SPRING_CHECK(need(c, c->fc3_set, "FC3"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    if (!c->mesh_zc) return fail(c, SPRING_ERR_STATE, "the path mode needs the zero-centred mesh (spring_make_mesh zero_centered = 1)");
+    if (n_q0 < 0 || (n_q0 > 0 && (!q0 || !zero_centered))) return fail(c, SPRING_ERR_ARG, "n_q0 < 0 or NULL q0 / flags");
+    if (delta_mode != SPRING_DELTA_GAUSS && delta_mode != SPRING_DELTA_TETRA)
+        return fail(c, SPRING_ERR_ARG, "delta_mode must be SPRING_DELTA_GAUSS or SPRING_DELTA_TETRA");
+    if (delta_mode == SPRING_DELTA_GAUSS && !(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    if (c->nT > 9) return fail(c, SPRING_ERR_UNSUPPORTED, "the path mode handles at most 9 temperatures per call");
+    if (n_q0 == 0) return SPRING_OK;
+    std::vector<double> buf(lw ? (size_t)c->nT * n_q0 * c->ndof : 0);
+    SPRING_CHECK(run_path(c, n_q0, q0, zero_centered, delta_mode, sigma, lw ? buf.data() : nullptr, omega_q0));
+    if (lw) std::memcpy(lw, buf.data(), sizeof(double) * buf.size());  // [T][p][s] is lw(Ndof, n_q0, n_temps)
     return SPRING_OK;
 }
 

@@ -25,6 +25,7 @@
 #include <cub/cub.cuh>
 
 #include "spring_internal.cuh"
+#include "tetra.cuh"
 
 namespace spring {
 namespace {
@@ -385,49 +386,6 @@ k_v4(V4Args a, const int4* __restrict__ quart, const double* __restrict__ fc4, c
 }
 
 // ------------------------------------------------------------------------- tetrahedron
-__device__ __forceinline__ void sort4s(const double* M, int* p) {
-    p[0] = 0; p[1] = 1; p[2] = 2; p[3] = 3;
-#define SWP(i, j)                                                                           \
-    {                                                                                       \
-        const double a_ = M[p[i]], b_ = M[p[j]];                                            \
-        if (b_ < a_ || (b_ == a_ && p[j] < p[i])) { int t_ = p[i]; p[i] = p[j]; p[j] = t_; } \
-    }
-    SWP(0, 1) SWP(2, 3) SWP(0, 2) SWP(1, 3) SWP(1, 2)
-#undef SWP
-}
-
-__device__ __forceinline__ bool g_iver_k(double Mqs, const double* M, double& g, double* I) {
-    if ((Mqs >= M[0]) && (Mqs < M[1])) {
-        g = (3.0 * ((Mqs - M[0]) * (Mqs - M[0]))) / ((M[1] - M[0]) * (M[2] - M[0]) * (M[3] - M[0]));
-        I[0] = (((Mqs - M[1]) / (M[0] - M[1])) + ((Mqs - M[2]) / (M[0] - M[2])) + ((Mqs - M[3]) / (M[0] - M[3]))) / 3.0;
-        for (int v = 1; v < 4; ++v) I[v] = ((Mqs - M[0]) / (M[v] - M[0])) / 3.0;
-        return true;
-    }
-    if ((Mqs >= M[1]) && (Mqs < M[2])) {
-        g = (3.0 / ((M[1] - M[2]) * (M[3] - M[0]))) *
-            ((((Mqs - M[0]) * (Mqs - M[2])) / (M[2] - M[0])) - (((Mqs - M[1]) * (Mqs - M[3])) / (M[1] - M[3])));
-        const double den = g * (M[3] - M[0]);
-        I[0] = (((Mqs - M[3]) / (M[0] - M[3])) / 3.0) +
-               ((((Mqs - M[2]) / (M[0] - M[2])) * ((Mqs - M[0]) / (M[2] - M[0])) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        const double t1 = (Mqs - M[3]) / (M[1] - M[3]);
-        I[1] = (((Mqs - M[2]) / (M[1] - M[2])) / 3.0) + (((t1 * t1) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        const double t2 = (Mqs - M[0]) / (M[2] - M[0]);
-        I[2] = (((Mqs - M[1]) / (M[2] - M[1])) / 3.0) + (((t2 * t2) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) / 3.0) +
-               ((((Mqs - M[1]) / (M[3] - M[1])) * ((Mqs - M[3]) / (M[1] - M[3])) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        return true;
-    }
-    if ((Mqs >= M[2]) && (Mqs <= M[3])) {
-        g = (3.0 * ((Mqs - M[3]) * (Mqs - M[3]))) / ((M[3] - M[0]) * (M[3] - M[1]) * (M[3] - M[2]));
-        for (int v = 0; v < 3; ++v) I[v] = ((Mqs - M[3]) / (M[v] - M[3])) / 3.0;
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) + ((Mqs - M[1]) / (M[3] - M[1])) + ((Mqs - M[2]) / (M[3] - M[2]))) / 3.0;
-        return true;
-    }
-    g = 0.0;
-    I[0] = I[1] = I[2] = I[3] = 0.0;
-    return false;
-}
-
 struct T4Args {
     int nq, nT, nq0, q0, ntet, nquart;
     int pol_lo[4], pol_hi[4];
@@ -485,7 +443,7 @@ __global__ void __launch_bounds__(128) k_tetra4(T4Args a, const int4* __restrict
         double Sm[3][4];
 #pragma unroll
         for (int ch = 0; ch < 3; ++ch) {
-            sort4s(M[ch], pm[ch]);
+            tet::sort4(M[ch], pm[ch]);
 #pragma unroll
             for (int v = 0; v < 4; ++v) Sm[ch][v] = M[ch][pm[ch][v]];
         }
@@ -505,7 +463,7 @@ __global__ void __launch_bounds__(128) k_tetra4(T4Args a, const int4* __restrict
 #pragma unroll
             for (int ch = 0; ch < 3; ++ch) {
                 double g, I[4];
-                const bool e = g_iver_k(Mqs, Sm[ch], g, I);
+                const bool e = tet::g_iver<false>(Mqs, Sm[ch], g, I);
 #pragma unroll
                 for (int v = 0; v < 4; ++v) if (isnan(I[v])) I[v] = 0.0;
                 if (isnan(g)) g = 0.0;

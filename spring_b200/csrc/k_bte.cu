@@ -27,6 +27,7 @@
 #include <cmath>
 
 #include "spring_internal.cuh"
+#include "tetra.cuh"
 
 namespace spring {
 namespace {
@@ -35,54 +36,6 @@ constexpr int NS0 = 6;
 constexpr double ZERO_PREC = 5.0e-5;
 constexpr double FUNIT_E = 1.054571817 / 1.380649;  // FunitE_11m_K (Src_iterative/constants.f90:56)
 constexpr double KW_MK = 1.054571817 * 0.001;       // kW_mK (:58)
-
-__device__ __forceinline__ void sort4(const double* M, int* p) {
-    p[0] = 0; p[1] = 1; p[2] = 2; p[3] = 3;
-#define SWP(i, j)                                                                           \
-    {                                                                                       \
-        const double a_ = M[p[i]], b_ = M[p[j]];                                            \
-        if (b_ < a_ || (b_ == a_ && p[j] < p[i])) { int t_ = p[i]; p[i] = p[j]; p[j] = t_; } \
-    }
-    SWP(0, 1) SWP(2, 3) SWP(0, 2) SWP(1, 3) SWP(1, 2)
-#undef SWP
-}
-
-// FindgAndIver with the strict bounds of kappa_iter (Quasi_momentum_consrv.f90:811-867).
-__device__ __forceinline__ bool g_iver_strict(double Mqs, const double* M, double& g, double* I) {
-    if ((Mqs > M[0]) && (Mqs < M[1])) {
-        g = (3.0 * ((Mqs - M[0]) * (Mqs - M[0]))) / ((M[1] - M[0]) * (M[2] - M[0]) * (M[3] - M[0]));
-        I[0] = (((Mqs - M[1]) / (M[0] - M[1])) + ((Mqs - M[2]) / (M[0] - M[2])) + ((Mqs - M[3]) / (M[0] - M[3]))) / 3.0;
-        for (int v = 1; v < 4; ++v) I[v] = ((Mqs - M[0]) / (M[v] - M[0])) / 3.0;
-        return true;
-    }
-    if ((Mqs > M[1]) && (Mqs < M[2])) {
-        g = (3.0 / ((M[1] - M[2]) * (M[3] - M[0]))) *
-            ((((Mqs - M[0]) * (Mqs - M[2])) / (M[2] - M[0])) - (((Mqs - M[1]) * (Mqs - M[3])) / (M[1] - M[3])));
-        const double den = g * (M[3] - M[0]);
-        I[0] = (((Mqs - M[3]) / (M[0] - M[3])) / 3.0) +
-               ((((Mqs - M[2]) / (M[0] - M[2])) * ((Mqs - M[0]) / (M[2] - M[0])) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        const double t1 = (Mqs - M[3]) / (M[1] - M[3]);
-        I[1] = (((Mqs - M[2]) / (M[1] - M[2])) / 3.0) + (((t1 * t1) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        const double t2 = (Mqs - M[0]) / (M[2] - M[0]);
-        I[2] = (((Mqs - M[1]) / (M[2] - M[1])) / 3.0) + (((t2 * t2) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) / 3.0) +
-               ((((Mqs - M[1]) / (M[3] - M[1])) * ((Mqs - M[3]) / (M[1] - M[3])) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        return true;
-    }
-    if ((Mqs > M[2]) && (Mqs < M[3])) {
-        g = (3.0 * ((Mqs - M[3]) * (Mqs - M[3]))) / ((M[3] - M[0]) * (M[3] - M[1]) * (M[3] - M[2]));
-        for (int v = 0; v < 3; ++v) I[v] = ((Mqs - M[3]) / (M[v] - M[3])) / 3.0;
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) + ((Mqs - M[1]) / (M[3] - M[1])) + ((Mqs - M[2]) / (M[3] - M[2]))) / 3.0;
-        return true;
-    }
-    g = 0.0;
-    return false;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
 
 struct PassArgs {
     int n, nq, ntet, q0_first, s0a, s0n;
@@ -145,7 +98,7 @@ __global__ void __launch_bounds__(128) k_bte_pass(PassArgs a, const int4* __rest
                 }
             }
             int pm[4];
-            sort4(M, pm);
+            tet::sort4(M, pm);
             double S[4];
 #pragma unroll
             for (int v = 0; v < 4; ++v) S[v] = M[pm[v]];
@@ -169,7 +122,7 @@ __global__ void __launch_bounds__(128) k_bte_pass(PassArgs a, const int4* __rest
                 const int s0 = a.s0a + si;
                 const double Mqs = a.omega[(size_t)g0 * n + s0];
                 double g, I[4];
-                if (!g_iver_strict(Mqs, S, g, I)) continue;
+                if (!tet::g_iver<true>(Mqs, S, g, I)) continue;
                 if (!(fabs(I[0] + I[1] + I[2] + I[3] - 1.0) < ZERO_PREC)) continue;
                 const double pre = ch == 0 ? ONEBYSIX * g : 0.5 * ONEBYSIX * g;
                 double tv[NC];
@@ -195,7 +148,7 @@ __global__ void __launch_bounds__(128) k_bte_pass(PassArgs a, const int4* __rest
     for (int s = 0; s < NS0; ++s)
 #pragma unroll
         for (int k = 0; k < NC; ++k) {
-            const double v = warp_sum(acc[s][k]);
+            const double v = tet::warp_sum(acc[s][k]);
             if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&sacc[s * 3 + k], v);
         }
     __syncthreads();

@@ -16,6 +16,7 @@
 // Roofline: FP64 ALU (about 60 flops and 10 divisions per tetrahedron, mode
 // triple and channel); W is read from the L2-resident W grid.
 #include "spring_internal.cuh"
+#include "tetra.cuh"
 
 namespace spring {
 namespace {
@@ -24,82 +25,29 @@ constexpr int NS0 = 6;  // s0 values per pass (register accumulators)
 
 struct TetArgs {
     int n, nq, nq0, nT, ntet;
+    long long ntab;  // rows of the q2 table (path mode)
     int q0_first;
     int s0a, s0n;  // s0 pass: [s0a, s0a + s0n)
     int lo1, n1, lo2, n2;
 };
 
-// Stable ascending order of four keys: p[] receives original vertex indices.
-__device__ __forceinline__ void sort4(const double* M, int* p) {
-    p[0] = 0; p[1] = 1; p[2] = 2; p[3] = 3;
-#define SWP(i, j)                                                              \
-    {                                                                          \
-        const double a_ = M[p[i]], b_ = M[p[j]];                               \
-        if (b_ < a_ || (b_ == a_ && p[j] < p[i])) { int t_ = p[i]; p[i] = p[j]; p[j] = t_; } \
-    }
-    SWP(0, 1) SWP(2, 3) SWP(0, 2) SWP(1, 3) SWP(1, 2)
-#undef SWP
-}
-
-// FindgAndIver on already sorted energies M[0..3]; strict = LineWidth/kappa_iter bounds.
-__device__ __forceinline__ bool g_iver(double Mqs, const double* M, double& g, double* I, bool strict) {
-    bool c1, c2, c3;
-    if (!strict) {
-        c1 = (Mqs >= M[0]) && (Mqs < M[1]);
-        c2 = (Mqs >= M[1]) && (Mqs < M[2]);
-        c3 = (Mqs >= M[2]) && (Mqs <= M[3]);
-    } else {
-        c1 = (Mqs > M[0]) && (Mqs < M[1]);
-        c2 = (Mqs > M[1]) && (Mqs < M[2]);
-        c3 = (Mqs > M[2]) && (Mqs < M[3]);
-    }
-    if (c1) {
-        g = (3.0 * ((Mqs - M[0]) * (Mqs - M[0]))) / ((M[1] - M[0]) * (M[2] - M[0]) * (M[3] - M[0]));
-        I[0] = (((Mqs - M[1]) / (M[0] - M[1])) + ((Mqs - M[2]) / (M[0] - M[2])) + ((Mqs - M[3]) / (M[0] - M[3]))) / 3.0;
-        for (int v = 1; v < 4; ++v) I[v] = ((Mqs - M[0]) / (M[v] - M[0])) / 3.0;
-        return true;
-    }
-    if (c2) {
-        g = (3.0 / ((M[1] - M[2]) * (M[3] - M[0]))) *
-            ((((Mqs - M[0]) * (Mqs - M[2])) / (M[2] - M[0])) - (((Mqs - M[1]) * (Mqs - M[3])) / (M[1] - M[3])));
-        const double den = g * (M[3] - M[0]);
-        I[0] = (((Mqs - M[3]) / (M[0] - M[3])) / 3.0) +
-               ((((Mqs - M[2]) / (M[0] - M[2])) * ((Mqs - M[0]) / (M[2] - M[0])) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        const double t1 = (Mqs - M[3]) / (M[1] - M[3]);
-        I[1] = (((Mqs - M[2]) / (M[1] - M[2])) / 3.0) + (((t1 * t1) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        const double t2 = (Mqs - M[0]) / (M[2] - M[0]);
-        I[2] = (((Mqs - M[1]) / (M[2] - M[1])) / 3.0) + (((t2 * t2) * ((Mqs - M[2]) / (M[1] - M[2]))) / den);
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) / 3.0) +
-               ((((Mqs - M[1]) / (M[3] - M[1])) * ((Mqs - M[3]) / (M[1] - M[3])) * ((Mqs - M[1]) / (M[2] - M[1]))) / den);
-        return true;
-    }
-    if (c3) {
-        g = (3.0 * ((Mqs - M[3]) * (Mqs - M[3]))) / ((M[3] - M[0]) * (M[3] - M[1]) * (M[3] - M[2]));
-        for (int v = 0; v < 3; ++v) I[v] = ((Mqs - M[3]) / (M[v] - M[3])) / 3.0;
-        I[3] = (((Mqs - M[0]) / (M[3] - M[0])) + ((Mqs - M[1]) / (M[3] - M[1])) + ((Mqs - M[2]) / (M[3] - M[2]))) / 3.0;
-        return true;
-    }
-    g = 0.0;
-    I[0] = I[1] = I[2] = I[3] = 0.0;
-    return false;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-
-template <int NTM>
+// Q2TAB = false: kappa.x, the q2 of vertex q1 is the grid partner p(q1) of this q0.
+// Q2TAB = true: LineWidth.x path mode, the q2 phonons of vertex q1 come from a
+// per-q1 table (omega_q2All / nBE_q2All of Linewidth_m.f90:48-231), [slot][q1][s]
+// and [T][row][s] with row = slot * Nq + q1 of a table of `ntab` rows.
+template <int NTM, bool STRICT, bool Q2TAB>
 __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restrict__ tet, const int* __restrict__ partner,
                                                 const double* __restrict__ wgrid, const double* __restrict__ om0,
                                                 const double* __restrict__ omg, const double* __restrict__ nbeg,
+                                                const double* __restrict__ om2t, const double* __restrict__ nbe2t,
                                                 double* __restrict__ out_lw, double* __restrict__ out_p3) {
     __shared__ double sacc[NS0 * (NTM + 1)];
     const int slot = blockIdx.y;
     const int q0 = a.q0_first + slot;
     const int n = a.n;
     const size_t n3 = (size_t)n * n * n;
-    const int* part = partner + (size_t)q0 * a.nq;
+    const int* part = Q2TAB ? nullptr : partner + (size_t)q0 * a.nq;
+    const size_t row0 = (size_t)slot * a.nq;  // first row of this slot in the q2 table
     const double* W = wgrid + (size_t)slot * a.nq * n3;
     for (int i = threadIdx.x; i < NS0 * (NTM + 1); i += blockDim.x) sacc[i] = 0.0;
     __syncthreads();
@@ -122,9 +70,9 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
         double o1[4], o2[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
-            v2[v] = part[v1[v]];
+            v2[v] = Q2TAB ? v1[v] : part[v1[v]];
             o1[v] = omg[(size_t)v1[v] * n + s1];
-            o2[v] = omg[(size_t)v2[v] * n + s2];
+            o2[v] = Q2TAB ? om2t[(row0 + v1[v]) * n + s2] : omg[(size_t)v2[v] * n + s2];
         }
         double M1[4], M2[4], M3[4];
 #pragma unroll
@@ -134,9 +82,9 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
             M3[v] = o1[v] - o2[v];
         }
         int p1[4], p2[4], p3[4];
-        sort4(M1, p1);
-        sort4(M2, p2);
-        sort4(M3, p3);
+        tet::sort4(M1, p1);
+        tet::sort4(M2, p2);
+        tet::sort4(M3, p3);
         double S1[4], S2[4], S3[4];
 #pragma unroll
         for (int v = 0; v < 4; ++v) {
@@ -152,7 +100,8 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
             for (int v = 0; v < 4; ++v) {
                 if (T < a.nT) {
                     const double n1 = nbeg[((size_t)T * a.nq + v1[v]) * n + s1];
-                    const double n2 = nbeg[((size_t)T * a.nq + v2[v]) * n + s2];
+                    const double n2 = Q2TAB ? nbe2t[((size_t)T * a.ntab + row0 + v1[v]) * n + s2]
+                                            : nbeg[((size_t)T * a.nq + v2[v]) * n + s2];
                     fa[T][v] = n1 + n2 + 1.0;
                     fb[T][v] = n1 - n2;
                 } else {
@@ -169,7 +118,7 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
             for (int v = 0; v < 4; ++v) Wv[v] = W[(size_t)v1[v] * n3 + (s0 * n + s1) * n + s2];
             double g, I[4];
             // channel 1: F = W (n1 + n2 + 1), M = w1 + w2, added
-            bool e = g_iver(Mqs, S1, g, I, false);
+            bool e = tet::g_iver<STRICT>(Mqs, S1, g, I);
             acc[si][NTM] += g;
             if (e) {
 #pragma unroll
@@ -181,7 +130,7 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
                 }
             }
             // channel 2: F = W (n1 - n2), M = w2 - w1, added
-            e = g_iver(Mqs, S2, g, I, false);
+            e = tet::g_iver<STRICT>(Mqs, S2, g, I);
             acc[si][NTM] += g;
             if (e) {
 #pragma unroll
@@ -193,7 +142,7 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
                 }
             }
             // channel 3: F = W (n1 - n2), M = w1 - w2, subtracted
-            e = g_iver(Mqs, S3, g, I, false);
+            e = tet::g_iver<STRICT>(Mqs, S3, g, I);
             acc[si][NTM] += g;
             if (e) {
 #pragma unroll
@@ -211,7 +160,7 @@ __global__ void __launch_bounds__(128) k_tetra3(TetArgs a, const int4* __restric
     for (int s = 0; s < NS0; ++s)
 #pragma unroll
         for (int T = 0; T <= NTM; ++T) {
-            const double v = warp_sum(acc[s][T]);
+            const double v = tet::warp_sum(acc[s][T]);
             if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&sacc[s * (NTM + 1) + T], v);
         }
     __syncthreads();
@@ -273,12 +222,12 @@ __global__ void __launch_bounds__(128) k_iso_tetra(int n, int nq, int nq0, int n
         double M[4];
         for (int v = 0; v < 4; ++v) M[v] = omg[(size_t)v1[v] * n + s1];
         int p[4];
-        sort4(M, p);
+        tet::sort4(M, p);
         double S[4];
         for (int v = 0; v < 4; ++v) S[v] = M[p[v]];
         for (int s0 = 0; s0 < n; ++s0) {
             double g, I[4];
-            const bool e = g_iver(om0[(size_t)q0 * n + s0], S, g, I, false);
+            const bool e = tet::g_iver<false>(om0[(size_t)q0 * n + s0], S, g, I);
             for (int v = 0; v < 4; ++v) if (isnan(I[v])) I[v] = 0.0;
             if (isnan(g)) g = 0.0;
             double s = 0.0;
@@ -324,16 +273,10 @@ int grid_x(long long items, int threads, int slots) {
     return (int)(want < 1 ? 1 : want);
 }
 
-}  // namespace
-
-int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const Pol& pol, double* d_lw, double* d_p3) {
-    TetArgs a;
-    a.n = c->ndof;
-    a.nq = c->nq;
-    a.nq0 = c->nq0;
-    a.nT = c->nT;
-    a.ntet = 6 * c->nq;
-    a.q0_first = q0_first;
+template <bool STRICT, bool Q2TAB>
+int launch_tetra3(spring_ctx* c, TetArgs a, int n_q0, const Pol& pol, const double* d_w, const int* part,
+                  const double* om0, const double* omg, const double* nbeg, const double* om2t, const double* nbe2t,
+                  double* d_lw, double* d_p3) {
     a.lo1 = pol.lo[1];
     a.n1 = pol.hi[1] - pol.lo[1] + 1;
     a.lo2 = pol.lo[2];
@@ -341,27 +284,59 @@ int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const P
     const long long items = (long long)a.ntet * a.n1 * a.n2;
     const int threads = 128;
     dim3 grid(grid_x(items, threads, n_q0), n_q0);
+    const int4* tet = reinterpret_cast<const int4*>(c->d_tetra.p);
     for (int s0a = pol.lo[0]; s0a <= pol.hi[0]; s0a += NS0) {
         a.s0a = s0a;
         a.s0n = std::min(NS0, pol.hi[0] - s0a + 1);
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "tetra3: injected launch failure");
-        const int4* tet = reinterpret_cast<const int4*>(c->d_tetra.p);
-        const int* part = c->ps_irr.partner.p;
         if (c->nT == 1) {
-            k_tetra3<1><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, c->ph_irr.omega.p, c->ph_grid.omega.p,
-                                                          c->ph_grid.nbe.p, d_lw, d_p3);
+            k_tetra3<1, STRICT, Q2TAB><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, om0, omg, nbeg, om2t, nbe2t,
+                                                                        d_lw, d_p3);
         } else if (c->nT <= 3) {
-            k_tetra3<3><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, c->ph_irr.omega.p, c->ph_grid.omega.p,
-                                                          c->ph_grid.nbe.p, d_lw, d_p3);
+            k_tetra3<3, STRICT, Q2TAB><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, om0, omg, nbeg, om2t, nbe2t,
+                                                                        d_lw, d_p3);
         } else if (c->nT <= 9) {
-            k_tetra3<9><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, c->ph_irr.omega.p, c->ph_grid.omega.p,
-                                                          c->ph_grid.nbe.p, d_lw, d_p3);
+            k_tetra3<9, STRICT, Q2TAB><<<grid, threads, 0, c->stream>>>(a, tet, part, d_w, om0, omg, nbeg, om2t, nbe2t,
+                                                                        d_lw, d_p3);
         } else {
             return fail(c, SPRING_ERR_UNSUPPORTED, "tetrahedron integration supports at most 9 temperatures per call");
         }
-        SPRING_CHECK(launch_check(c, "k_tetra3"));
+        SPRING_CHECK(launch_check(c, Q2TAB ? "k_tetra3<path>" : "k_tetra3"));
     }
     return SPRING_OK;
+}
+
+}  // namespace
+
+int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const Pol& pol, double* d_lw, double* d_p3) {
+    TetArgs a{};
+    a.n = c->ndof;
+    a.nq = c->nq;
+    a.nq0 = c->nq0;
+    a.nT = c->nT;
+    a.ntet = 6 * c->nq;
+    a.q0_first = q0_first;
+    return launch_tetra3<false, false>(c, a, n_q0, pol, d_w, c->ps_irr.partner.p, c->ph_irr.omega.p,
+                                       c->ph_grid.omega.p, c->ph_grid.nbe.p, nullptr, nullptr, d_lw, d_p3);
+}
+
+int run_tetra3_path(spring_ctx* c, int p_first, int n_slots, int n_path, const double* d_w, const double* om0,
+                    const double* om2t, const double* nbe2t, long long ntab, double* d_lw, double* d_scratch) {
+    TetArgs a{};
+    a.n = c->ndof;
+    a.nq = c->nq;
+    a.nq0 = n_path;
+    a.nT = c->nT;
+    a.ntet = 6 * c->nq;
+    a.q0_first = p_first;
+    a.ntab = ntab;
+    Pol pol;
+    for (int k = 0; k < 3; ++k) {
+        pol.lo[k] = 0;
+        pol.hi[k] = c->ndof - 1;
+    }
+    return launch_tetra3<true, true>(c, a, n_slots, pol, d_w, nullptr, om0, c->ph_grid.omega.p, c->ph_grid.nbe.p,
+                                     om2t, nbe2t, d_lw, d_scratch);
 }
 
 int run_iso(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const double* g2, double* d_rate) {

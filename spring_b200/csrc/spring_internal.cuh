@@ -124,6 +124,8 @@ struct spring_ctx {
 
     // mesh
     bool mesh_set = false;
+    bool mesh_zc = true;           // zero-centred folding (kappa.x) or [0, N) (LineWidth.x)
+    int mesh_shift[3] = {0, 0, 0};
     spring::DBuf<int> d_qint;      // [q][3]
     spring::DBuf<double> d_qpnt;   // [q][3]
     spring::DBuf<int> d_tetra;     // [t][4] 0-based grid indices
@@ -191,6 +193,8 @@ inline void free_pairs(PairSet& s) {
     s.h_pairoff.clear();
     s.done = false;
 }
+void free_phonons(Phonons& p);
+int alloc_phonons(spring_ctx* c, Phonons& p, int n);
 int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what);
@@ -221,10 +225,17 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
 // k_4ph.cu
 int run_enumerate4_fortran(spring_ctx* c, int q0, int* d_all, int* d_perm, long long cap, long long* h_counts);
 int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const int* pol4, double* d_rate);
+// k_path.cu: LineWidth.x path mode; h_q0 (3, n_path) Cartesian, h_lw [T][p][s], h_omega [p][s]
+int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
+             double* h_lw, double* h_omega);
+int path_points(const double* G, int n_nodes, const double* q_high_sym, double* qpoints, double* dist, int* zc);
 // k_bte.cu
 int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters);
 // k_tetra.cu
 int run_tetra3(spring_ctx* c, int q0_first, int n_q0, const double* d_w, const Pol& pol, double* d_lw, double* d_p3);
+// LineWidth.x form: strict bounds, q2 phonons of vertex q1 from a table of `ntab` rows (row = slot * Nq + q1)
+int run_tetra3_path(spring_ctx* c, int p_first, int n_slots, int n_path, const double* d_w, const double* om0,
+                    const double* om2t, const double* nbe2t, long long ntab, double* d_lw, double* d_scratch);
 int run_iso(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const double* g2, double* d_rate);
 // k_kappa.cu
 int run_axpy_lw(spring_ctx* c, double a, const double* d_x, double* d_y, int q0_first, int n_q0);
