@@ -44,7 +44,9 @@ typedef struct spring_ctx spring_ctx;
 #define SPRING_DELTA_TETRA 1 /* linear tetrahedron, ThirdOrder_m.f90:169-275 */
 
 /* arithmetic of the V3/V4 contractions (deltas, rates and kappa stay FP64) */
-#define SPRING_FP64 0
+#define SPRING_FP64 0   /* FP64 CUDA cores, the reference's arithmetic */
+#define SPRING_BF16 1   /* tcgen05 tensor cores, BF16 operands, FP32 accumulation */
+#define SPRING_BF16X3 2 /* as SPRING_BF16 with hi+lo BF16 splits (compensated, about FP32 accuracy) */
 
 typedef struct {
     int nbasis;  /* Nb: atoms in the unit cell (Ndof = 3*Nb), at most 8 */
@@ -214,6 +216,34 @@ int spring_path_qpoints(spring_ctx* ctx, int n_nodes, const double* q_high_sym, 
  * the resident LW_Allq0 is not touched. */
 int spring_linewidth_path(spring_ctx* ctx, int n_q0, const double* q0, const int* zero_centered, int delta_mode,
                           double sigma, double* lw, double* omega_q0);
+
+/* Arithmetic of the 3-phonon matrix elements in the fused Gaussian linewidth
+ * (spring_linewidth3 with SPRING_DELTA_GAUSS, two-atom cells): SPRING_FP64
+ * (default), SPRING_BF16 or SPRING_BF16X3.  No counterpart in the reference,
+ * which is FP64 throughout.  Other cells and the tetrahedron path stay FP64. */
+int spring_set_precision(spring_ctx* ctx, int precision);
+
+/* ---- surrogate network of the screened four-phonon path -------------- */
+/* No counterpart in the reference, which evaluates every four-phonon rate
+ * exactly.  A 5 -> 128 -> 128 -> 128 -> 1 network (SiLU) that maps per-mode
+ * harmonic features to the log four-phonon rate, trained and evaluated on the
+ * device; the exact spring_linewidth4 stays the judge of its error.
+ * X(SPRING_MLP_INPUTS, n) features (standardised by the caller), y(n) targets.
+ * Parameters: one FP32 vector of SPRING_MLP_PARAMS values, W1 (128x5 row-major),
+ * b1, W2 (128x128), b2, W3, b3, W4 (1x128), b4. */
+#define SPRING_MLP_INPUTS 5
+#define SPRING_MLP_PARAMS 33921
+int spring_mlp_init(spring_ctx* ctx, unsigned long long seed);
+int spring_mlp_set_params(spring_ctx* ctx, const float* params);
+int spring_mlp_get_params(spring_ctx* ctx, float* params);
+/* Mean-squared-error loss and its gradient (SPRING_MLP_PARAMS) over all n rows. */
+int spring_mlp_loss_grad(spring_ctx* ctx, int n, const float* X, const float* y, float* loss, float* grad);
+/* Adam (beta 0.9/0.999) over `epochs` shuffled passes in minibatches of `batch`
+ * rows (a trailing partial batch is skipped); epoch_loss(epochs) optional. */
+int spring_mlp_train(spring_ctx* ctx, int n, const float* X, const float* y, int epochs, int batch, float lr,
+                     unsigned long long seed, float* epoch_loss);
+/* y(n) = network(X); bf16 != 0 rounds weights and activations to BF16. */
+int spring_mlp_predict(spring_ctx* ctx, int n, const float* X, float* y, int bf16);
 
 /* Zero / read / replace the resident LW_Allq0(Ndof,Nq0,n_temps). */
 int spring_reset_linewidths(spring_ctx* ctx);

@@ -20,6 +20,11 @@ SPRING_ERR_UNSUPPORTED = 5
 SPRING_ERR_INJECTED = 6
 SPRING_DELTA_GAUSS = 0
 SPRING_DELTA_TETRA = 1
+SPRING_FP64 = 0
+SPRING_BF16 = 1
+SPRING_BF16X3 = 2
+SPRING_MLP_INPUTS = 5
+SPRING_MLP_PARAMS = 33921
 
 
 class spring_dims(ct.Structure):
@@ -51,6 +56,13 @@ SIGNATURES = {
     "spring_prepare3": [P],
     "spring_set_profiling": [P, I],
     "spring_set_option": [P, I, I],
+    "spring_set_precision": [P, I],
+    "spring_mlp_init": [P, ct.c_ulonglong],
+    "spring_mlp_set_params": [P, P],
+    "spring_mlp_get_params": [P, P],
+    "spring_mlp_loss_grad": [P, I, P, P, P, P],
+    "spring_mlp_train": [P, I, P, P, I, I, ct.c_float, ct.c_ulonglong, P],
+    "spring_mlp_predict": [P, I, P, P, I],
     "spring_kappa_iter": [P, D, I, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_scatter_w3": [P, I, P],

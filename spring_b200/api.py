@@ -94,6 +94,45 @@ class Context:
     def set_option(self, option: int, value: int):
         self._call("spring_set_option", int(option), int(value))
 
+    def set_precision(self, precision):
+        """"fp64" (default), "bf16" or "bf16x3": arithmetic of the fused Gaussian V3."""
+        code = {"fp64": L.SPRING_FP64, "bf16": L.SPRING_BF16, "bf16x3": L.SPRING_BF16X3}[precision]
+        self._call("spring_set_precision", code)
+
+    # -- surrogate network (no counterpart in the reference)
+    def mlp_init(self, seed: int = 0):
+        self._call("spring_mlp_init", int(seed))
+
+    def mlp_params(self):
+        p = np.zeros(L.SPRING_MLP_PARAMS, np.float32)
+        self._call("spring_mlp_get_params", _ptr(p))
+        return p
+
+    def mlp_set_params(self, p):
+        self._call("spring_mlp_set_params", _ptr(_c(p, np.float32)))
+
+    def mlp_loss_grad(self, X, y):
+        X = _c(X, np.float32)
+        y = _c(y, np.float32)
+        loss = np.zeros(1, np.float32)
+        g = np.zeros(L.SPRING_MLP_PARAMS, np.float32)
+        self._call("spring_mlp_loss_grad", int(len(y)), _ptr(X), _ptr(y), _ptr(loss), _ptr(g))
+        return float(loss[0]), g
+
+    def mlp_train(self, X, y, epochs=100, batch=256, lr=1e-3, seed=0):
+        X = _c(X, np.float32)
+        y = _c(y, np.float32)
+        hist = np.zeros(max(int(epochs), 1), np.float32)
+        self._call("spring_mlp_train", int(len(y)), _ptr(X), _ptr(y), int(epochs), int(batch), float(lr), int(seed),
+                   _ptr(hist))
+        return hist[: int(epochs)]
+
+    def mlp_predict(self, X, bf16=False):
+        X = _c(X, np.float32)
+        y = np.zeros(X.shape[0], np.float32)
+        self._call("spring_mlp_predict", int(X.shape[0]), _ptr(X), _ptr(y), int(bool(bf16)))
+        return y
+
     def use_generic_v3(self, on: bool = True):
         """Force the any-cell V3 kernel instead of the two-atom specialisation."""
         self.set_option(1, int(bool(on)))

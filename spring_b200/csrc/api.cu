@@ -252,6 +252,9 @@ int spring_ctx_destroy(spring_ctx* c) {
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
+        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_q); dfree(c->d_tc_entries);
+        dfree(c->d_tc_rec); dfree(c->d_tc_tiles); dfree(c->d_tc_err);
+        free_mlp(c->mlp);
         dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -838,6 +841,57 @@ int spring_linewidth_path(spring_ctx* c, int n_q0, const double* q0, const int* 
     std::vector<double> buf(lw ? (size_t)c->nT * n_q0 * c->ndof : 0);
     SPRING_CHECK(run_path(c, n_q0, q0, zero_centered, delta_mode, sigma, lw ? buf.data() : nullptr, omega_q0));
     if (lw) std::memcpy(lw, buf.data(), sizeof(double) * buf.size());  // [T][p][s] is lw(Ndof, n_q0, n_temps)
+    return SPRING_OK;
+}
+
+int spring_mlp_init(spring_ctx* c, unsigned long long seed) {
+    CTX_ENTER(c);
+    if (mlp_num_params() != SPRING_MLP_PARAMS) return fail(c, SPRING_ERR_STATE, "network size mismatch");
+    return run_mlp_init(c, seed);
+}
+
+int spring_mlp_set_params(spring_ctx* c, const float* params) {
+    CTX_ENTER(c);
+    if (!params) return fail(c, SPRING_ERR_ARG, "params is NULL");
+    return run_mlp_set(c, params);
+}
+
+int spring_mlp_get_params(spring_ctx* c, float* params) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mlp.set, "network parameters"));
+    if (!params) return fail(c, SPRING_ERR_ARG, "params is NULL");
+    return d2h(c, params, c->mlp.p.p, sizeof(float) * SPRING_MLP_PARAMS, "network parameters");
+}
+
+int spring_mlp_loss_grad(spring_ctx* c, int n, const float* X, const float* y, float* loss, float* grad) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mlp.set, "network parameters"));
+    if (n < 1 || !X || !y) return fail(c, SPRING_ERR_ARG, "n < 1 or NULL X / y");
+    return run_mlp_loss_grad(c, n, X, y, loss, grad);
+}
+
+int spring_mlp_train(spring_ctx* c, int n, const float* X, const float* y, int epochs, int batch, float lr,
+                     unsigned long long seed, float* epoch_loss) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mlp.set, "network parameters"));
+    if (n < 1 || !X || !y || epochs < 0 || batch < 1 || !(lr > 0.0f))
+        return fail(c, SPRING_ERR_ARG, "n, batch >= 1, epochs >= 0, lr > 0 and non-NULL X / y are required");
+    return run_mlp_train(c, n, X, y, epochs, batch, lr, seed, epoch_loss);
+}
+
+int spring_mlp_predict(spring_ctx* c, int n, const float* X, float* y, int bf16) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->mlp.set, "network parameters"));
+    if (n < 0 || (n > 0 && (!X || !y))) return fail(c, SPRING_ERR_ARG, "n < 0 or NULL X / y");
+    if (n == 0) return SPRING_OK;
+    return run_mlp_predict(c, n, X, y, bf16);
+}
+
+int spring_set_precision(spring_ctx* c, int precision) {
+    CTX_ENTER(c);
+    if (precision != SPRING_FP64 && precision != SPRING_BF16 && precision != SPRING_BF16X3)
+        return fail(c, SPRING_ERR_ARG, "precision must be SPRING_FP64, SPRING_BF16 or SPRING_BF16X3");
+    c->precision = precision;
     return SPRING_OK;
 }
 

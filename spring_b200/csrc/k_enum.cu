@@ -144,7 +144,10 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
         rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
     }
     dfree(rep);
-    if (rc == SPRING_OK) ps.done = true;
+    if (rc == SPRING_OK) {
+        ps.done = true;
+        ps.gen += 1;
+    }
     return rc;
 }
 

@@ -286,6 +286,10 @@ Q0View irr_view(spring_ctx* c) {
 
 int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3) {
     bool handled = false;
+    if (c->precision != SPRING_FP64) {
+        SPRING_CHECK(run_v3tc_gauss(c, q0_first, n_q0, sigma, pol, d_lw, d_p3, &handled));
+        if (handled) return SPRING_OK;
+    }
     if (!c->force_generic_v3)
         SPRING_CHECK(launch_v3s(c, c->ps_irr, irr_view(c), q0_first, n_q0, 0, sigma, &pol, d_lw, d_p3, nullptr,
                                 &handled));

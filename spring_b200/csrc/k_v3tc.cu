@@ -1,0 +1,663 @@
+// Three-phonon V3 on the 5th-generation tensor cores (tcgen05, BF16 in, FP32
+// accumulate), fused with the Gaussian linewidth sum.  Two-atom cells.
+//
+// Same quantity as ScatterMatEl / ScatterProbability + CalculateLinewidth
+// (src/Kappa/Src/ThirdOrder_m.f90:278-439, 442-543), regrouped so that the
+// bulk of the work is a GEMM with a shared operand:
+//   U_q[mu][N b][s]      = e^{i q.R_{mu N}} m_{nu(N)}^-1/2 e_q(nu(N) b, s)         (per grid q)
+//   Z_q1[mu][a s1][N2 c] = sum_{N1 b} FC3[mu][N1][N2][a b c] U_q1[mu][N1 b][s1]     (per grid q1)
+//   Y[mu][a s1][s2]      = sum_{N2 c} Z_q1[mu][a s1][N2 c] U_q2[mu][N2 c][s2]       (per pair: tensor cores)
+//   Phi[s0][s1][s2]      = sum_{mu a} m_mu^-1/2 e0(mu a, s0) Y[mu][a s1][s2]        (per pair: epilogue)
+// Pairs are grouped by q1, so one tile is up to 20 pairs sharing Z_q1: the MMA
+// computes Y^T for 120 rows (pair, s2) at once, M = 128, N = 48 (36 used:
+// Re/Im of (a, s1)), K = 48 (Re/Im of (N2, c), 42 used), one accumulator per
+// basis atom mu in tensor memory.  The complex product is written as a real one:
+//   A[(pair, s2)][k] = [Re U_q2 | Im U_q2],   B[(re, a s1)][k] = [Re Z | -Im Z],
+//   B[(im, a s1)][k] = [Im Z | Re Z].
+// Precision: SPRING_BF16 rounds A and B to BF16 once; SPRING_BF16X3 splits each
+// into hi + lo BF16 parts and accumulates hi*hi + hi*lo + lo*hi (compensated).
+// Frequencies, occupations, the delta weights and every sum stay FP64.  The
+// epilogue screens each mode triple in FP32 against the window where a delta
+// weight can exceed exp(-40) of its peak (4e-18) and evaluates Phi, W and the
+// FP64 deltas only for the triples inside it (about 1-2 % of them).
+// Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass),
+// L2 bandwidth for gathering the U_q2 rows, FP32/FP64 ALU for the screen.
+#include <algorithm>
+#include <cub/cub.cuh>
+#include <cuda_bf16.h>
+
+#include "spring_internal.cuh"
+#include "tc.cuh"
+
+namespace spring {
+namespace {
+
+constexpr int NMODE = 6;     // Ndof of the two-atom cell
+constexpr int KP = 48;       // padded K: Re/Im of (N2, c), 2 * 3 * Na3 <= 48
+constexpr int EPT = 20;      // pairs per tile: five per 32-row TMEM lane quarter (120 of 128 rows)
+constexpr int BROWS = 36;    // used B rows
+constexpr int QSMAX = 12 + 6 * 9;  // packed phonons of one grid point: omega[6], 1/omega[6], nBE[T][6]
+constexpr int Q0ROW = 50;    // packed q0 row in doubles (48 used; 400-byte stride spreads the banks)
+constexpr uint32_t LBO = 128, SBO = (KP / 8) * 128;
+constexpr int A_BYTES = (128 / 8) * SBO;  // 12288
+constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
+constexpr double EXP_CUT = 40.0;
+constexpr long long MAX_SPINS = 1LL << 26;
+
+// bf16 hi/lo split of an FP64 value
+__device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+    const float f = (float)x;
+    hi = __float2bfloat16_rn(f);
+    lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+}
+
+// U of one grid point, basis mu, slot k = N*3 + b, branch s (FP64)
+__device__ __forceinline__ double2 u_value(int q, int mu, int k, int s, int na, const double* __restrict__ posr,
+                                          const int* __restrict__ btyp, const double* __restrict__ mrs,
+                                          const double* __restrict__ qpnt, const double2* __restrict__ evg) {
+    const int N = k / 3, b = k % 3;
+    const double* R = posr + ((size_t)mu * na + N) * 3;
+    const double qr = qpnt[3 * q] * R[0] + qpnt[3 * q + 1] * R[1] + qpnt[3 * q + 2] * R[2];
+    double sn, cs;
+    sincos(qr, &sn, &cs);
+    const int nu = btyp[mu * na + N];
+    const double m = mrs[nu];
+    const double2 e = evg[((size_t)q * NMODE + s) * NMODE + nu * 3 + b];
+    return make_double2(m * (cs * e.x - sn * e.y), m * (cs * e.y + sn * e.x));
+}
+
+// A table: [q][mu][hl][s][KP] bf16
+__global__ void k_tc_tab_a(int nq, int na, const double* __restrict__ posr, const int* __restrict__ btyp,
+                           const double* __restrict__ mrs, const double* __restrict__ qpnt,
+                           const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
+    const int KR = 3 * na;
+    const long long total = (long long)nq * 2 * NMODE * KP;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(i % KP), s = (int)((i / KP) % NMODE), mu = (int)((i / (KP * NMODE)) % 2);
+        const int q = (int)(i / (KP * NMODE * 2));
+        double x = 0.0;
+        if (k < 2 * KR) {
+            const double2 u = u_value(q, mu, k % KR, s, na, posr, btyp, mrs, qpnt, evg);
+            x = k < KR ? u.x : u.y;
+        }
+        __nv_bfloat16 hi, lo;
+        split_bf16(x, hi, lo);
+        const size_t base = (((size_t)q * 2 + mu) * 2) * NMODE * KP + (size_t)s * KP + k;
+        tab[base] = hi;
+        tab[base + (size_t)NMODE * KP] = lo;
+    }
+}
+
+// B table: [q1][mu][hl][36][KP] bf16; one CTA per (q1, mu)
+__global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* __restrict__ fc3,
+                                                  const double* __restrict__ posr, const int* __restrict__ btyp,
+                                                  const double* __restrict__ mrs, const double* __restrict__ qpnt,
+                                                  const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
+    __shared__ double2 sU[24 * NMODE];  // [N b][s]
+    const int q = blockIdx.x / 2, mu = blockIdx.x % 2;
+    const int KR = 3 * na;
+    for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
+        sU[i] = u_value(q, mu, i / NMODE, i % NMODE, na, posr, btyp, mrs, qpnt, evg);
+    __syncthreads();
+    const double* f = fc3 + (size_t)mu * na * na * 27;
+    __nv_bfloat16* out = tab + ((size_t)q * 2 + mu) * 2 * BROWS * KP;
+    for (int i = threadIdx.x; i < 2 * BROWS * (KP - 2 * KR); i += blockDim.x) {  // zero K padding
+        const int hl = i / (BROWS * (KP - 2 * KR)), r = (i / (KP - 2 * KR)) % BROWS, k = 2 * KR + i % (KP - 2 * KR);
+        out[((size_t)hl * BROWS + r) * KP + k] = __float2bfloat16_rn(0.0f);
+    }
+    for (int i = threadIdx.x; i < 18 * KR; i += blockDim.x) {
+        const int r = i / KR, k2 = i % KR;  // r = a*6 + s1, k2 = N2*3 + c
+        const int al = r / NMODE, s1 = r % NMODE, N2 = k2 / 3, ga = k2 % 3;
+        double zr = 0.0, zi = 0.0;
+        for (int k1 = 0; k1 < KR; ++k1) {
+            const int N1 = k1 / 3, be = k1 % 3;
+            const double fv = f[((size_t)N1 * na + N2) * 27 + (al * 3 + be) * 3 + ga];
+            const double2 u = sU[k1 * NMODE + s1];
+            zr = fma(fv, u.x, zr);
+            zi = fma(fv, u.y, zi);
+        }
+        __nv_bfloat16 h, l;
+        // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
+        split_bf16(zr, h, l);
+        out[(size_t)r * KP + k2] = h;                       out[((size_t)BROWS + r) * KP + k2] = l;
+        out[(size_t)(18 + r) * KP + KR + k2] = h;           out[((size_t)BROWS + 18 + r) * KP + KR + k2] = l;
+        split_bf16(-zi, h, l);
+        out[(size_t)r * KP + KR + k2] = h;                  out[((size_t)BROWS + r) * KP + KR + k2] = l;
+        split_bf16(zi, h, l);
+        out[(size_t)(18 + r) * KP + k2] = h;                out[((size_t)BROWS + 18 + r) * KP + k2] = l;
+    }
+}
+
+// Packed q0 rows (Q0ROW doubles): e0' = m_mu^-1/2 e0(mu a, s0) as float2 [s0][row] (288 bytes), then
+// omega0[6] and 1/omega0[6].
+__global__ void k_tc_q0tab(int nq0, const double2* __restrict__ ev0, const double* __restrict__ om0,
+                           const double* __restrict__ ob0, const double* __restrict__ mrs, double* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq0 * 48; i += gridDim.x * blockDim.x) {
+        const int q = i / 48, k = i % 48;
+        double* row = out + (size_t)q * Q0ROW;
+        if (k < 36) {
+            const double2 e = ev0[(size_t)q * 36 + k];
+            const double m = mrs[(k % NMODE) / 3];
+            reinterpret_cast<float2*>(row)[k] = make_float2((float)(m * e.x), (float)(m * e.y));
+        } else if (k < 42) {
+            row[k] = om0[(size_t)q * NMODE + k - 36];
+        } else {
+            row[k] = ob0[(size_t)q * NMODE + k - 42];
+        }
+    }
+}
+
+// Packed grid rows (QS = 12 + 6 nT doubles): omega[6], 1/omega[6], nBE[T][6].
+__global__ void k_tc_qtab(int nq, int nT, const double* __restrict__ omg, const double* __restrict__ obg,
+                          const double* __restrict__ nbeg, double* __restrict__ out) {
+    const int qs = 12 + 6 * nT;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * qs;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i / qs), k = (int)(i % qs);
+        double v;
+        if (k < 6) v = omg[(size_t)q * NMODE + k];
+        else if (k < 12) v = obg[(size_t)q * NMODE + k - 6];
+        else v = nbeg[((size_t)((k - 12) / NMODE) * nq + q) * NMODE + (k - 12) % NMODE];
+        out[i] = v;
+    }
+}
+
+// ------------------------------------------------------------------ tiles
+__global__ void k_tc_keys(int n, int p0, const int2* __restrict__ pairs, int* __restrict__ keys, int* __restrict__ vals,
+                          int* __restrict__ cnt) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int g1 = pairs[p0 + i].x;
+        keys[i] = g1;
+        vals[i] = p0 + i;
+        atomicAdd(&cnt[g1], 1);
+    }
+}
+__global__ void k_tc_ntiles(int nq, const int* __restrict__ cnt, int* __restrict__ nt) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nq; g += gridDim.x * blockDim.x)
+        nt[g] = (cnt[g] + EPT - 1) / EPT;
+}
+__global__ void k_tc_tiles(int nq, const int* __restrict__ cnt, const int* __restrict__ seg, const int* __restrict__ toff,
+                           int4* __restrict__ tiles) {
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nq; g += gridDim.x * blockDim.x) {
+        const int c = cnt[g];
+        for (int t = 0; t * EPT < c; ++t) tiles[toff[g] + t] = make_int4(g, seg[g] + t * EPT, min(EPT, c - t * EPT), 0);
+    }
+}
+// Entry records in q1 order: (q0, q2, pair-folding weight, q0 is Gamma).
+__global__ void k_tc_entrec(int n, const int* __restrict__ entries, const int2* __restrict__ pairs,
+                            const int* __restrict__ pair_q0, const int* __restrict__ irr_int, int4* __restrict__ rec) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int pi = entries[i];
+        const int2 pq = pairs[pi];
+        const int q0 = pair_q0[pi];
+        const int g0 = irr_int[3 * q0] == 0 && irr_int[3 * q0 + 1] == 0 && irr_int[3 * q0 + 2] == 0;
+        rec[i] = make_int4(q0, pq.y, pq.x != pq.y ? 2 : 1, g0);
+    }
+}
+
+// ------------------------------------------------------------------ main kernel
+struct TcArgs {
+    int nq, nq0, nT, qs, ntiles, tiles_per_cta;
+    int lo[3], hi[3];
+    double mfac, half_os2, pre;
+};
+
+// One pipeline stage: the operands of one tile and everything its epilogue reads.
+struct TcStage {
+    alignas(128) uint8_t A[2][2][A_BYTES];  // [mu][hi, lo]: rows (pair, s2)
+    alignas(128) uint8_t B[2][2][B_BYTES];  // [mu][hi, lo]: rows (re/im, a, s1)
+    double q0d[EPT][Q0ROW];                 // packed q0 rows
+    double q2d[EPT][QSMAX];                 // packed q2 rows
+    double q1d[QSMAX];                      // packed q1 row
+    int4 ent[EPT];                          // (q0, q2, weight, q0 is Gamma)
+    int q1, ne;
+};
+
+struct TcSmem {
+    TcStage st[2];
+    int4 pf[2][EPT];   // entry records prefetched one tile ahead
+    int4 trec[4];      // tile records prefetched two tiles ahead
+    alignas(8) uint64_t ready[2], full[2], empty[2];
+    uint32_t tslot;
+    int abort_p, abort_e;  // a bounded wait gave up (decided by one thread, read by its role)
+};
+
+constexpr int EPI_THREADS = 256;   // warps 0-7: epilogue; warps w and w+4 share TMEM lanes, three s0 each
+constexpr int PRO_THREADS = 128;   // warps 8-11: operand gather and MMA issue
+constexpr int TC_THREADS = EPI_THREADS + PRO_THREADS;
+
+// TMEM row of (pair e, branch s2): five pairs per 32-lane quarter, lanes 30 and 31 unused.
+__host__ __device__ __forceinline__ int tc_row(int e, int s2) { return 32 * (e / 5) + NMODE * (e % 5) + s2; }
+
+// Warp-specialised, double-buffered: the producer warps gather tile i+1 into the
+// free stage (cp.async) and one of them issues its MMAs into the stage's TMEM
+// columns, while the epilogue warps reduce tile i.  mbarriers: ready[s] (the
+// stage's operands and phonon rows are in shared memory), full[s] (MMA
+// completion, tcgen05.commit), empty[s] (every epilogue warp is done with s).
+template <int NTM, bool SPLIT>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec, const __nv_bfloat16* __restrict__ tabA,
+       const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ q0tab, const double* __restrict__ qtab,
+       double* __restrict__ out_lw, double* __restrict__ out_p3, int* __restrict__ err) {
+    extern __shared__ __align__(128) uint8_t smraw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int H = SPLIT ? 2 : 1;
+    const int t0 = blockIdx.x * a.tiles_per_cta;
+    const int t1 = min(a.ntiles, t0 + a.tiles_per_cta);
+
+    for (int i = tid; i < (int)(2 * sizeof(S.st[0].B) / 16); i += blockDim.x) {
+        const int st = i / (int)(sizeof(S.st[0].B) / 16), k = i % (int)(sizeof(S.st[0].B) / 16);
+        reinterpret_cast<uint4*>(&S.st[st].B[0][0][0])[k] = make_uint4(0, 0, 0, 0);
+    }
+    if (tid == 0) {
+        S.st[0].q1 = S.st[1].q1 = -1;
+        S.abort_p = S.abort_e = 0;
+        for (int k = 0; k < 2; ++k) {
+            tc::mbar_init(tc::smem_u32(&S.ready[k]), 1);
+            tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
+            tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_THREADS / 32);
+        }
+        tc::mbar_fence_init();
+    }
+    if (tid < 2 && t0 + tid < t1) S.trec[tid] = tiles[t0 + tid];
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), 256);
+    tc::fence_before_sync();
+    __syncthreads();
+    if (t0 < t1 && tid < S.trec[0].z) S.pf[0][tid] = entrec[S.trec[0].y + tid];
+    tc::fence_after_sync();
+    __syncthreads();
+    const uint32_t tm = S.tslot;
+
+    if (tid >= EPI_THREADS) {
+        // ------------------------------------------------------------ producer
+        const int pt = tid - EPI_THREADS;
+        for (int t = t0, j = 0; t < t1; ++t, ++j) {
+            const int s = j & 1, u = j >> 1;
+            TcStage& G = S.st[s];
+            if (u > 0) {
+                if (pt == 0) S.abort_p = !tc::mbar_wait(tc::smem_u32(&S.empty[s]), (uint32_t)((u - 1) & 1), MAX_SPINS);
+                tc::named_bar(1, PRO_THREADS);
+                if (S.abort_p) {
+                    if (pt == 0) atomicExch(err, 1);
+                    break;
+                }
+            }
+            const int4 tile = S.trec[j & 3];
+            const int q1 = tile.x, ne = tile.z;
+            const int4* ent = S.pf[j & 1];
+            const bool newb = G.q1 != q1;
+            // prefetch the tile record two ahead and the entry records of the next tile
+            if (pt == 0 && t + 2 < t1) tc::cp_async16(tc::smem_u32(&S.trec[(j + 2) & 3]), tiles + t + 2);
+            if (t + 1 < t1) {
+                const int4 nx = S.trec[(j + 1) & 3];
+                if (pt < nx.z) tc::cp_async16(tc::smem_u32(&S.pf[(j + 1) & 1][pt]), entrec + nx.y + pt);
+            }
+            if (pt < ne) G.ent[pt] = ent[pt];
+            if (newb) {
+                for (int i = pt; i < 2 * H * BROWS * (KP / 8); i += PRO_THREADS) {
+                    const int kc = i % (KP / 8), n = (i / (KP / 8)) % BROWS, mh = i / (BROWS * (KP / 8));
+                    const int mu = mh / H, hl = mh % H;
+                    tc::cp_async16(tc::smem_u32(&G.B[mu][hl][tc::kmajor_offset(n, kc * 8, LBO, SBO)]),
+                                   tabB + ((((size_t)q1 * 2 + mu) * 2 + hl) * BROWS + n) * KP + kc * 8);
+                }
+                for (int i = pt; i < a.qs / 2; i += PRO_THREADS)
+                    tc::cp_async16(tc::smem_u32(&G.q1d[2 * i]), qtab + (size_t)q1 * a.qs + 2 * i);
+            }
+            for (int i = pt; i < ne * NMODE * 2 * H * (KP / 8); i += PRO_THREADS) {
+                int r = i;
+                const int kc = r % (KP / 8); r /= (KP / 8);
+                const int hl = r % H; r /= H;
+                const int mu = r % 2; r /= 2;
+                const int s2 = r % NMODE, e = r / NMODE;
+                tc::cp_async16(tc::smem_u32(&G.A[mu][hl][tc::kmajor_offset(tc_row(e, s2), kc * 8, LBO, SBO)]),
+                               tabA + ((((size_t)ent[e].y * 2 + mu) * 2 + hl) * NMODE + s2) * KP + kc * 8);
+            }
+            for (int i = pt; i < ne * 24; i += PRO_THREADS)  // 384-byte q0 rows into 400-byte slots
+                tc::cp_async16(tc::smem_u32(&G.q0d[i / 24][2 * (i % 24)]),
+                               q0tab + (size_t)ent[i / 24].x * Q0ROW + 2 * (i % 24));
+            for (int i = pt; i < ne * (a.qs / 2); i += PRO_THREADS) {
+                const int e = i / (a.qs / 2), k = i % (a.qs / 2);
+                tc::cp_async16(tc::smem_u32(&G.q2d[e][2 * k]), qtab + (size_t)ent[e].y * a.qs + 2 * k);
+            }
+            tc::cp_async_wait_all();
+            tc::fence_async_smem();
+            tc::named_bar(1, PRO_THREADS);
+            if (pt == 0) {
+                G.ne = ne;
+                G.q1 = q1;  // every producer thread has read the old value (newb) before the barrier
+                tc::mbar_arrive(tc::smem_u32(&S.ready[s]));
+                tc::fence_after_sync();
+                const uint32_t idesc = tc::idesc_bf16(128, 48);
+                for (int mu = 0; mu < 2; ++mu) {
+                    const uint32_t d = tm + (uint32_t)(s * 128 + mu * 64);
+                    for (int kk = 0; kk < KP / 16; ++kk) {
+                        const uint32_t ko = (uint32_t)kk * 2u * LBO;
+                        const uint64_t ah = tc::sdesc(tc::smem_u32(&G.A[mu][0][0]) + ko, LBO, SBO);
+                        const uint64_t bh = tc::sdesc(tc::smem_u32(&G.B[mu][0][0]) + ko, LBO, SBO);
+                        tc::mma_bf16(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                        if (SPLIT) {
+                            const uint64_t al = tc::sdesc(tc::smem_u32(&G.A[mu][1][0]) + ko, LBO, SBO);
+                            const uint64_t bl = tc::sdesc(tc::smem_u32(&G.B[mu][1][0]) + ko, LBO, SBO);
+                            tc::mma_bf16(d, ah, bl, idesc, 1u);
+                            tc::mma_bf16(d, al, bh, idesc, 1u);
+                        }
+                    }
+                }
+                tc::mma_commit(tc::smem_u32(&S.full[s]));
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int wq = warp & 3, h = warp >> 2;
+        const int e = 5 * wq + lane / NMODE, s2 = lane % NMODE;
+        const bool lane_ok = lane < 30;
+        const float Rf = (float)(sqrt(EXP_CUT / a.half_os2) * 1.0001 + 1e-3);
+        for (int t = t0, j = 0; t < t1; ++t, ++j) {
+            const int s = j & 1, u = j >> 1;
+            TcStage& G = S.st[s];
+            if (tid == 0)
+                S.abort_e = !(tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS) &&
+                              tc::mbar_wait(tc::smem_u32(&S.full[s]), (uint32_t)(u & 1), MAX_SPINS));
+            tc::named_bar(2, EPI_THREADS);
+            if (S.abort_e) {
+                if (tid == 0) atomicExch(err, 1);
+                break;
+            }
+            tc::fence_after_sync();
+            float y[2][48];
+            {
+                const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(s * 128);
+                tc::tmem_ld16(ta, y[0]);
+                tc::tmem_ld16(ta + 16, y[0] + 16);
+                tc::tmem_ld16(ta + 32, y[0] + 32);
+                tc::tmem_ld16(ta + 64, y[1]);
+                tc::tmem_ld16(ta + 80, y[1] + 16);
+                tc::tmem_ld16(ta + 96, y[1] + 32);
+                tc::tmem_ld_wait();
+            }
+            const int ne = G.ne;
+            const bool valid = lane_ok && e < ne;
+            const int4 en = valid ? G.ent[e] : make_int4(0, 0, 0, 0);
+            double acc[3][NTM + 1];
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                for (int T = 0; T <= NTM; ++T) acc[jj][T] = 0.0;
+            if (valid && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3)) {
+                const bool gq0 = en.w != 0, gq1 = G.q1 == 0;
+                const double* q1d = G.q1d;
+                const double* q2d = G.q2d[e];
+                const double* q0d = G.q0d[e];
+                const float2* E0 = reinterpret_cast<const float2*>(q0d);
+                const double w2 = q2d[s2], ob2v = q2d[6 + s2];
+                double n2[NTM];
+#pragma unroll
+                for (int T = 0; T < NTM; ++T) n2[T] = T < a.nT ? q2d[12 + 6 * T + s2] : 0.0;
+                float w1f[NMODE];
+#pragma unroll
+                for (int k = 0; k < NMODE; ++k) w1f[k] = (float)q1d[k];
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                    const int s0 = h * 3 + jj;
+                    if (s0 < a.lo[0] || s0 > a.hi[0]) continue;
+                    const double w0 = q0d[36 + s0];
+                    const float af = (float)(w0 - w2), bf = (float)(w0 + w2);
+                    // FP32 screen of the six s1: a bit for every triple inside the delta window
+                    unsigned act = 0u;
+#pragma unroll
+                    for (int s1 = 0; s1 < NMODE; ++s1) {
+                        const float w1 = w1f[s1];
+                        const bool in = fabsf(af - w1) < Rf || fabsf(af + w1) < Rf || fabsf(bf - w1) < Rf;
+                        const bool allowed = s1 >= a.lo[1] && s1 <= a.hi[1] && !(gq1 && s1 < 3);
+                        act |= (in && allowed) ? (1u << s1) : 0u;
+                    }
+                    const double obs = q0d[42 + s0] * ob2v;
+                    const float2* e0 = E0 + s0 * NMODE;
+                    while (act) {
+                        const int s1 = __ffs(act) - 1;
+                        act &= act - 1u;
+                        float yr[6], yi[6];  // (Re, Im) Y[mu][a] of this s1, k = mu*3 + a
+                        switch (s1) {
+#define SPRING_PICK(S1)                                                            \
+    case S1:                                                                       \
+        _Pragma("unroll") for (int k = 0; k < 6; ++k) {                            \
+            yr[k] = y[k / 3][(k % 3) * NMODE + S1];                                \
+            yi[k] = y[k / 3][18 + (k % 3) * NMODE + S1];                           \
+        }                                                                          \
+        break;
+                            SPRING_PICK(0) SPRING_PICK(1) SPRING_PICK(2) SPRING_PICK(3) SPRING_PICK(4)
+                            default: SPRING_PICK(5)
+#undef SPRING_PICK
+                        }
+                        const double w1d = q1d[s1];
+                        const double d1 = w0 - w1d - w2, d2 = w0 + w1d - w2, d3 = w0 - w1d + w2;
+                        const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2),
+                                     x3 = a.half_os2 * (d3 * d3);
+                        const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
+                        const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
+                        const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
+                        acc[jj][NTM] += e1 + e2 + e3;
+                        if (gq0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
+                        float pr = 0.0f, pim = 0.0f;
+#pragma unroll
+                        for (int k = 0; k < 6; ++k) {
+                            const float2 c = e0[k];
+                            pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
+                            pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+                        }
+                        const double W = (double)(pr * pr + pim * pim) * (obs * q1d[6 + s1]) * a.mfac;
+                        const double we1 = W * e1, wf2 = W * (e2 - e3);
+#pragma unroll
+                        for (int T = 0; T < NTM; ++T) {
+                            const double n1 = q1d[12 + 6 * (T < a.nT ? T : 0) + s1];
+                            acc[jj][T] += ((n1 + n2[T] + 1.0) * we1) + ((n1 - n2[T]) * wf2);
+                        }
+                    }
+                }
+            }
+            // sum the six rows (s2) of each pair: lanes 6k .. 6k+5 of the warp
+#pragma unroll
+            for (int jj = 0; jj < 3; ++jj)
+#pragma unroll
+                for (int T = 0; T <= NTM; ++T) {
+                    double v = acc[jj][T];
+#pragma unroll
+                    for (int off = 1; off < NMODE; off <<= 1) {
+                        const double o = __shfl_down_sync(0xffffffffu, v, off);
+                        if (s2 + off < NMODE) v += o;
+                    }
+                    acc[jj][T] = v;
+                }
+            if (valid && s2 == 0) {
+                const double wt = (double)en.z;
+#pragma unroll
+                for (int jj = 0; jj < 3; ++jj) {
+                    const int s0 = h * 3 + jj;
+#pragma unroll
+                    for (int T = 0; T < NTM; ++T)
+                        if (T < a.nT && acc[jj][T] != 0.0)
+                            atomicAdd(&out_lw[((size_t)T * a.nq0 + en.x) * NMODE + s0], wt * acc[jj][T]);
+                    if (acc[jj][NTM] != 0.0) atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * acc[jj][NTM]);
+                }
+            }
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[s]));
+        }
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (warp == 0) tc::tmem_dealloc(tm, 256);
+}
+
+template <int NTM, bool SPLIT>
+int launch_tc(spring_ctx* c, TcArgs a, double* lw, double* p3) {
+    const size_t smem = sizeof(TcSmem);
+    if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "tensor-core V3 needs %zu bytes of shared memory", smem);
+    cudaFuncSetAttribute(k_v3tc<NTM, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int ctas = std::max(1, std::min(a.ntiles, sms));
+    a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
+    const int grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
+    k_v3tc<NTM, SPLIT><<<grid, TC_THREADS, smem, c->stream>>>(
+        a, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_a.p),
+        reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->d_tc_q0.p, c->d_tc_q.p, lw, p3, c->d_tc_err.p);
+    return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
+}
+
+// Pairs of [p0, p1) sorted by q1 (stable radix sort), cut into tiles of at most EPT
+// pairs of one q1, with the entry record of every sorted pair.
+int build_tiles(spring_ctx* c, int p0, int p1) {
+    const PairSet& ps = c->ps_irr;
+    if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1) return SPRING_OK;
+    const int n = p1 - p0, nq = c->nq;
+    DBuf<int> keys, keys_s, vals, cnt, seg, ntl, toff;
+    int rc = SPRING_OK;
+    auto step = [&](int r) { if (rc == SPRING_OK) rc = r; };
+    step(dalloc(c, keys, std::max(n, 1), "tile keys"));
+    step(dalloc(c, keys_s, std::max(n, 1), "tile keys"));
+    step(dalloc(c, vals, std::max(n, 1), "tile values"));
+    step(dalloc(c, c->d_tc_entries, std::max(n, 1), "tile entries"));
+    step(dalloc(c, c->d_tc_rec, std::max(n, 1), "entry records"));
+    step(dalloc(c, cnt, nq, "tile counts"));
+    step(dalloc(c, seg, nq, "tile segments"));
+    step(dalloc(c, ntl, nq, "tile counts"));
+    step(dalloc(c, toff, nq, "tile offsets"));
+    if (rc == SPRING_OK) rc = zero(c, cnt.p, sizeof(int) * nq, "tile counts");
+    const int threads = 256;
+    if (rc == SPRING_OK && n > 0) {
+        if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
+        else {
+            k_tc_keys<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(n, p0, ps.pairs.p, keys.p,
+                                                                                                   vals.p, cnt.p);
+            rc = launch_check(c, "k_tc_keys");
+        }
+    }
+    int bits = 1;
+    while ((1 << bits) < nq) ++bits;
+    if (rc == SPRING_OK && n > 0) {
+        size_t bytes = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys_s.p, vals.p, c->d_tc_entries.p, n, 0, bits, c->stream);
+        DBuf<uint8_t> tmp;
+        rc = dalloc(c, tmp, std::max<size_t>(bytes, 1), "sort scratch");
+        if (rc == SPRING_OK) {
+            cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_s.p, vals.p, c->d_tc_entries.p, n,
+                                                            0, bits, c->stream);
+            c->launches += 1;
+            if (e != cudaSuccess) rc = cuda_fail(c, e, "pair sort");
+        }
+        cudaStreamSynchronize(c->stream);
+        dfree(tmp);
+    }
+    if (rc == SPRING_OK) rc = run_exclusive_scan(c, cnt.p, seg.p, nq);
+    if (rc == SPRING_OK) {
+        if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
+        else {
+            k_tc_ntiles<<<(nq + threads - 1) / threads, threads, 0, c->stream>>>(nq, cnt.p, ntl.p);
+            rc = launch_check(c, "k_tc_ntiles");
+        }
+    }
+    if (rc == SPRING_OK) rc = run_exclusive_scan(c, ntl.p, toff.p, nq);
+    int last[2] = {0, 0};
+    if (rc == SPRING_OK) rc = d2h(c, &last[0], toff.p + nq - 1, sizeof(int), "tile count");
+    if (rc == SPRING_OK) rc = d2h(c, &last[1], ntl.p + nq - 1, sizeof(int), "tile count");
+    const int ntiles = last[0] + last[1];
+    if (rc == SPRING_OK) rc = dalloc(c, c->d_tc_tiles, std::max(ntiles, 1), "tiles");
+    if (rc == SPRING_OK) {
+        if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
+        else {
+            k_tc_tiles<<<(nq + threads - 1) / threads, threads, 0, c->stream>>>(nq, cnt.p, seg.p, toff.p, c->d_tc_tiles.p);
+            rc = launch_check(c, "k_tc_tiles");
+        }
+    }
+    if (rc == SPRING_OK && n > 0) {
+        if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
+        else {
+            k_tc_entrec<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
+                n, c->d_tc_entries.p, ps.pairs.p, ps.pair_q0.p, c->d_irr_int.p, c->d_tc_rec.p);
+            rc = launch_check(c, "k_tc_entrec");
+        }
+    }
+    cudaStreamSynchronize(c->stream);
+    dfree(keys); dfree(keys_s); dfree(vals); dfree(cnt); dfree(seg); dfree(ntl); dfree(toff);
+    if (rc != SPRING_OK) return rc;
+    c->tc_ntiles = ntiles;
+    c->tc_gen = ps.gen;
+    c->tc_p0 = p0;
+    c->tc_p1 = p1;
+    return SPRING_OK;
+}
+
+}  // namespace
+
+int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
+                   bool* handled) {
+    *handled = false;
+    if (c->nb != 2 || c->na3 > 8 || c->nT > 9) return SPRING_OK;
+    const PairSet& ps = c->ps_irr;
+    const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
+    *handled = true;
+    if (p1 == p0) return SPRING_OK;
+    const int nq = c->nq;
+    const int qs = 12 + 6 * c->nT;
+    SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 2 * 2 * NMODE * KP, "V3 A table"));
+    SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 2 * 2 * BROWS * KP, "V3 B table"));
+    SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * Q0ROW, "V3 q0 rows"));
+    SPRING_CHECK(dalloc(c, c->d_tc_q, (size_t)nq * qs, "V3 grid rows"));
+    SPRING_CHECK(dalloc(c, c->d_tc_err, 1, "V3 status"));
+    SPRING_CHECK(zero(c, c->d_tc_err.p, sizeof(int), "V3 status"));
+    SPRING_CHECK(build_tiles(c, p0, p1));
+    const int threads = 256;
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+    {
+        const long long tot = (long long)nq * 2 * NMODE * KP;
+        k_tc_tab_a<<<(int)std::min<long long>((tot + threads - 1) / threads, 148LL * 16), threads, 0, c->stream>>>(
+            nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
+            reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
+        SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
+    }
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+    k_tc_tab_b<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
+                                               c->d_qpnt.p, c->ph_grid.evec.p,
+                                               reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
+    SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+    k_tc_q0tab<<<std::max(1, std::min((c->nq0 * 48 + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
+        c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p, c->d_tc_q0.p);
+    SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+    k_tc_qtab<<<std::max(1, (int)std::min<long long>(((long long)nq * qs + threads - 1) / threads, 148LL * 8)), threads,
+                0, c->stream>>>(nq, c->nT, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_tc_q.p);
+    SPRING_CHECK(launch_check(c, "k_tc_qtab"));
+
+    TcArgs a{};
+    a.nq = nq;
+    a.nq0 = c->nq0;
+    a.nT = c->nT;
+    a.qs = qs;
+    a.ntiles = c->tc_ntiles;
+    for (int k = 0; k < 3; ++k) {
+        a.lo[k] = pol.lo[k];
+        a.hi[k] = pol.hi[k];
+    }
+    a.mfac = host_constants().Sctr3THz2 / double(nq);
+    const double os = 1.0 / sigma;
+    a.half_os2 = 0.5 * (os * os);
+    a.pre = os * ONEBYSQRT2PI;
+    const bool split = c->precision == SPRING_BF16X3;
+    int rc;
+    if (c->nT == 1) rc = split ? launch_tc<1, true>(c, a, d_lw, d_p3) : launch_tc<1, false>(c, a, d_lw, d_p3);
+    else if (c->nT <= 3) rc = split ? launch_tc<3, true>(c, a, d_lw, d_p3) : launch_tc<3, false>(c, a, d_lw, d_p3);
+    else rc = split ? launch_tc<9, true>(c, a, d_lw, d_p3) : launch_tc<9, false>(c, a, d_lw, d_p3);
+    SPRING_CHECK(rc);
+    int herr = 0;
+    SPRING_CHECK(d2h(c, &herr, c->d_tc_err.p, sizeof(int), "V3 status"));
+    if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
+    return SPRING_OK;
+}
+
+}  // namespace spring

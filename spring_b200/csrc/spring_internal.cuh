@@ -45,6 +45,7 @@ struct PairSet {
     DBuf<int> pairpos;            // [q0][q1] exclusive-scan position of each representative
     std::vector<int> h_pairoff;
     bool done = false;
+    int gen = 0;                  // bumped every time the lists are rebuilt
 };
 
 // The q0 side of the V3 kernel: integer q0 vectors and the phonons of each q0.
@@ -63,6 +64,14 @@ struct Phonons {
     DBuf<double> oneby;              // [q][s]
     DBuf<double> nbe;                // [T][q][s]
     DBuf<double> vel;                // [q][s][3]
+    bool set = false;
+};
+
+// The surrogate network (k_mlp.cu): parameters, gradient, Adam moments, activations.
+struct Mlp {
+    DBuf<float> p, g, m, v, act, scal;
+    int cap = 0;          // rows the activation buffers hold
+    long long step = 0;   // Adam step
     bool set = false;
 };
 
@@ -163,6 +172,19 @@ struct spring_ctx {
     spring::DBuf<double> d_krn;    // [q0][s][9]
     spring::DBuf<double> d_rxyz;
     spring::DBuf<double> d_wiso;   // [slot][q1][s0][s1]
+
+    // tensor-core V3 (spring_set_precision): operand tables and pair tiles grouped by q1
+    spring::DBuf<uint16_t> d_tc_a;     // bf16 [q][mu][hi, lo][s][48]
+    spring::DBuf<uint16_t> d_tc_b;     // bf16 [q1][mu][hi, lo][36][48]
+    spring::DBuf<double> d_tc_q0;      // packed q0 rows: e0' float2[36], omega[6], 1/omega[6]
+    spring::DBuf<double> d_tc_q;       // packed grid rows: omega[6], 1/omega[6], nBE[T][6]
+    spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
+    spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
+    spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
+    spring::DBuf<int> d_tc_err;
+    int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1;
+
+    spring::Mlp mlp;
 };
 
 namespace spring {
@@ -222,6 +244,9 @@ int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first
 // k_v3s.cu: specialised V3 for two-atom cells; *handled is false when the cell does not fit it
 int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
                const Pol* pol, double* lw, double* p3, double* w, bool* handled);
+// k_v3tc.cu: tensor-core V3 + Gaussian sum (BF16 / BF16x3) for two-atom cells; *handled false otherwise
+int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
+                   bool* handled);
 // k_4ph.cu
 int run_enumerate4_fortran(spring_ctx* c, int q0, int* d_all, int* d_perm, long long cap, long long* h_counts);
 int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const int* pol4, double* d_rate);
@@ -229,6 +254,15 @@ int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma,
 int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
              double* h_lw, double* h_omega);
 int path_points(const double* G, int n_nodes, const double* q_high_sym, double* qpoints, double* dist, int* zc);
+// k_mlp.cu: the surrogate network (row-major X[n][SPRING_MLP_INPUTS], y[n])
+int mlp_num_params();
+int run_mlp_init(spring_ctx* c, unsigned long long seed);
+int run_mlp_set(spring_ctx* c, const float* params);
+int run_mlp_loss_grad(spring_ctx* c, int n, const float* hX, const float* hy, float* loss, float* grad);
+int run_mlp_train(spring_ctx* c, int n, const float* hX, const float* hy, int epochs, int batch, float lr,
+                  unsigned long long seed, float* epoch_loss);
+int run_mlp_predict(spring_ctx* c, int n, const float* hX, float* hy, int bf16);
+void free_mlp(Mlp& m);
 // k_bte.cu
 int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters);
 // k_tetra.cu

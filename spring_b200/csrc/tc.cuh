@@ -113,6 +113,24 @@ static __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Plain arrive on an mbarrier (release semantics at CTA scope).
+static __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+// Barrier over a subset of the CTA's warps (ids 1..15; count a multiple of 32).
+static __device__ __forceinline__ void named_bar(uint32_t id, uint32_t count) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory");
+}
+
+// 16-byte global -> shared asynchronous copy and the wait for all of this thread's copies.
+static __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+static __device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // Byte offset of element (row, k) in the canonical K-major layout.
 static __host__ __device__ __forceinline__ uint32_t kmajor_offset(int row, int k, uint32_t lbo, uint32_t sbo) {
     return (uint32_t)(row >> 3) * sbo + (uint32_t)(k >> 3) * lbo + (uint32_t)(row & 7) * 16u + (uint32_t)(k & 7) * 2u;

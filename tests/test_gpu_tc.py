@@ -1,0 +1,71 @@
+"""Tensor-core (tcgen05) V3 in the fused Gaussian linewidth: BF16 and compensated BF16x3 against the
+FP64 GPU path and the CPU oracle.  Tolerances are the accuracy targets of the mixed-precision path:
+linewidths within 2 % and kappa within 1 % of FP64 (BF16), and 1e-4 / 1e-5 for the compensated form."""
+import numpy as np
+import pytest
+
+from oracle import driver as D
+from spring_b200 import synthetic as S
+from spring_b200.api import from_crystal
+
+pytestmark = pytest.mark.gpu
+
+TEMPS = [100.0, 300.0, 700.0]
+SIGMA = 0.3767
+
+
+@pytest.fixture(scope="module", params=[8, 12])
+def runs(request):
+    cr = S.build("rocksalt2")
+    N = request.param
+    st = D.Setup(cr, (N, N, N), TEMPS)
+    ctx, info = from_crystal(cr, (N, N, N), TEMPS, phonons={"grid": st.ph, "irr": st.ph0})
+    out = {}
+    for prec in ("fp64", "bf16x3", "bf16"):
+        ctx.set_precision(prec)
+        ctx.reset_linewidths()
+        lw, p3 = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
+        kap = ctx.kappa_rta(info["Rxyz"])
+        out[prec] = (lw, p3, kap)
+    ctx.set_precision("fp64")
+    yield N, ctx, info, out, st
+    ctx.close()
+
+
+@pytest.mark.parametrize("prec,lw_tol,k_tol", [("bf16x3", 1e-4, 1e-5), ("bf16", 2e-2, 1e-2)])
+def test_tc_linewidths_and_kappa_vs_fp64(runs, prec, lw_tol, k_tol):
+    N, ctx, info, out, _ = runs
+    lw64, p364, k64 = out["fp64"]
+    lw, p3, k = out[prec]
+    for it in range(len(TEMPS)):
+        big = lw64[it] > 1e-3 * lw64[it].max()   # every mode whose linewidth is not negligible
+        rel = np.abs(lw[it][big] - lw64[it][big]) / lw64[it][big]
+        assert rel.max() < lw_tol, (prec, it, rel.max())
+        diag = np.array([k64[it][0], k64[it][4], k64[it][8]])
+        kd = np.array([k[it][0], k[it][4], k[it][8]])
+        assert np.abs(kd / diag - 1).max() < k_tol, (prec, it, kd, diag)
+    # the delta weights stay FP64: the phase space differs only by the exp cut (< 4e-18 of a peak)
+    np.testing.assert_allclose(p3, p364, rtol=1e-10, atol=1e-12 * np.abs(p364).max())
+
+
+def test_tc_matches_oracle_at_8(runs):
+    N, ctx, info, out, st = runs
+    if N != 8:
+        pytest.skip("oracle comparison on the 8^3 mesh only")
+    lw, _, _ = out["bf16x3"]
+    for i0 in (0, 3, st.nq0 - 1):
+        ref = D.linewidth3_q0(st, i0, "gauss", SIGMA, it=1)["lw"]
+        big = ref > 1e-3 * ref.max()
+        assert (np.abs(lw[1, i0][big] - ref[big]) / ref[big]).max() < 1e-4
+
+
+def test_tc_pair_subset_and_repeat(runs):
+    """A q0 block smaller than the whole set, called twice (tile cache reuse), equals the full run."""
+    N, ctx, info, out, _ = runs
+    lw_all, _, _ = out["bf16x3"]
+    ctx.set_precision("bf16x3")
+    for _ in range(2):
+        ctx.reset_linewidths()
+        lw, _ = ctx.linewidth3(2, 3, "gauss", SIGMA)
+        np.testing.assert_allclose(lw, lw_all[:, 1:4], rtol=1e-12, atol=1e-15)
+    ctx.set_precision("fp64")
