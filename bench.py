@@ -1,12 +1,15 @@
 #!/usr/bin/env python
 """Throughput of the 3-phonon scattering path on B200: one JSON line on stdout.
 
-Workload (BASELINE config "3-phonon at 24x24x24, T = 100/300/700 K" on the
-rocksalt crystal of config 1): fcc rocksalt 2-atom cell, seeded spring-model
-FC2 and FC3, 24^3 Gamma-centred mesh (13824 q, 413 irreducible q0), Gaussian
-smearing sigma = 2 cm^-1.  One step = the whole path for all temperatures:
-device phonons for the grid and the irreducible set, pair enumeration for every
-q0, V3 -> W -> Gaussian delta sum for every pair, RTA kappa (symmetrised).
+Workload: fcc rocksalt 2-atom cell (a = 4.21 A, Mg/O), seeded spring-model FC2
+and FC3, 24^3 Gamma-centred mesh (13824 q, 413 irreducible q0), T = 100/300/700 K,
+Gaussian smearing sigma = 2 cm^-1.  One step = the whole path for all
+temperatures: device phonons for the grid and the irreducible set, pair
+enumeration for every q0, V3 -> W -> Gaussian delta sum for every pair, RTA
+kappa (symmetrised).  V3 runs on the tensor cores (--precision, default the
+compensated BF16x3; phonons, deltas, rates and kappa stay FP64); the plain FP64
+path is timed in the same run, and the line reports the time-to-kappa of both
+and the largest linewidth and kappa error of the measured path against FP64.
 
 metric: 3-phonon scattering evaluations per second, one evaluation = one mode
 triple (s0,s1,s2) of one enumerated pair (sum over q0 of npairs * Ndof^3 per
@@ -49,6 +52,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
+                    help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
     return ap.parse_args()
 
 
@@ -56,6 +61,19 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
     """V3 in the factored form: phase-weighted FC sum 4*27*sum_mu Na3^2, three
     eigenvector contractions 3*8*Ndof^4, |Phi|^2 scaling 3*Ndof^3."""
     return 4 * 27 * int(np.sum(np.asarray(na3_counts) ** 2)) + 3 * 8 * ndof ** 4 + 3 * ndof ** 3
+
+
+BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
+TC_EPT = 20         # pairs per tensor-core tile
+
+
+def tc_issued_flops_per_tile(passes):
+    """Two basis atoms x 3 K-steps x passes MMAs of M128 N48 K16."""
+    return 2 * 3 * passes * 2 * 128 * 48 * 16
+
+
+def tc_tiles(counts_by_q1):
+    return int(np.sum((np.asarray(counts_by_q1) + TC_EPT - 1) // TC_EPT))
 
 
 class Clocks:
@@ -219,9 +237,13 @@ def run_ours(args):
     irr = ctx.find_irr_q(W)
     nq0 = ctx.nq0
     ctx.compute_phonons(TEMPS)
-    counts = np.array([ctx.enumerate3(i + 1)[2][0] for i in range(nq0)])
+    enum = [ctx.enumerate3(i + 1) for i in range(nq0)]
+    counts = np.array([e[2][0] for e in enum])
     lo, hi = partition(counts, world, rank)
     my_pairs = int(counts[lo:hi].sum())
+    counts_by_q1 = np.bincount(np.concatenate([enum[i][1][:, 0] - 1 for i in range(lo, hi)] or [np.zeros(0, int)]),
+                               minlength=int(np.prod(mesh)))
+    del enum
     evals_total = int(counts.sum()) * cr.ndof ** 3
     flops_pair = algorithmic_flops_per_pair(cr.ndof, cr.fc3_atm_num)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -239,14 +261,16 @@ def run_ours(args):
             ctx.set_linewidths(lw.cpu().numpy())
         ctx.kappa_rta(Rxyz, want=False)
 
-    with torch.cuda.stream(stream):
+    def timed(prec, clocks=None):
+        """K steps of the whole path with V3 in `prec`: (ms per step, launches, kernel times, lw, kappa)."""
+        ctx.set_precision(prec)
         for _ in range(args.warmup):
             step()
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
-        clocks = Clocks(local)
-        clocks.start()
+        if clocks:
+            clocks.start()
         ctx.set_profiling(True)
         l0 = ctx.kernel_launches()
         times = []
@@ -260,15 +284,29 @@ def run_ours(args):
             times.append(e0.elapsed_time(e1))
         torch.cuda.synchronize()
         launches = ctx.kernel_launches() - l0
-        v3_ms, v3_n = ctx.kernel_time("k_v3")
+        kt = {k: ctx.kernel_time(k) for k in ("k_v3tc", "k_v3s", "k_v3<", "k_phonons", "k_tc_tab", "k_kappa")}
         ctx.set_profiling(False)
-        clk = clocks.stop()
+        clk = clocks.stop() if clocks else None
         ms = float(np.sum(times)) / args.steps
         if world > 1:
             t = torch.tensor([ms], dtype=torch.float64, device=dev)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ms = float(t.item())
             dist.barrier()
+        lw = ctx.get_linewidths()
+        kap = ctx.kappa_rta(Rxyz)
+        return ms, launches, kt, lw, kap, clk
+
+    with torch.cuda.stream(stream):
+        ms64, _, kt64, lw64, kap64, _ = timed("fp64")
+        clocks = Clocks(local)
+        ms, launches, kt, lw_p, kap_p, clk = timed(args.precision, clocks)
+        big = lw64 > 1e-3 * lw64.max(axis=(1, 2), keepdims=True)
+        lw_err = float((np.abs(lw_p - lw64)[big] / lw64[big]).max())
+        diag = [0, 4, 8]
+        k_err = float(np.abs(kap_p[:, diag] / kap64[:, diag] - 1.0).max())
+        main_kernel = "k_v3tc" if args.precision != "fp64" else "k_v3s"
+        v3_ms, v3_n = kt[main_kernel] if kt[main_kernel][1] else kt["k_v3<"]
 
         # end to end through the public API: host inputs, pinned, copied every step
         pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -304,6 +342,7 @@ def run_ours(args):
                 ctx.set_linewidths(lw.cpu().numpy())
             ctx.kappa_rta(Rxyz, out=h_kap)
 
+        ctx.set_precision(args.precision)
         for _ in range(max(1, args.warmup)):
             step_e2e()
         torch.cuda.synchronize()
@@ -335,21 +374,41 @@ def run_ours(args):
     if rank == 0:
         value = evals_total / (ms * 1e-3)
         v3_per_launch = v3_ms / max(v3_n, 1)
-        achieved = flops_pair * my_pairs / (v3_per_launch * 1e-3) / 1e12 if v3_n else None
+        fp64_kernel_ms = kt64["k_v3s"][0] / max(kt64["k_v3s"][1], 1) if kt64["k_v3s"][1] else None
+        if args.precision == "fp64":
+            achieved = flops_pair * my_pairs / (v3_per_launch * 1e-3) / 1e12 if v3_n else None
+            roof = {"kernel": "k_v3s<gauss>", "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if (achieved and peak) else None, "traffic": None,
+                    "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json holds no FP64)"}
+        else:
+            passes = 3 if args.precision == "bf16x3" else 1
+            issued = tc_issued_flops_per_tile(passes) * tc_tiles(counts_by_q1)
+            achieved = issued / (v3_per_launch * 1e-3) / 1e12 if v3_n else None
+            roof = {"kernel": f"k_v3tc<{args.precision}>", "bound": "tensor", "achieved": achieved,
+                    "peak": BF16_PEAK, "unit": "TFLOP/s", "frac": (achieved / BF16_PEAK) if achieved else None,
+                    "traffic": None,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM) of measured",
+                    "issued_flops_per_launch": issued,
+                    "note": "issued tcgen05 MMA flops (M128 N48 K16 tiles, padding included); the kernel is bound "
+                            "by its epilogue and operand gathers, not by the tensor pipe"}
+        roof.update({"kernel_ms_per_launch": v3_per_launch, "kernel_share_of_step": v3_per_launch / ms,
+                     "algorithmic_fp64_flops_per_pair": flops_pair})
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "vs_baseline": None, "dtype": args.precision, "data": "synthetic",
                 "config": {"workload": WORKLOAD, "mesh": list(mesh), "irreducible_q0": nq0,
                            "pairs": int(counts.sum()), "temperatures": TEMPS, "sigma_rad_ps": SIGMA,
                            "delta": DELTA, "parallelism": f"q0-partition x{world}",
+                           "v3_arithmetic": args.precision,
+                           "fp64_parts": "phonons, deltas, rates and kappa",
                            "l2": "256 MiB buffer written between timed steps, outside the events"},
-                "roofline": {"kernel": "k_v3<gauss>", "bound": "fp64", "achieved": achieved, "peak": peak,
-                             "unit": "TFLOP/s", "frac": (achieved / peak) if (achieved and peak) else None,
-                             "traffic": None, "algorithmic_flops_per_pair": flops_pair,
-                             "kernel_ms_per_launch": v3_per_launch,
-                             "kernel_share_of_step": v3_per_launch / ms,
-                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run "
-                                            "(MEASURED_PEAKS.json holds no FP64 figure)"},
+                "time_to_kappa": {"ms": ms, "fp64_gpu_ms": ms64, "fp64_gpu_over_this": ms64 / ms,
+                                  "kappa_max_rel_err_vs_fp64": k_err, "linewidth_max_rel_err_vs_fp64": lw_err,
+                                  "fp64_v3_kernel_ms": fp64_kernel_ms,
+                                  "what": "one step = phonons + pairs + linewidths at 3 T + RTA kappa; errors over "
+                                          "every mode with a linewidth above 1e-3 of the largest, kappa diagonal"},
+                "fp64_path": {"value": evals_total / (ms64 * 1e-3), "unit": "evals/s", "ms_per_step": ms64},
+                "roofline": roof,
                 "cpu_baseline": cpu,
                 "e2e": {"value": evals_total / (e2e_ms * 1e-3), "unit": "evals/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

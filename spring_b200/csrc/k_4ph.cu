@@ -31,7 +31,7 @@ namespace spring {
 namespace {
 
 constexpr int NB = 2, N = 6, NA_MAX = 8, QB = 2;
-constexpr double EXP_UNDERFLOW = 745.2;
+constexpr double EXP_CUT = 40.0;  // exp(-40) = 4e-18 of a delta's peak: terms below it are dropped
 
 __device__ __forceinline__ int imod(int a, int n) {
     int r = a % n;
@@ -139,6 +139,8 @@ struct V4Smem {
     double2 phi[QB][1296];         // Phi, then W (as doubles in .x)
     double lw[MAX_NDOF][10];       // [s0][T] rate accumulators (T <= 9), last column unused
     double ph[QB][3][NA_MAX][2];
+    double wq[QB][3][N];           // omega of the quartet's three grid points
+    double nq[QB][9][3][N];        // their occupations per temperature
     int g[QB][4];                  // g1 g2 g3 valid
 };
 
@@ -329,9 +331,20 @@ k_v4(V4Args a, const int4* __restrict__ quart, const double* __restrict__ fc4, c
         }
         if (EPI == 0) {
             __syncthreads();
-            // Gaussian: every distinct ordering (qa, qb, qc) of the quartet's grid points
+            // Gaussian: every distinct ordering (qa, qb, qc) of the quartet's grid points.  The
+            // frequencies and occupations of the three points are staged; each (mode quad, ordering)
+            // is screened in FP32 against the window where a delta weight exceeds exp(-40) of its
+            // peak, and only the rest is evaluated in FP64.
+            for (int i = tid; i < QB * 3 * N; i += nt) {
+                const int p = i / (3 * N), k = (i / N) % 3, sx = i % N;
+                const int gg = S.g[p][k];
+                S.wq[p][k][sx] = omg[(size_t)gg * N + sx];
+                for (int t = 0; t < a.nT; ++t) S.nq[p][t][k][sx] = nbeg[(size_t)t * a.nq * N + (size_t)gg * N + sx];
+            }
+            __syncthreads();
             const int perms[6][3] = {{0, 1, 2}, {0, 2, 1}, {1, 0, 2}, {1, 2, 0}, {2, 0, 1}, {2, 1, 0}};
             const double pre = a.onebysigma * ONEBYSQRT2PI;
+            const float Rf = (float)(sqrt(2.0 * EXP_CUT) / a.onebysigma * 1.0001 + 1e-3);
             for (int i = tid; i < QB * 1296; i += nt) {
                 const int p = i / 1296, k = i % 1296;
                 if (!S.g[p][3]) continue;
@@ -342,30 +355,34 @@ k_v4(V4Args a, const int4* __restrict__ quart, const double* __restrict__ fc4, c
                     continue;
                 const int* G = S.g[p];
                 const double w0 = om0[s0];
+                const float f0 = (float)w0;
                 for (int pi = 0; pi < 6; ++pi) {
-                    const int ga = G[perms[pi][0]], gb = G[perms[pi][1]], gc = G[perms[pi][2]];
+                    const int ia = perms[pi][0], ib = perms[pi][1], ic = perms[pi][2];
+                    const int ga = G[ia], gb = G[ib];
                     bool dup = false;
                     for (int pj = 0; pj < pi; ++pj)
                         dup = dup || (G[perms[pj][0]] == ga && G[perms[pj][1]] == gb);
                     if (dup) continue;
+                    const double wa = S.wq[p][ia][sa], wb = S.wq[p][ib][sb], wc = S.wq[p][ic][sc];
+                    const float fa = (float)wa, fb = (float)wb, fc = (float)wc;
+                    if (fabsf(f0 - (fa + fb + fc)) >= Rf && fabsf(f0 - (fb + fc - fa)) >= Rf &&
+                        fabsf(f0 - (fc - fa - fb)) >= Rf)
+                        continue;
                     int m[3];
-                    m[perms[pi][0]] = sa;
-                    m[perms[pi][1]] = sb;
-                    m[perms[pi][2]] = sc;
+                    m[ia] = sa;
+                    m[ib] = sb;
+                    m[ic] = sc;
                     const double Wv = S.phi[p][((s0 * 6 + m[0]) * 6 + m[1]) * 6 + m[2]].x;
                     if (Wv == 0.0) continue;
-                    const double wa = omg[(size_t)ga * N + sa], wb = omg[(size_t)gb * N + sb], wc = omg[(size_t)gc * N + sc];
                     const double d1 = w0 - (wa + wb + wc), d2 = w0 - (wb + wc - wa), d3 = w0 - (wc - wa - wb);
                     const double x1 = 0.5 * a.onebysigma2 * (d1 * d1), x2 = 0.5 * a.onebysigma2 * (d2 * d2),
                                  x3 = 0.5 * a.onebysigma2 * (d3 * d3);
-                    const double e1 = x1 < EXP_UNDERFLOW ? pre * exp(-x1) : 0.0;
-                    const double e2 = x2 < EXP_UNDERFLOW ? pre * exp(-x2) : 0.0;
-                    const double e3 = x3 < EXP_UNDERFLOW ? pre * exp(-x3) : 0.0;
+                    const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
+                    const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
+                    const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
                     if (e1 == 0.0 && e2 == 0.0 && e3 == 0.0) continue;
                     for (int t = 0; t < a.nT; ++t) {
-                        const double* nb = nbeg + (size_t)t * a.nq * N;
-                        const double na_ = nb[(size_t)ga * N + sa], nbb = nb[(size_t)gb * N + sb],
-                                     nc = nb[(size_t)gc * N + sc];
+                        const double na_ = S.nq[p][t][ia][sa], nbb = S.nq[p][t][ib][sb], nc = S.nq[p][t][ic][sc];
                         const double n0 = nbe0[(size_t)t * a.nq0 * N + s0];
                         const double v = ONEBYSIX * (Wv * (na_ * nbb * nc / n0)) * e1 +
                                          0.5 * (Wv * ((1.0 + na_) * nbb * nc / n0)) * e2 +
