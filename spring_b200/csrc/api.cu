@@ -255,6 +255,8 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_q); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles); dfree(c->d_tc_err);
         free_mlp(c->mlp);
+        dfree(c->d_scr_rep); dfree(c->d_tc_keys); dfree(c->d_tc_keys_s); dfree(c->d_tc_vals); dfree(c->d_tc_cnt);
+        dfree(c->d_tc_seg); dfree(c->d_tc_ntl); dfree(c->d_tc_toff); dfree(c->d_tc_sort);
         dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);

@@ -113,7 +113,7 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
     ps.done = false;
     const long long total = (long long)ps.n0 * c->nq;
     if (total > 0x7fffffffLL) return fail(c, SPRING_ERR_UNSUPPORTED, "Nq0 * Nq exceeds 2^31");
-    DBuf<int> rep;
+    DBuf<int>& rep = c->d_scr_rep;
     SPRING_CHECK(dalloc(c, ps.partner, total, "partner map"));
     int rc = dalloc(c, rep, total, "representative flags");
     if (rc == SPRING_OK) rc = dalloc(c, ps.pairpos, total, "pair positions");
@@ -143,7 +143,6 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
         ps.h_pairoff.assign(ps.n0 + 1, 0);
         rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
     }
-    dfree(rep);
     if (rc == SPRING_OK) {
         ps.done = true;
         ps.gen += 1;

@@ -147,17 +147,18 @@ __global__ void k_tc_q0tab(int nq0, const double2* __restrict__ ev0, const doubl
     }
 }
 
-// Packed grid rows (QS = 12 + 6 nT doubles): omega[6], 1/omega[6], nBE[T][6].
-__global__ void k_tc_qtab(int nq, int nT, const double* __restrict__ omg, const double* __restrict__ obg,
+// Packed grid rows (qs = 12 + 6 x the kernel's temperature bucket doubles): omega[6], 1/omega[6],
+// nBE[T][6] (zero beyond the n_temps in use).
+__global__ void k_tc_qtab(int nq, int nT, int qs, const double* __restrict__ omg, const double* __restrict__ obg,
                           const double* __restrict__ nbeg, double* __restrict__ out) {
-    const int qs = 12 + 6 * nT;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * qs;
          i += (long long)gridDim.x * blockDim.x) {
         const int q = (int)(i / qs), k = (int)(i % qs);
         double v;
         if (k < 6) v = omg[(size_t)q * NMODE + k];
         else if (k < 12) v = obg[(size_t)q * NMODE + k - 6];
-        else v = nbeg[((size_t)((k - 12) / NMODE) * nq + q) * NMODE + (k - 12) % NMODE];
+        else if ((k - 12) / NMODE < nT) v = nbeg[((size_t)((k - 12) / NMODE) * nq + q) * NMODE + (k - 12) % NMODE];
+        else v = 0.0;
         out[i] = v;
     }
 }
@@ -243,6 +244,7 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int H = SPLIT ? 2 : 1;
+    constexpr int QS = 12 + 6 * NTM, QCH = QS / 2;  // packed grid row (the table is laid out for NTM)
     const int t0 = blockIdx.x * a.tiles_per_cta;
     const int t1 = min(a.ntiles, t0 + a.tiles_per_cta);
 
@@ -301,8 +303,8 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                     tc::cp_async16(tc::smem_u32(&G.B[mu][hl][tc::kmajor_offset(n, kc * 8, LBO, SBO)]),
                                    tabB + ((((size_t)q1 * 2 + mu) * 2 + hl) * BROWS + n) * KP + kc * 8);
                 }
-                for (int i = pt; i < a.qs / 2; i += PRO_THREADS)
-                    tc::cp_async16(tc::smem_u32(&G.q1d[2 * i]), qtab + (size_t)q1 * a.qs + 2 * i);
+                for (int i = pt; i < QCH; i += PRO_THREADS)
+                    tc::cp_async16(tc::smem_u32(&G.q1d[2 * i]), qtab + (size_t)q1 * QS + 2 * i);
             }
             for (int i = pt; i < ne * NMODE * 2 * H * (KP / 8); i += PRO_THREADS) {
                 int r = i;
@@ -316,9 +318,9 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
             for (int i = pt; i < ne * 24; i += PRO_THREADS)  // 384-byte q0 rows into 400-byte slots
                 tc::cp_async16(tc::smem_u32(&G.q0d[i / 24][2 * (i % 24)]),
                                q0tab + (size_t)ent[i / 24].x * Q0ROW + 2 * (i % 24));
-            for (int i = pt; i < ne * (a.qs / 2); i += PRO_THREADS) {
-                const int e = i / (a.qs / 2), k = i % (a.qs / 2);
-                tc::cp_async16(tc::smem_u32(&G.q2d[e][2 * k]), qtab + (size_t)ent[e].y * a.qs + 2 * k);
+            for (int i = pt; i < ne * QCH; i += PRO_THREADS) {
+                const int e = i / QCH, k = i % QCH;
+                tc::cp_async16(tc::smem_u32(&G.q2d[e][2 * k]), qtab + (size_t)ent[e].y * QS + 2 * k);
             }
             tc::cp_async_wait_all();
             tc::fence_async_smem();
@@ -515,7 +517,8 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
     const PairSet& ps = c->ps_irr;
     if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1) return SPRING_OK;
     const int n = p1 - p0, nq = c->nq;
-    DBuf<int> keys, keys_s, vals, cnt, seg, ntl, toff;
+    DBuf<int>&keys = c->d_tc_keys, &keys_s = c->d_tc_keys_s, &vals = c->d_tc_vals, &cnt = c->d_tc_cnt,
+              &seg = c->d_tc_seg, &ntl = c->d_tc_ntl, &toff = c->d_tc_toff;
     int rc = SPRING_OK;
     auto step = [&](int r) { if (rc == SPRING_OK) rc = r; };
     step(dalloc(c, keys, std::max(n, 1), "tile keys"));
@@ -542,7 +545,7 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
     if (rc == SPRING_OK && n > 0) {
         size_t bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys_s.p, vals.p, c->d_tc_entries.p, n, 0, bits, c->stream);
-        DBuf<uint8_t> tmp;
+        DBuf<uint8_t>& tmp = c->d_tc_sort;
         rc = dalloc(c, tmp, std::max<size_t>(bytes, 1), "sort scratch");
         if (rc == SPRING_OK) {
             cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp.p, bytes, keys.p, keys_s.p, vals.p, c->d_tc_entries.p, n,
@@ -550,8 +553,6 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
             c->launches += 1;
             if (e != cudaSuccess) rc = cuda_fail(c, e, "pair sort");
         }
-        cudaStreamSynchronize(c->stream);
-        dfree(tmp);
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, cnt.p, seg.p, nq);
     if (rc == SPRING_OK) {
@@ -582,8 +583,6 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
             rc = launch_check(c, "k_tc_entrec");
         }
     }
-    cudaStreamSynchronize(c->stream);
-    dfree(keys); dfree(keys_s); dfree(vals); dfree(cnt); dfree(seg); dfree(ntl); dfree(toff);
     if (rc != SPRING_OK) return rc;
     c->tc_ntiles = ntiles;
     c->tc_gen = ps.gen;
@@ -603,7 +602,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     *handled = true;
     if (p1 == p0) return SPRING_OK;
     const int nq = c->nq;
-    const int qs = 12 + 6 * c->nT;
+    const int ntm = c->nT == 1 ? 1 : (c->nT <= 3 ? 3 : 9);  // temperature bucket of the kernel instance
+    const int qs = 12 + 6 * ntm;
     SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 2 * 2 * NMODE * KP, "V3 A table"));
     SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 2 * 2 * BROWS * KP, "V3 B table"));
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * Q0ROW, "V3 q0 rows"));
@@ -631,7 +631,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     k_tc_qtab<<<std::max(1, (int)std::min<long long>(((long long)nq * qs + threads - 1) / threads, 148LL * 8)), threads,
-                0, c->stream>>>(nq, c->nT, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_tc_q.p);
+                0, c->stream>>>(nq, c->nT, qs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_tc_q.p);
     SPRING_CHECK(launch_check(c, "k_tc_qtab"));
 
     TcArgs a{};

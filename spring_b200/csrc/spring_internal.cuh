@@ -183,6 +183,9 @@ struct spring_ctx {
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
     spring::DBuf<int> d_tc_err;
     int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1;
+    // scratch kept between calls (the enumeration and the tile sort run every step)
+    spring::DBuf<int> d_scr_rep, d_tc_keys, d_tc_keys_s, d_tc_vals, d_tc_cnt, d_tc_seg, d_tc_ntl, d_tc_toff;
+    spring::DBuf<uint8_t> d_tc_sort;
 
     spring::Mlp mlp;
 };
