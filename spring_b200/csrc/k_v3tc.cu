@@ -306,14 +306,26 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                 for (int i = pt; i < QCH; i += PRO_THREADS)
                     tc::cp_async16(tc::smem_u32(&G.q1d[2 * i]), qtab + (size_t)q1 * QS + 2 * i);
             }
-            for (int i = pt; i < ne * NMODE * 2 * H * (KP / 8); i += PRO_THREADS) {
-                int r = i;
-                const int kc = r % (KP / 8); r /= (KP / 8);
-                const int hl = r % H; r /= H;
-                const int mu = r % 2; r /= 2;
-                const int s2 = r % NMODE, e = r / NMODE;
-                tc::cp_async16(tc::smem_u32(&G.A[mu][hl][tc::kmajor_offset(tc_row(e, s2), kc * 8, LBO, SBO)]),
-                               tabA + ((((size_t)ent[e].y * 2 + mu) * 2 + hl) * NMODE + s2) * KP + kc * 8);
+            {
+                // A rows: warp pw takes pairs pw, pw+4, ...; lane l the (s2, k-chunk) slots l and l+32 of 36
+                const int pw = pt >> 5, pl = pt & 31;
+                const int c0 = pl, c1 = pl + 32;
+                const int s2a = c0 / (KP / 8), kca = c0 % (KP / 8);
+                const int s2b = c1 / (KP / 8), kcb = c1 % (KP / 8);
+                for (int e = pw; e < ne; e += PRO_THREADS / 32) {
+                    const __nv_bfloat16* src = tabA + (size_t)ent[e].y * (2 * 2 * NMODE * KP);
+                    const int ra = tc_row(e, s2a), rb = tc_row(e, s2b);
+#pragma unroll
+                    for (int mh = 0; mh < 2 * H; ++mh) {
+                        const int mu = mh / H, hl = mh % H;
+                        const __nv_bfloat16* sm = src + (size_t)(mu * 2 + hl) * NMODE * KP;
+                        uint8_t* dst = &G.A[mu][hl][0];
+                        tc::cp_async16(tc::smem_u32(dst + tc::kmajor_offset(ra, kca * 8, LBO, SBO)), sm + s2a * KP + kca * 8);
+                        if (c1 < NMODE * (KP / 8))
+                            tc::cp_async16(tc::smem_u32(dst + tc::kmajor_offset(rb, kcb * 8, LBO, SBO)),
+                                           sm + s2b * KP + kcb * 8);
+                    }
+                }
             }
             for (int i = pt; i < ne * 24; i += PRO_THREADS)  // 384-byte q0 rows into 400-byte slots
                 tc::cp_async16(tc::smem_u32(&G.q0d[i / 24][2 * (i % 24)]),
@@ -458,29 +470,18 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                     }
                 }
             }
-            // sum the six rows (s2) of each pair: lanes 6k .. 6k+5 of the warp
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                for (int T = 0; T <= NTM; ++T) {
-                    double v = acc[jj][T];
-#pragma unroll
-                    for (int off = 1; off < NMODE; off <<= 1) {
-                        const double o = __shfl_down_sync(0xffffffffu, v, off);
-                        if (s2 + off < NMODE) v += o;
-                    }
-                    acc[jj][T] = v;
-                }
-            if (valid && s2 == 0) {
+            // this row's (pair, s2) sums go straight to the output (few rows hold any)
+            if (valid) {
                 const double wt = (double)en.z;
 #pragma unroll
                 for (int jj = 0; jj < 3; ++jj) {
+                    if (acc[jj][NTM] == 0.0) continue;  // no active triple for this s0 in this row
                     const int s0 = h * 3 + jj;
 #pragma unroll
                     for (int T = 0; T < NTM; ++T)
                         if (T < a.nT && acc[jj][T] != 0.0)
                             atomicAdd(&out_lw[((size_t)T * a.nq0 + en.x) * NMODE + s0], wt * acc[jj][T]);
-                    if (acc[jj][NTM] != 0.0) atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * acc[jj][NTM]);
+                    atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * acc[jj][NTM]);
                 }
             }
             tc::fence_before_sync();
