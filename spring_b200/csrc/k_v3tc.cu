@@ -393,95 +393,73 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
             const int ne = G.ne;
             const bool valid = lane_ok && e < ne;
             const int4 en = valid ? G.ent[e] : make_int4(0, 0, 0, 0);
-            double acc[3][NTM + 1];
-#pragma unroll
-            for (int jj = 0; jj < 3; ++jj)
-#pragma unroll
-                for (int T = 0; T <= NTM; ++T) acc[jj][T] = 0.0;
-            if (valid && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3)) {
-                const bool gq0 = en.w != 0, gq1 = G.q1 == 0;
-                const double* q1d = G.q1d;
-                const double* q2d = G.q2d[e];
-                const double* q0d = G.q0d[e];
-                const float2* E0 = reinterpret_cast<const float2*>(q0d);
-                const double w2 = q2d[s2], ob2v = q2d[6 + s2];
-                double n2[NTM];
-#pragma unroll
-                for (int T = 0; T < NTM; ++T) n2[T] = T < a.nT ? q2d[12 + 6 * T + s2] : 0.0;
-                float w1f[NMODE];
-#pragma unroll
-                for (int k = 0; k < NMODE; ++k) w1f[k] = (float)q1d[k];
+            const bool row_on = valid && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
+            const bool gq0 = en.w != 0, gq1 = G.q1 == 0;
+            const double* q1d = G.q1d;
+            const double* q2d = G.q2d[valid ? e : 0];
+            const double* q0d = G.q0d[valid ? e : 0];
+            const double w2 = q2d[s2];
+            // FP32 screen: bit 6*jj + s1 marks (s0 = 3h + jj, s1) inside the delta window
+            unsigned act = 0u;
+            if (row_on) {
 #pragma unroll
                 for (int jj = 0; jj < 3; ++jj) {
                     const int s0 = h * 3 + jj;
                     if (s0 < a.lo[0] || s0 > a.hi[0]) continue;
                     const double w0 = q0d[36 + s0];
                     const float af = (float)(w0 - w2), bf = (float)(w0 + w2);
-                    // FP32 screen of the six s1: a bit for every triple inside the delta window
-                    unsigned act = 0u;
 #pragma unroll
                     for (int s1 = 0; s1 < NMODE; ++s1) {
-                        const float w1 = w1f[s1];
+                        const float w1 = (float)q1d[s1];
                         const bool in = fabsf(af - w1) < Rf || fabsf(af + w1) < Rf || fabsf(bf - w1) < Rf;
                         const bool allowed = s1 >= a.lo[1] && s1 <= a.hi[1] && !(gq1 && s1 < 3);
-                        act |= (in && allowed) ? (1u << s1) : 0u;
-                    }
-                    const double obs = q0d[42 + s0] * ob2v;
-                    const float2* e0 = E0 + s0 * NMODE;
-                    while (act) {
-                        const int s1 = __ffs(act) - 1;
-                        act &= act - 1u;
-                        float yr[6], yi[6];  // (Re, Im) Y[mu][a] of this s1, k = mu*3 + a
-                        switch (s1) {
-#define SPRING_PICK(S1)                                                            \
-    case S1:                                                                       \
-        _Pragma("unroll") for (int k = 0; k < 6; ++k) {                            \
-            yr[k] = y[k / 3][(k % 3) * NMODE + S1];                                \
-            yi[k] = y[k / 3][18 + (k % 3) * NMODE + S1];                           \
-        }                                                                          \
-        break;
-                            SPRING_PICK(0) SPRING_PICK(1) SPRING_PICK(2) SPRING_PICK(3) SPRING_PICK(4)
-                            default: SPRING_PICK(5)
-#undef SPRING_PICK
-                        }
-                        const double w1d = q1d[s1];
-                        const double d1 = w0 - w1d - w2, d2 = w0 + w1d - w2, d3 = w0 - w1d + w2;
-                        const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2),
-                                     x3 = a.half_os2 * (d3 * d3);
-                        const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
-                        const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
-                        const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
-                        acc[jj][NTM] += e1 + e2 + e3;
-                        if (gq0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
-                        float pr = 0.0f, pim = 0.0f;
-#pragma unroll
-                        for (int k = 0; k < 6; ++k) {
-                            const float2 c = e0[k];
-                            pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
-                            pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
-                        }
-                        const double W = (double)(pr * pr + pim * pim) * (obs * q1d[6 + s1]) * a.mfac;
-                        const double we1 = W * e1, wf2 = W * (e2 - e3);
-#pragma unroll
-                        for (int T = 0; T < NTM; ++T) {
-                            const double n1 = q1d[12 + 6 * (T < a.nT ? T : 0) + s1];
-                            acc[jj][T] += ((n1 + n2[T] + 1.0) * we1) + ((n1 - n2[T]) * wf2);
-                        }
+                        act |= (in && allowed) ? (1u << (jj * NMODE + s1)) : 0u;
                     }
                 }
             }
-            // this row's (pair, s2) sums go straight to the output (few rows hold any)
-            if (valid) {
+            // rounds: every lane with work takes its next triple, so the warp runs the FP64 path once
+            // per round for all of them; each triple's contribution goes straight to the output
+            while (__any_sync(0xffffffffu, act != 0u)) {
+                if (act == 0u) continue;
+                const int bit = __ffs(act) - 1;
+                act &= act - 1u;
+                const int jj = bit / NMODE, s1 = bit % NMODE, s0 = h * 3 + jj;
+                float yr[6], yi[6];  // (Re, Im) Y[mu][a] of this s1, k = mu*3 + a
+#pragma unroll
+                for (int k = 0; k < 6; ++k) {
+                    float r = 0.0f, im = 0.0f;
+#pragma unroll
+                    for (int c1 = 0; c1 < NMODE; ++c1) {
+                        r = (c1 == s1) ? y[k / 3][(k % 3) * NMODE + c1] : r;
+                        im = (c1 == s1) ? y[k / 3][18 + (k % 3) * NMODE + c1] : im;
+                    }
+                    yr[k] = r;
+                    yi[k] = im;
+                }
+                const double w0 = q0d[36 + s0], w1d = q1d[s1];
+                const double d1 = w0 - w1d - w2, d2 = w0 + w1d - w2, d3 = w0 - w1d + w2;
+                const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2), x3 = a.half_os2 * (d3 * d3);
+                const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
+                const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
+                const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
                 const double wt = (double)en.z;
+                const double p3 = e1 + e2 + e3;
+                if (p3 != 0.0) atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * p3);
+                if (gq0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
+                const float2* e0 = reinterpret_cast<const float2*>(q0d) + s0 * NMODE;
+                float pr = 0.0f, pim = 0.0f;
 #pragma unroll
-                for (int jj = 0; jj < 3; ++jj) {
-                    if (acc[jj][NTM] == 0.0) continue;  // no active triple for this s0 in this row
-                    const int s0 = h * 3 + jj;
-#pragma unroll
-                    for (int T = 0; T < NTM; ++T)
-                        if (T < a.nT && acc[jj][T] != 0.0)
-                            atomicAdd(&out_lw[((size_t)T * a.nq0 + en.x) * NMODE + s0], wt * acc[jj][T]);
-                    atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * acc[jj][NTM]);
+                for (int k = 0; k < 6; ++k) {
+                    const float2 c = e0[k];
+                    pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
+                    pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+                }
+                const double W = (double)(pr * pr + pim * pim) * (q0d[42 + s0] * q2d[6 + s2] * q1d[6 + s1]) * a.mfac;
+                const double we1 = wt * W * e1, wf2 = wt * W * (e2 - e3);
+                for (int T = 0; T < a.nT; ++T) {
+                    const double n1 = q1d[12 + 6 * T + s1], n2 = q2d[12 + 6 * T + s2];
+                    const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
+                    if (v != 0.0) atomicAdd(&out_lw[((size_t)T * a.nq0 + en.x) * NMODE + s0], v);
                 }
             }
             tc::fence_before_sync();
