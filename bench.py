@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mesh4", type=int, default=12, help="mesh of the four-phonon leg (0 skips it)")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
                     help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
     return ap.parse_args()
@@ -209,6 +210,64 @@ def partition(counts, world, rank):
     return lo, hi
 
 
+def fourph_leg(torch, mesh4, frac=0.1):
+    """Four-phonon leg: exact Gaussian 4-phonon rates of every irreducible q0 (FP64 V4) on a mesh4^3
+    mesh at 300 K, timed; then the surrogate (trained on exact rates of the 8^3 mesh) screens the q0
+    blocks, exact V4 runs for the top `frac`, and kappa is compared with the all-exact one."""
+    from spring_b200 import surrogate as SG
+    from spring_b200 import synthetic as S
+    from spring_b200.api import from_crystal
+    cr = S.build("rocksalt2", fc4=True)
+    T = [300.0]
+
+    def ev_ms(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return r, e0.elapsed_time(e1)
+
+    def mesh_data(N):
+        ctx, info = from_crystal(cr, (N, N, N), T, with_fc4=True)
+        ctx.reset_linewidths()
+        lw3 = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)[0][0]
+        r4, ms = ev_ms(lambda: ctx.linewidth4(1, ctx.nq0, "gauss", SIGMA)[0])
+        ph = ctx.get_phonons(1)
+        q = ((cr.G / N) @ info["irr_q_pnt_int"].T.astype(float)).T
+        X = SG.mode_features(ph["omega"], ph["grp_vel"], 2.0 * lw3, q)
+        return ctx, info, lw3, r4, ph, X, ms
+
+    c8, _, _, r8, _, X8, _ = mesh_data(8)
+    y = r8.ravel()
+    m = (y > 0) & (X8[:, 2] > 0)
+    sur = SG.Surrogate(c8, seed=1)
+    _, train_ms = ev_ms(lambda: sur.fit(X8[m], np.log(y[m]), epochs=600, batch=32, lr=2e-3))
+    c, info, lw3, r_ex, ph, X, exact_ms = mesh_data(mesh4)
+    quartets = sum(c.count4(i + 1)[0] for i in range(c.nq0))
+    pred, pred_ms = ev_ms(lambda: np.exp(sur.predict(X, bf16=True)).reshape(c.nq0, -1))
+    w = SG.kappa_weight(ph["omega"], ph["nbe"][0], ph["grp_vel"], info["multiplicity"])
+    order, _ = SG.rank_blocks(2.0 * lw3, pred, w)
+    (scr, mask), scr_ms = ev_ms(lambda: SG.screened_rates4(c, pred, order, frac, delta="gauss", sigma=SIGMA))
+
+    def kappa(r4):
+        c.set_linewidths((lw3 + 0.5 * r4)[None])
+        k = c.kappa_rta(info["Rxyz"])[0]
+        return float(np.mean([k[0], k[4], k[8]]))
+
+    k_ex, k_scr, k_wo = kappa(r_ex), kappa(scr), kappa(np.where(mask[:, None], r_ex, 0.0))
+    c.close()
+    c8.close()
+    return {"mesh": [mesh4] * 3, "temperature": 300.0, "irreducible_q0": int(len(order)), "quartets": int(quartets),
+            "evals_per_s_exact": quartets * 36 * 36 / (exact_ms * 1e-3), "exact_ms": exact_ms,
+            "screened_ms": scr_ms + pred_ms, "exact_over_screened": exact_ms / (scr_ms + pred_ms),
+            "fraction_exact": frac, "kappa_exact": k_ex, "kappa_rel_err_screened": abs(k_scr / k_ex - 1),
+            "kappa_rel_err_same_blocks_without_network": abs(k_wo / k_ex - 1), "train_ms_8cubed": train_ms,
+            "v4_arithmetic": "f64", "what": "one 4ph eval = one (s0..s3) of one quartet; surrogate 5-128-128-128-1 "
+                                            "SiLU, trained on the GPU on exact 8^3 rates, BF16 inference"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -363,6 +422,7 @@ def run_ours(args):
             e2e_ms = float(t.item())
 
     peak = fp64_peak_tflops(torch) if rank == 0 else None
+    four = fourph_leg(torch, args.mesh4) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ph_grid, ph_irr = ctx.get_phonons(0), ctx.get_phonons(1)
@@ -408,6 +468,7 @@ def run_ours(args):
                                   "what": "one step = phonons + pairs + linewidths at 3 T + RTA kappa; errors over "
                                           "every mode with a linewidth above 1e-3 of the largest, kappa diagonal"},
                 "fp64_path": {"value": evals_total / (ms64 * 1e-3), "unit": "evals/s", "ms_per_step": ms64},
+                "fourph": four,
                 "roofline": roof,
                 "cpu_baseline": cpu,
                 "e2e": {"value": evals_total / (e2e_ms * 1e-3), "unit": "evals/s", "ms_per_step": e2e_ms,

@@ -220,6 +220,12 @@ class Context:
         return A, Pm[: cnt[0]].copy(), (int(cnt[0]), int(cnt[1]))
 
     # -- MomentumConsrv4th
+    def count4(self, i0: int):
+        """(q1q2q3_count, total_count) of q0 = i0, without copying the lists back."""
+        cnt = np.zeros(2, np.int64)
+        self._call("spring_enumerate4", int(i0), None, None, 0, _ptr(cnt))
+        return int(cnt[0]), int(cnt[1])
+
     def enumerate4(self, i0: int, cap=None):
         """Allq1q2q3 [q1][q2][3], q1q2q3_permuted [quartet][3] (1-based) and (count, total_count)."""
         A = np.zeros((self.nq, self.nq, 3), np.int32)

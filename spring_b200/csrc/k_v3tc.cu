@@ -214,8 +214,19 @@ struct TcStage {
     int q1, ne;
 };
 
+// An active mode triple handed from the screening thread to any epilogue thread:
+// (Re, Im) Y[mu][a] for its s1, and (pair, s2, s0, s1).
+struct QItem {
+    float yr[6], yi[6];
+    int meta;  // e | s2 << 8 | s0 << 12 | s1 << 16
+    int pad[3];
+};
+constexpr int QCAP = 512;
+
 struct TcSmem {
     TcStage st[2];
+    QItem q[QCAP];     // active triples of the tile being reduced
+    int qn, qmore;
     int4 pf[2][EPT];   // entry records prefetched one tile ahead
     int4 trec[4];      // tile records prefetched two tiles ahead
     alignas(8) uint64_t ready[2], full[2], empty[2];
@@ -255,6 +266,7 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
     if (tid == 0) {
         S.st[0].q1 = S.st[1].q1 = -1;
         S.abort_p = S.abort_e = 0;
+        S.qn = S.qmore = 0;
         for (int k = 0; k < 2; ++k) {
             tc::mbar_init(tc::smem_u32(&S.ready[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
@@ -417,50 +429,76 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                     }
                 }
             }
-            // rounds: every lane with work takes its next triple, so the warp runs the FP64 path once
-            // per round for all of them; each triple's contribution goes straight to the output
-            while (__any_sync(0xffffffffu, act != 0u)) {
-                if (act == 0u) continue;
-                const int bit = __ffs(act) - 1;
-                act &= act - 1u;
-                const int jj = bit / NMODE, s1 = bit % NMODE, s0 = h * 3 + jj;
-                float yr[6], yi[6];  // (Re, Im) Y[mu][a] of this s1, k = mu*3 + a
+            // Compaction: the screened triples of the whole tile go to a shared queue (several passes if it
+            // fills), and all epilogue threads evaluate them one per thread, so the FP64 work runs with
+            // full warps; each triple's contribution goes straight to the output.
+            for (;;) {
+                if (act) {
+                    const int n = __popc(act);
+                    const int base = atomicAdd(&S.qn, n);
+                    for (int i = 0; i < n && base + i < QCAP; ++i) {
+                        const int bit = __ffs(act) - 1;
+                        act &= act - 1u;
+                        const int jj = bit / NMODE, s1 = bit % NMODE;
+                        QItem& it = S.q[base + i];
 #pragma unroll
-                for (int k = 0; k < 6; ++k) {
-                    float r = 0.0f, im = 0.0f;
+                        for (int k = 0; k < 6; ++k) {
+                            float r = 0.0f, im = 0.0f;
 #pragma unroll
-                    for (int c1 = 0; c1 < NMODE; ++c1) {
-                        r = (c1 == s1) ? y[k / 3][(k % 3) * NMODE + c1] : r;
-                        im = (c1 == s1) ? y[k / 3][18 + (k % 3) * NMODE + c1] : im;
+                            for (int c1 = 0; c1 < NMODE; ++c1) {
+                                r = (c1 == s1) ? y[k / 3][(k % 3) * NMODE + c1] : r;
+                                im = (c1 == s1) ? y[k / 3][18 + (k % 3) * NMODE + c1] : im;
+                            }
+                            it.yr[k] = r;
+                            it.yi[k] = im;
+                        }
+                        it.meta = e | (s2 << 8) | ((h * 3 + jj) << 12) | (s1 << 16);
                     }
-                    yr[k] = r;
-                    yi[k] = im;
+                    if (act) S.qmore = 1;
                 }
-                const double w0 = q0d[36 + s0], w1d = q1d[s1];
-                const double d1 = w0 - w1d - w2, d2 = w0 + w1d - w2, d3 = w0 - w1d + w2;
-                const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2), x3 = a.half_os2 * (d3 * d3);
-                const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
-                const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
-                const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
-                const double wt = (double)en.z;
-                const double p3 = e1 + e2 + e3;
-                if (p3 != 0.0) atomicAdd(&out_p3[(size_t)en.x * NMODE + s0], wt * p3);
-                if (gq0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
-                const float2* e0 = reinterpret_cast<const float2*>(q0d) + s0 * NMODE;
-                float pr = 0.0f, pim = 0.0f;
+                tc::named_bar(2, EPI_THREADS);
+                const int cnt = min(S.qn, QCAP);
+                for (int i = tid; i < cnt; i += EPI_THREADS) {
+                    const QItem& it = S.q[i];
+                    const int ie = it.meta & 0xff, is2 = (it.meta >> 8) & 0xf, s0 = (it.meta >> 12) & 0xf,
+                              s1 = (it.meta >> 16) & 0xf;
+                    const int4 ien = G.ent[ie];
+                    const double* p0 = G.q0d[ie];
+                    const double* p2 = G.q2d[ie];
+                    const double w0 = p0[36 + s0], w1d = q1d[s1], w2d = p2[is2];
+                    const double d1 = w0 - w1d - w2d, d2 = w0 + w1d - w2d, d3 = w0 - w1d + w2d;
+                    const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2), x3 = a.half_os2 * (d3 * d3);
+                    const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
+                    const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
+                    const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
+                    const double wt = (double)ien.z;
+                    const double p3 = e1 + e2 + e3;
+                    if (p3 != 0.0) atomicAdd(&out_p3[(size_t)ien.x * NMODE + s0], wt * p3);
+                    if (ien.w != 0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
+                    const float2* e0 = reinterpret_cast<const float2*>(p0) + s0 * NMODE;
+                    float pr = 0.0f, pim = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) {
-                    const float2 c = e0[k];
-                    pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
-                    pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+                    for (int k = 0; k < 6; ++k) {
+                        const float2 c = e0[k];
+                        pr = fmaf(c.x, it.yr[k], fmaf(-c.y, it.yi[k], pr));
+                        pim = fmaf(c.x, it.yi[k], fmaf(c.y, it.yr[k], pim));
+                    }
+                    const double W = (double)(pr * pr + pim * pim) * (p0[42 + s0] * p2[6 + is2] * q1d[6 + s1]) * a.mfac;
+                    const double we1 = wt * W * e1, wf2 = wt * W * (e2 - e3);
+                    for (int T = 0; T < a.nT; ++T) {
+                        const double n1 = q1d[12 + 6 * T + s1], n2 = p2[12 + 6 * T + is2];
+                        const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
+                        if (v != 0.0) atomicAdd(&out_lw[((size_t)T * a.nq0 + ien.x) * NMODE + s0], v);
+                    }
                 }
-                const double W = (double)(pr * pr + pim * pim) * (q0d[42 + s0] * q2d[6 + s2] * q1d[6 + s1]) * a.mfac;
-                const double we1 = wt * W * e1, wf2 = wt * W * (e2 - e3);
-                for (int T = 0; T < a.nT; ++T) {
-                    const double n1 = q1d[12 + 6 * T + s1], n2 = q2d[12 + 6 * T + s2];
-                    const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
-                    if (v != 0.0) atomicAdd(&out_lw[((size_t)T * a.nq0 + en.x) * NMODE + s0], v);
+                const int more = S.qmore;
+                tc::named_bar(2, EPI_THREADS);
+                if (tid == 0) {
+                    S.qn = 0;
+                    S.qmore = 0;
                 }
+                tc::named_bar(2, EPI_THREADS);
+                if (!more) break;
             }
             tc::fence_before_sync();
             __syncwarp();
