@@ -65,7 +65,7 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
 
 
 BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
-TC_EPT = 20         # pairs per tensor-core tile
+TC_EPT = 16         # pairs per tensor-core tile
 
 
 def tc_issued_flops_per_tile(passes):

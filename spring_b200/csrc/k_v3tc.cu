@@ -8,8 +8,8 @@
 //   Z_q1[mu][a s1][N2 c] = sum_{N1 b} FC3[mu][N1][N2][a b c] U_q1[mu][N1 b][s1]     (per grid q1)
 //   Y[mu][a s1][s2]      = sum_{N2 c} Z_q1[mu][a s1][N2 c] U_q2[mu][N2 c][s2]       (per pair: tensor cores)
 //   Phi[s0][s1][s2]      = sum_{mu a} m_mu^-1/2 e0(mu a, s0) Y[mu][a s1][s2]        (per pair: epilogue)
-// Pairs are grouped by q1, so one tile is up to 20 pairs sharing Z_q1: the MMA
-// computes Y^T for 120 rows (pair, s2) at once, M = 128, N = 48 (36 used:
+// Pairs are grouped by q1, so one tile is up to 16 pairs sharing Z_q1: the MMA
+// computes Y^T for rows 8 pair + s2 at once, M = 128, N = 48 (36 used:
 // Re/Im of (a, s1)), K = 48 (Re/Im of (N2, c), 42 used), one accumulator per
 // basis atom mu in tensor memory.  The complex product is written as a real one:
 //   A[(pair, s2)][k] = [Re U_q2 | Im U_q2],   B[(re, a s1)][k] = [Re Z | -Im Z],
@@ -34,13 +34,17 @@ namespace {
 
 constexpr int NMODE = 6;     // Ndof of the two-atom cell
 constexpr int KP = 48;       // padded K: Re/Im of (N2, c), 2 * 3 * Na3 <= 48
-constexpr int EPT = 20;      // pairs per tile: five per 32-row TMEM lane quarter (120 of 128 rows)
+constexpr int EPT = 16;      // pairs per tile: one 8-row core-matrix group each (rows 8e .. 8e+5 of 128)
 constexpr int BROWS = 36;    // used B rows
 constexpr int QSMAX = 12 + 6 * 9;  // packed phonons of one grid point: omega[6], 1/omega[6], nBE[T][6]
 constexpr int Q0ROW = 50;    // packed q0 row in doubles (48 used; 400-byte stride spreads the banks)
 constexpr uint32_t LBO = 128, SBO = (KP / 8) * 128;
 constexpr int A_BYTES = (128 / 8) * SBO;  // 12288
 constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
+constexpr int AIMG = 8 * KP;              // bf16 elements of one (q, mu, hi/lo) A image: 8 rows x 48 (768 bytes)
+constexpr int BIMG = 48 * KP;             // bf16 elements of one (q1, mu, hi/lo) B image (4608 bytes)
+constexpr int AREC = 4 * AIMG * 2 / 8;    // doubles taken by the four A images of a grid record (384)
+constexpr int PBMAX = QSMAX * 8 + 4 * 768;  // bytes of the largest pair block in shared memory
 constexpr double EXP_CUT = 40.0;
 constexpr long long MAX_SPINS = 1LL << 26;
 
@@ -66,29 +70,38 @@ __device__ __forceinline__ double2 u_value(int q, int mu, int k, int s, int na, 
     return make_double2(m * (cs * e.x - sn * e.y), m * (cs * e.y + sn * e.x));
 }
 
-// A table: [q][mu][hl][s][KP] bf16
-__global__ void k_tc_tab_a(int nq, int na, const double* __restrict__ posr, const int* __restrict__ btyp,
+// A operand images, stored in the grid records after the packed row (qs doubles): per (hi/lo, mu)
+// the 768-byte shared-memory image of one 8-row group of the canonical K-major layout, element
+// (row s, k) at (k/8)*64 + s*8 + k%8, rows 6 and 7 zero.  Hi parts first, so a BF16 launch copies
+// the row and the two hi images as one block.
+__global__ void k_tc_tab_a(int nq, int na, int qs, const double* __restrict__ posr, const int* __restrict__ btyp,
                            const double* __restrict__ mrs, const double* __restrict__ qpnt,
-                           const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
+                           const double2* __restrict__ evg, double* __restrict__ rec) {
     const int KR = 3 * na;
-    const long long total = (long long)nq * 2 * NMODE * KP;
+    const long long total = (long long)nq * 2 * 8 * KP;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i % KP), s = (int)((i / KP) % NMODE), mu = (int)((i / (KP * NMODE)) % 2);
-        const int q = (int)(i / (KP * NMODE * 2));
+        const int k = (int)(i % KP), s = (int)((i / KP) % 8), mu = (int)((i / (KP * 8)) % 2);
+        const int q = (int)(i / (KP * 8 * 2));
         double x = 0.0;
-        if (k < 2 * KR) {
+        if (k < 2 * KR && s < NMODE) {
             const double2 u = u_value(q, mu, k % KR, s, na, posr, btyp, mrs, qpnt, evg);
             x = k < KR ? u.x : u.y;
         }
         __nv_bfloat16 hi, lo;
         split_bf16(x, hi, lo);
-        const size_t base = (((size_t)q * 2 + mu) * 2) * NMODE * KP + (size_t)s * KP + k;
-        tab[base] = hi;
-        tab[base + (size_t)NMODE * KP] = lo;
+        __nv_bfloat16* img = reinterpret_cast<__nv_bfloat16*>(rec + (size_t)q * (qs + AREC) + qs);
+        const int off = mu * AIMG + (k / 8) * 64 + s * 8 + k % 8;
+        img[off] = hi;
+        img[2 * AIMG + off] = lo;
     }
 }
 
-// B table: [q1][mu][hl][36][KP] bf16; one CTA per (q1, mu)
+// B table: per (q1, hi/lo, mu) the 4608-byte shared-memory image of the 48 x 48 B operand in the
+// canonical K-major layout: element (row n, k) at (n/8)*384 + (k/8)*64 + (n%8)*8 + k%8; rows 36-47
+// and the K padding are zero.  Hi parts first.  One CTA per (q1, mu).
+__device__ __forceinline__ size_t bimg(int n, int k) {
+    return (size_t)(n / 8) * 384 + (size_t)(k / 8) * 64 + (n % 8) * 8 + k % 8;
+}
 __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* __restrict__ fc3,
                                                   const double* __restrict__ posr, const int* __restrict__ btyp,
                                                   const double* __restrict__ mrs, const double* __restrict__ qpnt,
@@ -100,10 +113,14 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         sU[i] = u_value(q, mu, i / NMODE, i % NMODE, na, posr, btyp, mrs, qpnt, evg);
     __syncthreads();
     const double* f = fc3 + (size_t)mu * na * na * 27;
-    __nv_bfloat16* out = tab + ((size_t)q * 2 + mu) * 2 * BROWS * KP;
-    for (int i = threadIdx.x; i < 2 * BROWS * (KP - 2 * KR); i += blockDim.x) {  // zero K padding
-        const int hl = i / (BROWS * (KP - 2 * KR)), r = (i / (KP - 2 * KR)) % BROWS, k = 2 * KR + i % (KP - 2 * KR);
-        out[((size_t)hl * BROWS + r) * KP + k] = __float2bfloat16_rn(0.0f);
+    __nv_bfloat16* out = tab + (size_t)q * 4 * BIMG + mu * BIMG;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
+    for (int i = threadIdx.x; i < 48 * KP; i += blockDim.x) {  // zero rows 36-47 and the K padding
+        const int n = i / KP, k = i % KP;
+        if (n >= BROWS || k >= 2 * KR) {
+            out[bimg(n, k)] = zero;
+            out[2 * BIMG + bimg(n, k)] = zero;
+        }
     }
     for (int i = threadIdx.x; i < 18 * KR; i += blockDim.x) {
         const int r = i / KR, k2 = i % KR;  // r = a*6 + s1, k2 = N2*3 + c
@@ -119,12 +136,12 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         __nv_bfloat16 h, l;
         // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
         split_bf16(zr, h, l);
-        out[(size_t)r * KP + k2] = h;                       out[((size_t)BROWS + r) * KP + k2] = l;
-        out[(size_t)(18 + r) * KP + KR + k2] = h;           out[((size_t)BROWS + 18 + r) * KP + KR + k2] = l;
+        out[bimg(r, k2)] = h;                  out[2 * BIMG + bimg(r, k2)] = l;
+        out[bimg(18 + r, KR + k2)] = h;        out[2 * BIMG + bimg(18 + r, KR + k2)] = l;
         split_bf16(-zi, h, l);
-        out[(size_t)r * KP + KR + k2] = h;                  out[((size_t)BROWS + r) * KP + KR + k2] = l;
+        out[bimg(r, KR + k2)] = h;             out[2 * BIMG + bimg(r, KR + k2)] = l;
         split_bf16(zi, h, l);
-        out[(size_t)(18 + r) * KP + k2] = h;                out[((size_t)BROWS + 18 + r) * KP + k2] = l;
+        out[bimg(18 + r, k2)] = h;             out[2 * BIMG + bimg(18 + r, k2)] = l;
     }
 }
 
@@ -147,10 +164,10 @@ __global__ void k_tc_q0tab(int nq0, const double2* __restrict__ ev0, const doubl
     }
 }
 
-// Packed grid rows (qs = 12 + 6 x the kernel's temperature bucket doubles): omega[6], 1/omega[6],
-// nBE[T][6] (zero beyond the n_temps in use).
+// Packed grid rows at the head of each grid record (qs = 12 + 6 x the kernel's temperature bucket
+// doubles): omega[6], 1/omega[6], nBE[T][6] (zero beyond the n_temps in use).
 __global__ void k_tc_qtab(int nq, int nT, int qs, const double* __restrict__ omg, const double* __restrict__ obg,
-                          const double* __restrict__ nbeg, double* __restrict__ out) {
+                          const double* __restrict__ nbeg, double* __restrict__ rec) {
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * qs;
          i += (long long)gridDim.x * blockDim.x) {
         const int q = (int)(i / qs), k = (int)(i % qs);
@@ -159,7 +176,7 @@ __global__ void k_tc_qtab(int nq, int nT, int qs, const double* __restrict__ omg
         else if (k < 12) v = obg[(size_t)q * NMODE + k - 6];
         else if ((k - 12) / NMODE < nT) v = nbeg[((size_t)((k - 12) / NMODE) * nq + q) * NMODE + (k - 12) % NMODE];
         else v = 0.0;
-        out[i] = v;
+        rec[(size_t)q * (qs + AREC) + k] = v;
     }
 }
 
@@ -205,12 +222,13 @@ struct TcArgs {
 
 // One pipeline stage: the operands of one tile and everything its epilogue reads.
 struct TcStage {
-    alignas(128) uint8_t A[2][2][A_BYTES];  // [mu][hi, lo]: rows (pair, s2)
-    alignas(128) uint8_t B[2][2][B_BYTES];  // [mu][hi, lo]: rows (re/im, a, s1)
-    double q0d[EPT][Q0ROW];                 // packed q0 rows
-    double q2d[EPT][QSMAX];                 // packed q2 rows
-    double q1d[QSMAX];                      // packed q1 row
-    int4 ent[EPT];                          // (q0, q2, weight, q0 is Gamma)
+    // pair blocks, PB bytes apart: q2 row (QS doubles), then the A images [hi, lo][mu] of q2;
+    // pair e's images are rows 8e .. 8e+5 of the M = 128 operand (8-row group stride PB)
+    alignas(128) uint8_t P[EPT * PBMAX];
+    alignas(128) uint8_t B[2 * 2 * B_BYTES];  // [hi, lo][mu]: rows (re/im, a, s1)
+    alignas(16) double q0d[EPT][Q0ROW];       // packed q0 rows
+    alignas(16) double q1d[QSMAX];            // packed q1 row
+    int4 ent[EPT];                            // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
 };
 
@@ -225,169 +243,190 @@ constexpr int QCAP = 512;
 
 struct TcSmem {
     TcStage st[2];
-    QItem q[QCAP];     // active triples of the tile being reduced
-    int qn, qmore;
-    int4 pf[2][EPT];   // entry records prefetched one tile ahead
-    int4 trec[4];      // tile records prefetched two tiles ahead
-    alignas(8) uint64_t ready[2], full[2], empty[2];
+    QItem q[QCAP];                  // active triples of the tile being reduced
+    alignas(16) int4 pf[2][EPT];    // entry records, prefetched one tile ahead
+    alignas(16) int4 trec[4];       // tile records, prefetched two tiles ahead
+    alignas(8) uint64_t ready[2], full[2], empty[2], pfb[2], trb[4];
     uint32_t tslot;
-    int abort_p, abort_e;  // a bounded wait gave up (decided by one thread, read by its role)
+    int qn, qmore;
+    int abort_e;  // an epilogue wait gave up (set by any epilogue thread, read by all after a barrier)
 };
 
-constexpr int EPI_THREADS = 256;   // warps 0-7: epilogue; warps w and w+4 share TMEM lanes, three s0 each
-constexpr int PRO_THREADS = 128;   // warps 8-11: operand gather and MMA issue
-constexpr int TC_THREADS = EPI_THREADS + PRO_THREADS;
+constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s0 each
+constexpr int EPI_THREADS = EPI_WARPS * 32;
+constexpr int TC_THREADS = EPI_THREADS + 32;  // warp 12: bulk copies and MMA issue
 
-// TMEM row of (pair e, branch s2): five pairs per 32-lane quarter, lanes 30 and 31 unused.
-__host__ __device__ __forceinline__ int tc_row(int e, int s2) { return 32 * (e / 5) + NMODE * (e % 5) + s2; }
-
-// Warp-specialised, double-buffered: the producer warps gather tile i+1 into the
-// free stage (cp.async) and one of them issues its MMAs into the stage's TMEM
-// columns, while the epilogue warps reduce tile i.  mbarriers: ready[s] (the
-// stage's operands and phonon rows are in shared memory), full[s] (MMA
-// completion, tcgen05.commit), empty[s] (every epilogue warp is done with s).
+// Warp-specialised, double-buffered.  The producer warp fills stage s with TMA bulk copies of
+// ready-made shared-memory images, two per pair (the q2 grid record: packed row + A images; the
+// packed q0 row) and two when q1 changes (the B images, the q1 row), completing on ready[s].  At
+// its next iteration it first issues that tile's MMAs into the stage's TMEM columns (lane 0,
+// committed to full[s]) and then fills the other stage, so the MMAs of tile j overlap the
+// epilogue of tile j-1.  The epilogue warps reduce the tile, then arrive on empty[s].  Entry and
+// tile records are prefetched ahead on their own mbarriers.
 template <int NTM, bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec, const __nv_bfloat16* __restrict__ tabA,
-       const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ q0tab, const double* __restrict__ qtab,
-       double* __restrict__ out_lw, double* __restrict__ out_p3, int* __restrict__ err) {
+k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec, const double* __restrict__ rec,
+       const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ q0tab, double* __restrict__ out_lw,
+       double* __restrict__ out_p3, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int H = SPLIT ? 2 : 1;
-    constexpr int QS = 12 + 6 * NTM, QCH = QS / 2;  // packed grid row (the table is laid out for NTM)
+    constexpr int QS = 12 + 6 * NTM;       // packed grid row (the records are laid out for NTM)
+    constexpr int RSD = QS + AREC;         // grid record stride in doubles
+    constexpr int PB = QS * 8 + H * 1536;  // pair block bytes: the row and the hi (and lo) A images
+    static_assert(PB <= PBMAX && PB % 16 == 0, "pair block");
     const int t0 = blockIdx.x * a.tiles_per_cta;
     const int t1 = min(a.ntiles, t0 + a.tiles_per_cta);
+    const int nt = t1 - t0;
 
-    for (int i = tid; i < (int)(2 * sizeof(S.st[0].B) / 16); i += blockDim.x) {
-        const int st = i / (int)(sizeof(S.st[0].B) / 16), k = i % (int)(sizeof(S.st[0].B) / 16);
-        reinterpret_cast<uint4*>(&S.st[st].B[0][0][0])[k] = make_uint4(0, 0, 0, 0);
-    }
     if (tid == 0) {
         S.st[0].q1 = S.st[1].q1 = -1;
-        S.abort_p = S.abort_e = 0;
+        S.abort_e = 0;
         S.qn = S.qmore = 0;
         for (int k = 0; k < 2; ++k) {
             tc::mbar_init(tc::smem_u32(&S.ready[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
-            tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_THREADS / 32);
+            tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_WARPS);
+            tc::mbar_init(tc::smem_u32(&S.pfb[k]), 1);
         }
+        for (int k = 0; k < 4; ++k) tc::mbar_init(tc::smem_u32(&S.trb[k]), 1);
         tc::mbar_fence_init();
     }
-    if (tid < 2 && t0 + tid < t1) S.trec[tid] = tiles[t0 + tid];
+    if (tid < 2 && tid < nt) S.trec[tid] = tiles[t0 + tid];
     if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), 256);
     tc::fence_before_sync();
     __syncthreads();
-    if (t0 < t1 && tid < S.trec[0].z) S.pf[0][tid] = entrec[S.trec[0].y + tid];
+    if (nt > 0 && tid < S.trec[0].z) S.pf[0][tid] = entrec[S.trec[0].y + tid];
     tc::fence_after_sync();
     __syncthreads();
     const uint32_t tm = S.tslot;
 
-    if (tid >= EPI_THREADS) {
-        // ------------------------------------------------------------ producer
-        const int pt = tid - EPI_THREADS;
-        for (int t = t0, j = 0; t < t1; ++t, ++j) {
-            const int s = j & 1, u = j >> 1;
-            TcStage& G = S.st[s];
-            if (u > 0) {
-                if (pt == 0) S.abort_p = !tc::mbar_wait(tc::smem_u32(&S.empty[s]), (uint32_t)((u - 1) & 1), MAX_SPINS);
-                tc::named_bar(1, PRO_THREADS);
-                if (S.abort_p) {
-                    if (pt == 0) atomicExch(err, 1);
+    if (warp == EPI_WARPS) {
+        // ------------------------------------------------------------ producer warp
+        bool abort = false;
+        int filled = -1, issued = -1;  // last tile whose copies / MMAs were issued
+        for (int j = 0; j <= nt && !abort; ++j) {
+            if (j >= 1) {
+                // (a) MMAs of tile j-1 once its operands have landed; its TMEM columns were freed when
+                // the stage's previous tile (j-3) was drained, which the fill of j-1 waited for
+                const int jm = j - 1, s = jm & 1, u = jm >> 1;
+                TcStage& G = S.st[s];
+                bool ok = true;
+                if (lane == 0) {
+                    ok = tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS);
+                    if (ok) {
+                        tc::fence_after_sync();
+                        const uint32_t idesc = tc::idesc_bf16(128, 48);
+                        const uint32_t pa = tc::smem_u32(&G.P[QS * 8]), pb = tc::smem_u32(&G.B[0]);
+                        for (int mu = 0; mu < 2; ++mu) {
+                            const uint32_t d = tm + (uint32_t)(s * 128 + mu * 64);
+                            for (int kk = 0; kk < KP / 16; ++kk) {
+                                const uint32_t ko = (uint32_t)kk * 2u * LBO;
+                                const uint64_t ah = tc::sdesc(pa + mu * 768 + ko, LBO, PB);
+                                const uint64_t bh = tc::sdesc(pb + mu * B_BYTES + ko, LBO, SBO);
+                                tc::mma_bf16(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                                if (SPLIT) {
+                                    const uint64_t al = tc::sdesc(pa + (2 + mu) * 768 + ko, LBO, PB);
+                                    const uint64_t bl = tc::sdesc(pb + (2 + mu) * B_BYTES + ko, LBO, SBO);
+                                    tc::mma_bf16(d, ah, bl, idesc, 1u);
+                                    tc::mma_bf16(d, al, bh, idesc, 1u);
+                                }
+                            }
+                        }
+                        tc::mma_commit(tc::smem_u32(&S.full[s]));
+                        issued = jm;
+                    }
+                }
+                issued = __shfl_sync(0xffffffffu, issued, 0);
+                if (__any_sync(0xffffffffu, !ok)) {
+                    if (lane == 0) atomicExch(err, 1);
+                    abort = true;
                     break;
                 }
             }
-            const int4 tile = S.trec[j & 3];
-            const int q1 = tile.x, ne = tile.z;
-            const int4* ent = S.pf[j & 1];
-            const bool newb = G.q1 != q1;
-            // prefetch the tile record two ahead and the entry records of the next tile
-            if (pt == 0 && t + 2 < t1) tc::cp_async16(tc::smem_u32(&S.trec[(j + 2) & 3]), tiles + t + 2);
-            if (t + 1 < t1) {
-                const int4 nx = S.trec[(j + 1) & 3];
-                if (pt < nx.z) tc::cp_async16(tc::smem_u32(&S.pf[(j + 1) & 1][pt]), entrec + nx.y + pt);
-            }
-            if (pt < ne) G.ent[pt] = ent[pt];
-            if (newb) {
-                for (int i = pt; i < 2 * H * BROWS * (KP / 8); i += PRO_THREADS) {
-                    const int kc = i % (KP / 8), n = (i / (KP / 8)) % BROWS, mh = i / (BROWS * (KP / 8));
-                    const int mu = mh / H, hl = mh % H;
-                    tc::cp_async16(tc::smem_u32(&G.B[mu][hl][tc::kmajor_offset(n, kc * 8, LBO, SBO)]),
-                                   tabB + ((((size_t)q1 * 2 + mu) * 2 + hl) * BROWS + n) * KP + kc * 8);
+            if (j < nt) {
+                // (b) fill stage j & 1 with tile j
+                const int s = j & 1, u = j >> 1;
+                TcStage& G = S.st[s];
+                // every lane waits, so each one observes the completed copies it reads or overwrites
+                bool ok = true;
+                if (u > 0) ok = tc::mbar_wait(tc::smem_u32(&S.empty[s]), (uint32_t)((u - 1) & 1), MAX_SPINS);
+                if (ok && j > 0) ok = tc::mbar_wait(tc::smem_u32(&S.pfb[j & 1]), (uint32_t)(((j - 1) >> 1) & 1), MAX_SPINS);
+                if (ok && j >= 2) ok = tc::mbar_wait(tc::smem_u32(&S.trb[j & 3]), (uint32_t)(((j - 2) >> 2) & 1), MAX_SPINS);
+                if (ok && j + 1 < nt && j >= 1)
+                    ok = tc::mbar_wait(tc::smem_u32(&S.trb[(j + 1) & 3]), (uint32_t)(((j - 1) >> 2) & 1), MAX_SPINS);
+                if (__any_sync(0xffffffffu, !ok)) {
+                    if (lane == 0) atomicExch(err, 1);
+                    abort = true;
+                    break;
                 }
-                for (int i = pt; i < QCH; i += PRO_THREADS)
-                    tc::cp_async16(tc::smem_u32(&G.q1d[2 * i]), qtab + (size_t)q1 * QS + 2 * i);
-            }
-            {
-                // A rows: warp pw takes pairs pw, pw+4, ...; lane l the (s2, k-chunk) slots l and l+32 of 36
-                const int pw = pt >> 5, pl = pt & 31;
-                const int c0 = pl, c1 = pl + 32;
-                const int s2a = c0 / (KP / 8), kca = c0 % (KP / 8);
-                const int s2b = c1 / (KP / 8), kcb = c1 % (KP / 8);
-                for (int e = pw; e < ne; e += PRO_THREADS / 32) {
-                    const __nv_bfloat16* src = tabA + (size_t)ent[e].y * (2 * 2 * NMODE * KP);
-                    const int ra = tc_row(e, s2a), rb = tc_row(e, s2b);
-#pragma unroll
-                    for (int mh = 0; mh < 2 * H; ++mh) {
-                        const int mu = mh / H, hl = mh % H;
-                        const __nv_bfloat16* sm = src + (size_t)(mu * 2 + hl) * NMODE * KP;
-                        uint8_t* dst = &G.A[mu][hl][0];
-                        tc::cp_async16(tc::smem_u32(dst + tc::kmajor_offset(ra, kca * 8, LBO, SBO)), sm + s2a * KP + kca * 8);
-                        if (c1 < NMODE * (KP / 8))
-                            tc::cp_async16(tc::smem_u32(dst + tc::kmajor_offset(rb, kcb * 8, LBO, SBO)),
-                                           sm + s2b * KP + kcb * 8);
-                    }
+                const int4 tile = S.trec[j & 3];
+                const int q1 = tile.x, ne = tile.z;
+                const int4* ent = S.pf[j & 1];
+                const bool newb = G.q1 != q1;
+                if (lane < ne) G.ent[lane] = ent[lane];
+                __syncwarp();
+                const uint32_t rb = tc::smem_u32(&S.ready[s]);
+                if (lane == 0) {
+                    G.ne = ne;
+                    G.q1 = q1;
+                    uint32_t bytes = (uint32_t)ne * (uint32_t)(PB + 384);
+                    if (newb) bytes += (uint32_t)(2 * H * B_BYTES + QS * 8);
+                    tc::mbar_arrive_tx(rb, bytes);
                 }
-            }
-            for (int i = pt; i < ne * 24; i += PRO_THREADS)  // 384-byte q0 rows into 400-byte slots
-                tc::cp_async16(tc::smem_u32(&G.q0d[i / 24][2 * (i % 24)]),
-                               q0tab + (size_t)ent[i / 24].x * Q0ROW + 2 * (i % 24));
-            for (int i = pt; i < ne * QCH; i += PRO_THREADS) {
-                const int e = i / QCH, k = i % QCH;
-                tc::cp_async16(tc::smem_u32(&G.q2d[e][2 * k]), qtab + (size_t)ent[e].y * QS + 2 * k);
-            }
-            tc::cp_async_wait_all();
-            tc::fence_async_smem();
-            tc::named_bar(1, PRO_THREADS);
-            if (pt == 0) {
-                G.ne = ne;
-                G.q1 = q1;  // every producer thread has read the old value (newb) before the barrier
-                tc::mbar_arrive(tc::smem_u32(&S.ready[s]));
-                tc::fence_after_sync();
-                const uint32_t idesc = tc::idesc_bf16(128, 48);
-                for (int mu = 0; mu < 2; ++mu) {
-                    const uint32_t d = tm + (uint32_t)(s * 128 + mu * 64);
-                    for (int kk = 0; kk < KP / 16; ++kk) {
-                        const uint32_t ko = (uint32_t)kk * 2u * LBO;
-                        const uint64_t ah = tc::sdesc(tc::smem_u32(&G.A[mu][0][0]) + ko, LBO, SBO);
-                        const uint64_t bh = tc::sdesc(tc::smem_u32(&G.B[mu][0][0]) + ko, LBO, SBO);
-                        tc::mma_bf16(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
-                        if (SPLIT) {
-                            const uint64_t al = tc::sdesc(tc::smem_u32(&G.A[mu][1][0]) + ko, LBO, SBO);
-                            const uint64_t bl = tc::sdesc(tc::smem_u32(&G.B[mu][1][0]) + ko, LBO, SBO);
-                            tc::mma_bf16(d, ah, bl, idesc, 1u);
-                            tc::mma_bf16(d, al, bh, idesc, 1u);
-                        }
-                    }
+                __syncwarp();
+                if (lane < ne) {
+                    const int4 en = ent[lane];
+                    tc::bulk_g2s(tc::smem_u32(&G.P[lane * PB]), rec + (size_t)en.y * RSD, (uint32_t)PB, rb);
+                    tc::bulk_g2s(tc::smem_u32(&G.q0d[lane][0]), q0tab + (size_t)en.x * Q0ROW, 384u, rb);
                 }
-                tc::mma_commit(tc::smem_u32(&S.full[s]));
+                if (newb && lane == 30)
+                    tc::bulk_g2s(tc::smem_u32(&G.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
+                if (newb && lane == 31) tc::bulk_g2s(tc::smem_u32(&G.q1d[0]), rec + (size_t)q1 * RSD, (uint32_t)QS * 8u, rb);
+                // prefetch: entry records of tile j+1, tile record j+2
+                if (lane == 0 && j + 1 < nt) {
+                    const int4 nx = S.trec[(j + 1) & 3];
+                    const uint32_t pb = tc::smem_u32(&S.pfb[(j + 1) & 1]);
+                    tc::mbar_arrive_tx(pb, (uint32_t)nx.z * 16u);
+                    tc::bulk_g2s(tc::smem_u32(&S.pf[(j + 1) & 1][0]), entrec + nx.y, (uint32_t)nx.z * 16u, pb);
+                }
+                if (lane == 0 && j + 2 < nt) {
+                    const uint32_t tb = tc::smem_u32(&S.trb[(j + 2) & 3]);
+                    tc::mbar_arrive_tx(tb, 16u);
+                    tc::bulk_g2s(tc::smem_u32(&S.trec[(j + 2) & 3]), tiles + t0 + j + 2, 16u, tb);
+                }
+                filled = j;
             }
+        }
+        if (abort && lane == 0) {
+            // Error path: wait (bounded) for the copies and MMAs still in flight before the CTA
+            // releases its shared memory and TMEM.
+            for (int t = issued + 1; t <= filled; ++t)
+                tc::mbar_wait(tc::smem_u32(&S.ready[t & 1]), (uint32_t)((t >> 1) & 1), MAX_SPINS);
+            if (filled >= 0 && filled + 1 < nt)
+                tc::mbar_wait(tc::smem_u32(&S.pfb[(filled + 1) & 1]), (uint32_t)((filled >> 1) & 1), MAX_SPINS);
+            for (int t = max(2, filled + 1); t <= filled + 2 && t < nt; ++t)
+                tc::mbar_wait(tc::smem_u32(&S.trb[t & 3]), (uint32_t)(((t - 2) >> 2) & 1), MAX_SPINS);
+            if (issued >= 0)
+                tc::mbar_wait(tc::smem_u32(&S.full[issued & 1]), (uint32_t)((issued >> 1) & 1), MAX_SPINS);
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const int wq = warp & 3, h = warp >> 2;
-        const int e = 5 * wq + lane / NMODE, s2 = lane % NMODE;
-        const bool lane_ok = lane < 30;
+        const int wq = warp & 3, grp = warp >> 2;  // lane quarter, s0 pair (2 grp, 2 grp + 1)
+        const int e = 4 * wq + lane / 8, s2 = lane % 8;
         const float Rf = (float)(sqrt(EXP_CUT / a.half_os2) * 1.0001 + 1e-3);
-        for (int t = t0, j = 0; t < t1; ++t, ++j) {
+        const int etid = tid;  // 0 .. EPI_THREADS-1
+        for (int j = 0; j < nt; ++j) {
             const int s = j & 1, u = j >> 1;
             TcStage& G = S.st[s];
-            if (tid == 0)
-                S.abort_e = !(tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS) &&
-                              tc::mbar_wait(tc::smem_u32(&S.full[s]), (uint32_t)(u & 1), MAX_SPINS));
+            // every thread waits on both barriers: the copies and the accumulator it reads
+            if (!(tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS) &&
+                  tc::mbar_wait(tc::smem_u32(&S.full[s]), (uint32_t)(u & 1), MAX_SPINS)))
+                S.abort_e = 1;
             tc::named_bar(2, EPI_THREADS);
             if (S.abort_e) {
-                if (tid == 0) atomicExch(err, 1);
+                if (etid == 0) atomicExch(err, 1);
                 break;
             }
             tc::fence_after_sync();
@@ -403,20 +442,20 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                 tc::tmem_ld_wait();
             }
             const int ne = G.ne;
-            const bool valid = lane_ok && e < ne;
+            const bool valid = s2 < NMODE && e < ne;
             const int4 en = valid ? G.ent[e] : make_int4(0, 0, 0, 0);
             const bool row_on = valid && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
-            const bool gq0 = en.w != 0, gq1 = G.q1 == 0;
+            const bool gq1 = G.q1 == 0;
             const double* q1d = G.q1d;
-            const double* q2d = G.q2d[valid ? e : 0];
+            const double* q2d = reinterpret_cast<const double*>(&G.P[(valid ? e : 0) * PB]);
             const double* q0d = G.q0d[valid ? e : 0];
-            const double w2 = q2d[s2];
-            // FP32 screen: bit 6*jj + s1 marks (s0 = 3h + jj, s1) inside the delta window
+            const double w2 = q2d[valid ? s2 : 0];
+            // FP32 screen: bit 6*jj + s1 marks (s0 = 2 grp + jj, s1) inside the delta window
             unsigned act = 0u;
             if (row_on) {
 #pragma unroll
-                for (int jj = 0; jj < 3; ++jj) {
-                    const int s0 = h * 3 + jj;
+                for (int jj = 0; jj < 2; ++jj) {
+                    const int s0 = grp * 2 + jj;
                     if (s0 < a.lo[0] || s0 > a.hi[0]) continue;
                     const double w0 = q0d[36 + s0];
                     const float af = (float)(w0 - w2), bf = (float)(w0 + w2);
@@ -429,9 +468,9 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                     }
                 }
             }
-            // Compaction: the screened triples of the whole tile go to a shared queue (several passes if it
-            // fills), and all epilogue threads evaluate them one per thread, so the FP64 work runs with
-            // full warps; each triple's contribution goes straight to the output.
+            // Compaction: the screened triples of the whole tile go to a shared queue (several passes if
+            // it fills), and all epilogue threads evaluate them one per thread, so the FP64 work runs
+            // with full warps; each triple's contribution goes straight to the output.
             for (;;) {
                 if (act) {
                     const int n = __popc(act);
@@ -452,19 +491,19 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                             it.yr[k] = r;
                             it.yi[k] = im;
                         }
-                        it.meta = e | (s2 << 8) | ((h * 3 + jj) << 12) | (s1 << 16);
+                        it.meta = e | (s2 << 8) | ((grp * 2 + jj) << 12) | (s1 << 16);
                     }
                     if (act) S.qmore = 1;
                 }
                 tc::named_bar(2, EPI_THREADS);
                 const int cnt = min(S.qn, QCAP);
-                for (int i = tid; i < cnt; i += EPI_THREADS) {
+                for (int i = etid; i < cnt; i += EPI_THREADS) {
                     const QItem& it = S.q[i];
                     const int ie = it.meta & 0xff, is2 = (it.meta >> 8) & 0xf, s0 = (it.meta >> 12) & 0xf,
                               s1 = (it.meta >> 16) & 0xf;
                     const int4 ien = G.ent[ie];
                     const double* p0 = G.q0d[ie];
-                    const double* p2 = G.q2d[ie];
+                    const double* p2 = reinterpret_cast<const double*>(&G.P[ie * PB]);
                     const double w0 = p0[36 + s0], w1d = q1d[s1], w2d = p2[is2];
                     const double d1 = w0 - w1d - w2d, d2 = w0 + w1d - w2d, d3 = w0 - w1d + w2d;
                     const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2), x3 = a.half_os2 * (d3 * d3);
@@ -493,7 +532,7 @@ k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec
                 }
                 const int more = S.qmore;
                 tc::named_bar(2, EPI_THREADS);
-                if (tid == 0) {
+                if (etid == 0) {
                     S.qn = 0;
                     S.qmore = 0;
                 }
@@ -523,8 +562,8 @@ int launch_tc(spring_ctx* c, TcArgs a, double* lw, double* p3) {
     const int grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
     k_v3tc<NTM, SPLIT><<<grid, TC_THREADS, smem, c->stream>>>(
-        a, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_a.p),
-        reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->d_tc_q0.p, c->d_tc_q.p, lw, p3, c->d_tc_err.p);
+        a, c->d_tc_tiles.p, c->d_tc_rec.p, c->d_tc_q.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p),
+        c->d_tc_q0.p, lw, p3, c->d_tc_err.p);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -621,20 +660,19 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const int nq = c->nq;
     const int ntm = c->nT == 1 ? 1 : (c->nT <= 3 ? 3 : 9);  // temperature bucket of the kernel instance
     const int qs = 12 + 6 * ntm;
-    SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 2 * 2 * NMODE * KP, "V3 A table"));
-    SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 2 * 2 * BROWS * KP, "V3 B table"));
+    SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 4 * BIMG, "V3 B table"));
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * Q0ROW, "V3 q0 rows"));
-    SPRING_CHECK(dalloc(c, c->d_tc_q, (size_t)nq * qs, "V3 grid rows"));
+    SPRING_CHECK(dalloc(c, c->d_tc_q, (size_t)nq * (qs + AREC), "V3 grid records"));
     SPRING_CHECK(dalloc(c, c->d_tc_err, 1, "V3 status"));
     SPRING_CHECK(zero(c, c->d_tc_err.p, sizeof(int), "V3 status"));
     SPRING_CHECK(build_tiles(c, p0, p1));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     {
-        const long long tot = (long long)nq * 2 * NMODE * KP;
+        const long long tot = (long long)nq * 2 * 8 * KP;
         k_tc_tab_a<<<(int)std::min<long long>((tot + threads - 1) / threads, 148LL * 16), threads, 0, c->stream>>>(
-            nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
-            reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
+            nq, c->na3, qs, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
+            c->d_tc_q.p);
         SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
     }
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");

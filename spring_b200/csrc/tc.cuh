@@ -131,6 +131,18 @@ static __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// Bulk (non-tensor) global -> shared copy completing on an mbarrier's transaction count;
+// addresses 16-byte aligned, size a multiple of 16.
+static __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(mbar)
+                 : "memory");
+}
+// Arrive on the mbarrier and add `bytes` to the transactions its current phase waits for.
+static __device__ __forceinline__ void mbar_arrive_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
 // Byte offset of element (row, k) in the canonical K-major layout.
 static __host__ __device__ __forceinline__ uint32_t kmajor_offset(int row, int k, uint32_t lbo, uint32_t sbo) {
     return (uint32_t)(row >> 3) * sbo + (uint32_t)(k >> 3) * lbo + (uint32_t)(row & 7) * 16u + (uint32_t)(k & 7) * 2u;
