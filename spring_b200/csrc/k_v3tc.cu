@@ -23,7 +23,9 @@
 // Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass),
 // L2 bandwidth for gathering the U_q2 rows, FP32/FP64 ALU for the screen.
 #include <algorithm>
+#include <vector>
 #include <cub/cub.cuh>
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include "spring_internal.cuh"
@@ -36,15 +38,11 @@ constexpr int NMODE = 6;     // Ndof of the two-atom cell
 constexpr int KP = 48;       // padded K: Re/Im of (N2, c), 2 * 3 * Na3 <= 48
 constexpr int EPT = 16;      // pairs per tile: one 8-row core-matrix group each (rows 8e .. 8e+5 of 128)
 constexpr int BROWS = 36;    // used B rows
-constexpr int QSMAX = 12 + 6 * 9;  // packed phonons of one grid point: omega[6], 1/omega[6], nBE[T][6]
 constexpr int Q0ROW = 50;    // packed q0 row in doubles (48 used; 400-byte stride spreads the banks)
 constexpr uint32_t LBO = 128, SBO = (KP / 8) * 128;
-constexpr int A_BYTES = (128 / 8) * SBO;  // 12288
 constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
 constexpr int AIMG = 8 * KP;              // bf16 elements of one (q, mu, hi/lo) A image: 8 rows x 48 (768 bytes)
 constexpr int BIMG = 48 * KP;             // bf16 elements of one (q1, mu, hi/lo) B image (4608 bytes)
-constexpr int AREC = 4 * AIMG * 2 / 8;    // doubles taken by the four A images of a grid record (384)
-constexpr int PBMAX = QSMAX * 8 + 4 * 768;  // bytes of the largest pair block in shared memory
 constexpr double EXP_CUT = 40.0;
 constexpr long long MAX_SPINS = 1LL << 26;
 
@@ -70,13 +68,12 @@ __device__ __forceinline__ double2 u_value(int q, int mu, int k, int s, int na, 
     return make_double2(m * (cs * e.x - sn * e.y), m * (cs * e.y + sn * e.x));
 }
 
-// A operand images, stored in the grid records after the packed row (qs doubles): per (hi/lo, mu)
-// the 768-byte shared-memory image of one 8-row group of the canonical K-major layout, element
-// (row s, k) at (k/8)*64 + s*8 + k%8, rows 6 and 7 zero.  Hi parts first, so a BF16 launch copies
-// the row and the two hi images as one block.
-__global__ void k_tc_tab_a(int nq, int na, int qs, const double* __restrict__ posr, const int* __restrict__ btyp,
+// A table: per (q, hi/lo, mu) the 768-byte shared-memory image of one 8-row group of the canonical
+// K-major layout, element (row s, k) at (k/8)*64 + s*8 + k%8, rows 6 and 7 zero.  Hi parts first,
+// so a BF16 launch copies the two hi images as one block.
+__global__ void k_tc_tab_a(int nq, int na, const double* __restrict__ posr, const int* __restrict__ btyp,
                            const double* __restrict__ mrs, const double* __restrict__ qpnt,
-                           const double2* __restrict__ evg, double* __restrict__ rec) {
+                           const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
     const int KR = 3 * na;
     const long long total = (long long)nq * 2 * 8 * KP;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
@@ -89,7 +86,7 @@ __global__ void k_tc_tab_a(int nq, int na, int qs, const double* __restrict__ po
         }
         __nv_bfloat16 hi, lo;
         split_bf16(x, hi, lo);
-        __nv_bfloat16* img = reinterpret_cast<__nv_bfloat16*>(rec + (size_t)q * (qs + AREC) + qs);
+        __nv_bfloat16* img = tab + (size_t)q * 4 * AIMG;
         const int off = mu * AIMG + (k / 8) * 64 + s * 8 + k % 8;
         img[off] = hi;
         img[2 * AIMG + off] = lo;
@@ -164,22 +161,6 @@ __global__ void k_tc_q0tab(int nq0, const double2* __restrict__ ev0, const doubl
     }
 }
 
-// Packed grid rows at the head of each grid record (qs = 12 + 6 x the kernel's temperature bucket
-// doubles): omega[6], 1/omega[6], nBE[T][6] (zero beyond the n_temps in use).
-__global__ void k_tc_qtab(int nq, int nT, int qs, const double* __restrict__ omg, const double* __restrict__ obg,
-                          const double* __restrict__ nbeg, double* __restrict__ rec) {
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * qs;
-         i += (long long)gridDim.x * blockDim.x) {
-        const int q = (int)(i / qs), k = (int)(i % qs);
-        double v;
-        if (k < 6) v = omg[(size_t)q * NMODE + k];
-        else if (k < 12) v = obg[(size_t)q * NMODE + k - 6];
-        else if ((k - 12) / NMODE < nT) v = nbeg[((size_t)((k - 12) / NMODE) * nq + q) * NMODE + (k - 12) % NMODE];
-        else v = 0.0;
-        rec[(size_t)q * (qs + AREC) + k] = v;
-    }
-}
-
 // ------------------------------------------------------------------ tiles
 __global__ void k_tc_keys(int n, int p0, const int2* __restrict__ pairs, int* __restrict__ keys, int* __restrict__ vals,
                           int* __restrict__ cnt) {
@@ -213,357 +194,416 @@ __global__ void k_tc_entrec(int n, const int* __restrict__ entries, const int2* 
     }
 }
 
-// ------------------------------------------------------------------ main kernel
+// ------------------------------------------------------------------ main kernels
 struct TcArgs {
-    int nq, nq0, nT, qs, ntiles, tiles_per_cta;
+    int nq, nq0, nT, ntiles, tiles_per_cta, cap;
     int lo[3], hi[3];
-    double mfac, half_os2, pre;
+    double half_os2;
 };
 
-// One pipeline stage: the operands of one tile and everything its epilogue reads.
-struct TcStage {
-    // pair blocks, PB bytes apart: q2 row (QS doubles), then the A images [hi, lo][mu] of q2;
-    // pair e's images are rows 8e .. 8e+5 of the M = 128 operand (8-row group stride PB)
-    alignas(128) uint8_t P[EPT * PBMAX];
+constexpr int NOP = 2;  // operand stages (A and B images; free once the tile's MMAs completed)
+constexpr int NEP = 4;  // epilogue stages (frequencies and one 128-column accumulator each)
+
+struct OpStage {
+    alignas(128) uint8_t A[2][EPT * 1536];    // [hi, lo]: per pair its two mu images (pair stride 1536)
     alignas(128) uint8_t B[2 * 2 * B_BYTES];  // [hi, lo][mu]: rows (re/im, a, s1)
-    alignas(16) double q0d[EPT][Q0ROW];       // packed q0 rows
-    alignas(16) double q1d[QSMAX];            // packed q1 row
-    int4 ent[EPT];                            // (q0, q2, weight, q0 is Gamma)
+    int q1;                                   // q1 whose B images are resident
+};
+struct EpStage {
+    alignas(16) double w0[EPT][NMODE];  // omega of each pair's q0
+    alignas(16) double w2[EPT][NMODE];  // omega of each pair's q2
+    alignas(16) double w1[NMODE];       // omega of q1
+    int4 ent[EPT];                      // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
 };
-
-// An active mode triple handed from the screening thread to any epilogue thread:
-// (Re, Im) Y[mu][a] for its s1, and (pair, s2, s0, s1).
-struct QItem {
-    float yr[6], yi[6];
-    int meta;  // e | s2 << 8 | s0 << 12 | s1 << 16
-    int pad[3];
-};
-constexpr int QCAP = 512;
-
 struct TcSmem {
-    TcStage st[2];
-    QItem q[QCAP];                  // active triples of the tile being reduced
-    alignas(16) int4 pf[2][EPT];    // entry records, prefetched one tile ahead
-    alignas(16) int4 trec[4];       // tile records, prefetched two tiles ahead
-    alignas(8) uint64_t ready[2], full[2], empty[2], pfb[2], trb[4];
+    OpStage op[NOP];
+    EpStage ep[NEP];
+    alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP];
     uint32_t tslot;
-    int qn, qmore;
-    int abort_e;  // an epilogue wait gave up (set by any epilogue thread, read by all after a barrier)
+    int ihead;  // active triples written by this CTA
 };
 
 constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s0 each
 constexpr int EPI_THREADS = EPI_WARPS * 32;
-constexpr int TC_THREADS = EPI_THREADS + 32;  // warp 12: bulk copies and MMA issue
+constexpr int TC_THREADS = EPI_THREADS + 64;  // warp 12: TMA copies and frequency gathers; warp 13: MMA issue
+constexpr int TC_COLS = NEP * 128;
+constexpr int NW = EPT * NMODE * 2 + NMODE;   // frequencies gathered per tile
 
-// Warp-specialised, double-buffered.  The producer warp fills stage s with TMA bulk copies of
-// ready-made shared-memory images, two per pair (the q2 grid record: packed row + A images; the
-// packed q0 row) and two when q1 changes (the B images, the q1 row), completing on ready[s].  At
-// its next iteration it first issues that tile's MMAs into the stage's TMEM columns (lane 0,
-// committed to full[s]) and then fills the other stage, so the MMAs of tile j overlap the
-// epilogue of tile j-1.  The epilogue warps reduce the tile, then arrive on empty[s].  Entry and
-// tile records are prefetched ahead on their own mbarriers.
-template <int NTM, bool SPLIT>
+// An active mode triple, written by k_v3tc for k_v3tc_eval: the row (pair, s2) of Y for its s1,
+// (Re, Im) Y[mu][a] with k = mu * 3 + a, and k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29,
+// k1 = q1 * 6 + s1, k2 = q2 * 6 + s2.
+struct TcItem {
+    float yr[6], yi[6];
+    int k0, k1, k2, pad;
+};
+static_assert(sizeof(TcItem) == 64, "item");
+
+// Warp-specialised tensor-core pass.  The fill warp loads operand stage j % 2 and epilogue stage
+// j % 4 for tile j: TMA gathers of the A images, four pairs' table rows per request (hi and lo parts
+// as separate requests), one bulk copy of the B images when q1 changed, and the tile's frequencies
+// (plain loads issued one tile ahead); all complete on ready[j % 4].  The MMA warp issues tile j's
+// MMAs into the accumulator of epilogue stage j % 4 and commits them to full[j % 4] and
+// opfree[j % 2].  Each epilogue warp works on its own: it reads its 32 accumulator rows, screens its
+// 12 mode triples per row in FP32 against the delta window, releases the stage, and appends the
+// active triples (with their Y values) to this CTA's region of the item list.  The FP64 part runs
+// in k_v3tc_eval.
+template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-k_v3tc(TcArgs a, const int4* __restrict__ tiles, const int4* __restrict__ entrec, const double* __restrict__ rec,
-       const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ q0tab, double* __restrict__ out_lw,
-       double* __restrict__ out_p3, int* __restrict__ err) {
+k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict__ tiles, const int4* __restrict__ entrec,
+       const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ om0, const double* __restrict__ omg,
+       TcItem* __restrict__ items, int* __restrict__ counts, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int H = SPLIT ? 2 : 1;
-    constexpr int QS = 12 + 6 * NTM;       // packed grid row (the records are laid out for NTM)
-    constexpr int RSD = QS + AREC;         // grid record stride in doubles
-    constexpr int PB = QS * 8 + H * 1536;  // pair block bytes: the row and the hi (and lo) A images
-    static_assert(PB <= PBMAX && PB % 16 == 0, "pair block");
+    constexpr int PB = 1536;  // pair stride of the A images = their 8-row group stride
     const int t0 = blockIdx.x * a.tiles_per_cta;
     const int t1 = min(a.ntiles, t0 + a.tiles_per_cta);
     const int nt = t1 - t0;
+    if ((tc::smem_u32(smraw) & 127u) != 0u) {  // TMA destinations below assume a 128-byte aligned base
+        if (tid == 0) atomicExch(err, 2);
+        return;
+    }
 
     if (tid == 0) {
-        S.st[0].q1 = S.st[1].q1 = -1;
-        S.abort_e = 0;
-        S.qn = S.qmore = 0;
-        for (int k = 0; k < 2; ++k) {
-            tc::mbar_init(tc::smem_u32(&S.ready[k]), 1);
+        for (int k = 0; k < NOP; ++k) {
+            S.op[k].q1 = -1;
+            tc::mbar_init(tc::smem_u32(&S.opfree[k]), 1);
+        }
+        for (int k = 0; k < NEP; ++k) {
+            tc::mbar_init(tc::smem_u32(&S.ready[k]), 32);
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_WARPS);
-            tc::mbar_init(tc::smem_u32(&S.pfb[k]), 1);
         }
-        for (int k = 0; k < 4; ++k) tc::mbar_init(tc::smem_u32(&S.trb[k]), 1);
+        S.ihead = 0;
         tc::mbar_fence_init();
     }
-    if (tid < 2 && tid < nt) S.trec[tid] = tiles[t0 + tid];
-    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), 256);
+    if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), TC_COLS);
     tc::fence_before_sync();
     __syncthreads();
-    if (nt > 0 && tid < S.trec[0].z) S.pf[0][tid] = entrec[S.trec[0].y + tid];
     tc::fence_after_sync();
-    __syncthreads();
     const uint32_t tm = S.tslot;
 
     if (warp == EPI_WARPS) {
-        // ------------------------------------------------------------ producer warp
+        // ------------------------------------------------------------ fill warp
+        // Records in registers, loaded ahead so that their latency stays hidden: tile records of
+        // j .. j+3 (recA .. recD), entry lane of tiles j .. j+2 (entA .. entC), and the frequencies
+        // of tile j (wv, loaded during the fill of j-1).  No warp barrier follows a load: each lane
+        // arrives on ready itself, after its own stores and before it issues the next loads.
+        const int4 z4 = make_int4(0, 0, 0, 0);
+        int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
+        int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
+        int4 entB = lane < recB.z ? entrec[recB.y + lane] : z4;
+        double wv[(NW + 31) / 32];
+        // frequencies of a tile (pairs beyond ne repeat pair 0): q0 omegas, q2 omegas, q1 omegas
+        auto load_w = [&](const int4& ent, const int4& rec) {
+#pragma unroll
+            for (int k = 0; k < (NW + 31) / 32; ++k) {
+                const int i = lane + 32 * k;
+                const int pe = (i % (EPT * NMODE)) / NMODE, pr = pe < rec.z ? pe : 0, s = i % NMODE;
+                const int qa = __shfl_sync(0xffffffffu, ent.x, pr), qb = __shfl_sync(0xffffffffu, ent.y, pr);
+                wv[k] = i < EPT * NMODE       ? om0[(size_t)qa * NMODE + s]
+                        : i < 2 * EPT * NMODE ? omg[(size_t)qb * NMODE + s]
+                        : i < NW              ? omg[(size_t)rec.x * NMODE + s]
+                                              : 0.0;
+            }
+        };
+        if (nt > 0) load_w(entA, recA);
         bool abort = false;
-        int filled = -1, issued = -1;  // last tile whose copies / MMAs were issued
-        for (int j = 0; j <= nt && !abort; ++j) {
-            if (j >= 1) {
-                // (a) MMAs of tile j-1 once its operands have landed; its TMEM columns were freed when
-                // the stage's previous tile (j-3) was drained, which the fill of j-1 waited for
-                const int jm = j - 1, s = jm & 1, u = jm >> 1;
-                TcStage& G = S.st[s];
-                bool ok = true;
-                if (lane == 0) {
-                    ok = tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS);
-                    if (ok) {
-                        tc::fence_after_sync();
-                        const uint32_t idesc = tc::idesc_bf16(128, 48);
-                        const uint32_t pa = tc::smem_u32(&G.P[QS * 8]), pb = tc::smem_u32(&G.B[0]);
-                        for (int mu = 0; mu < 2; ++mu) {
-                            const uint32_t d = tm + (uint32_t)(s * 128 + mu * 64);
-                            for (int kk = 0; kk < KP / 16; ++kk) {
-                                const uint32_t ko = (uint32_t)kk * 2u * LBO;
-                                const uint64_t ah = tc::sdesc(pa + mu * 768 + ko, LBO, PB);
-                                const uint64_t bh = tc::sdesc(pb + mu * B_BYTES + ko, LBO, SBO);
-                                tc::mma_bf16(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
-                                if (SPLIT) {
-                                    const uint64_t al = tc::sdesc(pa + (2 + mu) * 768 + ko, LBO, PB);
-                                    const uint64_t bl = tc::sdesc(pb + (2 + mu) * B_BYTES + ko, LBO, SBO);
-                                    tc::mma_bf16(d, ah, bl, idesc, 1u);
-                                    tc::mma_bf16(d, al, bh, idesc, 1u);
-                                }
-                            }
-                        }
-                        tc::mma_commit(tc::smem_u32(&S.full[s]));
-                        issued = jm;
-                    }
-                }
-                issued = __shfl_sync(0xffffffffu, issued, 0);
-                if (__any_sync(0xffffffffu, !ok)) {
-                    if (lane == 0) atomicExch(err, 1);
-                    abort = true;
-                    break;
-                }
+        int filled = -1;
+        for (int j = 0; j < nt; ++j) {
+            const int es = j % NEP, os = j % NOP;
+            bool ok = true;
+            if (j >= NEP) ok = tc::mbar_wait(tc::smem_u32(&S.empty[es]), (uint32_t)(((j - NEP) / NEP) & 1), MAX_SPINS);
+            if (ok && j >= NOP) ok = tc::mbar_wait(tc::smem_u32(&S.opfree[os]), (uint32_t)(((j - NOP) / NOP) & 1), MAX_SPINS);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0) atomicExch(err, 1);
+                abort = true;
+                break;
             }
-            if (j < nt) {
-                // (b) fill stage j & 1 with tile j
-                const int s = j & 1, u = j >> 1;
-                TcStage& G = S.st[s];
-                // every lane waits, so each one observes the completed copies it reads or overwrites
-                bool ok = true;
-                if (u > 0) ok = tc::mbar_wait(tc::smem_u32(&S.empty[s]), (uint32_t)((u - 1) & 1), MAX_SPINS);
-                if (ok && j > 0) ok = tc::mbar_wait(tc::smem_u32(&S.pfb[j & 1]), (uint32_t)(((j - 1) >> 1) & 1), MAX_SPINS);
-                if (ok && j >= 2) ok = tc::mbar_wait(tc::smem_u32(&S.trb[j & 3]), (uint32_t)(((j - 2) >> 2) & 1), MAX_SPINS);
-                if (ok && j + 1 < nt && j >= 1)
-                    ok = tc::mbar_wait(tc::smem_u32(&S.trb[(j + 1) & 3]), (uint32_t)(((j - 1) >> 2) & 1), MAX_SPINS);
-                if (__any_sync(0xffffffffu, !ok)) {
-                    if (lane == 0) atomicExch(err, 1);
-                    abort = true;
-                    break;
+            EpStage& E = S.ep[es];
+            OpStage& O = S.op[os];
+            const int q1 = recA.x, ne = recA.z;
+            // gather rows for lane 0: q2 of pairs 0..15 (pairs beyond ne repeat pair 0)
+            int rows[EPT];
+#pragma unroll
+            for (int k = 0; k < EPT; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, k < ne ? k : 0);
+            const uint32_t rb = tc::smem_u32(&S.ready[es]);
+            if (lane == 0) {
+                const bool newb = O.q1 != q1;
+                const int ngroups = (ne + 3) / 4;
+                E.ne = ne;
+                E.q1 = q1;
+                O.q1 = q1;
+                tc::mbar_expect_tx(rb, (uint32_t)(ngroups * H * 4 * PB + (newb ? 2 * H * B_BYTES : 0)));
+#pragma unroll
+                for (int g = 0; g < EPT / 4; ++g) {
+                    if (g >= ngroups) break;
+#pragma unroll
+                    for (int part = 0; part < H; ++part)
+                        tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[4 * g],
+                                        rows[4 * g + 1], rows[4 * g + 2], rows[4 * g + 3], rb);
                 }
-                const int4 tile = S.trec[j & 3];
-                const int q1 = tile.x, ne = tile.z;
-                const int4* ent = S.pf[j & 1];
-                const bool newb = G.q1 != q1;
-                if (lane < ne) G.ent[lane] = ent[lane];
-                __syncwarp();
-                const uint32_t rb = tc::smem_u32(&S.ready[s]);
-                if (lane == 0) {
-                    G.ne = ne;
-                    G.q1 = q1;
-                    uint32_t bytes = (uint32_t)ne * (uint32_t)(PB + 384);
-                    if (newb) bytes += (uint32_t)(2 * H * B_BYTES + QS * 8);
-                    tc::mbar_arrive_tx(rb, bytes);
-                }
-                __syncwarp();
-                if (lane < ne) {
-                    const int4 en = ent[lane];
-                    tc::bulk_g2s(tc::smem_u32(&G.P[lane * PB]), rec + (size_t)en.y * RSD, (uint32_t)PB, rb);
-                    tc::bulk_g2s(tc::smem_u32(&G.q0d[lane][0]), q0tab + (size_t)en.x * Q0ROW, 384u, rb);
-                }
-                if (newb && lane == 30)
-                    tc::bulk_g2s(tc::smem_u32(&G.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
-                if (newb && lane == 31) tc::bulk_g2s(tc::smem_u32(&G.q1d[0]), rec + (size_t)q1 * RSD, (uint32_t)QS * 8u, rb);
-                // prefetch: entry records of tile j+1, tile record j+2
-                if (lane == 0 && j + 1 < nt) {
-                    const int4 nx = S.trec[(j + 1) & 3];
-                    const uint32_t pb = tc::smem_u32(&S.pfb[(j + 1) & 1]);
-                    tc::mbar_arrive_tx(pb, (uint32_t)nx.z * 16u);
-                    tc::bulk_g2s(tc::smem_u32(&S.pf[(j + 1) & 1][0]), entrec + nx.y, (uint32_t)nx.z * 16u, pb);
-                }
-                if (lane == 0 && j + 2 < nt) {
-                    const uint32_t tb = tc::smem_u32(&S.trb[(j + 2) & 3]);
-                    tc::mbar_arrive_tx(tb, 16u);
-                    tc::bulk_g2s(tc::smem_u32(&S.trec[(j + 2) & 3]), tiles + t0 + j + 2, 16u, tb);
-                }
-                filled = j;
+                if (newb) tc::bulk_g2s(tc::smem_u32(&O.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
             }
+            if (lane < ne) E.ent[lane] = entA;
+#pragma unroll
+            for (int k = 0; k < (NW + 31) / 32; ++k) {
+                const int i = lane + 32 * k;
+                if (i < EPT * NMODE) E.w0[i / NMODE][i % NMODE] = wv[k];
+                else if (i < 2 * EPT * NMODE) E.w2[(i - EPT * NMODE) / NMODE][i % NMODE] = wv[k];
+                else if (i < NW) E.w1[i % NMODE] = wv[k];
+            }
+            tc::mbar_arrive(rb);  // each lane releases its own stores
+            filled = j;
+            // loads for later fills
+            if (j + 1 < nt) load_w(entB, recB);
+            const int4 entC = (j + 2 < nt && lane < recC.z) ? entrec[recC.y + lane] : z4;
+            const int4 recD = j + 3 < nt ? tiles[t0 + j + 3] : z4;
+            recA = recB;
+            recB = recC;
+            recC = recD;
+            entA = entB;
+            entB = entC;
         }
         if (abort && lane == 0) {
-            // Error path: wait (bounded) for the copies and MMAs still in flight before the CTA
-            // releases its shared memory and TMEM.
-            for (int t = issued + 1; t <= filled; ++t)
-                tc::mbar_wait(tc::smem_u32(&S.ready[t & 1]), (uint32_t)((t >> 1) & 1), MAX_SPINS);
-            if (filled >= 0 && filled + 1 < nt)
-                tc::mbar_wait(tc::smem_u32(&S.pfb[(filled + 1) & 1]), (uint32_t)((filled >> 1) & 1), MAX_SPINS);
-            for (int t = max(2, filled + 1); t <= filled + 2 && t < nt; ++t)
-                tc::mbar_wait(tc::smem_u32(&S.trb[t & 3]), (uint32_t)(((t - 2) >> 2) & 1), MAX_SPINS);
-            if (issued >= 0)
-                tc::mbar_wait(tc::smem_u32(&S.full[issued & 1]), (uint32_t)((issued >> 1) & 1), MAX_SPINS);
+            // Error path: wait (bounded) for the copies still in flight before the CTA releases its
+            // shared memory.
+            for (int t = max(0, filled - NEP + 1); t <= filled; ++t)
+                tc::mbar_wait(tc::smem_u32(&S.ready[t % NEP]), (uint32_t)((t / NEP) & 1), MAX_SPINS);
         }
+    } else if (warp == EPI_WARPS + 1) {
+        // ------------------------------------------------------------ MMA warp
+        // Tile j's MMAs once its operands have landed (ready); its accumulator was drained before the
+        // fill of j (which waited for empty), its operands stay until the commit to opfree.
+        int issued = -1;
+        if (lane == 0) {
+            for (int j = 0; j < nt; ++j) {
+                const int es = j % NEP, os = j % NOP;
+                if (!tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)((j / NEP) & 1), MAX_SPINS)) {
+                    atomicExch(err, 1);
+                    break;
+                }
+                tc::fence_after_sync();
+                const uint32_t idesc = tc::idesc_bf16(128, 48);
+                const uint32_t pa = tc::smem_u32(&S.op[os].A[0][0]), pl = tc::smem_u32(&S.op[os].A[1][0]);
+                const uint32_t pb = tc::smem_u32(&S.op[os].B[0]);
+#pragma unroll
+                for (int mu = 0; mu < 2; ++mu) {
+                    const uint32_t d = tm + (uint32_t)(es * 128 + mu * 64);
+#pragma unroll
+                    for (int kk = 0; kk < KP / 16; ++kk) {
+                        const uint32_t ko = (uint32_t)kk * 2u * LBO;
+                        const uint64_t ah = tc::sdesc(pa + mu * 768 + ko, LBO, PB);
+                        const uint64_t bh = tc::sdesc(pb + mu * B_BYTES + ko, LBO, SBO);
+                        tc::mma_bf16(d, ah, bh, idesc, kk > 0 ? 1u : 0u);
+                        if (SPLIT) {
+                            const uint64_t al = tc::sdesc(pl + mu * 768 + ko, LBO, PB);
+                            const uint64_t bl = tc::sdesc(pb + (2 + mu) * B_BYTES + ko, LBO, SBO);
+                            tc::mma_bf16(d, ah, bl, idesc, 1u);
+                            tc::mma_bf16(d, al, bh, idesc, 1u);
+                        }
+                    }
+                }
+                tc::mma_commit(tc::smem_u32(&S.full[es]));
+                tc::mma_commit(tc::smem_u32(&S.opfree[os]));
+                issued = j;
+            }
+            // the last commit tracks every MMA issued: wait (bounded) before TMEM is released
+            if (issued >= 0)
+                tc::mbar_wait(tc::smem_u32(&S.full[issued % NEP]), (uint32_t)((issued / NEP) & 1), MAX_SPINS);
+        }
+        __syncwarp();
     } else {
-        // ------------------------------------------------------------ epilogue
+        // ------------------------------------------------------------ epilogue warps
         const int wq = warp & 3, grp = warp >> 2;  // lane quarter, s0 pair (2 grp, 2 grp + 1)
-        const int e = 4 * wq + lane / 8, s2 = lane % 8;
+        const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
         const float Rf = (float)(sqrt(EXP_CUT / a.half_os2) * 1.0001 + 1e-3);
-        const int etid = tid;  // 0 .. EPI_THREADS-1
+        TcItem* region = items + (size_t)blockIdx.x * a.cap;
+        // (s0, s1) slots allowed by the mode ranges and the Gamma acoustic rule (q1 = Gamma: amask_g)
+        unsigned s1m = 0u;
+#pragma unroll
+        for (int s1 = 0; s1 < NMODE; ++s1) s1m |= (s1 >= a.lo[1] && s1 <= a.hi[1]) ? (1u << s1) : 0u;
+        const unsigned s0m = ((grp * 2 >= a.lo[0] && grp * 2 <= a.hi[0]) ? 0x3fu : 0u) |
+                             ((grp * 2 + 1 >= a.lo[0] && grp * 2 + 1 <= a.hi[0]) ? 0xfc0u : 0u);
+        const unsigned amask_n = (s1m | (s1m << NMODE)) & s0m, amask_g = amask_n & ~0x1c7u;
         for (int j = 0; j < nt; ++j) {
-            const int s = j & 1, u = j >> 1;
-            TcStage& G = S.st[s];
-            // every thread waits on both barriers: the copies and the accumulator it reads
-            if (!(tc::mbar_wait(tc::smem_u32(&S.ready[s]), (uint32_t)(u & 1), MAX_SPINS) &&
-                  tc::mbar_wait(tc::smem_u32(&S.full[s]), (uint32_t)(u & 1), MAX_SPINS)))
-                S.abort_e = 1;
-            tc::named_bar(2, EPI_THREADS);
-            if (S.abort_e) {
-                if (etid == 0) atomicExch(err, 1);
+            const int es = j % NEP, u = j / NEP;
+            const EpStage& E = S.ep[es];
+            const bool ok = tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)(u & 1), MAX_SPINS) &&
+                            tc::mbar_wait(tc::smem_u32(&S.full[es]), (uint32_t)(u & 1), MAX_SPINS);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0) atomicExch(err, 1);
                 break;
             }
             tc::fence_after_sync();
-            float y[2][48];
+            float y[2][BROWS];  // this row's Y: (Re, Im) x (a, s1) per mu
             {
-                const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(s * 128);
+                const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(es * 128);
                 tc::tmem_ld16(ta, y[0]);
                 tc::tmem_ld16(ta + 16, y[0] + 16);
-                tc::tmem_ld16(ta + 32, y[0] + 32);
+                tc::tmem_ld4(ta + 32, y[0] + 32);
                 tc::tmem_ld16(ta + 64, y[1]);
                 tc::tmem_ld16(ta + 80, y[1] + 16);
-                tc::tmem_ld16(ta + 96, y[1] + 32);
-                tc::tmem_ld_wait();
+                tc::tmem_ld4(ta + 96, y[1] + 32);
             }
-            const int ne = G.ne;
-            const bool valid = s2 < NMODE && e < ne;
-            const int4 en = valid ? G.ent[e] : make_int4(0, 0, 0, 0);
-            const bool row_on = valid && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
-            const bool gq1 = G.q1 == 0;
-            const double* q1d = G.q1d;
-            const double* q2d = reinterpret_cast<const double*>(&G.P[(valid ? e : 0) * PB]);
-            const double* q0d = G.q0d[valid ? e : 0];
-            const double w2 = q2d[valid ? s2 : 0];
+            // shared-memory reads that do not depend on the accumulator, issued before its wait
+            const int ne = E.ne, q1 = E.q1;
+            const int4 en = E.ent[e];
+            const double w2 = E.w2[e][s2c];
+            const double w0a = E.w0[e][grp * 2], w0b = E.w0[e][grp * 2 + 1];
+            float w1f[NMODE];
+#pragma unroll
+            for (int s1 = 0; s1 < NMODE; ++s1) w1f[s1] = (float)E.w1[s1];
+            tc::tmem_ld_wait();
+            const bool row_on = s2 < NMODE && e < ne && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
+            const unsigned amask = q1 == 0 ? amask_g : amask_n;
             // FP32 screen: bit 6*jj + s1 marks (s0 = 2 grp + jj, s1) inside the delta window
+            // |w0 - w2 -+ w1| < R  or  |w0 + w2 - w1| < R; the first pair is ||w1| - |w0 - w2|| < R.
             unsigned act = 0u;
             if (row_on) {
 #pragma unroll
                 for (int jj = 0; jj < 2; ++jj) {
-                    const int s0 = grp * 2 + jj;
-                    if (s0 < a.lo[0] || s0 > a.hi[0]) continue;
-                    const double w0 = q0d[36 + s0];
-                    const float af = (float)(w0 - w2), bf = (float)(w0 + w2);
+                    const double w0 = jj ? w0b : w0a;
+                    const float c = fabsf((float)(w0 - w2)), bf = (float)(w0 + w2);
 #pragma unroll
                     for (int s1 = 0; s1 < NMODE; ++s1) {
-                        const float w1 = (float)q1d[s1];
-                        const bool in = fabsf(af - w1) < Rf || fabsf(af + w1) < Rf || fabsf(bf - w1) < Rf;
-                        const bool allowed = s1 >= a.lo[1] && s1 <= a.hi[1] && !(gq1 && s1 < 3);
-                        act |= (in && allowed) ? (1u << (jj * NMODE + s1)) : 0u;
+                        const bool in = fabsf(fabsf(w1f[s1]) - c) < Rf || fabsf(bf - w1f[s1]) < Rf;
+                        act |= in ? (1u << (jj * NMODE + s1)) : 0u;
                     }
                 }
+                act &= amask;
             }
-            // Compaction: the screened triples of the whole tile go to a shared queue (several passes if
-            // it fills), and all epilogue threads evaluate them one per thread, so the FP64 work runs
-            // with full warps; each triple's contribution goes straight to the output.
-            for (;;) {
-                if (act) {
-                    const int n = __popc(act);
-                    const int base = atomicAdd(&S.qn, n);
-                    for (int i = 0; i < n && base + i < QCAP; ++i) {
-                        const int bit = __ffs(act) - 1;
-                        act &= act - 1u;
-                        const int jj = bit / NMODE, s1 = bit % NMODE;
-                        QItem& it = S.q[base + i];
-#pragma unroll
-                        for (int k = 0; k < 6; ++k) {
-                            float r = 0.0f, im = 0.0f;
-#pragma unroll
-                            for (int c1 = 0; c1 < NMODE; ++c1) {
-                                r = (c1 == s1) ? y[k / 3][(k % 3) * NMODE + c1] : r;
-                                im = (c1 == s1) ? y[k / 3][18 + (k % 3) * NMODE + c1] : im;
-                            }
-                            it.yr[k] = r;
-                            it.yi[k] = im;
-                        }
-                        it.meta = e | (s2 << 8) | ((grp * 2 + jj) << 12) | (s1 << 16);
-                    }
-                    if (act) S.qmore = 1;
-                }
-                tc::named_bar(2, EPI_THREADS);
-                const int cnt = min(S.qn, QCAP);
-                for (int i = etid; i < cnt; i += EPI_THREADS) {
-                    const QItem& it = S.q[i];
-                    const int ie = it.meta & 0xff, is2 = (it.meta >> 8) & 0xf, s0 = (it.meta >> 12) & 0xf,
-                              s1 = (it.meta >> 16) & 0xf;
-                    const int4 ien = G.ent[ie];
-                    const double* p0 = G.q0d[ie];
-                    const double* p2 = reinterpret_cast<const double*>(&G.P[ie * PB]);
-                    const double w0 = p0[36 + s0], w1d = q1d[s1], w2d = p2[is2];
-                    const double d1 = w0 - w1d - w2d, d2 = w0 + w1d - w2d, d3 = w0 - w1d + w2d;
-                    const double x1 = a.half_os2 * (d1 * d1), x2 = a.half_os2 * (d2 * d2), x3 = a.half_os2 * (d3 * d3);
-                    const double e1 = x1 < EXP_CUT ? a.pre * exp(-x1) : 0.0;
-                    const double e2 = x2 < EXP_CUT ? a.pre * exp(-x2) : 0.0;
-                    const double e3 = x3 < EXP_CUT ? a.pre * exp(-x3) : 0.0;
-                    const double wt = (double)ien.z;
-                    const double p3 = e1 + e2 + e3;
-                    if (p3 != 0.0) atomicAdd(&out_p3[(size_t)ien.x * NMODE + s0], wt * p3);
-                    if (ien.w != 0 && s0 < 3) continue;  // W = 0 for the Gamma acoustic modes of q0
-                    const float2* e0 = reinterpret_cast<const float2*>(p0) + s0 * NMODE;
-                    float pr = 0.0f, pim = 0.0f;
-#pragma unroll
-                    for (int k = 0; k < 6; ++k) {
-                        const float2 c = e0[k];
-                        pr = fmaf(c.x, it.yr[k], fmaf(-c.y, it.yi[k], pr));
-                        pim = fmaf(c.x, it.yi[k], fmaf(c.y, it.yr[k], pim));
-                    }
-                    const double W = (double)(pr * pr + pim * pim) * (p0[42 + s0] * p2[6 + is2] * q1d[6 + s1]) * a.mfac;
-                    const double we1 = wt * W * e1, wf2 = wt * W * (e2 - e3);
-                    for (int T = 0; T < a.nT; ++T) {
-                        const double n1 = q1d[12 + 6 * T + s1], n2 = p2[12 + 6 * T + is2];
-                        const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
-                        if (v != 0.0) atomicAdd(&out_lw[((size_t)T * a.nq0 + ien.x) * NMODE + s0], v);
-                    }
-                }
-                const int more = S.qmore;
-                tc::named_bar(2, EPI_THREADS);
-                if (etid == 0) {
-                    S.qn = 0;
-                    S.qmore = 0;
-                }
-                tc::named_bar(2, EPI_THREADS);
-                if (!more) break;
-            }
+            // Reserve room in the CTA's region, release the stage (every read of it is done), then
+            // append the active triples slot by slot in lane order.
+            const int tot = __reduce_add_sync(0xffffffffu, (unsigned)__popc(act));
+            int base = 0;
+            if (lane == 0 && tot > 0) base = atomicAdd(&S.ihead, tot);
+            base = __shfl_sync(0xffffffffu, base, 0);
             tc::fence_before_sync();
             __syncwarp();
-            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[s]));
+            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
+            if (tot > 0) {
+                const unsigned lt = (1u << lane) - 1u;
+                const unsigned any = __reduce_or_sync(0xffffffffu, act);
+                const int kw = en.z == 2 ? (1 << 30) : 0;
+#pragma unroll
+                for (int jj = 0; jj < 2; ++jj) {
+                    const int s0 = grp * 2 + jj;
+                    const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
+#pragma unroll
+                    for (int s1 = 0; s1 < NMODE; ++s1) {
+                        if (!((any >> (jj * NMODE + s1)) & 1u)) continue;
+                        const bool has = (act >> (jj * NMODE + s1)) & 1u;
+                        const unsigned m = __ballot_sync(0xffffffffu, has);
+                        const int pos = base + __popc(m & lt);
+                        if (has && pos < a.cap) {
+                            float4* dst = reinterpret_cast<float4*>(region + pos);
+                            dst[0] = make_float4(y[0][s1], y[0][6 + s1], y[0][12 + s1], y[1][s1]);
+                            dst[1] = make_float4(y[1][6 + s1], y[1][12 + s1], y[0][18 + s1], y[0][24 + s1]);
+                            dst[2] = make_float4(y[0][30 + s1], y[1][18 + s1], y[1][24 + s1], y[1][30 + s1]);
+                            reinterpret_cast<int4*>(dst)[3] = make_int4(k0, q1 * NMODE + s1, en.y * NMODE + s2, 0);
+                        }
+                        base += __popc(m);
+                    }
+                }
+            }
         }
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (warp == 0) tc::tmem_dealloc(tm, 256);
+    if (warp == 0) tc::tmem_dealloc(tm, TC_COLS);
+    if (tid == 0) counts[blockIdx.x] = S.ihead;
 }
 
-template <int NTM, bool SPLIT>
-int launch_tc(spring_ctx* c, TcArgs a, double* lw, double* p3) {
+// FP64 part of the active triples: Phi = sum_k e0'(k, s0) Y_k (FP32), W = wt mfac |Phi|^2 /
+// (omega0 omega1 omega2), the three Gaussian delta weights, then the phase-space and linewidth
+// sums with atomics: P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].
+// Block (r, y) walks region r of the item list.
+__global__ void __launch_bounds__(256) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
+                                                   int cap, int nq, int nq0, int nT, double half_os2, double pre,
+                                                   double mfac, const double* __restrict__ q0tab,
+                                                   const double* __restrict__ om0, const double* __restrict__ ob0,
+                                                   const double* __restrict__ omg, const double* __restrict__ obg,
+                                                   const double* __restrict__ nbe, double* __restrict__ out_lw,
+                                                   double* __restrict__ out_p3) {
+    const int r = blockIdx.x;
+    const int n = min(counts[r], cap);
+    const TcItem* reg = items + (size_t)r * cap;
+    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += gridDim.y * blockDim.x) {
+        const float4* src = reinterpret_cast<const float4*>(reg + i);
+        const float4 v0 = src[0], v1 = src[1], v2 = src[2];
+        const int4 kk = reinterpret_cast<const int4*>(src)[3];
+        const int o = kk.x & 0x1fffffff, q0 = o / NMODE, s0 = o % NMODE;
+        const double w0 = om0[o], w1 = omg[kk.y], w2 = omg[kk.z];
+        const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
+        const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
+        const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
+        const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
+        const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
+        const double wt = (kk.x >> 30) & 1 ? 2.0 : 1.0;
+        const double p3 = e1 + e2 + e3;
+        if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
+        if ((kk.x >> 29) & 1) continue;  // W = 0 for the Gamma acoustic modes of q0
+        const float yr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y}, yi[6] = {v1.z, v1.w, v2.x, v2.y, v2.z, v2.w};
+        const float2* e0 = reinterpret_cast<const float2*>(q0tab + (size_t)q0 * Q0ROW) + s0 * NMODE;
+        float pr = 0.0f, pim = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float2 c = e0[k];
+            pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
+            pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+        }
+        const double W = (double)(pr * pr + pim * pim) * (ob0[o] * obg[kk.z] * obg[kk.y]) * mfac * wt;
+        const double we1 = W * e1, wf2 = W * (e2 - e3);
+        for (int T = 0; T < nT; ++T) {
+            const size_t tb = (size_t)T * nq * NMODE;
+            const double n1 = nbe[tb + kk.y], n2 = nbe[tb + kk.z];
+            const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
+            if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
+        }
+    }
+}
+
+// Tensor map of the A table as a 2-D array of 8-byte elements: rows = grid points, 384 columns
+// (the [hi, lo][mu] images of one point, 3072 bytes), box 192 x 1 (one part of one row).
+int make_tmap_a(spring_ctx* c, CUtensorMap* tm) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return fail(c, SPRING_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+        encode = reinterpret_cast<Encode>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)(4 * AIMG / 4), (cuuint64_t)c->nq};
+    const cuuint64_t strides[1] = {(cuuint64_t)(4 * AIMG * 2)};
+    const cuuint32_t box[2] = {(cuuint32_t)(2 * AIMG * 2 / 8), 1u};
+    const cuuint32_t estr[2] = {1u, 1u};
+    const CUresult r = encode(tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, c->d_tc_a.p, dims, strides, box, estr,
+                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(c, SPRING_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return SPRING_OK;
+}
+
+template <bool SPLIT>
+int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     const size_t smem = sizeof(TcSmem);
+    alignas(64) CUtensorMap tmA;
+    SPRING_CHECK(make_tmap_a(c, &tmA));
     if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "tensor-core V3 needs %zu bytes of shared memory", smem);
-    cudaFuncSetAttribute(k_v3tc<NTM, SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
-    const int ctas = std::max(1, std::min(a.ntiles, sms));
-    a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
-    const int grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
+    cudaFuncSetAttribute(k_v3tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
-    k_v3tc<NTM, SPLIT><<<grid, TC_THREADS, smem, c->stream>>>(
-        a, c->d_tc_tiles.p, c->d_tc_rec.p, c->d_tc_q.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p),
-        c->d_tc_q0.p, lw, p3, c->d_tc_err.p);
+    k_v3tc<SPLIT><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
+        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p, c->ph_grid.omega.p, items,
+        c->d_tc_cnt_cta.p, c->d_tc_err.p);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -652,17 +692,15 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
 int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
                    bool* handled) {
     *handled = false;
-    if (c->nb != 2 || c->na3 > 8 || c->nT > 9) return SPRING_OK;
+    if (c->nb != 2 || c->na3 > 8) return SPRING_OK;
     const PairSet& ps = c->ps_irr;
     const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
     *handled = true;
     if (p1 == p0) return SPRING_OK;
     const int nq = c->nq;
-    const int ntm = c->nT == 1 ? 1 : (c->nT <= 3 ? 3 : 9);  // temperature bucket of the kernel instance
-    const int qs = 12 + 6 * ntm;
+    SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 4 * AIMG, "V3 A table"));
     SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 4 * BIMG, "V3 B table"));
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * Q0ROW, "V3 q0 rows"));
-    SPRING_CHECK(dalloc(c, c->d_tc_q, (size_t)nq * (qs + AREC), "V3 grid records"));
     SPRING_CHECK(dalloc(c, c->d_tc_err, 1, "V3 status"));
     SPRING_CHECK(zero(c, c->d_tc_err.p, sizeof(int), "V3 status"));
     SPRING_CHECK(build_tiles(c, p0, p1));
@@ -671,8 +709,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     {
         const long long tot = (long long)nq * 2 * 8 * KP;
         k_tc_tab_a<<<(int)std::min<long long>((tot + threads - 1) / threads, 148LL * 16), threads, 0, c->stream>>>(
-            nq, c->na3, qs, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
-            c->d_tc_q.p);
+            nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
+            reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
         SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
     }
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
@@ -684,35 +722,56 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     k_tc_q0tab<<<std::max(1, std::min((c->nq0 * 48 + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
         c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p, c->d_tc_q0.p);
     SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_qtab<<<std::max(1, (int)std::min<long long>(((long long)nq * qs + threads - 1) / threads, 148LL * 8)), threads,
-                0, c->stream>>>(nq, c->nT, qs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_tc_q.p);
-    SPRING_CHECK(launch_check(c, "k_tc_qtab"));
 
     TcArgs a{};
     a.nq = nq;
     a.nq0 = c->nq0;
     a.nT = c->nT;
-    a.qs = qs;
     a.ntiles = c->tc_ntiles;
     for (int k = 0; k < 3; ++k) {
         a.lo[k] = pol.lo[k];
         a.hi[k] = pol.hi[k];
     }
-    a.mfac = host_constants().Sctr3THz2 / double(nq);
     const double os = 1.0 / sigma;
     a.half_os2 = 0.5 * (os * os);
-    a.pre = os * ONEBYSQRT2PI;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int ctas = std::max(1, std::min(a.ntiles, sms));
+    a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
+    c->tc_grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
+    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, c->tc_grid, "V3 item counts"));
+    // Item list: one region per CTA, first sized for 4 % of the CTA's mode triples (about 1-2 % pass
+    // the screen on meshes from 8^3 to 24^3), regrown to what the pass reports if that overflows.
+    const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE;
+    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 25, 1024);
     const bool split = c->precision == SPRING_BF16X3;
-    int rc;
-    if (c->nT == 1) rc = split ? launch_tc<1, true>(c, a, d_lw, d_p3) : launch_tc<1, false>(c, a, d_lw, d_p3);
-    else if (c->nT <= 3) rc = split ? launch_tc<3, true>(c, a, d_lw, d_p3) : launch_tc<3, false>(c, a, d_lw, d_p3);
-    else rc = split ? launch_tc<9, true>(c, a, d_lw, d_p3) : launch_tc<9, false>(c, a, d_lw, d_p3);
-    SPRING_CHECK(rc);
-    int herr = 0;
-    SPRING_CHECK(d2h(c, &herr, c->d_tc_err.p, sizeof(int), "V3 status"));
-    if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
-    return SPRING_OK;
+    std::vector<int> cnt(c->tc_grid);
+    int maxcnt = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        cap = std::min<long long>(cap, triples);
+        a.cap = (int)cap;
+        SPRING_CHECK(dalloc(c, c->d_tc_items, (size_t)c->tc_grid * cap * (sizeof(TcItem) / sizeof(float4)), "V3 items"));
+        TcItem* items = reinterpret_cast<TcItem*>(c->d_tc_items.p);
+        SPRING_CHECK(split ? launch_tc<true>(c, a, items) : launch_tc<false>(c, a, items));
+        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * c->tc_grid, "V3 item counts"));
+        int herr = 0;
+        SPRING_CHECK(d2h(c, &herr, c->d_tc_err.p, sizeof(int), "V3 status"));
+        if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
+        if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
+        maxcnt = *std::max_element(cnt.begin(), cnt.end());
+        if (maxcnt <= cap) break;
+        cap = (long long)(maxcnt * 1.25) + 1024;  // the pass only wrote what fit; run it again
+    }
+    if (maxcnt > cap) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: item list overflow");
+    c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
+    if (maxcnt == 0) return SPRING_OK;
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
+    const dim3 grid(c->tc_grid, std::max(1, std::min(64, (maxcnt + 4 * threads - 1) / (4 * threads))));
+    k_v3tc_eval<<<grid, threads, 0, c->stream>>>(
+        reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, nq, c->nq0, c->nT, a.half_os2,
+        os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), c->d_tc_q0.p, c->ph_irr.omega.p, c->ph_irr.oneby.p,
+        c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, d_lw, d_p3);
+    return launch_check(c, "k_v3tc_eval");
 }
 
 }  // namespace spring

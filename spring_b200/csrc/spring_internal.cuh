@@ -174,9 +174,13 @@ struct spring_ctx {
     spring::DBuf<double> d_wiso;   // [slot][q1][s0][s1]
 
     // tensor-core V3 (spring_set_precision): operand tables and pair tiles grouped by q1
+    spring::DBuf<uint16_t> d_tc_a;     // bf16 A operand images [q][hi, lo][mu]
     spring::DBuf<uint16_t> d_tc_b;     // bf16 B operand images [q1][hi, lo][mu]
     spring::DBuf<double> d_tc_q0;      // packed q0 rows: e0' float2[36], omega[6], 1/omega[6]
-    spring::DBuf<double> d_tc_q;       // grid records: omega[6], 1/omega[6], nBE[T][6], then the A operand images
+    spring::DBuf<float4> d_tc_items;   // active mode triples, one region per CTA (64 bytes each)
+    spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA
+    int tc_grid = 0;
+    double tc_cap_frac = 0.0;          // item region size as a fraction of the CTA's triples
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
