@@ -66,6 +66,9 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
 
 BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
 TC_EPT = 16         # pairs per tensor-core tile
+# DRAM bytes per pair of the tensor-core pass (read + write), from one ncu capture of the 16^3
+# rocksalt launch (297,076 pairs; 71.2 MB read, 18.2 MB written)
+TC_DRAM_BYTES_PER_PAIR = (71.164672e6 + 18.171648e6) / 297076
 
 
 def tc_issued_flops_per_tile(passes):
@@ -78,7 +81,7 @@ def tc_tiles(counts_by_q1):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (200 ms period)."""
+    """nvidia-smi sampling during the timed region (20 ms period)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -92,7 +95,7 @@ class Clocks:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                       "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -343,7 +346,8 @@ def run_ours(args):
             times.append(e0.elapsed_time(e1))
         torch.cuda.synchronize()
         launches = ctx.kernel_launches() - l0
-        kt = {k: ctx.kernel_time(k) for k in ("k_v3tc", "k_v3s", "k_v3<", "k_phonons", "k_tc_tab", "k_kappa")}
+        kt = {k: ctx.kernel_time(k) for k in ("k_v3tc<", "k_v3tc_eval", "k_v3s", "k_v3<", "k_phonons", "k_tc_tab",
+                                              "k_kappa")}
         ctx.set_profiling(False)
         clk = clocks.stop() if clocks else None
         ms = float(np.sum(times)) / args.steps
@@ -364,7 +368,7 @@ def run_ours(args):
         lw_err = float((np.abs(lw_p - lw64)[big] / lw64[big]).max())
         diag = [0, 4, 8]
         k_err = float(np.abs(kap_p[:, diag] / kap64[:, diag] - 1.0).max())
-        main_kernel = "k_v3tc" if args.precision != "fp64" else "k_v3s"
+        main_kernel = "k_v3tc<" if args.precision != "fp64" else "k_v3s"
         v3_ms, v3_n = kt[main_kernel] if kt[main_kernel][1] else kt["k_v3<"]
 
         # end to end through the public API: host inputs, pinned, copied every step
@@ -443,14 +447,24 @@ def run_ours(args):
         else:
             passes = 3 if args.precision == "bf16x3" else 1
             issued = tc_issued_flops_per_tile(passes) * tc_tiles(counts_by_q1)
-            achieved = issued / (v3_per_launch * 1e-3) / 1e12 if v3_n else None
+            algo = flops_pair * my_pairs
+            sec = v3_per_launch * 1e-3
+            achieved = algo / sec / 1e12 if v3_n else None
+            ev_ms, ev_n = kt["k_v3tc_eval"]
             roof = {"kernel": f"k_v3tc<{args.precision}>", "bound": "tensor", "achieved": achieved,
                     "peak": BF16_PEAK, "unit": "TFLOP/s", "frac": (achieved / BF16_PEAK) if achieved else None,
-                    "traffic": None,
+                    "traffic": TC_DRAM_BYTES_PER_PAIR * my_pairs,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM) of measured",
+                    "algorithmic_flops_per_launch": algo,
+                    "issued_mma_tflops": issued / sec / 1e12 if v3_n else None,
                     "issued_flops_per_launch": issued,
-                    "note": "issued tcgen05 MMA flops (M128 N48 K16 tiles, padding included); the kernel is bound "
-                            "by its epilogue and operand gathers, not by the tensor pipe"}
+                    "eval_kernel_ms_per_launch": ev_ms / max(ev_n, 1) if ev_n else None,
+                    "traffic_note": "dram read + write bytes per pair from an ncu capture of the 16^3 launch, "
+                                    "scaled by the pairs of this launch",
+                    "note": "achieved = algorithmic V3 flops (42336 per pair) / kernel time; issued_mma_tflops "
+                            "counts the tcgen05 MMAs as issued (M128 N48 K16 tiles, padding included).  The "
+                            "kernel is bound by its operand gathers and screening epilogue, not by the tensor "
+                            "pipe; the FP64 delta/rate part runs in k_v3tc_eval"}
         roof.update({"kernel_ms_per_launch": v3_per_launch, "kernel_share_of_step": v3_per_launch / ms,
                      "algorithmic_fp64_flops_per_pair": flops_pair})
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,

@@ -1,5 +1,5 @@
 // Three-phonon V3 on the 5th-generation tensor cores (tcgen05, BF16 in, FP32
-// accumulate), fused with the Gaussian linewidth sum.  Two-atom cells.
+// accumulate), with the Gaussian linewidth sum.  Two-atom cells.
 //
 // Same quantity as ScatterMatEl / ScatterProbability + CalculateLinewidth
 // (src/Kappa/Src/ThirdOrder_m.f90:278-439, 442-543), regrouped so that the
@@ -16,12 +16,15 @@
 //   B[(im, a s1)][k] = [Im Z | Re Z].
 // Precision: SPRING_BF16 rounds A and B to BF16 once; SPRING_BF16X3 splits each
 // into hi + lo BF16 parts and accumulates hi*hi + hi*lo + lo*hi (compensated).
-// Frequencies, occupations, the delta weights and every sum stay FP64.  The
-// epilogue screens each mode triple in FP32 against the window where a delta
-// weight can exceed exp(-40) of its peak (4e-18) and evaluates Phi, W and the
-// FP64 deltas only for the triples inside it (about 1-2 % of them).
-// Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass),
-// L2 bandwidth for gathering the U_q2 rows, FP32/FP64 ALU for the screen.
+// Frequencies, occupations, the delta weights and every sum stay FP64.  Two
+// passes: k_v3tc computes Y on the tensor cores and screens each mode triple in
+// FP32 against the window where a delta weight can exceed exp(-40) of its peak
+// (4e-18), writing the ~1-2 % inside it (with their Y values) to an item list;
+// k_v3tc_eval forms Phi, W and the FP64 delta weights of those and accumulates
+// the phase space and the linewidths.
+// Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass);
+// in practice the per-tile pipeline (TMA requests, FP32 screening issue) and, for
+// k_v3tc_eval, L2 latency of the scattered per-item loads.
 #include <algorithm>
 #include <vector>
 #include <cub/cub.cuh>
@@ -103,22 +106,16 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
                                                   const double* __restrict__ posr, const int* __restrict__ btyp,
                                                   const double* __restrict__ mrs, const double* __restrict__ qpnt,
                                                   const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
-    __shared__ double2 sU[24 * NMODE];  // [N b][s]
+    __shared__ double2 sU[24 * NMODE];                   // [N b][s]
+    __shared__ __align__(16) __nv_bfloat16 img[2][BIMG];  // hi, lo images of this (q1, mu), built here
     const int q = blockIdx.x / 2, mu = blockIdx.x % 2;
     const int KR = 3 * na;
     for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
         sU[i] = u_value(q, mu, i / NMODE, i % NMODE, na, posr, btyp, mrs, qpnt, evg);
+    for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // rows 36-47 and the K padding stay zero
+        reinterpret_cast<uint4*>(&img[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     const double* f = fc3 + (size_t)mu * na * na * 27;
-    __nv_bfloat16* out = tab + (size_t)q * 4 * BIMG + mu * BIMG;
-    const __nv_bfloat16 zero = __float2bfloat16_rn(0.0f);
-    for (int i = threadIdx.x; i < 48 * KP; i += blockDim.x) {  // zero rows 36-47 and the K padding
-        const int n = i / KP, k = i % KP;
-        if (n >= BROWS || k >= 2 * KR) {
-            out[bimg(n, k)] = zero;
-            out[2 * BIMG + bimg(n, k)] = zero;
-        }
-    }
     for (int i = threadIdx.x; i < 18 * KR; i += blockDim.x) {
         const int r = i / KR, k2 = i % KR;  // r = a*6 + s1, k2 = N2*3 + c
         const int al = r / NMODE, s1 = r % NMODE, N2 = k2 / 3, ga = k2 % 3;
@@ -133,13 +130,18 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         __nv_bfloat16 h, l;
         // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
         split_bf16(zr, h, l);
-        out[bimg(r, k2)] = h;                  out[2 * BIMG + bimg(r, k2)] = l;
-        out[bimg(18 + r, KR + k2)] = h;        out[2 * BIMG + bimg(18 + r, KR + k2)] = l;
+        img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
+        img[0][bimg(18 + r, KR + k2)] = h;     img[1][bimg(18 + r, KR + k2)] = l;
         split_bf16(-zi, h, l);
-        out[bimg(r, KR + k2)] = h;             out[2 * BIMG + bimg(r, KR + k2)] = l;
+        img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
         split_bf16(zi, h, l);
-        out[bimg(18 + r, k2)] = h;             out[2 * BIMG + bimg(18 + r, k2)] = l;
+        img[0][bimg(18 + r, k2)] = h;          img[1][bimg(18 + r, k2)] = l;
     }
+    __syncthreads();
+    constexpr int V = BIMG * 2 / 16;  // 16-byte vectors per image
+    uint4* out = reinterpret_cast<uint4*>(tab + (size_t)q * 4 * BIMG + mu * BIMG);
+    for (int i = threadIdx.x; i < 2 * V; i += blockDim.x)
+        out[(i / V) * 2 * V + i % V] = reinterpret_cast<const uint4*>(&img[0][0])[i];
 }
 
 // Packed q0 rows (Q0ROW doubles): e0' = m_mu^-1/2 e0(mu a, s0) as float2 [s0][row] (288 bytes), then
@@ -228,7 +230,6 @@ constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 sh
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int TC_THREADS = EPI_THREADS + 64;  // warp 12: TMA copies and frequency gathers; warp 13: MMA issue
 constexpr int TC_COLS = NEP * 128;
-constexpr int NW = EPT * NMODE * 2 + NMODE;   // frequencies gathered per tile
 
 // An active mode triple, written by k_v3tc for k_v3tc_eval: the row (pair, s2) of Y for its s1,
 // (Re, Im) Y[mu][a] with k = mu * 3 + a, and k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29,
@@ -289,24 +290,29 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         // ------------------------------------------------------------ fill warp
         // Records in registers, loaded ahead so that their latency stays hidden: tile records of
         // j .. j+3 (recA .. recD), entry lane of tiles j .. j+2 (entA .. entC), and the frequencies
-        // of tile j (wv, loaded during the fill of j-1).  No warp barrier follows a load: each lane
-        // arrives on ready itself, after its own stores and before it issues the next loads.
+        // of tile j (loaded during the fill of j-1: lane p < 16 holds pair p's q0 omegas, lane 16 + p
+        // pair p's q2 omegas, lane 0 also the q1 omegas).  No warp barrier follows a load: each lane
+        // arrives on ready itself, after its own copies and stores and before it issues new loads.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
         int4 entB = lane < recB.z ? entrec[recB.y + lane] : z4;
-        double wv[(NW + 31) / 32];
-        // frequencies of a tile (pairs beyond ne repeat pair 0): q0 omegas, q2 omegas, q1 omegas
+        double2 wv[3], wq1[3];
+        const int pw = lane & 15;  // pair whose omegas this lane moves
         auto load_w = [&](const int4& ent, const int4& rec) {
-#pragma unroll
-            for (int k = 0; k < (NW + 31) / 32; ++k) {
-                const int i = lane + 32 * k;
-                const int pe = (i % (EPT * NMODE)) / NMODE, pr = pe < rec.z ? pe : 0, s = i % NMODE;
-                const int qa = __shfl_sync(0xffffffffu, ent.x, pr), qb = __shfl_sync(0xffffffffu, ent.y, pr);
-                wv[k] = i < EPT * NMODE       ? om0[(size_t)qa * NMODE + s]
-                        : i < 2 * EPT * NMODE ? omg[(size_t)qb * NMODE + s]
-                        : i < NW              ? omg[(size_t)rec.x * NMODE + s]
-                                              : 0.0;
+            const int q2 = __shfl_sync(0xffffffffu, ent.y, pw);
+            if (pw < rec.z) {
+                const double2* src = reinterpret_cast<const double2*>(lane < 16 ? om0 + (size_t)ent.x * NMODE
+                                                                                 : omg + (size_t)q2 * NMODE);
+                wv[0] = src[0];
+                wv[1] = src[1];
+                wv[2] = src[2];
+            }
+            if (lane == 0) {
+                const double2* src = reinterpret_cast<const double2*>(omg + (size_t)rec.x * NMODE);
+                wq1[0] = src[0];
+                wq1[1] = src[1];
+                wq1[2] = src[2];
             }
         };
         if (nt > 0) load_w(entA, recA);
@@ -325,35 +331,38 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             EpStage& E = S.ep[es];
             OpStage& O = S.op[os];
             const int q1 = recA.x, ne = recA.z;
-            // gather rows for lane 0: q2 of pairs 0..15 (pairs beyond ne repeat pair 0)
-            int rows[EPT];
+            // lane l < 4 H gathers group g = l / H (pairs 4g .. 4g+3, beyond ne repeating pair 0),
+            // part l % H; lane 31 copies the B images when q1 changed.  Each issuing lane adds its
+            // own bytes to ready before its copy.
+            const int g = (lane / H) & 3, part = lane % H;
+            int rows[4];
 #pragma unroll
-            for (int k = 0; k < EPT; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, k < ne ? k : 0);
+            for (int k = 0; k < 4; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, 4 * g + k < ne ? 4 * g + k : 0);
             const uint32_t rb = tc::smem_u32(&S.ready[es]);
+            if (lane < 4 * H && 4 * g < ne) {
+                tc::mbar_expect_tx(rb, 4u * PB);
+                tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[0], rows[1], rows[2],
+                                rows[3], rb);
+            }
+            if (lane == 31 && O.q1 != q1) {
+                O.q1 = q1;
+                tc::mbar_expect_tx(rb, (uint32_t)(2 * H * B_BYTES));
+                tc::bulk_g2s(tc::smem_u32(&O.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
+            }
             if (lane == 0) {
-                const bool newb = O.q1 != q1;
-                const int ngroups = (ne + 3) / 4;
                 E.ne = ne;
                 E.q1 = q1;
-                O.q1 = q1;
-                tc::mbar_expect_tx(rb, (uint32_t)(ngroups * H * 4 * PB + (newb ? 2 * H * B_BYTES : 0)));
-#pragma unroll
-                for (int g = 0; g < EPT / 4; ++g) {
-                    if (g >= ngroups) break;
-#pragma unroll
-                    for (int part = 0; part < H; ++part)
-                        tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[4 * g],
-                                        rows[4 * g + 1], rows[4 * g + 2], rows[4 * g + 3], rb);
-                }
-                if (newb) tc::bulk_g2s(tc::smem_u32(&O.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
+                double2* d = reinterpret_cast<double2*>(E.w1);
+                d[0] = wq1[0];
+                d[1] = wq1[1];
+                d[2] = wq1[2];
             }
             if (lane < ne) E.ent[lane] = entA;
-#pragma unroll
-            for (int k = 0; k < (NW + 31) / 32; ++k) {
-                const int i = lane + 32 * k;
-                if (i < EPT * NMODE) E.w0[i / NMODE][i % NMODE] = wv[k];
-                else if (i < 2 * EPT * NMODE) E.w2[(i - EPT * NMODE) / NMODE][i % NMODE] = wv[k];
-                else if (i < NW) E.w1[i % NMODE] = wv[k];
+            if (pw < ne) {
+                double2* d = reinterpret_cast<double2*>(lane < 16 ? E.w0[pw] : E.w2[pw]);
+                d[0] = wv[0];
+                d[1] = wv[1];
+                d[2] = wv[2];
             }
             tc::mbar_arrive(rb);  // each lane releases its own stores
             filled = j;
@@ -766,7 +775,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
     if (maxcnt == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
-    const dim3 grid(c->tc_grid, std::max(1, std::min(64, (maxcnt + 4 * threads - 1) / (4 * threads))));
+    const dim3 grid(c->tc_grid, std::max(1, std::min(1024, (maxcnt + threads - 1) / threads)));
     k_v3tc_eval<<<grid, threads, 0, c->stream>>>(
         reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, nq, c->nq0, c->nT, a.half_os2,
         os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), c->d_tc_q0.p, c->ph_irr.omega.p, c->ph_irr.oneby.p,
