@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mesh4", type=int, default=12, help="mesh of the four-phonon leg (0 skips it)")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-workload leg")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
                     help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
     return ap.parse_args()
@@ -271,6 +272,83 @@ def fourph_leg(torch, mesh4, frac=0.1):
                                             "SiLU, trained on the GPU on exact 8^3 rates, BF16 inference"}
 
 
+BATCH_CELLS = (("rocksalt2", 12), ("rocksalt2", 16), ("rocksalt2", 20), ("rocksalt8", 8), ("rocksalt8", 10))
+# Gamma-X-W-K-Gamma-L in the fractional reciprocal basis, 200 points
+PATH_NODES = np.array([[0.0, 0.0, 0.0, 0], [0.0, 0.5, 0.5, 50], [0.25, 0.625, 0.625, 25], [0.375, 0.75, 0.375, 18],
+                       [0.0, 0.0, 0.0, 53], [0.5, 0.5, 0.5, 54]])
+
+
+def batched_leg(torch, steps=3):
+    """Batched uneven workload: the 2-atom cell at 12^3/16^3/20^3 and the 8-atom cubic cell at
+    8^3/10^3, 9 temperatures (100-900 K), Gaussian three-phonon linewidths of every irreducible q0
+    of all five in one persistent, graph-captured launch with the autotuned configuration; then
+    Gaussian linewidths at 200 path points (Gamma-X-W-K-Gamma-L) on the 2-atom 12^3 context.
+    Compared with each context's own spring_linewidth3 call (FP64) one after the other."""
+    from spring_b200 import synthetic as S
+    from spring_b200.api import Batch, from_crystal
+    temps = [100.0 * k for k in range(1, 10)]
+    cells = []
+    evals = 0
+    for name, N in BATCH_CELLS:
+        cr = S.build(name)
+        ctx, info = from_crystal(cr, (N, N, N), temps)
+        npairs = sum(ctx.enumerate3(i + 1)[2][0] for i in range(ctx.nq0))
+        evals += npairs * cr.ndof ** 3
+        cells.append((name, N, ctx, npairs))
+
+    def ev_ms(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def separate():
+        for _, _, ctx, _ in cells:
+            ctx.reset_linewidths()
+            ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA, want=False)
+        for _, _, ctx, _ in cells:
+            ctx.synchronize()
+
+    separate()
+    sep = min(ev_ms(separate) for _ in range(steps))
+    ref = [ctx.get_linewidths() for _, _, ctx, _ in cells]
+    b = Batch()
+    for _, _, ctx, _ in cells:
+        b.add_linewidth3(ctx, 1, ctx.nq0, SIGMA)
+    b.run()
+    cfg, tuned_ms, tried = b.tune()
+    for _, _, ctx, _ in cells:
+        ctx.reset_linewidths()
+    b.run()  # capture with the tuned configuration
+    err = max(float(np.abs(b.result(k)[0] - ref[k]).max() / np.abs(ref[k]).max()) for k in range(len(cells)))
+    runs = []
+    for _ in range(steps):
+        b.run()
+        runs.append(b.result(0)[2])
+    batch_ms = min(runs)
+    ctx12 = cells[0][2]
+    q, _, z = ctx12.path_qpoints(PATH_NODES)
+    ctx12.linewidth_path(q, z, delta="gauss", sigma=SIGMA)
+    path_ms = min(ev_ms(lambda: ctx12.linewidth_path(q, z, delta="gauss", sigma=SIGMA)) for _ in range(steps))
+    b.close()
+    for _, _, ctx, _ in cells:
+        ctx.close()
+    return {"workloads": [f"{n}-{N}^3" for n, N, _, _ in cells], "temperatures": temps,
+            "pairs": [int(p) for *_, p in cells], "evals_per_T": int(evals),
+            "batch_ms": batch_ms, "separate_calls_ms": sep, "separate_over_batch": sep / batch_ms,
+            "evals_per_s_batch": evals / (batch_ms * 1e-3),
+            "max_rel_diff_vs_separate": err,
+            "tuned_config": {"two_atom_layout": cfg[0], "ctas_per_sm": cfg[1], "s0_block_ndof24": cfg[2],
+                             "items_per_step": cfg[3]},
+            "tuning": {"configs_tried": tried, "best_trial_ms": tuned_ms},
+            "path_points": int(len(q)), "path_ms": path_ms, "path_mesh": [12, 12, 12],
+            "what": "one persistent FP64 launch over all five workloads' (pair, s0-block) items, heaviest "
+                    "first, replayed from a CUDA graph; path points on the 12^3 context afterwards"}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -427,6 +505,7 @@ def run_ours(args):
 
     peak = fp64_peak_tflops(torch) if rank == 0 else None
     four = fourph_leg(torch, args.mesh4) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
+    batched = batched_leg(torch) if (rank == 0 and world == 1 and not args.no_batch) else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ph_grid, ph_irr = ctx.get_phonons(0), ctx.get_phonons(1)
@@ -483,6 +562,7 @@ def run_ours(args):
                                           "every mode with a linewidth above 1e-3 of the largest, kappa diagonal"},
                 "fp64_path": {"value": evals_total / (ms64 * 1e-3), "unit": "evals/s", "ms_per_step": ms64},
                 "fourph": four,
+                "batched": batched,
                 "roofline": roof,
                 "cpu_baseline": cpu,
                 "e2e": {"value": evals_total / (e2e_ms * 1e-3), "unit": "evals/s", "ms_per_step": e2e_ms,

@@ -268,6 +268,45 @@ int spring_kappa_rta(spring_ctx* ctx, int symm, int nsym, const double* Rxyz, co
  * 0) and iters(n_temps) are outputs (NULL allowed). */
 int spring_kappa_iter(spring_ctx* ctx, double eps_k, int max_iter, double* kappa, double* kappa_rta, int* iters);
 
+/* ---- batched linewidths (several workloads, one persistent launch) ------ */
+/* A batch holds Gaussian three-phonon linewidth requests on several contexts
+ * (different cells, meshes and temperature sets, on one device) and runs them
+ * as one persistent FP64 kernel over all their (pair, s0-block) work items,
+ * heaviest workloads first, captured with its zero-fills and the LW_Allq0
+ * updates in one CUDA graph that later runs replay.  Each request has the
+ * meaning of spring_linewidth3(ctx, i0_first, n_q0, SPRING_DELTA_GAUSS, sigma,
+ * pol3, ...) on its context (the q0 loop body of main.f90:552-715 for many
+ * inputs at once); no counterpart in the reference, which runs one input per
+ * process.  Requests on one context must not overlap in q0. */
+typedef struct spring_batch spring_batch;
+int spring_batch_create(spring_batch** batch);
+int spring_batch_destroy(spring_batch* batch);
+const char* spring_batch_last_error(const spring_batch* batch);
+/* Add a request; returns its index (0-based) in *index (may be NULL). */
+int spring_batch_add_linewidth3(spring_batch* batch, spring_ctx* ctx, int i0_first, int n_q0, double sigma,
+                                const int* pol3, int* index);
+/* Launch configuration of the persistent kernel (288 threads per CTA):
+ * config[0] 1 = two-atom cells (7-atom FC3 clusters, <= 9 temperatures) run as
+ * groups of 8 pairs in the specialised layout, 0 = every cell as (pair, s0
+ * block) items of the any-cell layout; config[1] CTAs per SM (0 = as many as
+ * fit); config[2] s0 block for cells with Ndof > 12 (0 = 6, or 6, 12, 24);
+ * config[3] work items taken per scheduler step.  Default {1, 0, 0, 1}. */
+int spring_batch_set_config(spring_batch* batch, const int* config);
+int spring_batch_get_config(const spring_batch* batch, int* config);
+/* Autotuner: time the batch under candidate configurations (coordinate search
+ * over the four parameters, each run timed with CUDA events; LW_Allq0 is not
+ * touched) and keep the fastest.  The result is cached for the process by the
+ * batch's shape (cells, meshes, temperatures, pair counts), so a later batch
+ * of the same shape starts tuned.  best_ms and n_tried may be NULL. */
+int spring_batch_tune(spring_batch* batch, int* config, double* best_ms, int* n_tried);
+/* Run every request (accumulating into each context's LW_Allq0, as
+ * spring_linewidth3 does); the first run captures the CUDA graph. */
+int spring_batch_run(spring_batch* batch);
+/* Results of request `index` of the last run: lw(Ndof,n_q0,n_temps) and
+ * P3_q0(Ndof,n_q0) of its context (either may be NULL); device time of the last
+ * run in *ms (may be NULL). */
+int spring_batch_result(spring_batch* batch, int index, double* lw, double* p3_q0, double* ms);
+
 /* ---- options ----------------------------------------------------------- */
 /* SPRING_OPT_GENERIC_V3 = 1: always use the any-cell V3 kernel (default 0 picks the
  * two-atom specialisation when the cell fits it; both give the same W). */

@@ -78,8 +78,17 @@ SIGNATURES = {
     "spring_set_linewidths": [P, P],
     "spring_kappa_rta": [P, I, I, P, P, P, P],
     "spring_debug_inject_fault": [P, I, I],
+    "spring_batch_create": [ct.POINTER(P)],
+    "spring_batch_destroy": [P],
+    "spring_batch_last_error": [P],
+    "spring_batch_add_linewidth3": [P, P, I, I, D, P, P],
+    "spring_batch_set_config": [P, P],
+    "spring_batch_get_config": [P, P],
+    "spring_batch_tune": [P, P, P, P],
+    "spring_batch_run": [P],
+    "spring_batch_result": [P, I, P, P, P],
 }
-_RESTYPE = {"spring_last_error": ct.c_char_p}
+_RESTYPE = {"spring_last_error": ct.c_char_p, "spring_batch_last_error": ct.c_char_p}
 
 _lib = None
 

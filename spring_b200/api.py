@@ -371,3 +371,74 @@ def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=
         ctx.compute_phonons(temps)
     info = dict(q_pnt_int=qi, q_pnt=qf, tetra=tet, W=W, Rxyz=Rxyz, temps=temps, **irr)
     return ctx, info
+
+
+class Batch:
+    """A ``spring_batch``: Gaussian three-phonon linewidth requests on several contexts (cells,
+    meshes, temperature sets) run as one persistent, graph-captured launch."""
+
+    def __init__(self):
+        self._lib = L.load()
+        h = ct.c_void_p()
+        rc = self._lib.spring_batch_create(ct.byref(h))
+        if rc != 0:
+            raise SpringError(rc, "spring_batch_create failed")
+        self._h = h
+        self._reqs = []
+
+    def _call(self, name, *args):
+        rc = getattr(self._lib, name)(self._h, *args)
+        if rc != 0:
+            msg = self._lib.spring_batch_last_error(self._h)
+            raise SpringError(rc, (msg or b"").decode())
+
+    def add_linewidth3(self, ctx: Context, i0_first: int, n_q0: int, sigma: float, pol=None) -> int:
+        """Queue spring_linewidth3(ctx, i0_first, n_q0, Gaussian, sigma, pol); returns its index."""
+        idx = ct.c_int()
+        polp = None if pol is None else np.ascontiguousarray(pol, dtype=np.int32)
+        self._call("spring_batch_add_linewidth3", ctx._h, int(i0_first), int(n_q0), float(sigma), _ptr(polp),
+                   ct.byref(idx))
+        self._reqs.append((ctx, int(n_q0)))
+        return idx.value
+
+    def set_config(self, two_atom=1, ctas_per_sm=0, s0_block=0, chunk=1):
+        """two_atom: run two-atom cells in the specialised 8-pair layout; ctas_per_sm (0: as many as
+        fit); s0_block for Ndof > 12 (0: 6); chunk: work items per scheduler step."""
+        cfg = np.array([two_atom, ctas_per_sm, s0_block, chunk], dtype=np.int32)
+        self._call("spring_batch_set_config", _ptr(cfg))
+
+    def config(self):
+        cfg = np.zeros(4, dtype=np.int32)
+        self._call("spring_batch_get_config", _ptr(cfg))
+        return tuple(int(x) for x in cfg)
+
+    def tune(self):
+        """Autotune the launch configuration; returns (config, best ms, configurations tried)."""
+        cfg = np.zeros(4, dtype=np.int32)
+        ms = ct.c_double()
+        n = ct.c_int()
+        self._call("spring_batch_tune", _ptr(cfg), ct.byref(ms), ct.byref(n))
+        return tuple(int(x) for x in cfg), ms.value, n.value
+
+    def run(self):
+        self._call("spring_batch_run")
+
+    def result(self, index: int):
+        """(lw[T][n_q0][Ndof], p3[n_q0][Ndof], ms of the last run) of request ``index``."""
+        ctx, n_q0 = self._reqs[index]
+        lw = np.zeros((ctx.n_temps, n_q0, ctx.ndof))
+        p3 = np.zeros((n_q0, ctx.ndof))
+        ms = ct.c_double()
+        self._call("spring_batch_result", int(index), _ptr(lw), _ptr(p3), ct.byref(ms))
+        return lw, p3, ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.spring_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

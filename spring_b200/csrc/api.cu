@@ -942,3 +942,22 @@ int spring_kappa_rta(spring_ctx* c, int symm, int nsym, const double* rxyz, cons
 }
 
 }  // extern "C"
+
+namespace spring {
+
+// The checks and prerequisites of a Gaussian three-phonon linewidth request, as spring_linewidth3
+// makes them (used by the batch entry points).
+int prepare_lw3(spring_ctx* c, int i0_first, int n_q0, const int* pol3, Pol* pol) {
+    SPRING_CHECK(check_q0_range(c, i0_first, n_q0));
+    SPRING_CHECK(ready3(c));
+    SPRING_CHECK(check_pol(c, pol3));
+    SPRING_CHECK(ensure_enum3(c));
+    *pol = make_pol(c, pol3);
+    return SPRING_OK;
+}
+
+int lw_out(spring_ctx* c, const double* d_src, int q0_first, int n_q0, double* out) {
+    return copy_lw_out(c, d_src, q0_first, n_q0, out);
+}
+
+}  // namespace spring

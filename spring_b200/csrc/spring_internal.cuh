@@ -279,6 +279,9 @@ int run_tetra3_path(spring_ctx* c, int p_first, int n_slots, int n_path, const d
 int run_iso(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const double* g2, double* d_rate);
 // k_kappa.cu
 int run_axpy_lw(spring_ctx* c, double a, const double* d_x, double* d_y, int q0_first, int n_q0);
+// api.cu: checks and prerequisites of a Gaussian linewidth3 request; [T][q0 range][s] slab to the host
+int prepare_lw3(spring_ctx* c, int i0_first, int n_q0, const int* pol3, Pol* pol);
+int lw_out(spring_ctx* c, const double* d_src, int q0_first, int n_q0, double* out);
 int run_kappa_rta(spring_ctx* c, int symm, int nsym, const double* d_rxyz, int s_lo, int s_hi, double* d_kappa,
                   double* d_mode);
 
