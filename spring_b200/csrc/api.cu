@@ -252,7 +252,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
-        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_tc_entries);
+        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles); dfree(c->d_tc_err);
         free_mlp(c->mlp);
         dfree(c->d_scr_rep); dfree(c->d_tc_keys); dfree(c->d_tc_keys_s); dfree(c->d_tc_vals); dfree(c->d_tc_cnt);

@@ -4,7 +4,8 @@
 //   2. Hermitian eigensolve in FP64 by cyclic complex Jacobi with round-robin
 //      (parallel) pair ordering: n/2 disjoint rotations per step, column
 //      updates then row updates, until the off-diagonal mass is below 1e-30 of
-//      the diagonal's.  Eigenvalues ascending like LAPACK zheevd.  The
+//      the diagonal's or a sweep finds no element above 1e-16 sqrt|a_pp a_qq|
+//      (threshold Jacobi).  Eigenvalues ascending like LAPACK zheevd.  The
 //      eigenvector phase (gauge) is the eigensolver's own: only gauge-invariant
 //      quantities are comparable with LAPACK's.
 //   3. omega = sqrt|lambda| (negative for imaginary modes), v = Re(e^H dD e)/(2 omega),
@@ -31,7 +32,7 @@ __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -
 
 constexpr int MAX_SWEEPS = 30;
 
-__global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const double* __restrict__ fc2,
+__global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, const double* __restrict__ qpts, const double* __restrict__ fc2,
                           const int* __restrict__ idx, const int* __restrict__ num, const double* __restrict__ mrs,
                           const double* __restrict__ temps, double2* __restrict__ evec, double* __restrict__ omega,
                           double* __restrict__ oneby, double* __restrict__ nbe, double* __restrict__ vel, int nq) {
@@ -48,6 +49,7 @@ __global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const doubl
     int* rotP = reinterpret_cast<int*>(red + 2);             // [m/2]
     int* rotQ = rotP + m / 2;                                // [m/2]
     int* rank = rotQ + m / 2;                                // [n]
+    __shared__ int nrot;                                     // rotations applied in this sweep
     double* lam = reinterpret_cast<double*>(rank + n + (n & 1));  // [n]
 
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -83,6 +85,7 @@ __global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const doubl
         // --- cyclic complex Jacobi
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
             if (tid == 0) {
+                nrot = 0;
                 double off = 0.0, dg = 0.0;
                 for (int i = 0; i < n; ++i) {
                     dg += A[i * n + i].x * A[i * n + i].x;
@@ -107,7 +110,7 @@ __global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const doubl
                     if (valid) {
                         const double2 z = A[p * n + qq];
                         const double rr = hypot(z.x, z.y);
-                        if (rr > 1e-300) {
+                        if (rr > 1e-300 && rr > 1e-16 * sqrt(fabs(A[p * n + p].x * A[qq * n + qq].x))) {
                             const double app = A[p * n + p].x, aqq = A[qq * n + qq].x;
                             const double tau = (aqq - app) / (2.0 * rr);
                             const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
@@ -118,6 +121,7 @@ __global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const doubl
                             valid = false;
                         }
                     }
+                    if (valid) atomicAdd(&nrot, 1);
                     rotP[k] = valid ? p : -1;
                     rotQ[k] = qq;
                     rotC[k] = c;
@@ -165,6 +169,8 @@ __global__ void k_phonons(PhArgs a, const double* __restrict__ qpts, const doubl
                 }
                 __syncthreads();
             }
+            if (nrot == 0) break;  // nothing above the threshold: converged (nrot read after the last barrier)
+            __syncthreads();
         }
         // --- ascending order (stable): rank of each eigenvalue
         for (int i = tid; i < n; i += nt) {

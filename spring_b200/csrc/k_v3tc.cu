@@ -41,7 +41,6 @@ constexpr int NMODE = 6;     // Ndof of the two-atom cell
 constexpr int KP = 48;       // padded K: Re/Im of (N2, c), 2 * 3 * Na3 <= 48
 constexpr int EPT = 16;      // pairs per tile: one 8-row core-matrix group each (rows 8e .. 8e+5 of 128)
 constexpr int BROWS = 36;    // used B rows
-constexpr int Q0ROW = 50;    // packed q0 row in doubles (48 used; 400-byte stride spreads the banks)
 constexpr uint32_t LBO = 128, SBO = (KP / 8) * 128;
 constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
 constexpr int AIMG = 8 * KP;              // bf16 elements of one (q, mu, hi/lo) A image: 8 rows x 48 (768 bytes)
@@ -56,15 +55,25 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
     lo = __float2bfloat16_rn(f - __bfloat162float(hi));
 }
 
-// U of one grid point, basis mu, slot k = N*3 + b, branch s (FP64)
-__device__ __forceinline__ double2 u_value(int q, int mu, int k, int s, int na, const double* __restrict__ posr,
+// Phases e^{i q.R_{mu N}} of one grid point and basis atom, N < na, into ph[N] (threads 0..na-1).
+__device__ __forceinline__ void q_phases(int q, int mu, int na, const double* __restrict__ posr,
+                                         const double* __restrict__ qpnt, double2* ph) {
+    const int N = threadIdx.x;
+    if (N < na) {
+        const double* R = posr + ((size_t)mu * na + N) * 3;
+        const double qr = qpnt[3 * q] * R[0] + qpnt[3 * q + 1] * R[1] + qpnt[3 * q + 2] * R[2];
+        double sn, cs;
+        sincos(qr, &sn, &cs);
+        ph[N] = make_double2(cs, sn);
+    }
+}
+
+// U of one grid point, basis mu, slot k = N*3 + b, branch s (FP64), from the phases of (q, mu)
+__device__ __forceinline__ double2 u_value(const double2* ph, int q, int mu, int k, int s, int na,
                                           const int* __restrict__ btyp, const double* __restrict__ mrs,
-                                          const double* __restrict__ qpnt, const double2* __restrict__ evg) {
+                                          const double2* __restrict__ evg) {
     const int N = k / 3, b = k % 3;
-    const double* R = posr + ((size_t)mu * na + N) * 3;
-    const double qr = qpnt[3 * q] * R[0] + qpnt[3 * q + 1] * R[1] + qpnt[3 * q + 2] * R[2];
-    double sn, cs;
-    sincos(qr, &sn, &cs);
+    const double cs = ph[N].x, sn = ph[N].y;
     const int nu = btyp[mu * na + N];
     const double m = mrs[nu];
     const double2 e = evg[((size_t)q * NMODE + s) * NMODE + nu * 3 + b];
@@ -73,27 +82,36 @@ __device__ __forceinline__ double2 u_value(int q, int mu, int k, int s, int na, 
 
 // A table: per (q, hi/lo, mu) the 768-byte shared-memory image of one 8-row group of the canonical
 // K-major layout, element (row s, k) at (k/8)*64 + s*8 + k%8, rows 6 and 7 zero.  Hi parts first,
-// so a BF16 launch copies the two hi images as one block.
-__global__ void k_tc_tab_a(int nq, int na, const double* __restrict__ posr, const int* __restrict__ btyp,
-                           const double* __restrict__ mrs, const double* __restrict__ qpnt,
-                           const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
+// so a BF16 launch copies the two hi images as one block.  One CTA per (q, mu), images built in
+// shared memory and written as 16-byte vectors.
+__global__ void __launch_bounds__(128) k_tc_tab_a(int nq, int na, const double* __restrict__ posr,
+                                                  const int* __restrict__ btyp, const double* __restrict__ mrs,
+                                                  const double* __restrict__ qpnt, const double2* __restrict__ evg,
+                                                  __nv_bfloat16* __restrict__ tab) {
+    __shared__ double2 ph[8];
+    __shared__ __align__(16) __nv_bfloat16 img[2][AIMG];
+    const int q = blockIdx.x / 2, mu = blockIdx.x % 2;
     const int KR = 3 * na;
-    const long long total = (long long)nq * 2 * 8 * KP;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(i % KP), s = (int)((i / KP) % 8), mu = (int)((i / (KP * 8)) % 2);
-        const int q = (int)(i / (KP * 8 * 2));
+    q_phases(q, mu, na, posr, qpnt, ph);
+    __syncthreads();
+    for (int i = threadIdx.x; i < 8 * KP; i += blockDim.x) {
+        const int k = i % KP, s = i / KP;
         double x = 0.0;
         if (k < 2 * KR && s < NMODE) {
-            const double2 u = u_value(q, mu, k % KR, s, na, posr, btyp, mrs, qpnt, evg);
+            const double2 u = u_value(ph, q, mu, k % KR, s, na, btyp, mrs, evg);
             x = k < KR ? u.x : u.y;
         }
         __nv_bfloat16 hi, lo;
         split_bf16(x, hi, lo);
-        __nv_bfloat16* img = tab + (size_t)q * 4 * AIMG;
-        const int off = mu * AIMG + (k / 8) * 64 + s * 8 + k % 8;
-        img[off] = hi;
-        img[2 * AIMG + off] = lo;
+        const int off = (k / 8) * 64 + s * 8 + k % 8;
+        img[0][off] = hi;
+        img[1][off] = lo;
     }
+    __syncthreads();
+    constexpr int V = AIMG * 2 / 16;  // 16-byte vectors per image
+    uint4* out = reinterpret_cast<uint4*>(tab + (size_t)q * 4 * AIMG + mu * AIMG);
+    for (int i = threadIdx.x; i < 2 * V; i += blockDim.x)
+        out[(i / V) * 2 * V + i % V] = reinterpret_cast<const uint4*>(&img[0][0])[i];
 }
 
 // B table: per (q1, hi/lo, mu) the 4608-byte shared-memory image of the 48 x 48 B operand in the
@@ -108,34 +126,47 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
                                                   const double2* __restrict__ evg, __nv_bfloat16* __restrict__ tab) {
     __shared__ double2 sU[24 * NMODE];                   // [N b][s]
     __shared__ __align__(16) __nv_bfloat16 img[2][BIMG];  // hi, lo images of this (q1, mu), built here
+    __shared__ double2 ph[8];
+    __shared__ double sF[8 * 8 * 27];  // FC3 of mu
     const int q = blockIdx.x / 2, mu = blockIdx.x % 2;
     const int KR = 3 * na;
+    q_phases(q, mu, na, posr, qpnt, ph);
+    for (int i = threadIdx.x; i < na * na * 27; i += blockDim.x) sF[i] = fc3[(size_t)mu * na * na * 27 + i];
+    __syncthreads();
     for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
-        sU[i] = u_value(q, mu, i / NMODE, i % NMODE, na, posr, btyp, mrs, qpnt, evg);
+        sU[i] = u_value(ph, q, mu, i / NMODE, i % NMODE, na, btyp, mrs, evg);
     for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // rows 36-47 and the K padding stay zero
         reinterpret_cast<uint4*>(&img[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
-    const double* f = fc3 + (size_t)mu * na * na * 27;
-    for (int i = threadIdx.x; i < 18 * KR; i += blockDim.x) {
-        const int r = i / KR, k2 = i % KR;  // r = a*6 + s1, k2 = N2*3 + c
-        const int al = r / NMODE, s1 = r % NMODE, N2 = k2 / 3, ga = k2 % 3;
-        double zr = 0.0, zi = 0.0;
+    // Z[(a, s1)][(N2, c)] = sum_{N1, b} FC3[mu][N1][N2][a b c] U[N1 b][s1]: one thread per
+    // (a, N2, c, s1 half), each FC3 value (staged in shared memory) used for three s1.
+    for (int i = threadIdx.x; i < 3 * KR * 2; i += blockDim.x) {
+        const int half = i % 2, t = i / 2, al = t / KR, k2 = t % KR;  // k2 = N2*3 + c
+        const int N2 = k2 / 3, ga = k2 % 3;
+        double zr[3] = {0.0, 0.0, 0.0}, zi[3] = {0.0, 0.0, 0.0};
         for (int k1 = 0; k1 < KR; ++k1) {
             const int N1 = k1 / 3, be = k1 % 3;
-            const double fv = f[((size_t)N1 * na + N2) * 27 + (al * 3 + be) * 3 + ga];
-            const double2 u = sU[k1 * NMODE + s1];
-            zr = fma(fv, u.x, zr);
-            zi = fma(fv, u.y, zi);
+            const double fv = sF[(N1 * na + N2) * 27 + (al * 3 + be) * 3 + ga];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const double2 u = sU[k1 * NMODE + half * 3 + j];
+                zr[j] = fma(fv, u.x, zr[j]);
+                zi[j] = fma(fv, u.y, zi[j]);
+            }
         }
-        __nv_bfloat16 h, l;
-        // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
-        split_bf16(zr, h, l);
-        img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
-        img[0][bimg(18 + r, KR + k2)] = h;     img[1][bimg(18 + r, KR + k2)] = l;
-        split_bf16(-zi, h, l);
-        img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
-        split_bf16(zi, h, l);
-        img[0][bimg(18 + r, k2)] = h;          img[1][bimg(18 + r, k2)] = l;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const int r = al * NMODE + half * 3 + j;  // r = a*6 + s1
+            __nv_bfloat16 h, l;
+            // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
+            split_bf16(zr[j], h, l);
+            img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
+            img[0][bimg(18 + r, KR + k2)] = h;     img[1][bimg(18 + r, KR + k2)] = l;
+            split_bf16(-zi[j], h, l);
+            img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
+            split_bf16(zi[j], h, l);
+            img[0][bimg(18 + r, k2)] = h;          img[1][bimg(18 + r, k2)] = l;
+        }
     }
     __syncthreads();
     constexpr int V = BIMG * 2 / 16;  // 16-byte vectors per image
@@ -144,22 +175,41 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         out[(i / V) * 2 * V + i % V] = reinterpret_cast<const uint4*>(&img[0][0])[i];
 }
 
-// Packed q0 rows (Q0ROW doubles): e0' = m_mu^-1/2 e0(mu a, s0) as float2 [s0][row] (288 bytes), then
-// omega0[6] and 1/omega0[6].
+// q0 mode records, 64 bytes per (q0, s0): e0' = m_mu^-1/2 e0(mu a, s0) as float2[6], omega0, 1/omega0.
+struct Q0Rec {
+    float2 e0[NMODE];
+    double w, ob;
+};
+static_assert(sizeof(Q0Rec) == 64, "q0 record");
 __global__ void k_tc_q0tab(int nq0, const double2* __restrict__ ev0, const double* __restrict__ om0,
-                           const double* __restrict__ ob0, const double* __restrict__ mrs, double* __restrict__ out) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq0 * 48; i += gridDim.x * blockDim.x) {
-        const int q = i / 48, k = i % 48;
-        double* row = out + (size_t)q * Q0ROW;
-        if (k < 36) {
-            const double2 e = ev0[(size_t)q * 36 + k];
-            const double m = mrs[(k % NMODE) / 3];
-            reinterpret_cast<float2*>(row)[k] = make_float2((float)(m * e.x), (float)(m * e.y));
-        } else if (k < 42) {
-            row[k] = om0[(size_t)q * NMODE + k - 36];
-        } else {
-            row[k] = ob0[(size_t)q * NMODE + k - 42];
+                           const double* __restrict__ ob0, const double* __restrict__ mrs, Q0Rec* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq0 * NMODE; i += gridDim.x * blockDim.x) {
+        const int q = i / NMODE, s0 = i % NMODE;
+        Q0Rec r;
+        for (int k = 0; k < NMODE; ++k) {
+            const double2 e = ev0[((size_t)q * NMODE + s0) * NMODE + k];
+            const double m = mrs[k / 3];
+            r.e0[k] = make_float2((float)(m * e.x), (float)(m * e.y));
         }
+        r.w = om0[(size_t)q * NMODE + s0];
+        r.ob = ob0[(size_t)q * NMODE + s0];
+        out[i] = r;
+    }
+}
+
+// Grid mode records, `rs` doubles per (q, s) (a multiple of 4, so 32-byte aligned): omega,
+// 1/omega, nBE[T].
+__global__ void k_tc_modes(int nq, int nT, int rs, const double* __restrict__ omg, const double* __restrict__ obg,
+                           const double* __restrict__ nbeg, double* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * NMODE * rs;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long qs = i / rs;
+        const int k = (int)(i % rs);
+        double v = 0.0;
+        if (k == 0) v = omg[qs];
+        else if (k == 1) v = obg[qs];
+        else if (k - 2 < nT) v = nbeg[(size_t)(k - 2) * nq * NMODE + qs];
+        out[i] = v;
     }
 }
 
@@ -527,52 +577,85 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     if (tid == 0) counts[blockIdx.x] = S.ihead;
 }
 
+// One active triple whose item and records are already in registers.
+struct EvalIn {
+    float4 v0, v1, v2;
+    int4 kk;
+    Q0Rec q0;
+    double w1, ob1, w2, ob2;
+};
+
+__device__ __forceinline__ void eval_load(EvalIn& x, const TcItem* item, const Q0Rec* __restrict__ q0rec,
+                                          const double* __restrict__ modes, int rs) {
+    const float4* src = reinterpret_cast<const float4*>(item);
+    x.v0 = src[0];
+    x.v1 = src[1];
+    x.v2 = src[2];
+    x.kk = reinterpret_cast<const int4*>(src)[3];
+    x.q0 = q0rec[x.kk.x & 0x1fffffff];
+    const double2 a = *reinterpret_cast<const double2*>(modes + (size_t)x.kk.y * rs);
+    const double2 b = *reinterpret_cast<const double2*>(modes + (size_t)x.kk.z * rs);
+    x.w1 = a.x;
+    x.ob1 = a.y;
+    x.w2 = b.x;
+    x.ob2 = b.y;
+}
+
+__device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int rs, double half_os2, double pre,
+                                          double mfac, const double* __restrict__ modes, double* out_lw,
+                                          double* out_p3) {
+    const int o = x.kk.x & 0x1fffffff;
+    const double w0 = x.q0.w, w1 = x.w1, w2 = x.w2;
+    const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
+    const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
+    const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
+    const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
+    const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
+    const double wt = (x.kk.x >> 30) & 1 ? 2.0 : 1.0;
+    const double p3 = e1 + e2 + e3;
+    if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
+    if ((x.kk.x >> 29) & 1) return;  // W = 0 for the Gamma acoustic modes of q0
+    const float yr[6] = {x.v0.x, x.v0.y, x.v0.z, x.v0.w, x.v1.x, x.v1.y};
+    const float yi[6] = {x.v1.z, x.v1.w, x.v2.x, x.v2.y, x.v2.z, x.v2.w};
+    float pr = 0.0f, pim = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float2 c = x.q0.e0[k];
+        pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
+        pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+    }
+    const double W = (double)(pr * pr + pim * pim) * (x.q0.ob * x.ob2 * x.ob1) * mfac * wt;
+    const double we1 = W * e1, wf2 = W * (e2 - e3);
+    const double* m1 = modes + (size_t)x.kk.y * rs + 2;
+    const double* m2 = modes + (size_t)x.kk.z * rs + 2;
+    for (int T = 0; T < nT; ++T) {
+        const double n1 = m1[T], n2 = m2[T];
+        const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
+        if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
+    }
+}
+
 // FP64 part of the active triples: Phi = sum_k e0'(k, s0) Y_k (FP32), W = wt mfac |Phi|^2 /
 // (omega0 omega1 omega2), the three Gaussian delta weights, then the phase-space and linewidth
 // sums with atomics: P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].
-// Block (r, y) walks region r of the item list.
-__global__ void __launch_bounds__(256) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
-                                                   int cap, int nq, int nq0, int nT, double half_os2, double pre,
-                                                   double mfac, const double* __restrict__ q0tab,
-                                                   const double* __restrict__ om0, const double* __restrict__ ob0,
-                                                   const double* __restrict__ omg, const double* __restrict__ obg,
-                                                   const double* __restrict__ nbe, double* __restrict__ out_lw,
+// Block (r, y) walks region r of the item list, two items per thread at a time with both items'
+// loads issued first.
+__global__ void __launch_bounds__(256, 3) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
+                                                   int cap, int nq0, int nT, int rs, double half_os2, double pre,
+                                                   double mfac, const Q0Rec* __restrict__ q0rec,
+                                                   const double* __restrict__ modes, double* __restrict__ out_lw,
                                                    double* __restrict__ out_p3) {
     const int r = blockIdx.x;
     const int n = min(counts[r], cap);
     const TcItem* reg = items + (size_t)r * cap;
-    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += gridDim.y * blockDim.x) {
-        const float4* src = reinterpret_cast<const float4*>(reg + i);
-        const float4 v0 = src[0], v1 = src[1], v2 = src[2];
-        const int4 kk = reinterpret_cast<const int4*>(src)[3];
-        const int o = kk.x & 0x1fffffff, q0 = o / NMODE, s0 = o % NMODE;
-        const double w0 = om0[o], w1 = omg[kk.y], w2 = omg[kk.z];
-        const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
-        const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
-        const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
-        const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
-        const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
-        const double wt = (kk.x >> 30) & 1 ? 2.0 : 1.0;
-        const double p3 = e1 + e2 + e3;
-        if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
-        if ((kk.x >> 29) & 1) continue;  // W = 0 for the Gamma acoustic modes of q0
-        const float yr[6] = {v0.x, v0.y, v0.z, v0.w, v1.x, v1.y}, yi[6] = {v1.z, v1.w, v2.x, v2.y, v2.z, v2.w};
-        const float2* e0 = reinterpret_cast<const float2*>(q0tab + (size_t)q0 * Q0ROW) + s0 * NMODE;
-        float pr = 0.0f, pim = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            const float2 c = e0[k];
-            pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
-            pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
-        }
-        const double W = (double)(pr * pr + pim * pim) * (ob0[o] * obg[kk.z] * obg[kk.y]) * mfac * wt;
-        const double we1 = W * e1, wf2 = W * (e2 - e3);
-        for (int T = 0; T < nT; ++T) {
-            const size_t tb = (size_t)T * nq * NMODE;
-            const double n1 = nbe[tb + kk.y], n2 = nbe[tb + kk.z];
-            const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
-            if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
-        }
+    const int stride = gridDim.y * blockDim.x;
+    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
+        const int j = i + stride;
+        EvalIn a, b;
+        eval_load(a, reg + i, q0rec, modes, rs);
+        if (j < n) eval_load(b, reg + j, q0rec, modes, rs);
+        eval_item(a, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
+        if (j < n) eval_item(b, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
     }
 }
 
@@ -709,28 +792,33 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const int nq = c->nq;
     SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 4 * AIMG, "V3 A table"));
     SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 4 * BIMG, "V3 B table"));
-    SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * Q0ROW, "V3 q0 rows"));
+    SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
+    const int rs = (2 + c->nT + 3) / 4 * 4;
+    SPRING_CHECK(dalloc(c, c->d_tc_modes, (size_t)nq * NMODE * rs, "V3 mode records"));
     SPRING_CHECK(dalloc(c, c->d_tc_err, 1, "V3 status"));
     SPRING_CHECK(zero(c, c->d_tc_err.p, sizeof(int), "V3 status"));
     SPRING_CHECK(build_tiles(c, p0, p1));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    {
-        const long long tot = (long long)nq * 2 * 8 * KP;
-        k_tc_tab_a<<<(int)std::min<long long>((tot + threads - 1) / threads, 148LL * 16), threads, 0, c->stream>>>(
-            nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p, c->d_qpnt.p, c->ph_grid.evec.p,
-            reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
-        SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
-    }
+    k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
+                                               c->d_qpnt.p, c->ph_grid.evec.p,
+                                               reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
+    SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     k_tc_tab_b<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
                                                c->d_qpnt.p, c->ph_grid.evec.p,
                                                reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
     SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_q0tab<<<std::max(1, std::min((c->nq0 * 48 + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
-        c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p, c->d_tc_q0.p);
+    k_tc_q0tab<<<std::max(1, std::min((c->nq0 * NMODE + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
+        c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p,
+        reinterpret_cast<Q0Rec*>(c->d_tc_q0.p));
     SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+    k_tc_modes<<<(int)std::min<long long>(((long long)nq * NMODE * rs + threads - 1) / threads, 148LL * 8), threads, 0,
+                 c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p,
+                              c->d_tc_modes.p);
+    SPRING_CHECK(launch_check(c, "k_tc_modes"));
 
     TcArgs a{};
     a.nq = nq;
@@ -775,11 +863,11 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
     if (maxcnt == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
-    const dim3 grid(c->tc_grid, std::max(1, std::min(1024, (maxcnt + threads - 1) / threads)));
+    const dim3 grid(c->tc_grid, std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads))));
     k_v3tc_eval<<<grid, threads, 0, c->stream>>>(
-        reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, nq, c->nq0, c->nT, a.half_os2,
-        os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), c->d_tc_q0.p, c->ph_irr.omega.p, c->ph_irr.oneby.p,
-        c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, d_lw, d_p3);
+        reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2,
+        os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p),
+        c->d_tc_modes.p, d_lw, d_p3);
     return launch_check(c, "k_v3tc_eval");
 }
 

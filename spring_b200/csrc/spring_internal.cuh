@@ -176,7 +176,8 @@ struct spring_ctx {
     // tensor-core V3 (spring_set_precision): operand tables and pair tiles grouped by q1
     spring::DBuf<uint16_t> d_tc_a;     // bf16 A operand images [q][hi, lo][mu]
     spring::DBuf<uint16_t> d_tc_b;     // bf16 B operand images [q1][hi, lo][mu]
-    spring::DBuf<double> d_tc_q0;      // packed q0 rows: e0' float2[36], omega[6], 1/omega[6]
+    spring::DBuf<double> d_tc_q0;      // q0 mode records: e0' float2[6], omega, 1/omega (64 bytes each)
+    spring::DBuf<double> d_tc_modes;   // grid mode records: omega, 1/omega, nBE[T] (padded to 4 doubles)
     spring::DBuf<float4> d_tc_items;   // active mode triples, one region per CTA (64 bytes each)
     spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA
     int tc_grid = 0;
