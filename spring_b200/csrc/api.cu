@@ -247,6 +247,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_fc4); dfree(c->d_fc4_posr); dfree(c->d_fc4_btyp); dfree(c->d_fc4_off);
         dfree(c->d_fc3); dfree(c->d_fc3_off); dfree(c->d_fc3_posr); dfree(c->d_fc3_btyp);
         dfree(c->d_qint); dfree(c->d_qpnt); dfree(c->d_tetra);
+        dfree(c->d_tr_partner); dfree(c->d_tr_solve); dfree(c->d_tr_fill);
         dfree(c->d_irr_int); dfree(c->d_irr_q); dfree(c->d_mult); dfree(c->d_pos); dfree(c->d_temps);
         free_phonons(c->ph_grid); free_phonons(c->ph_irr);
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
@@ -528,6 +529,7 @@ int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_
     SPRING_CHECK(spring_synchronize(c));
     c->mesh_set = true;
     c->mesh_zc = zero_centered != 0;
+    c->tr_nq = -1;  // time-reversal lists belong to the previous mesh
     for (int k = 0; k < 3; ++k) c->mesh_shift[k] = sh[k];
     c->ps_irr.done = false;
     c->ps_tr.done = false;
@@ -612,8 +614,7 @@ int spring_compute_phonons(spring_ctx* c, const double* temps, double freq_cut) 
     SPRING_CHECK(set_temps(c, temps));
     SPRING_CHECK(alloc_phonons(c, c->ph_grid, c->nq));
     SPRING_CHECK(alloc_phonons(c, c->ph_irr, c->nq0));
-    SPRING_CHECK(run_phonons(c, c->ph_grid, c->d_qpnt.p, c->nq));
-    SPRING_CHECK(run_phonons(c, c->ph_irr, c->d_irr_q.p, c->nq0));
+    SPRING_CHECK(run_phonons_mesh(c));
     c->ph_grid.set = c->ph_irr.set = true;
     dfree(c->d_wtr);  // cached W grids depend on the phonons
     return SPRING_OK;

@@ -10,7 +10,13 @@
 //      quantities are comparable with LAPACK's.
 //   3. omega = sqrt|lambda| (negative for imaginary modes), v = Re(e^H dD e)/(2 omega),
 //      nBE for every temperature, 1/(omega wTHz); Gamma acoustic modes zeroed.
-// FP64 ALU bound (~10 n^3 flops per sweep); negligible next to the scattering path.
+//   4. On a Gamma-centred mesh only one point of each (q, -q) pair is solved: the
+//      other gets e(-q) = conj(e(q)) (D(-q) = D(q)* for real force constants),
+//      the same omega, 1/omega and nBE, and v(-q) = -v(q).  The irreducible
+//      points run in the same launch.
+// FP64 ALU bound (~10 n^3 flops per sweep).
+#include <vector>
+
 #include "spring_internal.cuh"
 
 namespace spring {
@@ -32,10 +38,23 @@ __device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -
 
 constexpr int MAX_SWEEPS = 30;
 
-__global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, const double* __restrict__ qpts, const double* __restrict__ fc2,
-                          const int* __restrict__ idx, const int* __restrict__ num, const double* __restrict__ mrs,
-                          const double* __restrict__ temps, double2* __restrict__ evec, double* __restrict__ omega,
-                          double* __restrict__ oneby, double* __restrict__ nbe, double* __restrict__ vel, int nq) {
+// Outputs of one set of q-points: [q][s][row] eigenvectors, [q][s] scalars, [T][nq][s] nBE,
+// [q][s][3] velocities; q vectors qpts[q][3].
+struct PhSet {
+    const double* qpts;
+    double2* evec;
+    double* omega;
+    double* oneby;
+    double* nbe;
+    double* vel;
+    int nq;
+};
+
+// Work item i < n_a: point list_a[i] (or i when list_a is null) of set SA; else point i - n_a of set SB.
+__global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, PhSet SA, const int* __restrict__ list_a, int n_a,
+                                                    PhSet SB, int n_b, const double* __restrict__ fc2,
+                                                    const int* __restrict__ idx, const int* __restrict__ num,
+                                                    const double* __restrict__ mrs, const double* __restrict__ temps) {
     extern __shared__ double2 sm[];
     const int n = a.n;
     const int m = n + (n & 1);  // even size for round-robin pairing (index n is a dummy)
@@ -53,8 +72,17 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, const double* __re
     double* lam = reinterpret_cast<double*>(rank + n + (n & 1));  // [n]
 
     const int tid = threadIdx.x, nt = blockDim.x;
-    for (int q = blockIdx.x; q < nq; q += gridDim.x) {
-        const double qx = qpts[3 * q], qy = qpts[3 * q + 1], qz = qpts[3 * q + 2];
+    for (int item = blockIdx.x; item < n_a + n_b; item += gridDim.x) {
+        const bool in_a = item < n_a;
+        const PhSet& P = in_a ? SA : SB;
+        const int q = in_a ? (list_a ? list_a[item] : item) : item - n_a;
+        const int nq = P.nq;
+        double2* __restrict__ evec = P.evec;
+        double* __restrict__ omega = P.omega;
+        double* __restrict__ oneby = P.oneby;
+        double* __restrict__ nbe = P.nbe;
+        double* __restrict__ vel = P.vel;
+        const double qx = P.qpts[3 * q], qy = P.qpts[3 * q + 1], qz = P.qpts[3 * q + 2];
         for (int i = tid; i < 5 * n * n; i += nt) A[i] = make_double2(0.0, 0.0);  // A, V, dD
         __syncthreads();
         // --- D(q), dD/dq: thread per (mu, alpha, beta); neighbours in reference order
@@ -84,7 +112,24 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, const double* __re
 
         // --- cyclic complex Jacobi
         for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
-            if (tid == 0) {
+            if (nt == 32) {  // one warp: lane-parallel sums
+                double off = 0.0, dg = 0.0;
+                for (int w = tid; w < n * n; w += 32) {
+                    const int i = w / n, j = w % n;
+                    const double2 z = A[w];
+                    if (i == j) dg += z.x * z.x;
+                    else if (j > i) off += z.x * z.x + z.y * z.y;
+                }
+                for (int o = 16; o > 0; o >>= 1) {
+                    off += __shfl_xor_sync(0xffffffffu, off, o);
+                    dg += __shfl_xor_sync(0xffffffffu, dg, o);
+                }
+                if (tid == 0) {
+                    nrot = 0;
+                    red[0] = off;
+                    red[1] = dg;
+                }
+            } else if (tid == 0) {
                 nrot = 0;
                 double off = 0.0, dg = 0.0;
                 for (int i = 0; i < n; ++i) {
@@ -219,9 +264,33 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, const double* __re
     }
 }
 
-}  // namespace
+// Points of the other half of the (q, -q) pairs: copies of their partner with conjugate
+// eigenvectors and reversed velocities.
+__global__ void k_phonons_tr(int n, int nT, int nq, const int* __restrict__ fill, const int* __restrict__ partner,
+                             double2* __restrict__ evec, double* __restrict__ omega, double* __restrict__ oneby,
+                             double* __restrict__ nbe, double* __restrict__ vel, int n_fill) {
+    const int per = n * n + n * (3 + nT + 2);
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < (long long)n_fill * per;
+         w += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(w / per), k = (int)(w % per);
+        const int g = fill[i], p = partner[g];
+        if (k < n * n) {
+            const double2 e = evec[(size_t)p * n * n + k];
+            evec[(size_t)g * n * n + k] = make_double2(e.x, -e.y);
+        } else {
+            const int r = k - n * n, s = r % n, what = r / n;  // 0..2 velocity, 3 omega, 4 1/omega, 5.. nBE
+            if (what < 3) vel[((size_t)g * n + s) * 3 + what] = -vel[((size_t)p * n + s) * 3 + what];
+            else if (what == 3) omega[(size_t)g * n + s] = omega[(size_t)p * n + s];
+            else if (what == 4) oneby[(size_t)g * n + s] = oneby[(size_t)p * n + s];
+            else {
+                const int t = what - 5;
+                nbe[((size_t)t * nq + g) * n + s] = nbe[((size_t)t * nq + p) * n + s];
+            }
+        }
+    }
+}
 
-int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq) {
+PhArgs ph_args(spring_ctx* c) {
     PhArgs a;
     a.nb = c->nb;
     a.n = c->ndof;
@@ -232,19 +301,79 @@ int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq) {
     a.vg_ms = k.vg_ms;
     a.BEConv = k.BEConv;
     a.nT = c->nT;
-    const int n = c->ndof, m = n + (n & 1);
-    size_t smem = sizeof(double2) * (5 * n * n + m / 2) + sizeof(double) * (2 * (m / 2) + 2) +
-                  sizeof(int) * (2 * (m / 2) + n + (n & 1)) + sizeof(double) * n + 16;
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_phonons, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    }
+    return a;
+}
+
+size_t ph_smem(int n) {
+    const int m = n + (n & 1);
+    return sizeof(double2) * (5 * n * n + m / 2) + sizeof(double) * (2 * (m / 2) + 2) +
+           sizeof(int) * (2 * (m / 2) + n + (n & 1)) + sizeof(double) * n + 16;
+}
+
+int launch_phonons(spring_ctx* c, const PhSet& A, const int* list_a, int n_a, const PhSet& B, int n_b) {
+    const PhArgs a = ph_args(c);
+    const int n = c->ndof;
+    const size_t smem = ph_smem(n);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_phonons, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int threads = n <= 6 ? 32 : 128;
-    const int blocks = nq < 148 * 32 ? nq : 148 * 32;
+    const int items = n_a + n_b;
+    const int blocks = items < 148 * 32 ? items : 148 * 32;
+    if (items == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "phonons: injected launch failure");
-    k_phonons<<<blocks, threads, smem, c->stream>>>(a, d_q, c->d_fc2.p, c->d_fc2_idx.p, c->d_fc2_num.p,
-                                                    c->d_mass_rs.p, c->d_temps.p, ph.evec.p, ph.omega.p, ph.oneby.p,
-                                                    ph.nbe.p, ph.vel.p, nq);
+    k_phonons<<<blocks, threads, smem, c->stream>>>(a, A, list_a, n_a, B, n_b, c->d_fc2.p, c->d_fc2_idx.p,
+                                                    c->d_fc2_num.p, c->d_mass_rs.p, c->d_temps.p);
     return launch_check(c, "k_phonons");
+}
+
+PhSet ph_set(Phonons& ph, const double* q, int nq) {
+    return PhSet{q, ph.evec.p, ph.omega.p, ph.oneby.p, ph.nbe.p, ph.vel.p, nq};
+}
+
+}  // namespace
+
+int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq) {
+    const PhSet A = ph_set(ph, d_q, nq);
+    return launch_phonons(c, A, nullptr, nq, A, 0);
+}
+
+// Grid and irreducible phonons in one launch; on a Gamma-centred mesh only one point of each
+// (q, -q) pair of the grid is solved and the other filled by time reversal.
+int run_phonons_mesh(spring_ctx* c) {
+    const int nq = c->nq;
+    const PhSet G = ph_set(c->ph_grid, c->d_qpnt.p, nq), I = ph_set(c->ph_irr, c->d_irr_q.p, c->nq0);
+    const bool tr = c->mesh_shift[0] == 0 && c->mesh_shift[1] == 0 && c->mesh_shift[2] == 0;
+    if (!tr) {
+        SPRING_CHECK(launch_phonons(c, G, nullptr, nq, G, 0));
+        return launch_phonons(c, I, nullptr, c->nq0, I, 0);
+    }
+    if (c->tr_nq != nq) {  // partner of every grid point and the two lists (built once per mesh)
+        std::vector<int> partner(nq), solve, fill;
+        for (int g = 0; g < nq; ++g) {
+            const int x = g % c->mesh[0], y = (g / c->mesh[0]) % c->mesh[1], z = g / (c->mesh[0] * c->mesh[1]);
+            const int xm = (c->mesh[0] - x) % c->mesh[0], ym = (c->mesh[1] - y) % c->mesh[1],
+                      zm = (c->mesh[2] - z) % c->mesh[2];
+            const int p = xm + c->mesh[0] * (ym + c->mesh[1] * zm);
+            partner[g] = p;
+            (g <= p ? solve : fill).push_back(g);
+        }
+        SPRING_CHECK(dalloc(c, c->d_tr_partner, nq, "time-reversal partners"));
+        SPRING_CHECK(dalloc(c, c->d_tr_solve, std::max<size_t>(solve.size(), 1), "time-reversal lists"));
+        SPRING_CHECK(dalloc(c, c->d_tr_fill, std::max<size_t>(fill.size(), 1), "time-reversal lists"));
+        SPRING_CHECK(h2d(c, c->d_tr_partner.p, partner.data(), sizeof(int) * nq, "time-reversal partners"));
+        SPRING_CHECK(h2d(c, c->d_tr_solve.p, solve.data(), sizeof(int) * solve.size(), "time-reversal lists"));
+        SPRING_CHECK(h2d(c, c->d_tr_fill.p, fill.data(), sizeof(int) * fill.size(), "time-reversal lists"));
+        c->tr_nsolve = (int)solve.size();
+        c->tr_nfill = (int)fill.size();
+        c->tr_nq = nq;
+    }
+    SPRING_CHECK(launch_phonons(c, G, c->d_tr_solve.p, c->tr_nsolve, I, c->nq0));
+    if (c->tr_nfill == 0) return SPRING_OK;
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "phonons: injected launch failure");
+    const int n = c->ndof;
+    const long long work = (long long)c->tr_nfill * (n * n + n * (5 + c->nT));
+    k_phonons_tr<<<(int)std::min<long long>((work + 255) / 256, 148LL * 16), 256, 0, c->stream>>>(
+        n, c->nT, nq, c->d_tr_fill.p, c->d_tr_partner.p, G.evec, G.omega, G.oneby, G.nbe, G.vel, c->tr_nfill);
+    return launch_check(c, "k_phonons_tr");
 }
 
 }  // namespace spring

@@ -136,6 +136,10 @@ struct spring_ctx {
     bool mesh_zc = true;           // zero-centred folding (kappa.x) or [0, N) (LineWidth.x)
     int mesh_shift[3] = {0, 0, 0};
     spring::DBuf<int> d_qint;      // [q][3]
+    // time-reversal pairs of the grid (Gamma-centred meshes): partner of each point, points solved /
+    // filled, for the mesh of tr_nq points
+    spring::DBuf<int> d_tr_partner, d_tr_solve, d_tr_fill;
+    int tr_nq = -1, tr_nsolve = 0, tr_nfill = 0;
     spring::DBuf<double> d_qpnt;   // [q][3]
     spring::DBuf<int> d_tetra;     // [t][4] 0-based grid indices
     bool irr_set = false;
@@ -239,6 +243,7 @@ int run_make_mesh(spring_ctx* c, const int shift[3], int zero_centered);
 int run_irr_map(spring_ctx* c, const int* d_rot, int nrot, int time_rev, int* d_map);
 // k_phonon.cu
 int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int n);
+int run_phonons_mesh(spring_ctx* c);  // grid + irreducible points (time reversal on Gamma-centred meshes)
 // k_enum.cu
 int run_enumerate3(spring_ctx* c, PairSet& ps);
 int run_enumerate3_fortran(spring_ctx* c, int i0, int* d_allq1q2, int* d_perm, int* d_counts);
