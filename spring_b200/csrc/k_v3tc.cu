@@ -278,7 +278,7 @@ struct TcSmem {
 
 constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s0 each
 constexpr int EPI_THREADS = EPI_WARPS * 32;
-constexpr int TC_THREADS = EPI_THREADS + 64;  // warp 12: TMA copies and frequency gathers; warp 13: MMA issue
+constexpr int TC_THREADS = EPI_THREADS + 96;  // warp 12: TMA copies; warp 13: MMA issue; warp 14: frequencies
 constexpr int TC_COLS = NEP * 128;
 
 // An active mode triple, written by k_v3tc for k_v3tc_eval: the row (pair, s2) of Y for its s1,
@@ -290,15 +290,15 @@ struct TcItem {
 };
 static_assert(sizeof(TcItem) == 64, "item");
 
-// Warp-specialised tensor-core pass.  The fill warp loads operand stage j % 2 and epilogue stage
-// j % 4 for tile j: TMA gathers of the A images, four pairs' table rows per request (hi and lo parts
-// as separate requests), one bulk copy of the B images when q1 changed, and the tile's frequencies
-// (plain loads issued one tile ahead); all complete on ready[j % 4].  The MMA warp issues tile j's
-// MMAs into the accumulator of epilogue stage j % 4 and commits them to full[j % 4] and
-// opfree[j % 2].  Each epilogue warp works on its own: it reads its 32 accumulator rows, screens its
-// 12 mode triples per row in FP32 against the delta window, releases the stage, and appends the
-// active triples (with their Y values) to this CTA's region of the item list.  The FP64 part runs
-// in k_v3tc_eval.
+// Warp-specialised tensor-core pass.  For tile j the copy warp loads operand stage j % 2 (TMA
+// gathers of the A images, four pairs' table rows per request, hi and lo parts as separate
+// requests; one bulk copy of the B images when q1 changed) and the frequency warp epilogue stage
+// j % 4 (entry records and the tile's omegas, plain loads issued one tile ahead); both complete on
+// ready[j % 4].  The MMA warp issues tile j's MMAs into the accumulator of epilogue stage j % 4 and
+// commits them to full[j % 4] and opfree[j % 2].  Each epilogue warp works on its own: it reads its
+// 32 accumulator rows, screens its 12 mode triples per row in FP32 against the delta window,
+// releases the stage, and appends the active triples (with their Y values) to this CTA's region of
+// the item list.  The FP64 part runs in k_v3tc_eval.
 template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict__ tiles, const int4* __restrict__ entrec,
@@ -323,7 +323,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             tc::mbar_init(tc::smem_u32(&S.opfree[k]), 1);
         }
         for (int k = 0; k < NEP; ++k) {
-            tc::mbar_init(tc::smem_u32(&S.ready[k]), 32);
+            tc::mbar_init(tc::smem_u32(&S.ready[k]), 64);  // copy-warp and frequency-warp lanes
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_WARPS);
         }
@@ -337,12 +337,65 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     const uint32_t tm = S.tslot;
 
     if (warp == EPI_WARPS) {
-        // ------------------------------------------------------------ fill warp
-        // Records in registers, loaded ahead so that their latency stays hidden: tile records of
-        // j .. j+3 (recA .. recD), entry lane of tiles j .. j+2 (entA .. entC), and the frequencies
-        // of tile j (loaded during the fill of j-1: lane p < 16 holds pair p's q0 omegas, lane 16 + p
-        // pair p's q2 omegas, lane 0 also the q1 omegas).  No warp barrier follows a load: each lane
-        // arrives on ready itself, after its own copies and stores and before it issues new loads.
+        // ------------------------------------------------------------ copy warp
+        // Operand stage j % 2 for tile j, after the MMAs of tile j-2 released it (so every earlier
+        // phase of ready[j % 4] has completed): TMA gathers of the A images and, when q1 changed,
+        // the B images; each issuing lane adds its own bytes to ready before its copy, then every
+        // lane arrives.  Tile and entry records are loaded ahead into registers.
+        const int4 z4 = make_int4(0, 0, 0, 0);
+        int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4;
+        int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
+        bool abort = false;
+        int filled = -1;
+        for (int j = 0; j < nt; ++j) {
+            const int es = j % NEP, os = j % NOP;
+            const bool ok = j < NOP || tc::mbar_wait(tc::smem_u32(&S.opfree[os]), (uint32_t)(((j - NOP) / NOP) & 1),
+                                                     MAX_SPINS);
+            if (__any_sync(0xffffffffu, !ok)) {
+                if (lane == 0) atomicExch(err, 1);
+                abort = true;
+                break;
+            }
+            OpStage& O = S.op[os];
+            const int q1 = recA.x, ne = recA.z;
+            // lane l < 4 H gathers group g = l / H (pairs 4g .. 4g+3, beyond ne repeating pair 0),
+            // part l % H; lane 31 copies the B images when q1 changed.
+            const int g = (lane / H) & 3, part = lane % H;
+            int rows[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, 4 * g + k < ne ? 4 * g + k : 0);
+            const uint32_t rb = tc::smem_u32(&S.ready[es]);
+            if (lane < 4 * H && 4 * g < ne) {
+                tc::mbar_expect_tx(rb, 4u * PB);
+                tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[0], rows[1], rows[2],
+                                rows[3], rb);
+            }
+            if (lane == 31 && O.q1 != q1) {
+                O.q1 = q1;
+                tc::mbar_expect_tx(rb, (uint32_t)(2 * H * B_BYTES));
+                tc::bulk_g2s(tc::smem_u32(&O.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
+            }
+            tc::mbar_arrive(rb);
+            filled = j;
+            const int4 entB = (j + 1 < nt && lane < recB.z) ? entrec[recB.y + lane] : z4;
+            const int4 recC = j + 2 < nt ? tiles[t0 + j + 2] : z4;
+            recA = recB;
+            recB = recC;
+            entA = entB;
+        }
+        if (abort && lane == 0) {
+            // Error path: wait (bounded) for the copies still in flight before the CTA releases its
+            // shared memory.
+            for (int t = max(0, filled - NEP + 1); t <= filled; ++t)
+                tc::mbar_wait(tc::smem_u32(&S.ready[t % NEP]), (uint32_t)((t / NEP) & 1), MAX_SPINS);
+        }
+    } else if (warp == EPI_WARPS + 2) {
+        // ------------------------------------------------------------ frequency warp
+        // Epilogue stage j % 4 for tile j, after the epilogue of tile j-4 released it: entry
+        // records, the q1 and per-pair q0 / q2 omegas (loaded during the fill of j-1: lane p < 16
+        // holds pair p's q0 omegas, lane 16 + p pair p's q2 omegas, lane 0 also the q1 omegas).
+        // No warp barrier follows a load: each lane arrives on ready itself, after its own stores
+        // and before it issues new loads.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
@@ -366,39 +419,16 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
         };
         if (nt > 0) load_w(entA, recA);
-        bool abort = false;
-        int filled = -1;
         for (int j = 0; j < nt; ++j) {
-            const int es = j % NEP, os = j % NOP;
-            bool ok = true;
-            if (j >= NEP) ok = tc::mbar_wait(tc::smem_u32(&S.empty[es]), (uint32_t)(((j - NEP) / NEP) & 1), MAX_SPINS);
-            if (ok && j >= NOP) ok = tc::mbar_wait(tc::smem_u32(&S.opfree[os]), (uint32_t)(((j - NOP) / NOP) & 1), MAX_SPINS);
+            const int es = j % NEP;
+            const bool ok = j < NEP || tc::mbar_wait(tc::smem_u32(&S.empty[es]), (uint32_t)(((j - NEP) / NEP) & 1),
+                                                     MAX_SPINS);
             if (__any_sync(0xffffffffu, !ok)) {
                 if (lane == 0) atomicExch(err, 1);
-                abort = true;
                 break;
             }
             EpStage& E = S.ep[es];
-            OpStage& O = S.op[os];
             const int q1 = recA.x, ne = recA.z;
-            // lane l < 4 H gathers group g = l / H (pairs 4g .. 4g+3, beyond ne repeating pair 0),
-            // part l % H; lane 31 copies the B images when q1 changed.  Each issuing lane adds its
-            // own bytes to ready before its copy.
-            const int g = (lane / H) & 3, part = lane % H;
-            int rows[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, 4 * g + k < ne ? 4 * g + k : 0);
-            const uint32_t rb = tc::smem_u32(&S.ready[es]);
-            if (lane < 4 * H && 4 * g < ne) {
-                tc::mbar_expect_tx(rb, 4u * PB);
-                tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[0], rows[1], rows[2],
-                                rows[3], rb);
-            }
-            if (lane == 31 && O.q1 != q1) {
-                O.q1 = q1;
-                tc::mbar_expect_tx(rb, (uint32_t)(2 * H * B_BYTES));
-                tc::bulk_g2s(tc::smem_u32(&O.B[0]), tabB + (size_t)q1 * 4 * BIMG, (uint32_t)(2 * H * B_BYTES), rb);
-            }
             if (lane == 0) {
                 E.ne = ne;
                 E.q1 = q1;
@@ -414,8 +444,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 d[1] = wv[1];
                 d[2] = wv[2];
             }
-            tc::mbar_arrive(rb);  // each lane releases its own stores
-            filled = j;
+            tc::mbar_arrive(tc::smem_u32(&S.ready[es]));  // each lane releases its own stores
             // loads for later fills
             if (j + 1 < nt) load_w(entB, recB);
             const int4 entC = (j + 2 < nt && lane < recC.z) ? entrec[recC.y + lane] : z4;
@@ -425,12 +454,6 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             recC = recD;
             entA = entB;
             entB = entC;
-        }
-        if (abort && lane == 0) {
-            // Error path: wait (bounded) for the copies still in flight before the CTA releases its
-            // shared memory.
-            for (int t = max(0, filled - NEP + 1); t <= filled; ++t)
-                tc::mbar_wait(tc::smem_u32(&S.ready[t % NEP]), (uint32_t)((t / NEP) & 1), MAX_SPINS);
         }
     } else if (warp == EPI_WARPS + 1) {
         // ------------------------------------------------------------ MMA warp
