@@ -76,6 +76,16 @@ int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* wha
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
 }
 
+__global__ void k_sum2(const int* __restrict__ a, const int* __restrict__ b, int* __restrict__ out) { *out = *a + *b; }
+
+// *a + *b of two device ints with one readback.
+int d2h_sum2(spring_ctx* c, const int* a, const int* b, int* out, const char* what) {
+    SPRING_CHECK(dalloc(c, c->d_scr_sum, 1, what));
+    k_sum2<<<1, 1, 0, c->stream>>>(a, b, c->d_scr_sum.p);
+    SPRING_CHECK(launch_check(c, "k_sum2"));
+    return d2h(c, out, c->d_scr_sum.p, sizeof(int), what);
+}
+
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what) {
     cudaError_t e = cudaMemsetAsync(dst, 0, bytes, c->stream);
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
@@ -253,8 +263,8 @@ int spring_ctx_destroy(spring_ctx* c) {
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
-        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_tc_entries);
-        dfree(c->d_tc_rec); dfree(c->d_tc_tiles); dfree(c->d_tc_err);
+        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_tc_entries);
+        dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
         dfree(c->d_scr_rep); dfree(c->d_tc_keys); dfree(c->d_tc_keys_s); dfree(c->d_tc_vals); dfree(c->d_tc_cnt);
         dfree(c->d_tc_seg); dfree(c->d_tc_ntl); dfree(c->d_tc_toff); dfree(c->d_tc_sort);

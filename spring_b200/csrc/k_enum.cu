@@ -126,10 +126,8 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
         rc = launch_check(c, "k_enum3_flags");
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, rep.p, ps.pairpos.p, (int)total);
-    int last[2] = {0, 0};
-    if (rc == SPRING_OK) rc = d2h(c, &last[0], ps.pairpos.p + total - 1, sizeof(int), "pair count");
-    if (rc == SPRING_OK) rc = d2h(c, &last[1], rep.p + total - 1, sizeof(int), "pair count");
-    const int npairs = last[0] + last[1];
+    int npairs = 0;
+    if (rc == SPRING_OK) rc = d2h_sum2(c, ps.pairpos.p + total - 1, rep.p + total - 1, &npairs, "pair count");
     if (rc == SPRING_OK) rc = dalloc(c, ps.pairs, npairs, "pair list");
     if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, npairs, "pair list");
     if (rc == SPRING_OK) rc = dalloc(c, ps.pairoff, ps.n0 + 1, "pair offsets");

@@ -3,8 +3,11 @@
 //   rotation-averaged v(x)v of GrVelKronProdSymm (VelocityKronProd_symm.f90:34-91),
 //   or kappa_noIter over the full grid (ThermalConductivity.f90:36-164).
 // kappa_ab = kW_m_k / (T^2 V Nq) * sum_{q,s} w^2 n (n+1) tau (v(x)v)_ab,  tau = 0.5/Gamma;
-// Gamma-point acoustic modes are skipped.  One CTA per temperature; the sum is
-// reduced per thread, then as a tree in shared memory.  Negligible cost.
+// Gamma-point acoustic modes are skipped.  Up to 64 CTAs per temperature each reduce a slice of
+// the mode points (per thread, then as a tree in shared memory) into a partial sum; k_kappa_sum adds
+// the partial sums in block order, so the result does not depend on scheduling.  Negligible cost.
+#include <algorithm>
+
 #include "spring_internal.cuh"
 
 namespace spring {
@@ -30,17 +33,16 @@ __global__ void __launch_bounds__(256) k_kappa(KapArgs a, const double* __restri
                                                const double* __restrict__ rxyz, const int* __restrict__ qint,
                                                const int* __restrict__ pos, const double* __restrict__ om,
                                                const double* __restrict__ nbe, const double* __restrict__ vel,
-                                               const double* __restrict__ lw, double* __restrict__ kappa,
-                                               double* __restrict__ mode) {
+                                               const double* __restrict__ lw, double* __restrict__ part) {
     __shared__ double red[256][9];
     __shared__ double smode[MAX_NDOF * 9];
-    const int T = blockIdx.x;
+    const int T = blockIdx.y, nbk = gridDim.x;
     const double temp = temps[T];
     const int npts = a.symm ? a.nq0 : a.nq;
     for (int i = threadIdx.x; i < a.n * 9; i += blockDim.x) smode[i] = 0.0;
     __syncthreads();
     double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int it = threadIdx.x; it < npts * a.n; it += blockDim.x) {
+    for (int it = blockIdx.x * blockDim.x + threadIdx.x; it < npts * a.n; it += nbk * blockDim.x) {
         const int q = it / a.n, s = it % a.n;
         const int* qi = a.symm ? irr_int + 3 * q : qint + 3 * q;
         const bool gamma = qi[0] == 0 && qi[1] == 0 && qi[2] == 0;
@@ -71,7 +73,7 @@ __global__ void __launch_bounds__(256) k_kappa(KapArgs a, const double* __restri
         for (int k = 0; k < 9; ++k) {
             const double kq = pre * kr[k];
             acc[k] += kq;
-            if (mode) atomicAdd(&smode[s * 9 + k], kq);
+            atomicAdd(&smode[s * 9 + k], kq);
         }
     }
     for (int k = 0; k < 9; ++k) red[threadIdx.x][k] = acc[k];
@@ -81,10 +83,26 @@ __global__ void __launch_bounds__(256) k_kappa(KapArgs a, const double* __restri
             for (int k = 0; k < 9; ++k) red[threadIdx.x][k] += red[threadIdx.x + h][k];
         __syncthreads();
     }
+    // this block's partial sums: [T][block][kappa 9, then mode n x 9]
+    double* out = part + ((size_t)T * nbk + blockIdx.x) * (9 + a.n * 9);
+    if (threadIdx.x < 9) out[threadIdx.x] = red[0][threadIdx.x];
+    for (int i = threadIdx.x; i < a.n * 9; i += blockDim.x) out[9 + i] = smode[i];
+}
+
+// kappa[T][9] and mode[T][n][9] (mode may be null): the blocks' partial sums in block order, times
+// the prefactor.
+__global__ void k_kappa_sum(KapArgs a, int nbk, const double* __restrict__ temps, const double* __restrict__ part,
+                            double* __restrict__ kappa, double* __restrict__ mode) {
+    const int T = blockIdx.x;
+    const int w = 9 + a.n * 9;
+    const double temp = temps[T];
     const double f2 = a.kwmk / ((temp * temp) * a.vol) / double(a.nq);
-    if (threadIdx.x < 9) kappa[T * 9 + threadIdx.x] = red[0][threadIdx.x] * f2;
-    if (mode)
-        for (int i = threadIdx.x; i < a.n * 9; i += blockDim.x) mode[(size_t)T * a.n * 9 + i] = smode[i] * f2;
+    for (int i = threadIdx.x; i < w; i += blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < nbk; ++b) acc += part[((size_t)T * nbk + b) * w + i];
+        if (i < 9) kappa[T * 9 + i] = acc * f2;
+        else if (mode) mode[(size_t)T * a.n * 9 + (i - 9)] = acc * f2;
+    }
 }
 
 }  // namespace
@@ -111,10 +129,18 @@ int run_kappa_rta(spring_ctx* c, int symm, int nsym, const double* d_rxyz, int s
     a.kwmk = host_constants().kW_m_k;
     a.vol = c->vol;
     const Phonons& ph = symm ? c->ph_irr : c->ph_grid;
+    // blocks per temperature: about two mode points per thread, at most 64 blocks
+    const int npts = (symm ? c->nq0 : c->nq) * c->ndof;
+    const int nbk = std::max(1, std::min(64, (npts + 511) / 512));
+    SPRING_CHECK(dalloc(c, c->d_kap_part, (size_t)c->nT * nbk * (9 + c->ndof * 9), "kappa partial sums"));
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "kappa: injected launch failure");
-    k_kappa<<<c->nT, 256, 0, c->stream>>>(a, c->d_temps.p, c->d_irr_int.p, c->d_mult.p, d_rxyz, c->d_qint.p,
-                                          c->d_pos.p, ph.omega.p, ph.nbe.p, ph.vel.p, c->d_lw_all.p, d_kappa, d_mode);
-    return launch_check(c, "k_kappa");
+    k_kappa<<<dim3(nbk, c->nT), 256, 0, c->stream>>>(a, c->d_temps.p, c->d_irr_int.p, c->d_mult.p, d_rxyz,
+                                                      c->d_qint.p, c->d_pos.p, ph.omega.p, ph.nbe.p, ph.vel.p,
+                                                      c->d_lw_all.p, c->d_kap_part.p);
+    SPRING_CHECK(launch_check(c, "k_kappa"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "kappa: injected launch failure");
+    k_kappa_sum<<<c->nT, 256, 0, c->stream>>>(a, nbk, c->d_temps.p, c->d_kap_part.p, d_kappa, d_mode);
+    return launch_check(c, "k_kappa_sum");
 }
 
 }  // namespace spring

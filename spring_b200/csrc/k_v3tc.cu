@@ -718,7 +718,7 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
     k_v3tc<SPLIT><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
         a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p, c->ph_grid.omega.p, items,
-        c->d_tc_cnt_cta.p, c->d_tc_err.p);
+        c->d_tc_cnt_cta.p, c->d_tc_cnt_cta.p + c->tc_grid);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -774,10 +774,8 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
         }
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, ntl.p, toff.p, nq);
-    int last[2] = {0, 0};
-    if (rc == SPRING_OK) rc = d2h(c, &last[0], toff.p + nq - 1, sizeof(int), "tile count");
-    if (rc == SPRING_OK) rc = d2h(c, &last[1], ntl.p + nq - 1, sizeof(int), "tile count");
-    const int ntiles = last[0] + last[1];
+    int ntiles = 0;
+    if (rc == SPRING_OK) rc = d2h_sum2(c, toff.p + nq - 1, ntl.p + nq - 1, &ntiles, "tile count");
     if (rc == SPRING_OK) rc = dalloc(c, c->d_tc_tiles, std::max(ntiles, 1), "tiles");
     if (rc == SPRING_OK) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
@@ -818,8 +816,6 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
     const int rs = (2 + c->nT + 3) / 4 * 4;
     SPRING_CHECK(dalloc(c, c->d_tc_modes, (size_t)nq * NMODE * rs, "V3 mode records"));
-    SPRING_CHECK(dalloc(c, c->d_tc_err, 1, "V3 status"));
-    SPRING_CHECK(zero(c, c->d_tc_err.p, sizeof(int), "V3 status"));
     SPRING_CHECK(build_tiles(c, p0, p1));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
@@ -859,26 +855,26 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const int ctas = std::max(1, std::min(a.ntiles, sms));
     a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
     c->tc_grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
-    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, c->tc_grid, "V3 item counts"));
+    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, c->tc_grid + 1, "V3 item counts"));  // + the status word
     // Item list: one region per CTA, first sized for 4 % of the CTA's mode triples (about 1-2 % pass
     // the screen on meshes from 8^3 to 24^3), regrown to what the pass reports if that overflows.
     const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE;
     long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 25, 1024);
     const bool split = c->precision == SPRING_BF16X3;
-    std::vector<int> cnt(c->tc_grid);
+    std::vector<int> cnt(c->tc_grid + 1);
     int maxcnt = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         cap = std::min<long long>(cap, triples);
         a.cap = (int)cap;
         SPRING_CHECK(dalloc(c, c->d_tc_items, (size_t)c->tc_grid * cap * (sizeof(TcItem) / sizeof(float4)), "V3 items"));
         TcItem* items = reinterpret_cast<TcItem*>(c->d_tc_items.p);
+        SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p + c->tc_grid, sizeof(int), "V3 status"));
         SPRING_CHECK(split ? launch_tc<true>(c, a, items) : launch_tc<false>(c, a, items));
-        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * c->tc_grid, "V3 item counts"));
-        int herr = 0;
-        SPRING_CHECK(d2h(c, &herr, c->d_tc_err.p, sizeof(int), "V3 status"));
+        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * (c->tc_grid + 1), "V3 item counts"));
+        const int herr = cnt[c->tc_grid];
         if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
         if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
-        maxcnt = *std::max_element(cnt.begin(), cnt.end());
+        maxcnt = *std::max_element(cnt.begin(), cnt.begin() + c->tc_grid);
         if (maxcnt <= cap) break;
         cap = (long long)(maxcnt * 1.25) + 1024;  // the pass only wrote what fit; run it again
     }

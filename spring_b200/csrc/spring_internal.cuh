@@ -173,6 +173,7 @@ struct spring_ctx {
     spring::DBuf<double> d_lw_tmp; // per-call output [T][q0][s]
     spring::DBuf<double> d_p3;     // per-call phase space [q0][s]
     spring::DBuf<double> d_kappa;  // [T][9] and mode [T][s][9]
+    spring::DBuf<double> d_kap_part;  // per-block partial sums of the kappa kernel
     spring::DBuf<double> d_krn;    // [q0][s][9]
     spring::DBuf<double> d_rxyz;
     spring::DBuf<double> d_wiso;   // [slot][q1][s0][s1]
@@ -183,13 +184,13 @@ struct spring_ctx {
     spring::DBuf<double> d_tc_q0;      // q0 mode records: e0' float2[6], omega, 1/omega (64 bytes each)
     spring::DBuf<double> d_tc_modes;   // grid mode records: omega, 1/omega, nBE[T] (padded to 4 doubles)
     spring::DBuf<float4> d_tc_items;   // active mode triples, one region per CTA (64 bytes each)
-    spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA
+    spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA, then the status word
+    spring::DBuf<int> d_scr_sum;       // one-int readback scratch
     int tc_grid = 0;
     double tc_cap_frac = 0.0;          // item region size as a fraction of the CTA's triples
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
-    spring::DBuf<int> d_tc_err;
     int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1;
     // scratch kept between calls (the enumeration and the tile sort run every step)
     spring::DBuf<int> d_scr_rep, d_tc_keys, d_tc_keys_s, d_tc_vals, d_tc_cnt, d_tc_seg, d_tc_ntl, d_tc_toff;
@@ -231,6 +232,7 @@ int alloc_phonons(spring_ctx* c, Phonons& p, int n);
 int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what);
+int d2h_sum2(spring_ctx* c, const int* a, const int* b, int* out, const char* what);
 // Every kernel launch site calls launch_injected() first (fault injection and,
 // when profiling, the start event) and launch_check() right after the launch
 // (error check, launch count, stop event named after the kernel).
