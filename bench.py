@@ -82,48 +82,103 @@ def tc_tiles(counts_by_q1):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (20 ms period)."""
+    """SM clock and clock-event reasons sampled through NVML by a background thread while a timed
+    region is open (begin/end around each one); median SM clock under load, max clock and the
+    reasons seen.  Falls back to nvidia-smi polling when the NVML bindings are missing."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index):
-        self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+    def __init__(self, index, bus_id=None):
+        import threading
+        self.index, self.bus_id = index, bus_id
+        self.rows = []
+        self.active = threading.Event()
+        self.done = threading.Event()
+        self.thread = None
         self.p = None
+        self.f = None
+
+    def _nvml_loop(self, nv, h):
+        names = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                 "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                 "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.done.is_set():
+            if not self.active.wait(0.05):
+                continue
+            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            if self.active.is_set():
+                self.rows.append((float(sm), float(smax), sorted(k for k, v in names.items() if r & v)))
+            time.sleep(0.002)
 
     def start(self):
         try:
-            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                       "--format=csv,noheader,nounits", "-lms", "20"], stdout=self.f,
-                                      stderr=subprocess.DEVNULL)
-        except OSError:
-            self.p = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = (nv.nvmlDeviceGetHandleByPciBusId(self.bus_id) if self.bus_id
+                 else nv.nvmlDeviceGetHandleByIndex(self.index))
+            import threading
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+        except Exception:
+            self.thread = None
+            self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            try:
+                self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                           "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                          stderr=subprocess.DEVNULL)
+            except OSError:
+                self.p = None
+
+    def begin(self):
+        self.active.set()
+
+    def end(self):
+        self.active.clear()
 
     def stop(self):
-        if self.p is None:
-            return None
-        self.p.terminate()
-        try:
-            self.p.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.p.kill()
-        self.f.flush()
         rows = []
-        with open(self.f.name) as fh:
-            for r in csv.reader(fh):
-                if len(r) >= 9:
-                    rows.append([x.strip() for x in r])
-        os.unlink(self.f.name)
+        if self.thread is not None:
+            self.done.set()
+            self.active.set()
+            self.thread.join(timeout=5)
+            rows = self.rows
+        elif self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+            self.f.flush()
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            with open(self.f.name) as fh:
+                for r in csv.reader(fh):
+                    r = [x.strip() for x in r]
+                    if len(r) >= 9 and r[1].replace(".", "").isdigit() and r[2].replace(".", "").isdigit():
+                        rows.append((float(r[1]), float(r[2]), [names[k] for k in range(4) if r[5 + k].lower() == "active"]))
+            os.unlink(self.f.name)
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
-        load = [s for s in sm if s > 0.5 * smax] or sm
-        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows)}
+        smax = max(r[1] for r in rows)
+        sm = [r[0] for r in rows]
+        load = [x for x in sm if x > 0.5 * smax] or sm
+        reasons = sorted({k for r in rows for k in r[2]})
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": smax, "reasons": reasons, "samples": len(rows),
+                "source": "nvml" if self.thread is not None else "nvidia-smi"}
+
+
+def pci_bus_id(torch, index):
+    """NVML bus id ('dddddddd:bb:dd.0') of a CUDA device, so the sampler reads the GPU this process
+    runs on whatever CUDA_VISIBLE_DEVICES maps; None when torch does not expose it."""
+    try:
+        p = torch.cuda.get_device_properties(index)
+        return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    except Exception:
+        return None
 
 
 def fp64_peak_tflops(torch):
@@ -411,6 +466,7 @@ def run_ours(args):
             dist.barrier()
         if clocks:
             clocks.start()
+            clocks.begin()
         ctx.set_profiling(True)
         l0 = ctx.kernel_launches()
         times = []
@@ -427,6 +483,8 @@ def run_ours(args):
         kt = {k: ctx.kernel_time(k) for k in ("k_v3tc<", "k_v3tc_eval", "k_v3s", "k_v3<", "k_phonons", "k_tc_tab",
                                               "k_kappa")}
         ctx.set_profiling(False)
+        if clocks:
+            clocks.end()
         clk = clocks.stop() if clocks else None
         ms = float(np.sum(times)) / args.steps
         if world > 1:
@@ -440,7 +498,7 @@ def run_ours(args):
 
     with torch.cuda.stream(stream):
         ms64, _, kt64, lw64, kap64, _ = timed("fp64")
-        clocks = Clocks(local)
+        clocks = Clocks(local, pci_bus_id(torch, local))
         ms, launches, kt, lw_p, kap_p, clk = timed(args.precision, clocks)
         big = lw64 > 1e-3 * lw64.max(axis=(1, 2), keepdims=True)
         lw_err = float((np.abs(lw_p - lw64)[big] / lw64[big]).max())

@@ -263,7 +263,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
-        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_tc_entries);
+        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
         dfree(c->d_scr_rep); dfree(c->d_tc_keys); dfree(c->d_tc_keys_s); dfree(c->d_tc_vals); dfree(c->d_tc_cnt);
@@ -574,7 +574,7 @@ static int install_irr(spring_ctx* c, int nq0, const int* irr_int, const int* po
     c->ps_irr.done = false;
     c->ps_irr.n0 = nq0;
     c->ps_irr.q0_int = c->d_irr_int.p;
-    free_phonons(c->ph_irr);
+    c->ph_irr.set = false;  // buffers kept; recomputed for the new set
     return SPRING_OK;
 }
 
@@ -583,7 +583,7 @@ int spring_find_irr_q(spring_ctx* c, int nrot, const int* rot, int time_rev, int
     CTX_ENTER(c);
     SPRING_CHECK(need(c, c->mesh_set, "mesh"));
     if (nrot < 1 || nrot > 192 || !rot) return fail(c, SPRING_ERR_ARG, "rotations: need 1..192 matrices");
-    DBuf<int> d_rot, d_map;
+    DBuf<int>&d_rot = c->d_scr_rot, &d_map = c->d_scr_map;  // kept between calls
     int rc = dalloc(c, d_rot, (size_t)nrot * 9, "rotations");
     if (rc == SPRING_OK) rc = dalloc(c, d_map, c->nq, "irreducible map");
     if (rc == SPRING_OK) rc = h2d(c, d_rot.p, rot, sizeof(int) * 9 * nrot, "rotations");
@@ -591,8 +591,6 @@ int spring_find_irr_q(spring_ctx* c, int nrot, const int* rot, int time_rev, int
     std::vector<int> map(c->nq), qint((size_t)c->nq * 3);
     if (rc == SPRING_OK) rc = d2h(c, map.data(), d_map.p, sizeof(int) * c->nq, "irreducible map");
     if (rc == SPRING_OK) rc = d2h(c, qint.data(), c->d_qint.p, sizeof(int) * c->nq * 3, "q_pnt_int");
-    dfree(d_rot);
-    dfree(d_map);
     if (rc != SPRING_OK) return rc;
     // unique_sort + FindPositionAndMultiplicity (Helper_m.f90:510-594)
     std::vector<int> uniq(map);

@@ -186,6 +186,7 @@ struct spring_ctx {
     spring::DBuf<float4> d_tc_items;   // active mode triples, one region per CTA (64 bytes each)
     spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA, then the status word
     spring::DBuf<int> d_scr_sum;       // one-int readback scratch
+    spring::DBuf<int> d_scr_rot, d_scr_map;  // spring_find_irr_q scratch: rotations, orbit map
     int tc_grid = 0;
     double tc_cap_frac = 0.0;          // item region size as a fraction of the CTA's triples
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
