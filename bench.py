@@ -68,8 +68,8 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
 BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
 TC_EPT = 16         # pairs per tensor-core tile
 # DRAM bytes per pair of the tensor-core pass (read + write), from one ncu capture of the 16^3
-# rocksalt launch (297,076 pairs; 71.2 MB read, 18.2 MB written)
-TC_DRAM_BYTES_PER_PAIR = (71.164672e6 + 18.171648e6) / 297076
+# rocksalt launch (297,076 pairs; 71.0 MB read, 18.8 MB written)
+TC_DRAM_BYTES_PER_PAIR = (70.992384e6 + 18.826752e6) / 297076
 
 
 def tc_issued_flops_per_tile(passes):
