@@ -624,6 +624,7 @@ int spring_compute_phonons(spring_ctx* c, const double* temps, double freq_cut) 
     SPRING_CHECK(alloc_phonons(c, c->ph_irr, c->nq0));
     SPRING_CHECK(run_phonons_mesh(c));
     c->ph_grid.set = c->ph_irr.set = true;
+    c->ph_gen += 1;
     dfree(c->d_wtr);  // cached W grids depend on the phonons
     return SPRING_OK;
 }
@@ -646,6 +647,7 @@ int spring_set_phonons(spring_ctx* c, int which, const double* temps, const doub
     SPRING_CHECK(h2d(c, p.vel.p, vel, sizeof(double) * n * nd * 3, "group velocity"));
     SPRING_CHECK(spring_synchronize(c));
     p.set = true;
+    c->ph_gen += 1;
     if (which == 0) dfree(c->d_wtr);  // cached W grids depend on the grid phonons
     return SPRING_OK;
 }

@@ -16,7 +16,9 @@
 //   B[(im, a s1)][k] = [Im Z | Re Z].
 // Precision: SPRING_BF16 rounds A and B to BF16 once; SPRING_BF16X3 splits each
 // into hi + lo BF16 parts and accumulates hi*hi + hi*lo + lo*hi (compensated).
-// Frequencies, occupations, the delta weights and every sum stay FP64.  Two
+// Frequencies, occupations, the delta weights and every sum stay FP64.  Pairs with
+// no mode triple inside the delta window are dropped before the tiles are cut
+// (k_tc_keys, about half of them).  Two
 // passes: k_v3tc computes Y on the tensor cores and screens each mode triple in
 // FP32 against the window where a delta weight can exceed exp(-40) of its peak
 // (4e-18), writing the ~1-2 % inside it (with their Y values) to an item list;
@@ -53,6 +55,14 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
     const float f = (float)x;
     hi = __float2bfloat16_rn(f);
     lo = __float2bfloat16_rn(f - __bfloat162float(hi));
+}
+
+// FP32 delta-window test of one mode triple, shared by the pair pre-screen and the tensor-core
+// pass so that both decide alike: with c = |w0 - w2| and b = w0 + w2 (rounded from FP64), the
+// triple is kept when ||w1| - c| < R or |b - w1| < R, R covering every delta weight above exp(-40)
+// of its peak.
+__device__ __forceinline__ bool tc_window(float c, float b, float w1, float rf) {
+    return fabsf(fabsf(w1) - c) < rf || fabsf(b - w1) < rf;
 }
 
 // Phases e^{i q.R_{mu N}} of one grid point and basis atom, N < na, into ph[N] (threads 0..na-1).
@@ -214,13 +224,33 @@ __global__ void k_tc_modes(int nq, int nT, int rs, const double* __restrict__ om
 }
 
 // ------------------------------------------------------------------ tiles
-__global__ void k_tc_keys(int n, int p0, const int2* __restrict__ pairs, int* __restrict__ keys, int* __restrict__ vals,
-                          int* __restrict__ cnt) {
+// Sort keys of the pairs: q1 for a pair with at least one mode triple inside the delta window,
+// nq (sorted after every q1, and left out of the tiles) for a pair with none.  The test is the
+// tensor-core pass's own, so a pair left out would have produced no item there.  About half the
+// pairs of a 24^3 mesh (Gaussian width 0.38 rad/ps) have no triple in the window.
+__global__ void k_tc_keys(int n, int p0, int nq, const int2* __restrict__ pairs, const int* __restrict__ pair_q0,
+                          const double* __restrict__ om0, const double* __restrict__ omg, float rf,
+                          int* __restrict__ keys, int* __restrict__ vals, int* __restrict__ cnt) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int g1 = pairs[p0 + i].x;
-        keys[i] = g1;
+        const int2 pq = pairs[p0 + i];
+        const double* w0 = om0 + (size_t)pair_q0[p0 + i] * NMODE;
+        const double* w2 = omg + (size_t)pq.y * NMODE;
+        float w1[NMODE];
+#pragma unroll
+        for (int s1 = 0; s1 < NMODE; ++s1) w1[s1] = (float)omg[(size_t)pq.x * NMODE + s1];
+        bool any = false;
+        for (int s0 = 0; s0 < NMODE && !any; ++s0) {
+            const double a0 = w0[s0];
+            for (int s2 = 0; s2 < NMODE && !any; ++s2) {
+                const double a2 = w2[s2];
+                const float c = fabsf((float)(a0 - a2)), b = (float)(a0 + a2);
+#pragma unroll
+                for (int s1 = 0; s1 < NMODE; ++s1) any |= tc_window(c, b, w1[s1], rf);
+            }
+        }
+        keys[i] = any ? pq.x : nq;
         vals[i] = p0 + i;
-        atomicAdd(&cnt[g1], 1);
+        if (any) atomicAdd(&cnt[pq.x], 1);
     }
 }
 __global__ void k_tc_ntiles(int nq, const int* __restrict__ cnt, int* __restrict__ nt) {
@@ -251,10 +281,12 @@ struct TcArgs {
     int nq, nq0, nT, ntiles, tiles_per_cta, cap;
     int lo[3], hi[3];
     double half_os2;
+    float rf;  // delta window of the FP32 screen (tc_window)
 };
 
 constexpr int NOP = 2;  // operand stages (A and B images; free once the tile's MMAs completed)
 constexpr int NEP = 4;  // epilogue stages (frequencies and one 128-column accumulator each)
+static_assert(NOP <= NEP, "a fill of ready[j % NEP] must follow the completion of its previous phase");
 
 struct OpStage {
     alignas(128) uint8_t A[2][EPT * 1536];    // [hi, lo]: per pair its two mu images (pair stride 1536)
@@ -339,7 +371,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     if (warp == EPI_WARPS) {
         // ------------------------------------------------------------ copy warp
         // Operand stage j % 2 for tile j, after the MMAs of tile j-2 released it (so every earlier
-        // phase of ready[j % 4] has completed): TMA gathers of the A images and, when q1 changed,
+        // phase of ready[j % 4] has completed, NOP <= NEP): TMA gathers of the A images and, when q1 changed,
         // the B images; each issuing lane adds its own bytes to ready before its copy, then every
         // lane arrives.  Tile and entry records are loaded ahead into registers.
         const int4 z4 = make_int4(0, 0, 0, 0);
@@ -501,7 +533,6 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         // ------------------------------------------------------------ epilogue warps
         const int wq = warp & 3, grp = warp >> 2;  // lane quarter, s0 pair (2 grp, 2 grp + 1)
         const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
-        const float Rf = (float)(sqrt(EXP_CUT / a.half_os2) * 1.0001 + 1e-3);
         TcItem* region = items + (size_t)blockIdx.x * a.cap;
         // (s0, s1) slots allowed by the mode ranges and the Gamma acoustic rule (q1 = Gamma: amask_g)
         unsigned s1m = 0u;
@@ -550,10 +581,8 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     const double w0 = jj ? w0b : w0a;
                     const float c = fabsf((float)(w0 - w2)), bf = (float)(w0 + w2);
 #pragma unroll
-                    for (int s1 = 0; s1 < NMODE; ++s1) {
-                        const bool in = fabsf(fabsf(w1f[s1]) - c) < Rf || fabsf(bf - w1f[s1]) < Rf;
-                        act |= in ? (1u << (jj * NMODE + s1)) : 0u;
-                    }
+                    for (int s1 = 0; s1 < NMODE; ++s1)
+                        act |= tc_window(c, bf, w1f[s1], a.rf) ? (1u << (jj * NMODE + s1)) : 0u;
                 }
                 act &= amask;
             }
@@ -722,11 +751,13 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
-// Pairs of [p0, p1) sorted by q1 (stable radix sort), cut into tiles of at most EPT
-// pairs of one q1, with the entry record of every sorted pair.
-int build_tiles(spring_ctx* c, int p0, int p1) {
+// Pairs of [p0, p1) with a mode triple inside the delta window `rf`, sorted by q1 (stable radix
+// sort), cut into tiles of at most EPT pairs of one q1, with the entry record of every sorted pair.
+// Cached until the pair list, the phonons or the window change.
+int build_tiles(spring_ctx* c, int p0, int p1, float rf) {
     const PairSet& ps = c->ps_irr;
-    if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1) return SPRING_OK;
+    if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1 && c->tc_ph_gen == c->ph_gen && c->tc_rf == rf)
+        return SPRING_OK;
     const int n = p1 - p0, nq = c->nq;
     DBuf<int>&keys = c->d_tc_keys, &keys_s = c->d_tc_keys_s, &vals = c->d_tc_vals, &cnt = c->d_tc_cnt,
               &seg = c->d_tc_seg, &ntl = c->d_tc_ntl, &toff = c->d_tc_toff;
@@ -746,13 +777,13 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
     if (rc == SPRING_OK && n > 0) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
         else {
-            k_tc_keys<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(n, p0, ps.pairs.p, keys.p,
-                                                                                                   vals.p, cnt.p);
+            k_tc_keys<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
+                n, p0, nq, ps.pairs.p, ps.pair_q0.p, c->ph_irr.omega.p, c->ph_grid.omega.p, rf, keys.p, vals.p, cnt.p);
             rc = launch_check(c, "k_tc_keys");
         }
     }
     int bits = 1;
-    while ((1 << bits) < nq) ++bits;
+    while ((1 << bits) <= nq) ++bits;  // keys run to nq (pairs outside the window)
     if (rc == SPRING_OK && n > 0) {
         size_t bytes = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, bytes, keys.p, keys_s.p, vals.p, c->d_tc_entries.p, n, 0, bits, c->stream);
@@ -797,6 +828,8 @@ int build_tiles(spring_ctx* c, int p0, int p1) {
     c->tc_gen = ps.gen;
     c->tc_p0 = p0;
     c->tc_p1 = p1;
+    c->tc_ph_gen = c->ph_gen;
+    c->tc_rf = rf;
     return SPRING_OK;
 }
 
@@ -816,7 +849,11 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
     const int rs = (2 + c->nT + 3) / 4 * 4;
     SPRING_CHECK(dalloc(c, c->d_tc_modes, (size_t)nq * NMODE * rs, "V3 mode records"));
-    SPRING_CHECK(build_tiles(c, p0, p1));
+    const double os = 1.0 / sigma;
+    const double half_os2 = 0.5 * (os * os);
+    const float rf = (float)(sqrt(EXP_CUT / half_os2) * 1.0001 + 1e-3);
+    SPRING_CHECK(build_tiles(c, p0, p1, rf));
+    if (c->tc_ntiles == 0) return SPRING_OK;  // no pair has a mode triple inside the window
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
@@ -848,18 +885,19 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
         a.lo[k] = pol.lo[k];
         a.hi[k] = pol.hi[k];
     }
-    const double os = 1.0 / sigma;
-    a.half_os2 = 0.5 * (os * os);
+    a.half_os2 = half_os2;
+    a.rf = rf;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const int ctas = std::max(1, std::min(a.ntiles, sms));
     a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
     c->tc_grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
     SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, c->tc_grid + 1, "V3 item counts"));  // + the status word
-    // Item list: one region per CTA, first sized for 4 % of the CTA's mode triples (about 1-2 % pass
-    // the screen on meshes from 8^3 to 24^3), regrown to what the pass reports if that overflows.
+    // Item list: one region per CTA, first sized for 8 % of the CTA's mode triples (about 3 % of the
+    // triples of the pairs left after the pre-screen pass the screen on meshes from 8^3 to 24^3),
+    // regrown to what the pass reports if that overflows.
     const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE;
-    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 25, 1024);
+    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 12, 1024);
     const bool split = c->precision == SPRING_BF16X3;
     std::vector<int> cnt(c->tc_grid + 1);
     int maxcnt = 0;

@@ -192,7 +192,9 @@ struct spring_ctx {
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
-    int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1;
+    int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1, tc_ph_gen = -1;
+    float tc_rf = 0.0f;                // delta window the cached tiles were screened with
+    int ph_gen = 0;                    // bumped whenever the grid or irreducible phonons change
     // scratch kept between calls (the enumeration and the tile sort run every step)
     spring::DBuf<int> d_scr_rep, d_tc_keys, d_tc_keys_s, d_tc_vals, d_tc_cnt, d_tc_seg, d_tc_ntl, d_tc_toff;
     spring::DBuf<uint8_t> d_tc_sort;

@@ -69,3 +69,48 @@ def test_tc_pair_subset_and_repeat(runs):
         lw, _ = ctx.linewidth3(2, 3, "gauss", SIGMA)
         np.testing.assert_allclose(lw, lw_all[:, 1:4], rtol=1e-12, atol=1e-15)
     ctx.set_precision("fp64")
+
+
+def test_tc_pair_prescreen_follows_sigma_and_phonons(runs):
+    """Pairs with no mode triple inside the delta window are left out of the tiles; the tiles are
+    rebuilt when the Gaussian width or the phonons change.  The phase space (FP64 delta weights of
+    every triple above the exp cut) shows a dropped pair at once, so it is compared at 1e-10."""
+    N, ctx, info, out, st = runs
+    if N != 8:
+        pytest.skip("8^3 mesh only")
+
+    def both(sigma):
+        res = {}
+        for prec in ("fp64", "bf16x3"):
+            ctx.set_precision(prec)
+            ctx.reset_linewidths()
+            res[prec] = ctx.linewidth3(1, ctx.nq0, "gauss", sigma)
+        ctx.set_precision("fp64")
+        return res
+
+    for sigma in (0.05, 1.5, SIGMA):  # narrow window (most pairs dropped), wide (few), default
+        r = both(sigma)
+        p64, p = r["fp64"][1], r["bf16x3"][1]
+        np.testing.assert_allclose(p, p64, rtol=1e-10, atol=1e-12 * np.abs(p64).max())
+        lw64, lw = r["fp64"][0], r["bf16x3"][0]
+        big = lw64 > 1e-3 * lw64.max()
+        assert (np.abs(lw[big] - lw64[big]) / lw64[big]).max() < 1e-4, sigma
+    np.testing.assert_allclose(r["bf16x3"][0], out["bf16x3"][0], rtol=1e-12, atol=1e-15)
+    # a window almost no pair reaches (possibly none: then nothing is launched); the FP64 path keeps
+    # the Gaussian tails below exp(-40) of the peak that the tensor-core path drops, at most
+    # 3 channels x weight 2 x exp(-40) / (sqrt(2 pi) sigma) per mode triple
+    sig = 1e-7
+    r = both(sig)
+    cut = 6.0 * np.exp(-40.0) / (np.sqrt(2.0 * np.pi) * sig) * ctx.nq * 216
+    np.testing.assert_allclose(r["bf16x3"][1], r["fp64"][1], rtol=1e-10, atol=cut)
+    # new grid phonons (frequencies scaled by 1.05): the cached tiles must not be reused
+    ph = {k: np.array(v, copy=True) for k, v in st.ph.items()}
+    ph["omega"] = ph["omega"] * 1.05
+    ph["onebyomega"] = ph["onebyomega"] / 1.05
+    ctx.set_phonons(0, TEMPS, ph)
+    try:
+        r = both(SIGMA)
+        p64, p = r["fp64"][1], r["bf16x3"][1]
+        np.testing.assert_allclose(p, p64, rtol=1e-10, atol=1e-12 * np.abs(p64).max())
+    finally:
+        ctx.set_phonons(0, TEMPS, st.ph)
