@@ -9,9 +9,9 @@
 //   Y[mu][a s1][s2]      = sum_{N2 c} Z_q1[mu][a s1][N2 c] U_q2[mu][N2 c][s2]       (per pair: tensor cores)
 //   Phi[s0][s1][s2]      = sum_{mu a} m_mu^-1/2 e0(mu a, s0) Y[mu][a s1][s2]        (per pair: epilogue)
 // Pairs are grouped by q1, so one tile is up to 16 pairs sharing Z_q1: the MMA
-// computes Y^T for rows 8 pair + s2 at once, M = 128, N = 48 (36 used:
-// Re/Im of (a, s1)), K = 48 (Re/Im of (N2, c), 42 used), one accumulator per
-// basis atom mu in tensor memory.  The complex product is written as a real one:
+// computes Y^T for rows 8 pair + s2 at once, M = 128, N = 48 (8 columns per
+// s1: Re/Im of a and two zero rows, s1 in the order 0 3 1 4 2 5), K = 48 (Re/Im
+// of (N2, c), 42 used), one accumulator per basis atom mu in tensor memory.  The complex product is written as a real one:
 //   A[(pair, s2)][k] = [Re U_q2 | Im U_q2],   B[(re, a s1)][k] = [Re Z | -Im Z],
 //   B[(im, a s1)][k] = [Im Z | Re Z].
 // Precision: SPRING_BF16 rounds A and B to BF16 once; SPRING_BF16X3 splits each
@@ -42,7 +42,6 @@ namespace {
 constexpr int NMODE = 6;     // Ndof of the two-atom cell
 constexpr int KP = 48;       // padded K: Re/Im of (N2, c), 2 * 3 * Na3 <= 48
 constexpr int EPT = 16;      // pairs per tile: one 8-row core-matrix group each (rows 8e .. 8e+5 of 128)
-constexpr int BROWS = 36;    // used B rows
 constexpr uint32_t LBO = 128, SBO = (KP / 8) * 128;
 constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
 constexpr int AIMG = 8 * KP;              // bf16 elements of one (q, mu, hi/lo) A image: 8 rows x 48 (768 bytes)
@@ -125,8 +124,11 @@ __global__ void __launch_bounds__(128) k_tc_tab_a(int nq, int na, const double* 
 }
 
 // B table: per (q1, hi/lo, mu) the 4608-byte shared-memory image of the 48 x 48 B operand in the
-// canonical K-major layout: element (row n, k) at (n/8)*384 + (k/8)*64 + (n%8)*8 + k%8; rows 36-47
-// and the K padding are zero.  Hi parts first.  One CTA per (q1, mu).
+// canonical K-major layout: element (row n, k) at (n/8)*384 + (k/8)*64 + (n%8)*8 + k%8.  Row
+// n = 8 slot(s1) + 3 part + a (part 0: Re output, 1: Im output) with slot(s1) = 2 (s1 % 3) + s1 / 3,
+// so that the accumulator columns of s1 = g and g + 3 are the 16 columns from 16 g; rows 8 slot + 6,
+// 8 slot + 7 and the K padding are zero.  Hi parts first.  One CTA per (q1, mu).
+__host__ __device__ constexpr int b_slot(int s1) { return 2 * (s1 % 3) + s1 / 3; }
 __device__ __forceinline__ size_t bimg(int n, int k) {
     return (size_t)(n / 8) * 384 + (size_t)(k / 8) * 64 + (n % 8) * 8 + k % 8;
 }
@@ -145,7 +147,7 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
     __syncthreads();
     for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
         sU[i] = u_value(ph, q, mu, i / NMODE, i % NMODE, na, btyp, mrs, evg);
-    for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // rows 36-47 and the K padding stay zero
+    for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // padding rows and K stay zero
         reinterpret_cast<uint4*>(&img[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
     __syncthreads();
     // Z[(a, s1)][(N2, c)] = sum_{N1, b} FC3[mu][N1][N2][a b c] U[N1 b][s1]: one thread per
@@ -166,16 +168,16 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         }
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
-            const int r = al * NMODE + half * 3 + j;  // r = a*6 + s1
+            const int r = 8 * b_slot(half * 3 + j) + al, ri = r + 3;  // Re and Im output rows of (a, s1)
             __nv_bfloat16 h, l;
-            // row r (Re output): [Re Z | -Im Z];  row 18 + r (Im output): [Im Z | Re Z]
+            // row r (Re output): [Re Z | -Im Z];  row ri (Im output): [Im Z | Re Z]
             split_bf16(zr[j], h, l);
             img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
-            img[0][bimg(18 + r, KR + k2)] = h;     img[1][bimg(18 + r, KR + k2)] = l;
+            img[0][bimg(ri, KR + k2)] = h;         img[1][bimg(ri, KR + k2)] = l;
             split_bf16(-zi[j], h, l);
             img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
             split_bf16(zi[j], h, l);
-            img[0][bimg(18 + r, k2)] = h;          img[1][bimg(18 + r, k2)] = l;
+            img[0][bimg(ri, k2)] = h;              img[1][bimg(ri, k2)] = l;
         }
     }
     __syncthreads();
@@ -294,10 +296,9 @@ struct OpStage {
     int q1;                                   // q1 whose B images are resident
 };
 struct EpStage {
-    alignas(16) double w0[EPT][NMODE];  // omega of each pair's q0
-    alignas(16) double w2[EPT][NMODE];  // omega of each pair's q2
-    alignas(16) double w1[NMODE];       // omega of q1
-    int4 ent[EPT];                      // (q0, q2, weight, q0 is Gamma)
+    alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: (|w0 - w2|, w0 + w2) rounded from FP64
+    alignas(8) float w1s[NMODE];               // omega of q1 in FP32, s1 in slot order 0 3 1 4 2 5
+    int4 ent[EPT];                             // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
 };
 struct TcSmem {
@@ -308,7 +309,7 @@ struct TcSmem {
     int ihead;  // active triples written by this CTA
 };
 
-constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s0 each
+constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s1 each
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int TC_THREADS = EPI_THREADS + 96;  // warp 12: TMA copies; warp 13: MMA issue; warp 14: frequencies
 constexpr int TC_COLS = NEP * 128;
@@ -424,24 +425,29 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     } else if (warp == EPI_WARPS + 2) {
         // ------------------------------------------------------------ frequency warp
         // Epilogue stage j % 4 for tile j, after the epilogue of tile j-4 released it: entry
-        // records, the q1 and per-pair q0 / q2 omegas (loaded during the fill of j-1: lane p < 16
-        // holds pair p's q0 omegas, lane 16 + p pair p's q2 omegas, lane 0 also the q1 omegas).
-        // No warp barrier follows a load: each lane arrives on ready itself, after its own stores
-        // and before it issues new loads.
+        // records, the q1 omegas and, per pair, s2 and s0, the window values (|w0 - w2|, w0 + w2)
+        // of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16) .. 3 (l / 16) + 2 from
+        // omegas loaded during the fill of tile j-1; no warp barrier follows a load: each lane
+        // arrives on ready itself, after its own stores and before it issues new loads.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
         int4 entB = lane < recB.z ? entrec[recB.y + lane] : z4;
-        double2 wv[3], wq1[3];
-        const int pw = lane & 15;  // pair whose omegas this lane moves
+        double2 w0v[3], wq1[3];
+        double w2v[3];
+        const int pw = lane & 15, hw = lane >> 4;
         auto load_w = [&](const int4& ent, const int4& rec) {
+            const int q0 = __shfl_sync(0xffffffffu, ent.x, pw);
             const int q2 = __shfl_sync(0xffffffffu, ent.y, pw);
             if (pw < rec.z) {
-                const double2* src = reinterpret_cast<const double2*>(lane < 16 ? om0 + (size_t)ent.x * NMODE
-                                                                                 : omg + (size_t)q2 * NMODE);
-                wv[0] = src[0];
-                wv[1] = src[1];
-                wv[2] = src[2];
+                const double2* src = reinterpret_cast<const double2*>(om0 + (size_t)q0 * NMODE);
+                w0v[0] = src[0];
+                w0v[1] = src[1];
+                w0v[2] = src[2];
+                const double* s2p = omg + (size_t)q2 * NMODE + 3 * hw;
+                w2v[0] = s2p[0];
+                w2v[1] = s2p[1];
+                w2v[2] = s2p[2];
             }
             if (lane == 0) {
                 const double2* src = reinterpret_cast<const double2*>(omg + (size_t)rec.x * NMODE);
@@ -464,17 +470,21 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             if (lane == 0) {
                 E.ne = ne;
                 E.q1 = q1;
-                double2* d = reinterpret_cast<double2*>(E.w1);
-                d[0] = wq1[0];
-                d[1] = wq1[1];
-                d[2] = wq1[2];
+                const double w1[NMODE] = {wq1[0].x, wq1[0].y, wq1[1].x, wq1[1].y, wq1[2].x, wq1[2].y};
+#pragma unroll
+                for (int s1 = 0; s1 < NMODE; ++s1) E.w1s[b_slot(s1)] = (float)w1[s1];
             }
             if (lane < ne) E.ent[lane] = entA;
             if (pw < ne) {
-                double2* d = reinterpret_cast<double2*>(lane < 16 ? E.w0[pw] : E.w2[pw]);
-                d[0] = wv[0];
-                d[1] = wv[1];
-                d[2] = wv[2];
+                const double w0[NMODE] = {w0v[0].x, w0v[0].y, w0v[1].x, w0v[1].y, w0v[2].x, w0v[2].y};
+                float4* d = reinterpret_cast<float4*>(&E.cb[pw][3 * hw][0]);
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+#pragma unroll
+                    for (int s0 = 0; s0 < NMODE; s0 += 2)
+                        d[i * 3 + s0 / 2] = make_float4(fabsf((float)(w0[s0] - w2v[i])), (float)(w0[s0] + w2v[i]),
+                                                        fabsf((float)(w0[s0 + 1] - w2v[i])),
+                                                        (float)(w0[s0 + 1] + w2v[i]));
             }
             tc::mbar_arrive(tc::smem_u32(&S.ready[es]));  // each lane releases its own stores
             // loads for later fills
@@ -531,16 +541,24 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         __syncwarp();
     } else {
         // ------------------------------------------------------------ epilogue warps
-        const int wq = warp & 3, grp = warp >> 2;  // lane quarter, s0 pair (2 grp, 2 grp + 1)
+        // Warp (wq, g): TMEM lanes 32 wq .. 32 wq + 31 (pairs 4 wq .. 4 wq + 3, s2 = lane % 8), the
+        // q1 branches s1 = g and g + 3 (accumulator columns 16 g .. 16 g + 15 of each mu) and every
+        // s0; slot bit 6 sl + s0 stands for (s0, s1 = g + 3 sl).  One acoustic and one optical s1
+        // per warp keeps the active triples even across the three warps of a lane quarter.
+        const int wq = warp & 3, g = warp >> 2;
         const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
         TcItem* region = items + (size_t)blockIdx.x * a.cap;
-        // (s0, s1) slots allowed by the mode ranges and the Gamma acoustic rule (q1 = Gamma: amask_g)
-        unsigned s1m = 0u;
+        // slots allowed by the mode ranges, and by the Gamma acoustic rule when q1 = Gamma (amask_g:
+        // s1 = g < 3 drops out)
+        unsigned amask_n = 0u;
 #pragma unroll
-        for (int s1 = 0; s1 < NMODE; ++s1) s1m |= (s1 >= a.lo[1] && s1 <= a.hi[1]) ? (1u << s1) : 0u;
-        const unsigned s0m = ((grp * 2 >= a.lo[0] && grp * 2 <= a.hi[0]) ? 0x3fu : 0u) |
-                             ((grp * 2 + 1 >= a.lo[0] && grp * 2 + 1 <= a.hi[0]) ? 0xfc0u : 0u);
-        const unsigned amask_n = (s1m | (s1m << NMODE)) & s0m, amask_g = amask_n & ~0x1c7u;
+        for (int sl = 0; sl < 2; ++sl) {
+            const int s1 = g + 3 * sl;
+#pragma unroll
+            for (int s0 = 0; s0 < NMODE; ++s0)
+                if (s1 >= a.lo[1] && s1 <= a.hi[1] && s0 >= a.lo[0] && s0 <= a.hi[0]) amask_n |= 1u << (6 * sl + s0);
+        }
+        const unsigned amask_g = amask_n & ~0x3fu;
         for (int j = 0; j < nt; ++j) {
             const int es = j % NEP, u = j / NEP;
             const EpStage& E = S.ep[es];
@@ -551,38 +569,27 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 break;
             }
             tc::fence_after_sync();
-            float y[2][BROWS];  // this row's Y: (Re, Im) x (a, s1) per mu
-            {
-                const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(es * 128);
-                tc::tmem_ld16(ta, y[0]);
-                tc::tmem_ld16(ta + 16, y[0] + 16);
-                tc::tmem_ld4(ta + 32, y[0] + 32);
-                tc::tmem_ld16(ta + 64, y[1]);
-                tc::tmem_ld16(ta + 80, y[1] + 16);
-                tc::tmem_ld4(ta + 96, y[1] + 32);
-            }
+            float y[2][16];  // per mu, this row's Y for s1 = g (columns 0-7) and g + 3 (8-15): Re a, Im a, 0, 0
+            const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(es * 128 + 16 * g);
+            tc::tmem_ld16(ta, y[0]);
+            tc::tmem_ld16(ta + 64, y[1]);
             // shared-memory reads that do not depend on the accumulator, issued before its wait
             const int ne = E.ne, q1 = E.q1;
             const int4 en = E.ent[e];
-            const double w2 = E.w2[e][s2c];
-            const double w0a = E.w0[e][grp * 2], w0b = E.w0[e][grp * 2 + 1];
-            float w1f[NMODE];
-#pragma unroll
-            for (int s1 = 0; s1 < NMODE; ++s1) w1f[s1] = (float)E.w1[s1];
+            const float4* cbp = reinterpret_cast<const float4*>(&E.cb[e][s2c][0]);
+            const float4 c01 = cbp[0], c23 = cbp[1], c45 = cbp[2];
+            const float2 w1 = *reinterpret_cast<const float2*>(&E.w1s[2 * g]);
             tc::tmem_ld_wait();
             const bool row_on = s2 < NMODE && e < ne && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
             const unsigned amask = q1 == 0 ? amask_g : amask_n;
-            // FP32 screen: bit 6*jj + s1 marks (s0 = 2 grp + jj, s1) inside the delta window
-            // |w0 - w2 -+ w1| < R  or  |w0 + w2 - w1| < R; the first pair is ||w1| - |w0 - w2|| < R.
             unsigned act = 0u;
             if (row_on) {
+                const float cc[NMODE] = {c01.x, c01.z, c23.x, c23.z, c45.x, c45.z};
+                const float bb[NMODE] = {c01.y, c01.w, c23.y, c23.w, c45.y, c45.w};
 #pragma unroll
-                for (int jj = 0; jj < 2; ++jj) {
-                    const double w0 = jj ? w0b : w0a;
-                    const float c = fabsf((float)(w0 - w2)), bf = (float)(w0 + w2);
-#pragma unroll
-                    for (int s1 = 0; s1 < NMODE; ++s1)
-                        act |= tc_window(c, bf, w1f[s1], a.rf) ? (1u << (jj * NMODE + s1)) : 0u;
+                for (int s0 = 0; s0 < NMODE; ++s0) {
+                    act |= tc_window(cc[s0], bb[s0], w1.x, a.rf) ? (1u << s0) : 0u;
+                    act |= tc_window(cc[s0], bb[s0], w1.y, a.rf) ? (1u << (6 + s0)) : 0u;
                 }
                 act &= amask;
             }
@@ -599,24 +606,30 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 const unsigned lt = (1u << lane) - 1u;
                 const unsigned any = __reduce_or_sync(0xffffffffu, act);
                 const int kw = en.z == 2 ? (1 << 30) : 0;
+                const int k2 = en.y * NMODE + s2;
 #pragma unroll
-                for (int jj = 0; jj < 2; ++jj) {
-                    const int s0 = grp * 2 + jj;
-                    const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
-#pragma unroll
-                    for (int s1 = 0; s1 < NMODE; ++s1) {
-                        if (!((any >> (jj * NMODE + s1)) & 1u)) continue;
-                        const bool has = (act >> (jj * NMODE + s1)) & 1u;
-                        const unsigned m = __ballot_sync(0xffffffffu, has);
-                        const int pos = base + __popc(m & lt);
+                for (int sl = 0; sl < 2; ++sl) {
+                    const int b = 8 * sl, k1 = q1 * NMODE + g + 3 * sl;
+                    // item (Re, Im) Y[mu][a], k = mu * 3 + a
+                    const float4 v0 = make_float4(y[0][b], y[0][b + 1], y[0][b + 2], y[1][b]);
+                    const float4 v1 = make_float4(y[1][b + 1], y[1][b + 2], y[0][b + 3], y[0][b + 4]);
+                    const float4 v2 = make_float4(y[0][b + 5], y[1][b + 3], y[1][b + 4], y[1][b + 5]);
+                    unsigned m = (any >> (6 * sl)) & 0x3fu;  // warp-uniform
+                    while (m != 0u) {
+                        const int s0 = __ffs(m) - 1;
+                        m &= m - 1u;
+                        const bool has = (act >> (6 * sl + s0)) & 1u;
+                        const unsigned bm = __ballot_sync(0xffffffffu, has);
+                        const int pos = base + __popc(bm & lt);
                         if (has && pos < a.cap) {
                             float4* dst = reinterpret_cast<float4*>(region + pos);
-                            dst[0] = make_float4(y[0][s1], y[0][6 + s1], y[0][12 + s1], y[1][s1]);
-                            dst[1] = make_float4(y[1][6 + s1], y[1][12 + s1], y[0][18 + s1], y[0][24 + s1]);
-                            dst[2] = make_float4(y[0][30 + s1], y[1][18 + s1], y[1][24 + s1], y[1][30 + s1]);
-                            reinterpret_cast<int4*>(dst)[3] = make_int4(k0, q1 * NMODE + s1, en.y * NMODE + s2, 0);
+                            dst[0] = v0;
+                            dst[1] = v1;
+                            dst[2] = v2;
+                            const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
+                            reinterpret_cast<int4*>(dst)[3] = make_int4(k0, k1, k2, 0);
                         }
-                        base += __popc(m);
+                        base += __popc(bm);
                     }
                 }
             }
