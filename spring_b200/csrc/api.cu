@@ -539,7 +539,7 @@ int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_
     SPRING_CHECK(spring_synchronize(c));
     c->mesh_set = true;
     c->mesh_zc = zero_centered != 0;
-    c->tr_nq = -1;  // time-reversal lists belong to the previous mesh
+    // the time-reversal lists depend only on the mesh dimensions (fixed per context): kept
     for (int k = 0; k < 3; ++k) c->mesh_shift[k] = sh[k];
     c->ps_irr.done = false;
     c->ps_tr.done = false;
@@ -592,18 +592,23 @@ int spring_find_irr_q(spring_ctx* c, int nrot, const int* rot, int time_rev, int
     if (rc == SPRING_OK) rc = d2h(c, map.data(), d_map.p, sizeof(int) * c->nq, "irreducible map");
     if (rc == SPRING_OK) rc = d2h(c, qint.data(), c->d_qint.p, sizeof(int) * c->nq * 3, "q_pnt_int");
     if (rc != SPRING_OK) return rc;
-    // unique_sort + FindPositionAndMultiplicity (Helper_m.f90:510-594)
-    std::vector<int> uniq(map);
-    std::sort(uniq.begin(), uniq.end());
-    uniq.erase(std::unique(uniq.begin(), uniq.end()), uniq.end());
-    const int nq0 = (int)uniq.size();
-    std::vector<int> irr((size_t)nq0 * 3), ps(c->nq), mu(nq0, 0);
-    for (int k = 0; k < nq0; ++k)
-        for (int d = 0; d < 3; ++d) irr[3 * k + d] = qint[3 * (size_t)uniq[k] + d];
+    // unique_sort + FindPositionAndMultiplicity (Helper_m.f90:510-594): the representatives are grid
+    // indices, so their ascending order and ranks come from one pass over a flag array.
+    std::vector<int> rank(c->nq, -1);
     for (int i = 0; i < c->nq; ++i) {
-        int k = (int)(std::lower_bound(uniq.begin(), uniq.end(), map[i]) - uniq.begin());
-        ps[i] = k + 1;
-        mu[k] += 1;
+        if (map[i] < 0 || map[i] >= c->nq) return fail(c, SPRING_ERR_CUDA, "irreducible map out of range");
+        rank[map[i]] = 0;
+    }
+    int nq0 = 0;
+    for (int g = 0; g < c->nq; ++g)
+        if (rank[g] == 0) rank[g] = ++nq0;  // 1-based position
+    std::vector<int> irr((size_t)nq0 * 3), ps(c->nq), mu(nq0, 0);
+    for (int g = 0; g < c->nq; ++g)
+        if (rank[g] > 0)
+            for (int d = 0; d < 3; ++d) irr[3 * (rank[g] - 1) + d] = qint[3 * (size_t)g + d];
+    for (int i = 0; i < c->nq; ++i) {
+        ps[i] = rank[map[i]];
+        mu[ps[i] - 1] += 1;
     }
     SPRING_CHECK(install_irr(c, nq0, irr.data(), ps.data(), mu.data()));
     if (nq0_out) *nq0_out = nq0;

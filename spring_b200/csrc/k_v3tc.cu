@@ -57,11 +57,13 @@ __device__ __forceinline__ void split_bf16(double x, __nv_bfloat16& hi, __nv_bfl
 }
 
 // FP32 delta-window test of one mode triple, shared by the pair pre-screen and the tensor-core
-// pass so that both decide alike: with c = |w0 - w2| and b = w0 + w2 (rounded from FP64), the
-// triple is kept when ||w1| - c| < R or |b - w1| < R, R covering every delta weight above exp(-40)
-// of its peak.
-__device__ __forceinline__ bool tc_window(float c, float b, float w1, float rf) {
-    return fabsf(fabsf(w1) - c) < rf || fabsf(b - w1) < rf;
+// pass so that both decide alike.  From the FP32 omegas, (d, b) = (w0 - w2, w0 + w2) of (s0, s2)
+// (tc_window_vals); the triple is kept when ||w1| - |d|| < R or |b - w1| < R.  R is the half-width
+// where a delta weight falls to exp(-40) of its peak, times 1.0001, plus 1e-3 rad/ps: far above the
+// FP32 rounding of the omegas (~1e-5 rad/ps), so every triple with a weight above the cut passes.
+__device__ __forceinline__ float2 tc_window_vals(float w0, float w2) { return make_float2(w0 - w2, w0 + w2); }
+__device__ __forceinline__ bool tc_window(float d, float b, float w1, float rf) {
+    return fabsf(fabsf(w1) - fabsf(d)) < rf || fabsf(b - w1) < rf;
 }
 
 // Phases e^{i q.R_{mu N}} of one grid point and basis atom, N < na, into ph[N] (threads 0..na-1).
@@ -235,21 +237,25 @@ __global__ void k_tc_keys(int n, int p0, int nq, const int2* __restrict__ pairs,
                           int* __restrict__ keys, int* __restrict__ vals, int* __restrict__ cnt) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int2 pq = pairs[p0 + i];
-        const double* w0 = om0 + (size_t)pair_q0[p0 + i] * NMODE;
-        const double* w2 = omg + (size_t)pq.y * NMODE;
-        float w1[NMODE];
+        const double* w0d = om0 + (size_t)pair_q0[p0 + i] * NMODE;
+        const double* w1d = omg + (size_t)pq.x * NMODE;
+        const double* w2d = omg + (size_t)pq.y * NMODE;
+        float w0[NMODE], w1[NMODE], w2[NMODE];
 #pragma unroll
-        for (int s1 = 0; s1 < NMODE; ++s1) w1[s1] = (float)omg[(size_t)pq.x * NMODE + s1];
-        bool any = false;
-        for (int s0 = 0; s0 < NMODE && !any; ++s0) {
-            const double a0 = w0[s0];
-            for (int s2 = 0; s2 < NMODE && !any; ++s2) {
-                const double a2 = w2[s2];
-                const float c = fabsf((float)(a0 - a2)), b = (float)(a0 + a2);
-#pragma unroll
-                for (int s1 = 0; s1 < NMODE; ++s1) any |= tc_window(c, b, w1[s1], rf);
-            }
+        for (int s = 0; s < NMODE; ++s) {
+            w0[s] = (float)w0d[s];
+            w1[s] = (float)w1d[s];
+            w2[s] = (float)w2d[s];
         }
+        bool any = false;
+#pragma unroll
+        for (int s0 = 0; s0 < NMODE; ++s0)
+#pragma unroll
+            for (int s2 = 0; s2 < NMODE; ++s2) {
+                const float2 v = tc_window_vals(w0[s0], w2[s2]);
+#pragma unroll
+                for (int s1 = 0; s1 < NMODE; ++s1) any |= tc_window(v.x, v.y, w1[s1], rf);
+            }
         keys[i] = any ? pq.x : nq;
         vals[i] = p0 + i;
         if (any) atomicAdd(&cnt[pq.x], 1);
@@ -296,7 +302,7 @@ struct OpStage {
     int q1;                                   // q1 whose B images are resident
 };
 struct EpStage {
-    alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: (|w0 - w2|, w0 + w2) rounded from FP64
+    alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: tc_window_vals of the FP32 omegas
     alignas(8) float w1s[NMODE];               // omega of q1 in FP32, s1 in slot order 0 3 1 4 2 5
     int4 ent[EPT];                             // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
@@ -306,7 +312,6 @@ struct TcSmem {
     EpStage ep[NEP];
     alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP];
     uint32_t tslot;
-    int ihead;  // active triples written by this CTA
 };
 
 constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s1 each
@@ -330,7 +335,7 @@ static_assert(sizeof(TcItem) == 64, "item");
 // ready[j % 4].  The MMA warp issues tile j's MMAs into the accumulator of epilogue stage j % 4 and
 // commits them to full[j % 4] and opfree[j % 2].  Each epilogue warp works on its own: it reads its
 // 32 accumulator rows, screens its 12 mode triples per row in FP32 against the delta window,
-// releases the stage, and appends the active triples (with their Y values) to this CTA's region of
+// releases the stage, and appends the active triples (with their Y values) to its own region of
 // the item list.  The FP64 part runs in k_v3tc_eval.
 template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
@@ -360,7 +365,6 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_WARPS);
         }
-        S.ihead = 0;
         tc::mbar_fence_init();
     }
     if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), TC_COLS);
@@ -425,7 +429,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     } else if (warp == EPI_WARPS + 2) {
         // ------------------------------------------------------------ frequency warp
         // Epilogue stage j % 4 for tile j, after the epilogue of tile j-4 released it: entry
-        // records, the q1 omegas and, per pair, s2 and s0, the window values (|w0 - w2|, w0 + w2)
+        // records, the q1 omegas and, per pair, s2 and s0, the window values (w0 - w2, w0 + w2)
         // of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16) .. 3 (l / 16) + 2 from
         // omegas loaded during the fill of tile j-1; no warp barrier follows a load: each lane
         // arrives on ready itself, after its own stores and before it issues new loads.
@@ -476,15 +480,18 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
             if (lane < ne) E.ent[lane] = entA;
             if (pw < ne) {
-                const double w0[NMODE] = {w0v[0].x, w0v[0].y, w0v[1].x, w0v[1].y, w0v[2].x, w0v[2].y};
+                const float w0[NMODE] = {(float)w0v[0].x, (float)w0v[0].y, (float)w0v[1].x,
+                                         (float)w0v[1].y, (float)w0v[2].x, (float)w0v[2].y};
                 float4* d = reinterpret_cast<float4*>(&E.cb[pw][3 * hw][0]);
 #pragma unroll
-                for (int i = 0; i < 3; ++i)
+                for (int i = 0; i < 3; ++i) {
+                    const float w2 = (float)w2v[i];
 #pragma unroll
-                    for (int s0 = 0; s0 < NMODE; s0 += 2)
-                        d[i * 3 + s0 / 2] = make_float4(fabsf((float)(w0[s0] - w2v[i])), (float)(w0[s0] + w2v[i]),
-                                                        fabsf((float)(w0[s0 + 1] - w2v[i])),
-                                                        (float)(w0[s0 + 1] + w2v[i]));
+                    for (int s0 = 0; s0 < NMODE; s0 += 2) {
+                        const float2 u = tc_window_vals(w0[s0], w2), v = tc_window_vals(w0[s0 + 1], w2);
+                        d[i * 3 + s0 / 2] = make_float4(u.x, u.y, v.x, v.y);
+                    }
+                }
             }
             tc::mbar_arrive(tc::smem_u32(&S.ready[es]));  // each lane releases its own stores
             // loads for later fills
@@ -547,7 +554,9 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         // per warp keeps the active triples even across the three warps of a lane quarter.
         const int wq = warp & 3, g = warp >> 2;
         const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
-        TcItem* region = items + (size_t)blockIdx.x * a.cap;
+        // this warp's region of the item list and its fill
+        TcItem* region = items + ((size_t)blockIdx.x * EPI_WARPS + warp) * a.cap;
+        int base = 0;
         // slots allowed by the mode ranges, and by the Gamma acoustic rule when q1 = Gamma (amask_g:
         // s1 = g < 3 drops out)
         unsigned amask_n = 0u;
@@ -593,35 +602,36 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 }
                 act &= amask;
             }
-            // Reserve room in the CTA's region, release the stage (every read of it is done), then
-            // append the active triples slot by slot in lane order.
-            const int tot = __reduce_add_sync(0xffffffffu, (unsigned)__popc(act));
-            int base = 0;
-            if (lane == 0 && tot > 0) base = atomicAdd(&S.ihead, tot);
-            base = __shfl_sync(0xffffffffu, base, 0);
+            // Positions in this warp's region (exclusive prefix of the lanes' counts), release the
+            // stage (every read of it is done), then each lane writes its own active triples.
+            const int cnt = __popc(act);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            int pos = base + incl - cnt;
+            base += __shfl_sync(0xffffffffu, incl, 31);
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
-            if (tot > 0) {
-                const unsigned lt = (1u << lane) - 1u;
-                const unsigned any = __reduce_or_sync(0xffffffffu, act);
+            if (cnt > 0) {
                 const int kw = en.z == 2 ? (1 << 30) : 0;
                 const int k2 = en.y * NMODE + s2;
 #pragma unroll
                 for (int sl = 0; sl < 2; ++sl) {
+                    unsigned m = (act >> (6 * sl)) & 0x3fu;
+                    if (m == 0u) continue;
                     const int b = 8 * sl, k1 = q1 * NMODE + g + 3 * sl;
                     // item (Re, Im) Y[mu][a], k = mu * 3 + a
                     const float4 v0 = make_float4(y[0][b], y[0][b + 1], y[0][b + 2], y[1][b]);
                     const float4 v1 = make_float4(y[1][b + 1], y[1][b + 2], y[0][b + 3], y[0][b + 4]);
                     const float4 v2 = make_float4(y[0][b + 5], y[1][b + 3], y[1][b + 4], y[1][b + 5]);
-                    unsigned m = (any >> (6 * sl)) & 0x3fu;  // warp-uniform
-                    while (m != 0u) {
+                    do {
                         const int s0 = __ffs(m) - 1;
                         m &= m - 1u;
-                        const bool has = (act >> (6 * sl + s0)) & 1u;
-                        const unsigned bm = __ballot_sync(0xffffffffu, has);
-                        const int pos = base + __popc(bm & lt);
-                        if (has && pos < a.cap) {
+                        if (pos < a.cap) {
                             float4* dst = reinterpret_cast<float4*>(region + pos);
                             dst[0] = v0;
                             dst[1] = v1;
@@ -629,17 +639,17 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                             const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
                             reinterpret_cast<int4*>(dst)[3] = make_int4(k0, k1, k2, 0);
                         }
-                        base += __popc(bm);
-                    }
+                        ++pos;
+                    } while (m != 0u);
                 }
             }
         }
+        if (lane == 0) counts[blockIdx.x * EPI_WARPS + warp] = base;
     }
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_dealloc(tm, TC_COLS);
-    if (tid == 0) counts[blockIdx.x] = S.ihead;
 }
 
 // One active triple whose item and records are already in registers.
@@ -760,7 +770,7 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
     k_v3tc<SPLIT><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
         a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p, c->ph_grid.omega.p, items,
-        c->d_tc_cnt_cta.p, c->d_tc_cnt_cta.p + c->tc_grid);
+        c->d_tc_cnt_cta.p, c->d_tc_cnt_cta.p + c->tc_grid * EPI_WARPS);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -905,35 +915,36 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const int ctas = std::max(1, std::min(a.ntiles, sms));
     a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
     c->tc_grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
-    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, c->tc_grid + 1, "V3 item counts"));  // + the status word
-    // Item list: one region per CTA, first sized for 8 % of the CTA's mode triples (about 3 % of the
-    // triples of the pairs left after the pre-screen pass the screen on meshes from 8^3 to 24^3),
-    // regrown to what the pass reports if that overflows.
-    const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE;
-    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 12, 1024);
+    const int nreg = c->tc_grid * EPI_WARPS;  // item regions: one per epilogue warp
+    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, nreg + 1, "V3 item counts"));  // + the status word
+    // Item list: one region per epilogue warp, first sized for 8 % of its share of the CTA's mode
+    // triples (about 3 % of the triples of the pairs left after the pre-screen pass the screen on
+    // meshes from 8^3 to 24^3), regrown to what the pass reports if that overflows.
+    const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE / EPI_WARPS;
+    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 12, 256);
     const bool split = c->precision == SPRING_BF16X3;
-    std::vector<int> cnt(c->tc_grid + 1);
+    std::vector<int> cnt(nreg + 1);
     int maxcnt = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         cap = std::min<long long>(cap, triples);
         a.cap = (int)cap;
-        SPRING_CHECK(dalloc(c, c->d_tc_items, (size_t)c->tc_grid * cap * (sizeof(TcItem) / sizeof(float4)), "V3 items"));
+        SPRING_CHECK(dalloc(c, c->d_tc_items, (size_t)nreg * cap * (sizeof(TcItem) / sizeof(float4)), "V3 items"));
         TcItem* items = reinterpret_cast<TcItem*>(c->d_tc_items.p);
-        SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p + c->tc_grid, sizeof(int), "V3 status"));
+        SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p + nreg, sizeof(int), "V3 status"));
         SPRING_CHECK(split ? launch_tc<true>(c, a, items) : launch_tc<false>(c, a, items));
-        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * (c->tc_grid + 1), "V3 item counts"));
-        const int herr = cnt[c->tc_grid];
+        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * (nreg + 1), "V3 item counts"));
+        const int herr = cnt[nreg];
         if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
         if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
-        maxcnt = *std::max_element(cnt.begin(), cnt.begin() + c->tc_grid);
+        maxcnt = *std::max_element(cnt.begin(), cnt.begin() + nreg);
         if (maxcnt <= cap) break;
-        cap = (long long)(maxcnt * 1.25) + 1024;  // the pass only wrote what fit; run it again
+        cap = (long long)(maxcnt * 1.25) + 256;  // the pass only wrote what fit; run it again
     }
     if (maxcnt > cap) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: item list overflow");
     c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
     if (maxcnt == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
-    const dim3 grid(c->tc_grid, std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads))));
+    const dim3 grid(nreg, std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads))));
     k_v3tc_eval<<<grid, threads, 0, c->stream>>>(
         reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2,
         os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p),

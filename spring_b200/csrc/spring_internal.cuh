@@ -188,7 +188,7 @@ struct spring_ctx {
     spring::DBuf<int> d_scr_sum;       // one-int readback scratch
     spring::DBuf<int> d_scr_rot, d_scr_map;  // spring_find_irr_q scratch: rotations, orbit map
     int tc_grid = 0;
-    double tc_cap_frac = 0.0;          // item region size as a fraction of the CTA's triples
+    double tc_cap_frac = 0.0;          // item region size as a fraction of its share of the triples
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
