@@ -15,6 +15,7 @@
 //      the same omega, 1/omega and nBE, and v(-q) = -v(q).  The irreducible
 //      points run in the same launch.
 // FP64 ALU bound (~10 n^3 flops per sweep).
+#include <algorithm>
 #include <vector>
 
 #include "spring_internal.cuh"
@@ -264,6 +265,227 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, PhSet SA, const in
     }
 }
 
+// Two-atom cells (n = 6): eight lanes per q-point, four points per one-warp block, each group
+// with its own shared-memory state (16 KB per block: 14 blocks, 56 points, per SM).  The same steps as k_phonons (phases once
+// per (mu, N), then D and dD/dq in reference neighbour order; the same round-robin Jacobi rotations
+// and stopping rules; ordering, velocities, nBE), with every control decision warp-uniform: the
+// groups synchronise with full-warp barriers, a converged or idle group only skips work, and the
+// sweep loop ends when every group of the warp has converged.
+constexpr int PH6_LANES = 8, PH6_PTS = 4, PH6_NA2 = 32;
+struct Ph6 {
+    double2 A[36], V[36], dD[3 * 36];
+    double2 ph[2 * PH6_NA2];  // e^{i q.R} per (mu, N)
+    double2 rotE[3];
+    double rotC[3], rotS[3], lam[6];
+    int rotP[3], rotQ[3], rank[6], nrot;
+};
+
+__global__ void __launch_bounds__(32) k_phonons_n6(PhArgs a, PhSet SA, const int* __restrict__ list_a, int n_a,
+                                                  PhSet SB, int n_b, const double* __restrict__ fc2,
+                                                  const int* __restrict__ idx, const int* __restrict__ num,
+                                                  const double* __restrict__ mrs, const double* __restrict__ temps) {
+    constexpr int n = 6, m = 6, L = PH6_LANES;
+    constexpr unsigned FULL = 0xffffffffu;
+    __shared__ Ph6 sh[PH6_PTS];
+    const int gi = threadIdx.x / L, gl = threadIdx.x % L;
+    Ph6& S = sh[gi];
+    const int total = n_a + n_b;
+    for (int base = blockIdx.x * PH6_PTS; base < total; base += gridDim.x * PH6_PTS) {
+        const int item = base + gi;
+        const bool act = item < total;
+        const bool in_a = item < n_a;
+        const PhSet& P = in_a ? SA : SB;
+        const int q = act ? (in_a ? (list_a ? list_a[item] : item) : item - n_a) : 0;
+        double qx = 0.0, qy = 0.0, qz = 0.0;
+        if (act) {
+            qx = P.qpts[3 * q];
+            qy = P.qpts[3 * q + 1];
+            qz = P.qpts[3 * q + 2];
+            for (int w = gl; w < 4 * 36; w += L) {
+                if (w < 36) S.A[w] = make_double2(0.0, 0.0);
+                else S.dD[w - 36] = make_double2(0.0, 0.0);
+            }
+            for (int w = gl; w < 36; w += L) S.V[w] = make_double2(w % 7 == 0 ? 1.0 : 0.0, 0.0);
+            for (int w = gl; w < 2 * a.na2; w += L) {
+                const int mu = w / a.na2, N = w % a.na2;
+                if (N < num[mu]) {
+                    const int* e = idx + 4 * (N + a.na2 * mu);
+                    double R[3];
+                    for (int r = 0; r < 3; ++r)
+                        R[r] = a.latvec[r] * e[0] + a.latvec[r + 3] * e[1] + a.latvec[r + 6] * e[2];
+                    const double qr = qx * R[0] + qy * R[1] + qz * R[2];
+                    double sn, cs;
+                    sincos(qr, &sn, &cs);
+                    S.ph[mu * PH6_NA2 + N] = make_double2(cs, sn);
+                }
+            }
+        }
+        __syncwarp();
+        // D(q), dD/dq: lane per (mu, alpha, beta); neighbours in reference order
+        if (act)
+            for (int w = gl; w < 18; w += L) {
+                const int mu = w / 9, al = (w / 3) % 3, be = w % 3;
+                const int row = 3 * mu + al;
+                for (int N = 0; N < num[mu]; ++N) {
+                    const int* e = idx + 4 * (N + a.na2 * mu);
+                    const int nu = e[3] - 1;
+                    double R[3];
+                    for (int r = 0; r < 3; ++r)
+                        R[r] = a.latvec[r] * e[0] + a.latvec[r + 3] * e[1] + a.latvec[r + 6] * e[2];
+                    const double2 pe = S.ph[mu * PH6_NA2 + N];
+                    const double f = fc2[((mu * a.na2 + N) * 3 + al) * 3 + be];  // fC(1,be,al,N,mu)
+                    const double mf = mrs[mu] * mrs[nu];
+                    const int col = 3 * nu + be;
+                    const double2 t = make_double2(f * pe.x * mf, f * pe.y * mf);
+                    S.A[row * n + col] = cadd(S.A[row * n + col], t);
+                    for (int k = 0; k < 3; ++k)  // (i R_k) * t
+                        S.dD[(k * n + row) * n + col] =
+                            cadd(S.dD[(k * n + row) * n + col], make_double2(-t.y * R[k], t.x * R[k]));
+                }
+            }
+        __syncwarp();
+
+        // --- cyclic complex Jacobi, one group per point
+        bool gdone = !act;
+        for (int sweep = 0; sweep < MAX_SWEEPS; ++sweep) {
+            double off = 0.0, dg = 0.0;
+            if (!gdone)
+                for (int w = gl; w < 36; w += L) {
+                    const int i = w / n, j = w % n;
+                    const double2 z = S.A[w];
+                    if (i == j) dg += z.x * z.x;
+                    else if (j > i) off += z.x * z.x + z.y * z.y;
+                }
+            for (int o = L / 2; o > 0; o >>= 1) {  // within the group; every lane gets the same sums
+                off += __shfl_xor_sync(FULL, off, o);
+                dg += __shfl_xor_sync(FULL, dg, o);
+            }
+            if (!gdone && (off <= 1e-30 * dg || off == 0.0)) gdone = true;
+            if (__all_sync(FULL, gdone)) break;
+            if (gl == 0) S.nrot = 0;
+            __syncwarp();
+            for (int r = 0; r < m - 1; ++r) {
+                if (!gdone && gl < m / 2) {
+                    const int k = gl;
+                    int p, qq;
+                    if (k == 0) { p = r; qq = m - 1; }
+                    else { p = (r + k) % (m - 1); qq = (r - k + (m - 1)) % (m - 1); }
+                    if (p > qq) { const int t = p; p = qq; qq = t; }
+                    double c = 1.0, sn = 0.0;
+                    double2 ee = make_double2(1.0, 0.0);
+                    bool valid = false;
+                    const double2 z = S.A[p * n + qq];
+                    const double rr = hypot(z.x, z.y);
+                    if (rr > 1e-300 && rr > 1e-16 * sqrt(fabs(S.A[p * n + p].x * S.A[qq * n + qq].x))) {
+                        const double app = S.A[p * n + p].x, aqq = S.A[qq * n + qq].x;
+                        const double tau = (aqq - app) / (2.0 * rr);
+                        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+                        c = 1.0 / sqrt(1.0 + t * t);
+                        sn = t * c;
+                        ee = make_double2(z.x / rr, z.y / rr);
+                        valid = true;
+                        atomicAdd(&S.nrot, 1);
+                    }
+                    S.rotP[k] = valid ? p : -1;
+                    S.rotQ[k] = qq;
+                    S.rotC[k] = c;
+                    S.rotS[k] = sn;
+                    S.rotE[k] = ee;
+                }
+                __syncwarp();
+                if (!gdone)  // A <- A U and V <- V U (columns p, q of every row)
+                    for (int w = gl; w < 2 * n * (m / 2); w += L) {
+                        const int k = w % (m / 2), i = (w / (m / 2)) % n;
+                        double2* M = (w / (m / 2)) >= n ? S.V : S.A;
+                        const int p = S.rotP[k];
+                        if (p < 0) continue;
+                        const int qq = S.rotQ[k];
+                        const double c = S.rotC[k], sn = S.rotS[k];
+                        const double2 eb = conj2(S.rotE[k]);
+                        const double2 x = M[i * n + p], y = M[i * n + qq];
+                        const double2 ey = cmul(eb, y);
+                        M[i * n + p] = make_double2(c * x.x - sn * ey.x, c * x.y - sn * ey.y);
+                        M[i * n + qq] = make_double2(sn * x.x + c * ey.x, sn * x.y + c * ey.y);
+                    }
+                __syncwarp();
+                if (!gdone)  // A <- U^H A (rows p, q of every column)
+                    for (int w = gl; w < n * (m / 2); w += L) {
+                        const int k = w % (m / 2), j = w / (m / 2);
+                        const int p = S.rotP[k];
+                        if (p < 0) continue;
+                        const int qq = S.rotQ[k];
+                        const double c = S.rotC[k], sn = S.rotS[k];
+                        const double2 e = S.rotE[k];
+                        const double2 x = S.A[p * n + j], y = S.A[qq * n + j];
+                        const double2 ey = cmul(e, y);
+                        S.A[p * n + j] = make_double2(c * x.x - sn * ey.x, c * x.y - sn * ey.y);
+                        S.A[qq * n + j] = make_double2(sn * x.x + c * ey.x, sn * x.y + c * ey.y);
+                    }
+                __syncwarp();
+                if (!gdone && gl < m / 2) {
+                    const int p = S.rotP[gl];
+                    if (p >= 0) {
+                        const int qq = S.rotQ[gl];
+                        S.A[p * n + qq] = make_double2(0.0, 0.0);
+                        S.A[qq * n + p] = make_double2(0.0, 0.0);
+                        S.A[p * n + p].y = 0.0;
+                        S.A[qq * n + qq].y = 0.0;
+                    }
+                }
+                __syncwarp();
+            }
+            if (!gdone && S.nrot == 0) gdone = true;  // nothing above the threshold: converged
+            __syncwarp();
+        }
+        // --- ascending order (stable): rank of each eigenvalue
+        if (act && gl < n) {
+            const double li = S.A[gl * n + gl].x;
+            int rk = 0;
+            for (int j = 0; j < n; ++j) {
+                const double lj = S.A[j * n + j].x;
+                rk += (lj < li) || (lj == li && j < gl);
+            }
+            S.rank[gl] = rk;
+            S.lam[rk] = li;
+        }
+        __syncwarp();
+        if (act) {
+            const int nq = P.nq;
+            const bool gamma = fabs(qx) < CMP_PREC && fabs(qy) < CMP_PREC && fabs(qz) < CMP_PREC;
+            for (int w = gl; w < 36; w += L) {
+                const int col = w / n, row = w % n;
+                P.evec[((size_t)q * n + S.rank[col]) * n + row] = S.V[row * n + col];
+            }
+            if (gl < n) {
+                const int col = gl, s = S.rank[col];
+                const double lv = S.A[col * n + col].x;
+                double W = sqrt(fabs(lv));
+                if (fabs(lv) > EPS_F32 && lv < 0.0) W = -W;
+                P.omega[(size_t)q * n + s] = W * a.wTHz;
+                const bool zero_mode = gamma && s < 3;
+                double v3[3] = {0.0, 0.0, 0.0};
+                if (!zero_mode) {
+                    for (int k = 0; k < 3; ++k) {
+                        double2 acc = make_double2(0.0, 0.0);
+                        for (int i = 0; i < n; ++i) {
+                            double2 t = make_double2(0.0, 0.0);
+                            for (int j = 0; j < n; ++j) t = cadd(t, cmul(S.dD[(k * n + i) * n + j], S.V[j * n + col]));
+                            acc = cadd(acc, cmul(conj2(S.V[i * n + col]), t));
+                        }
+                        v3[k] = acc.x / (2.0 * W) * a.vg_ms;
+                    }
+                }
+                for (int k = 0; k < 3; ++k) P.vel[((size_t)q * n + s) * 3 + k] = v3[k];
+                P.oneby[(size_t)q * n + s] = zero_mode ? 0.0 : 1.0 / (W * a.wTHz);
+                for (int t = 0; t < a.nT; ++t)
+                    P.nbe[((size_t)t * nq + q) * n + s] =
+                        zero_mode ? 0.0 : 1.0 / (exp(a.BEConv * fabs(W) / temps[t]) - 1.0);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // Points of the other half of the (q, -q) pairs: copies of their partner with conjugate
 // eigenvectors and reversed velocities.
 __global__ void k_phonons_tr(int n, int nT, int nq, const int* __restrict__ fill, const int* __restrict__ partner,
@@ -317,9 +539,16 @@ int launch_phonons(spring_ctx* c, const PhSet& A, const int* list_a, int n_a, co
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_phonons, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     const int threads = n <= 6 ? 32 : 128;
     const int items = n_a + n_b;
-    const int blocks = items < 148 * 32 ? items : 148 * 32;
     if (items == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "phonons: injected launch failure");
+    if (n == 6 && a.nb == 2 && a.na2 <= PH6_NA2) {
+        const int blocks = std::min((items + PH6_PTS - 1) / PH6_PTS, 148 * 14);
+        k_phonons_n6<<<blocks, PH6_LANES * PH6_PTS, 0, c->stream>>>(a, A, list_a, n_a, B, n_b, c->d_fc2.p,
+                                                                   c->d_fc2_idx.p, c->d_fc2_num.p, c->d_mass_rs.p,
+                                                                   c->d_temps.p);
+        return launch_check(c, "k_phonons_n6");
+    }
+    const int blocks = items < 148 * 32 ? items : 148 * 32;
     k_phonons<<<blocks, threads, smem, c->stream>>>(a, A, list_a, n_a, B, n_b, c->d_fc2.p, c->d_fc2_idx.p,
                                                     c->d_fc2_num.p, c->d_mass_rs.p, c->d_temps.p);
     return launch_check(c, "k_phonons");
