@@ -86,6 +86,31 @@ int d2h_sum2(spring_ctx* c, const int* a, const int* b, int* out, const char* wh
     return d2h(c, out, c->d_scr_sum.p, sizeof(int), what);
 }
 
+int d2h_pin_async(spring_ctx* c, const void* src, size_t bytes, const char* what) {
+    if (injected(c, 1)) return fail(c, SPRING_ERR_INJECTED, "%s: injected copy failure", what);
+    const size_t n = (bytes + sizeof(int) - 1) / sizeof(int);
+    if (c->h_pin_n < n) {
+        if (c->h_pin) cudaFreeHost(c->h_pin);
+        c->h_pin = nullptr;
+        c->h_pin_n = 0;
+        cudaError_t e = cudaHostAlloc((void**)&c->h_pin, std::max<size_t>(n, 1024) * sizeof(int), cudaHostAllocDefault);
+        if (e != cudaSuccess) return cuda_fail(c, e, what);
+        c->h_pin_n = std::max<size_t>(n, 1024);
+    }
+    if (!c->ev_aux) {
+        cudaError_t e = cudaEventCreateWithFlags(&c->ev_aux, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(c, e, what);
+    }
+    cudaError_t e = cudaMemcpyAsync(c->h_pin, src, bytes, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_aux, c->stream);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
+int pin_wait(spring_ctx* c, const char* what) {
+    cudaError_t e = cudaEventSynchronize(c->ev_aux);
+    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+}
+
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what) {
     cudaError_t e = cudaMemsetAsync(dst, 0, bytes, c->stream);
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
@@ -172,6 +197,9 @@ int set_temps(spring_ctx* c, const double* temps) {
     if (!temps) return fail(c, SPRING_ERR_ARG, "temps is NULL");
     for (int i = 0; i < c->nT; ++i)
         if (!(temps[i] > 0.0)) return fail(c, SPRING_ERR_ARG, "temperature %d is not positive", i + 1);
+    // unchanged temperatures are not copied again (a copy from pageable memory may wait for the stream)
+    if (c->d_temps.p && c->temps.size() == (size_t)c->nT && std::equal(temps, temps + c->nT, c->temps.begin()))
+        return SPRING_OK;
     c->temps.assign(temps, temps + c->nT);
     SPRING_CHECK(dalloc(c, c->d_temps, c->nT, "temperatures"));
     return h2d(c, c->d_temps.p, temps, sizeof(double) * c->nT, "temperatures");
@@ -270,6 +298,8 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_tc_seg); dfree(c->d_tc_ntl); dfree(c->d_tc_toff); dfree(c->d_tc_sort);
         dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
+        if (c->h_pin) cudaFreeHost(c->h_pin);
+        if (c->ev_aux) cudaEventDestroy(c->ev_aux);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
     }
     delete c;

@@ -16,6 +16,7 @@
 // where q1 == p(q1) but the integer vectors differ (the reference then
 // overwrites the direct entry with flag 0), are bit-identical to the
 // reference algorithm's.  HBM bound: 8 bytes per pair written.
+#include <algorithm>
 #include <cub/cub.cuh>
 
 #include "spring_internal.cuh"
@@ -58,7 +59,8 @@ __global__ void k_enum3_flags(int nq, int nq0, int n0, int n1, int n2, const int
     }
 }
 
-__global__ void k_enum3_pairs(int nq, int nq0, const int* __restrict__ partner, const int* __restrict__ rep,
+// Pairs beyond `cap` are not written (the host compares pairoff[nq0] with cap and re-runs).
+__global__ void k_enum3_pairs(int nq, int nq0, int cap, const int* __restrict__ partner, const int* __restrict__ rep,
                               const int* __restrict__ pos, int2* __restrict__ pairs, int* __restrict__ pair_q0,
                               int* __restrict__ pairoff) {
     const long long total = (long long)nq0 * nq;
@@ -66,7 +68,7 @@ __global__ void k_enum3_pairs(int nq, int nq0, const int* __restrict__ partner, 
         const int q0 = (int)(i / nq), g = (int)(i % nq);
         if (g == 0) pairoff[q0] = pos[i];
         if (i == total - 1) pairoff[nq0] = pos[i] + rep[i];
-        if (rep[i]) {
+        if (rep[i] && pos[i] < cap) {
             pairs[pos[i]] = make_int2(g, partner[i]);
             pair_q0[pos[i]] = q0;
         }
@@ -126,21 +128,30 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
         rc = launch_check(c, "k_enum3_flags");
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, rep.p, ps.pairpos.p, (int)total);
-    int npairs = 0;
-    if (rc == SPRING_OK) rc = d2h_sum2(c, ps.pairpos.p + total - 1, rep.p + total - 1, &npairs, "pair count");
-    if (rc == SPRING_OK) rc = dalloc(c, ps.pairs, npairs, "pair list");
-    if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, npairs, "pair list");
+    // The pair list is sized without a readback: each q0 has at most Nq/2 + 8 representatives (a
+    // pair and its swap fold into one; q1 = q2 has at most 8 solutions), and the offsets read back
+    // at the end confirm it (else the list is regrown to the exact count and written again).
+    const long long bound = std::min<long long>(total, (long long)ps.n0 * (c->nq / 2 + 8));
+    int cap = (int)std::max<long long>(bound, 1);
     if (rc == SPRING_OK) rc = dalloc(c, ps.pairoff, ps.n0 + 1, "pair offsets");
-    if (rc == SPRING_OK && launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
-    if (rc == SPRING_OK) {
-        k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, ps.partner.p, rep.p, ps.pairpos.p, ps.pairs.p,
-                                                         ps.pair_q0.p, ps.pairoff.p);
-        rc = launch_check(c, "k_enum3_pairs");
+    for (int attempt = 0; attempt < 2 && rc == SPRING_OK; ++attempt) {
+        rc = dalloc(c, ps.pairs, cap, "pair list");
+        if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, cap, "pair list");
+        if (rc == SPRING_OK && launch_injected(c))
+            rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
+        if (rc == SPRING_OK) {
+            k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, cap, ps.partner.p, rep.p, ps.pairpos.p,
+                                                             ps.pairs.p, ps.pair_q0.p, ps.pairoff.p);
+            rc = launch_check(c, "k_enum3_pairs");
+        }
+        if (rc == SPRING_OK) {
+            ps.h_pairoff.assign(ps.n0 + 1, 0);
+            rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
+        }
+        if (rc != SPRING_OK || ps.h_pairoff[ps.n0] <= cap) break;
+        cap = ps.h_pairoff[ps.n0];
     }
-    if (rc == SPRING_OK) {
-        ps.h_pairoff.assign(ps.n0 + 1, 0);
-        rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
-    }
+    if (rc == SPRING_OK && ps.h_pairoff[ps.n0] > cap) rc = fail(c, SPRING_ERR_CUDA, "enumerate3: pair list overflow");
     if (rc == SPRING_OK) {
         ps.done = true;
         ps.gen += 1;

@@ -261,6 +261,7 @@ __global__ void k_tc_keys(int n, int p0, int nq, const int2* __restrict__ pairs,
         if (any) atomicAdd(&cnt[pq.x], 1);
     }
 }
+__global__ void k_tc_sum2(const int* __restrict__ a, const int* __restrict__ b, int* __restrict__ out) { *out = *a + *b; }
 __global__ void k_tc_ntiles(int nq, const int* __restrict__ cnt, int* __restrict__ nt) {
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nq; g += gridDim.x * blockDim.x)
         nt[g] = (cnt[g] + EPT - 1) / EPT;
@@ -776,11 +777,16 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
 
 // Pairs of [p0, p1) with a mode triple inside the delta window `rf`, sorted by q1 (stable radix
 // sort), cut into tiles of at most EPT pairs of one q1, with the entry record of every sorted pair.
-// Cached until the pair list, the phonons or the window change.
-int build_tiles(spring_ctx* c, int p0, int p1, float rf) {
+// Cached until the pair list, the phonons or the window change.  build_tiles_begin queues the keys,
+// the sort, the tile counts and an asynchronous readback of their total (c->tc_pending);
+// build_tiles_end waits for it and cuts the tiles, so that work queued between the two (the
+// operand tables) runs while the host waits.
+int build_tiles_begin(spring_ctx* c, int p0, int p1, float rf) {
     const PairSet& ps = c->ps_irr;
+    c->tc_pending = false;
     if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1 && c->tc_ph_gen == c->ph_gen && c->tc_rf == rf)
         return SPRING_OK;
+    c->tc_gen = -1;  // no valid tiles until build_tiles_end has cut them
     const int n = p1 - p0, nq = c->nq;
     DBuf<int>&keys = c->d_tc_keys, &keys_s = c->d_tc_keys_s, &vals = c->d_tc_vals, &cnt = c->d_tc_cnt,
               &seg = c->d_tc_seg, &ntl = c->d_tc_ntl, &toff = c->d_tc_toff;
@@ -828,8 +834,29 @@ int build_tiles(spring_ctx* c, int p0, int p1, float rf) {
         }
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, ntl.p, toff.p, nq);
-    int ntiles = 0;
-    if (rc == SPRING_OK) rc = d2h_sum2(c, toff.p + nq - 1, ntl.p + nq - 1, &ntiles, "tile count");
+    if (rc == SPRING_OK) rc = dalloc(c, c->d_scr_sum, 1, "tile count");
+    if (rc == SPRING_OK) {
+        k_tc_sum2<<<1, 1, 0, c->stream>>>(toff.p + nq - 1, ntl.p + nq - 1, c->d_scr_sum.p);
+        rc = launch_check(c, "k_tc_sum2");
+    }
+    if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, sizeof(int), "tile count");
+    if (rc != SPRING_OK) return rc;
+    c->tc_pending = true;
+    c->tc_p0 = p0;
+    c->tc_p1 = p1;
+    c->tc_rf = rf;
+    return SPRING_OK;
+}
+
+int build_tiles_end(spring_ctx* c) {
+    if (!c->tc_pending) return SPRING_OK;
+    c->tc_pending = false;
+    const PairSet& ps = c->ps_irr;
+    const int n = c->tc_p1 - c->tc_p0, nq = c->nq;
+    DBuf<int>&cnt = c->d_tc_cnt, &seg = c->d_tc_seg, &toff = c->d_tc_toff;
+    const int threads = 256;
+    int rc = pin_wait(c, "tile count");
+    const int ntiles = rc == SPRING_OK ? c->h_pin[0] : 0;
     if (rc == SPRING_OK) rc = dalloc(c, c->d_tc_tiles, std::max(ntiles, 1), "tiles");
     if (rc == SPRING_OK) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
@@ -849,10 +876,7 @@ int build_tiles(spring_ctx* c, int p0, int p1, float rf) {
     if (rc != SPRING_OK) return rc;
     c->tc_ntiles = ntiles;
     c->tc_gen = ps.gen;
-    c->tc_p0 = p0;
-    c->tc_p1 = p1;
     c->tc_ph_gen = c->ph_gen;
-    c->tc_rf = rf;
     return SPRING_OK;
 }
 
@@ -875,8 +899,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const double os = 1.0 / sigma;
     const double half_os2 = 0.5 * (os * os);
     const float rf = (float)(sqrt(EXP_CUT / half_os2) * 1.0001 + 1e-3);
-    SPRING_CHECK(build_tiles(c, p0, p1, rf));
-    if (c->tc_ntiles == 0) return SPRING_OK;  // no pair has a mode triple inside the window
+    SPRING_CHECK(build_tiles_begin(c, p0, p1, rf));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
@@ -898,6 +921,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
                  c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p,
                               c->d_tc_modes.p);
     SPRING_CHECK(launch_check(c, "k_tc_modes"));
+    SPRING_CHECK(build_tiles_end(c));  // the tile count was read while the tables were queued
+    if (c->tc_ntiles == 0) return SPRING_OK;  // no pair has a mode triple inside the window
 
     TcArgs a{};
     a.nq = nq;
@@ -923,7 +948,6 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE / EPI_WARPS;
     long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 12, 256);
     const bool split = c->precision == SPRING_BF16X3;
-    std::vector<int> cnt(nreg + 1);
     int maxcnt = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         cap = std::min<long long>(cap, triples);
@@ -932,24 +956,35 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
         TcItem* items = reinterpret_cast<TcItem*>(c->d_tc_items.p);
         SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p + nreg, sizeof(int), "V3 status"));
         SPRING_CHECK(split ? launch_tc<true>(c, a, items) : launch_tc<false>(c, a, items));
-        SPRING_CHECK(d2h(c, cnt.data(), c->d_tc_cnt_cta.p, sizeof(int) * (nreg + 1), "V3 item counts"));
+        SPRING_CHECK(d2h_pin_async(c, c->d_tc_cnt_cta.p, sizeof(int) * (nreg + 1), "V3 item counts"));
+        // The evaluation pass is queued at once: it reads the item counts on the device and clamps
+        // them to the region size, so the host checks them while it runs.
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
+        const int gy = c->tc_eval_y > 0 ? c->tc_eval_y : (int)std::min<long long>(1024, (cap + 2 * threads - 1) / (2 * threads));
+        k_v3tc_eval<<<dim3(nreg, gy), threads, 0, c->stream>>>(
+            items, c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2, os * ONEBYSQRT2PI,
+            host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p,
+            d_lw, d_p3);
+        SPRING_CHECK(launch_check(c, "k_v3tc_eval"));
+        SPRING_CHECK(pin_wait(c, "V3 item counts"));
+        const int* cnt = c->h_pin;
         const int herr = cnt[nreg];
         if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
         if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
-        maxcnt = *std::max_element(cnt.begin(), cnt.begin() + nreg);
+        maxcnt = *std::max_element(cnt, cnt + nreg);
         if (maxcnt <= cap) break;
-        cap = (long long)(maxcnt * 1.25) + 256;  // the pass only wrote what fit; run it again
+        // The pass wrote only what fit and the evaluation summed that part: clear this block's sums
+        // and run both again with regions sized from the counts.
+        for (int T = 0; T < c->nT; ++T)
+            SPRING_CHECK(zero(c, d_lw + ((size_t)T * c->nq0 + q0_first) * NMODE, sizeof(double) * n_q0 * NMODE,
+                              "linewidths"));
+        SPRING_CHECK(zero(c, d_p3 + (size_t)q0_first * NMODE, sizeof(double) * n_q0 * NMODE, "phase space"));
+        cap = (long long)(maxcnt * 1.25) + 256;
     }
     if (maxcnt > cap) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: item list overflow");
     c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
-    if (maxcnt == 0) return SPRING_OK;
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
-    const dim3 grid(nreg, std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads))));
-    k_v3tc_eval<<<grid, threads, 0, c->stream>>>(
-        reinterpret_cast<const TcItem*>(c->d_tc_items.p), c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2,
-        os * ONEBYSQRT2PI, host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p),
-        c->d_tc_modes.p, d_lw, d_p3);
-    return launch_check(c, "k_v3tc_eval");
+    c->tc_eval_y = std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads)));
+    return SPRING_OK;
 }
 
 }  // namespace spring

@@ -84,6 +84,9 @@ struct spring_ctx {
     int nq = 0, nq0 = 0, nT = 1;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
+    int* h_pin = nullptr;              // pinned host scratch for readbacks that overlap queued work
+    size_t h_pin_n = 0;                // its size in ints
+    cudaEvent_t ev_aux = nullptr;      // marks the end of such a readback
     std::string err;
     long long launches = 0;
     int precision = SPRING_FP64;
@@ -194,6 +197,8 @@ struct spring_ctx {
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
     int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1, tc_ph_gen = -1;
     float tc_rf = 0.0f;                // delta window the cached tiles were screened with
+    int tc_eval_y = 0;                 // blocks per item region of the last evaluation pass
+    bool tc_pending = false;           // tile count read back asynchronously, tiles not cut yet
     int ph_gen = 0;                    // bumped whenever the grid or irreducible phonons change
     // scratch kept between calls (the enumeration and the tile sort run every step)
     spring::DBuf<int> d_scr_rep, d_tc_keys, d_tc_keys_s, d_tc_vals, d_tc_cnt, d_tc_seg, d_tc_ntl, d_tc_toff;
@@ -236,6 +241,9 @@ int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* wha
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what);
 int d2h_sum2(spring_ctx* c, const int* a, const int* b, int* out, const char* what);
+// Device -> pinned host copy of `bytes` ending in an event; pin_wait() waits for it.
+int d2h_pin_async(spring_ctx* c, const void* src, size_t bytes, const char* what);
+int pin_wait(spring_ctx* c, const char* what);
 // Every kernel launch site calls launch_injected() first (fault injection and,
 // when profiling, the start event) and launch_check() right after the launch
 // (error check, launch count, stop event named after the kernel).
