@@ -998,6 +998,7 @@ int prepare_lw3(spring_ctx* c, int i0_first, int n_q0, const int* pol3, Pol* pol
     SPRING_CHECK(ready3(c));
     SPRING_CHECK(check_pol(c, pol3));
     SPRING_CHECK(ensure_enum3(c));
+    SPRING_CHECK(pairoff_host(c, c->ps_irr));  // the batch kernel's descriptors take host pair ranges
     *pol = make_pol(c, pol3);
     return SPRING_OK;
 }

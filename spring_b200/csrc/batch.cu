@@ -203,6 +203,7 @@ int build_desc(spring_batch* b, std::vector<BatchDesc>& D, std::vector<long long
         spring_ctx* c = w.c;
         const int n = c->ndof, sb = n <= 12 ? n : sb_big;
         const spring::PairSet& ps = c->ps_irr;
+        if (spring::pairoff_host(c, ps) != SPRING_OK) return bfail(b, SPRING_ERR_CUDA, "%s", c->err.c_str());
         w.pairs = ps.h_pairoff[w.q0 + w.n_q0] - ps.h_pairoff[w.q0];
         w.kind = (b->cfg[0] && c->nb == spring::s3::NB && c->na3 == spring::s3::NA && c->nT <= spring::s3::MAXT) ? 0 : 1;
         if (w.kind == 0) {

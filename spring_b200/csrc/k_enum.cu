@@ -111,6 +111,16 @@ int run_exclusive_scan(spring_ctx* c, const int* d_in, int* d_out, int n) {
     return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, "exclusive scan");
 }
 
+int pairoff_host(spring_ctx* c, const PairSet& ps) {
+    if (ps.h_ok) return SPRING_OK;
+    ps.h_pairoff.assign(ps.n0 + 1, 0);
+    SPRING_CHECK(d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets"));
+    if (ps.h_pairoff[ps.n0] > ps.cap) return fail(c, SPRING_ERR_CUDA, "enumerate3: %d pairs exceed the list's %d",
+                                                 ps.h_pairoff[ps.n0], ps.cap);
+    ps.h_ok = true;
+    return SPRING_OK;
+}
+
 int run_enumerate3(spring_ctx* c, PairSet& ps) {
     ps.done = false;
     const long long total = (long long)ps.n0 * c->nq;
@@ -128,30 +138,23 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
         rc = launch_check(c, "k_enum3_flags");
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, rep.p, ps.pairpos.p, (int)total);
-    // The pair list is sized without a readback: each q0 has at most Nq/2 + 8 representatives (a
-    // pair and its swap fold into one; q1 = q2 has at most 8 solutions), and the offsets read back
-    // at the end confirm it (else the list is regrown to the exact count and written again).
+    // The pair list is sized without a readback: q1 is a representative iff its partner p(q1) >= q1,
+    // so each q0 has at most (Nq + F) / 2 of them, F <= 8 the points with p(q1) = q1 (two solutions
+    // of 2 x = c mod N per dimension).  The writes are guarded all the same, and pairoff_host checks
+    // the total when the offsets are first read.
     const long long bound = std::min<long long>(total, (long long)ps.n0 * (c->nq / 2 + 8));
-    int cap = (int)std::max<long long>(bound, 1);
+    const int cap = (int)std::max<long long>(bound, 1);
     if (rc == SPRING_OK) rc = dalloc(c, ps.pairoff, ps.n0 + 1, "pair offsets");
-    for (int attempt = 0; attempt < 2 && rc == SPRING_OK; ++attempt) {
-        rc = dalloc(c, ps.pairs, cap, "pair list");
-        if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, cap, "pair list");
-        if (rc == SPRING_OK && launch_injected(c))
-            rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
-        if (rc == SPRING_OK) {
-            k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, cap, ps.partner.p, rep.p, ps.pairpos.p,
-                                                             ps.pairs.p, ps.pair_q0.p, ps.pairoff.p);
-            rc = launch_check(c, "k_enum3_pairs");
-        }
-        if (rc == SPRING_OK) {
-            ps.h_pairoff.assign(ps.n0 + 1, 0);
-            rc = d2h(c, ps.h_pairoff.data(), ps.pairoff.p, sizeof(int) * (ps.n0 + 1), "pair offsets");
-        }
-        if (rc != SPRING_OK || ps.h_pairoff[ps.n0] <= cap) break;
-        cap = ps.h_pairoff[ps.n0];
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pairs, cap, "pair list");
+    if (rc == SPRING_OK) rc = dalloc(c, ps.pair_q0, cap, "pair list");
+    if (rc == SPRING_OK && launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "enumerate3: injected launch failure");
+    if (rc == SPRING_OK) {
+        k_enum3_pairs<<<blocks, threads, 0, c->stream>>>(c->nq, ps.n0, cap, ps.partner.p, rep.p, ps.pairpos.p,
+                                                         ps.pairs.p, ps.pair_q0.p, ps.pairoff.p);
+        rc = launch_check(c, "k_enum3_pairs");
     }
-    if (rc == SPRING_OK && ps.h_pairoff[ps.n0] > cap) rc = fail(c, SPRING_ERR_CUDA, "enumerate3: pair list overflow");
+    ps.cap = cap;
+    ps.h_ok = false;
     if (rc == SPRING_OK) {
         ps.done = true;
         ps.gen += 1;
@@ -162,6 +165,7 @@ int run_enumerate3(spring_ctx* c, PairSet& ps) {
 int run_enumerate3_fortran(spring_ctx* c, int q0, int* d_allq1q2, int* d_perm, int* d_counts) {
     PairSet& ps = c->ps_irr;
     if (!ps.done) SPRING_CHECK(run_enumerate3(c, ps));
+    SPRING_CHECK(pairoff_host(c, ps));
     const int* p = ps.pairpos.p + (size_t)q0 * c->nq;
     const int base = ps.h_pairoff[q0];
     SPRING_CHECK(zero(c, d_counts, 2 * sizeof(int), "counts"));

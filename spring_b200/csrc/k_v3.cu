@@ -56,6 +56,7 @@ int launch_v3(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, i
     a.sb = v3_block(c->ndof);
     a.nsb = (c->ndof + a.sb - 1) / a.sb;
     a.mfac = host_constants().Sctr3THz2 / double(c->nq);
+    SPRING_CHECK(pairoff_host(c, ps));
     const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
     a.pair_first = p0;
     const size_t smem = v3_smem(a.n, a.na, a.sb, a.nT);

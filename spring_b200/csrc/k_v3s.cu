@@ -44,6 +44,7 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
     a.nT = c->nT;
     a.nq0 = ps.n0;
     a.q0_first = q0_first;
+    SPRING_CHECK(pairoff_host(c, ps));
     a.pair_first = ps.h_pairoff[q0_first];
     a.pair_end = ps.h_pairoff[q0_first + n_q0];
     a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;

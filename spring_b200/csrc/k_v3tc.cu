@@ -232,10 +232,22 @@ __global__ void k_tc_modes(int nq, int nT, int rs, const double* __restrict__ om
 // nq (sorted after every q1, and left out of the tiles) for a pair with none.  The test is the
 // tensor-core pass's own, so a pair left out would have produced no item there.  About half the
 // pairs of a 24^3 mesh (Gaussian width 0.38 rad/ps) have no triple in the window.
-__global__ void k_tc_keys(int n, int p0, int nq, const int2* __restrict__ pairs, const int* __restrict__ pair_q0,
+// The pairs of q0 block [q0_first, q0_first + n_q0) are read from the device offsets; slots
+// i >= their count (up to nmax) get key nq too.  The count goes to *n_out for the host to check
+// against nmax; no pair at or beyond `cap` (the list's size) is read.
+__global__ void k_tc_keys(int nmax, int cap, int q0_first, int n_q0, int nq, const int* __restrict__ pairoff,
+                          const int2* __restrict__ pairs, const int* __restrict__ pair_q0,
                           const double* __restrict__ om0, const double* __restrict__ omg, float rf,
-                          int* __restrict__ keys, int* __restrict__ vals, int* __restrict__ cnt) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+                          int* __restrict__ keys, int* __restrict__ vals, int* __restrict__ cnt,
+                          int* __restrict__ n_out) {
+    const int p0 = pairoff[q0_first], n = pairoff[q0_first + n_q0] - p0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *n_out = n;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nmax; i += gridDim.x * blockDim.x) {
+        if (i >= n || p0 + i >= cap) {
+            keys[i] = nq;
+            vals[i] = -1;
+            continue;
+        }
         const int2 pq = pairs[p0 + i];
         const double* w0d = om0 + (size_t)pair_q0[p0 + i] * NMODE;
         const double* w1d = omg + (size_t)pq.x * NMODE;
@@ -273,10 +285,13 @@ __global__ void k_tc_tiles(int nq, const int* __restrict__ cnt, const int* __res
         for (int t = 0; t * EPT < c; ++t) tiles[toff[g] + t] = make_int4(g, seg[g] + t * EPT, min(EPT, c - t * EPT), 0);
     }
 }
-// Entry records in q1 order: (q0, q2, pair-folding weight, q0 is Gamma).
-__global__ void k_tc_entrec(int n, const int* __restrict__ entries, const int2* __restrict__ pairs,
-                            const int* __restrict__ pair_q0, const int* __restrict__ irr_int, int4* __restrict__ rec) {
+// Entry records in q1 order: (q0, q2, pair-folding weight, q0 is Gamma); entries with key nq
+// (outside the window or past the block's pairs, all after the tiled ones) are skipped.
+__global__ void k_tc_entrec(int n, int nq, const int* __restrict__ entries, const int* __restrict__ keys_s,
+                            const int2* __restrict__ pairs, const int* __restrict__ pair_q0,
+                            const int* __restrict__ irr_int, int4* __restrict__ rec) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (keys_s[i] >= nq) continue;
         const int pi = entries[i];
         const int2 pq = pairs[pi];
         const int q0 = pair_q0[pi];
@@ -775,19 +790,20 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
-// Pairs of [p0, p1) with a mode triple inside the delta window `rf`, sorted by q1 (stable radix
-// sort), cut into tiles of at most EPT pairs of one q1, with the entry record of every sorted pair.
-// Cached until the pair list, the phonons or the window change.  build_tiles_begin queues the keys,
+// Pairs of q0 block [q0, q0 + n0) with a mode triple inside the delta window `rf`, sorted by q1
+// (stable radix sort over nmax >= their count slots), cut into tiles of at most EPT pairs of one
+// q1, with the entry record of every sorted pair.  Cached until the pair list, the phonons or the
+// window change.  build_tiles_begin queues the keys,
 // the sort, the tile counts and an asynchronous readback of their total (c->tc_pending);
 // build_tiles_end waits for it and cuts the tiles, so that work queued between the two (the
 // operand tables) runs while the host waits.
-int build_tiles_begin(spring_ctx* c, int p0, int p1, float rf) {
+int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
     const PairSet& ps = c->ps_irr;
     c->tc_pending = false;
-    if (c->tc_gen == ps.gen && c->tc_p0 == p0 && c->tc_p1 == p1 && c->tc_ph_gen == c->ph_gen && c->tc_rf == rf)
+    if (c->tc_gen == ps.gen && c->tc_q0 == q0 && c->tc_n0 == n0 && c->tc_ph_gen == c->ph_gen && c->tc_rf == rf)
         return SPRING_OK;
     c->tc_gen = -1;  // no valid tiles until build_tiles_end has cut them
-    const int n = p1 - p0, nq = c->nq;
+    const int n = nmax, nq = c->nq;
     DBuf<int>&keys = c->d_tc_keys, &keys_s = c->d_tc_keys_s, &vals = c->d_tc_vals, &cnt = c->d_tc_cnt,
               &seg = c->d_tc_seg, &ntl = c->d_tc_ntl, &toff = c->d_tc_toff;
     int rc = SPRING_OK;
@@ -801,13 +817,16 @@ int build_tiles_begin(spring_ctx* c, int p0, int p1, float rf) {
     step(dalloc(c, seg, nq, "tile segments"));
     step(dalloc(c, ntl, nq, "tile counts"));
     step(dalloc(c, toff, nq, "tile offsets"));
+    step(dalloc(c, c->d_scr_sum, 2, "tile and pair counts"));
     if (rc == SPRING_OK) rc = zero(c, cnt.p, sizeof(int) * nq, "tile counts");
+    if (rc == SPRING_OK) rc = zero(c, c->d_scr_sum.p, 2 * sizeof(int), "tile and pair counts");
     const int threads = 256;
     if (rc == SPRING_OK && n > 0) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
         else {
             k_tc_keys<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
-                n, p0, nq, ps.pairs.p, ps.pair_q0.p, c->ph_irr.omega.p, c->ph_grid.omega.p, rf, keys.p, vals.p, cnt.p);
+                n, ps.cap, q0, n0, nq, ps.pairoff.p, ps.pairs.p, ps.pair_q0.p, c->ph_irr.omega.p, c->ph_grid.omega.p,
+                rf, keys.p, vals.p, cnt.p, c->d_scr_sum.p + 1);
             rc = launch_check(c, "k_tc_keys");
         }
     }
@@ -834,16 +853,16 @@ int build_tiles_begin(spring_ctx* c, int p0, int p1, float rf) {
         }
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, ntl.p, toff.p, nq);
-    if (rc == SPRING_OK) rc = dalloc(c, c->d_scr_sum, 1, "tile count");
     if (rc == SPRING_OK) {
         k_tc_sum2<<<1, 1, 0, c->stream>>>(toff.p + nq - 1, ntl.p + nq - 1, c->d_scr_sum.p);
         rc = launch_check(c, "k_tc_sum2");
     }
-    if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, sizeof(int), "tile count");
+    if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, 2 * sizeof(int), "tile and pair counts");
     if (rc != SPRING_OK) return rc;
     c->tc_pending = true;
-    c->tc_p0 = p0;
-    c->tc_p1 = p1;
+    c->tc_q0 = q0;
+    c->tc_n0 = n0;
+    c->tc_nmax = nmax;
     c->tc_rf = rf;
     return SPRING_OK;
 }
@@ -852,11 +871,13 @@ int build_tiles_end(spring_ctx* c) {
     if (!c->tc_pending) return SPRING_OK;
     c->tc_pending = false;
     const PairSet& ps = c->ps_irr;
-    const int n = c->tc_p1 - c->tc_p0, nq = c->nq;
+    const int n = c->tc_nmax, nq = c->nq;
     DBuf<int>&cnt = c->d_tc_cnt, &seg = c->d_tc_seg, &toff = c->d_tc_toff;
     const int threads = 256;
     int rc = pin_wait(c, "tile count");
     const int ntiles = rc == SPRING_OK ? c->h_pin[0] : 0;
+    if (rc == SPRING_OK && c->h_pin[1] > n)
+        rc = fail(c, SPRING_ERR_CUDA, "tiles: %d pairs in the q0 block exceed the %d slots", c->h_pin[1], n);
     if (rc == SPRING_OK) rc = dalloc(c, c->d_tc_tiles, std::max(ntiles, 1), "tiles");
     if (rc == SPRING_OK) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
@@ -869,7 +890,7 @@ int build_tiles_end(spring_ctx* c) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
         else {
             k_tc_entrec<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
-                n, c->d_tc_entries.p, ps.pairs.p, ps.pair_q0.p, c->d_irr_int.p, c->d_tc_rec.p);
+                n, nq, c->d_tc_entries.p, c->d_tc_keys_s.p, ps.pairs.p, ps.pair_q0.p, c->d_irr_int.p, c->d_tc_rec.p);
             rc = launch_check(c, "k_tc_entrec");
         }
     }
@@ -887,10 +908,10 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     *handled = false;
     if (c->nb != 2 || c->na3 > 8) return SPRING_OK;
     const PairSet& ps = c->ps_irr;
-    const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
     *handled = true;
-    if (p1 == p0) return SPRING_OK;
     const int nq = c->nq;
+    // slots for the block's pairs without reading their count: at most Nq/2 + 8 per q0
+    const int nmax = (int)std::min<long long>(ps.cap, (long long)n_q0 * (nq / 2 + 8));
     SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 4 * AIMG, "V3 A table"));
     SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 4 * BIMG, "V3 B table"));
     SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
@@ -899,7 +920,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const double os = 1.0 / sigma;
     const double half_os2 = 0.5 * (os * os);
     const float rf = (float)(sqrt(EXP_CUT / half_os2) * 1.0001 + 1e-3);
-    SPRING_CHECK(build_tiles_begin(c, p0, p1, rf));
+    SPRING_CHECK(build_tiles_begin(c, q0_first, n_q0, nmax, rf));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
     k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,

@@ -43,7 +43,9 @@ struct PairSet {
     DBuf<int2> pairs;             // (g1, g2) 0-based, grouped by q0
     DBuf<int> pair_q0;            // q0 of each pair
     DBuf<int> pairpos;            // [q0][q1] exclusive-scan position of each representative
-    std::vector<int> h_pairoff;
+    mutable std::vector<int> h_pairoff;  // host copy of pairoff, read on first use (pairoff_host)
+    mutable bool h_ok = false;
+    int cap = 0;                  // pairs and pair_q0 hold this many entries
     bool done = false;
     int gen = 0;                  // bumped every time the lists are rebuilt
 };
@@ -195,7 +197,7 @@ struct spring_ctx {
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
-    int tc_ntiles = 0, tc_gen = -1, tc_p0 = -1, tc_p1 = -1, tc_ph_gen = -1;
+    int tc_ntiles = 0, tc_gen = -1, tc_q0 = -1, tc_n0 = -1, tc_nmax = 0, tc_ph_gen = -1;  // tile cache key
     float tc_rf = 0.0f;                // delta window the cached tiles were screened with
     int tc_eval_y = 0;                 // blocks per item region of the last evaluation pass
     bool tc_pending = false;           // tile count read back asynchronously, tiles not cut yet
@@ -233,6 +235,7 @@ void dfree(DBuf<T>& b) {
 inline void free_pairs(PairSet& s) {
     dfree(s.partner); dfree(s.pairoff); dfree(s.pairs); dfree(s.pair_q0); dfree(s.pairpos);
     s.h_pairoff.clear();
+    s.h_ok = false;
     s.done = false;
 }
 void free_phonons(Phonons& p);
@@ -241,6 +244,8 @@ int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* wha
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what);
 int zero(spring_ctx* c, void* dst, size_t bytes, const char* what);
 int d2h_sum2(spring_ctx* c, const int* a, const int* b, int* out, const char* what);
+// Host copy of a pair set's offsets (one readback after each enumeration, on first use).
+int pairoff_host(spring_ctx* c, const PairSet& ps);
 // Device -> pinned host copy of `bytes` ending in an event; pin_wait() waits for it.
 int d2h_pin_async(spring_ctx* c, const void* src, size_t bytes, const char* what);
 int pin_wait(spring_ctx* c, const char* what);
