@@ -67,9 +67,10 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
 
 BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
 TC_EPT = 16         # pairs per tensor-core tile
-# DRAM bytes per pair of the tensor-core pass (read + write), from one ncu capture of the 16^3
-# rocksalt launch (297,076 pairs; 71.0 MB read, 18.8 MB written)
-TC_DRAM_BYTES_PER_PAIR = (70.992384e6 + 18.826752e6) / 297076
+# DRAM bytes per tiled pair of the tensor-core pass (read + write), from one ncu capture of the
+# 16^3 rocksalt launch (140,383 of its 297,076 pairs have a mode triple inside the delta window and
+# are tiled; 61.6 MB read, 16.9 MB written)
+TC_DRAM_BYTES_PER_TILED_PAIR = (61.563904e6 + 16.864768e6) / 140383
 
 
 def tc_issued_flops_per_tile(passes):
@@ -77,8 +78,6 @@ def tc_issued_flops_per_tile(passes):
     return 2 * 3 * passes * 2 * 128 * 48 * 16
 
 
-def tc_tiles(counts_by_q1):
-    return int(np.sum((np.asarray(counts_by_q1) + TC_EPT - 1) // TC_EPT))
 
 
 class Clocks:
@@ -94,6 +93,7 @@ class Clocks:
         import threading
         self.index, self.bus_id = index, bus_id
         self.rows = []
+        self.lock = threading.Lock()
         self.active = threading.Event()
         self.done = threading.Event()
         self.thread = None
@@ -107,11 +107,11 @@ class Clocks:
                  "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
         smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
         while not self.done.is_set():
-            if not self.active.wait(0.05):
+            if not self.active.wait(0.05) or self.done.is_set():
                 continue
-            sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-            r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-            if self.active.is_set():
+            with self.lock:  # a query that began inside the timed region is kept, however short it is
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
                 self.rows.append((float(sm), float(smax), sorted(k for k, v in names.items() if r & v)))
             time.sleep(0.002)
 
@@ -139,6 +139,8 @@ class Clocks:
 
     def end(self):
         self.active.clear()
+        with self.lock:  # let a query in flight finish and be recorded
+            pass
 
     def stop(self):
         rows = []
@@ -321,6 +323,7 @@ def fourph_leg(torch, mesh4, frac=0.1):
     return {"mesh": [mesh4] * 3, "temperature": 300.0, "irreducible_q0": int(len(order)), "quartets": int(quartets),
             "evals_per_s_exact": quartets * 36 * 36 / (exact_ms * 1e-3), "exact_ms": exact_ms,
             "screened_ms": scr_ms + pred_ms, "exact_over_screened": exact_ms / (scr_ms + pred_ms),
+            "screened_exact_part_ms": scr_ms, "prediction_ms": pred_ms,
             "fraction_exact": frac, "kappa_exact": k_ex, "kappa_rel_err_screened": abs(k_scr / k_ex - 1),
             "kappa_rel_err_same_blocks_without_network": abs(k_wo / k_ex - 1), "train_ms_8cubed": train_ms,
             "v4_arithmetic": "f64", "what": "one 4ph eval = one (s0..s3) of one quartet; surrogate 5-128-128-128-1 "
@@ -436,8 +439,6 @@ def run_ours(args):
     counts = np.array([e[2][0] for e in enum])
     lo, hi = partition(counts, world, rank)
     my_pairs = int(counts[lo:hi].sum())
-    counts_by_q1 = np.bincount(np.concatenate([enum[i][1][:, 0] - 1 for i in range(lo, hi)] or [np.zeros(0, int)]),
-                               minlength=int(np.prod(mesh)))
     del enum
     evals_total = int(counts.sum()) * cr.ndof ** 3
     flops_pair = algorithmic_flops_per_pair(cr.ndof, cr.fc3_atm_num)
@@ -500,6 +501,7 @@ def run_ours(args):
         ms64, _, kt64, lw64, kap64, _ = timed("fp64")
         clocks = Clocks(local, pci_bus_id(torch, local))
         ms, launches, kt, lw_p, kap_p, clk = timed(args.precision, clocks)
+        tc_tiles_run, tc_pairs_run = ctx.tc_stats() if args.precision != "fp64" else (0, 0)
         big = lw64 > 1e-3 * lw64.max(axis=(1, 2), keepdims=True)
         lw_err = float((np.abs(lw_p - lw64)[big] / lw64[big]).max())
         diag = [0, 4, 8]
@@ -583,25 +585,29 @@ def run_ours(args):
                     "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (MEASURED_PEAKS.json holds no FP64)"}
         else:
             passes = 3 if args.precision == "bf16x3" else 1
-            issued = tc_issued_flops_per_tile(passes) * tc_tiles(counts_by_q1)
-            algo = flops_pair * my_pairs
+            issued = tc_issued_flops_per_tile(passes) * tc_tiles_run
+            algo = flops_pair * tc_pairs_run
             sec = v3_per_launch * 1e-3
             achieved = algo / sec / 1e12 if v3_n else None
             ev_ms, ev_n = kt["k_v3tc_eval"]
             roof = {"kernel": f"k_v3tc<{args.precision}>", "bound": "tensor", "achieved": achieved,
                     "peak": BF16_PEAK, "unit": "TFLOP/s", "frac": (achieved / BF16_PEAK) if achieved else None,
-                    "traffic": TC_DRAM_BYTES_PER_PAIR * my_pairs,
+                    "traffic": TC_DRAM_BYTES_PER_TILED_PAIR * tc_pairs_run,
+                    "pairs_tiled": tc_pairs_run, "tiles": tc_tiles_run, "pairs_all": my_pairs,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM) of measured",
                     "algorithmic_flops_per_launch": algo,
                     "issued_mma_tflops": issued / sec / 1e12 if v3_n else None,
                     "issued_flops_per_launch": issued,
                     "eval_kernel_ms_per_launch": ev_ms / max(ev_n, 1) if ev_n else None,
-                    "traffic_note": "dram read + write bytes per pair from an ncu capture of the 16^3 launch, "
-                                    "scaled by the pairs of this launch",
-                    "note": "achieved = algorithmic V3 flops (42336 per pair) / kernel time; issued_mma_tflops "
-                            "counts the tcgen05 MMAs as issued (M128 N48 K16 tiles, padding included).  The "
-                            "kernel is bound by its operand gathers and screening epilogue, not by the tensor "
-                            "pipe; the FP64 delta/rate part runs in k_v3tc_eval"}
+                    "traffic_note": "dram read + write bytes per tiled pair from an ncu capture of the 16^3 "
+                                    "launch, scaled by the tiled pairs of this launch",
+                    "note": "achieved = algorithmic V3 flops (42336 per pair) x the pairs the kernel computes "
+                            "(pairs_tiled: those with a mode triple inside the delta window; the pre-screen "
+                            "drops the others, whose every weight is below the exp(-40) cut) / kernel time; "
+                            "issued_mma_tflops counts the tcgen05 MMAs as issued (M128 N48 K16, padding "
+                            "included) over its tiles.  The kernel is bound by its epilogue (accumulator "
+                            "reads, window masks, item stores), not by the tensor pipe; the FP64 delta/rate "
+                            "part runs in k_v3tc_eval"}
         roof.update({"kernel_ms_per_launch": v3_per_launch, "kernel_share_of_step": v3_per_launch / ms,
                      "algorithmic_fp64_flops_per_pair": flops_pair})
         line = {"metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,

@@ -320,6 +320,9 @@ int spring_set_profiling(spring_ctx* ctx, int on);
 /* Device time (ms) and launch count of the recorded launches whose kernel
  * name starts with `prefix` (e.g. "k_v3"); synchronizes the stream. */
 int spring_kernel_time(spring_ctx* ctx, const char* prefix, double* ms, long long* launches);
+/* Pairs and 16-pair tiles of the last tensor-core linewidth pass (the pairs with a mode
+ * triple inside the delta window); 0 and 0 before one ran.  No reference counterpart. */
+int spring_tc_stats(const spring_ctx* ctx, int* n_tiles, int* n_pairs);
 
 /* Make the n-th (1-based) subsequent device allocation (kind 0), host<->device
  * copy (kind 1) or kernel launch (kind 2) report failure without performing

@@ -65,6 +65,7 @@ SIGNATURES = {
     "spring_mlp_predict": [P, I, P, P, I],
     "spring_kappa_iter": [P, D, I, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
+    "spring_tc_stats": [P, P, P],
     "spring_scatter_w3": [P, I, P],
     "spring_linewidth3": [P, I, I, I, D, P, P, P],
     "spring_linewidth_iso": [P, I, I, I, D, P, P],

@@ -147,6 +147,13 @@ class Context:
         self._call("spring_kernel_time", prefix.encode(), ct.byref(ms), ct.byref(n))
         return float(ms.value), int(n.value)
 
+    def tc_stats(self):
+        """(tiles, pairs) of the last tensor-core linewidth pass: the pairs with a mode triple inside
+        the delta window, cut into 16-pair tiles."""
+        nt, npr = ct.c_int(), ct.c_int()
+        self._call("spring_tc_stats", ct.byref(nt), ct.byref(npr))
+        return int(nt.value), int(npr.value)
+
     def prepare3(self):
         self._call("spring_prepare3")
 

@@ -326,6 +326,14 @@ int spring_kernel_launches(const spring_ctx* c, long long* count) {
     return SPRING_OK;
 }
 
+int spring_tc_stats(const spring_ctx* c, int* n_tiles, int* n_pairs) {
+    if (!c || !n_tiles || !n_pairs) return SPRING_ERR_ARG;
+    const bool valid = c->tc_gen >= 0;
+    *n_tiles = valid ? c->tc_ntiles : 0;
+    *n_pairs = valid ? c->tc_npairs : 0;
+    return SPRING_OK;
+}
+
 int spring_kappa_iter(spring_ctx* c, double eps_k, int max_iter, double* kappa, double* kappa_rta, int* iters) {
     CTX_ENTER(c);
     SPRING_CHECK(need(c, c->fc3_set, "FC3"));

@@ -273,7 +273,12 @@ __global__ void k_tc_keys(int nmax, int cap, int q0_first, int n_q0, int nq, con
         if (any) atomicAdd(&cnt[pq.x], 1);
     }
 }
-__global__ void k_tc_sum2(const int* __restrict__ a, const int* __restrict__ b, int* __restrict__ out) { *out = *a + *b; }
+// Tiles (out[0]) and tiled pairs (out[2]) from the last entries of the exclusive scans.
+__global__ void k_tc_totals(int nq, const int* __restrict__ toff, const int* __restrict__ ntl,
+                            const int* __restrict__ seg, const int* __restrict__ cnt, int* __restrict__ out) {
+    out[0] = toff[nq - 1] + ntl[nq - 1];
+    out[2] = seg[nq - 1] + cnt[nq - 1];
+}
 __global__ void k_tc_ntiles(int nq, const int* __restrict__ cnt, int* __restrict__ nt) {
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nq; g += gridDim.x * blockDim.x)
         nt[g] = (cnt[g] + EPT - 1) / EPT;
@@ -817,9 +822,9 @@ int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
     step(dalloc(c, seg, nq, "tile segments"));
     step(dalloc(c, ntl, nq, "tile counts"));
     step(dalloc(c, toff, nq, "tile offsets"));
-    step(dalloc(c, c->d_scr_sum, 2, "tile and pair counts"));
+    step(dalloc(c, c->d_scr_sum, 3, "tile and pair counts"));
     if (rc == SPRING_OK) rc = zero(c, cnt.p, sizeof(int) * nq, "tile counts");
-    if (rc == SPRING_OK) rc = zero(c, c->d_scr_sum.p, 2 * sizeof(int), "tile and pair counts");
+    if (rc == SPRING_OK) rc = zero(c, c->d_scr_sum.p, 3 * sizeof(int), "tile and pair counts");
     const int threads = 256;
     if (rc == SPRING_OK && n > 0) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
@@ -854,10 +859,10 @@ int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
     }
     if (rc == SPRING_OK) rc = run_exclusive_scan(c, ntl.p, toff.p, nq);
     if (rc == SPRING_OK) {
-        k_tc_sum2<<<1, 1, 0, c->stream>>>(toff.p + nq - 1, ntl.p + nq - 1, c->d_scr_sum.p);
-        rc = launch_check(c, "k_tc_sum2");
+        k_tc_totals<<<1, 1, 0, c->stream>>>(nq, toff.p, ntl.p, seg.p, cnt.p, c->d_scr_sum.p);
+        rc = launch_check(c, "k_tc_totals");
     }
-    if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, 2 * sizeof(int), "tile and pair counts");
+    if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, 3 * sizeof(int), "tile and pair counts");
     if (rc != SPRING_OK) return rc;
     c->tc_pending = true;
     c->tc_q0 = q0;
@@ -896,6 +901,7 @@ int build_tiles_end(spring_ctx* c) {
     }
     if (rc != SPRING_OK) return rc;
     c->tc_ntiles = ntiles;
+    c->tc_npairs = c->h_pin[2];
     c->tc_gen = ps.gen;
     c->tc_ph_gen = c->ph_gen;
     return SPRING_OK;

@@ -198,6 +198,7 @@ struct spring_ctx {
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
     int tc_ntiles = 0, tc_gen = -1, tc_q0 = -1, tc_n0 = -1, tc_nmax = 0, tc_ph_gen = -1;  // tile cache key
+    int tc_npairs = 0;                 // pairs in those tiles
     float tc_rf = 0.0f;                // delta window the cached tiles were screened with
     int tc_eval_y = 0;                 // blocks per item region of the last evaluation pass
     bool tc_pending = false;           // tile count read back asynchronously, tiles not cut yet

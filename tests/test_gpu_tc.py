@@ -114,3 +114,36 @@ def test_tc_pair_prescreen_follows_sigma_and_phonons(runs):
         np.testing.assert_allclose(p, p64, rtol=1e-10, atol=1e-12 * np.abs(p64).max())
     finally:
         ctx.set_phonons(0, TEMPS, st.ph)
+
+
+def test_tc_prescreen_counts_match_numpy(runs):
+    """The pairs the tensor-core pass keeps (and their 16-pair tiles per q1) are exactly those a
+    float32 restatement of the delta-window test keeps: |(|w1| - |w0 - w2|)| < R or |w0 + w2 - w1| < R
+    for some mode triple, R = sqrt(40 / (0.5 / sigma^2)) * 1.0001 + 1e-3."""
+    N, ctx, info, out, st = runs
+    if N != 8:
+        pytest.skip("8^3 mesh only")
+    ctx.set_precision("bf16x3")
+    ctx.reset_linewidths()
+    ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
+    tiles, pairs = ctx.tc_stats()
+    ctx.set_precision("fp64")
+    os_ = 1.0 / SIGMA
+    rf = np.float32(np.sqrt(40.0 / (0.5 * (os_ * os_))) * 1.0001 + 1e-3)
+    om = st.ph["omega"].astype(np.float32)
+    om0 = st.ph0["omega"].astype(np.float32)
+    kept = 0
+    by_q1 = np.zeros(st.nq, np.int64)
+    for i0 in range(st.nq0):
+        _, perm, cnt = D.momentum3(st.mesh, st.q_pnt_int, st.irr_int[i0])
+        q1 = perm[: cnt[0], 0] - 1
+        q2 = perm[: cnt[0], 1] - 1
+        w0 = om0[i0][None, :, None, None]
+        w1 = om[q1][:, None, :, None]
+        w2 = om[q2][:, None, None, :]
+        a = (np.abs(np.abs(w1) - np.abs(w0 - w2)) < rf) | (np.abs((w0 + w2) - w1) < rf)
+        m = a.reshape(cnt[0], -1).any(1)
+        kept += int(m.sum())
+        np.add.at(by_q1, q1[m], 1)
+    assert pairs == kept
+    assert tiles == int(((by_q1 + 15) // 16).sum())
