@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, PhSet SA, const in
 }
 
 // Two-atom cells (n = 6): eight lanes per q-point, four points per one-warp block, each group
-// with its own shared-memory state (16 KB per block: 14 blocks, 56 points, per SM).  The same steps as k_phonons (phases once
+// with its own shared-memory state (16 KB per block: 13 blocks, 52 points, per SM).  The same steps as k_phonons (phases once
 // per (mu, N), then D and dD/dq in reference neighbour order; the same round-robin Jacobi rotations
 // and stopping rules; ordering, velocities, nBE), with every control decision warp-uniform: the
 // groups synchronise with full-warp barriers, a converged or idle group only skips work, and the
@@ -542,7 +542,7 @@ int launch_phonons(spring_ctx* c, const PhSet& A, const int* list_a, int n_a, co
     if (items == 0) return SPRING_OK;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "phonons: injected launch failure");
     if (n == 6 && a.nb == 2 && a.na2 <= PH6_NA2) {
-        const int blocks = std::min((items + PH6_PTS - 1) / PH6_PTS, 148 * 14);
+        const int blocks = std::min((items + PH6_PTS - 1) / PH6_PTS, 148 * 13);
         k_phonons_n6<<<blocks, PH6_LANES * PH6_PTS, 0, c->stream>>>(a, A, list_a, n_a, B, n_b, c->d_fc2.p,
                                                                    c->d_fc2_idx.p, c->d_fc2_num.p, c->d_mass_rs.p,
                                                                    c->d_temps.p);
