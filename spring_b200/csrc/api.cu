@@ -300,6 +300,9 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
         if (c->h_pin) cudaFreeHost(c->h_pin);
         if (c->ev_aux) cudaEventDestroy(c->ev_aux);
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        if (c->ev_join) cudaEventDestroy(c->ev_join);
+        if (c->stream2) cudaStreamDestroy(c->stream2);
         if (c->own_stream) cudaStreamDestroy(c->own_stream);
     }
     delete c;

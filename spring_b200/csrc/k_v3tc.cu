@@ -926,29 +926,62 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const double os = 1.0 / sigma;
     const double half_os2 = 0.5 * (os * os);
     const float rf = (float)(sqrt(EXP_CUT / half_os2) * 1.0001 + 1e-3);
-    SPRING_CHECK(build_tiles_begin(c, q0_first, n_q0, nmax, rf));
     const int threads = 256;
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
-                                               c->d_qpnt.p, c->ph_grid.evec.p,
-                                               reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
-    SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_tab_b<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
-                                               c->d_qpnt.p, c->ph_grid.evec.p,
-                                               reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
-    SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_q0tab<<<std::max(1, std::min((c->nq0 * NMODE + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
-        c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p,
-        reinterpret_cast<Q0Rec*>(c->d_tc_q0.p));
-    SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
-    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-    k_tc_modes<<<(int)std::min<long long>(((long long)nq * NMODE * rs + threads - 1) / threads, 148LL * 8), threads, 0,
-                 c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p,
-                              c->d_tc_modes.p);
-    SPRING_CHECK(launch_check(c, "k_tc_modes"));
-    SPRING_CHECK(build_tiles_end(c));  // the tile count was read while the tables were queued
+    // The operand tables depend only on the phonons: they run on a side stream, forked after every
+    // earlier launch on the main stream, beside the tile build, and are joined before the pass.
+    if (!c->stream2) {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(c, e, "side stream");
+    }
+    {
+        cudaError_t e = cudaEventRecord(c->ev_fork, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+        if (e != cudaSuccess) return cuda_fail(c, e, "side stream fork");
+    }
+    auto tables = [&]() -> int {
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+        k_tc_tab_a<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
+                                                   c->d_qpnt.p, c->ph_grid.evec.p,
+                                                   reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
+        SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+        k_tc_tab_b<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
+                                                   c->d_qpnt.p, c->ph_grid.evec.p,
+                                                   reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
+        SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+        k_tc_q0tab<<<std::max(1, std::min((c->nq0 * NMODE + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
+            c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p,
+            reinterpret_cast<Q0Rec*>(c->d_tc_q0.p));
+        SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
+        k_tc_modes<<<(int)std::min<long long>(((long long)nq * NMODE * rs + threads - 1) / threads, 148LL * 8), threads, 0,
+                     c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p,
+                                  c->d_tc_modes.p);
+        SPRING_CHECK(launch_check(c, "k_tc_modes"));
+        return SPRING_OK;
+    };
+    cudaStream_t main_stream = c->stream;
+    c->stream = c->stream2;  // launches (and their profiling events) go to the side stream
+    const int trc = tables();
+    c->stream = main_stream;
+    {
+        const cudaError_t e = cudaEventRecord(c->ev_join, c->stream2);
+        if (trc != SPRING_OK) {
+            cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+            return trc;
+        }
+        if (e != cudaSuccess) return cuda_fail(c, e, "side stream join");
+    }
+    int brc = build_tiles_begin(c, q0_first, n_q0, nmax, rf);
+    if (brc == SPRING_OK) brc = build_tiles_end(c);  // the tile count was read while the tables ran
+    {
+        const cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);  // join the tables
+        if (brc != SPRING_OK) return brc;
+        if (e != cudaSuccess) return cuda_fail(c, e, "side stream join");
+    }
     if (c->tc_ntiles == 0) return SPRING_OK;  // no pair has a mode triple inside the window
 
     TcArgs a{};

@@ -89,6 +89,8 @@ struct spring_ctx {
     int* h_pin = nullptr;              // pinned host scratch for readbacks that overlap queued work
     size_t h_pin_n = 0;                // its size in ints
     cudaEvent_t ev_aux = nullptr;      // marks the end of such a readback
+    cudaStream_t stream2 = nullptr;    // side stream for work that overlaps the main stream's
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
     int precision = SPRING_FP64;
