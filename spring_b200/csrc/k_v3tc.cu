@@ -625,15 +625,18 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
             // Positions in this warp's region (exclusive prefix of the lanes' counts), release the
             // stage (every read of it is done), then each lane writes its own active triples.
+            // counts are at most 12: four bit-plane ballots give the exclusive prefix and the total
             const int cnt = __popc(act);
-            int incl = cnt;
+            const unsigned lt = (1u << lane) - 1u;
+            int pre = 0, tot = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int v = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += v;
+            for (int bp = 0; bp < 4; ++bp) {
+                const unsigned bal = __ballot_sync(0xffffffffu, (cnt >> bp) & 1);
+                pre += __popc(bal & lt) << bp;
+                tot += __popc(bal) << bp;
             }
-            int pos = base + incl - cnt;
-            base += __shfl_sync(0xffffffffu, incl, 31);
+            int pos = base + pre;
+            base += tot;
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
