@@ -69,8 +69,8 @@ BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
 TC_EPT = 16         # pairs per tensor-core tile
 # DRAM bytes per tiled pair of the tensor-core pass (read + write), from one ncu capture of the
 # 16^3 rocksalt launch (140,383 of its 297,076 pairs have a mode triple inside the delta window and
-# are tiled; 61.6 MB read, 16.9 MB written)
-TC_DRAM_BYTES_PER_TILED_PAIR = (61.563904e6 + 16.864768e6) / 140383
+# are tiled; 61.7 MB read, 17.9 MB written)
+TC_DRAM_BYTES_PER_TILED_PAIR = (61.688320e6 + 17.917696e6) / 140383
 
 
 def tc_issued_flops_per_tile(passes):
