@@ -227,7 +227,7 @@ int spring_set_precision(spring_ctx* ctx, int precision);
 /* No counterpart in the reference, which evaluates every four-phonon rate
  * exactly.  A 5 -> 128 -> 128 -> 128 -> 1 network (SiLU) that maps per-mode
  * harmonic features to the log four-phonon rate, trained and evaluated on the
- * device; the exact spring_linewidth4 stays the judge of its error.
+ * device; its error is measured against the exact spring_linewidth4.
  * X(SPRING_MLP_INPUTS, n) features (standardised by the caller), y(n) targets.
  * Parameters: one FP32 vector of SPRING_MLP_PARAMS values, W1 (128x5 row-major),
  * b1, W2 (128x128), b2, W3, b3, W4 (1x128), b4. */

@@ -2,7 +2,7 @@
 // SiLU after every hidden layer, trained on the device in FP32 with Adam on a
 // mean-squared-error loss, evaluated in FP32 or with BF16-rounded weights and
 // activations.  No counterpart in the reference (which computes every
-// four-phonon rate exactly); the exact path stays the judge of its error.
+// four-phonon rate exactly); its error is measured against the exact path.
 //
 // Kernels: a tiled FP32 GEMM C = op(A) op(B) (+ bias) used for the forward pass
 // (Z = A W^T + b), the weight gradients (dZ^T A) and the backpropagated

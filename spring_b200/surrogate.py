@@ -7,8 +7,8 @@ mesh, predicts per-mode four-phonon rates from harmonic features; the
 irreducible q0 blocks (all quartets of one q0) are ranked by the predicted
 effect of their four-phonon scattering on kappa, the exact path
 (``spring_linewidth4``) runs for the top fraction, and the prediction stands in
-for the rest.  The exact path is both the fallback (fraction 1) and the judge of
-the surrogate's error.
+for the rest.  The exact path is both the fallback (fraction 1) and the measure
+of the surrogate's error.
 
 Features of a mode: omega (rad/ps), |group velocity| (m/s), its 3-phonon
 scattering rate (2 x linewidth), branch index, |q| (1/A).  Target: log of the

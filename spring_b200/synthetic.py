@@ -19,7 +19,7 @@ axes reversed, so the flat memory is identical to the Fortran array):
 * ``atm_indx`` Fortran ``atmIndx(4, Na, Nb)`` -> numpy ``(Nb, Na, 4)``: integer
   lattice cell ``(R1, R2, R3)`` and the 1-based basis index of the neighbour.
 
-Spring model (the BASELINE crystal "fcc rocksalt, 1st+2nd neighbour
+Spring model (the benchmark crystal "fcc rocksalt, 1st+2nd neighbour
 central/tangential springs k1=8, k2=1.5 eV/A^2"): for a bond with unit vector
 ``r`` the pair force constant is ``-(kc r r^T + kt (1 - r r^T))``.  The
 tangential constant is not pinned by the workload description; this generator
@@ -231,7 +231,7 @@ def make_fc4(cr: Crystal, sigma=5.0, seed=SEED_FC4, iters=200) -> None:
 
 
 def build(name: str = "rocksalt2", fc4: bool = False, seeds=(SEED_FC2, SEED_FC3, SEED_FC4)) -> Crystal:
-    """The BASELINE crystals: ``rocksalt2`` (Ndof 6) or ``rocksalt8`` (Ndof 24)."""
+    """The benchmark crystals: ``rocksalt2`` (Ndof 6) or ``rocksalt8`` (Ndof 24)."""
     cr = rocksalt_primitive() if name == "rocksalt2" else rocksalt_cubic()
     make_fc2(cr, seed=seeds[0])
     make_fc3(cr, seed=seeds[1])

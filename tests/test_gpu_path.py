@@ -57,7 +57,7 @@ def test_linewidth_path_matches_oracle(setup, delta):
 
 
 def test_linewidth_path_high_symmetry_runs(setup):
-    """The BASELINE path Gamma-X-W-K-Gamma-L: finite, non-negative, degenerate-insensitive sums close."""
+    """The benchmark path Gamma-X-W-K-Gamma-L: finite, non-negative, degenerate-insensitive sums close."""
     st, ctx = setup
     q, _, z = ctx.path_qpoints(HIGHSYM)
     lw, om = ctx.linewidth_path(q, z, delta="tetra")
