@@ -158,14 +158,18 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
         const int half = i % 2, t = i / 2, al = t / KR, k2 = t % KR;  // k2 = N2*3 + c
         const int N2 = k2 / 3, ga = k2 % 3;
         double zr[3] = {0.0, 0.0, 0.0}, zi[3] = {0.0, 0.0, 0.0};
-        for (int k1 = 0; k1 < KR; ++k1) {
-            const int N1 = k1 / 3, be = k1 % 3;
-            const double fv = sF[(N1 * na + N2) * 27 + (al * 3 + be) * 3 + ga];
+        for (int N1 = 0; N1 < na; ++N1) {  // k1 = N1*3 + b in order
+            const double* f = sF + (N1 * na + N2) * 27 + al * 9 + ga;
+            const double2* u1 = sU + N1 * 3 * NMODE + half * 3;
 #pragma unroll
-            for (int j = 0; j < 3; ++j) {
-                const double2 u = sU[k1 * NMODE + half * 3 + j];
-                zr[j] = fma(fv, u.x, zr[j]);
-                zi[j] = fma(fv, u.y, zi[j]);
+            for (int be = 0; be < 3; ++be) {
+                const double fv = f[be * 3];
+#pragma unroll
+                for (int j = 0; j < 3; ++j) {
+                    const double2 u = u1[be * NMODE + j];
+                    zr[j] = fma(fv, u.x, zr[j]);
+                    zi[j] = fma(fv, u.y, zi[j]);
+                }
             }
         }
 #pragma unroll
