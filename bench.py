@@ -66,7 +66,6 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
 
 
 BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
-TC_EPT = 16         # pairs per tensor-core tile
 # DRAM bytes per tiled pair of the tensor-core pass (read + write), from one ncu capture of the
 # 16^3 rocksalt launch (140,383 of its 297,076 pairs have a mode triple inside the delta window and
 # are tiled; 61.7 MB read, 17.9 MB written)
