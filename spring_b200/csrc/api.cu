@@ -504,7 +504,7 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc3.p, t.data(), sizeof(double) * t.size(), "FC3"));
     SPRING_CHECK(h2d(c, c->d_fc3_posr.p, posr.data(), sizeof(double) * posr.size(), "FC3 positions"));
     SPRING_CHECK(h2d(c, c->d_fc3_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC3 basis"));
-    SPRING_CHECK(spring_synchronize(c));
+    // no stream wait: the copies read only this call's own host arrays, staged when queued
     c->fc3_set = true;
     dfree(c->d_wtr);  // cached W grids depend on FC3
     return SPRING_OK;
@@ -554,7 +554,7 @@ int spring_set_fc4(spring_ctx* c, int na4, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc4_posr.p, posr.data(), sizeof(double) * posr.size(), "FC4 positions"));
     SPRING_CHECK(h2d(c, c->d_fc4_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC4 basis"));
     SPRING_CHECK(h2d(c, c->d_fc4_off.p, off.data(), sizeof(int) * off.size(), "FC4 slot offsets"));
-    SPRING_CHECK(spring_synchronize(c));
+    // no stream wait: the copies read only this call's own host arrays, staged when queued
     c->fc4_set = true;
     return SPRING_OK;
 }
@@ -577,7 +577,7 @@ int spring_make_mesh(spring_ctx* c, const int* shift, int zero_centered, int* q_
         SPRING_CHECK(d2h(c, t.data(), c->d_tetra.p, sizeof(int) * nq * 24, "tetrahedrons"));
         for (size_t i = 0; i < t.size(); ++i) tetrahedrons[i] = t[i] + 1;
     }
-    SPRING_CHECK(spring_synchronize(c));
+    // no stream wait: the mesh kernels are queued like any other, and each requested readback waits
     c->mesh_set = true;
     c->mesh_zc = zero_centered != 0;
     // the time-reversal lists depend only on the mesh dimensions (fixed per context): kept
@@ -610,7 +610,7 @@ static int install_irr(spring_ctx* c, int nq0, const int* irr_int, const int* po
     SPRING_CHECK(h2d(c, c->d_pos.p, pos, sizeof(int) * c->nq, "pos"));
     SPRING_CHECK(dalloc(c, c->d_lw_all, (size_t)c->nT * nq0 * c->ndof, "LW_Allq0"));
     SPRING_CHECK(zero(c, c->d_lw_all.p, sizeof(double) * c->nT * nq0 * c->ndof, "LW_Allq0"));
-    SPRING_CHECK(spring_synchronize(c));
+    // no stream wait: the copies read only this call's own host arrays, staged when queued
     c->irr_set = true;
     c->ps_irr.done = false;
     c->ps_irr.n0 = nq0;
