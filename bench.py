@@ -65,7 +65,41 @@ def algorithmic_flops_per_pair(ndof, na3_counts):
     return 4 * 27 * int(np.sum(np.asarray(na3_counts) ** 2)) + 3 * 8 * ndof ** 4 + 3 * ndof ** 3
 
 
-BF16_PEAK = 1604.5  # TFLOP/s, MEASURED_PEAKS.json bf16_tflops
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}  # the pool's earlier measurement
+
+
+def measured_peaks():
+    """Roofline denominators: the driver-written MEASURED_PEAKS.json beside this file when present
+    ("of measured"), else the pool's earlier measurement ("of fallback")."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        flat = {}
+
+        def walk(x, pre=""):
+            if isinstance(x, dict):
+                for k, v in x.items():
+                    walk(v, f"{pre}{k}.")
+            elif isinstance(x, (int, float)) and not isinstance(x, bool):
+                flat[pre[:-1]] = float(x)
+        walk(d)
+
+        def pick(*keys):
+            for k in keys:
+                for fk, v in flat.items():
+                    if fk == k or fk.endswith("." + k):
+                        return v
+            return None
+        bf = pick("bf16_tflops", "bf16_dense_tflops")
+        hbm = pick("hbm_gbs", "hbm_copy_gbs")
+        if bf:
+            return {"bf16_tflops": bf, "hbm_gbs": hbm or FALLBACK_PEAKS["hbm_gbs"],
+                    "source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM), of measured"}
+    except (OSError, ValueError):
+        pass
+    return dict(FALLBACK_PEAKS, source="no MEASURED_PEAKS.json: the pool's earlier 1.59 PFLOP/s bf16, of fallback")
+
 # DRAM bytes per tiled pair of the tensor-core pass (read + write), from one ncu capture of the
 # 16^3 rocksalt launch (140,383 of its 297,076 pairs have a mode triple inside the delta window and
 # are tiled; 61.7 MB read, 17.9 MB written)
@@ -201,9 +235,10 @@ def fp64_peak_tflops(torch):
     return best
 
 
-def cpu_baseline(cr, mesh, temps, ph_grid, ph_irr, irr_int, sample, threads_note):
+def cpu_baseline(cr, mesh, temps, ph_grid, ph_irr, irr_int, sample, threads_note, lw_out=None):
     """The oracle (CPU restatement of the reference loops) on a sample of q0: enumeration,
-    naive V3 (ScatterMatEl loop order) and the Gaussian sum at every temperature."""
+    naive V3 (ScatterMatEl loop order) and the Gaussian sum at every temperature.  lw_out (a
+    dict) receives the oracle linewidths of each sampled q0, [T][s]."""
     from oracle import driver as D
     qi, qf, _ = D.make_tetrahedron(mesh, cr.G)
     evals = 0
@@ -212,8 +247,12 @@ def cpu_baseline(cr, mesh, temps, ph_grid, ph_irr, irr_int, sample, threads_note
         A, perm, cnt = D.momentum3(mesh, qi, irr_int[i0])
         sctr = D.scatter_w3(cr, qf, qi, irr_int[i0], ph_irr["evec"][i0], ph_irr["onebyomega"][i0], ph_grid["evec"],
                             ph_grid["onebyomega"], perm)
+        lws = []
         for it in range(len(temps)):
-            D.lw3_gauss(ph_irr["omega"][i0], ph_grid["omega"], ph_grid["nbe"][it], sctr, A, qi, SIGMA)
+            r = D.lw3_gauss(ph_irr["omega"][i0], ph_grid["omega"], ph_grid["nbe"][it], sctr, A, qi, SIGMA)
+            lws.append(np.asarray(r[0] if isinstance(r, tuple) else r))
+        if lw_out is not None:
+            lw_out[i0] = np.array(lws)
         evals += cnt[0] * cr.ndof ** 3
     dt = time.perf_counter() - t0
     return evals / dt, dt, D.lib().orc_num_threads()
@@ -259,15 +298,6 @@ def run_reference(args):
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
-
-
-def partition(counts, world, rank):
-    """Contiguous q0 block of this rank, balanced by pair count (DistributeQpoints balanced by cost)."""
-    c = np.cumsum(counts)
-    tot = c[-1]
-    lo = 0 if rank == 0 else int(np.searchsorted(c, tot * rank / world, side="right"))
-    hi = len(counts) if rank == world - 1 else int(np.searchsorted(c, tot * (rank + 1) / world, side="right"))
-    return lo, hi
 
 
 def fourph_leg(torch, mesh4, frac=0.1):
@@ -409,6 +439,7 @@ def batched_leg(torch, steps=3):
 def run_ours(args):
     import torch
     import torch.distributed as dist
+    from spring_b200 import distributed as DD
     from spring_b200 import synthetic as S
     from spring_b200.api import Context
 
@@ -436,7 +467,7 @@ def run_ours(args):
     ctx.compute_phonons(TEMPS)
     enum = [ctx.enumerate3(i + 1) for i in range(nq0)]
     counts = np.array([e[2][0] for e in enum])
-    lo, hi = partition(counts, world, rank)
+    lo, hi = DD.partition_by_cost(counts, world, rank)
     my_pairs = int(counts[lo:hi].sum())
     del enum
     evals_total = int(counts.sum()) * cr.ndof ** 3
@@ -451,9 +482,7 @@ def run_ours(args):
         if hi > lo:
             ctx.linewidth3(lo + 1, hi - lo, delta=DELTA, sigma=SIGMA, want=False)
         if world > 1:
-            lw = torch.from_numpy(ctx.get_linewidths()).to(dev)
-            dist.all_reduce(lw)
-            ctx.set_linewidths(lw.cpu().numpy())
+            ctx.set_linewidths(DD.allreduce_linewidths(ctx.get_linewidths()[:, lo:hi], lo, hi, nq0, device=dev))
         ctx.kappa_rta(Rxyz, want=False)
 
     def timed(prec, clocks=None):
@@ -535,11 +564,7 @@ def run_ours(args):
             if hi > lo:
                 ctx.linewidth3(lo + 1, hi - lo, delta=DELTA, sigma=SIGMA, out=h_lw)
             if world > 1:
-                lw = torch.zeros(len(TEMPS), nq0, cr.ndof, dtype=torch.float64)
-                lw[:, lo:hi] = torch.from_numpy(h_lw[:, : hi - lo])
-                lw = lw.to(dev)
-                dist.all_reduce(lw)
-                ctx.set_linewidths(lw.cpu().numpy())
+                ctx.set_linewidths(DD.allreduce_linewidths(h_lw[:, : hi - lo], lo, hi, nq0, device=dev))
             ctx.kappa_rta(Rxyz, out=h_kap)
 
         ctx.set_precision(args.precision)
@@ -566,13 +591,31 @@ def run_ours(args):
     four = fourph_leg(torch, args.mesh4) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
     batched = batched_leg(torch) if (rank == 0 and world == 1 and not args.no_batch) else None
     cpu = None
+    oracle_check = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         ph_grid, ph_irr = ctx.get_phonons(0), ctx.get_phonons(1)
         sample = [1, nq0 // 2, nq0 - 1]
-        v, dt, thr = cpu_baseline(cr, mesh, TEMPS, ph_grid, ph_irr, irr["irr_q_pnt_int"], sample, "")
+        lw_orc = {}
+        v, dt, thr = cpu_baseline(cr, mesh, TEMPS, ph_grid, ph_irr, irr["irr_q_pnt_int"], sample, "", lw_orc)
         cpu = {"value": v, "unit": "evals/s", "cores": thr, "kind": "port",
                "sample": f"{len(sample)} of {nq0} irreducible q0: enumeration, V3 in the reference loop order, "
                          f"Gaussian sum at 3 T; phonons excluded ({dt:.1f} s)"}
+        # parity at the full size: the measured path's and the FP64 path's linewidths of the sampled q0
+        # against the oracle's (same device phonons), every mode above 1e-3 of the q0's largest
+        def max_rel(lw_gpu):
+            e = 0.0
+            for i0, ref in lw_orc.items():
+                g = lw_gpu[:, i0 - lo] if lo <= i0 < hi else None
+                if g is None:
+                    continue
+                big = ref > 1e-3 * ref.max()
+                e = max(e, float((np.abs(g[big] - ref[big]) / ref[big]).max()))
+            return e
+        oracle_check = {"q0": [int(i) for i in sample], "mesh": list(mesh),
+                        "lw_max_rel_err_measured_path": max_rel(lw_p),
+                        "lw_max_rel_err_fp64_path": max_rel(lw64),
+                        "what": "GPU linewidths of these irreducible q0 at every temperature against the oracle "
+                                "(CPU restatement of the reference loops, FP64) on the device phonons"}
     if rank == 0:
         value = evals_total / (ms * 1e-3)
         v3_per_launch = v3_ms / max(v3_n, 1)
@@ -589,11 +632,13 @@ def run_ours(args):
             sec = v3_per_launch * 1e-3
             achieved = algo / sec / 1e12 if v3_n else None
             ev_ms, ev_n = kt["k_v3tc_eval"]
+            pk = measured_peaks()
             roof = {"kernel": f"k_v3tc<{args.precision}>", "bound": "tensor", "achieved": achieved,
-                    "peak": BF16_PEAK, "unit": "TFLOP/s", "frac": (achieved / BF16_PEAK) if achieved else None,
+                    "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+                    "frac": (achieved / pk["bf16_tflops"]) if achieved else None,
                     "traffic": TC_DRAM_BYTES_PER_TILED_PAIR * tc_pairs_run,
                     "pairs_tiled": tc_pairs_run, "tiles": tc_tiles_run, "pairs_all": my_pairs,
-                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst, cuBLAS bf16 GEMM) of measured",
+                    "peak_source": pk["source"],
                     "algorithmic_flops_per_launch": algo,
                     "issued_mma_tflops": issued / sec / 1e12 if v3_n else None,
                     "issued_flops_per_launch": issued,
@@ -628,6 +673,7 @@ def run_ours(args):
                 "batched": batched,
                 "roofline": roof,
                 "cpu_baseline": cpu,
+                "oracle_check_24": oracle_check,
                 "e2e": {"value": evals_total / (e2e_ms * 1e-3), "unit": "evals/s", "ms_per_step": e2e_ms,
                         "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
                 "gpu_launches": int(launches),

@@ -38,6 +38,7 @@ typedef struct spring_ctx spring_ctx;
 #define SPRING_ERR_ALLOC 4       /* device allocation failed */
 #define SPRING_ERR_UNSUPPORTED 5 /* valid request this build does not handle */
 #define SPRING_ERR_INJECTED 6    /* failure injected by spring_debug_inject_fault */
+#define SPRING_ERR_TIMEOUT 7     /* a bounded device-side wait ran out; the kernel stopped, the context stays usable */
 
 /* delta-function schemes */
 #define SPRING_DELTA_GAUSS 0 /* Gaussian smearing, ThirdOrder_m.f90:442-543 */
@@ -311,6 +312,12 @@ int spring_batch_result(spring_batch* batch, int index, double* lw, double* p3_q
 /* SPRING_OPT_GENERIC_V3 = 1: always use the any-cell V3 kernel (default 0 picks the
  * two-atom specialisation when the cell fits it; both give the same W). */
 #define SPRING_OPT_GENERIC_V3 1
+/* SPRING_OPT_WAIT_POLLS = 2: poll limit of each wait of one warp on another inside the
+ * tensor-core kernels (value >= 0; a negative value restores the default, 2^26).  When a wait
+ * runs out, the kernel drains the copies and MMAs it issued, releases its shared and tensor
+ * memory and returns; the call fails with SPRING_ERR_TIMEOUT.  For testing callers' handling
+ * of that status: 0 makes every such wait run out at once. */
+#define SPRING_OPT_WAIT_POLLS 2
 int spring_set_option(spring_ctx* ctx, int option, int value);
 
 /* ---- diagnostics ------------------------------------------------------- */
@@ -320,6 +327,9 @@ int spring_set_profiling(spring_ctx* ctx, int on);
 /* Device time (ms) and launch count of the recorded launches whose kernel
  * name starts with `prefix` (e.g. "k_v3"); synchronizes the stream. */
 int spring_kernel_time(spring_ctx* ctx, const char* prefix, double* ms, long long* launches);
+/* Binary architecture of this library's kernels as the runtime loaded them on `device`
+ * (cudaFuncGetAttributes binaryVersion: 100 for sm_100a).  No reference counterpart. */
+int spring_binary_version(int device, int* version);
 /* Pairs and 16-pair tiles of the last tensor-core linewidth pass (the pairs with a mode
  * triple inside the delta window); 0 and 0 before one ran.  No reference counterpart. */
 int spring_tc_stats(const spring_ctx* ctx, int* n_tiles, int* n_pairs);

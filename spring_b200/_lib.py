@@ -18,6 +18,9 @@ SPRING_ERR_CUDA = 3
 SPRING_ERR_ALLOC = 4
 SPRING_ERR_UNSUPPORTED = 5
 SPRING_ERR_INJECTED = 6
+SPRING_ERR_TIMEOUT = 7
+SPRING_OPT_GENERIC_V3 = 1
+SPRING_OPT_WAIT_POLLS = 2
 SPRING_DELTA_GAUSS = 0
 SPRING_DELTA_TETRA = 1
 SPRING_FP64 = 0
@@ -66,6 +69,7 @@ SIGNATURES = {
     "spring_kappa_iter": [P, D, I, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_tc_stats": [P, P, P],
+    "spring_binary_version": [I, P],
     "spring_scatter_w3": [P, I, P],
     "spring_linewidth3": [P, I, I, I, D, P, P, P],
     "spring_linewidth_iso": [P, I, I, I, D, P, P],

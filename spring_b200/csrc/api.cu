@@ -63,10 +63,45 @@ int dalloc_bytes(spring_ctx* c, void** p, size_t bytes, const char* what) {
     return SPRING_OK;
 }
 
+// Host -> device copy of `bytes` at `src`.  The bytes are first copied on the CPU into the context's
+// pinned staging ring and the asynchronous copy reads them from there, so the caller's memory (and
+// any temporary of the library) may be reused as soon as this returns, whatever kind of host memory
+// it is, and the copy never waits for the stream.  Ring bytes are overwritten only once every copy
+// queued from them has completed (ev_stage, recorded behind each staged copy).
 int h2d(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
     if (injected(c, 1)) return fail(c, SPRING_ERR_INJECTED, "%s: injected copy failure", what);
-    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream);
-    return e == cudaSuccess ? SPRING_OK : cuda_fail(c, e, what);
+    if (bytes == 0) return SPRING_OK;
+    if (!c->ev_stage) {
+        cudaError_t e = cudaEventCreateWithFlags(&c->ev_stage, cudaEventDisableTiming);
+        if (e != cudaSuccess) return cuda_fail(c, e, what);
+    }
+    const size_t need = (bytes + 255) & ~(size_t)255;
+    if (c->h_stage_off + need > c->h_stage_cap) {
+        // wrap (or grow): every copy queued from the ring must have read its bytes first
+        if (c->stage_pending) {
+            cudaError_t e = cudaEventSynchronize(c->ev_stage);
+            if (e != cudaSuccess) return cuda_fail(c, e, what);
+            c->stage_pending = false;
+        }
+        c->h_stage_off = 0;
+        if (need > c->h_stage_cap) {
+            if (c->h_stage) cudaFreeHost(c->h_stage);
+            c->h_stage = nullptr;
+            c->h_stage_cap = 0;
+            const size_t cap = std::max<size_t>(need, (size_t)4 << 20);
+            cudaError_t e = cudaHostAlloc((void**)&c->h_stage, cap, cudaHostAllocDefault);
+            if (e != cudaSuccess) return cuda_fail(c, e, what);
+            c->h_stage_cap = cap;
+        }
+    }
+    char* st = c->h_stage + c->h_stage_off;
+    std::memcpy(st, src, bytes);
+    c->h_stage_off += need;
+    cudaError_t e = cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(c->ev_stage, c->stream);
+    if (e != cudaSuccess) return cuda_fail(c, e, what);
+    c->stage_pending = true;
+    return SPRING_OK;
 }
 
 int d2h(spring_ctx* c, void* dst, const void* src, size_t bytes, const char* what) {
@@ -197,7 +232,7 @@ int set_temps(spring_ctx* c, const double* temps) {
     if (!temps) return fail(c, SPRING_ERR_ARG, "temps is NULL");
     for (int i = 0; i < c->nT; ++i)
         if (!(temps[i] > 0.0)) return fail(c, SPRING_ERR_ARG, "temperature %d is not positive", i + 1);
-    // unchanged temperatures are not copied again (a copy from pageable memory may wait for the stream)
+    // unchanged temperatures are not copied again
     if (c->d_temps.p && c->temps.size() == (size_t)c->nT && std::equal(temps, temps + c->nT, c->temps.begin()))
         return SPRING_OK;
     c->temps.assign(temps, temps + c->nT);
@@ -298,7 +333,13 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_tc_seg); dfree(c->d_tc_ntl); dfree(c->d_tc_toff); dfree(c->d_tc_sort);
         dfree(c->d_scan_tmp); dfree(c->d_w); dfree(c->d_lw_all); dfree(c->d_lw_tmp); dfree(c->d_p3);
         dfree(c->d_kappa); dfree(c->d_krn); dfree(c->d_rxyz); dfree(c->d_wiso);
+        free_enum4(c);
+        dfree(c->d_v4_ph); dfree(c->d_v4_etab); dfree(c->d_v4_wf); dfree(c->d_v4_c); dfree(c->d_v4_map);
+        dfree(c->d_v4_img); dfree(c->d_v4_cnt); dfree(c->d_v4_seg); dfree(c->d_v4_ntl); dfree(c->d_v4_toff);
+        dfree(c->d_v4_stat); dfree(c->d_v4_tiles);
         if (c->h_pin) cudaFreeHost(c->h_pin);
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        if (c->ev_stage) cudaEventDestroy(c->ev_stage);
         if (c->ev_aux) cudaEventDestroy(c->ev_aux);
         if (c->ev_fork) cudaEventDestroy(c->ev_fork);
         if (c->ev_join) cudaEventDestroy(c->ev_join);
@@ -329,6 +370,22 @@ int spring_kernel_launches(const spring_ctx* c, long long* count) {
     return SPRING_OK;
 }
 
+int spring_binary_version(int device, int* version) {
+    if (!version) return SPRING_ERR_ARG;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(device);
+    cudaFuncAttributes fa{};
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_sum2);
+    if (prev >= 0) cudaSetDevice(prev);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return SPRING_ERR_CUDA;
+    }
+    *version = fa.binaryVersion;
+    return SPRING_OK;
+}
+
 int spring_tc_stats(const spring_ctx* c, int* n_tiles, int* n_pairs) {
     if (!c || !n_tiles || !n_pairs) return SPRING_ERR_ARG;
     const bool valid = c->tc_gen >= 0;
@@ -350,6 +407,7 @@ int spring_set_option(spring_ctx* c, int option, int value) {
     CTX_ENTER(c);
     switch (option) {
         case SPRING_OPT_GENERIC_V3: c->force_generic_v3 = value != 0; return SPRING_OK;
+        case SPRING_OPT_WAIT_POLLS: c->tc_max_spins = value < 0 ? -1 : (long long)value; return SPRING_OK;
         default: return fail(c, SPRING_ERR_ARG, "unknown option %d", option);
     }
 }
@@ -449,7 +507,6 @@ int spring_set_fc2(spring_ctx* c, int na2, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc2.p, fc, sizeof(double) * c->nb * na2 * 9, "FC2"));
     SPRING_CHECK(h2d(c, c->d_fc2_idx.p, idx, sizeof(int) * c->nb * na2 * 4, "FC2 index"));
     SPRING_CHECK(h2d(c, c->d_fc2_num.p, num, sizeof(int) * c->nb, "FC2 counts"));
-    SPRING_CHECK(spring_synchronize(c));
     c->fc2_set = true;
     return SPRING_OK;
 }
@@ -504,7 +561,7 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc3.p, t.data(), sizeof(double) * t.size(), "FC3"));
     SPRING_CHECK(h2d(c, c->d_fc3_posr.p, posr.data(), sizeof(double) * posr.size(), "FC3 positions"));
     SPRING_CHECK(h2d(c, c->d_fc3_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC3 basis"));
-    // no stream wait: the copies read only this call's own host arrays, staged when queued
+    // no stream wait: h2d staged every byte in the context's pinned ring before queuing its copy
     c->fc3_set = true;
     dfree(c->d_wtr);  // cached W grids depend on FC3
     return SPRING_OK;
@@ -554,7 +611,7 @@ int spring_set_fc4(spring_ctx* c, int na4, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc4_posr.p, posr.data(), sizeof(double) * posr.size(), "FC4 positions"));
     SPRING_CHECK(h2d(c, c->d_fc4_btyp.p, btyp.data(), sizeof(int) * btyp.size(), "FC4 basis"));
     SPRING_CHECK(h2d(c, c->d_fc4_off.p, off.data(), sizeof(int) * off.size(), "FC4 slot offsets"));
-    // no stream wait: the copies read only this call's own host arrays, staged when queued
+    // no stream wait: h2d staged every byte in the context's pinned ring before queuing its copy
     c->fc4_set = true;
     return SPRING_OK;
 }
@@ -610,7 +667,7 @@ static int install_irr(spring_ctx* c, int nq0, const int* irr_int, const int* po
     SPRING_CHECK(h2d(c, c->d_pos.p, pos, sizeof(int) * c->nq, "pos"));
     SPRING_CHECK(dalloc(c, c->d_lw_all, (size_t)c->nT * nq0 * c->ndof, "LW_Allq0"));
     SPRING_CHECK(zero(c, c->d_lw_all.p, sizeof(double) * c->nT * nq0 * c->ndof, "LW_Allq0"));
-    // no stream wait: the copies read only this call's own host arrays, staged when queued
+    // no stream wait: h2d staged every byte in the context's pinned ring before queuing its copy
     c->irr_set = true;
     c->ps_irr.done = false;
     c->ps_irr.n0 = nq0;
@@ -691,7 +748,6 @@ int spring_set_phonons(spring_ctx* c, int which, const double* temps, const doub
     SPRING_CHECK(h2d(c, p.oneby.p, oneby, sizeof(double) * n * nd, "1/omega"));
     SPRING_CHECK(h2d(c, p.nbe.p, nbe, sizeof(double) * c->nT * n * nd, "nBE"));
     SPRING_CHECK(h2d(c, p.vel.p, vel, sizeof(double) * n * nd * 3, "group velocity"));
-    SPRING_CHECK(spring_synchronize(c));
     p.set = true;
     c->ph_gen += 1;
     if (which == 0) dfree(c->d_wtr);  // cached W grids depend on the grid phonons
@@ -866,7 +922,15 @@ int spring_linewidth4(spring_ctx* c, int i0_first, int n_q0, int delta_mode, dou
     const size_t nl = (size_t)c->nT * c->nq0 * c->ndof;
     SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
     SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
-    SPRING_CHECK(run_lw4(c, q0, n_q0, delta_mode, sigma, pol4, c->d_lw_tmp.p));
+    // Tensor cores (spring_set_precision BF16 / BF16x3) for the Gaussian rate of two-atom cells over
+    // every branch; otherwise (and for the tetrahedron form) the FP64 kernels.
+    bool handled = false;
+    bool all_modes = true;
+    if (pol4)
+        for (int k = 0; k < 4; ++k) all_modes = all_modes && pol4[2 * k] == 1 && pol4[2 * k + 1] == c->ndof;
+    if (delta_mode == SPRING_DELTA_GAUSS && all_modes)
+        SPRING_CHECK(run_v4tc_gauss(c, q0, n_q0, sigma, c->d_lw_tmp.p, &handled));
+    if (!handled) SPRING_CHECK(run_lw4(c, q0, n_q0, delta_mode, sigma, pol4, c->d_lw_tmp.p));
     SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
     SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
     return SPRING_OK;

@@ -578,6 +578,25 @@ int run_enumerate4_fortran(spring_ctx* c, int q0, int* d_all, int* d_perm, long 
     return rc;
 }
 
+// Quartet list of q0 (0-based) in buffers kept by the context: (g1, g2, g3, 0) sorted by (g1, g2).
+int run_enum4_list(spring_ctx* c, int q0, const int4** d_quart, long long* nquart) {
+    if (!c->e4) c->e4 = new Enum4Bufs();
+    Enum4Bufs& b = *static_cast<Enum4Bufs*>(c->e4);
+    long long cnt[2] = {0, 0};
+    SPRING_CHECK(enumerate4(c, q0, b, false, nullptr, 0, cnt));
+    *d_quart = b.quart.p;
+    *nquart = cnt[0];
+    return SPRING_OK;
+}
+
+void free_enum4(spring_ctx* c) {
+    if (!c->e4) return;
+    Enum4Bufs* b = static_cast<Enum4Bufs*>(c->e4);
+    free4(*b);
+    delete b;
+    c->e4 = nullptr;
+}
+
 int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const int* pol4, double* d_rate) {
     if (c->nb != NB || c->na4 > NA_MAX || c->nT > 9)
         return fail(c, SPRING_ERR_UNSUPPORTED, "four-phonon path handles two-atom cells, Na4 <= %d, <= 9 temperatures",

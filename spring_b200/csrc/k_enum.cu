@@ -59,7 +59,9 @@ __global__ void k_enum3_flags(int nq, int nq0, int n0, int n1, int n2, const int
     }
 }
 
-// Pairs beyond `cap` are not written (the host compares pairoff[nq0] with cap and re-runs).
+// Pairs beyond `cap` are not written.  cap is the proven bound (at most Nq/2 + 8 pairs per q0), so
+// nothing is dropped; pairoff_host fails with an error if the total ever exceeded it, and kernels
+// that read their pair range on the device clamp it to cap.
 __global__ void k_enum3_pairs(int nq, int nq0, int cap, const int* __restrict__ partner, const int* __restrict__ rep,
                               const int* __restrict__ pos, int2* __restrict__ pairs, int* __restrict__ pair_q0,
                               int* __restrict__ pairoff) {

@@ -29,17 +29,26 @@
 //          Sctrq1(s2,s1,s0,q) for every grid q, for the tetrahedron integration.
 // Roofline: FP64 FMA pipe; inputs per pair are two eigenvector sets (2 Ndof^2
 // complex, L2-resident), outputs a few atomics (GAUSS) or 2 Ndof^3 doubles (WGRID).
+#include <algorithm>
+
 #include "v3item.cuh"
 
 namespace spring {
 namespace {
 
+// range != null: the pair range is read on the device, pairs range[0] .. range[n_q0] (clamped to
+// the list's capacity); the grid then covers the bound and CTAs past the range return at once.
 template <int EPI>
-__global__ void __launch_bounds__(128) k_v3(V3Args a_, V3Ptrs P_) {
+__global__ void __launch_bounds__(128) k_v3(V3Args a_, V3Ptrs P_, const int* __restrict__ range, int n_q0, int cap) {
     extern __shared__ double2 smem2[];
-    const V3Args a = a_;  // local copies: the device function takes references
+    V3Args a = a_;  // local copies: the device function takes references
     const V3Ptrs P = P_;
     const int work = blockIdx.x;
+    if (range) {
+        a.pair_first = min(range[0], cap);
+        const int pr = a.pair_first + work / a.nsb;
+        if (pr >= min(range[n_q0], cap)) return;
+    }
     v3_item<EPI>(a, P, a.pair_first + work / a.nsb, (work % a.nsb) * a.sb, smem2);
 }
 
@@ -56,20 +65,28 @@ int launch_v3(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, i
     a.sb = v3_block(c->ndof);
     a.nsb = (c->ndof + a.sb - 1) / a.sb;
     a.mfac = host_constants().Sctr3THz2 / double(c->nq);
-    SPRING_CHECK(pairoff_host(c, ps));
-    const int p0 = ps.h_pairoff[q0_first], p1 = ps.h_pairoff[q0_first + n_q0];
-    a.pair_first = p0;
+    // Host offsets when they were read already; otherwise the range is read on the device and the
+    // grid covers the bound of at most Nq/2 + 8 pairs per q0 (no readback, no wait).
+    const int* range = nullptr;
+    long long npairs;
+    if (ps.h_ok) {
+        a.pair_first = ps.h_pairoff[q0_first];
+        npairs = ps.h_pairoff[q0_first + n_q0] - a.pair_first;
+    } else {
+        range = ps.pairoff.p + q0_first;
+        npairs = std::min<long long>((long long)n_q0 * (c->nq / 2 + 8), ps.cap);
+    }
     const size_t smem = v3_smem(a.n, a.na, a.sb, a.nT);
     if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "V3 tile needs %zu bytes of shared memory", smem);
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_v3<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const long long items = (long long)(p1 - p0) * a.nsb;
+    const long long items = npairs * a.nsb;
     if (items == 0) return SPRING_OK;
     if (items > 0x7fffffffLL) return fail(c, SPRING_ERR_UNSUPPORTED, "too many V3 work items");
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3: injected launch failure");
     const V3Ptrs P{ps.pairs.p, ps.pair_q0.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
                    c->d_qpnt.p, v.q0_int, v.q0_grid, v.evec, v.omega, v.oneby, c->ph_grid.evec.p,
                    c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, lw, p3, w};
-    k_v3<EPI><<<(unsigned)items, 128, smem, c->stream>>>(a, P);
+    k_v3<EPI><<<(unsigned)items, 128, smem, c->stream>>>(a, P, range, n_q0, ps.cap);
     return launch_check(c, EPI == 0 ? "k_v3<gauss>" : "k_v3<wgrid>");
 }
 

@@ -14,6 +14,8 @@
 //     8 consecutive threads hit distinct banks;
 //   - the grid is persistent (FC3 is staged once per CTA).
 // Roofline: FP64 FMA (41.7 kflop per pair) with shared-memory operands.
+#include <algorithm>
+
 #include "v3sitem.cuh"
 
 namespace spring {
@@ -21,12 +23,20 @@ namespace {
 
 using namespace s3;
 
+// range != null: the pair range is read on the device, pairs range[0] .. range[n_q0] (the pair
+// offsets of the enumeration, clamped to the list's capacity), instead of a.pair_first/pair_end.
 template <int EPI>
-__global__ void __launch_bounds__(THREADS, 2) k_v3s(S3Args a_, S3Ptrs P_) {
+__global__ void __launch_bounds__(THREADS, 2) k_v3s(S3Args a_, S3Ptrs P_, const int* __restrict__ range, int n_q0,
+                                                    int cap) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     Smem& S = *reinterpret_cast<Smem*>(smem_raw);
-    const S3Args a = a_;  // local copies: the device functions take references
+    S3Args a = a_;  // local copies: the device functions take references
     const S3Ptrs P = P_;
+    if (range) {
+        a.pair_first = min(range[0], cap);
+        a.pair_end = min(range[n_q0], cap);
+        a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;
+    }
     v3s_stage(S, P);
     for (int grp = blockIdx.x; grp < a.ngroups; grp += gridDim.x) v3s_group<EPI>(S, a, P, grp);
 }
@@ -44,10 +54,18 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
     a.nT = c->nT;
     a.nq0 = ps.n0;
     a.q0_first = q0_first;
-    SPRING_CHECK(pairoff_host(c, ps));
-    a.pair_first = ps.h_pairoff[q0_first];
-    a.pair_end = ps.h_pairoff[q0_first + n_q0];
-    a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;
+    // Host offsets when they were read already; otherwise the kernel reads its range on the device
+    // and the grid is sized by the bound of at most Nq/2 + 8 pairs per q0 (no readback, no wait).
+    const int* range = nullptr;
+    if (ps.h_ok) {
+        a.pair_first = ps.h_pairoff[q0_first];
+        a.pair_end = ps.h_pairoff[q0_first + n_q0];
+        a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;
+    } else {
+        range = ps.pairoff.p + q0_first;
+        const long long bound = std::min<long long>((long long)n_q0 * (c->nq / 2 + 8), ps.cap);
+        a.ngroups = (int)((bound + PP - 1) / PP);
+    }
     a.mfac = host_constants().Sctr3THz2 / double(c->nq);
     if (epi == 0) {
         a.onebysigma = 1.0 / sigma;
@@ -68,7 +86,7 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
     const S3Ptrs P{ps.pairs.p, ps.pair_q0.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_fc3_off.p,
                    c->d_mass_rs.p, c->d_qpnt.p, v.q0_int, v.q0_grid, v.evec, v.omega, v.oneby, c->ph_grid.evec.p,
                    c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, lw, p3, w};
-    kern<<<grid, THREADS, smem, c->stream>>>(a, P);
+    kern<<<grid, THREADS, smem, c->stream>>>(a, P, range, n_q0, ps.cap);
     return launch_check(c, epi == 0 ? "k_v3s<gauss>" : "k_v3s<wgrid>");
 }
 

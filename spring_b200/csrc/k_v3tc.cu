@@ -47,6 +47,8 @@ constexpr int B_BYTES = (48 / 8) * SBO;   // 4608
 constexpr int AIMG = 8 * KP;              // bf16 elements of one (q, mu, hi/lo) A image: 8 rows x 48 (768 bytes)
 constexpr int BIMG = 48 * KP;             // bf16 elements of one (q1, mu, hi/lo) B image (4608 bytes)
 constexpr double EXP_CUT = 40.0;
+// Poll limit of the waits that drain work already issued (TMA copies, MMAs) before shared and
+// tensor memory are released: these always complete, the limit only bounds a broken device.
 constexpr long long MAX_SPINS = 1LL << 26;
 
 // bf16 hi/lo split of an FP64 value
@@ -314,7 +316,8 @@ struct TcArgs {
     int nq, nq0, nT, ntiles, tiles_per_cta, cap;
     int lo[3], hi[3];
     double half_os2;
-    float rf;  // delta window of the FP32 screen (tc_window)
+    float rf;             // delta window of the FP32 screen (tc_window)
+    long long max_spins;  // poll limit of every wait of one warp on another (the pipeline waits)
 };
 
 constexpr int NOP = 2;  // operand stages (A and B images; free once the tile's MMAs completed)
@@ -337,6 +340,8 @@ struct TcSmem {
     EpStage ep[NEP];
     alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP];
     uint32_t tslot;
+    int abort;  // set by any warp whose pipeline wait ran out
+    int fdone;  // tiles the frequency warp arrived on ready for (written when it leaves its loop)
 };
 
 constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s1 each
@@ -381,6 +386,8 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     }
 
     if (tid == 0) {
+        S.abort = 0;
+        S.fdone = 0;
         for (int k = 0; k < NOP; ++k) {
             S.op[k].q1 = -1;
             tc::mbar_init(tc::smem_u32(&S.opfree[k]), 1);
@@ -397,6 +404,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     __syncthreads();
     tc::fence_after_sync();
     const uint32_t tm = S.tslot;
+    int filled = -1;  // copy warp: last tile whose operand copies were issued
 
     if (warp == EPI_WARPS) {
         // ------------------------------------------------------------ copy warp
@@ -407,15 +415,15 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
-        bool abort = false;
-        int filled = -1;
         for (int j = 0; j < nt; ++j) {
             const int es = j % NEP, os = j % NOP;
             const bool ok = j < NOP || tc::mbar_wait(tc::smem_u32(&S.opfree[os]), (uint32_t)(((j - NOP) / NOP) & 1),
-                                                     MAX_SPINS);
+                                                     a.max_spins);
             if (__any_sync(0xffffffffu, !ok)) {
-                if (lane == 0) atomicExch(err, 1);
-                abort = true;
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    *(volatile int*)&S.abort = 1;
+                }
                 break;
             }
             OpStage& O = S.op[os];
@@ -444,12 +452,6 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             recA = recB;
             recB = recC;
             entA = entB;
-        }
-        if (abort && lane == 0) {
-            // Error path: wait (bounded) for the copies still in flight before the CTA releases its
-            // shared memory.
-            for (int t = max(0, filled - NEP + 1); t <= filled; ++t)
-                tc::mbar_wait(tc::smem_u32(&S.ready[t % NEP]), (uint32_t)((t / NEP) & 1), MAX_SPINS);
         }
     } else if (warp == EPI_WARPS + 2) {
         // ------------------------------------------------------------ frequency warp
@@ -486,12 +488,16 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
         };
         if (nt > 0) load_w(entA, recA);
-        for (int j = 0; j < nt; ++j) {
+        int j = 0;
+        for (; j < nt; ++j) {
             const int es = j % NEP;
             const bool ok = j < NEP || tc::mbar_wait(tc::smem_u32(&S.empty[es]), (uint32_t)(((j - NEP) / NEP) & 1),
-                                                     MAX_SPINS);
+                                                     a.max_spins);
             if (__any_sync(0xffffffffu, !ok)) {
-                if (lane == 0) atomicExch(err, 1);
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    *(volatile int*)&S.abort = 1;
+                }
                 break;
             }
             EpStage& E = S.ep[es];
@@ -529,6 +535,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             entA = entB;
             entB = entC;
         }
+        if (lane == 0) S.fdone = j;
     } else if (warp == EPI_WARPS + 1) {
         // ------------------------------------------------------------ MMA warp
         // Tile j's MMAs once its operands have landed (ready); its accumulator was drained before the
@@ -537,8 +544,9 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         if (lane == 0) {
             for (int j = 0; j < nt; ++j) {
                 const int es = j % NEP, os = j % NOP;
-                if (!tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)((j / NEP) & 1), MAX_SPINS)) {
+                if (!tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)((j / NEP) & 1), a.max_spins)) {
                     atomicExch(err, 1);
+                    *(volatile int*)&S.abort = 1;
                     break;
                 }
                 tc::fence_after_sync();
@@ -596,10 +604,13 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         for (int j = 0; j < nt; ++j) {
             const int es = j % NEP, u = j / NEP;
             const EpStage& E = S.ep[es];
-            const bool ok = tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)(u & 1), MAX_SPINS) &&
-                            tc::mbar_wait(tc::smem_u32(&S.full[es]), (uint32_t)(u & 1), MAX_SPINS);
+            const bool ok = tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)(u & 1), a.max_spins) &&
+                            tc::mbar_wait(tc::smem_u32(&S.full[es]), (uint32_t)(u & 1), a.max_spins);
             if (__any_sync(0xffffffffu, !ok)) {
-                if (lane == 0) atomicExch(err, 1);
+                if (lane == 0) {
+                    atomicExch(err, 1);
+                    *(volatile int*)&S.abort = 1;
+                }
                 break;
             }
             tc::fence_after_sync();
@@ -674,7 +685,23 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         }
         if (lane == 0) counts[blockIdx.x * EPI_WARPS + warp] = base;
     }
+    // Every role has left its loop (each of its waits is bounded).  After a time-out the operand
+    // copies of up to NOP tiles may be in flight, unconsumed by the MMA warp: a copy of tile t is
+    // only issued once the MMAs of tile t - NOP completed, so those tiles are filled - NOP + 1 ..
+    // filled, and each of their ready phases completes once the copy lands (the frequency warp
+    // arrived for them: it runs NEP >= NOP tiles ahead without waiting).  The copy warp waits for
+    // them before the CTA releases its shared memory.  The MMA warp already waited for its last
+    // commit, so no MMA writes tensor memory after the release below.
+    // Where the frequency warp stopped before tile t, the copy warp arrives in its place, so that
+    // the phase completes on the copies' bytes alone.
     tc::fence_before_sync();
+    __syncthreads();
+    if (warp == EPI_WARPS && lane == 0 && *(volatile int*)&S.abort)
+        for (int t = max(0, filled - NOP + 1); t <= filled; ++t) {
+            const uint32_t rb = tc::smem_u32(&S.ready[t % NEP]);
+            if (t >= S.fdone) tc::mbar_arrive_cnt(rb, 32);
+            tc::mbar_wait(rb, (uint32_t)((t / NEP) & 1), MAX_SPINS);
+        }
     __syncthreads();
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_dealloc(tm, TC_COLS);
@@ -1002,6 +1029,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     }
     a.half_os2 = half_os2;
     a.rf = rf;
+    a.max_spins = c->tc_max_spins >= 0 ? c->tc_max_spins : MAX_SPINS;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
     const int ctas = std::max(1, std::min(a.ntiles, sms));
@@ -1037,7 +1065,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
         const int* cnt = c->h_pin;
         const int herr = cnt[nreg];
         if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
-        if (herr) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: an mbarrier wait timed out");
+        if (herr) return fail(c, SPRING_ERR_TIMEOUT, "tensor-core V3: a pipeline wait ran out after %lld polls",
+                              a.max_spins);
         maxcnt = *std::max_element(cnt, cnt + nreg);
         if (maxcnt <= cap) break;
         // The pass wrote only what fit and the evaluation summed that part: clear this block's sums

@@ -89,12 +89,21 @@ struct spring_ctx {
     int* h_pin = nullptr;              // pinned host scratch for readbacks that overlap queued work
     size_t h_pin_n = 0;                // its size in ints
     cudaEvent_t ev_aux = nullptr;      // marks the end of such a readback
+    // Pinned staging ring for host -> device copies: every upload copies the caller's bytes here on
+    // the CPU before its cudaMemcpyAsync is queued, so no copy ever reads host memory the library
+    // does not own.  Bytes are reused only after ev_stage (recorded behind the last staged copy)
+    // has completed.
+    char* h_stage = nullptr;
+    size_t h_stage_cap = 0, h_stage_off = 0;
+    cudaEvent_t ev_stage = nullptr;
+    bool stage_pending = false;
     cudaStream_t stream2 = nullptr;    // side stream for work that overlaps the main stream's
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string err;
     long long launches = 0;
     int precision = SPRING_FP64;
     bool force_generic_v3 = false;  // spring_set_option(SPRING_OPT_GENERIC_V3): use the any-cell V3 kernel
+    long long tc_max_spins = -1;    // spring_set_option(SPRING_OPT_WAIT_POLLS); -1: the kernels' default
 
     // per-launch CUDA-event records (spring_set_profiling)
     struct ProfRec {
@@ -172,6 +181,17 @@ struct spring_ctx {
     spring::DBuf<int> d_tr_deg;    // [ntr]
     spring::DBuf<int> d_neg;       // [q] grid index of -q
     spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
+
+    // four-phonon quartet lists (k_4ph.cu, opaque) and the tensor-core V4 buffers (k_v4tc.cu)
+    void* e4 = nullptr;
+    spring::DBuf<double2> d_v4_ph;    // [q][mu][8] phases
+    spring::DBuf<float2> d_v4_etab;   // [q][nu c][s] m^-1/2 e
+    spring::DBuf<float> d_v4_wf;      // [q][s] FP32 omega
+    spring::DBuf<float2> d_v4_c;      // C of one q0
+    spring::DBuf<short> d_v4_map;     // (mu, N2, N3) -> block entry
+    spring::DBuf<uint4> d_v4_img;     // B images [q1][chunk][part]
+    spring::DBuf<int> d_v4_cnt, d_v4_seg, d_v4_ntl, d_v4_toff, d_v4_stat;
+    spring::DBuf<int4> d_v4_tiles;
 
     // scratch
     spring::DBuf<int> d_scan_tmp;
@@ -283,6 +303,11 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
 // k_4ph.cu
 int run_enumerate4_fortran(spring_ctx* c, int q0, int* d_all, int* d_perm, long long cap, long long* h_counts);
 int run_lw4(spring_ctx* c, int q0_first, int n_q0, int delta_mode, double sigma, const int* pol4, double* d_rate);
+int run_enum4_list(spring_ctx* c, int q0, const int4** d_quart, long long* nquart);
+void free_enum4(spring_ctx* c);
+// k_v4tc.cu: tensor-core V4 + Gaussian four-phonon rate (BF16 / BF16x3) for two-atom cells;
+// *handled false when the cell or the precision does not take it
+int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, double* d_rate, bool* handled);
 // k_path.cu: LineWidth.x path mode; h_q0 (3, n_path) Cartesian, h_lw [T][p][s], h_omega [p][s]
 int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
              double* h_lw, double* h_omega);

@@ -118,6 +118,12 @@ static __device__ __forceinline__ void tmem_ld4(uint32_t taddr, float* v) {
 #pragma unroll
     for (int i = 0; i < 4; ++i) v[i] = __uint_as_float(r[i]);
 }
+static __device__ __forceinline__ void tmem_ld2(uint32_t taddr, float* v) {
+    uint32_t r[2];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(taddr) : "memory");
+    v[0] = __uint_as_float(r[0]);
+    v[1] = __uint_as_float(r[1]);
+}
 static __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -125,6 +131,10 @@ static __device__ __forceinline__ void tmem_ld_wait() {
 // Plain arrive on an mbarrier (release semantics at CTA scope).
 static __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+// `count` arrivals on an mbarrier at once.
+static __device__ __forceinline__ void mbar_arrive_cnt(uint32_t mbar, uint32_t count) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
 // Barrier over a subset of the CTA's warps (ids 1..15; count a multiple of 32).

@@ -147,3 +147,28 @@ def test_tc_prescreen_counts_match_numpy(runs):
         np.add.at(by_q1, q1[m], 1)
     assert pairs == kept
     assert tiles == int(((by_q1 + 15) // 16).sum())
+
+
+def test_tc_wait_timeout_returns_status_and_context_recovers(runs):
+    """Every wait of one warp on another in the tensor-core kernel is bounded.  With a poll limit of 0
+    each such wait runs out at once: the kernel drains the copies it issued, frees its tensor memory
+    and returns, the call fails with SPRING_ERR_TIMEOUT, and the next call on the same context (with
+    the default limit) gives the normal result.  No GPU fault is involved: the waits simply stop."""
+    from spring_b200 import _lib as L
+    from spring_b200.api import SpringError
+    N, ctx, info, out, _ = runs
+    if N != 8:
+        pytest.skip("8^3 mesh only")
+    ctx.set_precision("bf16x3")
+    ctx.set_option(L.SPRING_OPT_WAIT_POLLS, 0)
+    try:
+        with pytest.raises(SpringError) as ei:
+            ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
+        assert ei.value.code == L.SPRING_ERR_TIMEOUT
+    finally:
+        ctx.set_option(L.SPRING_OPT_WAIT_POLLS, -1)
+    ctx.synchronize()  # the context and its stream are still usable
+    ctx.reset_linewidths()
+    lw, _ = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
+    ctx.set_precision("fp64")
+    np.testing.assert_allclose(lw, out["bf16x3"][0], rtol=1e-12, atol=0.0)

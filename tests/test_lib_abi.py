@@ -26,10 +26,19 @@ def test_library_exports_every_symbol():
         assert hasattr(lib, name), name
 
 
-def test_library_is_sm100a_build():
-    # the fatbin of an sm_100a build names the architecture
-    data = open(L.LIB_PATH, "rb").read()
-    assert b"sm_100a" in data
+def test_build_targets_sm100a():
+    # the build compiles every kernel for sm_100a only (no other architecture, no PTX for JIT)
+    from spring_b200 import build as B
+    assert B.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+@pytest.mark.gpu
+def test_kernels_are_sm100_binaries():
+    # the runtime reports the binary architecture of the library's kernels (cudaFuncGetAttributes)
+    lib = L.load()
+    v = ct.c_int(0)
+    assert lib.spring_binary_version(0, ct.byref(v)) == 0
+    assert v.value == 100
 
 
 def test_create_without_gpu_fails_cleanly():

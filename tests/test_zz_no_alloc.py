@@ -29,7 +29,8 @@ def test_noalloc_matches_allocating_entry_point_twice():
     lib = L.load()
     nd, nT = ctx.ndof, ctx.n_temps
     for call, i0 in enumerate((2, 5)):
-        ref, ref_p3 = ctx.linewidth3(i0, 1, delta="tetra")          # allocating entry point
+        # the no-alloc call comes first, straight after spring_prepare3: it reads the pair range of
+        # its q0 on the device, so nothing before it needs to have read the pair offsets back
         d_lw = torch.full((nT, nd), float("nan"), dtype=torch.float64, device="cuda")
         d_p3 = torch.full((nd,), float("nan"), dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
@@ -37,6 +38,7 @@ def test_noalloc_matches_allocating_entry_point_twice():
                                                  ct.c_void_p(d_p3.data_ptr()))
         assert rc == 0, lib.spring_last_error(ctx._h)
         ctx.synchronize()
+        ref, ref_p3 = ctx.linewidth3(i0, 1, delta="tetra")          # allocating entry point
         got = d_lw.cpu().numpy()
         np.testing.assert_allclose(got, ref[:, 0, :], rtol=1e-9, atol=1e-14 * np.abs(ref).max())
         np.testing.assert_allclose(d_p3.cpu().numpy(), ref_p3[0], rtol=1e-9, atol=1e-14 * np.abs(ref_p3).max())
