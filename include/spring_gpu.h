@@ -195,6 +195,14 @@ int spring_enumerate4(spring_ctx* ctx, int i0, int* Allq1q2q3, int* q1q2q3_permu
 int spring_linewidth4(spring_ctx* ctx, int i0_first, int n_q0, int delta_mode, double sigma, const int* pol4,
                       double* rate);
 
+/* No counterpart in the reference.  The Gaussian 4-phonon rate of selected branches only: bit s-1 of
+ * s0_mask(k) selects branch s of irreducible point i0_first + k - 1.  With the tensor-core V4
+ * (spring_set_precision BF16 / BF16x3, two-atom cells) the work is proportional to the selected
+ * branches; the FP64 path computes every branch.  rate(Ndof,n_q0,n_temps) receives the selected
+ * rates and zero elsewhere; the resident LW_Allq0 is not touched.  Used by the surrogate-screened
+ * path to spend exact evaluation on the modes it ranks first. */
+int spring_linewidth4_modes(spring_ctx* ctx, int i0_first, int n_q0, double sigma, const int* s0_mask, double* rate);
+
 /* ---- LineWidth.x path mode ------------------------------------------- */
 /* q_points_highsymm, src/LineWidth/Src/CreateMesh_mod.f90:85-172: path points
  * from q_high_sym(4,n_nodes) (fractional node, points on the segment ending at
@@ -218,10 +226,12 @@ int spring_path_qpoints(spring_ctx* ctx, int n_nodes, const double* q_high_sym, 
 int spring_linewidth_path(spring_ctx* ctx, int n_q0, const double* q0, const int* zero_centered, int delta_mode,
                           double sigma, double* lw, double* omega_q0);
 
-/* Arithmetic of the 3-phonon matrix elements in the fused Gaussian linewidth
- * (spring_linewidth3 with SPRING_DELTA_GAUSS, two-atom cells): SPRING_FP64
- * (default), SPRING_BF16 or SPRING_BF16X3.  No counterpart in the reference,
- * which is FP64 throughout.  Other cells and the tetrahedron path stay FP64. */
+/* Arithmetic of the 3- and 4-phonon matrix elements in the Gaussian rates
+ * (spring_linewidth3 / spring_linewidth4 / spring_linewidth4_modes with SPRING_DELTA_GAUSS,
+ * two-atom cells; spring_linewidth4 over every branch): SPRING_FP64 (default), SPRING_BF16 or
+ * SPRING_BF16X3, the contractions on the tensor cores with FP64 frequencies, occupations, delta
+ * weights and sums.  No counterpart in the reference, which is FP64 throughout.  Other cells and
+ * the tetrahedron path stay FP64. */
 int spring_set_precision(spring_ctx* ctx, int precision);
 
 /* ---- surrogate network of the screened four-phonon path -------------- */

@@ -76,6 +76,7 @@ SIGNATURES = {
     "spring_linewidth3_tetra_noalloc": [P, I, P, P, P],
     "spring_enumerate4": [P, I, P, P, ct.c_longlong, P],
     "spring_linewidth4": [P, I, I, I, D, P, P],
+    "spring_linewidth4_modes": [P, I, I, D, P, P],
     "spring_path_qpoints": [P, I, P, P, P, P, P],
     "spring_linewidth_path": [P, I, P, P, I, D, P, P],
     "spring_reset_linewidths": [P],

@@ -95,7 +95,7 @@ class Context:
         self._call("spring_set_option", int(option), int(value))
 
     def set_precision(self, precision):
-        """"fp64" (default), "bf16" or "bf16x3": arithmetic of the fused Gaussian V3."""
+        """"fp64" (default), "bf16" or "bf16x3": arithmetic of the Gaussian V3 and V4 contractions."""
         code = {"fp64": L.SPRING_FP64, "bf16": L.SPRING_BF16, "bf16x3": L.SPRING_BF16X3}[precision]
         self._call("spring_set_precision", code)
 
@@ -288,6 +288,15 @@ class Context:
             return None
         rate = np.zeros((self.n_temps, n_q0, self.ndof))
         self._call("spring_linewidth4", int(i0_first), int(n_q0), mode, float(sigma), _ptr(pol), _ptr(rate))
+        return rate
+
+    def linewidth4_modes(self, i0_first: int, s0_mask, sigma: float = 0.3767):
+        """Gaussian four-phonon rates (nT, n_q0, Ndof) of the selected branches only (bit s of
+        s0_mask[k] selects branch s of q0 = i0_first + k), zero elsewhere; LW_Allq0 untouched."""
+        m = _c(s0_mask, np.int32)
+        n = int(m.shape[0])
+        rate = np.zeros((self.n_temps, n, self.ndof))
+        self._call("spring_linewidth4_modes", int(i0_first), n, float(sigma), _ptr(m), _ptr(rate))
         return rate
 
     # -- LineWidth.x path mode

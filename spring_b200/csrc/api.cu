@@ -929,10 +929,39 @@ int spring_linewidth4(spring_ctx* c, int i0_first, int n_q0, int delta_mode, dou
     if (pol4)
         for (int k = 0; k < 4; ++k) all_modes = all_modes && pol4[2 * k] == 1 && pol4[2 * k + 1] == c->ndof;
     if (delta_mode == SPRING_DELTA_GAUSS && all_modes)
-        SPRING_CHECK(run_v4tc_gauss(c, q0, n_q0, sigma, c->d_lw_tmp.p, &handled));
+        SPRING_CHECK(run_v4tc_gauss(c, q0, n_q0, sigma, nullptr, c->d_lw_tmp.p, &handled));
     if (!handled) SPRING_CHECK(run_lw4(c, q0, n_q0, delta_mode, sigma, pol4, c->d_lw_tmp.p));
     SPRING_CHECK(run_axpy_lw(c, 0.5, c->d_lw_tmp.p, c->d_lw_all.p, q0, n_q0));
     SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
+    return SPRING_OK;
+}
+
+int spring_linewidth4_modes(spring_ctx* c, int i0_first, int n_q0, double sigma, const int* s0_mask, double* rate) {
+    CTX_ENTER(c);
+    SPRING_CHECK(check_q0_range(c, i0_first, n_q0));
+    SPRING_CHECK(need(c, c->fc4_set, "FC4"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    SPRING_CHECK(need(c, c->ph_irr.set, "irreducible-point phonons"));
+    if (!s0_mask || !rate) return fail(c, SPRING_ERR_ARG, "s0_mask and rate must not be NULL");
+    if (!(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    const int full = (1 << c->ndof) - 1;
+    for (int k = 0; k < n_q0; ++k)
+        if (s0_mask[k] & ~full) return fail(c, SPRING_ERR_ARG, "s0_mask(%d) has bits beyond Ndof", k + 1);
+    if (n_q0 == 0) return SPRING_OK;
+    const int q0 = i0_first - 1;
+    const size_t nl = (size_t)c->nT * c->nq0 * c->ndof;
+    SPRING_CHECK(dalloc(c, c->d_lw_tmp, nl, "linewidth scratch"));
+    SPRING_CHECK(zero(c, c->d_lw_tmp.p, sizeof(double) * nl, "linewidth scratch"));
+    bool handled = false;
+    SPRING_CHECK(run_v4tc_gauss(c, q0, n_q0, sigma, s0_mask, c->d_lw_tmp.p, &handled));
+    if (!handled) SPRING_CHECK(run_lw4(c, q0, n_q0, SPRING_DELTA_GAUSS, sigma, nullptr, c->d_lw_tmp.p));
+    SPRING_CHECK(copy_lw_out(c, c->d_lw_tmp.p, q0, n_q0, rate));
+    // branches outside the mask are zero (the FP64 path computes every branch)
+    for (int T = 0; T < c->nT; ++T)
+        for (int k = 0; k < n_q0; ++k)
+            for (int s = 0; s < c->ndof; ++s)
+                if (!((s0_mask[k] >> s) & 1)) rate[((size_t)T * n_q0 + k) * c->ndof + s] = 0.0;
     return SPRING_OK;
 }
 

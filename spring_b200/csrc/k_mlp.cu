@@ -7,7 +7,8 @@
 // Kernels: a tiled FP32 GEMM C = op(A) op(B) (+ bias) used for the forward pass
 // (Z = A W^T + b), the weight gradients (dZ^T A) and the backpropagated
 // activations (dZ W); element-wise SiLU and its derivative; the loss; a
-// column sum for the bias gradients; Adam.  Parameters are one flat FP32 vector:
+// column sum for the bias gradients; Adam; and the BF16 inference kernel on
+// the tensor cores (k_mlp_bf16, mma.sync BF16 with FP32 accumulation).  Parameters are one flat FP32 vector:
 // W1 (128x5, row-major), b1, W2 (128x128), b2, W3, b3, W4 (1x128), b4.
 // Roofline: tiny GEMMs (B x 128 x 128), latency- and launch-bound; the data of a
 // training run fits in L2.
@@ -177,6 +178,123 @@ Bufs carve(spring_ctx* c, int nb) {
     return b;
 }
 
+// ---- BF16 inference on the tensor cores: the whole network per warp, in registers.
+// mma.sync m16n8k16 (BF16 operands, FP32 accumulation): a warp takes 16 rows; each hidden layer is
+// 16 column tiles x 8 K steps of MMAs with the weights (BF16, row-major W[out][in] in shared memory)
+// as the B operand; the FP32 accumulators get the bias and SiLU and are packed to BF16 as the next
+// layer's A fragments (the C layout of two adjacent 8-column tiles is the A layout of one 16-wide K
+// step).  The input layer pads K 5 -> 16, the output layer N 1 -> 8.
+constexpr int MW = 4;  // warps per CTA (64 rows)
+struct MlpBf16Smem {
+    __nv_bfloat16 w1[128][16];
+    __nv_bfloat16 w2[128][128 + 8];  // rows padded by 16 bytes: conflict-free B fragment loads
+    __nv_bfloat16 w3[128][128 + 8];
+    __nv_bfloat16 w4[8][128 + 8];
+    float b[3][128];
+    float b4;
+};
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// One hidden layer of K = 16 * KT inputs: acc[16 tiles][4] = A W^T (+ bias, SiLU) -> A fragments.
+template <int KT>
+__device__ __forceinline__ void mlp_layer(const uint32_t (&a)[KT][4], const __nv_bfloat16* w, int ldw,
+                                          const float* bias, uint32_t (&out)[8][4], int g, int t) {
+    float acc[16][4];
+#pragma unroll
+    for (int n = 0; n < 16; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.f;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const __nv_bfloat16* row = w + (size_t)(8 * n + g) * ldw + 16 * kt + 2 * t;
+            const uint32_t b0 = *reinterpret_cast<const uint32_t*>(row);
+            const uint32_t b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+            mma_bf16_16816(acc[n], a[kt], b0, b1);
+        }
+#pragma unroll
+    for (int n = 0; n < 16; ++n) {
+        const float c0 = bias[8 * n + 2 * t], c1 = bias[8 * n + 2 * t + 1];
+        float v[4] = {acc[n][0] + c0, acc[n][1] + c1, acc[n][2] + c0, acc[n][3] + c1};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = v[i] * (1.0f / (1.0f + expf(-v[i])));
+        // C tile n -> A step n / 2: even tiles give a0a1 / a2a3, odd tiles a4a5 / a6a7
+        out[n / 2][(n & 1) * 2 + 0] = pack_bf16(v[0], v[1]);
+        out[n / 2][(n & 1) * 2 + 1] = pack_bf16(v[2], v[3]);
+    }
+}
+
+__global__ void __launch_bounds__(MW * 32) k_mlp_bf16(int n, const float* __restrict__ X, const float* __restrict__ P,
+                                                      int o1, int o2, int o3, int o4, float* __restrict__ y) {
+    extern __shared__ __align__(16) unsigned char mlp_sm[];
+    MlpBf16Smem& S = *reinterpret_cast<MlpBf16Smem*>(mlp_sm);
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 128 * 16; i += blockDim.x) {
+        const int r = i / 16, k = i % 16;
+        S.w1[r][k] = __float2bfloat16_rn(k < SPRING_MLP_INPUTS ? P[o1 + r * SPRING_MLP_INPUTS + k] : 0.f);
+    }
+    for (int i = tid; i < 128 * 128; i += blockDim.x) {
+        const int r = i / 128, k = i % 128;
+        S.w2[r][k] = __float2bfloat16_rn(P[o2 + i]);
+        S.w3[r][k] = __float2bfloat16_rn(P[o3 + i]);
+    }
+    for (int i = tid; i < 8 * 128; i += blockDim.x) {
+        const int r = i / 128, k = i % 128;
+        S.w4[r][k] = __float2bfloat16_rn(r == 0 ? P[o4 + k] : 0.f);
+    }
+    for (int i = tid; i < 3 * 128; i += blockDim.x) {
+        const int l = i / 128, j = i % 128;
+        const int ob = (l == 0 ? o1 + 128 * SPRING_MLP_INPUTS : (l == 1 ? o2 : o3) + 128 * 128);
+        S.b[l][j] = P[ob + j];
+    }
+    if (tid == 0) S.b4 = P[o4 + 128];
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    for (int r0 = (blockIdx.x * MW + warp) * 16; r0 < n; r0 += gridDim.x * MW * 16) {
+        // input fragment: rows r0 + g and r0 + g + 8, columns 2t, 2t + 1 (the rest of K is zero)
+        uint32_t a0[1][4];
+        float x[2][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int row = r0 + g + 8 * h, col = 2 * t + c;
+                x[h][c] = (row < n && col < SPRING_MLP_INPUTS) ? X[(size_t)row * SPRING_MLP_INPUTS + col] : 0.f;
+            }
+        a0[0][0] = pack_bf16(x[0][0], x[0][1]);
+        a0[0][1] = pack_bf16(x[1][0], x[1][1]);
+        a0[0][2] = 0u;  // columns 8 .. 15
+        a0[0][3] = 0u;
+        uint32_t h1[8][4], h2[8][4];
+        mlp_layer<1>(a0, &S.w1[0][0], 16, S.b[0], h1, g, t);
+        mlp_layer<8>(h1, &S.w2[0][0], 128 + 8, S.b[1], h2, g, t);
+        mlp_layer<8>(h2, &S.w3[0][0], 128 + 8, S.b[2], h1, g, t);
+        // output layer: one column (a tile of 8, the other weights zero)
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int kt = 0; kt < 8; ++kt) {
+            const __nv_bfloat16* row = &S.w4[g][16 * kt + 2 * t];
+            mma_bf16_16816(acc, h1[kt], *reinterpret_cast<const uint32_t*>(row),
+                           *reinterpret_cast<const uint32_t*>(row + 8));
+        }
+        if (t == 0) {  // column 0 of rows g and g + 8
+            if (r0 + g < n) y[r0 + g] = acc[0] + S.b4;
+            if (r0 + g + 8 < n) y[r0 + g + 8] = acc[2] + S.b4;
+        }
+    }
+}
+
 // forward over nb rows already in b.x; output in b.z[NL] (and b.a[NL])
 int forward(spring_ctx* c, const Bufs& b, int nb, const float* params, int round_bf16) {
     for (int l = 1; l <= NL; ++l) {
@@ -303,6 +421,27 @@ int run_mlp_train(spring_ctx* c, int n, const float* hX, const float* hy, int ep
 
 int run_mlp_predict(spring_ctx* c, int n, const float* hX, float* hy, int bf16) {
     Mlp& m = c->mlp;
+    if (bf16) {  // BF16 on the tensor cores, FP32 accumulation
+        DBuf<float> dx, dy;
+        int rc = dalloc(c, dx, (size_t)std::max(n, 1) * SZ[0], "network inputs");
+        if (rc == SPRING_OK) rc = dalloc(c, dy, std::max(n, 1), "network outputs");
+        if (rc == SPRING_OK) rc = h2d(c, dx.p, hX, sizeof(float) * n * SZ[0], "network inputs");
+        if (rc == SPRING_OK && n > 0) {
+            if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "mlp: injected launch failure");
+            else {
+                const int grid = std::max(1, std::min((n + MW * 16 - 1) / (MW * 16), 148 * 8));
+                cudaFuncSetAttribute(k_mlp_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpBf16Smem));
+                k_mlp_bf16<<<grid, MW * 32, sizeof(MlpBf16Smem), c->stream>>>(n, dx.p, m.p.p, w_off(0), w_off(1),
+                                                                                w_off(2), w_off(3), dy.p);
+                rc = launch_check(c, "k_mlp_bf16");
+            }
+        }
+        if (rc == SPRING_OK && n > 0) rc = d2h(c, hy, dy.p, sizeof(float) * n, "network outputs");
+        cudaStreamSynchronize(c->stream);
+        dfree(dx);
+        dfree(dy);
+        return rc;
+    }
     const int np = mlp_num_params();
     const int chunk = std::min(n, 1 << 16);
     SPRING_CHECK(ensure_buffers(c, chunk));

@@ -56,6 +56,11 @@ constexpr double EXP_CUT = 40.0;
 constexpr long long MAX_SPINS = 1LL << 26;  // drains of work already issued
 constexpr int E2S = 37;         // float2 stride of one quartet's E_q2 in shared memory (36 used)
 
+// Row of the B image (= accumulator column inside a block's 64) of value i = c*6 + ri*3 + d
+// (ri = 0 Re, 1 Im) of s1 slot j: the first 16 values of each j at 16 j, the last two at 48 + 2 j,
+// so that the epilogue reads them with one 16-column and one 2-column load at aligned columns.
+__host__ __device__ __forceinline__ int brow(int j, int i) { return i < 16 ? 16 * j + i : 48 + 2 * j + (i - 16); }
+
 // The block structure of the X' GEMM (host-built from the FC4 cluster's basis types).
 struct Blk4 {
     int kb[NBLK];                // complex K entries of each block
@@ -129,18 +134,18 @@ __global__ void k4_c0(int na, const double* __restrict__ fc4, const double2* __r
 }
 
 // B images of one q1: for chunk ch = (s0, s1 half) and part (hi, lo), the blocks' canonical K-major
-// images (LBO 128, SBO kpad/8 * 128) one after the other, rows n = j*18 + c*6 + ri*3 + d (j = s1 % 3,
+// images (LBO 128, SBO kpad/8 * 128) one after the other, rows brow(j, c*6 + ri*3 + d) (j = s1 % 3,
 // ri = 0 Re / 1 Im row of the real product), columns [Re P | Im P] of the block's entries.  One
 // CTA per (q1, s0) builds the two chunks of s0 in shared memory (from X_mu[s0 s1][a2][a3] =
 // sum_a1 C_mu[s0][a1][a2][a3] D_mu(q1)[a1][s1]) and writes them as 16-byte vectors.
 // map[mu][N2][N3] = block * 256 + entry of (mu, N2, N3), or -1.
-__global__ void __launch_bounds__(256) k4_bimg(int nq, int na, int H, Blk4 bk, const int* __restrict__ qcnt,
+__global__ void __launch_bounds__(256) k4_bimg(int nq, int na, int H, int s0mask, Blk4 bk, const int* __restrict__ qcnt,
                                                const short* __restrict__ map, const float2* __restrict__ cq,
                                                const double2* __restrict__ ph, const float2* __restrict__ etab,
                                                const int* __restrict__ btyp, __nv_bfloat16* __restrict__ img) {
     extern __shared__ __align__(16) unsigned char sm4[];
     const int q1 = blockIdx.x / NM, s0 = blockIdx.x % NM;
-    if (qcnt[q1] == 0) return;  // no quartet of this q0 starts at q1
+    if (qcnt[q1] == 0 || !((s0mask >> s0) & 1)) return;  // no quartet of q0 starts at q1, or s0 not wanted
     const int cimg = CROWS * bk.ktot;               // bf16 elements of one (chunk, part) image
     __nv_bfloat16* simg = reinterpret_cast<__nv_bfloat16*>(sm4);  // [2 chunks][H][cimg]
     float2* sD = reinterpret_cast<float2*>(sm4 + (size_t)2 * H * cimg * 2);  // [mu][a1][s1]
@@ -185,7 +190,7 @@ __global__ void __launch_bounds__(256) k4_bimg(int nq, int na, int H, Blk4 bk, c
 #pragma unroll
         for (int s = 0; s < NM; ++s) {
             const int ch = s / 3, j = s % 3;
-            const int nre = j * 18 + c * 6 + d, nim = nre + 3;
+            const int nre = brow(j, c * 6 + d), nim = brow(j, c * 6 + 3 + d);
             __nv_bfloat16 h, l;
             __nv_bfloat16* I0 = simg + (size_t)(ch * H) * cimg + base;
             __nv_bfloat16* I1 = I0 + cimg;  // lo part (H == 2)
@@ -232,6 +237,8 @@ __global__ void k4_total(int nq, const int* __restrict__ toff, const int* __rest
 // ------------------------------------------------------------------ the tensor-core pass
 struct V4Args {
     int nq, nT, nq0, q0, ntiles, tiles_per_cta, H, gq0;
+    int nch;                     // chunks per tile: two for every branch s0 of the mask
+    int chunk[NCHUNK];           // the chunks, in order (chunk c is s0 = c / 2, s1 = 3 (c % 2) .. + 2)
     double mfac, half_os2, pre;  // Sctr4THz2 / Nq^2; 1 / (2 sigma^2); 1 / (sigma sqrt(2 pi))
     float rf;                    // FP32 window half-width of a delta term
     long long max_spins;
@@ -306,8 +313,8 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
             const uint32_t bytes = (uint32_t)bbytes;
             for (int t = 0; t < nt; ++t) {
                 const int q1 = tiles[t0 + t].x;
-                for (int ch = 0; ch < NCHUNK * H; ++ch) {
-                    const int u = t * NCHUNK * H + ch;
+                for (int ch = 0; ch < a.nch * H; ++ch) {
+                    const int u = t * a.nch * H + ch;
                     if (u > 0 && !tc::mbar_wait(tc::smem_u32(&S.bfree), (uint32_t)((u - 1) & 1), a.max_spins)) {
                         atomicExch(err, 1);
                         *(volatile int*)&S.abort = 1;
@@ -316,7 +323,8 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                     }
                     const uint32_t fb = tc::smem_u32(&S.bfull);
                     tc::mbar_expect_tx(fb, bytes);
-                    tc::bulk_g2s(tc::smem_u32(sB), img + ((size_t)q1 * NCHUNK * H + ch) * CROWS * bk.ktot, bytes, fb);
+                    const int cpart = a.chunk[ch / H] * H + ch % H;  // (chunk, part) of the image
+                    tc::bulk_g2s(tc::smem_u32(sB), img + ((size_t)q1 * NCHUNK * H + cpart) * CROWS * bk.ktot, bytes, fb);
                     tc::mbar_arrive(fb);
                     issued_copies = u + 1;
                 }
@@ -334,8 +342,8 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
             bool ok = true;
             for (int t = 0; ok && t < nt; ++t) {
                 ok = tc::mbar_wait(tc::smem_u32(&S.afull), (uint32_t)(t & 1), a.max_spins);
-                for (int ch = 0; ok && ch < NCHUNK; ++ch) {
-                    const int k = t * NCHUNK + ch, buf = k & 1;
+                for (int ch = 0; ok && ch < a.nch; ++ch) {
+                    const int k = t * a.nch + ch, buf = k & 1;
                     ok = k < 2 || tc::mbar_wait(tc::smem_u32(&S.tempty[buf]), (uint32_t)(((k >> 1) - 1) & 1),
                                                 a.max_spins);
                     for (int part = 0; ok && part < H; ++part) {
@@ -361,7 +369,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                     }
                     if (!ok) break;
                     tc::mma_commit(tc::smem_u32(&S.tfull[buf]));
-                    if (ch == NCHUNK - 1) tc::mma_commit(tc::smem_u32(&S.afree));
+                    if (ch == a.nch - 1) tc::mma_commit(tc::smem_u32(&S.afree));
                 }
             }
             if (!ok) {
@@ -459,9 +467,9 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
             }
             const bool gam1 = g1 == 0, gam2 = g2 == 0, gam3 = g3 == 0;
             // ---- chunks
-            for (int ch = 0; ch < NCHUNK; ++ch) {
-                const int k = t * NCHUNK + ch, buf = k & 1;
-                const int s0 = ch >> 1, s1b = 3 * (ch & 1);
+            for (int ch = 0; ch < a.nch; ++ch) {
+                const int k = t * a.nch + ch, buf = k & 1;
+                const int s0 = a.chunk[ch] >> 1, s1b = 3 * (a.chunk[ch] & 1);
                 ok = tc::mbar_wait(tc::smem_u32(&S.tfull[buf]), (uint32_t)((k >> 1) & 1), a.max_spins);
                 if (__any_sync(0xffffffffu, !ok)) {
                     if (lane == 0) {
@@ -486,14 +494,15 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                         for (int y = 0; y < 3; ++y) phi[x][y] = make_float2(0.f, 0.f);
 #pragma unroll
                     for (int nu2 = 0; nu2 < 2; ++nu2) {
-                        // blocks (nu2, 0) = 2 nu2 and (nu2, 1) = 2 nu2 + 1: 18 columns each at 18 j
+                        // blocks (nu2, 0) = 2 nu2 and (nu2, 1) = 2 nu2 + 1: the 18 values of slot j
+                        // (value i = c*6 + ri*3 + d at column brow(j, i))
                         float xv[2][18];
                         __syncwarp();
 #pragma unroll
                         for (int nu3 = 0; nu3 < 2; ++nu3) {
-                            const uint32_t ca = tb + (uint32_t)((2 * nu2 + nu3) * CROWS + 18 * j);
-                            tc::tmem_ld16(ca, xv[nu3]);
-                            tc::tmem_ld2(ca + 16, xv[nu3] + 16);
+                            const uint32_t cb = tb + (uint32_t)((2 * nu2 + nu3) * CROWS);
+                            tc::tmem_ld16(cb + (uint32_t)(16 * j), xv[nu3]);
+                            tc::tmem_ld2(cb + (uint32_t)(48 + 2 * j), xv[nu3] + 16);
                         }
                         tc::tmem_ld_wait();
                         if (j == 2 && nu2 == 1) {  // this warp's reads of the buffer are done
@@ -504,7 +513,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                         if (act) {
 #pragma unroll
                             for (int c = 0; c < 3; ++c) {
-                                // Z[s3] = sum_{nu3 d} X'[c d][nu2 nu3] E3[nu3 d][s3]; column c*6 + ri*3 + d
+                                // Z[s3] = sum_{nu3 d} X'[c d][nu2 nu3] E3[nu3 d][s3]; value c*6 + ri*3 + d
                                 float2 z[3];
 #pragma unroll
                                 for (int y = 0; y < 3; ++y) z[y] = make_float2(0.f, 0.f);
@@ -648,7 +657,8 @@ static int v4_blocks(spring_ctx* c, Blk4& bk, std::vector<short>& map) {
     return SPRING_OK;
 }
 
-int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, double* d_rate, bool* handled) {
+int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const int* h_mask, double* d_rate,
+                   bool* handled) {
     *handled = false;
     if (c->nb != 2 || c->na4 > NA4 || c->nT > 9 || c->precision == SPRING_FP64) return SPRING_OK;
     *handled = true;
@@ -697,6 +707,14 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, double* 
     a.rf = (float)(std::sqrt(EXP_CUT / a.half_os2) * 1.0001 + 1e-3);
     a.max_spins = c->tc_max_spins >= 0 ? c->tc_max_spins : MAX_SPINS;
     for (int q0 = q0_first; q0 < q0_first + n_q0; ++q0) {
+        const int mask = h_mask ? (h_mask[q0 - q0_first] & 0x3f) : 0x3f;
+        a.nch = 0;
+        for (int s0 = 0; s0 < NM; ++s0)
+            if ((mask >> s0) & 1) {
+                a.chunk[a.nch++] = 2 * s0;
+                a.chunk[a.nch++] = 2 * s0 + 1;
+            }
+        if (a.nch == 0) continue;
         const int4* d_quart = nullptr;
         long long nquart = 0;
         SPRING_CHECK(run_enum4_list(c, q0, &d_quart, &nquart));
@@ -718,7 +736,7 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, double* 
             c->na4, c->d_fc4.p, c->ph_irr.evec.p + (size_t)q0 * 36, c->d_mass_rs.p, c->d_v4_c.p);
         SPRING_CHECK(launch_check(c, "k4_c0"));
         k4_bimg<<<nq * NM, 256, bimg_smem, c->stream>>>(
-            nq, c->na4, H, bk, c->d_v4_cnt.p, c->d_v4_map.p, c->d_v4_c.p, c->d_v4_ph.p, c->d_v4_etab.p,
+            nq, c->na4, H, mask, bk, c->d_v4_cnt.p, c->d_v4_map.p, c->d_v4_c.p, c->d_v4_ph.p, c->d_v4_etab.p,
             c->d_fc4_btyp.p, reinterpret_cast<__nv_bfloat16*>(c->d_v4_img.p));
         SPRING_CHECK(launch_check(c, "k4_bimg"));
         int ntiles = 0;

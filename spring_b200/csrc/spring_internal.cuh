@@ -307,7 +307,9 @@ int run_enum4_list(spring_ctx* c, int q0, const int4** d_quart, long long* nquar
 void free_enum4(spring_ctx* c);
 // k_v4tc.cu: tensor-core V4 + Gaussian four-phonon rate (BF16 / BF16x3) for two-atom cells;
 // *handled false when the cell or the precision does not take it
-int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, double* d_rate, bool* handled);
+// h_mask: per q0 of the block, the branches s0 (bit s0) to compute; null for all
+int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const int* h_mask, double* d_rate,
+                   bool* handled);
 // k_path.cu: LineWidth.x path mode; h_q0 (3, n_path) Cartesian, h_lw [T][p][s], h_omega [p][s]
 int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
              double* h_lw, double* h_omega);

@@ -97,3 +97,20 @@ def test_v4tc_wait_timeout_returns_status(runs):
     rate = ctx.linewidth4(1, ctx.nq0, delta="gauss", sigma=0.8)
     ctx.set_precision("fp64")
     np.testing.assert_allclose(rate, out[("bf16x3", 0.8)], rtol=1e-12, atol=0.0)
+
+
+def test_v4tc_branch_mask(runs):
+    """spring_linewidth4_modes: the selected branches of each q0 equal the full call's, the others
+    are zero (the surrogate-screened path spends exact work on selected modes only)."""
+    N, st, ctx, out = runs
+    ctx.set_precision("bf16x3")
+    rng = np.random.default_rng(N)
+    mask = rng.integers(0, 64, size=ctx.nq0).astype(np.int32)
+    mask[0] = 0x3f
+    rate = ctx.linewidth4_modes(1, mask, sigma=0.8)
+    ctx.set_precision("fp64")
+    full = out[("bf16x3", 0.8)]
+    sel = ((mask[:, None] >> np.arange(6)[None, :]) & 1).astype(bool)
+    for it in range(len(TEMPS)):
+        np.testing.assert_allclose(rate[it][sel], full[it][sel], rtol=1e-12, atol=1e-300)
+        assert not rate[it][~sel].any()
