@@ -56,6 +56,38 @@ def _compile(src: str, verbose_ptxas: bool) -> str:
     return obj
 
 
+HOST = os.path.join(HERE, "host")
+HOST_LIB = os.path.join(HERE, "libspring_host.so")
+CLI = os.path.join(HERE, "spring_kappa")
+CXX_FLAGS = ["-O2", "-std=c++17", "-Wall"]
+
+
+def _cxx() -> str:
+    for cand in (os.environ.get("CXX"), shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def build_host() -> str:
+    """libspring_host.so (the FC / result file formats, no CUDA) and the spring_kappa driver, which
+    links libspring_b200.so and libspring_host.so from its own directory."""
+    hsrc = [os.path.join(HOST, f) for f in ("h5lite.cpp", "namelist.cpp", "host_api.cpp")]
+    deps = hsrc + glob.glob(os.path.join(HOST, "*.hpp")) + [os.path.join(INCLUDE, "spring_host.h")]
+    if not os.path.exists(HOST_LIB) or any(os.path.getmtime(d) > os.path.getmtime(HOST_LIB) for d in deps):
+        r = subprocess.run([_cxx(), *CXX_FLAGS, "-fPIC", "-shared", *hsrc, "-o", HOST_LIB], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"host library build failed:\n{r.stdout}\n{r.stderr}")
+    cli_src = [os.path.join(HOST, "spring_kappa.cpp"), os.path.join(HOST, "namelist.cpp")]
+    cdeps = cli_src + [HOST_LIB, LIB, os.path.join(INCLUDE, "spring_gpu.h")]
+    if not os.path.exists(CLI) or any(os.path.getmtime(d) > os.path.getmtime(CLI) for d in cdeps):
+        r = subprocess.run([_cxx(), *CXX_FLAGS, *cli_src, "-L" + HERE, "-lspring_host", "-lspring_b200",
+                            "-Wl,-rpath,$ORIGIN", "-o", CLI], capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"spring_kappa build failed:\n{r.stdout}\n{r.stderr}")
+    return CLI
+
+
 def build(verbose_ptxas: bool = False) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
@@ -67,6 +99,7 @@ def build(verbose_ptxas: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
         os.replace(tmp, LIB)
+    build_host()
     return LIB
 
 

@@ -1,0 +1,121 @@
+"""The reference's input and output files, through libspring_host.so (include/spring_host.h).
+
+write_fc / read_fc: FC2nd_/FC3rd_/FC4th_<prefix><T>K_F.h5 in the layout r2ndFC / r3rdFC / r4thFC read
+(src/Kappa/Src/hdf5_wrap_mod.f90:40-337).  read_f64: one dataset of an output file such as
+kappa_<prefix><T>K.h5.  write_input: an input.nml with the namelists kappa.x reads.  The command-line
+driver ``spring_b200/spring_kappa`` runs kappa.x's flow on these files (its arguments are kappa.x's).
+Arrays follow the package's convention: C-order numpy arrays whose memory is the Fortran array.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+HOST_LIB = os.path.join(_HERE, "libspring_host.so")
+CLI = os.path.join(_HERE, "spring_kappa")
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(HOST_LIB):
+            raise ImportError(f"{HOST_LIB} is missing: build with `python -m spring_b200.build`")
+        lib = ct.CDLL(HOST_LIB)
+        P, I = ct.c_void_p, ct.c_int
+        sig = {"spring_h5_write_fc": [ct.c_char_p, I, I, I, P, P, P],
+               "spring_h5_fc_dims": [ct.c_char_p, I, P, P],
+               "spring_h5_read_fc": [ct.c_char_p, I, I, I, P, P, P],
+               "spring_h5_write_kappa": [ct.c_char_p, P, I, I, P, P, P],
+               "spring_h5_read_f64": [ct.c_char_p, ct.c_char_p, P, P, P, ct.c_longlong]}
+        for name, args in sig.items():
+            getattr(lib, name).argtypes = args
+            getattr(lib, name).restype = I
+        lib.spring_host_last_error.restype = ct.c_char_p
+        _lib = lib
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ct.c_void_p)
+
+
+def _check(rc):
+    if rc != 0:
+        raise OSError(load().spring_host_last_error().decode())
+
+
+def fc_file_name(order: int, prefix: str, T: float) -> str:
+    """'FC2nd_'//prefix//Temp_char//'K_F.h5' with Temp_char = F6.1 of T (main.f90:182-195)."""
+    tag = {2: "FC2nd_", 3: "FC3rd_", 4: "FC4th_"}[order]
+    return f"{tag}{prefix}{T:6.1f}".replace(" ", "") + "K_F.h5"
+
+
+def write_fc(path, order, atm_num, atm_indx, fc):
+    atm_num = np.ascontiguousarray(atm_num, np.int32)
+    atm_indx = np.ascontiguousarray(atm_indx, np.int32)
+    fc = np.ascontiguousarray(fc, np.float64)
+    nb, na = atm_indx.shape[0], atm_indx.shape[1]
+    _check(load().spring_h5_write_fc(os.fsencode(path), int(order), nb, na, _ptr(atm_num), _ptr(atm_indx), _ptr(fc)))
+
+
+def read_fc(path, order):
+    """(atm_num (Nb,), atm_indx (Nb, Na, 4), fc) with fc shaped like the synthetic crystal's."""
+    lib = load()
+    nb, na = ct.c_int(), ct.c_int()
+    _check(lib.spring_h5_fc_dims(os.fsencode(path), int(order), ct.byref(nb), ct.byref(na)))
+    nb, na = nb.value, na.value
+    num = np.zeros(nb, np.int32)
+    idx = np.zeros((nb, na, 4), np.int32)
+    shape = {2: (nb, na, 3, 3, 1), 3: (nb, na, na, 3, 3, 3), 4: (nb, na, na, na, 3, 3, 3, 3)}[order]
+    fc = np.zeros(shape)
+    _check(lib.spring_h5_read_fc(os.fsencode(path), int(order), nb, na, _ptr(num), _ptr(idx), _ptr(fc)))
+    return num, idx, fc
+
+
+def read_f64(path, name):
+    """A double dataset as a C-order array with the Fortran dimensions reversed."""
+    lib = load()
+    rank = ct.c_int()
+    dims = (ct.c_longlong * 8)()
+    _check(lib.spring_h5_read_f64(os.fsencode(path), name.encode(), ct.byref(rank), dims, None, 0))
+    fd = [int(dims[i]) for i in range(rank.value)]
+    out = np.zeros(int(np.prod(fd)) if fd else 1)
+    _check(lib.spring_h5_read_f64(os.fsencode(path), name.encode(), ct.byref(rank), dims, _ptr(out), out.size))
+    return out.reshape(fd[::-1])
+
+
+def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, four_phonon=False,
+                selection3=("D", "D", "D"), time_rev=0):
+    """An input.nml with &FCInfo, &CrystalInfo, &AtmInfo (unit_mod.f90:64-209) and &AnhInfo
+    (Helper_m.f90:37-132) for a synthetic crystal: one species per distinct mass."""
+    masses, typ = [], []
+    for m in cr.mass:
+        if float(m) not in masses:
+            masses.append(float(m))
+        typ.append(masses.index(float(m)) + 1)
+    L = []
+    L.append("&FCInfo\n    prefix = '%s'\n    SecondFC = .true.\n    ThirdFC = .true.\n    FourthFC = %s\n/\n"
+             % (prefix, ".true." if four_phonon else ".false."))
+    L.append("&CrystalInfo\n    Nbasis = %d\n    Ntyp = %d\n" % (cr.nbasis, len(masses)))
+    for k in range(3):
+        L.append("    Latvec(:, %d) = %s\n" % (k + 1, " ".join("%.16g" % v for v in cr.latvec[:, k])))
+    L.append("/\n&AtmInfo\n")
+    for i in range(cr.nbasis):
+        L.append("    atm_pos(:, %d) = %s\n" % (i + 1, " ".join("%.16g" % v for v in cr.basis_frac[i])))
+    L.append("    typ_indx = %s\n" % " ".join(str(t) for t in typ))
+    L.append("    mass = %s\n/\n" % " ".join("%.10g" % m for m in masses))
+    L.append("&AnhInfo\n    qmesh = %d %d %d\n    time_rev = %d\n" % (*qmesh, time_rev))
+    L.append("    SelectionRule3 = %s\n" % " ".join("'%s'" % s for s in selection3))
+    if sigma is not None:
+        L.append("    Sigma = %.16g\n" % sigma)
+    if isotope:
+        L.append("    isotope = .true.\n    g2iso = %s\n" % " ".join("%.16g" % g for g in g2iso))
+    if four_phonon:
+        L.append("    FourPhonon = .true.\n")
+    L.append("/\n")
+    with open(path, "w") as f:
+        f.write("".join(L))

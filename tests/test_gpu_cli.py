@@ -1,0 +1,72 @@
+"""spring_kappa end to end on the GPU: kappa.x's command line, namelists and FC files in, the kappa
+HDF5 file and the linewidth text file out, against the same computation through the Python API."""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+from spring_b200 import host_io as H
+from spring_b200 import synthetic as S
+from spring_b200.api import from_crystal
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(cr, d, extra, **nml):
+    H.write_input(os.path.join(d, "input.nml"), cr, "MgO", nml.pop("qmesh"), **nml)
+    for order in (2, 3, 4):
+        a = getattr(cr, f"fc{order}")
+        if a is None:
+            continue
+        H.write_fc(os.path.join(d, H.fc_file_name(order, "MgO", 300.0)), order, getattr(cr, f"fc{order}_atm_num"),
+                   getattr(cr, f"fc{order}_atm_indx"), a)
+    r = subprocess.run([H.CLI, "-inp", "input.nml", "-T", "300", *extra], cwd=d, capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    kap = H.read_f64(os.path.join(d, "kappa_MgO300.0K.h5"), "ThermalConductivityTensor")
+    lwf = H.read_f64(os.path.join(d, "kappa_MgO300.0K.h5"), "LineWidth")
+    txt = np.loadtxt(os.path.join(d, "linewidth_IBZ_MgO300.0K.txt"), comments="#")
+    return kap, lwf, txt
+
+
+def test_cli_three_phonon_tetrahedron_matches_api():
+    cr = S.build("rocksalt2")
+    N = 6
+    with tempfile.TemporaryDirectory() as d:
+        kap, lwf, txt = _run(cr, d, ["-Mode_resolved_k", "T"], qmesh=(N, N, N))
+        mk = H.read_f64(os.path.join(d, "kappa_MgO300.0K.h5"), "ModeResolvedKappa")
+    ctx, info = from_crystal(cr, (N, N, N), [300.0])
+    ctx.reset_linewidths()
+    ctx.linewidth3(1, ctx.nq0, delta="tetra", want=False)
+    lw = ctx.get_linewidths()[0]
+    om = ctx.get_phonons(1)["omega"]
+    k_api, mk_api = ctx.kappa_rta(info["Rxyz"], mode=True)
+    ctx.close()
+    np.testing.assert_allclose(kap, k_api[0], rtol=1e-9, atol=1e-12 * np.abs(k_api).max())
+    np.testing.assert_allclose(mk, mk_api[0], rtol=1e-9, atol=1e-12 * np.abs(mk_api).max())
+    np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(lwf[:, :6], om, rtol=1e-12, atol=0)
+    # the text file: Ndof frequencies then Ndof linewidths per irreducible point, 12 significant digits
+    np.testing.assert_allclose(txt[:, :6], om, rtol=1e-11, atol=1e-11)
+    np.testing.assert_allclose(txt[:, 6:], lw, rtol=1e-11, atol=1e-14)
+
+
+def test_cli_four_phonon_isotope_gauss_bf16x3_matches_api():
+    cr = S.build("rocksalt2", fc4=True)
+    N = 4
+    g2 = [1e-3, 1e-3]
+    with tempfile.TemporaryDirectory() as d:
+        kap, lwf, _ = _run(cr, d, ["-delta", "gauss", "-precision", "bf16x3"], qmesh=(N, N, N), sigma=0.8,
+                           isotope=True, g2iso=g2, four_phonon=True)
+    ctx, info = from_crystal(cr, (N, N, N), [300.0], with_fc4=True)
+    ctx.set_precision("bf16x3")
+    ctx.reset_linewidths()
+    ctx.linewidth3(1, ctx.nq0, delta="gauss", sigma=0.8, want=False)
+    ctx.linewidth_iso(1, ctx.nq0, g2, delta="gauss", sigma=0.8, want=False)
+    ctx.linewidth4(1, ctx.nq0, delta="gauss", sigma=0.8, want=False)
+    lw = ctx.get_linewidths()[0]
+    k_api = ctx.kappa_rta(info["Rxyz"])[0]
+    ctx.close()
+    np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-10, atol=1e-14)
+    np.testing.assert_allclose(kap, k_api, rtol=1e-9, atol=1e-12 * np.abs(k_api).max())
