@@ -34,6 +34,12 @@ int spring_h5_read_fc(const char* path, int order, int nb, int na, int* atm_num,
 int spring_h5_write_kappa(const char* path, const double* kappa, int ndof, int nq0, const double* linewidth,
                           const double* phase_space, const double* mode_k);
 
+/* The linewidth restart file of kappa.x (w_RestartLW / r_RestartLW, hdf5_wrap_mod.f90:340-401 and
+ * :562-647; Restart_<prefix>/<prefix><T>K_LW_Restart.h5): progress(2) = (last irreducible point
+ * done, 1 when it completed) and LW_data(Ndof, Nq0). */
+int spring_h5_write_restart(const char* path, int ndof, int nq0, int i0, int complete, const double* lw);
+int spring_h5_read_restart(const char* path, int ndof, int nq0, int* progress, double* lw);
+
 /* One double dataset at `name` ("a/b" for a dataset in a group): *rank and fdims (Fortran order,
  * up to 8); the data go to out when out != NULL and cap (elements) is large enough. */
 int spring_h5_read_f64(const char* path, const char* name, int* rank, long long* fdims, double* out, long long cap);

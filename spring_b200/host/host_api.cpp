@@ -152,6 +152,33 @@ int spring_h5_write_kappa(const char* path, const double* kappa, int ndof, int n
     return e.empty() ? 0 : fail(e);
 }
 
+int spring_h5_write_restart(const char* path, int ndof, int nq0, int i0, int complete, const double* lw) {
+    if (!path || !lw || ndof < 1 || nq0 < 1) return fail("spring_h5_write_restart: bad arguments");
+    h5lite::Group root;
+    const int32_t prog[2] = {i0, complete};
+    root.datasets["progress"] = h5lite::make_i32(prog, {2});
+    root.datasets["LW_data"] = h5lite::make_f64(lw, {(uint64_t)ndof, (uint64_t)nq0});
+    const std::string e = h5lite::write_file(path, root);
+    return e.empty() ? 0 : fail(e);
+}
+
+int spring_h5_read_restart(const char* path, int ndof, int nq0, int* progress, double* lw) {
+    if (!path || !progress || !lw) return fail("spring_h5_read_restart: bad arguments");
+    h5lite::Group root;
+    std::string e = h5lite::read_file(path, root);
+    if (!e.empty()) return fail(e);
+    const h5lite::Dataset* p = find(root, "progress");
+    const h5lite::Dataset* d = find(root, "LW_data");
+    if (!p || p->type != h5lite::Type::I32 || p->count() != 2) return fail(std::string(path) + ": no progress(2)");
+    if (!d || d->type != h5lite::Type::F64) return fail(std::string(path) + ": no LW_data");
+    const std::vector<uint64_t> fd = h5lite::fortran_dims(*d);
+    if (fd.size() != 2 || (int)fd[0] != ndof || (int)fd[1] != nq0)
+        return fail(std::string(path) + ": LW_data is not (Ndof, Nq0) of this run");
+    std::memcpy(progress, p->data.data(), 2 * sizeof(int));
+    std::memcpy(lw, d->data.data(), d->data.size());
+    return 0;
+}
+
 int spring_h5_read_f64(const char* path, const char* name, int* rank, long long* fdims, double* out, long long cap) {
     if (!path || !name || !rank || !fdims) return fail("spring_h5_read_f64: bad arguments");
     h5lite::Group root;

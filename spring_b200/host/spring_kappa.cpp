@@ -11,11 +11,16 @@
 // (WriteAsciiOutFile, Helper_m.f90:597-667, format Ndof-1 (G20.12,'  '), G20.12).  Every q0 is
 // computed by the library in one call (the q0 loop of main.f90:552-715): tetrahedron 3-phonon
 // linewidths (the scheme kappa.x ships; -delta gauss uses Sigma), isotope scattering when isotope
-// is set, four-phonon rates when FourPhonon is set, RTA kappa (symmetrised by default).  The point
+// is set, four-phonon rates when FourPhonon is set, RTA kappa (symmetrised by default); with
+// WriteRestart / ReadRestart the linewidth restart file (main.f90:502-545) is rewritten after every
+// block of points and read back to skip the points already done.  The point
 // group comes from the lattice and basis (the rotations spg_get_symmetry gives for a primitive
 // cell); the phonons from the device eigensolver.  Extensions: -precision selects the tensor-core
 // arithmetic of the Gaussian V3/V4; -dry-run reads and checks every input and prints them as JSON
 // without a GPU.
+#include <sys/stat.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -227,7 +232,7 @@ int main(int argc, char** argv) {
     std::vector<double> g2iso(nb, 0.0);
     std::vector<int> qmesh{7, 7, 7}, shift{0, 0, 0};
     int time_rev = 0;
-    bool isotope = false, four = false;
+    bool isotope = false, four = false, wrestart = false, rrestart = false;
     check(nml::get(anh, "SelectionRule3", {3}, sel3));
     check(nml::get(anh, "SelectionRule4", {4}, sel4));
     check(nml::get(anh, "Sigma", sigma));
@@ -238,6 +243,8 @@ int main(int argc, char** argv) {
     check(nml::get(anh, "time_rev", time_rev));
     check(nml::get(anh, "isotope", isotope));
     check(nml::get(anh, "FourPhonon", four));
+    check(nml::get(anh, "WriteRestart", wrestart));
+    check(nml::get(anh, "ReadRestart", rrestart));
     const int ndof = 3 * nb;
     auto pol = [&](const std::vector<std::string>& sel) {  // PolarizationStrtEnd, Helper_m.f90:310-353
         std::vector<int> p;
@@ -307,12 +314,37 @@ int main(int argc, char** argv) {
     if (precision != "fp64" && precision != "bf16" && precision != "bf16x3") die("-precision: fp64, bf16 or bf16x3");
     gpu(c, spring_set_precision(c, prec));
     const int dm = delta == "gauss" ? SPRING_DELTA_GAUSS : SPRING_DELTA_TETRA;
-    std::vector<double> lw((size_t)ndof * nq0), p3((size_t)ndof * nq0);
+    std::vector<double> lw_all((size_t)ndof * nq0, 0.0), omega((size_t)ndof * nq0), p3((size_t)ndof * nq0, 0.0);
     gpu(c, spring_reset_linewidths(c));
-    gpu(c, spring_linewidth3(c, 1, nq0, dm, sigma, pol3.data(), lw.data(), p3.data()));
-    if (isotope) gpu(c, spring_linewidth_iso(c, 1, nq0, dm, sigma, g2iso.data(), nullptr));
-    if (four) gpu(c, spring_linewidth4(c, 1, nq0, dm, sigma, pol4.data(), nullptr));
-    std::vector<double> lw_all((size_t)ndof * nq0), omega((size_t)ndof * nq0);
+    // Restart (main.f90:502-545, 630-713): LW_Allq0 of the points already done comes from the
+    // restart file, and the loop starts after them; with WriteRestart the file is rewritten after
+    // every block of points.
+    const std::string rdir = "Restart_" + prefix, rfile = rdir + "/" + prefix + tc + "K_LW_Restart.h5";
+    int start = 1;
+    if (rrestart) {
+        int prog[2] = {0, 0};
+        if (spring_h5_read_restart(rfile.c_str(), ndof, nq0, prog, lw_all.data())) die(spring_host_last_error());
+        start = prog[1] == 1 ? prog[0] + 1 : std::max(1, prog[0]);
+        for (int q = start - 1; q < nq0; ++q)
+            for (int s = 0; s < ndof; ++s) lw_all[(size_t)ndof * q + s] = 0.0;  // recomputed below
+        gpu(c, spring_set_linewidths(c, lw_all.data()));
+        std::printf("restart: %d of %d irreducible points read from %s\n", start - 1, nq0, rfile.c_str());
+    }
+    if (wrestart) mkdir(rdir.c_str(), 0755);
+    const int block = wrestart ? std::max(1, (nq0 + 15) / 16) : nq0;
+    for (int i0 = start; i0 <= nq0; i0 += block) {
+        const int n = std::min(block, nq0 - i0 + 1);
+        std::vector<double> p3b((size_t)ndof * n);
+        gpu(c, spring_linewidth3(c, i0, n, dm, sigma, pol3.data(), nullptr, p3b.data()));
+        std::copy(p3b.begin(), p3b.end(), p3.begin() + (size_t)ndof * (i0 - 1));
+        if (isotope) gpu(c, spring_linewidth_iso(c, i0, n, dm, sigma, g2iso.data(), nullptr));
+        if (four) gpu(c, spring_linewidth4(c, i0, n, dm, sigma, pol4.data(), nullptr));
+        if (wrestart) {
+            gpu(c, spring_get_linewidths(c, lw_all.data()));
+            if (spring_h5_write_restart(rfile.c_str(), ndof, nq0, i0 + n - 1, 1, lw_all.data()))
+                die(spring_host_last_error());
+        }
+    }
     gpu(c, spring_get_linewidths(c, lw_all.data()));
     gpu(c, spring_get_phonons(c, 1, nullptr, omega.data(), nullptr, nullptr, nullptr));
     // branch window of the kappa sum: Polarization3rd (and 4th) first rows

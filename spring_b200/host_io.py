@@ -30,7 +30,9 @@ def load():
                "spring_h5_fc_dims": [ct.c_char_p, I, P, P],
                "spring_h5_read_fc": [ct.c_char_p, I, I, I, P, P, P],
                "spring_h5_write_kappa": [ct.c_char_p, P, I, I, P, P, P],
-               "spring_h5_read_f64": [ct.c_char_p, ct.c_char_p, P, P, P, ct.c_longlong]}
+               "spring_h5_read_f64": [ct.c_char_p, ct.c_char_p, P, P, P, ct.c_longlong],
+               "spring_h5_write_restart": [ct.c_char_p, I, I, I, I, P],
+               "spring_h5_read_restart": [ct.c_char_p, I, I, P, P]}
         for name, args in sig.items():
             getattr(lib, name).argtypes = args
             getattr(lib, name).restype = I
@@ -88,8 +90,22 @@ def read_f64(path, name):
     return out.reshape(fd[::-1])
 
 
+def write_restart(path, progress, lw):
+    """Restart file (w_RestartLW): progress (i0, complete) and LW_data, lw shaped (Nq0, Ndof)."""
+    lw = np.ascontiguousarray(lw, np.float64)
+    _check(load().spring_h5_write_restart(os.fsencode(path), lw.shape[1], lw.shape[0], int(progress[0]),
+                                          int(progress[1]), _ptr(lw)))
+
+
+def read_restart(path, ndof, nq0):
+    prog = np.zeros(2, np.int32)
+    lw = np.zeros((nq0, ndof))
+    _check(load().spring_h5_read_restart(os.fsencode(path), int(ndof), int(nq0), _ptr(prog), _ptr(lw)))
+    return (int(prog[0]), int(prog[1])), lw
+
+
 def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, four_phonon=False,
-                selection3=("D", "D", "D"), time_rev=0):
+                selection3=("D", "D", "D"), time_rev=0, write_restart=False, read_restart=False):
     """An input.nml with &FCInfo, &CrystalInfo, &AtmInfo (unit_mod.f90:64-209) and &AnhInfo
     (Helper_m.f90:37-132) for a synthetic crystal: one species per distinct mass."""
     masses, typ = [], []
@@ -116,6 +132,10 @@ def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, 
         L.append("    isotope = .true.\n    g2iso = %s\n" % " ".join("%.16g" % g for g in g2iso))
     if four_phonon:
         L.append("    FourPhonon = .true.\n")
+    if write_restart:
+        L.append("    WriteRestart = .true.\n")
+    if read_restart:
+        L.append("    ReadRestart = .true.\n")
     L.append("/\n")
     with open(path, "w") as f:
         f.write("".join(L))

@@ -70,3 +70,23 @@ def test_cli_four_phonon_isotope_gauss_bf16x3_matches_api():
     ctx.close()
     np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-10, atol=1e-14)
     np.testing.assert_allclose(kap, k_api, rtol=1e-9, atol=1e-12 * np.abs(k_api).max())
+
+
+def test_cli_restart_skips_the_points_already_done():
+    """WriteRestart leaves the linewidth restart file; a run with ReadRestart from a file that holds
+    only the first points (progress (k, 1)) computes the rest and gives the same results."""
+    cr = S.build("rocksalt2")
+    N = 5
+    with tempfile.TemporaryDirectory() as d:
+        kap1, lwf1, _ = _run(cr, d, [], qmesh=(N, N, N), write_restart=True)
+        rfile = os.path.join(d, "Restart_MgO", "MgO300.0K_LW_Restart.h5")
+        prog, lw = H.read_restart(rfile, 6, lwf1.shape[0])
+        assert prog == (lwf1.shape[0], 1)
+        np.testing.assert_array_equal(lw, lwf1[:, 6:])
+        k = lwf1.shape[0] // 2
+        part = lw.copy()
+        part[k:] = 0.0
+        H.write_restart(rfile, (k, 1), part)
+        kap2, lwf2, _ = _run(cr, d, [], qmesh=(N, N, N), read_restart=True)
+    np.testing.assert_allclose(lwf2, lwf1, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(kap2, kap1, rtol=1e-12, atol=1e-14 * np.abs(kap1).max())

@@ -100,3 +100,15 @@ def test_driver_reports_missing_files(cr4):
         H.write_input(os.path.join(d, "input.nml"), cr4, "MgO", (4, 4, 4))
         r = subprocess.run([H.CLI, "-inp", "input.nml", "-T", "300", "-dry-run"], cwd=d, capture_output=True, text=True)
         assert r.returncode != 0 and "FC2nd_MgO300.0K_F.h5" in r.stderr
+
+
+def test_restart_file_round_trip():
+    lw = np.random.default_rng(1).normal(size=(29, 6))
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "MgO300.0K_LW_Restart.h5")
+        H.write_restart(p, (17, 1), lw)
+        prog, back = H.read_restart(p, 6, 29)
+        assert prog == (17, 1)
+        assert np.array_equal(back, lw)
+        with pytest.raises(OSError, match="not \\(Ndof, Nq0\\)"):
+            H.read_restart(p, 6, 30)  # another run's file
