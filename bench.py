@@ -52,7 +52,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mesh4", type=int, default=12, help="mesh of the four-phonon leg (0 skips it)")
+    ap.add_argument("--mesh4", type=int, default=16, help="mesh of the four-phonon leg (0 skips it)")
+    ap.add_argument("--no-fp64-4ph", action="store_true", help="skip the FP64 run of the four-phonon leg")
+    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-screened leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-workload leg")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
                     help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
@@ -300,63 +302,146 @@ def run_reference(args):
     return 0
 
 
-def fourph_leg(torch, mesh4, frac=0.1):
-    """Four-phonon leg: exact Gaussian 4-phonon rates of every irreducible q0 (FP64 V4) on a mesh4^3
-    mesh at 300 K, timed; then the surrogate (trained on exact rates of the 8^3 mesh) screens the q0
-    blocks, exact V4 runs for the top `frac`, and kappa is compared with the all-exact one."""
-    from spring_b200 import surrogate as SG
+def _ev_ms(torch, fn):
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    r = fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return r, e0.elapsed_time(e1)
+
+
+def _kdiag(k):
+    return np.array([k[0], k[4], k[8]])
+
+
+def fourph_c3_leg(torch, mesh=16, prec4="bf16x3", fp64=True):
+    """Three-phonon + four-phonon + isotope kappa of the rocksalt cell with FC4 at mesh^3, 300 K,
+    Gaussian 2 cm^-1, isotope g2 = 1e-3 on both atoms.  Timed from the phonons to kappa, once with
+    the tensor-core V3 (BF16x3) and V4 (prec4), once with the plain FP64 path (k_v3s + k_v4); the
+    line gives both times, the kappa and rate errors of the mixed path against FP64, and the
+    tensor-core V4 kernel time."""
     from spring_b200 import synthetic as S
     from spring_b200.api import from_crystal
     cr = S.build("rocksalt2", fc4=True)
     T = [300.0]
+    g2 = [1e-3, 1e-3]
+    ctx, info = from_crystal(cr, (mesh,) * 3, T, with_fc4=True)
+    quartets = sum(ctx.count4(i + 1)[0] for i in range(ctx.nq0))
 
-    def ev_ms(fn):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize()
-        e0.record()
-        r = fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return r, e0.elapsed_time(e1)
+    def run(p3, p4):
+        def step():
+            ctx.compute_phonons(T)
+            ctx.reset_linewidths()
+            ctx.set_precision(p3)
+            ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA, want=False)
+            ctx.linewidth_iso(1, ctx.nq0, g2, delta="gauss", sigma=SIGMA, want=False)
+            ctx.set_precision(p4)
+            r4 = ctx.linewidth4(1, ctx.nq0, "gauss", SIGMA)
+            return r4, ctx.get_linewidths(), ctx.kappa_rta(info["Rxyz"])[0]
+        return _ev_ms(torch, step)
+
+    run("bf16x3", prec4)  # warm-up (allocations, tables)
+    ctx.set_profiling(True)
+    (r4m, lwm, km), ms_m = run("bf16x3", prec4)
+    v4_ms, v4_n = ctx.kernel_time("k_v4tc")
+    ctx.set_profiling(False)
+    out = {"mesh": [mesh] * 3, "temperature": 300.0, "isotope_g2": g2, "sigma_rad_ps": SIGMA,
+           "irreducible_q0": int(ctx.nq0), "quartets": int(quartets), "v4_arithmetic": prec4,
+           "time_to_kappa_ms": ms_m, "v4tc_kernel_ms": v4_ms, "v4tc_launches": v4_n,
+           "evals_per_s_4ph": quartets * 6 ** 4 / (v4_ms * 1e-3) if v4_ms else None,
+           "kappa_diag": _kdiag(km).tolist(),
+           "what": "phonons + 3ph (bf16x3 V3) + isotope + 4ph (tensor-core V4) + RTA kappa, every q0; one 4ph eval = "
+                   "one (s0..s3) of one quartet"}
+    if fp64:
+        (r4f, lwf, kf), ms_f = run("fp64", "fp64")
+        big = r4f > 1e-3 * r4f.max()
+        lbig = lwf > 1e-3 * lwf.max()
+        out.update({"fp64_time_to_kappa_ms": ms_f, "fp64_over_mixed": ms_f / ms_m,
+                    "kappa_max_rel_err_vs_fp64": float(np.abs(_kdiag(km) / _kdiag(kf) - 1).max()),
+                    "linewidth_max_rel_err_vs_fp64": float((np.abs(lwm[lbig] - lwf[lbig]) / lwf[lbig]).max()),
+                    "rate4_max_rel_err_vs_fp64": float((np.abs(r4m[big] - r4f[big]) / r4f[big]).max()),
+                    "fp64_kappa_diag": _kdiag(kf).tolist()})
+    ctx.close()
+    return out
+
+
+def surrogate_c5_leg(torch, train_mesh=12, mesh=20, frac=0.25, members=3):
+    """Surrogate-screened four-phonon kappa: a network ensemble (5-128-128-128-1, SiLU, trained on
+    the GPU with the library's kernels on the exact rates of a train_mesh^3 mesh at 300 and 900 K)
+    ranks the (q0, branch) blocks of the mesh^3 mesh; exact tensor-core V4 runs for the top `frac`
+    of them and the prediction (BF16 tensor-core inference) stands in elsewhere.  Compared with the
+    full exact four-phonon kappa on the same GPU, and with a network-free estimate
+    (log r4 = a + b log r3 fitted on the same training rates) given the same exact budget."""
+    from spring_b200 import surrogate as SG
+    from spring_b200 import synthetic as S
+    from spring_b200.api import from_crystal
+    cr = S.build("rocksalt2", fc4=True)
+    T = [300.0, 900.0]
 
     def mesh_data(N):
         ctx, info = from_crystal(cr, (N, N, N), T, with_fc4=True)
+        ctx.set_precision("bf16x3")
         ctx.reset_linewidths()
-        lw3 = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)[0][0]
-        r4, ms = ev_ms(lambda: ctx.linewidth4(1, ctx.nq0, "gauss", SIGMA)[0])
+        lw3 = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)[0]
         ph = ctx.get_phonons(1)
         q = ((cr.G / N) @ info["irr_q_pnt_int"].T.astype(float)).T
-        X = SG.mode_features(ph["omega"], ph["grp_vel"], 2.0 * lw3, q)
-        return ctx, info, lw3, r4, ph, X, ms
+        X = [SG.mode_features(ph["omega"], ph["grp_vel"], 2.0 * lw3[t], q) for t in range(len(T))]
+        return ctx, info, lw3, ph, X
 
-    c8, _, _, r8, _, X8, _ = mesh_data(8)
-    y = r8.ravel()
-    m = (y > 0) & (X8[:, 2] > 0)
-    sur = SG.Surrogate(c8, seed=1)
-    _, train_ms = ev_ms(lambda: sur.fit(X8[m], np.log(y[m]), epochs=600, batch=32, lr=2e-3))
-    c, info, lw3, r_ex, ph, X, exact_ms = mesh_data(mesh4)
+    ct, _, lw_t, _, X_t = mesh_data(train_mesh)
+    r_t, train_exact_ms = _ev_ms(torch, lambda: ct.linewidth4(1, ct.nq0, "gauss", SIGMA))
+    X_all = np.concatenate(X_t)
+    y_all = r_t.reshape(-1)
+    m = (y_all > 0) & (X_all[:, 2] > 0)
+    sur = SG.Surrogate(ct, seed=1, members=members)
+    _, train_ms = _ev_ms(torch, lambda: sur.fit(X_all[m], np.log(y_all[m]), epochs=300, batch=64, lr=2e-3))
+    pl = SG.PowerLaw().fit(X_all[:, 2], y_all)
+
+    c, info, lw3, ph, X = mesh_data(mesh)
     quartets = sum(c.count4(i + 1)[0] for i in range(c.nq0))
-    pred, pred_ms = ev_ms(lambda: np.exp(sur.predict(X, bf16=True)).reshape(c.nq0, -1))
-    w = SG.kappa_weight(ph["omega"], ph["nbe"][0], ph["grp_vel"], info["multiplicity"])
-    order, _ = SG.rank_blocks(2.0 * lw3, pred, w)
-    (scr, mask), scr_ms = ev_ms(lambda: SG.screened_rates4(c, pred, order, frac, delta="gauss", sigma=SIGMA))
+    r_ex, exact_ms = _ev_ms(torch, lambda: c.linewidth4(1, c.nq0, "gauss", SIGMA))
+
+    def predict():
+        out = [sur.predict(X[t], bf16=True) for t in range(len(T))]
+        return (np.exp(np.array([o[0] for o in out])).reshape(len(T), c.nq0, -1),
+                np.array([o[1] for o in out]).reshape(len(T), c.nq0, -1))
+    (pred, spread), pred_ms = _ev_ms(torch, predict)
+    pred_pl = np.array([pl.predict(2.0 * lw3[t]) for t in range(len(T))])
+    w = np.array([SG.kappa_weight(ph["omega"], ph["nbe"][t], ph["grp_vel"], info["multiplicity"]) for t in range(len(T))])
 
     def kappa(r4):
-        c.set_linewidths((lw3 + 0.5 * r4)[None])
-        k = c.kappa_rta(info["Rxyz"])[0]
-        return float(np.mean([k[0], k[4], k[8]]))
+        c.set_linewidths(lw3 + 0.5 * r4)
+        return c.kappa_rta(info["Rxyz"])
 
-    k_ex, k_scr, k_wo = kappa(r_ex), kappa(scr), kappa(np.where(mask[:, None], r_ex, 0.0))
+    def screened(p, unc):
+        sc = np.max([SG.mode_scores(2.0 * lw3[t], p[t], w[t], None if unc is None else unc[t])
+                     for t in range(len(T))], axis=0)
+        masks, sel = SG.select_modes(sc, frac)
+        (r, _), ms = _ev_ms(torch, lambda: SG.screened_rates4(c, p, masks, sigma=SIGMA))
+        return r, ms
+
+    r_net, scr_ms = screened(pred, spread)
+    r_pl, _ = screened(pred_pl, None)
+    k_ex, k_net, k_pl = kappa(r_ex), kappa(r_net), kappa(r_pl)
+    err = lambda k: [float(np.abs(_kdiag(k[t]) / _kdiag(k_ex[t]) - 1).max()) for t in range(len(T))]
+    ok = (r_ex > 0) & (np.stack([x[:, 2] for x in X]).reshape(r_ex.shape) > 0)
+    out = {"train_mesh": [train_mesh] * 3, "mesh": [mesh] * 3, "temperatures": T, "irreducible_q0": int(c.nq0),
+           "quartets": int(quartets), "fraction_exact_blocks": frac, "ensemble_members": members,
+           "exact_ms": exact_ms, "screened_ms": scr_ms + pred_ms, "exact_over_screened": exact_ms / (scr_ms + pred_ms),
+           "screened_exact_part_ms": scr_ms, "prediction_ms": pred_ms, "train_ms": train_ms,
+           "train_exact_rates_ms": train_exact_ms,
+           "kappa_exact_diag": [_kdiag(k).tolist() for k in k_ex],
+           "kappa_rel_err_screened": err(k_net), "kappa_rel_err_network_free_same_budget": err(k_pl),
+           "median_abs_log_err_prediction": float(np.median(np.abs(np.log(pred[ok]) - np.log(r_ex[ok])))),
+           "v4_arithmetic": "bf16x3",
+           "what": "blocks = (irreducible q0, branch s0) of the quartet sum; ranked by predicted kappa impact x "
+                   "(1 + ensemble spread of the log prediction); exact V4 (spring_linewidth4_modes) on the top "
+                   "fraction, network (BF16 tensor-core inference) elsewhere"}
     c.close()
-    c8.close()
-    return {"mesh": [mesh4] * 3, "temperature": 300.0, "irreducible_q0": int(len(order)), "quartets": int(quartets),
-            "evals_per_s_exact": quartets * 36 * 36 / (exact_ms * 1e-3), "exact_ms": exact_ms,
-            "screened_ms": scr_ms + pred_ms, "exact_over_screened": exact_ms / (scr_ms + pred_ms),
-            "screened_exact_part_ms": scr_ms, "prediction_ms": pred_ms,
-            "fraction_exact": frac, "kappa_exact": k_ex, "kappa_rel_err_screened": abs(k_scr / k_ex - 1),
-            "kappa_rel_err_same_blocks_without_network": abs(k_wo / k_ex - 1), "train_ms_8cubed": train_ms,
-            "v4_arithmetic": "f64", "what": "one 4ph eval = one (s0..s3) of one quartet; surrogate 5-128-128-128-1 "
-                                            "SiLU, trained on the GPU on exact 8^3 rates, BF16 inference"}
+    ct.close()
+    return out
 
 
 BATCH_CELLS = (("rocksalt2", 12), ("rocksalt2", 16), ("rocksalt2", 20), ("rocksalt8", 8), ("rocksalt8", 10))
@@ -588,7 +673,8 @@ def run_ours(args):
             e2e_ms = float(t.item())
 
     peak = fp64_peak_tflops(torch) if rank == 0 else None
-    four = fourph_leg(torch, args.mesh4) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
+    four = fourph_c3_leg(torch, args.mesh4, fp64=not args.no_fp64_4ph) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
+    sur = surrogate_c5_leg(torch) if (rank == 0 and world == 1 and not args.no_surrogate) else None
     batched = batched_leg(torch) if (rank == 0 and world == 1 and not args.no_batch) else None
     cpu = None
     oracle_check = None
@@ -669,7 +755,8 @@ def run_ours(args):
                                   "what": "one step = phonons + pairs + linewidths at 3 T + RTA kappa; errors over "
                                           "every mode with a linewidth above 1e-3 of the largest, kappa diagonal"},
                 "fp64_path": {"value": evals_total / (ms64 * 1e-3), "unit": "evals/s", "ms_per_step": ms64},
-                "fourph": four,
+                "fourph_c3": four,
+                "surrogate_c5": sur,
                 "batched": batched,
                 "roofline": roof,
                 "cpu_baseline": cpu,

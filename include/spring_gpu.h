@@ -328,6 +328,11 @@ int spring_batch_result(spring_batch* batch, int index, double* lw, double* p3_q
  * memory and returns; the call fails with SPRING_ERR_TIMEOUT.  For testing callers' handling
  * of that status: 0 makes every such wait run out at once. */
 #define SPRING_OPT_WAIT_POLLS 2
+/* SPRING_OPT_FP64_PRESCREEN = 3: value 1 makes the FP64 Gaussian 3-phonon linewidth of two-atom
+ * cells (k_v3s) skip the pairs with no mode triple inside the window where a delta weight exceeds
+ * exp(-40) of its peak (the tensor-core path's pre-screen; the linewidths change below 1e-13
+ * relative); 0 (default) evaluates every pair. */
+#define SPRING_OPT_FP64_PRESCREEN 3
 int spring_set_option(spring_ctx* ctx, int option, int value);
 
 /* ---- diagnostics ------------------------------------------------------- */

@@ -21,6 +21,7 @@ SPRING_ERR_INJECTED = 6
 SPRING_ERR_TIMEOUT = 7
 SPRING_OPT_GENERIC_V3 = 1
 SPRING_OPT_WAIT_POLLS = 2
+SPRING_OPT_FP64_PRESCREEN = 3
 SPRING_DELTA_GAUSS = 0
 SPRING_DELTA_TETRA = 1
 SPRING_FP64 = 0

@@ -408,6 +408,7 @@ int spring_set_option(spring_ctx* c, int option, int value) {
     switch (option) {
         case SPRING_OPT_GENERIC_V3: c->force_generic_v3 = value != 0; return SPRING_OK;
         case SPRING_OPT_WAIT_POLLS: c->tc_max_spins = value < 0 ? -1 : (long long)value; return SPRING_OK;
+        case SPRING_OPT_FP64_PRESCREEN: c->fp64_prescreen = value != 0; return SPRING_OK;
         default: return fail(c, SPRING_ERR_ARG, "unknown option %d", option);
     }
 }

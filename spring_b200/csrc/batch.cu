@@ -255,6 +255,7 @@ int build_desc(spring_batch* b, std::vector<BatchDesc>& D, std::vector<long long
             a3.q0_first = w.q0;
             a3.pair_first = c->ps_irr.h_pairoff[w.q0];
             a3.pair_end = c->ps_irr.h_pairoff[w.q0 + w.n_q0];
+            a3.plist = nullptr;
             a3.ngroups = (int)w.items;
             a3.mfac = a.mfac;
             a3.onebysigma = a.onebysigma;

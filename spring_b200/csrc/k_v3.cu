@@ -102,9 +102,18 @@ int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol&
         SPRING_CHECK(run_v3tc_gauss(c, q0_first, n_q0, sigma, pol, d_lw, d_p3, &handled));
         if (handled) return SPRING_OK;
     }
-    if (!c->force_generic_v3)
+    if (!c->force_generic_v3) {
+        // optional: only the pairs with a mode triple inside the Gaussian's exp(-40) window (the
+        // tensor-core path's pre-screen), every weight of the others being below that cut
+        const int* plist = nullptr;
+        int nlist = 0;
+        if (c->fp64_prescreen && c->nb == 2 && c->na3 <= 8) {
+            SPRING_CHECK(run_v3_prescreen(c, q0_first, n_q0, sigma, &plist, &nlist));
+            if (nlist == 0) return SPRING_OK;
+        }
         SPRING_CHECK(launch_v3s(c, c->ps_irr, irr_view(c), q0_first, n_q0, 0, sigma, &pol, d_lw, d_p3, nullptr,
-                                &handled));
+                                &handled, plist, nlist));
+    }
     if (handled) return SPRING_OK;
     V3Args a{};
     a.onebysigma = 1.0 / sigma;

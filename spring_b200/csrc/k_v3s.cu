@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_v3s(S3Args a_, S3Ptrs P_, const 
 
 // Launch the specialised kernel when the cell fits it; *handled tells the caller.
 int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
-               const Pol* pol, double* lw, double* p3, double* w, bool* handled) {
+               const Pol* pol, double* lw, double* p3, double* w, bool* handled, const int* plist, int nlist) {
     *handled = false;
     if (c->nb != NB || c->na3 != NA || c->nT > MAXT) return SPRING_OK;
     *handled = true;
@@ -57,7 +57,12 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
     // Host offsets when they were read already; otherwise the kernel reads its range on the device
     // and the grid is sized by the bound of at most Nq/2 + 8 pairs per q0 (no readback, no wait).
     const int* range = nullptr;
-    if (ps.h_ok) {
+    a.plist = plist;
+    if (plist) {  // an explicit list of pairs (the Gaussian window's pre-screen)
+        a.pair_first = 0;
+        a.pair_end = nlist;
+        a.ngroups = (nlist + PP - 1) / PP;
+    } else if (ps.h_ok) {
         a.pair_first = ps.h_pairoff[q0_first];
         a.pair_end = ps.h_pairoff[q0_first + n_q0];
         a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;

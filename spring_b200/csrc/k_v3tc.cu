@@ -943,6 +943,18 @@ int build_tiles_end(spring_ctx* c) {
 
 }  // namespace
 
+int run_v3_prescreen(spring_ctx* c, int q0_first, int n_q0, double sigma, const int** d_list, int* n) {
+    const PairSet& ps = c->ps_irr;
+    const int nmax = (int)std::min<long long>(ps.cap, (long long)n_q0 * (c->nq / 2 + 8));
+    const double os = 1.0 / sigma;
+    const float rf = (float)(sqrt(EXP_CUT / (0.5 * (os * os))) * 1.0001 + 1e-3);
+    SPRING_CHECK(build_tiles_begin(c, q0_first, n_q0, nmax, rf));
+    SPRING_CHECK(build_tiles_end(c));
+    *d_list = c->d_tc_entries.p;  // sorted by q1; the pairs with a triple in the window come first
+    *n = c->tc_npairs;
+    return SPRING_OK;
+}
+
 int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
                    bool* handled) {
     *handled = false;

@@ -104,6 +104,7 @@ struct spring_ctx {
     int precision = SPRING_FP64;
     bool force_generic_v3 = false;  // spring_set_option(SPRING_OPT_GENERIC_V3): use the any-cell V3 kernel
     long long tc_max_spins = -1;    // spring_set_option(SPRING_OPT_WAIT_POLLS); -1: the kernels' default
+    bool fp64_prescreen = false;    // spring_set_option(SPRING_OPT_FP64_PRESCREEN)
 
     // per-launch CUDA-event records (spring_set_profiling)
     struct ProfRec {
@@ -296,7 +297,11 @@ int run_v3_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol&
 int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, double* d_w);
 // k_v3s.cu: specialised V3 for two-atom cells; *handled is false when the cell does not fit it
 int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
-               const Pol* pol, double* lw, double* p3, double* w, bool* handled);
+               const Pol* pol, double* lw, double* p3, double* w, bool* handled, const int* plist = nullptr,
+               int nlist = 0);
+// k_v3tc.cu: the pairs of a q0 block with a mode triple inside the Gaussian's exp(-40) window (the
+// tensor-core path's pre-screen), as a device list of pair indices and its length
+int run_v3_prescreen(spring_ctx* c, int q0_first, int n_q0, double sigma, const int** d_list, int* n);
 // k_v3tc.cu: tensor-core V3 + Gaussian sum (BF16 / BF16x3) for two-atom cells; *handled false otherwise
 int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
                    bool* handled);

@@ -15,6 +15,7 @@ constexpr double EXP_UNDERFLOW = 745.2;
 
 struct S3Args {
     int nq, nT, nq0, q0_first, pair_first, pair_end, ngroups;
+    const int* plist;  // null: pairs pair_first .. pair_end - 1; else the pairs plist[pair_first .. pair_end - 1]
     double mfac, onebysigma, onebysigma2;
     int pol_lo[3], pol_hi[3];
 };
@@ -100,10 +101,11 @@ __device__ __forceinline__ void v3s_group(Smem& S, const S3Args& a, const S3Ptrs
     __syncthreads();  // previous group done with every buffer; constants staged
     // --- 0: pair descriptors
     if (tid < PP) {
-        const int pr = a.pair_first + grp * PP + tid;
-        const int v = pr < a.pair_end;
+        const int idx = a.pair_first + grp * PP + tid;
+        const int v = idx < a.pair_end;
         S.valid[tid] = v;
         if (v) {
+            const int pr = a.plist ? a.plist[idx] : idx;
             const int2 g = pairs[pr];
             const int q = pair_q0[pr];
             S.g1[tid] = g.x;

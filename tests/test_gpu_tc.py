@@ -172,3 +172,20 @@ def test_tc_wait_timeout_returns_status_and_context_recovers(runs):
     lw, _ = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
     ctx.set_precision("fp64")
     np.testing.assert_allclose(lw, out["bf16x3"][0], rtol=1e-12, atol=0.0)
+
+
+def test_fp64_prescreen_matches_full_fp64(runs):
+    """SPRING_OPT_FP64_PRESCREEN: the FP64 kernel on the pre-screened pairs only gives the FP64
+    linewidths and phase space of every pair (the dropped pairs' weights are below exp(-40))."""
+    from spring_b200 import _lib as L
+    N, ctx, info, out, _ = runs
+    ctx.set_precision("fp64")
+    ctx.set_option(L.SPRING_OPT_FP64_PRESCREEN, 1)
+    try:
+        ctx.reset_linewidths()
+        lw, p3 = ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA)
+    finally:
+        ctx.set_option(L.SPRING_OPT_FP64_PRESCREEN, 0)
+    lw64, p364, _ = out["fp64"]
+    np.testing.assert_allclose(lw, lw64, rtol=1e-12, atol=1e-13 * np.abs(lw64).max())
+    np.testing.assert_allclose(p3, p364, rtol=1e-10, atol=1e-12 * np.abs(p364).max())
