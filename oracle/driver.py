@@ -79,6 +79,10 @@ def lib():
                                    f64p, f64p, i32p, ct.c_double, ct.c_double, ct.c_double, ct.c_int, f64p, f64p,
                                    f64p, f64p]
         L.orc_bte_iter.restype = ct.c_int
+        L.orc_bte_iter_gauss.argtypes = [ct.c_int, ct.c_int, ct.c_double, ct.c_int, i32p, i32p, i32p, i32p, i32p,
+                                         f64p, f64p, f64p, f64p, i32p, ct.c_double, ct.c_double, ct.c_double,
+                                         ct.c_int, f64p, f64p, f64p, f64p]
+        L.orc_bte_iter_gauss.restype = ct.c_int
         L.orc_num_threads.restype = ct.c_int
         _LIB = L
     return _LIB
@@ -380,6 +384,29 @@ def bte_iter(st: Setup, it=0, eps_k=1e-6, max_iter=1000):
     iters = lib().orc_bte_iter(nd, st.nq, _i(st.tetra), nirr, irr_grid, pos, sgn, neg, part, _f(sctr),
                                _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _f(st.ph["grp_vel"]), deg,
                                float(st.temps[it]), st.cr.vol, eps_k, max_iter, inv_tau, F, krta, kap)
+    return dict(kappa=kap, kappa_rta=krta, inv_tau=inv_tau, F=F, iters=iters, irr_grid=irr_grid, deg=deg)
+
+
+def bte_iter_gauss(st: Setup, sigma, it=0, eps_k=1e-6, max_iter=1000):
+    """The iterative BTE with Gaussian delta weights (build-side form) on the grid phonons of ``st``."""
+    irr_grid, pos, sgn, neg, deg = time_reversal_set(st.mesh, st.q_pnt_int)
+    nirr = len(irr_grid)
+    nd = st.cr.ndof
+    sctr = np.zeros((nirr, st.nq, nd, nd, nd))
+    part = np.zeros((nirr, st.nq), np.int32)
+    for i, g0 in enumerate(irr_grid):
+        q0 = st.q_pnt_int[g0]
+        A, perm, _ = momentum3(st.mesh, st.q_pnt_int, q0)
+        sctr[i] = scatter_w3(st.cr, st.q_pnt, st.q_pnt_int, q0, st.ph["evec"][g0], st.ph["onebyomega"][g0],
+                             st.ph["evec"], st.ph["onebyomega"], perm)
+        part[i] = partner_map(st.mesh, st.q_pnt_int, q0)
+    inv_tau = np.zeros((nirr, nd))
+    F = np.zeros((nirr, nd, 3))
+    krta = np.zeros(9)
+    kap = np.zeros(9)
+    iters = lib().orc_bte_iter_gauss(nd, st.nq, float(sigma), nirr, irr_grid, pos, sgn, neg, part, _f(sctr),
+                                     _f(st.ph["omega"]), _f(st.ph["nbe"][it]), _f(st.ph["grp_vel"]), deg,
+                                     float(st.temps[it]), st.cr.vol, eps_k, max_iter, inv_tau, F, krta, kap)
     return dict(kappa=kap, kappa_rta=krta, inv_tau=inv_tau, F=F, iters=iters, irr_grid=irr_grid, deg=deg)
 
 

@@ -1181,6 +1181,124 @@ int orc_bte_iter(int ndof, int nq, const int* tetra, int n_irr, const int* irr_g
     return iter;
 }
 
+// Iterative BTE with Gaussian delta weights (build-side form of kappa_iter.x; the reference's
+// iterative solver integrates with tetrahedra only).  The same two channels and vertex structure as
+// orc_bte_iter above, each grid point x taken once with the weight d(w0 - M) of a Gaussian of width
+// sigma instead of the tetrahedron weights (the Gaussian form of kappa.x's linewidth, ThirdOrder_m.f90
+// :521-533, applied to TetrahedronWplus/Wminus and TetrahedronIterPlus/Minus):
+//   plus  at x:  M = w(-p(x),s2) - w(x,s1), W+ = 4 W3(q0; x s1; p(x) s2)(n(x,s1) - n(p(x),s2)),
+//                1/tau += W+ d,   dF += W+ d (F(-p(x),s2) - F(x,s1));
+//   minus at x:  u = -p(-x), M = w(x,s1) + w(u,s2), W- = 4 W3(q0; -x s1; p(-x) s2)(1 + n(-x,s1) + n(p(-x),s2)),
+//                1/tau += 0.5 W- d, dF += 0.5 W- d (F(u,s2) + F(x,s1)).
+// Arguments as orc_bte_iter, with sigma (rad/ps) in place of the tetrahedra.
+int orc_bte_iter_gauss(int ndof, int nq, double sigma, int n_irr, const int* irr_grid, const int* pos_tr,
+                       const int* sgn_tr, const int* neg, const int* partner, const double* sctr, const double* omega,
+                       const double* nbe, const double* vel, const int* deg, double T, double vol, double eps_k,
+                       int max_iter, double* inv_tau, double* F, double* kappa_rta, double* kappa) {
+    const int n = ndof;
+    const size_t n3 = (size_t)n * n * n;
+    const double FunitE = 1.054571817 / 1.380649;
+    const double kW_mK = 1.054571817 * 0.001;
+    const double mfac_k = 1.0 / (double(nq) * vol);
+    const double os = 1.0 / sigma, os2 = os * os;
+    std::vector<double> F0((size_t)n_irr * n * 3, 0.0), dF((size_t)n_irr * n * 3, 0.0);
+    auto Fat = [&](const double* Fv, int q, int s, int k) { return sgn_tr[q] * Fv[((size_t)pos_tr[q] * n + s) * 3 + k]; };
+    auto delta = [&](double d) { return os * Onebysqrt2PI * std::exp(-0.5 * os2 * (d * d)); };
+    auto pass = [&](int mode, const double* Fv) {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            const int* p = partner + (size_t)i * nq;
+            const double* W3 = sctr + (size_t)i * nq * n3;
+            for (int s = 0; s < n; ++s) {
+                const double w0 = omega[(size_t)g0 * n + s];
+                double tv = 0.0, tf[3] = {0.0, 0.0, 0.0};
+                for (int x = 0; x < nq; ++x)
+                    for (int s1 = 0; s1 < n; ++s1)
+                        for (int s2 = 0; s2 < n; ++s2) {
+                            {  // plus
+                                const int q2 = neg[p[x]];
+                                const double M = omega[(size_t)q2 * n + s2] - omega[(size_t)x * n + s1];
+                                const double w3 = 4.0 * W3[(size_t)x * n3 + ((size_t)s * n + s1) * n + s2];
+                                const double Wv = w3 * (nbe[(size_t)x * n + s1] - nbe[(size_t)p[x] * n + s2]) * delta(w0 - M);
+                                if (mode == 0) tv += Wv;
+                                else
+                                    for (int k = 0; k < 3; ++k) tf[k] += Wv * (Fat(Fv, q2, s2, k) - Fat(Fv, x, s1, k));
+                            }
+                            {  // minus
+                                const int y = neg[x];
+                                const int u = neg[p[y]];
+                                const double M = omega[(size_t)x * n + s1] + omega[(size_t)u * n + s2];
+                                const double w3 = 4.0 * W3[(size_t)y * n3 + ((size_t)s * n + s1) * n + s2];
+                                const double Wv = 0.5 * w3 * (1.0 + nbe[(size_t)y * n + s1] + nbe[(size_t)p[y] * n + s2]) *
+                                                  delta(w0 - M);
+                                if (mode == 0) tv += Wv;
+                                else
+                                    for (int k = 0; k < 3; ++k) tf[k] += Wv * (Fat(Fv, u, s2, k) + Fat(Fv, x, s1, k));
+                            }
+                        }
+                if (mode == 0) inv_tau[(size_t)i * n + s] = tv;
+                else
+                    for (int k = 0; k < 3; ++k) dF[((size_t)i * n + s) * 3 + k] = tf[k];
+            }
+        }
+    };
+    auto kappa_of = [&](const double* Fv, double* out) {
+        for (int k = 0; k < 9; ++k) out[k] = 0.0;
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            for (int s = (g0 == 0 ? 3 : 0); s < n; ++s) {
+                const double w = omega[(size_t)g0 * n + s], nq_ = nbe[(size_t)g0 * n + s];
+                const double* v = vel + ((size_t)g0 * n + s) * 3;
+                const double* f = Fv + ((size_t)i * n + s) * 3;
+                const double pre = double(deg[i]) * w * nq_ * (nq_ + 1.0);
+                for (int a = 0; a < 3; ++a)
+                    for (int b = 0; b < 3; ++b) out[3 * a + b] += pre * (v[a] * f[b]);
+            }
+        }
+        for (int k = 0; k < 9; ++k) out[k] = kW_mK * mfac_k * out[k];
+    };
+    pass(0, nullptr);
+    for (int i = 0; i < n_irr; ++i) {
+        const int g0 = irr_grid[i];
+        for (int s = (g0 == 0 ? 3 : 0); s < n; ++s) {
+            const double it = inv_tau[(size_t)i * n + s];
+            if (std::fabs(it) > zero_prec)
+                for (int k = 0; k < 3; ++k)
+                    F0[((size_t)i * n + s) * 3 + k] =
+                        FunitE * omega[(size_t)g0 * n + s] * vel[((size_t)g0 * n + s) * 3 + k] / (it * (T * T));
+        }
+    }
+    std::vector<double> Fc(F0);
+    kappa_of(Fc.data(), kappa_rta);
+    double kold[9];
+    for (int k = 0; k < 9; ++k) kold[k] = kappa_rta[k];
+    int iter = 0;
+    for (;;) {
+        ++iter;
+        pass(1, Fc.data());
+        for (int i = 0; i < n_irr; ++i) {
+            const int g0 = irr_grid[i];
+            for (int s = 0; s < n; ++s) {
+                const double it = inv_tau[(size_t)i * n + s];
+                const bool on = !(g0 == 0 && s < 3) && std::fabs(it) > zero_prec;
+                for (int k = 0; k < 3; ++k) {
+                    double& d = dF[((size_t)i * n + s) * 3 + k];
+                    d = on ? d / it : d;
+                }
+            }
+        }
+        for (size_t k = 0; k < Fc.size(); ++k) Fc[k] = F0[k] + dF[k];
+        kappa_of(Fc.data(), kappa);
+        double acc = 0.0;
+        for (int k = 0; k < 9; ++k) acc = std::max(acc, std::fabs(kappa[k] - kold[k]));
+        if (acc < eps_k || iter > max_iter) break;
+        for (int k = 0; k < 9; ++k) kold[k] = kappa[k];
+    }
+    std::memcpy(F, Fc.data(), sizeof(double) * Fc.size());
+    return iter;
+}
+
 int orc_num_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();
