@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-fp64-4ph", action="store_true", help="skip the FP64 run of the four-phonon leg")
     ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-screened leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-workload leg")
+    ap.add_argument("--no-bte", action="store_true", help="skip the iterative-kappa leg")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
                     help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
     return ap.parse_args()
@@ -444,6 +445,40 @@ def surrogate_c5_leg(torch, train_mesh=12, mesh=20, frac=0.25, members=3):
     return out
 
 
+def bte_c2_leg(torch, ctx, mesh):
+    """Iterative (non-RTA) kappa of the benchmark context (mesh^3, T = 100/300/700 K) to the
+    tolerance 1e-6, in the Gaussian operator form (delta weights of width SIGMA, FP64 throughout).
+    First call: time-reversal pairs, operator build (FP64 V3 of every pair, the entries inside the
+    delta window, row sort) and the iterations; then the iterations alone on the kept operator,
+    and the operator pass's achieved HBM bandwidth."""
+    r1, first_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
+    r2, iter_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
+    ctx.set_profiling(True)
+    ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6)
+    rows_ms, rows_n = ctx.kernel_time("k_bteg_rows<dF>")
+    ctx.set_profiling(False)
+    E = r2["entries"]
+    n_iter = int(r2["iters"].sum())
+    # per operator pass: (k1, k2) and the coefficient of every entry, the row offsets, dF out
+    ntr_rows = (mesh ** 3 // 2 + 8) * 6
+    bytes_pass = E * (8 + 8) + ntr_rows * (4 + 24)
+    per_ms = rows_ms / rows_n if rows_n else None
+    peaks = measured_peaks()
+    return {"mesh": [mesh] * 3, "temperatures": TEMPS, "sigma_rad_ps": SIGMA, "eps_k": 1e-6,
+            "operator_entries": E, "pairs": r2["pairs"], "iterations": r2["iters"].tolist(),
+            "converged": bool((r2["iters"] <= 1000).all()),
+            "first_call_ms": first_ms, "iterations_only_ms": iter_ms,
+            "ms_per_iteration": iter_ms / max(n_iter, 1),
+            "operator_pass_ms": per_ms,
+            "operator_pass_gbs": bytes_pass / (per_ms * 1e-3) / 1e9 if per_ms else None,
+            "operator_pass_frac_hbm": (bytes_pass / (per_ms * 1e-3) / 1e9) / peaks["hbm_gbs"] if per_ms else None,
+            "kappa_diag": [_kdiag(k).tolist() for k in r2["kappa"]],
+            "kappa_rta_diag": [_kdiag(k).tolist() for k in r2["kappa_rta"]],
+            "same_as_first_call": bool(np.array_equal(r1["kappa"], r2["kappa"])),
+            "what": "spring_kappa_iter_gauss: F <- F0 + tau sum over both channels until max|dkappa| < 1e-6; "
+                    "operator = one entry per pair and mode triple inside the exp(-40) window, kept in HBM"}
+
+
 BATCH_CELLS = (("rocksalt2", 12), ("rocksalt2", 16), ("rocksalt2", 20), ("rocksalt8", 8), ("rocksalt8", 10))
 # Gamma-X-W-K-Gamma-L in the fractional reciprocal basis, 200 points
 PATH_NODES = np.array([[0.0, 0.0, 0.0, 0], [0.0, 0.5, 0.5, 50], [0.25, 0.625, 0.625, 25], [0.375, 0.75, 0.375, 18],
@@ -676,6 +711,7 @@ def run_ours(args):
     four = fourph_c3_leg(torch, args.mesh4, fp64=not args.no_fp64_4ph) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
     sur = surrogate_c5_leg(torch) if (rank == 0 and world == 1 and not args.no_surrogate) else None
     batched = batched_leg(torch) if (rank == 0 and world == 1 and not args.no_batch) else None
+    bte = bte_c2_leg(torch, ctx, mesh[0]) if (rank == 0 and world == 1 and not args.no_bte) else None
     cpu = None
     oracle_check = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -758,6 +794,7 @@ def run_ours(args):
                 "fourph_c3": four,
                 "surrogate_c5": sur,
                 "batched": batched,
+                "bte_c2": bte,
                 "roofline": roof,
                 "cpu_baseline": cpu,
                 "oracle_check_24": oracle_check,

@@ -279,6 +279,17 @@ int spring_kappa_rta(spring_ctx* ctx, int symm, int nsym, const double* Rxyz, co
  * 0) and iters(n_temps) are outputs (NULL allowed). */
 int spring_kappa_iter(spring_ctx* ctx, double eps_k, int max_iter, double* kappa, double* kappa_rta, int* iters);
 
+/* The same iteration with Gaussian delta weights of width sigma (THz) in place of the
+ * tetrahedra: both channels of TetrahedronIterPlus / TetrahedronIterMinus
+ * (src/Kappa/Src_iterative/Quasi_momentum_consrv.f90:701-1208) with d(w0 - M) a
+ * Gaussian, as kappa.x's Gaussian linewidths are to its tetrahedron ones.  The scattering
+ * operator (one entry per pair and mode triple inside the exp(-40) window) is built once
+ * on the device, sorted by row and kept until sigma, FC3 or the phonons change; every
+ * iteration is then one pass over it.  Two-atom cells with 7-atom FC3 clusters.
+ * stats(2) optional: number of operator entries, number of enumerated pairs. */
+int spring_kappa_iter_gauss(spring_ctx* ctx, double sigma, double eps_k, int max_iter, double* kappa,
+                            double* kappa_rta, int* iters, double* stats);
+
 /* ---- batched linewidths (several workloads, one persistent launch) ------ */
 /* A batch holds Gaussian three-phonon linewidth requests on several contexts
  * (different cells, meshes and temperature sets, on one device) and runs them

@@ -68,6 +68,7 @@ SIGNATURES = {
     "spring_mlp_train": [P, I, P, P, I, I, ct.c_float, ct.c_ulonglong, P],
     "spring_mlp_predict": [P, I, P, P, I],
     "spring_kappa_iter": [P, D, I, P, P, P],
+    "spring_kappa_iter_gauss": [P, D, D, I, P, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_tc_stats": [P, P, P],
     "spring_binary_version": [I, P],

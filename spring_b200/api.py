@@ -359,6 +359,17 @@ class Context:
         self._call("spring_kappa_iter", float(eps_k), int(max_iter), _ptr(kap), _ptr(k0), _ptr(it))
         return dict(kappa=kap, kappa_rta=k0, iters=it)
 
+    def kappa_iter_gauss(self, sigma: float, eps_k: float = 1e-6, max_iter: int = 1000):
+        """Iterative kappa with Gaussian delta weights of width sigma (THz): dict(kappa (nT,9),
+        kappa_rta (nT,9), iters (nT,), entries, pairs)."""
+        kap = np.zeros((self.n_temps, 9))
+        k0 = np.zeros((self.n_temps, 9))
+        it = np.zeros(self.n_temps, np.int32)
+        st = np.zeros(2)
+        self._call("spring_kappa_iter_gauss", float(sigma), float(eps_k), int(max_iter), _ptr(kap), _ptr(k0),
+                   _ptr(it), _ptr(st))
+        return dict(kappa=kap, kappa_rta=k0, iters=it, entries=int(st[0]), pairs=int(st[1]))
+
 
 def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True, with_fc4=False):
     """A ready context for a :class:`spring_b200.synthetic.Crystal`.

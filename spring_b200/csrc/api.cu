@@ -326,6 +326,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         free_pairs(c->ps_irr); free_pairs(c->ps_tr);
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
+        dfree(c->d_bteg_row); dfree(c->d_bteg_kk); dfree(c->d_bteg_pq);
         dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
@@ -401,6 +402,17 @@ int spring_kappa_iter(spring_ctx* c, double eps_k, int max_iter, double* kappa, 
     SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
     if (!(eps_k > 0.0) || max_iter < 0) return fail(c, SPRING_ERR_ARG, "eps_k must be > 0 and max_iter >= 0");
     return run_bte(c, eps_k, max_iter, kappa, kappa_rta, iters);
+}
+
+int spring_kappa_iter_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, double* kappa, double* kappa_rta,
+                            int* iters, double* stats) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->fc3_set, "FC3"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    SPRING_CHECK(need(c, c->ph_grid.set, "grid phonons"));
+    if (!(eps_k > 0.0) || max_iter < 0) return fail(c, SPRING_ERR_ARG, "eps_k must be > 0 and max_iter >= 0");
+    if (!(sigma > 0.0)) return fail(c, SPRING_ERR_ARG, "sigma must be > 0");
+    return run_bte_gauss(c, sigma, eps_k, max_iter, kappa, kappa_rta, iters, stats);
 }
 
 int spring_set_option(spring_ctx* c, int option, int value) {
@@ -565,6 +577,7 @@ int spring_set_fc3(spring_ctx* c, int na3, const int* num, const int* idx, const
     // no stream wait: h2d staged every byte in the context's pinned ring before queuing its copy
     c->fc3_set = true;
     dfree(c->d_wtr);  // cached W grids depend on FC3
+    c->bteg_n = 0;    // and so does the Gaussian BTE operator
     return SPRING_OK;
 }
 

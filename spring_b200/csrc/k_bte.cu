@@ -25,9 +25,11 @@
 // Roofline: FP64 ALU (divisions of the tetrahedron weights), like k_tetra3.
 #include <algorithm>
 #include <cmath>
+#include <cub/cub.cuh>
 
 #include "spring_internal.cuh"
 #include "tetra.cuh"
+#include "v3sitem.cuh"
 
 namespace spring {
 namespace {
@@ -273,7 +275,239 @@ int build_tr_set(spring_ctx* c) {
     return SPRING_OK;
 }
 
+// ---------------------------------------------------------------- Gaussian operator
+// The iterative BTE with Gaussian delta weights in place of the tetrahedra (build-side form): per
+// enumerated pair (q0 of the time-reversal set, q1, q2 = p(q1)) and mode triple with a weight above
+// the exp(-40) cut, one operator entry (r0, k1, k2, P, Q); with c = (n1 - n2) P + (1 + n1 + n2) Q,
+//   1/tau(r0) = sum c,   dF(r0) = -sum c (F(k1) + F(k2)),
+// which is the reference's two channels (TetrahedronWplus / Wminus and TetrahedronIterPlus / Minus,
+// Quasi_momentum_consrv.f90:701-1208, TetrahedronDeltaSum.f90:22-607) summed over every grid q1 with
+// d(w0 - M): the plus channel at q1 and at q2 gives (n1 - n2) d(w0 + w1 - w2) + (n2 - n1) d(w0 + w2 - w1)
+// and the minus channel at -q1 and -q2 gives (1 + n1 + n2) d(w0 - w1 - w2), each times 4 W3 and -(F1 + F2)
+// because F(-q) = -F(q).  The entries are sorted by row once and kept in HBM (CSR); an iteration is one
+// pass over them.
+__global__ void k_bteg_keys(long long n, const s3::BteEntry* __restrict__ e, int* __restrict__ key,
+                            int* __restrict__ idx, int* __restrict__ rowcnt) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        key[i] = e[i].r0;
+        idx[i] = (int)i;
+        atomicAdd(&rowcnt[e[i].r0], 1);
+    }
+}
+__global__ void k_bteg_gather(long long n, const s3::BteEntry* __restrict__ e, const int* __restrict__ idx,
+                              int2* __restrict__ kk, double2* __restrict__ pq) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const s3::BteEntry x = e[idx[i]];
+        kk[i] = make_int2(x.k1, x.k2);
+        pq[i] = make_double2(x.P, x.Q);
+    }
+}
+// c = (n1 - n2) P + (1 + n1 + n2) Q at one temperature
+__global__ void k_bteg_coef(long long n, const int2* __restrict__ kk, const double2* __restrict__ pq,
+                            const double* __restrict__ nbe, double* __restrict__ cf) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int2 k = kk[i];
+        const double2 v = pq[i];
+        const double n1 = nbe[k.x], n2 = nbe[k.y];
+        cf[i] = (n1 - n2) * v.x + (1.0 + n1 + n2) * v.y;
+    }
+}
+// F at every grid mode from the time-reversal slots: Fg[g][s] = sgn(g) F[pos(g)][s]
+__global__ void k_bteg_expand(int nq, int n, const int* __restrict__ pos, const int* __restrict__ sgn,
+                              const double* __restrict__ F, double* __restrict__ Fg) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq * n; i += gridDim.x * blockDim.x) {
+        const int g = i / n, sx = i % n;
+        const double sg = sgn[g];
+        const double* f = F + ((size_t)pos[g] * n + sx) * 3;
+        Fg[3 * (size_t)i] = sg * f[0];
+        Fg[3 * (size_t)i + 1] = sg * f[1];
+        Fg[3 * (size_t)i + 2] = sg * f[2];
+    }
+}
+// One warp per row: MODE 0 inv_tau[r] = sum c; MODE 1 dF[r] = -sum c (Fg[k1] + Fg[k2]).
+template <int MODE>
+__global__ void __launch_bounds__(256) k_bteg_rows(int rows, const int* __restrict__ rowoff, const int2* __restrict__ kk,
+                                                  const double* __restrict__ cf, const double* __restrict__ Fg,
+                                                  double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        for (int i = rowoff[r] + lane; i < rowoff[r + 1]; i += 32) {
+            const double c = cf[i];
+            if (MODE == 0) {
+                a0 += c;
+            } else {
+                const int2 k = kk[i];
+                const double* f1 = Fg + 3 * (size_t)k.x;
+                const double* f2 = Fg + 3 * (size_t)k.y;
+                a0 -= c * (f1[0] + f2[0]);
+                a1 -= c * (f1[1] + f2[1]);
+                a2 -= c * (f1[2] + f2[2]);
+            }
+        }
+        a0 = tet::warp_sum(a0);
+        if (MODE == 1) {
+            a1 = tet::warp_sum(a1);
+            a2 = tet::warp_sum(a2);
+        }
+        if (lane == 0) {
+            if (MODE == 0) {
+                out[r] = a0;
+            } else {
+                out[3 * (size_t)r] = a0;
+                out[3 * (size_t)r + 1] = a1;
+                out[3 * (size_t)r + 2] = a2;
+            }
+        }
+    }
+}
+
 }  // namespace
+
+int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta,
+                  int* h_iters, double* h_stats) {
+    if (c->nb != 2 || c->na3 != 7) return fail(c, SPRING_ERR_UNSUPPORTED, "Gaussian iterative kappa: two-atom cells with 7-atom FC3 clusters");
+    if (c->ntr == 0) SPRING_CHECK(build_tr_set(c));
+    if (!c->ps_tr.done) SPRING_CHECK(run_enumerate3(c, c->ps_tr));
+    SPRING_CHECK(pairoff_host(c, c->ps_tr));
+    const int n = c->ndof, ntr = c->ntr, nq = c->nq, rows = ntr * n;
+    const Q0View view{c->d_tr_int.p, c->d_tr_grid.p, c->ph_grid.evec.p, c->ph_grid.omega.p, c->ph_grid.oneby.p};
+    const long long npairs = c->ps_tr.h_pairoff[ntr];
+    const int threads = 256;
+    auto blocks_for = [&](long long m) { return (int)std::max<long long>(1, std::min<long long>((m + threads - 1) / threads, 148LL * 16)); };
+    // ---- the operator: entries, sorted by row (kept until sigma, the phonons or the pairs change)
+    if (!(c->bteg_sigma == sigma && c->bteg_gen == c->ph_gen && c->bteg_pairs == c->ps_tr.gen && c->bteg_n > 0)) {
+        c->bteg_n = 0;
+        DBuf<s3::BteEntry> ent;
+        DBuf<unsigned long long> ctr;
+        SPRING_CHECK(dalloc(c, ctr, 1, "operator count"));
+        long long cap = std::max<long long>(1 << 20, npairs * 216 / 40);  // the window passes ~1-2% of the triples
+        long long cnt = 0;
+        for (int attempt = 0; attempt < 2; ++attempt) {
+            int rc = dalloc(c, ent, (size_t)cap, "BTE operator entries");
+            if (rc == SPRING_OK) rc = zero(c, ctr.p, sizeof(unsigned long long), "operator count");
+            bool handled = false;
+            if (rc == SPRING_OK) rc = launch_v3s_bte(c, c->ps_tr, view, 0, ntr, sigma, ent.p, ctr.p, cap, &handled);
+            unsigned long long h = 0;
+            if (rc == SPRING_OK) rc = d2h(c, &h, ctr.p, sizeof h, "operator count");
+            if (rc != SPRING_OK) { dfree(ent); dfree(ctr); return rc; }
+            cnt = (long long)h;
+            if (cnt <= cap) break;
+            dfree(ent);
+            cap = cnt + cnt / 16 + 1024;
+        }
+        dfree(ctr);
+        if (cnt > cap) { dfree(ent); return fail(c, SPRING_ERR_CUDA, "BTE operator: entry count changed between runs"); }
+        if (cnt > 0x7fffffffLL) { dfree(ent); return fail(c, SPRING_ERR_UNSUPPORTED, "BTE operator above 2^31 entries"); }
+        DBuf<int> key, keys, idx, idxs, cntr;
+        int rc = dalloc(c, key, std::max<long long>(cnt, 1), "operator keys");
+        if (rc == SPRING_OK) rc = dalloc(c, keys, std::max<long long>(cnt, 1), "operator keys");
+        if (rc == SPRING_OK) rc = dalloc(c, idx, std::max<long long>(cnt, 1), "operator keys");
+        if (rc == SPRING_OK) rc = dalloc(c, idxs, std::max<long long>(cnt, 1), "operator keys");
+        if (rc == SPRING_OK) rc = dalloc(c, cntr, rows + 1, "operator rows");
+        if (rc == SPRING_OK) rc = dalloc(c, c->d_bteg_row, rows + 1, "operator rows");
+        if (rc == SPRING_OK) rc = zero(c, cntr.p, sizeof(int) * (rows + 1), "operator rows");
+        if (rc == SPRING_OK && cnt > 0) {
+            k_bteg_keys<<<blocks_for(cnt), threads, 0, c->stream>>>(cnt, ent.p, key.p, idx.p, cntr.p);
+            rc = launch_check(c, "k_bteg_keys");
+        }
+        if (rc == SPRING_OK) rc = run_exclusive_scan(c, cntr.p, c->d_bteg_row.p, rows + 1);
+        if (rc == SPRING_OK && cnt > 0) {
+            int bits = 1;
+            while ((1 << bits) <= rows) ++bits;
+            size_t tb = 0;
+            cub::DeviceRadixSort::SortPairs(nullptr, tb, key.p, keys.p, idx.p, idxs.p, (int)cnt, 0, bits, c->stream);
+            DBuf<uint8_t> tmp;
+            rc = dalloc(c, tmp, std::max<size_t>(tb, 1), "operator sort");
+            if (rc == SPRING_OK) {
+                const cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp.p, tb, key.p, keys.p, idx.p, idxs.p, (int)cnt,
+                                                                      0, bits, c->stream);
+                c->launches += 1;
+                if (e != cudaSuccess) rc = cuda_fail(c, e, "operator sort");
+            }
+            if (rc == SPRING_OK) rc = dalloc(c, c->d_bteg_kk, cnt, "BTE operator");
+            if (rc == SPRING_OK) rc = dalloc(c, c->d_bteg_pq, cnt, "BTE operator");
+            if (rc == SPRING_OK) {
+                k_bteg_gather<<<blocks_for(cnt), threads, 0, c->stream>>>(cnt, ent.p, idxs.p, c->d_bteg_kk.p, c->d_bteg_pq.p);
+                rc = launch_check(c, "k_bteg_gather");
+            }
+            cudaStreamSynchronize(c->stream);
+            dfree(tmp);
+        }
+        cudaStreamSynchronize(c->stream);
+        dfree(ent); dfree(key); dfree(keys); dfree(idx); dfree(idxs); dfree(cntr);
+        if (rc != SPRING_OK) return rc;
+        c->bteg_n = cnt;
+        c->bteg_sigma = sigma;
+        c->bteg_gen = c->ph_gen;
+        c->bteg_pairs = c->ps_tr.gen;
+    }
+    const long long cnt = c->bteg_n;
+    if (h_stats) {
+        h_stats[0] = (double)cnt;
+        h_stats[1] = (double)npairs;
+    }
+    // ---- iterations per temperature
+    DBuf<double> inv_tau, F0, F, dF, kap, cf, Fg;
+    int rc = dalloc(c, inv_tau, (size_t)rows, "1/tau");
+    if (rc == SPRING_OK) rc = dalloc(c, F0, (size_t)rows * 3, "F0");
+    if (rc == SPRING_OK) rc = dalloc(c, F, (size_t)rows * 3, "F");
+    if (rc == SPRING_OK) rc = dalloc(c, dF, (size_t)rows * 3, "dF");
+    if (rc == SPRING_OK) rc = dalloc(c, kap, 9, "kappa");
+    if (rc == SPRING_OK) rc = dalloc(c, cf, std::max<long long>(cnt, 1), "operator coefficients");
+    if (rc == SPRING_OK) rc = dalloc(c, Fg, (size_t)nq * n * 3, "F on the grid");
+    const int rblocks = std::max(1, std::min((rows + 7) / 8, 148 * 16));
+    const int eblocks = std::max(1, std::min((rows + threads - 1) / threads, 148 * 8));
+    auto kappa_of = [&](int T, const double* Fv, double* out9) -> int {
+        k_bte_kappa<<<1, 256, 0, c->stream>>>(ntr, n, nq, c->vol, c->d_tr_grid.p, c->d_tr_deg.p, c->ph_grid.omega.p,
+                                              c->ph_grid.nbe.p + (size_t)T * nq * n, c->ph_grid.vel.p, Fv, kap.p);
+        SPRING_CHECK(launch_check(c, "k_bte_kappa"));
+        return d2h(c, out9, kap.p, sizeof(double) * 9, "kappa");
+    };
+    for (int T = 0; rc == SPRING_OK && T < c->nT; ++T) {
+        const double* nbeT = c->ph_grid.nbe.p + (size_t)T * nq * n;
+        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
+        if (cnt > 0) {
+            k_bteg_coef<<<blocks_for(cnt), threads, 0, c->stream>>>(cnt, c->d_bteg_kk.p, c->d_bteg_pq.p, nbeT, cf.p);
+            if ((rc = launch_check(c, "k_bteg_coef")) != SPRING_OK) break;
+        }
+        k_bteg_rows<0><<<rblocks, 256, 0, c->stream>>>(rows, c->d_bteg_row.p, c->d_bteg_kk.p, cf.p, nullptr, inv_tau.p);
+        if ((rc = launch_check(c, "k_bteg_rows<tau>")) != SPRING_OK) break;
+        k_bte_f0<<<eblocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, c->ph_grid.omega.p, c->ph_grid.vel.p,
+                                                    inv_tau.p, c->temps[T], F0.p);
+        if ((rc = launch_check(c, "k_bte_f0")) != SPRING_OK) break;
+        if (cudaMemcpyAsync(F.p, F0.p, sizeof(double) * rows * 3, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
+            rc = fail(c, SPRING_ERR_CUDA, "F copy");
+            break;
+        }
+        double k0[9], kold[9], knew[9];
+        if ((rc = kappa_of(T, F.p, k0)) != SPRING_OK) break;
+        std::copy(k0, k0 + 9, kold);
+        std::copy(k0, k0 + 9, knew);
+        int iter = 0;
+        for (;;) {
+            ++iter;
+            k_bteg_expand<<<blocks_for((long long)nq * n), threads, 0, c->stream>>>(nq, n, c->d_tr_pos.p, c->d_tr_sgn.p,
+                                                                                     F.p, Fg.p);
+            if ((rc = launch_check(c, "k_bteg_expand")) != SPRING_OK) break;
+            k_bteg_rows<1><<<rblocks, 256, 0, c->stream>>>(rows, c->d_bteg_row.p, c->d_bteg_kk.p, cf.p, Fg.p, dF.p);
+            if ((rc = launch_check(c, "k_bteg_rows<dF>")) != SPRING_OK) break;
+            k_bte_update<<<eblocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, inv_tau.p, F0.p, dF.p, F.p);
+            if ((rc = launch_check(c, "k_bte_update")) != SPRING_OK) break;
+            if ((rc = kappa_of(T, F.p, knew)) != SPRING_OK) break;
+            double d = 0.0;
+            for (int k = 0; k < 9; ++k) d = std::max(d, std::fabs(knew[k] - kold[k]));
+            if (d < eps_k || iter > max_iter) break;
+            std::copy(knew, knew + 9, kold);
+        }
+        if (rc != SPRING_OK) break;
+        if (h_kappa) std::copy(knew, knew + 9, h_kappa + 9 * T);
+        if (h_kappa_rta) std::copy(k0, k0 + 9, h_kappa_rta + 9 * T);
+        if (h_iters) h_iters[T] = iter;
+    }
+    dfree(inv_tau); dfree(F0); dfree(F); dfree(dF); dfree(kap); dfree(cf); dfree(Fg);
+    return rc;
+}
 
 int run_bte(spring_ctx* c, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta, int* h_iters) {
     if (c->ntr == 0) SPRING_CHECK(build_tr_set(c));

@@ -95,4 +95,42 @@ int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, 
     return launch_check(c, epi == 0 ? "k_v3s<gauss>" : "k_v3s<wgrid>");
 }
 
+// Entries of the Gaussian BTE operator (EPI 2) of pair set ps, q0 block [q0_first, +n_q0): every
+// mode triple with a delta weight above the exp(-40) cut is appended to `items` (capacity cap) at
+// *ctr (zeroed by the caller); *ctr ends as the number of entries, those past cap not written.
+int launch_v3s_bte(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, double sigma,
+                   void* items, unsigned long long* ctr, long long cap, bool* handled) {
+    *handled = false;
+    if (c->nb != NB || c->na3 != NA) return SPRING_OK;
+    *handled = true;
+    S3Args a{};
+    a.nq = c->nq;
+    a.nT = c->nT;
+    a.nq0 = ps.n0;
+    a.q0_first = q0_first;
+    a.plist = nullptr;
+    SPRING_CHECK(pairoff_host(c, ps));
+    a.pair_first = ps.h_pairoff[q0_first];
+    a.pair_end = ps.h_pairoff[q0_first + n_q0];
+    a.ngroups = (a.pair_end - a.pair_first + PP - 1) / PP;
+    a.mfac = host_constants().Sctr3THz2 / double(c->nq);
+    a.onebysigma = 1.0 / sigma;
+    a.onebysigma2 = a.onebysigma * a.onebysigma;
+    if (a.ngroups == 0) return SPRING_OK;
+    const size_t smem = sizeof(Smem);
+    cudaFuncSetAttribute(k_v3s<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int dev_sms = 148;
+    cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
+    const int grid = std::min(a.ngroups, dev_sms * 2);
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3: injected launch failure");
+    S3Ptrs P{ps.pairs.p, ps.pair_q0.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_fc3_off.p,
+             c->d_mass_rs.p, c->d_qpnt.p, v.q0_int, v.q0_grid, v.evec, v.omega, v.oneby, c->ph_grid.evec.p,
+             c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, nullptr, nullptr, nullptr};
+    P.out_items = items;
+    P.item_ctr = ctr;
+    P.item_cap = cap;
+    k_v3s<2><<<grid, THREADS, smem, c->stream>>>(a, P, nullptr, n_q0, ps.cap);
+    return launch_check(c, "k_v3s<bte>");
+}
+
 }  // namespace spring

@@ -182,6 +182,13 @@ struct spring_ctx {
     spring::DBuf<int> d_tr_deg;    // [ntr]
     spring::DBuf<int> d_neg;       // [q] grid index of -q
     spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
+    // sorted Gaussian BTE operator (k_bte.cu run_bte_gauss): rows, (k1, k2), (P, Q)
+    spring::DBuf<int> d_bteg_row;
+    spring::DBuf<int2> d_bteg_kk;
+    spring::DBuf<double2> d_bteg_pq;
+    long long bteg_n = 0;
+    double bteg_sigma = 0.0;
+    int bteg_gen = -1, bteg_pairs = -1;
 
     // four-phonon quartet lists (k_4ph.cu, opaque) and the tensor-core V4 buffers (k_v4tc.cu)
     void* e4 = nullptr;
@@ -299,6 +306,11 @@ int run_v3_wgrid(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first
 int launch_v3s(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, int epi, double sigma,
                const Pol* pol, double* lw, double* p3, double* w, bool* handled, const int* plist = nullptr,
                int nlist = 0);
+int launch_v3s_bte(spring_ctx* c, const PairSet& ps, const Q0View& v, int q0_first, int n_q0, double sigma,
+                   void* items, unsigned long long* ctr, long long cap, bool* handled);
+// k_bteg.cu: iterative kappa with Gaussian deltas (the operator stored sparse in HBM)
+int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, double* h_kappa, double* h_kappa_rta,
+                  int* h_iters, double* h_stats);
 // k_v3tc.cu: the pairs of a q0 block with a mode triple inside the Gaussian's exp(-40) window (the
 // tensor-core path's pre-screen), as a device list of pair indices and its length
 int run_v3_prescreen(spring_ctx* c, int q0_first, int n_q0, double sigma, const int** d_list, int* n);

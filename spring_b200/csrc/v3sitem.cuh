@@ -64,7 +64,23 @@ struct S3Ptrs {
     double* out_lw;
     double* out_p3;
     double* out_w;
+    // EPI 2 (the Gaussian BTE operator): entries appended at *item_ctr (those past item_cap are
+    // counted, not written)
+    void* out_items;
+    unsigned long long* item_ctr;
+    long long item_cap;
 };
+
+// One entry of the Gaussian BTE scattering operator (EPI 2): row r0 = q0 slot * 6 + s0, grid modes
+// k1 = g1 * 6 + s1 and k2 = g2 * 6 + s2 of an enumerated pair, and the temperature-free parts of
+// its coefficient c = (n1 - n2) P + (1 + n1 + n2) Q: P = 4 W (d(w0 + w1 - w2) - d(w0 + w2 - w1)),
+// Q = 4 W d(w0 - w1 - w2) (halved, and the second delta of P absent, when q1 = q2).
+struct BteEntry {
+    int r0, k1, k2, pad;
+    double P, Q;
+};
+static_assert(sizeof(BteEntry) == 32, "BTE entry");
+constexpr double EXP_CUT_BTE = 40.0;  // exp(-40) = 4e-18 of a delta's peak: terms below are dropped
 
 // Stage the cell's constants (FC3, neighbour positions and basis, masses, slot groups).
 __device__ __forceinline__ void v3s_stage(Smem& S, const S3Ptrs& P) {
@@ -223,6 +239,9 @@ __device__ __forceinline__ void v3s_group(Smem& S, const S3Args& a, const S3Ptrs
         for (int s = 0; s < N; ++s) cfma(phi[s], e, S.A[p][(k * 6 + lo) * RS + s]);
     }
     // --- 7: W and epilogue
+    double bP[N], bQ[N];  // EPI 2: this thread's operator entries (s2)
+#pragma unroll
+    for (int s2 = 0; s2 < N; ++s2) bP[s2] = bQ[s2] = 0.0;
     if (S.valid[p]) {
         const int g1 = S.g1[p], g2 = S.g2[p], q0 = S.q0[p], p0 = S.p0[p];
         const int s0 = hi, s1 = lo;
@@ -236,7 +255,26 @@ __device__ __forceinline__ void v3s_group(Smem& S, const S3Args& a, const S3Ptrs
             const double abs2 = phi[s2].x * phi[s2].x + phi[s2].y * phi[s2].y;
             W[s2] = zero ? 0.0 : abs2 * (o01 * obg[(size_t)g2 * N + s2]) * a.mfac;
         }
-        if (EPI == 1) {
+        if (EPI == 2) {
+            // entries of the Gaussian BTE operator (appended below, outside this branch)
+            const double w0 = om0[(size_t)p0 * N + s0];
+            const double w1 = omg[(size_t)g1 * N + s1];
+            const double pre = a.onebysigma * ONEBYSQRT2PI;
+            const bool self = g1 == g2;
+#pragma unroll
+            for (int s2 = 0; s2 < N; ++s2) {
+                if (W[s2] == 0.0) continue;
+                const double w2 = omg[(size_t)g2 * N + s2];
+                const double da = w0 + w1 - w2, db = w0 + w2 - w1, dm = w0 - w1 - w2;
+                const double xa = 0.5 * a.onebysigma2 * (da * da), xb = 0.5 * a.onebysigma2 * (db * db),
+                             xm = 0.5 * a.onebysigma2 * (dm * dm);
+                const double ea = xa < EXP_CUT_BTE ? pre * exp(-xa) : 0.0;
+                const double eb = (!self && xb < EXP_CUT_BTE) ? pre * exp(-xb) : 0.0;
+                const double em = xm < EXP_CUT_BTE ? pre * exp(-xm) : 0.0;
+                bP[s2] = 4.0 * W[s2] * (ea - eb);
+                bQ[s2] = 4.0 * W[s2] * (self ? 0.5 : 1.0) * em;
+            }
+        } else if (EPI == 1) {
             const int slot = q0 - a.q0_first;
             double* w1 = out_w + ((size_t)slot * a.nq + g1) * 216 + (s0 * N + s1) * N;
 #pragma unroll
@@ -283,6 +321,47 @@ __device__ __forceinline__ void v3s_group(Smem& S, const S3Args& a, const S3Ptrs
                     }
                     atomicAdd(&S.lw[p][MAXT][s0], esum);
                 }
+            }
+        }
+    }
+    if (EPI == 2) {
+        // append this thread's nonzero entries: one atomic per warp for the warp's block
+        const bool on = S.valid[p] != 0;
+        int cnt = 0;
+        if (on)
+#pragma unroll
+            for (int s2 = 0; s2 < N; ++s2) cnt += (bP[s2] != 0.0 || bQ[s2] != 0.0) ? 1 : 0;
+        const int lane = tid & 31;
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        unsigned long long base = 0;
+        if (lane == 31 && total > 0) base = atomicAdd(P.item_ctr, (unsigned long long)total);
+        base = __shfl_sync(0xffffffffu, base, 31);
+        if (cnt > 0) {
+            unsigned long long pos = base + (unsigned long long)(incl - cnt);
+            const int g1 = S.g1[p], g2 = S.g2[p];
+            const int r0 = (S.q0[p] - a.q0_first) * N + hi;  // row: q0 slot of this launch, s0
+            BteEntry* out = static_cast<BteEntry*>(P.out_items);
+#pragma unroll
+            for (int s2 = 0; s2 < N; ++s2) {
+                const double bp = bP[s2], bq = bQ[s2];
+                if (bp == 0.0 && bq == 0.0) continue;
+                if ((long long)pos < P.item_cap) {
+                    BteEntry e;
+                    e.r0 = r0;
+                    e.k1 = g1 * N + lo;
+                    e.k2 = g2 * N + s2;
+                    e.pad = 0;
+                    e.P = bp;
+                    e.Q = bq;
+                    out[pos] = e;
+                }
+                ++pos;
             }
         }
     }

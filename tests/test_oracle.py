@@ -217,6 +217,17 @@ def test_bte_iteration0_is_full_grid_rta(cr):
     assert r["iters"] > 1 and r["kappa"][0] > r["kappa_rta"][0]
 
 
+def test_bte_gauss_iteration0_is_gaussian_linewidth(cr):
+    """The Gaussian operator's 1/tau is twice kappa.x's Gaussian linewidth per mode (full grid), and
+    the iteration converges above the RTA start."""
+    N, sigma = 4, 1.5
+    st = D.Setup(cr, (N, N, N), [300.0], W=np.eye(3, dtype=np.int32)[None], Rxyz=np.eye(3)[None])
+    r = D.bte_iter_gauss(st, sigma)
+    lw = D.linewidth3_all(st, "gauss", sigma=sigma)
+    np.testing.assert_allclose(r["inv_tau"], 2.0 * lw[0][r["irr_grid"]], rtol=1e-10, atol=1e-16)
+    assert 1 < r["iters"] < 1000 and r["kappa"][0] > r["kappa_rta"][0]
+
+
 def test_constants():
     assert abs(C.wTHz - 98.22693) < 1e-4
     assert abs(0.3767 - 2 * 2 * np.pi * 2.99792458e-2) < 2e-4   # 2 cm^-1 in rad/ps
