@@ -73,6 +73,19 @@ int spring_kernel_launches(const spring_ctx* ctx, long long* count);
  * volume and the reciprocal vectors G like the reference. */
 int spring_set_crystal(spring_ctx* ctx, const double* latvec, const double* mass);
 
+/* Dipole-dipole (Ewald) term of D(q) for polar crystals (LongEw = &FCInfo Force_dd):
+ * EwaldParam%set_EwaldParam (src/Kappa/Src/EwaldParam.f90) with &AtmInfo atm_pos(3,Nb),
+ * dielec(3,3), BornZ(3,3,Nb), &CrystalInfo Sup_Cell(3) and &EwaldInfo decide_EwParam, prec_Ew,
+ * Lmb, Gmesh(3), Rmesh(3) (Gmesh and Lmb are used only when decide_ew_param = 0; sup_cell NULL
+ * = 5 5 5).  The phonons computed afterwards add DynMatgv_Ew (DynaMat_mod.f90:285-380), and
+ * DynMat_NA with finite-difference velocities at q = 0 (get_phonon, :548-590).  dielec = NULL
+ * switches the term off.  Needs spring_set_crystal; at most 8 basis atoms. */
+int spring_set_dipole(spring_ctx* ctx, const double* atm_pos, const double* dielec, const double* born_z,
+                      int decide_ew_param, double prec_ew, double lmb, const int* gmesh, const int* rmesh,
+                      const int* sup_cell);
+/* The parameters in use: on (0/1), Lmb, Gmesh(3), number of R and G points (NULL allowed). */
+int spring_get_dipole(spring_ctx* ctx, int* on, double* lmb, int* gmesh, int* n_r, int* n_g);
+
 /* FC2type%set_FC2, src/Kappa/Src/FC2_mod.f90:46-65:
  * atm_num(Nb), atm_indx(4,na2,Nb) = (cell R1,R2,R3, basis index), fc2(1,3,3,na2,Nb). */
 int spring_set_fc2(spring_ctx* ctx, int na2, const int* atm_num, const int* atm_indx, const double* fc2);

@@ -44,6 +44,15 @@ int spring_h5_read_restart(const char* path, int ndof, int nq0, int* progress, d
  * up to 8); the data go to out when out != NULL and cap (elements) is large enough. */
 int spring_h5_read_f64(const char* path, const char* name, int* rank, long long* fdims, double* out, long long cap);
 
+/* The host part of the dipole-dipole term (the same code the device library runs in
+ * spring_set_dipole): Lmb and Gmesh (DecideEwaldParameters when decide != 0), counts = (number of R
+ * points, number of G points), cc(2, 9 Nb^2) = -CombineZStar(CConst) - CSumq0 on the diagonal
+ * blocks (complex, C(beta, alpha, nu, mu) order), hz(9 Nb^2, NR) the Born-charge-folded real-space
+ * terms.  Any output may be NULL.  Arguments as spring_set_dipole plus latvec(3,3). */
+int spring_ewald_setup(const double* latvec, int nb, const double* atm_pos, const double* dielec, const double* born_z,
+                       int decide, double prec_ew, double lmb, const int* gmesh, const int* rmesh, const int* sup_cell,
+                       double* lmb_out, int* gmesh_out, int* counts, double* cc_out, double* hz_out, long long hz_cap);
+
 #ifdef __cplusplus
 }
 #endif

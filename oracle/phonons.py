@@ -5,8 +5,8 @@ with ``DynMatgv_SR`` (``DynaMat_mod.f90:98-190``) and ``SolveEigen``
 (``src/Kappa/Src/lapack_gfort.f90:212-265``).  ``numpy.linalg.eigh`` with
 ``UPLO='U'`` calls LAPACK ``zheevd('V','U')`` exactly as the reference does,
 so eigenvalue order and eigenvector gauge follow the same library routine.
-Only the short-range dynamical matrix is restated (``LongEw = .false.``;
-the Ewald/non-analytic term is outside the hot path).
+With ``ewald`` (an :class:`oracle.ewald.Ewald`) the ``LongEw`` branch adds the
+dipole-dipole matrix and its q-derivative (``DynaMat_mod.f90:548-590``).
 
 Only ``tests/``, ``bench.py``'s CPU-baseline leg and ``__graft_entry__.smoke``
 may import this module; the product never does.
@@ -38,7 +38,7 @@ def dynmat(latvec, mass, atm_num, atm_indx, fc2, q):
     return D, dD
 
 
-def get_phonon(latvec, mass, atm_num, atm_indx, fc2, qpoints, temps):
+def get_phonon(latvec, mass, atm_num, atm_indx, fc2, qpoints, temps, ewald=None, gamma_dir=None):
     """Per q: omega (rad/ps), 1/(omega wTHz), nBE per T, group velocity, eigenvectors.
 
     ``qpoints`` is (Nq, 3) Cartesian.  Returns a dict of arrays in
@@ -59,6 +59,10 @@ def get_phonon(latvec, mass, atm_num, atm_indx, fc2, qpoints, temps):
     for i in range(nq):
         q = qpoints[i]
         D, dD = dynmat(latvec, mass, atm_num, atm_indx, fc2, q)
+        if ewald is not None:
+            De, dDe = ewald.term(qpoints, i, mass, gamma_dir)
+            D = D + De
+            dD = dD + dDe
         w, v = np.linalg.eigh(D, UPLO="U")
         neg = (np.abs(w) > C.EPS) & (w < 0.0)
         W = np.sqrt(np.abs(w))

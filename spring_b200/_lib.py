@@ -69,6 +69,8 @@ SIGNATURES = {
     "spring_mlp_predict": [P, I, P, P, I],
     "spring_kappa_iter": [P, D, I, P, P, P],
     "spring_kappa_iter_gauss": [P, D, D, I, P, P, P, P],
+    "spring_set_dipole": [P, P, P, P, I, D, D, P, P, P],
+    "spring_get_dipole": [P, P, P, P, P, P],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_tc_stats": [P, P, P],
     "spring_binary_version": [I, P],

@@ -162,6 +162,26 @@ class Context:
         lat = _c(np.asarray(latvec).T, np.float64)  # Fortran latvec(3,3): columns are vectors
         self._call("spring_set_crystal", _ptr(lat), _ptr(_c(mass, np.float64)))
 
+    def set_dipole(self, basis_frac, eps, zstar, rmesh, decide=True, prec_ew=1e-6, lmb=0.8, gmesh=None,
+                   sup_cell=(5, 5, 5)):
+        """The dipole-dipole term (Force_dd): ``basis_frac`` (Nb, 3) fractional positions, ``eps`` the
+        3x3 dielectric tensor with ``eps[i, j]`` = dielec(i, j), ``zstar`` (Nb, 3, 3) with
+        ``zstar[mu][i, j]`` = BornZ(i, j, mu).  ``eps=None`` switches it off.  Set before the phonons
+        are computed.  Returns (Lmb, Gmesh, number of R points, number of G points)."""
+        if eps is None:
+            self._call("spring_set_dipole", None, None, None, 0, 0.0, 0.0, None, None, None)
+            return None
+        bf = _c(basis_frac, np.float64)
+        ep = _c(np.asarray(eps, np.float64).T, np.float64)               # Fortran order of dielec(3,3)
+        zs = _c(np.asarray(zstar, np.float64).transpose(0, 2, 1), np.float64)  # BornZ(3,3,Nb)
+        gm = _c(gmesh if gmesh is not None else (1, 1, 1), np.int32)
+        self._call("spring_set_dipole", _ptr(bf), _ptr(ep), _ptr(zs), int(bool(decide)), float(prec_ew),
+                   float(lmb), _ptr(gm), _ptr(_c(rmesh, np.int32)), _ptr(_c(sup_cell, np.int32)))
+        on, lm, nr, ng = ct.c_int(), ct.c_double(), ct.c_int(), ct.c_int()
+        g = np.zeros(3, np.int32)
+        self._call("spring_get_dipole", ct.byref(on), ct.byref(lm), _ptr(g), ct.byref(nr), ct.byref(ng))
+        return float(lm.value), tuple(int(x) for x in g), int(nr.value), int(ng.value)
+
     def set_fc2(self, atm_num, atm_indx, fc2):
         na = int(np.asarray(atm_indx).shape[1])
         self._call("spring_set_fc2", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),
@@ -371,11 +391,14 @@ class Context:
         return dict(kappa=kap, kappa_rta=k0, iters=it, entries=int(st[0]), pairs=int(st[1]))
 
 
-def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True, with_fc4=False):
+def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=True, with_fc4=False,
+                 dipole=None):
     """A ready context for a :class:`spring_b200.synthetic.Crystal`.
 
     ``phonons="device"`` computes them with the device eigensolver; a dict
-    ``{"grid": ph, "irr": ph}`` loads host-computed ones instead.
+    ``{"grid": ph, "irr": ph}`` loads host-computed ones instead.  ``dipole``: keyword
+    arguments of :meth:`Context.set_dipole` (rmesh, decide, prec_ew, ...) to add the
+    dipole-dipole term with the crystal's Born charges and dielectric tensor.
     Returns ``(ctx, info)`` where ``info`` holds the mesh and irreducible set.
     """
     from . import synthetic as S
@@ -387,6 +410,7 @@ def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=
         ctx.set_fc3(cr.fc3_atm_num, cr.fc3_atm_indx, cr.fc3)
     if with_fc4:
         ctx.set_fc4(cr.fc4_atm_num, cr.fc4_atm_indx, cr.fc4)
+    ew = ctx.set_dipole(cr.basis_frac, cr.eps, cr.zstar, **dipole) if dipole is not None else None
     qi, qf, tet = ctx.make_mesh()
     if W is None:
         W, Rxyz = S.point_group(cr)
@@ -396,7 +420,7 @@ def from_crystal(cr, mesh, temps, phonons="device", W=None, Rxyz=None, with_fc3=
         ctx.set_phonons(1, temps, phonons["irr"])
     else:
         ctx.compute_phonons(temps)
-    info = dict(q_pnt_int=qi, q_pnt=qf, tetra=tet, W=W, Rxyz=Rxyz, temps=temps, **irr)
+    info = dict(q_pnt_int=qi, q_pnt=qf, tetra=tet, W=W, Rxyz=Rxyz, temps=temps, ewald=ew, **irr)
     return ctx, info
 
 

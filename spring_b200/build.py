@@ -32,7 +32,8 @@ def nvcc() -> str:
 
 
 def _deps() -> list[str]:
-    return glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(INCLUDE, "*.h")) +
+            glob.glob(os.path.join(os.path.dirname(CSRC), "host", "*.hpp")))
 
 
 def _stale(obj: str, src: str) -> bool:

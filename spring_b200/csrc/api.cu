@@ -327,6 +327,8 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_tr_int); dfree(c->d_tr_grid); dfree(c->d_tr_pos); dfree(c->d_tr_sgn); dfree(c->d_tr_deg);
         dfree(c->d_neg); dfree(c->d_wtr);
         dfree(c->d_bteg_row); dfree(c->d_bteg_kk); dfree(c->d_bteg_pq);
+        dfree(c->ew.g); dfree(c->ew.r); dfree(c->ew.hz); dfree(c->ew.tau); dfree(c->ew.z); dfree(c->ew.cc);
+        dfree(c->ew.dd);
         dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
@@ -500,6 +502,25 @@ int spring_set_crystal(spring_ctx* c, const double* latvec, const double* mass) 
     SPRING_CHECK(dalloc(c, c->d_mass_rs, c->nb, "masses"));
     SPRING_CHECK(h2d(c, c->d_mass_rs.p, rs.data(), sizeof(double) * c->nb, "masses"));
     c->crystal_set = true;
+    return SPRING_OK;
+}
+
+int spring_set_dipole(spring_ctx* c, const double* atm_pos, const double* dielec, const double* born_z,
+                      int decide_ew_param, double prec_ew, double lmb, const int* gmesh, const int* rmesh,
+                      const int* sup_cell) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->crystal_set, "crystal"));
+    return set_dipole(c, atm_pos, dielec, born_z, decide_ew_param, prec_ew, lmb, gmesh, rmesh, sup_cell);
+}
+
+int spring_get_dipole(spring_ctx* c, int* on, double* lmb, int* gmesh, int* n_r, int* n_g) {
+    CTX_ENTER(c);
+    if (on) *on = c->ew.on ? 1 : 0;
+    if (lmb) *lmb = c->ew.lmb;
+    if (gmesh)
+        for (int k = 0; k < 3; ++k) gmesh[k] = c->ew.gmesh[k];
+    if (n_r) *n_r = c->ew.nr;
+    if (n_g) *n_g = c->ew.ng;
     return SPRING_OK;
 }
 

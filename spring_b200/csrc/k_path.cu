@@ -467,7 +467,7 @@ int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int
         if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
         k_path_q2<<<blocks, threads, 0, c->stream>>>(qa, ns, q0v.p, zc.p, c->d_qpnt.p, q1v.p, q2v.p, ex.p);
         if ((rc = launch_check(c, "k_path_q2")) != SPRING_OK) break;
-        if ((rc = run_phonons(c, ph2, q2v.p, (int)rows)) != SPRING_OK) break;
+        if ((rc = run_phonons(c, ph2, q2v.p, (int)rows, 1)) != SPRING_OK) break;  // single points (get_phonon_singleq)
         if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
         k_path_clear_missing<<<blocks, threads, 0, c->stream>>>(rows, n, c->nT, ex.p, ph2.omega.p, ph2.nbe.p);
         if ((rc = launch_check(c, "k_path_clear_missing")) != SPRING_OK) break;

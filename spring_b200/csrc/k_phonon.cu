@@ -28,6 +28,7 @@ struct PhArgs {
     double latvec[9];
     double wTHz, vg_ms, BEConv;
     int nT;
+    const double2* dd;  // dipole-dipole D and dD/dq per work item ([4][n][n]), or null
 };
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -106,6 +107,14 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, PhSet SA, const in
                 A[row * n + col] = cadd(A[row * n + col], t);
                 for (int k = 0; k < 3; ++k)  // (i R_k) * t
                     dD[(k * n + row) * n + col] = cadd(dD[(k * n + row) * n + col], make_double2(-t.y * R[k], t.x * R[k]));
+            }
+        }
+        __syncthreads();
+        if (a.dd) {  // + DynEw, dDynEw/dq (LongEw)
+            const double2* d = a.dd + (size_t)item * 4 * n * n;
+            for (int i = tid; i < 4 * n * n; i += nt) {
+                double2& t = i < n * n ? A[i] : dD[i - n * n];
+                t = cadd(t, d[i]);
             }
         }
         for (int i = tid; i < n; i += nt) V[i * n + i] = make_double2(1.0, 0.0);
@@ -344,6 +353,14 @@ __global__ void __launch_bounds__(32) k_phonons_n6(PhArgs a, PhSet SA, const int
                 }
             }
         __syncwarp();
+        if (act && a.dd) {  // + DynEw, dDynEw/dq (LongEw)
+            const double2* d = a.dd + (size_t)item * 4 * 36;
+            for (int w = gl; w < 4 * 36; w += L) {
+                double2& t = w < 36 ? S.A[w] : S.dD[w - 36];
+                t = cadd(t, d[w]);
+            }
+        }
+        __syncwarp();
 
         // --- cyclic complex Jacobi, one group per point
         bool gdone = !act;
@@ -523,6 +540,7 @@ PhArgs ph_args(spring_ctx* c) {
     a.vg_ms = k.vg_ms;
     a.BEConv = k.BEConv;
     a.nT = c->nT;
+    a.dd = nullptr;
     return a;
 }
 
@@ -532,8 +550,10 @@ size_t ph_smem(int n) {
            sizeof(int) * (2 * (m / 2) + n + (n & 1)) + sizeof(double) * n + 16;
 }
 
-int launch_phonons(spring_ctx* c, const PhSet& A, const int* list_a, int n_a, const PhSet& B, int n_b) {
-    const PhArgs a = ph_args(c);
+int launch_phonons(spring_ctx* c, const PhSet& A, const int* list_a, int n_a, const PhSet& B, int n_b,
+                   int gamma_mode = 0) {
+    PhArgs a = ph_args(c);
+    SPRING_CHECK(launch_ewald(c, A.qpts, A.nq, list_a, n_a, B.qpts, B.nq, n_b, gamma_mode, &a.dd));
     const int n = c->ndof;
     const size_t smem = ph_smem(n);
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_phonons, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -560,9 +580,9 @@ PhSet ph_set(Phonons& ph, const double* q, int nq) {
 
 }  // namespace
 
-int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq) {
+int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq, int gamma_mode) {
     const PhSet A = ph_set(ph, d_q, nq);
-    return launch_phonons(c, A, nullptr, nq, A, 0);
+    return launch_phonons(c, A, nullptr, nq, A, 0, gamma_mode);
 }
 
 // Grid and irreducible phonons in one launch; on a Gamma-centred mesh only one point of each
@@ -570,7 +590,8 @@ int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int nq) {
 int run_phonons_mesh(spring_ctx* c) {
     const int nq = c->nq;
     const PhSet G = ph_set(c->ph_grid, c->d_qpnt.p, nq), I = ph_set(c->ph_irr, c->d_irr_q.p, c->nq0);
-    const bool tr = c->mesh_shift[0] == 0 && c->mesh_shift[1] == 0 && c->mesh_shift[2] == 0;
+    const bool tr = c->mesh_shift[0] == 0 && c->mesh_shift[1] == 0 && c->mesh_shift[2] == 0 &&
+                    !(c->ew.on && c->ew.even);
     if (!tr) {
         SPRING_CHECK(launch_phonons(c, G, nullptr, nq, G, 0));
         return launch_phonons(c, I, nullptr, c->nq0, I, 0);

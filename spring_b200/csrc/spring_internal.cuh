@@ -77,6 +77,15 @@ struct Mlp {
     bool set = false;
 };
 
+// Dipole-dipole term (spring_set_dipole, k_ewald.cu): the q-independent tables on the device.
+struct EwaldDev {
+    bool on = false, even = false;  // even: a G or R mesh of even size (no time-reversal shortcut)
+    int ng = 0, nr = 0, gmesh[3] = {0, 0, 0}, rmesh[3] = {0, 0, 0};
+    double lmb = 0.0, vol = 0.0, eps[9] = {};
+    DBuf<double> g, r, hz, tau, z;
+    DBuf<double2> cc, dd;
+};
+
 }  // namespace spring
 
 struct spring_ctx {
@@ -182,6 +191,7 @@ struct spring_ctx {
     spring::DBuf<int> d_tr_deg;    // [ntr]
     spring::DBuf<int> d_neg;       // [q] grid index of -q
     spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
+    spring::EwaldDev ew;
     // sorted Gaussian BTE operator (k_bte.cu run_bte_gauss): rows, (k1, k2), (P, Q)
     spring::DBuf<int> d_bteg_row;
     spring::DBuf<int2> d_bteg_kk;
@@ -291,7 +301,13 @@ bool launch_injected(spring_ctx* c);
 int run_make_mesh(spring_ctx* c, const int shift[3], int zero_centered);
 int run_irr_map(spring_ctx* c, const int* d_rot, int nrot, int time_rev, int* d_map);
 // k_phonon.cu
-int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int n);
+// gamma_mode: how the dipole term picks the Gamma direction (0: the next point of the list, 1: a
+// fixed direction, for single points)
+int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int n, int gamma_mode = 0);
+int set_dipole(spring_ctx* c, const double* atm_pos, const double* eps, const double* zstar, int decide,
+               double prec_ew, double lmb, const int* gmesh, const int* rmesh, const int* sup_cell);
+int launch_ewald(spring_ctx* c, const double* qa, int nqa, const int* list_a, int n_a, const double* qb, int nqb,
+                 int n_b, int gamma_mode, const double2** dd_out);
 int run_phonons_mesh(spring_ctx* c);  // grid + irreducible points (time reversal on Gamma-centred meshes)
 // k_enum.cu
 int run_enumerate3(spring_ctx* c, PairSet& ps);

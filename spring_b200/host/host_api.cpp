@@ -4,6 +4,7 @@
 #include <vector>
 
 #include "../../include/spring_host.h"
+#include "ewald.hpp"
 #include "h5lite.hpp"
 
 namespace {
@@ -194,6 +195,29 @@ int spring_h5_read_f64(const char* path, const char* name, int* rank, long long*
     if (out) {
         if ((long long)d->count() > cap) return fail("output buffer too small");
         std::memcpy(out, d->data.data(), d->data.size());
+    }
+    return 0;
+}
+
+int spring_ewald_setup(const double* latvec, int nb, const double* atm_pos, const double* dielec, const double* born_z,
+                       int decide, double prec_ew, double lmb, const int* gmesh, const int* rmesh, const int* sup_cell,
+                       double* lmb_out, int* gmesh_out, int* counts, double* cc_out, double* hz_out, long long hz_cap) {
+    if (!latvec || !atm_pos || !dielec || !born_z || !rmesh || !sup_cell) return fail("spring_ewald_setup: bad arguments");
+    spring_ewald::Setup S;
+    std::string err;
+    if (spring_ewald::setup(latvec, nb, atm_pos, dielec, born_z, decide, prec_ew, lmb, gmesh, rmesh, sup_cell, S, err))
+        return fail(err);
+    if (lmb_out) *lmb_out = S.lmb;
+    if (gmesh_out)
+        for (int k = 0; k < 3; ++k) gmesh_out[k] = S.gmesh[k];
+    if (counts) {
+        counts[0] = S.nr();
+        counts[1] = S.ng();
+    }
+    if (cc_out) std::memcpy(cc_out, S.cc.data(), sizeof(double) * S.cc.size());
+    if (hz_out) {
+        if ((long long)S.hz.size() > hz_cap) return fail("spring_ewald_setup: hz buffer too small");
+        std::memcpy(hz_out, S.hz.data(), sizeof(double) * S.hz.size());
     }
     return 0;
 }

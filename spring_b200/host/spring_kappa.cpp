@@ -257,6 +257,31 @@ int main(int argc, char** argv) {
         return p;
     };
     const std::vector<int> pol3 = pol(sel3), pol4 = pol(sel4);
+    // Dipole-dipole term: &FCInfo Force_dd, &CrystalInfo Sup_Cell, &AtmInfo dielec / BornZ
+    // (unit_mod.f90:64-209; dielec defaults to 1.0 in every element) and &EwaldInfo
+    // (EwaldParam.f90: decide_EwParam = .true., prec_Ew = 1e-6, Lmb = 0.8, Gmesh, Rmesh)
+    bool force_dd = false, decide_ew = true;
+    std::vector<int> sup_cell{5, 5, 5}, gmesh{0, 0, 0}, rmesh{0, 0, 0};
+    std::vector<double> dielec(9, 1.0), born((size_t)9 * nb, 0.0);
+    double prec_ew = 1e-6, lmb = 0.8;
+    check(nml::get(fci, "Force_dd", force_dd));
+    check(nml::get(cri, "Sup_Cell", {3}, sup_cell));
+    check(nml::get(ati, "dielec", {3, 3}, dielec));
+    check(nml::get(ati, "BornZ", {3, 3, nb}, born));
+    double ew_lmb = 0.0;
+    int ew_g[3] = {0, 0, 0}, ew_cnt[2] = {0, 0};
+    if (force_dd) {
+        if (!groups.count("ewaldinfo")) die("Force_dd = .true. needs the &EwaldInfo namelist (Rmesh)");
+        const nml::Group& ewi = groups["ewaldinfo"];
+        check(nml::get(ewi, "decide_EwParam", decide_ew));
+        check(nml::get(ewi, "prec_Ew", prec_ew));
+        check(nml::get(ewi, "Lmb", lmb));
+        check(nml::get(ewi, "Gmesh", {3}, gmesh));
+        check(nml::get(ewi, "Rmesh", {3}, rmesh));
+        if (spring_ewald_setup(lat.data(), nb, pos.data(), dielec.data(), born.data(), decide_ew ? 1 : 0, prec_ew, lmb,
+                               gmesh.data(), rmesh.data(), sup_cell.data(), &ew_lmb, ew_g, ew_cnt, nullptr, nullptr, 0))
+            die(spring_host_last_error());
+    }
 
     // ---- force constants
     const std::string tc = temp_char(T);
@@ -287,8 +312,10 @@ int main(int argc, char** argv) {
         for (double v : f3.fc) s3 += v * v;
         for (double v : f4.fc) s4 += v * v;
         std::printf("], \"na2\": %d, \"na3\": %d, \"na4\": %d, \"fc2_sum\": %.15g, \"fc3_sumsq\": %.15g, "
-                    "\"fc4_sumsq\": %.15g, \"n_rotations\": %d}\n",
-                    f2.na, f3.na, four ? f4.na : 0, s2, s3, s4, nrot);
+                    "\"fc4_sumsq\": %.15g, \"n_rotations\": %d, \"force_dd\": %s, \"ewald_lmb\": %.15g, "
+                    "\"ewald_gmesh\": [%d, %d, %d], \"ewald_points\": [%d, %d]}\n",
+                    f2.na, f3.na, four ? f4.na : 0, s2, s3, s4, nrot, force_dd ? "true" : "false", ew_lmb, ew_g[0],
+                    ew_g[1], ew_g[2], ew_cnt[0], ew_cnt[1]);
         return 0;
     }
 
@@ -304,6 +331,9 @@ int main(int argc, char** argv) {
     gpu(c, spring_set_fc2(c, f2.na, f2.num.data(), f2.idx.data(), f2.fc.data()));
     gpu(c, spring_set_fc3(c, f3.na, f3.num.data(), f3.idx.data(), f3.fc.data()));
     if (four) gpu(c, spring_set_fc4(c, f4.na, f4.num.data(), f4.idx.data(), f4.fc.data()));
+    if (force_dd)
+        gpu(c, spring_set_dipole(c, pos.data(), dielec.data(), born.data(), decide_ew ? 1 : 0, prec_ew, lmb,
+                                 gmesh.data(), rmesh.data(), sup_cell.data()));
     gpu(c, spring_make_mesh(c, shift.data(), 1, nullptr, nullptr, nullptr));
     const int nq = qmesh[0] * qmesh[1] * qmesh[2];
     int nq0 = 0;

@@ -32,7 +32,9 @@ def load():
                "spring_h5_write_kappa": [ct.c_char_p, P, I, I, P, P, P],
                "spring_h5_read_f64": [ct.c_char_p, ct.c_char_p, P, P, P, ct.c_longlong],
                "spring_h5_write_restart": [ct.c_char_p, I, I, I, I, P],
-               "spring_h5_read_restart": [ct.c_char_p, I, I, P, P]}
+               "spring_h5_read_restart": [ct.c_char_p, I, I, P, P],
+               "spring_ewald_setup": [P, I, P, P, P, I, ct.c_double, ct.c_double, P, P, P, P, P, P, P, P,
+                                      ct.c_longlong]}
         for name, args in sig.items():
             getattr(lib, name).argtypes = args
             getattr(lib, name).restype = I
@@ -105,25 +107,46 @@ def read_restart(path, ndof, nq0):
 
 
 def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, four_phonon=False,
-                selection3=("D", "D", "D"), time_rev=0, write_restart=False, read_restart=False):
+                selection3=("D", "D", "D"), time_rev=0, write_restart=False, read_restart=False, dipole=None):
     """An input.nml with &FCInfo, &CrystalInfo, &AtmInfo (unit_mod.f90:64-209) and &AnhInfo
-    (Helper_m.f90:37-132) for a synthetic crystal: one species per distinct mass."""
+    (Helper_m.f90:37-132) for a synthetic crystal: one species per distinct mass.  ``dipole``
+    (dict: rmesh, and optionally decide, prec_ew, lmb, gmesh, sup_cell) adds Force_dd, the crystal's
+    dielec and BornZ, and &EwaldInfo (EwaldParam.f90)."""
     masses, typ = [], []
     for m in cr.mass:
         if float(m) not in masses:
             masses.append(float(m))
         typ.append(masses.index(float(m)) + 1)
     L = []
-    L.append("&FCInfo\n    prefix = '%s'\n    SecondFC = .true.\n    ThirdFC = .true.\n    FourthFC = %s\n/\n"
+    L.append("&FCInfo\n    prefix = '%s'\n    SecondFC = .true.\n    ThirdFC = .true.\n    FourthFC = %s\n"
              % (prefix, ".true." if four_phonon else ".false."))
-    L.append("&CrystalInfo\n    Nbasis = %d\n    Ntyp = %d\n" % (cr.nbasis, len(masses)))
+    if dipole is not None:
+        L.append("    Force_dd = .true.\n")
+    L.append("/\n&CrystalInfo\n    Nbasis = %d\n    Ntyp = %d\n" % (cr.nbasis, len(masses)))
+    if dipole is not None:
+        L.append("    Sup_Cell = %d %d %d\n" % tuple(dipole.get("sup_cell", (5, 5, 5))))
     for k in range(3):
         L.append("    Latvec(:, %d) = %s\n" % (k + 1, " ".join("%.16g" % v for v in cr.latvec[:, k])))
     L.append("/\n&AtmInfo\n")
     for i in range(cr.nbasis):
         L.append("    atm_pos(:, %d) = %s\n" % (i + 1, " ".join("%.16g" % v for v in cr.basis_frac[i])))
     L.append("    typ_indx = %s\n" % " ".join(str(t) for t in typ))
-    L.append("    mass = %s\n/\n" % " ".join("%.10g" % m for m in masses))
+    L.append("    mass = %s\n" % " ".join("%.10g" % m for m in masses))
+    if dipole is not None:
+        for j in range(3):
+            L.append("    dielec(:, %d) = %s\n" % (j + 1, " ".join("%.16g" % cr.eps[i, j] for i in range(3))))
+        for mu in range(cr.nbasis):
+            for j in range(3):
+                L.append("    BornZ(:, %d, %d) = %s\n" % (j + 1, mu + 1,
+                                                         " ".join("%.16g" % cr.zstar[mu][i, j] for i in range(3))))
+    L.append("/\n")
+    if dipole is not None:
+        L.append("&EwaldInfo\n    decide_EwParam = %s\n    prec_Ew = %.16g\n    Lmb = %.16g\n"
+                 % (".true." if dipole.get("decide", True) else ".false.", dipole.get("prec_ew", 1e-6),
+                    dipole.get("lmb", 0.8)))
+        if dipole.get("gmesh") is not None:
+            L.append("    Gmesh = %d %d %d\n" % tuple(dipole["gmesh"]))
+        L.append("    Rmesh = %d %d %d\n/\n" % tuple(dipole["rmesh"]))
     L.append("&AnhInfo\n    qmesh = %d %d %d\n    time_rev = %d\n" % (*qmesh, time_rev))
     L.append("    SelectionRule3 = %s\n" % " ".join("'%s'" % s for s in selection3))
     if sigma is not None:

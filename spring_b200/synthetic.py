@@ -65,6 +65,8 @@ class Crystal:
     fc4_atm_num: np.ndarray = None
     fc4_atm_indx: np.ndarray = None
     fc4: np.ndarray = None
+    zstar: np.ndarray = None    # (Nb, 3, 3) Born charges, zstar[mu][i, j] = Fortran BornZ(i, j, mu)
+    eps: np.ndarray = None      # (3, 3) high-frequency dielectric tensor, eps[i, j] = dielec(i, j)
 
     @property
     def nbasis(self) -> int:
@@ -237,6 +239,15 @@ def build(name: str = "rocksalt2", fc4: bool = False, seeds=(SEED_FC2, SEED_FC3,
     make_fc3(cr, seed=seeds[1])
     if fc4:
         make_fc4(cr, seed=seeds[2])
+    return cr
+
+
+def make_polar(cr: Crystal, z: float = 1.986, eps: float = 3.0) -> Crystal:
+    """Born charges +z (species 1) / -z (species 2) times the identity and an isotropic dielectric
+    tensor: the inputs of the dipole-dipole term (``&AtmInfo`` BornZ, dielec).  The default z is
+    MgO's."""
+    cr.zstar = np.array([(1.0 if t == 1 else -1.0) * z * np.eye(3) for t in cr.typ_indx])
+    cr.eps = eps * np.eye(3)
     return cr
 
 

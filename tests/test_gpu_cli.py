@@ -90,3 +90,23 @@ def test_cli_restart_skips_the_points_already_done():
         kap2, lwf2, _ = _run(cr, d, [], qmesh=(N, N, N), read_restart=True)
     np.testing.assert_allclose(lwf2, lwf1, rtol=1e-12, atol=0)
     np.testing.assert_allclose(kap2, kap1, rtol=1e-12, atol=1e-14 * np.abs(kap1).max())
+
+
+def test_cli_dipole_term_matches_api():
+    """Force_dd with &EwaldInfo through the driver: the same phonons, linewidths and kappa as the
+    API with spring_set_dipole."""
+    cr = S.make_polar(S.build("rocksalt2"))
+    N = 4
+    dip = dict(rmesh=(5, 5, 5), prec_ew=1e-8)
+    with tempfile.TemporaryDirectory() as d:
+        kap, lwf, _ = _run(cr, d, [], qmesh=(N, N, N), dipole=dip)
+    ctx, info = from_crystal(cr, (N, N, N), [300.0], dipole=dip)
+    ctx.reset_linewidths()
+    ctx.linewidth3(1, ctx.nq0, delta="tetra", want=False)
+    lw = ctx.get_linewidths()[0]
+    om = ctx.get_phonons(1)["omega"]
+    k_api = ctx.kappa_rta(info["Rxyz"])[0]
+    ctx.close()
+    np.testing.assert_allclose(lwf[:, :6], om, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(kap, k_api, rtol=1e-9, atol=1e-12 * np.abs(k_api).max())
