@@ -86,6 +86,22 @@ int spring_set_dipole(spring_ctx* ctx, const double* atm_pos, const double* diel
 /* The parameters in use: on (0/1), Lmb, Gmesh(3), number of R and G points (NULL allowed). */
 int spring_get_dipole(spring_ctx* ctx, int* on, double* lmb, int* gmesh, int* n_r, int* n_g);
 
+/* Point-defect scattering (&PointDefInfo, ReadPointDefVar src/Kappa/Src/Helper_m.f90:135-307):
+ * the perturbed FC2 of the defect cell (IFC2_file_pd: na2_pd, atm_num, atm_indx, fc2 in the
+ * spring_set_fc2 layout), Mass_def(Nb) per basis atom (the pristine mass where no defect sits),
+ * rho_def (defects per A^3), MatInvFull and OptcTherm (0/1), and qMesh_pd(3), the mesh of the
+ * Green's-function tetrahedron integration.  Builds PerturbationMatrix
+ * (point_defect_m.f90:40-108), the defect mesh (make_tetrahedron, zero-centred, the run's shift)
+ * and its phonons.  Call after spring_set_fc2 (and spring_set_dipole) and spring_make_mesh.
+ * qmesh_pd = NULL switches it off. */
+int spring_set_point_defect(spring_ctx* ctx, const int* qmesh_pd, int na2_pd, const int* num_pd, const int* idx_pd,
+                            const double* fc2_pd, const double* mass_def, double rho_def, int mat_inv_full,
+                            int optc_therm);
+/* ScatterRatePointDefect (point_defect_m.f90:139-376) for irreducible points i0_first ..
+ * i0_first + n_q0 - 1 (1-based): rate(Ndof, n_q0) = 1/tau (NULL allowed; the Scatter_pd dataset);
+ * add != 0 also adds 0.5 rate to the resident LW_Allq0 at every temperature (main.f90:685). */
+int spring_linewidth_pd(spring_ctx* ctx, int i0_first, int n_q0, double* rate, int add);
+
 /* FC2type%set_FC2, src/Kappa/Src/FC2_mod.f90:46-65:
  * atm_num(Nb), atm_indx(4,na2,Nb) = (cell R1,R2,R3, basis index), fc2(1,3,3,na2,Nb). */
 int spring_set_fc2(spring_ctx* ctx, int na2, const int* atm_num, const int* atm_indx, const double* fc2);

@@ -30,9 +30,10 @@ int spring_h5_read_fc(const char* path, int order, int nb, int na, int* atm_num,
 /* Write kappa_<prefix><T>K.h5 like kappa.x (main.f90:775-798, w1dh5_no_grp / w2dh5_no_grp_type2 /
  * w2dh5_no_grp, hdf5_wrap_mod.f90:650-766): ThermalConductivityTensor(9) = kappa, LineWidth and
  * PhaseSpace3rd (2 Ndof, nq0) = omega in rows 1..Ndof and the value in Ndof+1..2 Ndof, and
- * ModeResolvedKappa(9, Ndof) when mode_k is not NULL. */
+ * ModeResolvedKappa(9, Ndof) when mode_k is not NULL, Scatter_pd (2 Ndof, nq0) (the point-defect
+ * rates with omega alongside, main.f90:778) when scatter_pd is not NULL. */
 int spring_h5_write_kappa(const char* path, const double* kappa, int ndof, int nq0, const double* linewidth,
-                          const double* phase_space, const double* mode_k);
+                          const double* phase_space, const double* mode_k, const double* scatter_pd);
 
 /* The linewidth restart file of kappa.x (w_RestartLW / r_RestartLW, hdf5_wrap_mod.f90:340-401 and
  * :562-647; Restart_<prefix>/<prefix><T>K_LW_Restart.h5): progress(2) = (last irreducible point

@@ -410,6 +410,62 @@ def bte_iter_gauss(st: Setup, sigma, it=0, eps_k=1e-6, max_iter=1000):
     return dict(kappa=kap, kappa_rta=krta, inv_tau=inv_tau, F=F, iters=iters, irr_grid=irr_grid, deg=deg)
 
 
+# ----------------------------------------------------------------------------- point defect
+def _lpd():
+    L = lib()
+    if not hasattr(L, "_pd_set"):
+        L.orc_pd_coeff.argtypes = [ct.c_double, f64p, i32p, f64p, f64p]
+        L.orc_pd_coeff.restype = None
+        L.orc_pd_perturbation.argtypes = [ct.c_int, ct.c_int, i32p, i32p, f64p, ct.c_int, i32p, i32p, f64p, f64p, f64p,
+                                          f64p, f64p]
+        L.orc_pd_perturbation.restype = None
+        L.orc_pd_rate.argtypes = [ct.c_int, ct.c_int, i32p, f64p, c128p, f64p, c128p, ct.c_int, f64p, f64p,
+                                  ct.c_double, ct.c_double, ct.c_int, ct.c_int, f64p]
+        L.orc_pd_rate.restype = None
+        L._pd_set = True
+    return L
+
+
+def pd_coeff(E, W, v=(0, 1, 2, 3)):
+    """CoefAtVertOfTetrhd: (sorted W, vertex order, Coeff = d - i pi c) for one tetrahedron."""
+    W = _f(W).copy()
+    v = _i(v).copy()
+    re = np.zeros(4)
+    im = np.zeros(4)
+    _lpd().orc_pd_coeff(float(E), W, v, re, im)
+    return W, v, re + 1j * im
+
+
+def pd_perturbation(cr, num_p, idx_p, fc_p, mass_def):
+    """PerturbationMatrix: (V_FC, V_M) as Fortran-order (Ndof, Ndof) arrays, [col][row] in memory."""
+    n = cr.ndof
+    vfc = np.zeros(n * n)
+    vm = np.zeros(n * n)
+    _lpd().orc_pd_perturbation(cr.nbasis, cr.fc2_atm_indx.shape[1], _i(cr.fc2_atm_num), _i(cr.fc2_atm_indx),
+                               _f(cr.fc2), idx_p.shape[1], _i(num_p), _i(idx_p), _f(fc_p), _f(cr.mass), _f(mass_def),
+                               vfc, vm)
+    return vfc, vm
+
+
+def pd_rates(st: Setup, qmesh_pd, num_p, idx_p, fc_p, mass_def, rho, mat_inv_full=True, optc_therm=True, ewald=None):
+    """ScatterRatePointDefect for every irreducible q0 of ``st``: (Nq0, Ndof) rates."""
+    from . import phonons as Ph
+    cr = st.cr
+    qi, qf, tet = make_tetrahedron(qmesh_pd, cr.G, zero_centered=True)
+    ph = Ph.get_phonon(cr.latvec, cr.mass, cr.fc2_atm_num, cr.fc2_atm_indx, cr.fc2, qf, [300.0], ewald=ewald)
+    w2 = _f(ph["omega"] ** 2)
+    vfc, vm = pd_perturbation(cr, num_p, idx_p, fc_p, mass_def)
+    n = cr.ndof
+    out = np.zeros((st.nq0, n))
+    for i in range(st.nq0):
+        g0 = int(np.all(st.irr_int[i] == 0))
+        r = np.zeros(n)
+        _lpd().orc_pd_rate(n, qi.shape[0], _i(tet), w2, _c(ph["evec"]), _f(st.ph0["omega"][i]), _c(st.ph0["evec"][i]),
+                           g0, vfc, vm, float(rho), cr.vol, int(mat_inv_full), int(optc_therm), r)
+        out[i] = r
+    return out
+
+
 # ----------------------------------------------------------------------------- four-phonon
 def _l4():
     L = lib()

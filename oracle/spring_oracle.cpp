@@ -1299,6 +1299,332 @@ int orc_bte_iter_gauss(int ndof, int nq, double sigma, int n_irr, const int* irr
     return iter;
 }
 
+// ---------------------------------------------------------------------------
+// Point-defect scattering: T-matrix with the tetrahedron Green's function
+// (src/Kappa/Src/point_defect_m.f90:40-376, GreensFunc_m.f90:35-587).
+// Energies are omega^2 in (rad/ps)^2 throughout, as ph_pd%omega and Wq0s02.
+
+// my_sort_GF (GreensFunc_m.f90:80-150): ascending sort, vertex ids (and F) follow; equal values
+// keep their original order (the first uncovered occurrence, as my_sort's cyclic search)
+static void sort_gf(double* W, int* v, double* F) {
+    double Wc[4], Fc[4] = {0, 0, 0, 0};
+    int vc[4];
+    for (int i = 0; i < 4; ++i) { Wc[i] = W[i]; vc[i] = v[i]; if (F) Fc[i] = F[i]; }
+    std::sort(W, W + 4);
+    bool covered[4] = {false, false, false, false};
+    for (int ii = 0; ii < 4; ++ii) {
+        int act = 0;
+        for (int k = 0; k < 4; ++k)
+            if (!covered[k] && Wc[k] == W[ii]) { act = k; break; }
+        covered[act] = true;
+        v[ii] = vc[act];
+        if (F) F[ii] = Fc[act];
+    }
+}
+
+static inline double sq(double x) { return x * x; }
+static inline double cube(double x) { return x * x * x; }
+
+// CoeffAtVerticesType0_1984 (:272-333): one pair (l, m) of equal vertex energies
+static void coef_type0(const double* Wv, double W0, int l, int m, double* d) {
+    int diff[2], c = 0;
+    for (int v = 0; v < 4; ++v) if (v != l && v != m) diff[c++] = v;
+    const int j = diff[0], k = diff[1];
+    for (int v = 0; v < 4; ++v) d[v] = 0.0;
+    const double Tjm = (W0 - Wv[j]) / (Wv[m] - Wv[j]);
+    const double Tkm = (W0 - Wv[k]) / (Wv[m] - Wv[k]);
+    const double dlm = (cube(W0 - Wv[j]) / ((Wv[j] - Wv[k]) * cube(Wv[j] - Wv[m]))) * std::log(std::fabs(W0 - Wv[j])) +
+                       (cube(W0 - Wv[k]) / ((Wv[k] - Wv[j]) * cube(Wv[k] - Wv[m]))) * std::log(std::fabs(W0 - Wv[k])) +
+                       ((W0 - Wv[m]) / ((Wv[m] - Wv[j]) * (Wv[m] - Wv[k]))) *
+                           (0.5 + Tjm + Tkm + (Tjm * Tjm + Tkm * Tkm + Tjm * Tkm) * std::log(std::fabs(W0 - Wv[m])));
+    d[l] = dlm;
+    d[m] = dlm;
+    for (int vv = 0; vv < 2; ++vv) {
+        const int i = diff[vv], L = diff[(vv + 1) % 2];
+        d[i] = (sq(W0 - Wv[i]) / (sq(Wv[i] - Wv[m]) * (Wv[L] - Wv[i]))) *
+                   (1.0 + ((2.0 * (W0 - Wv[m]) / (Wv[i] - Wv[m])) + ((W0 - Wv[L]) / (Wv[i] - Wv[L]))) *
+                              std::log(std::fabs(W0 - Wv[i]))) +
+               (sq(W0 - Wv[m]) / (sq(Wv[m] - Wv[i]) * (Wv[L] - Wv[m]))) *
+                   (1.0 + ((2.0 * (W0 - Wv[i]) / (Wv[m] - Wv[i])) + ((W0 - Wv[L]) / (Wv[m] - Wv[L]))) *
+                              std::log(std::fabs(W0 - Wv[m]))) +
+               (cube(W0 - Wv[L]) / (sq(Wv[L] - Wv[i]) * sq(Wv[L] - Wv[m]))) * std::log(std::fabs(W0 - Wv[L]));
+    }
+}
+
+// CoeffAtVerticesType1_2004 (:336-371): vertices 1, 2, 3 equal
+static void coef_type1(const double* Wv, double W0, double* d) {
+    const double g1 = W0 - Wv[0], g4 = W0 - Wv[3];
+    const double g41 = g4 / g1, g14 = g1 / g4;
+    const double q = 11.0 / (6.0 * (1.0 - g41)) - 5.0 / (2.0 * sq(1.0 - g41)) + 1.0 / cube(1.0 - g41) +
+                     std::log(std::fabs(g41)) / (sq(sq(1.0 - g14)) * g41);
+    d[0] = d[1] = d[2] = q / g1;
+    d[3] = (3.0 / sq(1.0 - g41) - 6.0 / cube(1.0 - g41) + 3.0 / sq(sq(1.0 - g41))) * (std::log(std::fabs(g14)) / g14) +
+           1.0 / cube(1.0 - g14) + 2.5 * g41 / sq(1.0 - g41) - 2.0 * g41 / cube(1.0 - g41);
+    d[3] = d[3] / g4;
+}
+
+// CoeffAtVerticesType3_2004 (:374-409): vertices 2, 3, 4 equal
+static void coef_type3(const double* Wv, double W0, double* d) {
+    const double g1 = W0 - Wv[0], g2 = W0 - Wv[1];
+    const double g12 = g1 / g2, g21 = g2 / g1;
+    const double q = 11.0 / (6.0 * (1.0 - g12)) - 5.0 / (2.0 * sq(1.0 - g12)) + 1.0 / cube(1.0 - g12) +
+                     std::log(std::fabs(g12)) / (sq(sq(1.0 - g21)) * g12);
+    d[1] = d[2] = d[3] = q / g2;
+    d[0] = (3.0 / sq(1.0 - g12) - 6.0 / cube(1.0 - g12) + 3.0 / sq(sq(1.0 - g12))) * (std::log(std::fabs(g21)) / g21) +
+           1.0 / cube(1.0 - g21) + 2.5 * g12 / sq(1.0 - g12) - 2.0 * g12 / cube(1.0 - g12);
+    d[0] = d[0] / g1;
+}
+
+// CoeffAtVerticesType2_2004 (:412-447): vertices 1 = 2 and 3 = 4
+static void coef_type2(const double* Wv, double W0, double* d) {
+    const double g1 = W0 - Wv[0], g3 = W0 - Wv[2];
+    const double g31 = g3 / g1, g13 = g1 / g3;
+    const double q12 = 2.5 / sq(1.0 - g31) - 2.0 / cube(1.0 - g31) + g13 / cube(1.0 - g13) +
+                       3.0 * (1.0 / cube(1.0 - g13) - 1.0 / sq(sq(1.0 - g13))) * (std::log(std::fabs(g31)) / g31);
+    const double q34 = 2.5 / sq(1.0 - g13) - 2.0 / cube(1.0 - g13) + g31 / cube(1.0 - g31) +
+                       3.0 * (1.0 / cube(1.0 - g31) - 1.0 / sq(sq(1.0 - g31))) * (std::log(std::fabs(g13)) / g13);
+    d[0] = d[1] = q12 / g1;
+    d[2] = d[3] = q34 / g3;
+}
+
+// CoeffAtVerticesTypeD_2004 (:450-496): all vertex energies distinct
+static void coef_typeD(const double* Wv, double W0, double* d) {
+    for (int v = 0; v < 4; ++v) {
+        const double g1 = W0 - Wv[v], g2 = W0 - Wv[(v + 1) % 4], g3 = W0 - Wv[(v + 2) % 4], g4 = W0 - Wv[(v + 3) % 4];
+        const double q = 1.0 / ((1.0 - g2 / g1) * (1.0 - g3 / g1) * (1.0 - g4 / g1)) +
+                         (1.0 / (sq(1.0 - g1 / g2) * (1.0 - g3 / g2) * (1.0 - g4 / g2))) * (std::log(std::fabs(g2 / g1)) / (g2 / g1)) +
+                         (1.0 / (sq(1.0 - g1 / g3) * (1.0 - g2 / g3) * (1.0 - g4 / g3))) * (std::log(std::fabs(g3 / g1)) / (g3 / g1)) +
+                         (1.0 / (sq(1.0 - g1 / g4) * (1.0 - g2 / g4) * (1.0 - g3 / g4))) * (std::log(std::fabs(g4 / g1)) / (g4 / g1));
+        d[v] = q / g1;
+    }
+}
+
+// GFcoeffv_RealPart (:153-269): the degeneracy pattern of the sorted vertex energies picks the form
+static void gf_real(const double* Wv, double W0, double* d) {
+    bool check[4] = {true, true, true, true};
+    int same = 0, types = 0, pairs[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+    for (int i = 0; i < 4; ++i) {
+        bool first = true;
+        if (!check[i]) continue;
+        for (int j = i + 1; j < 4; ++j)
+            if (std::fabs(Wv[i] - Wv[j]) < zero_prec) {
+                if (same < 3) { pairs[same][0] = i; pairs[same][1] = j; }
+                ++same;
+                if (first) { first = false; ++types; }
+                check[j] = false;
+            }
+    }
+    for (int v = 0; v < 4; ++v) d[v] = 0.0;
+    if (same == 0) coef_typeD(Wv, W0, d);
+    else if (same == 1) coef_type0(Wv, W0, pairs[0][0], pairs[0][1], d);
+    else if (same == 2) {
+        if (types == 1) {
+            if (pairs[0][0] == 0 && pairs[1][0] == 0) coef_type1(Wv, W0, d);
+            else if (pairs[0][0] == 1 && pairs[1][0] == 1) coef_type3(Wv, W0, d);
+        } else if (types == 2) coef_type2(Wv, W0, d);
+    } else if (same == 3) {
+        for (int v = 0; v < 4; ++v) d[v] = 0.25 / (W0 - Wv[0]);
+    }
+}
+
+// DiracDeltaCoeffVertices_1984 (:499-587), sorted energies E1..E4 and E
+static void delta_coef(const double* Ev, double E, double* c) {
+    const double E1 = Ev[0], E2 = Ev[1], E3 = Ev[2], E4 = Ev[3];
+    const double cp = 1.0e-8;
+    if ((E1 - E) <= cp && (E - E2) <= cp) {
+        c[0] = ((E2 - E) / (E2 - E1) + (E3 - E) / (E3 - E1) + (E4 - E) / (E4 - E1)) *
+               (sq(E - E1) / ((E4 - E1) * (E3 - E1) * (E2 - E1)));
+        c[1] = cube(E - E1) / (sq(E2 - E1) * (E3 - E1) * (E4 - E1));
+        c[2] = cube(E - E1) / ((E2 - E1) * sq(E3 - E1) * (E4 - E1));
+        c[3] = cube(E - E1) / ((E2 - E1) * (E3 - E1) * sq(E4 - E1));
+    } else if ((E2 - E) <= cp && (E - E3) <= cp) {
+        const double a = ((E3 - E) * (E - E2)) / ((E4 - E2) * (E3 - E2)), b = ((E4 - E) * (E - E1)) / ((E4 - E1) * (E4 - E2)),
+                     cc = ((E3 - E) * (E - E1)) / ((E3 - E2) * (E4 - E1));
+        const double a2 = ((E4 - E) * (E - E1)) / ((E4 - E2) * (E3 - E1)), b2 = ((E4 - E) * (E - E2)) / ((E4 - E2) * (E3 - E2)),
+                     c2 = ((E3 - E) * (E - E1)) / ((E3 - E1) * (E3 - E2));
+        const double a3 = ((E3 - E) * (E - E2)) / ((E4 - E2) * (E3 - E1)), b3 = ((E4 - E) * (E - E2)) / ((E4 - E2) * (E4 - E1)),
+                     c3 = ((E3 - E) * (E - E1)) / ((E3 - E1) * (E4 - E1));
+        const double a4 = ((E3 - E) * (E - E2)) / ((E3 - E2) * (E3 - E1)), b4 = ((E4 - E) * (E - E1)) / ((E4 - E1) * (E3 - E1)),
+                     c4 = ((E4 - E) * (E - E2)) / ((E3 - E2) * (E4 - E1));
+        c[0] = ((E3 - E) / sq(E3 - E1)) * (a + b + cc) + ((E4 - E) / sq(E4 - E1)) * (a2 + b2 + c2);
+        c[1] = ((E3 - E) / sq(E3 - E2)) * (a3 + b3 + c3) + ((E4 - E) / sq(E4 - E2)) * (a4 + b4 + c4);
+        c[2] = ((E - E2) / sq(E3 - E2)) * (a3 + b3 + c3) + ((E - E1) / sq(E3 - E1)) * (a + b + cc);
+        c[3] = ((E - E2) / sq(E4 - E2)) * (a4 + b4 + c4) + ((E - E1) / sq(E4 - E1)) * (a2 + b2 + c2);
+        for (int v = 0; v < 4; ++v) c[v] *= 0.5;
+    } else if ((E3 - E) <= cp && (E - E4) <= cp) {
+        c[0] = cube(E4 - E) / (sq(E4 - E1) * (E4 - E2) * (E4 - E3));
+        c[1] = cube(E4 - E) / ((E4 - E1) * sq(E4 - E2) * (E4 - E3));
+        c[2] = cube(E4 - E) / ((E4 - E1) * (E4 - E2) * sq(E4 - E3));
+        c[3] = ((E - E3) / (E4 - E3) + (E - E2) / (E4 - E2) + (E - E1) / (E4 - E1)) *
+               (sq(E4 - E) / ((E4 - E1) * (E4 - E2) * (E4 - E3)));
+    } else {
+        for (int v = 0; v < 4; ++v) c[v] = 0.0;
+    }
+}
+
+// CoefAtVertOfTetrhd (:35-77): sorts W (and v, F) in place; coefficient d - i pi c per sorted vertex,
+// NaN parts set to zero.
+void orc_pd_coeff(double W0, double* W, int* v, double* re, double* im) {
+    sort_gf(W, v, nullptr);
+    double d[4], c[4];
+    gf_real(W, W0, d);
+    delta_coef(W, W0, c);
+    for (int k = 0; k < 4; ++k) {
+        if (std::isnan(d[k])) d[k] = 0.0;
+        if (std::isnan(c[k])) c[k] = 0.0;
+        re[k] = d[k];
+        im[k] = -PI * c[k];
+    }
+}
+
+// PerturbationMatrix (point_defect_m.f90:40-108) and IFC2 (:111-136): home-cell FC2 blocks of the
+// perturbed and pristine crystals (0 where the pair is absent).  V_FC(Ndof,Ndof) in (rad/ps)^2,
+// V_M(Ndof,Ndof) diagonal (M_def - m) / m.
+void orc_pd_perturbation(int nb, int na, const int* num, const int* idx, const double* fc, int na_p,
+                         const int* num_p, const int* idx_p, const double* fc_p, const double* mass,
+                         const double* mass_def, double* vfc, double* vm) {
+    const int ndof = 3 * nb;
+    const double wTHz = std::sqrt(1.60217733 * 6.02214076 * 10.0) * 10.0;
+    auto ifc2 = [&](int nA, const int* nm, const int* ix, const double* f, int mu, int nu, int al, int be) {
+        for (int N = 0; N < nm[mu]; ++N) {
+            const int* e = ix + 4 * (N + nA * mu);
+            if (e[3] - 1 == nu && e[0] == 0 && e[1] == 0 && e[2] == 0)
+                return f[be + 3 * al + 9 * N + (size_t)9 * nA * mu];   // fC(1, beta, alpha, N, mu)
+        }
+        return 0.0;
+    };
+    for (int i = 0; i < ndof * ndof; ++i) { vfc[i] = 0.0; vm[i] = 0.0; }
+    for (int nu = 0; nu < nb; ++nu)
+        for (int be = 0; be < 3; ++be) {
+            const int col = 3 * nu + be;
+            for (int mu = 0; mu < nb; ++mu)
+                for (int al = 0; al < 3; ++al) {
+                    const int row = 3 * mu + al;
+                    const double p = ifc2(na, num, idx, fc, mu, nu, al, be);
+                    const double d = ifc2(na_p, num_p, idx_p, fc_p, mu, nu, al, be);
+                    vfc[row + ndof * col] = (d - p) / std::sqrt(mass[mu] * mass[nu]) * (wTHz * wTHz);
+                    if (mu == nu && al == be) vm[row + ndof * col] = (mass_def[mu] - mass[mu]) / mass[mu];
+                }
+        }
+}
+
+// zinverse (LAPACK zgetrf + zgetri): in place, false when a pivot is exactly zero
+static bool cinverse(std::vector<cplx>& A, int n) {
+    std::vector<int> piv(n);
+    for (int k = 0; k < n; ++k) {  // LU with partial pivoting, column-major A(i, j) = A[i + n j]
+        int p = k;
+        for (int i = k + 1; i < n; ++i) if (std::abs(A[i + n * k]) > std::abs(A[p + n * k])) p = i;
+        piv[k] = p;
+        if (A[p + n * k] == cplx(0.0, 0.0)) return false;
+        if (p != k) for (int j = 0; j < n; ++j) std::swap(A[k + n * j], A[p + n * j]);
+        for (int i = k + 1; i < n; ++i) A[i + n * k] /= A[k + n * k];
+        for (int j = k + 1; j < n; ++j)
+            for (int i = k + 1; i < n; ++i) A[i + n * j] -= A[i + n * k] * A[k + n * j];
+    }
+    // inverse by solving A X = P I column by column
+    std::vector<cplx> X((size_t)n * n, cplx(0.0, 0.0));
+    for (int c = 0; c < n; ++c) {
+        std::vector<cplx> b(n, cplx(0.0, 0.0));
+        b[c] = 1.0;
+        for (int k = 0; k < n; ++k) std::swap(b[k], b[piv[k]]);
+        for (int i = 0; i < n; ++i) for (int j = 0; j < i; ++j) b[i] -= A[i + n * j] * b[j];
+        for (int i = n - 1; i >= 0; --i) {
+            for (int j = i + 1; j < n; ++j) b[i] -= A[i + n * j] * b[j];
+            b[i] /= A[i + n * i];
+        }
+        for (int i = 0; i < n; ++i) X[i + n * c] = b[i];
+    }
+    A = X;
+    return true;
+}
+
+// ScatterRatePointDefect (point_defect_m.f90:139-231) for one irreducible q0: tau_inv(Ndof).
+// Point-defect mesh: tetra(4, 6 Nq) 1-based, w2(Ndof, Nq) = omega^2, evec(Ndof, Ndof, Nq)
+// (Evec(row, s, q)); q0: omega0(Ndof) (rad/ps), e0(Ndof, Ndof); gamma0: q0 is Gamma.
+void orc_pd_rate(int ndof, int nq, const int* tetra, const double* w2, const double* evec_ri,
+                 const double* omega0, const double* e0_ri, int gamma0, const double* vfc, const double* vm,
+                 double rho, double vol, int mat_inv_full, int optc_therm, double* tau_inv) {
+    const cplx* ev = reinterpret_cast<const cplx*>(evec_ri);
+    const cplx* e0 = reinterpret_cast<const cplx*>(e0_ri);
+    const int n = ndof, ntet = 6 * nq;
+    for (int s0 = 0; s0 < n; ++s0) tau_inv[s0] = 0.0;
+    for (int s0 = gamma0 ? 3 : 0; s0 < n; ++s0) {
+        const double W0 = omega0[s0] * omega0[s0];
+        // GreensFunction: G = sum_tet sum_s sum_v Coeff_v F_v / NT, F_v = e e^H at the sorted vertex
+        std::vector<cplx> G((size_t)n * n, cplx(0.0, 0.0));
+        for (int t = 0; t < ntet; ++t)
+            for (int s = 0; s < n; ++s) {
+                double W[4], re[4], im[4];
+                int v[4];
+                for (int k = 0; k < 4; ++k) { v[k] = tetra[4 * t + k] - 1; W[k] = w2[s + (size_t)n * v[k]]; }
+                orc_pd_coeff(W0, W, v, re, im);
+                for (int k = 0; k < 4; ++k) {
+                    const cplx cf(re[k], im[k]);
+                    const cplx* e = ev + (size_t)n * s + (size_t)n * n * v[k];
+                    for (int b = 0; b < n; ++b)
+                        for (int a = 0; a < n; ++a) G[a + n * b] += cf * (e[a] * std::conj(e[b]));
+                }
+            }
+        for (auto& g : G) g /= double(ntet);
+        std::vector<double> V((size_t)n * n);
+        for (int i = 0; i < n * n; ++i) V[i] = vfc[i] - W0 * vm[i];
+        std::vector<cplx> VG((size_t)n * n, cplx(0.0, 0.0)), T((size_t)n * n, cplx(0.0, 0.0));
+        for (int j = 0; j < n; ++j)
+            for (int k = 0; k < n; ++k)
+                for (int i = 0; i < n; ++i) VG[i + n * j] += V[i + n * k] * G[k + n * j];
+        auto v_plus_vgv = [&]() {
+            for (int j = 0; j < n; ++j)
+                for (int i = 0; i < n; ++i) {
+                    cplx acc = V[i + n * j];
+                    for (int k = 0; k < n; ++k) acc += VG[i + n * k] * V[k + n * j];
+                    T[i + n * j] = acc;
+                }
+        };
+        if (mat_inv_full) {
+            std::vector<cplx> M((size_t)n * n);
+            for (int i = 0; i < n * n; ++i) M[i] = -VG[i];
+            for (int i = 0; i < n; ++i) M[i + n * i] += 1.0;
+            if (!cinverse(M, n)) v_plus_vgv();
+            else
+                for (int j = 0; j < n; ++j)
+                    for (int i = 0; i < n; ++i) {
+                        cplx acc(0.0, 0.0);
+                        for (int k = 0; k < n; ++k) acc += M[i + n * k] * V[k + n * j];
+                        T[i + n * j] = acc;
+                    }
+        } else {
+            v_plus_vgv();
+        }
+        const cplx* e = e0 + (size_t)n * s0;
+        std::vector<cplx> Te(n, cplx(0.0, 0.0));
+        for (int i = 0; i < n; ++i) for (int k = 0; k < n; ++k) Te[i] += T[i + n * k] * e[k];
+        if (optc_therm) {
+            cplx x(0.0, 0.0);
+            for (int i = 0; i < n; ++i) x += std::conj(e[i]) * Te[i];
+            tau_inv[s0] = rho * vol * (-x.imag() / omega0[s0]);
+        } else {  // TetrahedronIntrg (:293-351)
+            double acc = 0.0;
+            for (int t = 0; t < ntet; ++t)
+                for (int s = 0; s < n; ++s) {
+                    double W[4], F[4], c[4];
+                    int v[4];
+                    for (int k = 0; k < 4; ++k) {
+                        v[k] = tetra[4 * t + k] - 1;
+                        W[k] = w2[s + (size_t)n * v[k]];
+                        const cplx* eq = ev + (size_t)n * s + (size_t)n * n * v[k];
+                        cplx d(0.0, 0.0);
+                        for (int i = 0; i < n; ++i) d += std::conj(eq[i]) * Te[i];
+                        F[k] = d.real() * d.real() + d.imag() * d.imag();
+                    }
+                    sort_gf(W, v, F);
+                    delta_coef(W, W0, c);
+                    for (int k = 0; k < 4; ++k) acc += c[k] * F[k];
+                }
+            tau_inv[s0] = rho * vol * (PI * acc / double(ntet)) / omega0[s0];
+        }
+    }
+}
+
 int orc_num_threads() {
 #ifdef _OPENMP
     return omp_get_max_threads();

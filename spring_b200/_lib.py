@@ -71,6 +71,8 @@ SIGNATURES = {
     "spring_kappa_iter_gauss": [P, D, D, I, P, P, P, P],
     "spring_set_dipole": [P, P, P, P, I, D, D, P, P, P],
     "spring_get_dipole": [P, P, P, P, P, P],
+    "spring_set_point_defect": [P, P, I, P, P, P, P, D, I, I],
+    "spring_linewidth_pd": [P, I, I, P, I],
     "spring_kernel_time": [P, ct.c_char_p, P, P],
     "spring_tc_stats": [P, P, P],
     "spring_binary_version": [I, P],

@@ -182,6 +182,26 @@ class Context:
         self._call("spring_get_dipole", ct.byref(on), ct.byref(lm), _ptr(g), ct.byref(nr), ct.byref(ng))
         return float(lm.value), tuple(int(x) for x in g), int(nr.value), int(ng.value)
 
+    def set_point_defect(self, qmesh_pd, atm_num, atm_indx, fc2, mass_def, rho_def=1e-6, mat_inv_full=True,
+                         optc_therm=True):
+        """Point-defect scattering: the perturbed FC2 (same layout as :meth:`set_fc2`), the defect masses
+        per basis atom, the defect density (A^-3) and the Green's-function mesh.  ``qmesh_pd=None``
+        switches it off."""
+        if qmesh_pd is None:
+            self._call("spring_set_point_defect", None, 0, None, None, None, None, 0.0, 0, 0)
+            return
+        na = int(np.asarray(atm_indx).shape[1])
+        self._call("spring_set_point_defect", _ptr(_c(qmesh_pd, np.int32)), na, _ptr(_c(atm_num, np.int32)),
+                   _ptr(_c(atm_indx, np.int32)), _ptr(_c(fc2, np.float64)), _ptr(_c(mass_def, np.float64)),
+                   float(rho_def), int(bool(mat_inv_full)), int(bool(optc_therm)))
+
+    def linewidth_pd(self, i0_first: int = 1, n_q0: int | None = None, add: bool = False):
+        """Point-defect scattering rates (n_q0, Ndof); with add, 0.5 x rate joins LW_Allq0."""
+        n_q0 = self.nq0 - i0_first + 1 if n_q0 is None else n_q0
+        out = np.zeros((n_q0, self.ndof))
+        self._call("spring_linewidth_pd", int(i0_first), int(n_q0), _ptr(out), int(bool(add)))
+        return out
+
     def set_fc2(self, atm_num, atm_indx, fc2):
         na = int(np.asarray(atm_indx).shape[1])
         self._call("spring_set_fc2", na, _ptr(_c(atm_num, np.int32)), _ptr(_c(atm_indx, np.int32)),

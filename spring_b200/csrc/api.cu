@@ -329,6 +329,9 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_bteg_row); dfree(c->d_bteg_kk); dfree(c->d_bteg_pq);
         dfree(c->ew.g); dfree(c->ew.r); dfree(c->ew.hz); dfree(c->ew.tau); dfree(c->ew.z); dfree(c->ew.cc);
         dfree(c->ew.dd);
+        dfree(c->pd.vfc); dfree(c->pd.vm); dfree(c->pd.qpnt); dfree(c->pd.w2); dfree(c->pd.qint); dfree(c->pd.tet);
+        dfree(c->pd.inc); dfree(c->pd.gamma0); dfree(c->pd.wgt); dfree(c->pd.G); dfree(c->pd.te0);
+        free_phonons(c->pd.ph);
         dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_items); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
@@ -513,6 +516,32 @@ int spring_set_dipole(spring_ctx* c, const double* atm_pos, const double* dielec
     return set_dipole(c, atm_pos, dielec, born_z, decide_ew_param, prec_ew, lmb, gmesh, rmesh, sup_cell);
 }
 
+int spring_set_point_defect(spring_ctx* c, const int* qmesh_pd, int na2_pd, const int* num_pd, const int* idx_pd,
+                            const double* fc2_pd, const double* mass_def, double rho_def, int mat_inv_full,
+                            int optc_therm) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->fc2_set, "FC2"));
+    SPRING_CHECK(need(c, c->mesh_set, "mesh"));
+    return set_point_defect(c, qmesh_pd, na2_pd, num_pd, idx_pd, fc2_pd, mass_def, rho_def, mat_inv_full, optc_therm);
+}
+
+int spring_linewidth_pd(spring_ctx* c, int i0_first, int n_q0, double* rate, int add) {
+    CTX_ENTER(c);
+    SPRING_CHECK(need(c, c->pd.on, "point defect (spring_set_point_defect)"));
+    SPRING_CHECK(need(c, c->ph_irr.set, "irreducible phonons"));
+    if (i0_first < 1 || n_q0 < 0 || i0_first - 1 + n_q0 > c->nq0) return fail(c, SPRING_ERR_ARG, "q0 range out of bounds");
+    if (n_q0 == 0) return SPRING_OK;
+    const int q0 = i0_first - 1, n = c->ndof;
+    DBuf<double> d_rate;
+    SPRING_CHECK(dalloc(c, d_rate, (size_t)n_q0 * n, "point-defect rate"));
+    int rc = run_point_defect(c, q0, n_q0, d_rate.p);
+    if (rc == SPRING_OK && add) rc = run_point_defect_add(c, q0, n_q0, d_rate.p);
+    if (rc == SPRING_OK && rate) rc = d2h(c, rate, d_rate.p, sizeof(double) * n_q0 * n, "point-defect rate");
+    cudaStreamSynchronize(c->stream);
+    dfree(d_rate);
+    return rc;
+}
+
 int spring_get_dipole(spring_ctx* c, int* on, double* lmb, int* gmesh, int* n_r, int* n_g) {
     CTX_ENTER(c);
     if (on) *on = c->ew.on ? 1 : 0;
@@ -541,6 +570,9 @@ int spring_set_fc2(spring_ctx* c, int na2, const int* num, const int* idx, const
     SPRING_CHECK(h2d(c, c->d_fc2.p, fc, sizeof(double) * c->nb * na2 * 9, "FC2"));
     SPRING_CHECK(h2d(c, c->d_fc2_idx.p, idx, sizeof(int) * c->nb * na2 * 4, "FC2 index"));
     SPRING_CHECK(h2d(c, c->d_fc2_num.p, num, sizeof(int) * c->nb, "FC2 counts"));
+    c->h_fc2.assign(fc, fc + (size_t)c->nb * na2 * 9);
+    c->h_fc2_idx.assign(idx, idx + (size_t)c->nb * na2 * 4);
+    c->h_fc2_num.assign(num, num + c->nb);
     c->fc2_set = true;
     return SPRING_OK;
 }

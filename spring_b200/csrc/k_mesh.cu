@@ -125,6 +125,23 @@ int run_make_mesh(spring_ctx* c, const int shift[3], int zc) {
     return launch_check(c, "k_tetrahedra");
 }
 
+int run_make_mesh_on(spring_ctx* c, const int mesh[3], const int shift[3], int zc, int* d_qint, double* d_qpnt,
+                     int* d_tet) {
+    MeshArgs a = mesh_args(c, shift, zc);
+    a.n0 = mesh[0];
+    a.n1 = mesh[1];
+    a.n2 = mesh[2];
+    for (int r = 0; r < 3; ++r)
+        for (int k = 0; k < 3; ++k) a.ru[r * 3 + k] = c->G[r + 3 * k] / mesh[k];
+    const int nq = mesh[0] * mesh[1] * mesh[2];
+    const int threads = 256, blocks = (nq + threads - 1) / threads;
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "make_mesh: injected launch failure");
+    k_grid_points<<<blocks, threads, 0, c->stream>>>(a, d_qint, d_qpnt);
+    SPRING_CHECK(launch_check(c, "k_grid_points"));
+    k_tetrahedra<<<blocks, threads, 0, c->stream>>>(a, reinterpret_cast<int4*>(d_tet));
+    return launch_check(c, "k_tetrahedra");
+}
+
 int run_irr_map(spring_ctx* c, const int* d_rot, int nrot, int time_rev, int* d_map) {
     const int threads = 256;
     const int blocks = (c->nq + threads - 1) / threads;

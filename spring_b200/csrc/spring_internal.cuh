@@ -86,6 +86,17 @@ struct EwaldDev {
     DBuf<double2> cc, dd;
 };
 
+// Point-defect scattering (spring_set_point_defect, k_pdef.cu).
+struct PointDefectDev {
+    bool on = false, mat_inv_full = true, optc_therm = true;
+    int nq = 0;
+    double rho = 0.0;
+    DBuf<double> vfc, vm, qpnt, w2;
+    DBuf<int> qint, tet, inc, gamma0;
+    DBuf<double2> wgt, G, te0;
+    Phonons ph;
+};
+
 }  // namespace spring
 
 struct spring_ctx {
@@ -192,6 +203,9 @@ struct spring_ctx {
     spring::DBuf<int> d_neg;       // [q] grid index of -q
     spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
     spring::EwaldDev ew;
+    spring::PointDefectDev pd;
+    std::vector<double> h_fc2;     // host copies of FC2 (the point-defect perturbation)
+    std::vector<int> h_fc2_idx, h_fc2_num;
     // sorted Gaussian BTE operator (k_bte.cu run_bte_gauss): rows, (k1, k2), (P, Q)
     spring::DBuf<int> d_bteg_row;
     spring::DBuf<int2> d_bteg_kk;
@@ -306,6 +320,13 @@ int run_irr_map(spring_ctx* c, const int* d_rot, int nrot, int time_rev, int* d_
 int run_phonons(spring_ctx* c, Phonons& ph, const double* d_q, int n, int gamma_mode = 0);
 int set_dipole(spring_ctx* c, const double* atm_pos, const double* eps, const double* zstar, int decide,
                double prec_ew, double lmb, const int* gmesh, const int* rmesh, const int* sup_cell);
+int set_point_defect(spring_ctx* c, const int* qmesh, int na_p, const int* num_p, const int* idx_p, const double* fc_p,
+                     const double* mass_def, double rho, int mat_inv_full, int optc_therm);
+int run_point_defect(spring_ctx* c, int i0_first, int n_q0, double* d_rate);
+int run_point_defect_add(spring_ctx* c, int i0_first, int n_q0, const double* d_rate);
+// make_tetrahedron for another mesh into the given buffers (qint [nq][3], qpnt [nq][3], tet [6 nq][4])
+int run_make_mesh_on(spring_ctx* c, const int mesh[3], const int shift[3], int zc, int* d_qint, double* d_qpnt,
+                     int* d_tet);
 int launch_ewald(spring_ctx* c, const double* qa, int nqa, const int* list_a, int n_a, const double* qb, int nqb,
                  int n_b, int gamma_mode, const double2** dd_out);
 int run_phonons_mesh(spring_ctx* c);  // grid + irreducible points (time reversal on Gamma-centred meshes)

@@ -142,13 +142,14 @@ int spring_h5_read_fc(const char* path, int order, int nb, int na, int* atm_num,
 }
 
 int spring_h5_write_kappa(const char* path, const double* kappa, int ndof, int nq0, const double* linewidth,
-                          const double* phase_space, const double* mode_k) {
+                          const double* phase_space, const double* mode_k, const double* scatter_pd) {
     if (!path || !kappa || !linewidth || !phase_space || ndof < 1 || nq0 < 1) return fail("spring_h5_write_kappa: bad arguments");
     h5lite::Group root;
     root.datasets["ThermalConductivityTensor"] = h5lite::make_f64(kappa, {9});
     root.datasets["LineWidth"] = h5lite::make_f64(linewidth, {(uint64_t)(2 * ndof), (uint64_t)nq0});
     root.datasets["PhaseSpace3rd"] = h5lite::make_f64(phase_space, {(uint64_t)(2 * ndof), (uint64_t)nq0});
     if (mode_k) root.datasets["ModeResolvedKappa"] = h5lite::make_f64(mode_k, {9, (uint64_t)ndof});
+    if (scatter_pd) root.datasets["Scatter_pd"] = h5lite::make_f64(scatter_pd, {(uint64_t)(2 * ndof), (uint64_t)nq0});
     const std::string e = h5lite::write_file(path, root);
     return e.empty() ? 0 : fail(e);
 }

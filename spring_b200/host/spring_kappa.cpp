@@ -285,12 +285,55 @@ int main(int argc, char** argv) {
 
     // ---- force constants
     const std::string tc = temp_char(T);
+    // Point defects: &PointDefInfo (ReadPointDefVar, Helper_m.f90:135-307) with its defaults and checks
+    const double FILL = 99999.0;
+    const bool point_def = groups.count("pointdefinfo") > 0;
+    std::string ifc2_pd = "FC2nd_" + prefix + tc + "K_F_pd.h5";
+    std::vector<double> mass_def(mass);
+    double rho_def = 1.0e-6;
+    std::vector<int> qmesh_pd{7, 7, 7};
+    bool mat_inv_full = true, optc_therm = true;
+    if (point_def) {
+        const nml::Group& pdi = groups["pointdefinfo"];
+        std::vector<double> mdef_in(nb, FILL);
+        std::vector<int> def_pos(nb, 0), cell_atom(4 * 5, (int)FILL);
+        int numdef = 0;
+        check(nml::get(pdi, "IFC2_file_pd", ifc2_pd));
+        check(nml::get(pdi, "Mass_def", {nb}, mdef_in));
+        check(nml::get(pdi, "rho_def", rho_def));
+        check(nml::get(pdi, "qMesh_pd", {3}, qmesh_pd));
+        check(nml::get(pdi, "def_pos", {nb}, def_pos));
+        check(nml::get(pdi, "NumDef_sup", numdef));
+        check(nml::get(pdi, "cell_atom", {4, 5}, cell_atom));
+        check(nml::get(pdi, "MatInvFull", mat_inv_full));
+        check(nml::get(pdi, "OptcTherm", optc_therm));
+        if (std::all_of(def_pos.begin(), def_pos.end(), [](int v) { return v == 0; }))
+            die("&PointDefInfo: def_pos (mandatory) is not provided");
+        int cnt = 0;
+        for (int mu = 0; mu < nb; ++mu)
+            if (def_pos[mu] != 0) {
+                if (std::fabs(mdef_in[cnt] - FILL) < 1e-8)
+                    die("&PointDefInfo: def_pos names more defects than Mass_def gives masses");
+                mass_def[mu] = mdef_in[cnt];
+                mdef_in[cnt++] = 0.0;
+            }
+        for (int mu = 0; mu < nb; ++mu)
+            if (!(mdef_in[mu] < 1e-8 || std::fabs(mdef_in[mu] - FILL) < 1e-8))
+                die("&PointDefInfo: mismatch between def_pos and Mass_def");
+        if (numdef <= 0) die("&PointDefInfo: NumDef_sup is 0");
+        for (int k = 0; k < std::min(numdef, 5); ++k)
+            for (int r = 0; r < 4; ++r)
+                if (cell_atom[4 * k + r] == (int)FILL) die("&PointDefInfo: NumDef_sup and cell_atom do not match");
+    }
     const Fc f2 = read_fc("FC2nd_" + prefix + tc + "K_F.h5", 2);
     const Fc f3 = read_fc("FC3rd_" + prefix + tc + "K_F.h5", 3);
     Fc f4;
     if (four) f4 = read_fc("FC4th_" + prefix + tc + "K_F.h5", 4);
+    Fc f2pd;
+    if (point_def) f2pd = read_fc(ifc2_pd, 2);
     for (const Fc* f : {&f2, &f3})
         if (f->nb != nb) die("FC file basis count differs from Nbasis");
+    if (point_def && f2pd.nb != nb) die(ifc2_pd + ": basis count differs from Nbasis");
     const std::vector<int> rot = point_group(lat, pos, typ, nb, std::max(symprec, 1e-7));
     const int nrot = (int)rot.size() / 9;
 
@@ -313,9 +356,15 @@ int main(int argc, char** argv) {
         for (double v : f4.fc) s4 += v * v;
         std::printf("], \"na2\": %d, \"na3\": %d, \"na4\": %d, \"fc2_sum\": %.15g, \"fc3_sumsq\": %.15g, "
                     "\"fc4_sumsq\": %.15g, \"n_rotations\": %d, \"force_dd\": %s, \"ewald_lmb\": %.15g, "
-                    "\"ewald_gmesh\": [%d, %d, %d], \"ewald_points\": [%d, %d]}\n",
+                    "\"ewald_gmesh\": [%d, %d, %d], \"ewald_points\": [%d, %d], \"point_defect\": %s, "
+                    "\"qmesh_pd\": [%d, %d, %d], \"rho_def\": %.15g, \"mat_inv_full\": %s, \"optc_therm\": %s, "
+                    "\"ifc2_file_pd\": \"%s\", \"mass_def\": [",
                     f2.na, f3.na, four ? f4.na : 0, s2, s3, s4, nrot, force_dd ? "true" : "false", ew_lmb, ew_g[0],
-                    ew_g[1], ew_g[2], ew_cnt[0], ew_cnt[1]);
+                    ew_g[1], ew_g[2], ew_cnt[0], ew_cnt[1], point_def ? "true" : "false", qmesh_pd[0], qmesh_pd[1],
+                    qmesh_pd[2], rho_def, mat_inv_full ? "true" : "false", optc_therm ? "true" : "false",
+                    ifc2_pd.c_str());
+        for (int i = 0; i < nb; ++i) std::printf("%s%.10g", i ? ", " : "", mass_def[i]);
+        std::printf("]}\n");
         return 0;
     }
 
@@ -340,6 +389,10 @@ int main(int argc, char** argv) {
     std::vector<int> irr((size_t)3 * nq), posq(nq), mult(nq);
     gpu(c, spring_find_irr_q(c, nrot, rot.data(), time_rev, &nq0, irr.data(), posq.data(), mult.data()));
     gpu(c, spring_compute_phonons(c, &T, freq_cut));
+    if (point_def)
+        gpu(c, spring_set_point_defect(c, qmesh_pd.data(), f2pd.na, f2pd.num.data(), f2pd.idx.data(), f2pd.fc.data(),
+                                       mass_def.data(), rho_def, mat_inv_full ? 1 : 0, optc_therm ? 1 : 0));
+    std::vector<double> scat_pd(point_def ? (size_t)ndof * nq0 : 0, 0.0);
     const int prec = precision == "bf16x3" ? SPRING_BF16X3 : (precision == "bf16" ? SPRING_BF16 : SPRING_FP64);
     if (precision != "fp64" && precision != "bf16" && precision != "bf16x3") die("-precision: fp64, bf16 or bf16x3");
     gpu(c, spring_set_precision(c, prec));
@@ -369,6 +422,7 @@ int main(int argc, char** argv) {
         std::copy(p3b.begin(), p3b.end(), p3.begin() + (size_t)ndof * (i0 - 1));
         if (isotope) gpu(c, spring_linewidth_iso(c, i0, n, dm, sigma, g2iso.data(), nullptr));
         if (four) gpu(c, spring_linewidth4(c, i0, n, dm, sigma, pol4.data(), nullptr));
+        if (point_def) gpu(c, spring_linewidth_pd(c, i0, n, scat_pd.data() + (size_t)ndof * (i0 - 1), 1));
         if (wrestart) {
             gpu(c, spring_get_linewidths(c, lw_all.data()));
             if (spring_h5_write_restart(rfile.c_str(), ndof, nq0, i0 + n - 1, 1, lw_all.data()))
@@ -423,9 +477,32 @@ int main(int argc, char** argv) {
             // P_Allq0 = P_q0 * 1000 / (9 Ndof^2 Nq1points), in fs (main.f90:687)
             p3o[(size_t)2 * ndof * q + ndof + s] = p3[(size_t)ndof * q + s] * 1000.0 / (9.0 * ndof * ndof * (double)nq);
         }
+    std::vector<double> pdo;
+    if (point_def) {  // Scatter_pd: omega alongside the rates (w2dh5_no_grp_type2, main.f90:778)
+        pdo.resize((size_t)2 * ndof * nq0);
+        for (int q = 0; q < nq0; ++q)
+            for (int s = 0; s < ndof; ++s) {
+                pdo[(size_t)2 * ndof * q + s] = omega[(size_t)ndof * q + s];
+                pdo[(size_t)2 * ndof * q + ndof + s] = scat_pd[(size_t)ndof * q + s];
+            }
+    }
     if (spring_h5_write_kappa(kfile.c_str(), kappa.data(), ndof, nq0, lwo.data(), p3o.data(),
-                              mode_k ? modek.data() : nullptr))
+                              mode_k ? modek.data() : nullptr, point_def ? pdo.data() : nullptr))
         die(spring_host_last_error());
+    if (point_def) {  // ScatterRate_pd_IBZ_<prefix><T>K.txt (WriteAsciiOutFile, main.f90:669-670)
+        const std::string pfile = "ScatterRate_pd_IBZ_" + prefix + tc + "K.txt";
+        FILE* fp = std::fopen(pfile.c_str(), "w");
+        if (!fp) die("cannot write " + pfile);
+        std::fprintf(fp, "#--------- phonon_frequency(rad.THz) ( %4d columns) ---------      ---------- scattering "
+                         "rate(1/ps) ( %4d columns) ----------\n", ndof, ndof);
+        for (int q = 0; q < nq0; ++q) {
+            std::string line;
+            for (int s = 0; s < ndof; ++s) line += g20(omega[(size_t)ndof * q + s]) + "  ";
+            for (int s = 0; s < ndof; ++s) line += g20(scat_pd[(size_t)ndof * q + s]) + (s + 1 < ndof ? "  " : "");
+            std::fprintf(fp, "%s\n", line.c_str());
+        }
+        std::fclose(fp);
+    }
     FILE* fa = std::fopen(afile.c_str(), "w");
     if (!fa) die("cannot write " + afile);
     std::fprintf(fa, "#--------- phonon_frequency(rad.THz) ( %4d columns) ---------      ---------- linewidth(rad.THz) "

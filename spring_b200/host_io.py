@@ -29,7 +29,7 @@ def load():
         sig = {"spring_h5_write_fc": [ct.c_char_p, I, I, I, P, P, P],
                "spring_h5_fc_dims": [ct.c_char_p, I, P, P],
                "spring_h5_read_fc": [ct.c_char_p, I, I, I, P, P, P],
-               "spring_h5_write_kappa": [ct.c_char_p, P, I, I, P, P, P],
+               "spring_h5_write_kappa": [ct.c_char_p, P, I, I, P, P, P, P],
                "spring_h5_read_f64": [ct.c_char_p, ct.c_char_p, P, P, P, ct.c_longlong],
                "spring_h5_write_restart": [ct.c_char_p, I, I, I, I, P],
                "spring_h5_read_restart": [ct.c_char_p, I, I, P, P],
@@ -107,11 +107,14 @@ def read_restart(path, ndof, nq0):
 
 
 def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, four_phonon=False,
-                selection3=("D", "D", "D"), time_rev=0, write_restart=False, read_restart=False, dipole=None):
+                selection3=("D", "D", "D"), time_rev=0, write_restart=False, read_restart=False, dipole=None,
+                point_defect=None):
     """An input.nml with &FCInfo, &CrystalInfo, &AtmInfo (unit_mod.f90:64-209) and &AnhInfo
     (Helper_m.f90:37-132) for a synthetic crystal: one species per distinct mass.  ``dipole``
     (dict: rmesh, and optionally decide, prec_ew, lmb, gmesh, sup_cell) adds Force_dd, the crystal's
-    dielec and BornZ, and &EwaldInfo (EwaldParam.f90)."""
+    dielec and BornZ, and &EwaldInfo (EwaldParam.f90).  ``point_defect`` (dict: def_pos, Mass_def,
+    rho_def, qMesh_pd, NumDef_sup, cell_atom, MatInvFull, OptcTherm, IFC2_file_pd; any subset) writes
+    &PointDefInfo (Helper_m.f90:135-307)."""
     masses, typ = [], []
     for m in cr.mass:
         if float(m) not in masses:
@@ -147,6 +150,21 @@ def write_input(path, cr, prefix, qmesh, sigma=None, isotope=False, g2iso=None, 
         if dipole.get("gmesh") is not None:
             L.append("    Gmesh = %d %d %d\n" % tuple(dipole["gmesh"]))
         L.append("    Rmesh = %d %d %d\n/\n" % tuple(dipole["rmesh"]))
+    if point_defect is not None:
+        L.append("&PointDefInfo\n")
+        for k, v in point_defect.items():
+            if isinstance(v, bool):
+                L.append("    %s = %s\n" % (k, ".true." if v else ".false."))
+            elif isinstance(v, str):
+                L.append("    %s = '%s'\n" % (k, v))
+            elif k == "cell_atom":
+                for j, col in enumerate(v):
+                    L.append("    cell_atom(:, %d) = %s\n" % (j + 1, " ".join(str(int(x)) for x in col)))
+            elif np.ndim(v) == 0:
+                L.append("    %s = %.16g\n" % (k, v))
+            else:
+                L.append("    %s = %s\n" % (k, " ".join("%.16g" % x for x in np.ravel(v))))
+        L.append("/\n")
     L.append("&AnhInfo\n    qmesh = %d %d %d\n    time_rev = %d\n" % (*qmesh, time_rev))
     L.append("    SelectionRule3 = %s\n" % " ".join("'%s'" % s for s in selection3))
     if sigma is not None:

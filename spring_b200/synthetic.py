@@ -242,6 +242,17 @@ def build(name: str = "rocksalt2", fc4: bool = False, seeds=(SEED_FC2, SEED_FC3,
     return cr
 
 
+def defect_fc2(cr: Crystal, site: int = 0, scale: float = 1.15):
+    """The FC2 of a cell with a substitutional defect on basis atom `site`: the pristine arrays with
+    that atom's on-site block scaled (the home-cell block PerturbationMatrix reads), as
+    (atm_num, atm_indx, fc2) in the set_fc2 layout."""
+    fc = cr.fc2.copy()
+    for n in range(int(cr.fc2_atm_num[site])):
+        if np.all(cr.fc2_atm_indx[site, n, :3] == 0) and cr.fc2_atm_indx[site, n, 3] == site + 1:
+            fc[site, n] *= scale
+    return cr.fc2_atm_num.copy(), cr.fc2_atm_indx.copy(), fc
+
+
 def make_polar(cr: Crystal, z: float = 1.986, eps: float = 3.0) -> Crystal:
     """Born charges +z (species 1) / -z (species 2) times the identity and an isotropic dielectric
     tensor: the inputs of the dipole-dipole term (``&AtmInfo`` BornZ, dielec).  The default z is

@@ -110,3 +110,31 @@ def test_cli_dipole_term_matches_api():
     np.testing.assert_allclose(lwf[:, :6], om, rtol=1e-12, atol=0)
     np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-12, atol=0)
     np.testing.assert_allclose(kap, k_api, rtol=1e-9, atol=1e-12 * np.abs(k_api).max())
+
+
+def test_cli_point_defect_matches_api():
+    """&PointDefInfo through the driver: Scatter_pd, the ScatterRate_pd text file and the linewidths
+    (0.5 x rate added) equal the API's spring_linewidth_pd on the same inputs."""
+    cr = S.build("rocksalt2")
+    N = 4
+    num, idx, fc = S.defect_fc2(cr, site=0, scale=1.2)
+    mdef = np.array([40.078, cr.mass[1]])
+    pd = dict(def_pos=[1, 0], Mass_def=[40.078], NumDef_sup=1, cell_atom=[[0, 0, 0, 1]], qMesh_pd=[5, 5, 5],
+              rho_def=1e-3)
+    with tempfile.TemporaryDirectory() as d:
+        H.write_fc(os.path.join(d, "FC2nd_MgO300.0K_F_pd.h5"), 2, num, idx, fc)
+        kap, lwf, _ = _run(cr, d, [], qmesh=(N, N, N), point_defect=pd)
+        spd = H.read_f64(os.path.join(d, "kappa_MgO300.0K.h5"), "Scatter_pd")
+        txt = np.loadtxt(os.path.join(d, "ScatterRate_pd_IBZ_MgO300.0K.txt"), comments="#")
+    ctx, info = from_crystal(cr, (N, N, N), [300.0])
+    ctx.set_point_defect((5, 5, 5), num, idx, fc, mdef, rho_def=1e-3)
+    ctx.reset_linewidths()
+    ctx.linewidth3(1, ctx.nq0, delta="tetra", want=False)
+    rate = ctx.linewidth_pd(add=True)
+    lw = ctx.get_linewidths()[0]
+    k_api = ctx.kappa_rta(info["Rxyz"])[0]
+    ctx.close()
+    np.testing.assert_allclose(spd[:, 6:], rate, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(txt[:, 6:], rate, rtol=1e-11, atol=1e-14)
+    np.testing.assert_allclose(lwf[:, 6:], lw, rtol=1e-12, atol=0)
+    np.testing.assert_allclose(kap, k_api, rtol=1e-9, atol=1e-12 * np.abs(k_api).max())

@@ -48,11 +48,14 @@ def test_kappa_file_datasets():
     mk = rng.normal(size=(nd, 9))
     with tempfile.TemporaryDirectory() as d:
         p = os.path.join(d, "kappa_X300.0K.h5")
-        assert lib.spring_h5_write_kappa(p.encode(), H._ptr(kap), nd, nq0, H._ptr(lw), H._ptr(p3), H._ptr(mk)) == 0
+        pd = rng.normal(size=(nq0, 2 * nd))
+        assert lib.spring_h5_write_kappa(p.encode(), H._ptr(kap), nd, nq0, H._ptr(lw), H._ptr(p3), H._ptr(mk),
+                                         H._ptr(pd)) == 0
         assert np.array_equal(H.read_f64(p, "ThermalConductivityTensor"), kap)
         assert np.array_equal(H.read_f64(p, "LineWidth"), lw)
         assert np.array_equal(H.read_f64(p, "PhaseSpace3rd"), p3)
         assert np.array_equal(H.read_f64(p, "ModeResolvedKappa"), mk)
+        assert np.array_equal(H.read_f64(p, "Scatter_pd"), pd)
         with pytest.raises(OSError):
             H.read_f64(p, "NoSuchDataset")
 
