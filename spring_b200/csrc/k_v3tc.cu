@@ -707,14 +707,19 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     if (warp == 0) tc::tmem_dealloc(tm, TC_COLS);
 }
 
-// One active triple whose item and records are already in registers.
+// One active triple whose item and records are already in registers.  FAST (mode records of 8
+// doubles, n_temps <= 4): the occupations come with omega and 1/omega in the same load, so an item
+// needs a single round trip to memory after its own load.
+constexpr int NT_FAST = 4;
 struct EvalIn {
     float4 v0, v1, v2;
     int4 kk;
     Q0Rec q0;
     double w1, ob1, w2, ob2;
+    double n1[NT_FAST], n2[NT_FAST];
 };
 
+template <bool FAST>
 __device__ __forceinline__ void eval_load(EvalIn& x, const TcItem* item, const Q0Rec* __restrict__ q0rec,
                                           const double* __restrict__ modes, int rs) {
     const float4* src = reinterpret_cast<const float4*>(item);
@@ -723,14 +728,27 @@ __device__ __forceinline__ void eval_load(EvalIn& x, const TcItem* item, const Q
     x.v2 = src[2];
     x.kk = reinterpret_cast<const int4*>(src)[3];
     x.q0 = q0rec[x.kk.x & 0x1fffffff];
-    const double2 a = *reinterpret_cast<const double2*>(modes + (size_t)x.kk.y * rs);
-    const double2 b = *reinterpret_cast<const double2*>(modes + (size_t)x.kk.z * rs);
+    const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)x.kk.y * rs);
+    const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)x.kk.z * rs);
+    const double2 a = pa[0], b = pb[0];
     x.w1 = a.x;
     x.ob1 = a.y;
     x.w2 = b.x;
     x.ob2 = b.y;
+    if (FAST) {
+        const double2 a1 = pa[1], a2 = pa[2], b1 = pb[1], b2 = pb[2];
+        x.n1[0] = a1.x;
+        x.n1[1] = a1.y;
+        x.n1[2] = a2.x;
+        x.n1[3] = a2.y;
+        x.n2[0] = b1.x;
+        x.n2[1] = b1.y;
+        x.n2[2] = b2.x;
+        x.n2[3] = b2.y;
+    }
 }
 
+template <bool FAST>
 __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int rs, double half_os2, double pre,
                                           double mfac, const double* __restrict__ modes, double* out_lw,
                                           double* out_p3) {
@@ -756,6 +774,16 @@ __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int 
     }
     const double W = (double)(pr * pr + pim * pim) * (x.q0.ob * x.ob2 * x.ob1) * mfac * wt;
     const double we1 = W * e1, wf2 = W * (e2 - e3);
+    if (FAST) {
+#pragma unroll
+        for (int T = 0; T < NT_FAST; ++T)
+            if (T < nT) {
+                const double n1 = x.n1[T], n2 = x.n2[T];
+                const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
+                if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
+            }
+        return;
+    }
     const double* m1 = modes + (size_t)x.kk.y * rs + 2;
     const double* m2 = modes + (size_t)x.kk.z * rs + 2;
     for (int T = 0; T < nT; ++T) {
@@ -770,7 +798,8 @@ __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int 
 // sums with atomics: P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].
 // Block (r, y) walks region r of the item list, two items per thread at a time with both items'
 // loads issued first.
-__global__ void __launch_bounds__(256, 3) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
+template <bool FAST>
+__global__ void __launch_bounds__(256, 2) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
                                                    int cap, int nq0, int nT, int rs, double half_os2, double pre,
                                                    double mfac, const Q0Rec* __restrict__ q0rec,
                                                    const double* __restrict__ modes, double* __restrict__ out_lw,
@@ -782,10 +811,10 @@ __global__ void __launch_bounds__(256, 3) k_v3tc_eval(const TcItem* __restrict__
     for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
         const int j = i + stride;
         EvalIn a, b;
-        eval_load(a, reg + i, q0rec, modes, rs);
-        if (j < n) eval_load(b, reg + j, q0rec, modes, rs);
-        eval_item(a, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
-        if (j < n) eval_item(b, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
+        eval_load<FAST>(a, reg + i, q0rec, modes, rs);
+        if (j < n) eval_load<FAST>(b, reg + j, q0rec, modes, rs);
+        eval_item<FAST>(a, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
+        if (j < n) eval_item<FAST>(b, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
     }
 }
 
@@ -1068,7 +1097,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
         // them to the region size, so the host checks them while it runs.
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
         const int gy = c->tc_eval_y > 0 ? c->tc_eval_y : (int)std::min<long long>(1024, (cap + 2 * threads - 1) / (2 * threads));
-        k_v3tc_eval<<<dim3(nreg, gy), threads, 0, c->stream>>>(
+        auto eval = (rs == 8 && c->nT <= NT_FAST) ? k_v3tc_eval<true> : k_v3tc_eval<false>;
+        eval<<<dim3(nreg, gy), threads, 0, c->stream>>>(
             items, c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2, os * ONEBYSQRT2PI,
             host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p,
             d_lw, d_p3);
