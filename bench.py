@@ -52,11 +52,14 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mesh4", type=int, default=16, help="mesh of the four-phonon leg (0 skips it)")
-    ap.add_argument("--no-fp64-4ph", action="store_true", help="skip the FP64 run of the four-phonon leg")
-    ap.add_argument("--no-surrogate", action="store_true", help="skip the surrogate-screened leg")
-    ap.add_argument("--no-batch", action="store_true", help="skip the batched multi-workload leg")
-    ap.add_argument("--no-bte", action="store_true", help="skip the iterative-kappa leg")
+    ap.add_argument("--legs", default="c2,c3,c4",
+                    help="extra legs on their own configurations: c2 iterative kappa (24^3), c3 four-phonon + "
+                         "isotope (16^3), c4 batched workloads + path points, c5 surrogate screening (12^3 -> 20^3; "
+                         "about 20 minutes, so not in the default run); 'none' for the main leg alone")
+    ap.add_argument("--mesh4", type=int, default=16, help="mesh of the four-phonon leg")
+    ap.add_argument("--c3-fp64", default="sample", choices=["sample", "full", "off"],
+                    help="FP64 comparison of the four-phonon leg: 'sample' times 8 evenly spaced q0 and "
+                         "extrapolates by quartet count (kappa error not reported), 'full' runs every q0")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"],
                     help="arithmetic of V3 on the measured path (FP64 is always timed beside it)")
     return ap.parse_args()
@@ -317,19 +320,21 @@ def _kdiag(k):
     return np.array([k[0], k[4], k[8]])
 
 
-def fourph_c3_leg(torch, mesh=16, prec4="bf16x3", fp64=True):
+def fourph_c3_leg(torch, mesh=16, prec4="bf16x3", fp64="sample"):
     """Three-phonon + four-phonon + isotope kappa of the rocksalt cell with FC4 at mesh^3, 300 K,
-    Gaussian 2 cm^-1, isotope g2 = 1e-3 on both atoms.  Timed from the phonons to kappa, once with
-    the tensor-core V3 (BF16x3) and V4 (prec4), once with the plain FP64 path (k_v3s + k_v4); the
-    line gives both times, the kappa and rate errors of the mixed path against FP64, and the
-    tensor-core V4 kernel time."""
+    Gaussian 2 cm^-1, isotope g2 = 1e-3 on both atoms.  Timed from the phonons to kappa with the
+    tensor-core V3 (BF16x3) and V4 (prec4).  The plain FP64 path (k_v3s + k_v4) beside it: 'full'
+    runs it for every q0 (times and kappa, rate and linewidth errors), 'sample' runs the FP64
+    four-phonon rates of 8 evenly spaced q0 (their errors, and the FP64 four-phonon time
+    extrapolated by quartet count), 'off' skips it."""
     from spring_b200 import synthetic as S
     from spring_b200.api import from_crystal
     cr = S.build("rocksalt2", fc4=True)
     T = [300.0]
     g2 = [1e-3, 1e-3]
     ctx, info = from_crystal(cr, (mesh,) * 3, T, with_fc4=True)
-    quartets = sum(ctx.count4(i + 1)[0] for i in range(ctx.nq0))
+    counts = np.array([ctx.count4(i + 1)[0] for i in range(ctx.nq0)], dtype=np.int64)
+    quartets = int(counts.sum())
 
     def run(p3, p4):
         def step():
@@ -343,19 +348,20 @@ def fourph_c3_leg(torch, mesh=16, prec4="bf16x3", fp64=True):
             return r4, ctx.get_linewidths(), ctx.kappa_rta(info["Rxyz"])[0]
         return _ev_ms(torch, step)
 
-    run("bf16x3", prec4)  # warm-up (allocations, tables)
+    ctx.set_precision(prec4)
+    ctx.linewidth4(1, 1, "gauss", SIGMA)  # warm-up (allocations, tables)
     ctx.set_profiling(True)
     (r4m, lwm, km), ms_m = run("bf16x3", prec4)
     v4_ms, v4_n = ctx.kernel_time("k_v4tc")
     ctx.set_profiling(False)
     out = {"mesh": [mesh] * 3, "temperature": 300.0, "isotope_g2": g2, "sigma_rad_ps": SIGMA,
-           "irreducible_q0": int(ctx.nq0), "quartets": int(quartets), "v4_arithmetic": prec4,
+           "irreducible_q0": int(ctx.nq0), "quartets": quartets, "v4_arithmetic": prec4,
            "time_to_kappa_ms": ms_m, "v4tc_kernel_ms": v4_ms, "v4tc_launches": v4_n,
            "evals_per_s_4ph": quartets * 6 ** 4 / (v4_ms * 1e-3) if v4_ms else None,
            "kappa_diag": _kdiag(km).tolist(),
            "what": "phonons + 3ph (bf16x3 V3) + isotope + 4ph (tensor-core V4) + RTA kappa, every q0; one 4ph eval = "
                    "one (s0..s3) of one quartet"}
-    if fp64:
+    if fp64 == "full":
         (r4f, lwf, kf), ms_f = run("fp64", "fp64")
         big = r4f > 1e-3 * r4f.max()
         lbig = lwf > 1e-3 * lwf.max()
@@ -364,6 +370,23 @@ def fourph_c3_leg(torch, mesh=16, prec4="bf16x3", fp64=True):
                     "linewidth_max_rel_err_vs_fp64": float((np.abs(lwm[lbig] - lwf[lbig]) / lwf[lbig]).max()),
                     "rate4_max_rel_err_vs_fp64": float((np.abs(r4m[big] - r4f[big]) / r4f[big]).max()),
                     "fp64_kappa_diag": _kdiag(kf).tolist()})
+    elif fp64 == "sample":
+        ctx.set_precision("fp64")
+        sample = list(np.linspace(0, ctx.nq0 - 1, 8).round().astype(int))
+        f_ms, err = 0.0, 0.0
+        for i in sample:
+            r, ms = _ev_ms(torch, lambda: ctx.linewidth4(int(i) + 1, 1, "gauss", SIGMA))
+            f_ms += ms
+            ref = r[0, 0]
+            big = ref > 1e-3 * ref.max()
+            if big.any():
+                err = max(err, float((np.abs(r4m[0, i][big] - ref[big]) / ref[big]).max()))
+        fp64_4ph_ms = f_ms * quartets / counts[sample].sum()
+        out.update({"fp64_4ph_ms_extrapolated": fp64_4ph_ms, "fp64_sample_q0": [int(i) + 1 for i in sample],
+                    "fp64_sample_ms": f_ms, "fp64_4ph_over_v4tc": fp64_4ph_ms / v4_ms if v4_ms else None,
+                    "rate4_max_rel_err_vs_fp64_sample": err,
+                    "fp64_note": "FP64 four-phonon time of the whole leg extrapolated from the sampled q0 by their "
+                                 "quartet counts; rate errors over the sampled q0"})
     ctx.close()
     return out
 
@@ -708,10 +731,11 @@ def run_ours(args):
             e2e_ms = float(t.item())
 
     peak = fp64_peak_tflops(torch) if rank == 0 else None
-    four = fourph_c3_leg(torch, args.mesh4, fp64=not args.no_fp64_4ph) if (rank == 0 and world == 1 and args.mesh4 > 0) else None
-    sur = surrogate_c5_leg(torch) if (rank == 0 and world == 1 and not args.no_surrogate) else None
-    batched = batched_leg(torch) if (rank == 0 and world == 1 and not args.no_batch) else None
-    bte = bte_c2_leg(torch, ctx, mesh[0]) if (rank == 0 and world == 1 and not args.no_bte) else None
+    legs = set(x.strip() for x in args.legs.split(",")) if rank == 0 and world == 1 else set()
+    four = fourph_c3_leg(torch, args.mesh4, fp64=args.c3_fp64) if "c3" in legs else None
+    sur = surrogate_c5_leg(torch) if "c5" in legs else None
+    batched = batched_leg(torch) if "c4" in legs else None
+    bte = bte_c2_leg(torch, ctx, mesh[0]) if "c2" in legs else None
     cpu = None
     oracle_check = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -328,7 +328,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->d_neg); dfree(c->d_wtr);
         dfree(c->d_bteg_row); dfree(c->d_bteg_kk); dfree(c->d_bteg_pq);
         dfree(c->ew.g); dfree(c->ew.r); dfree(c->ew.hz); dfree(c->ew.tau); dfree(c->ew.z); dfree(c->ew.cc);
-        dfree(c->ew.dd);
+        dfree(c->ew.dd); dfree(c->d_v4_rec);
         dfree(c->pd.vfc); dfree(c->pd.vm); dfree(c->pd.qpnt); dfree(c->pd.w2); dfree(c->pd.qint); dfree(c->pd.tet);
         dfree(c->pd.inc); dfree(c->pd.gamma0); dfree(c->pd.wgt); dfree(c->pd.G); dfree(c->pd.te0);
         free_phonons(c->pd.ph);

@@ -459,6 +459,7 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
     const int rblocks = std::max(1, std::min((rows + 7) / 8, 148 * 16));
     const int eblocks = std::max(1, std::min((rows + threads - 1) / threads, 148 * 8));
     auto kappa_of = [&](int T, const double* Fv, double* out9) -> int {
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure");
         k_bte_kappa<<<1, 256, 0, c->stream>>>(ntr, n, nq, c->vol, c->d_tr_grid.p, c->d_tr_deg.p, c->ph_grid.omega.p,
                                               c->ph_grid.nbe.p + (size_t)T * nq * n, c->ph_grid.vel.p, Fv, kap.p);
         SPRING_CHECK(launch_check(c, "k_bte_kappa"));
@@ -466,13 +467,15 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
     };
     for (int T = 0; rc == SPRING_OK && T < c->nT; ++T) {
         const double* nbeT = c->ph_grid.nbe.p + (size_t)T * nq * n;
-        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
         if (cnt > 0) {
+            if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
             k_bteg_coef<<<blocks_for(cnt), threads, 0, c->stream>>>(cnt, c->d_bteg_kk.p, c->d_bteg_pq.p, nbeT, cf.p);
             if ((rc = launch_check(c, "k_bteg_coef")) != SPRING_OK) break;
         }
+        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
         k_bteg_rows<0><<<rblocks, 256, 0, c->stream>>>(rows, c->d_bteg_row.p, c->d_bteg_kk.p, cf.p, nullptr, inv_tau.p);
         if ((rc = launch_check(c, "k_bteg_rows<tau>")) != SPRING_OK) break;
+        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
         k_bte_f0<<<eblocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, c->ph_grid.omega.p, c->ph_grid.vel.p,
                                                     inv_tau.p, c->temps[T], F0.p);
         if ((rc = launch_check(c, "k_bte_f0")) != SPRING_OK) break;
@@ -487,11 +490,14 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
         int iter = 0;
         for (;;) {
             ++iter;
+            if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
             k_bteg_expand<<<blocks_for((long long)nq * n), threads, 0, c->stream>>>(nq, n, c->d_tr_pos.p, c->d_tr_sgn.p,
                                                                                      F.p, Fg.p);
             if ((rc = launch_check(c, "k_bteg_expand")) != SPRING_OK) break;
+            if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
             k_bteg_rows<1><<<rblocks, 256, 0, c->stream>>>(rows, c->d_bteg_row.p, c->d_bteg_kk.p, cf.p, Fg.p, dF.p);
             if ((rc = launch_check(c, "k_bteg_rows<dF>")) != SPRING_OK) break;
+            if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "bte: injected launch failure"); break; }
             k_bte_update<<<eblocks, threads, 0, c->stream>>>(ntr, n, c->d_tr_grid.p, inv_tau.p, F0.p, dF.p, F.p);
             if ((rc = launch_check(c, "k_bte_update")) != SPRING_OK) break;
             if ((rc = kappa_of(T, F.p, knew)) != SPRING_OK) break;

@@ -108,6 +108,22 @@ __global__ void k4_grid_tabs(int nq, int na, const double* __restrict__ posr, co
     }
 }
 
+// Mode records [q][s][rs]: omega, 1/omega, then n(T) for every temperature (FP64), so that the
+// FP64 terms of a mode quad read each grid mode with one contiguous load.
+__global__ void k4_modes(int nq, int nT, int rs, const double* __restrict__ omg, const double* __restrict__ obg,
+                         const double* __restrict__ nbeg, double* __restrict__ out) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < (long long)nq * NM * rs;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long qs = i / rs;
+        const int k = (int)(i % rs);
+        double v = 0.0;
+        if (k == 0) v = omg[qs];
+        else if (k == 1) v = obg[qs];
+        else if (k - 2 < nT) v = nbeg[(size_t)(k - 2) * nq * NM + qs];
+        out[i] = v;
+    }
+}
+
 // C_mu[s0][a1][a2][a3] of one q0 (FP32 complex), a = N * 3 + b over the slots of mu's cluster
 // (slots grouped by basis atom, zero beyond na), [mu][s0][a1][a2][a3] with extent KA each.
 __global__ void k4_c0(int na, const double* __restrict__ fc4, const double2* __restrict__ ev0,
@@ -237,6 +253,7 @@ __global__ void k4_total(int nq, const int* __restrict__ toff, const int* __rest
 // ------------------------------------------------------------------ the tensor-core pass
 struct V4Args {
     int nq, nT, nq0, q0, ntiles, tiles_per_cta, H, gq0;
+    int rs;                      // doubles per mode record (omega, 1/omega, n(T)), even
     int nch;                     // chunks per tile: two for every branch s0 of the mask
     int chunk[NCHUNK];           // the chunks, in order (chunk c is s0 = c / 2, s1 = 3 (c % 2) .. + 2)
     double mfac, half_os2, pre;  // Sctr4THz2 / Nq^2; 1 / (2 sigma^2); 1 / (sigma sqrt(2 pi))
@@ -250,7 +267,7 @@ struct V4Sm {
     alignas(8) uint64_t afull, afree, bfull, bfree, tfull[2], tempty[2];
     uint32_t tslot;
     int abort;
-    double w0[NM], ob0[NM], n0[9][NM];
+    double w0[NM], ob0[NM], n0inv[9][NM];
     float w0f[NM];
     double rate[NM][9];  // this CTA's sums for q0, flushed once at the end
 };
@@ -259,8 +276,8 @@ __global__ void __launch_bounds__(V4_THREADS, 1)
 k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict__ quart,
        const __nv_bfloat16* __restrict__ img, const double2* __restrict__ ph, const float2* __restrict__ etab,
        const float* __restrict__ wf, const double* __restrict__ om0, const double* __restrict__ ob0,
-       const double* __restrict__ nbe0, const double* __restrict__ omg, const double* __restrict__ obg,
-       const double* __restrict__ nbeg, double* __restrict__ out_rate, int* __restrict__ err) {
+       const double* __restrict__ nbe0, const double* __restrict__ rec, double* __restrict__ out_rate,
+       int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     const int H = a.H;
     const size_t abytes = (size_t)H * QT * bk.ktot * 2, bbytes = (size_t)CROWS * bk.ktot * 2;
@@ -295,7 +312,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
         S.w0[i] = om0[i];
         S.w0f[i] = (float)om0[i];
         S.ob0[i] = ob0[i];
-        for (int t = 0; t < a.nT; ++t) S.n0[t][i] = nbe0[(size_t)t * a.nq0 * NM + i];
+        for (int t = 0; t < a.nT; ++t) S.n0inv[t][i] = 1.0 / nbe0[(size_t)t * a.nq0 * NM + i];
     }
     if (warp == 0) tc::tmem_alloc(tc::smem_u32(&S.tslot), TCOLS);
     tc::fence_async_smem();
@@ -547,6 +564,8 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                     // ---- screen every (s2, s3) of this (s0, s1) against the seven windows:
                     // with u = w0 - w1, v = w0 + w1, P = w2 + w3, M = w2 - w3 the terms are u - P, v - P,
                     // u + P, u + M, u - M, v - M, v + M; min(|x - y|, |x + y|) = ||x| - |y||
+                    const double* r1 = rec + ((size_t)g1 * NM + s1) * a.rs;
+                    const double2 m1 = *reinterpret_cast<const double2*>(r1);
                     const float u = S.w0f[s0] - w1f[s1], v = S.w0f[s0] + w1f[s1];
                     const float au = fabsf(u), av = fabsf(v);
 #pragma unroll
@@ -562,40 +581,43 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                                              fabsf(au - aM) < a.rf || fabsf(av - aM) < a.rf;
                             if (!any) continue;
                             const float a2 = phi[s2][y].x * phi[s2][y].x + phi[s2][y].y * phi[s2][y].y;
-                            // FP64: W, the seven terms and their occupation factors
-                            const double W0 = S.w0[s0], W1 = omg[(size_t)g1 * NM + s1];
-                            const double W2 = omg[(size_t)g2 * NM + s2], W3 = omg[(size_t)g3 * NM + s3];
-                            const double Wv = (double)a2 * S.ob0[s0] * obg[(size_t)g1 * NM + s1] *
-                                              obg[(size_t)g2 * NM + s2] * obg[(size_t)g3 * NM + s3] * a.mfac;
+                            // FP64: W and the seven terms, from the mode records (omega, 1/omega, n(T))
+                            // of q2 and q3, one load each; the q1 record was read for this s1
+                            const double* r2 = rec + ((size_t)g2 * NM + s2) * a.rs;
+                            const double* r3 = rec + ((size_t)g3 * NM + s3) * a.rs;
+                            const double2 m2 = *reinterpret_cast<const double2*>(r2);
+                            const double2 m3 = *reinterpret_cast<const double2*>(r3);
+                            const double W0 = S.w0[s0], W1 = m1.x, W2 = m2.x, W3 = m3.x;
+                            const double Wv = (double)a2 * S.ob0[s0] * m1.y * m2.y * m3.y * a.mfac;
                             const double dd[7] = {W0 - W1 - W2 - W3, W0 + W1 - W2 - W3, W0 + W2 - W1 - W3,
                                                   W0 + W3 - W1 - W2, W0 + W2 + W3 - W1, W0 + W1 + W3 - W2,
                                                   W0 + W1 + W2 - W3};
                             const int cw[7] = {c1, c2[0], c2[1], c2[2], c3[0], c3[1], c3[2]};
+                            double gm[7];
+                            bool anyg = false;
 #pragma unroll
                             for (int m = 0; m < 7; ++m) {
+                                gm[m] = 0.0;
                                 if (cw[m] == 0) continue;
                                 const double x = a.half_os2 * (dd[m] * dd[m]);
                                 if (!(x < EXP_CUT)) continue;
                                 const double wt = m == 0 ? cw[m] * ONEBYSIX : cw[m] * 0.5;
-                                const double g = (a.pre * exp(-x)) * wt * Wv;
+                                gm[m] = (a.pre * exp(-x)) * wt * Wv;
+                                anyg = true;
+                            }
+                            if (!anyg) continue;
+                            // occupation factors of the seven terms, per temperature:
+                            // n1 n2 n3, (1+n1) n2 n3, (1+n2) n1 n3, (1+n3) n1 n2, (1+n2)(1+n3) n1,
+                            // (1+n1)(1+n3) n2, (1+n1)(1+n2) n3, over n0
 #pragma unroll
-                                for (int T = 0; T < 9; ++T) {
-                                    if (T >= a.nT) break;
-                                    const double n1 = nbeg[((size_t)T * a.nq + g1) * NM + s1];
-                                    const double n2 = nbeg[((size_t)T * a.nq + g2) * NM + s2];
-                                    const double n3 = nbeg[((size_t)T * a.nq + g3) * NM + s3];
-                                    double f;
-                                    switch (m) {
-                                        case 0: f = n1 * n2 * n3; break;
-                                        case 1: f = (1.0 + n1) * n2 * n3; break;
-                                        case 2: f = (1.0 + n2) * n1 * n3; break;
-                                        case 3: f = (1.0 + n3) * n1 * n2; break;
-                                        case 4: f = (1.0 + n2) * (1.0 + n3) * n1; break;
-                                        case 5: f = (1.0 + n1) * (1.0 + n3) * n2; break;
-                                        default: f = (1.0 + n1) * (1.0 + n2) * n3; break;
-                                    }
-                                    acc[T] += g * (f / S.n0[T][s0]);
-                                }
+                            for (int T = 0; T < 9; ++T) {
+                                if (T >= a.nT) break;
+                                const double n1 = r1[2 + T], n2 = r2[2 + T], n3 = r3[2 + T];
+                                const double p1 = 1.0 + n1, p2 = 1.0 + n2, p3 = 1.0 + n3;
+                                const double f = gm[0] * (n1 * n2 * n3) + gm[1] * (p1 * n2 * n3) + gm[2] * (p2 * n1 * n3) +
+                                                 gm[3] * (p3 * n1 * n2) + gm[4] * (p2 * p3 * n1) + gm[5] * (p1 * p3 * n2) +
+                                                 gm[6] * (p1 * p2 * n3);
+                                acc[T] += f * S.n0inv[T][s0];
                             }
                         }
                     }
@@ -684,6 +706,8 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
     SPRING_CHECK(dalloc(c, c->d_v4_ntl, nq, "V4 tile counts"));
     SPRING_CHECK(dalloc(c, c->d_v4_toff, nq, "V4 tile counts"));
     SPRING_CHECK(dalloc(c, c->d_v4_stat, 2, "V4 status"));
+    const int rs = (2 + c->nT + 1) / 2 * 2;
+    SPRING_CHECK(dalloc(c, c->d_v4_rec, (size_t)nq * NM * rs, "V4 mode records"));
     SPRING_CHECK(h2d(c, c->d_v4_map.p, hmap.data(), sizeof(short) * hmap.size(), "V4 block map"));
     const int threads = 256;
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v4tc tables: injected launch failure");
@@ -691,6 +715,9 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
                    c->stream>>>(nq, c->na4, c->d_fc4_posr.p, c->d_qpnt.p, c->ph_grid.evec.p, c->d_mass_rs.p,
                                 c->ph_grid.omega.p, c->d_v4_ph.p, c->d_v4_etab.p, c->d_v4_wf.p);
     SPRING_CHECK(launch_check(c, "k4_grid_tabs"));
+    k4_modes<<<(int)std::min<long long>(((long long)nq * NM * rs + threads - 1) / threads, 148LL * 16), threads, 0,
+               c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_v4_rec.p);
+    SPRING_CHECK(launch_check(c, "k4_modes"));
     cudaFuncSetAttribute(k_v4tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     cudaFuncSetAttribute(k4_bimg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bimg_smem);
     int sms = 148;
@@ -701,6 +728,7 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
     a.nT = c->nT;
     a.nq0 = c->nq0;
     a.H = H;
+    a.rs = rs;
     a.mfac = host_constants().Sctr4THz2 / (double(nq) * double(nq));
     a.half_os2 = 0.5 * os * os;
     a.pre = os * ONEBYSQRT2PI;
@@ -759,8 +787,7 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
         k_v4tc<<<grid, V4_THREADS, smem, c->stream>>>(
             a, bk, c->d_v4_tiles.p, d_quart, reinterpret_cast<const __nv_bfloat16*>(c->d_v4_img.p), c->d_v4_ph.p,
             c->d_v4_etab.p, c->d_v4_wf.p, c->ph_irr.omega.p + (size_t)q0 * NM, c->ph_irr.oneby.p + (size_t)q0 * NM,
-            c->ph_irr.nbe.p + (size_t)q0 * NM, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, d_rate,
-            c->d_v4_stat.p + 1);
+            c->ph_irr.nbe.p + (size_t)q0 * NM, c->d_v4_rec.p, d_rate, c->d_v4_stat.p + 1);
         SPRING_CHECK(launch_check(c, H == 2 ? "k_v4tc<bf16x3>" : "k_v4tc<bf16>"));
         int st = 0;
         SPRING_CHECK(d2h(c, &st, c->d_v4_stat.p + 1, sizeof(int), "V4 status"));

@@ -202,6 +202,7 @@ struct spring_ctx {
     spring::DBuf<int> d_tr_deg;    // [ntr]
     spring::DBuf<int> d_neg;       // [q] grid index of -q
     spring::DBuf<double> d_wtr;    // cached W grids of the time-reversal set
+    spring::DBuf<double> d_v4_rec;  // V4 tensor-core mode records (omega, 1/omega, n(T))
     spring::EwaldDev ew;
     spring::PointDefectDev pd;
     std::vector<double> h_fc2;     // host copies of FC2 (the point-defect perturbation)
