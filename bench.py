@@ -139,20 +139,30 @@ class Clocks:
         self.p = None
         self.f = None
 
-    def _nvml_loop(self, nv, h):
+    def _query(self, nv, h):
         names = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
                  "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
                  "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
                  "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
         smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        return (float(sm), float(smax), sorted(k for k, v in names.items() if r & v))
+
+    def _nvml_loop(self, nv, h):
         while not self.done.is_set():
             if not self.active.wait(0.05) or self.done.is_set():
                 continue
             with self.lock:  # a query that began inside the timed region is kept, however short it is
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.rows.append((float(sm), float(smax), sorted(k for k, v in names.items() if r & v)))
+                self.rows.append(self._query(nv, h))
             time.sleep(0.002)
+
+    def sample(self):
+        """One query from the calling thread, made while the GPU runs the step just queued (a timed
+        region of a few milliseconds can fall between two of the background thread's queries)."""
+        if self.thread is not None and self.active.is_set():
+            with self.lock:
+                self.rows.append(self._query(self.nv, self.h))
 
     def start(self):
         try:
@@ -160,6 +170,7 @@ class Clocks:
             nv.nvmlInit()
             h = (nv.nvmlDeviceGetHandleByPciBusId(self.bus_id) if self.bus_id
                  else nv.nvmlDeviceGetHandleByIndex(self.index))
+            self.nv, self.h = nv, h
             import threading
             self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
             self.thread.start()
@@ -648,6 +659,8 @@ def run_ours(args):
             e0.record(stream)
             step()
             e1.record(stream)
+            if clocks:
+                clocks.sample()     # while the step's kernels run
             e1.synchronize()
             times.append(e0.elapsed_time(e1))
         torch.cuda.synchronize()
@@ -670,6 +683,14 @@ def run_ours(args):
 
     with torch.cuda.stream(stream):
         ms64, _, kt64, lw64, kap64, _ = timed("fp64")
+        # the FP64 path on the pairs that the delta-window pre-screen keeps (the same pre-screen as
+        # the tensor-core path's): the strongest FP64 baseline
+        from spring_b200 import _lib as L
+        ctx.set_option(L.SPRING_OPT_FP64_PRESCREEN, 1)
+        ms64p, _, kt64p, lw64p, _, _ = timed("fp64")
+        ctx.set_option(L.SPRING_OPT_FP64_PRESCREEN, 0)
+        big64 = lw64 > 1e-3 * lw64.max(axis=(1, 2), keepdims=True)
+        lw64p_err = float((np.abs(lw64p - lw64)[big64] / lw64[big64]).max())
         clocks = Clocks(local, pci_bus_id(torch, local))
         ms, launches, kt, lw_p, kap_p, clk = timed(args.precision, clocks)
         tc_tiles_run, tc_pairs_run = ctx.tc_stats() if args.precision != "fp64" else (0, 0)
@@ -810,6 +831,8 @@ def run_ours(args):
                            "fp64_parts": "phonons, deltas, rates and kappa",
                            "l2": "256 MiB buffer written between timed steps, outside the events"},
                 "time_to_kappa": {"ms": ms, "fp64_gpu_ms": ms64, "fp64_gpu_over_this": ms64 / ms,
+                                  "fp64_prescreened_gpu_ms": ms64p, "fp64_prescreened_over_this": ms64p / ms,
+                                  "fp64_prescreened_lw_max_rel_diff_vs_fp64": lw64p_err,
                                   "kappa_max_rel_err_vs_fp64": k_err, "linewidth_max_rel_err_vs_fp64": lw_err,
                                   "fp64_v3_kernel_ms": fp64_kernel_ms,
                                   "what": "one step = phonons + pairs + linewidths at 3 T + RTA kappa; errors over "

@@ -139,7 +139,9 @@ int spring_find_irr_q(spring_ctx* ctx, int nrot, const int* rotations, int time_
 int spring_compute_phonons(spring_ctx* ctx, const double* temps, double freq_cut);
 
 /* Load phonons computed by the host (e.g. with LAPACK zheevd) instead.
- * which = 0: the Nq grid points; which = 1: the Nq0 irreducible points.
+ * which = 0: the Nq grid points; which = 1: the Nq0 irreducible points; which = 2: the
+ * point-defect mesh (after spring_set_point_defect; evec and omega only, the rest may be NULL:
+ * ph_pd of the reference, whose rates depend on the eigenvector gauge at degenerate levels).
  * evec(2,Ndof,Ndof,n) interleaved complex Evec(row,s,q); omega(Ndof,n);
  * onebyomega(Ndof,n); nbe(Ndof,n,n_temps); grp_vel(3,Ndof,n).  temps(n_temps). */
 int spring_set_phonons(spring_ctx* ctx, int which, const double* temps, const double* evec, const double* omega,

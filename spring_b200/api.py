@@ -183,7 +183,7 @@ class Context:
         return float(lm.value), tuple(int(x) for x in g), int(nr.value), int(ng.value)
 
     def set_point_defect(self, qmesh_pd, atm_num, atm_indx, fc2, mass_def, rho_def=1e-6, mat_inv_full=True,
-                         optc_therm=True):
+                         optc_therm=True, phonons=None):
         """Point-defect scattering: the perturbed FC2 (same layout as :meth:`set_fc2`), the defect masses
         per basis atom, the defect density (A^-3) and the Green's-function mesh.  ``qmesh_pd=None``
         switches it off."""
@@ -194,6 +194,8 @@ class Context:
         self._call("spring_set_point_defect", _ptr(_c(qmesh_pd, np.int32)), na, _ptr(_c(atm_num, np.int32)),
                    _ptr(_c(atm_indx, np.int32)), _ptr(_c(fc2, np.float64)), _ptr(_c(mass_def, np.float64)),
                    float(rho_def), int(bool(mat_inv_full)), int(bool(optc_therm)))
+        if phonons is not None:   # host phonons of the defect mesh (dict with evec, omega) instead of the device's
+            self.set_phonons(2, None, phonons)
 
     def linewidth_pd(self, i0_first: int = 1, n_q0: int | None = None, add: bool = False):
         """Point-defect scattering rates (n_q0, Ndof); with add, 0.5 x rate joins LW_Allq0."""
@@ -245,6 +247,11 @@ class Context:
         self._call("spring_compute_phonons", _ptr(_c(temps, np.float64)), float(freq_cut))
 
     def set_phonons(self, which: int, temps, ph: dict):
+        """which 0: grid, 1: irreducible set, 2: the point-defect mesh (evec and omega only)."""
+        if which == 2:
+            self._call("spring_set_phonons", 2, None, _ptr(_c(ph["evec"], np.complex128)),
+                       _ptr(_c(ph["omega"], np.float64)), None, None, None)
+            return
         self._call("spring_set_phonons", int(which), _ptr(_c(temps, np.float64)), _ptr(_c(ph["evec"], np.complex128)),
                    _ptr(_c(ph["omega"], np.float64)), _ptr(_c(ph["onebyomega"], np.float64)),
                    _ptr(_c(ph["nbe"], np.float64)), _ptr(_c(ph["grp_vel"], np.float64)))

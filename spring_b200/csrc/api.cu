@@ -802,7 +802,15 @@ int spring_compute_phonons(spring_ctx* c, const double* temps, double freq_cut) 
 int spring_set_phonons(spring_ctx* c, int which, const double* temps, const double* evec, const double* omega,
                        const double* oneby, const double* nbe, const double* vel) {
     CTX_ENTER(c);
-    if (which != 0 && which != 1) return fail(c, SPRING_ERR_ARG, "which must be 0 (grid) or 1 (irreducible)");
+    if (which == 2) {  // the point-defect mesh: eigenvectors and omegas only
+        SPRING_CHECK(need(c, c->pd.on, "point defect (spring_set_point_defect)"));
+        if (!evec || !omega) return fail(c, SPRING_ERR_ARG, "phonon arrays are NULL");
+        const size_t nd = c->ndof, n = c->pd.nq;
+        SPRING_CHECK(h2d(c, c->pd.ph.evec.p, evec, sizeof(double2) * n * nd * nd, "eigenvectors"));
+        SPRING_CHECK(h2d(c, c->pd.ph.omega.p, omega, sizeof(double) * n * nd, "omega"));
+        return SPRING_OK;
+    }
+    if (which != 0 && which != 1) return fail(c, SPRING_ERR_ARG, "which must be 0 (grid), 1 (irreducible) or 2");
     if (!evec || !omega || !oneby || !nbe || !vel) return fail(c, SPRING_ERR_ARG, "phonon arrays are NULL");
     if (which == 1) SPRING_CHECK(need(c, c->irr_set, "irreducible q-points"));
     SPRING_CHECK(set_temps(c, temps));
@@ -824,8 +832,15 @@ int spring_set_phonons(spring_ctx* c, int which, const double* temps, const doub
 int spring_get_phonons(spring_ctx* c, int which, double* evec, double* omega, double* oneby, double* nbe,
                        double* vel) {
     CTX_ENTER(c);
-    if (which != 0 && which != 1) return fail(c, SPRING_ERR_ARG, "which must be 0 or 1");
-    Phonons& p = which == 0 ? c->ph_grid : c->ph_irr;
+    if (which == 2) SPRING_CHECK(need(c, c->pd.on, "point defect (spring_set_point_defect)"));
+    if (which < 0 || which > 2) return fail(c, SPRING_ERR_ARG, "which must be 0, 1 or 2");
+    Phonons& p = which == 0 ? c->ph_grid : (which == 1 ? c->ph_irr : c->pd.ph);
+    if (which == 2) {
+        const size_t nd = c->ndof, n = c->pd.nq;
+        if (evec) SPRING_CHECK(d2h(c, evec, p.evec.p, sizeof(double2) * n * nd * nd, "eigenvectors"));
+        if (omega) SPRING_CHECK(d2h(c, omega, p.omega.p, sizeof(double) * n * nd, "omega"));
+        return SPRING_OK;
+    }
     SPRING_CHECK(need(c, p.set, "phonons"));
     const size_t nd = c->ndof, n = p.n;
     if (evec) SPRING_CHECK(d2h(c, evec, p.evec.p, sizeof(double2) * n * nd * nd, "eigenvectors"));

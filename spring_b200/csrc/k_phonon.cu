@@ -110,11 +110,17 @@ __global__ void __launch_bounds__(128, 8) k_phonons(PhArgs a, PhSet SA, const in
             }
         }
         __syncthreads();
-        if (a.dd) {  // + DynEw, dDynEw/dq (LongEw)
+        if (a.dd) {  // + DynEw, dDynEw/dq (LongEw); then the lower triangle from the upper one, as zheevd('U')
             const double2* d = a.dd + (size_t)item * 4 * n * n;
             for (int i = tid; i < 4 * n * n; i += nt) {
                 double2& t = i < n * n ? A[i] : dD[i - n * n];
                 t = cadd(t, d[i]);
+            }
+            __syncthreads();
+            for (int i = tid; i < n * n; i += nt) {
+                const int r = i / n, cc = i % n;
+                if (r > cc) A[i] = conj2(A[cc * n + r]);
+                else if (r == cc) A[i].y = 0.0;
             }
         }
         for (int i = tid; i < n; i += nt) V[i * n + i] = make_double2(1.0, 0.0);
@@ -360,6 +366,13 @@ __global__ void __launch_bounds__(32) k_phonons_n6(PhArgs a, PhSet SA, const int
                 t = cadd(t, d[w]);
             }
         }
+        __syncwarp();
+        if (act && a.dd)  // the lower triangle from the upper one, as zheevd('U') reads it
+            for (int w = gl; w < 36; w += L) {
+                const int r = w / n, cc = w % n;
+                if (r > cc) S.A[w] = conj2(S.A[cc * n + r]);
+                else if (r == cc) S.A[w].y = 0.0;
+            }
         __syncwarp();
 
         // --- cyclic complex Jacobi, one group per point
