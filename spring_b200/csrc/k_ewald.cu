@@ -206,12 +206,13 @@ __device__ void ew_eval(const EwArgs& a, const double q[3], bool grad, const EwS
     __syncthreads();
 }
 
-__device__ __forceinline__ void put(const EwArgs& a, const EwSmem& S, int k, double2* out) {
+// comb[src] (src 0: D_ew, 1..3: its derivatives) into slot dst of the item's output
+__device__ __forceinline__ void put(const EwArgs& a, const EwSmem& S, int src, int dst, double2* out) {
     const int n = a.n;
     for (int e = threadIdx.x; e < a.E; e += blockDim.x) {
         int b, al, nu, mu;
         decode(e, a.nb, b, al, nu, mu);
-        out[(k * n + 3 * mu + al) * n + 3 * nu + b] = S.comb[e];
+        out[(dst * n + 3 * mu + al) * n + 3 * nu + b] = S.comb[src * a.E + e];
     }
 }
 
@@ -238,7 +239,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_ewald(EwArgs a, const double* __
         const bool gamma = fabs(q[0]) < CMP_PREC && fabs(q[1]) < CMP_PREC && fabs(q[2]) < CMP_PREC;
         if (!gamma) {
             ew_eval(a, q, true, S);
-            for (int k = 0; k < 4; ++k) put(a, S, k, out);
+            for (int k = 0; k < 4; ++k) put(a, S, k, k, out);
             __syncthreads();
             continue;
         }
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(EW_THREADS) k_ewald(EwArgs a, const double* __
             double qp[3] = {q[0], q[1], q[2]};
             qp[k] += 0.5 * h;
             ew_eval(a, qp, false, S);
-            put(a, S, 1 + k, out);
+            put(a, S, 0, 1 + k, out);
             __syncthreads();
             double qm[3] = {q[0], q[1], q[2]};
             qm[k] -= 0.5 * h;

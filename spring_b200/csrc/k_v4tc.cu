@@ -715,6 +715,7 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
                    c->stream>>>(nq, c->na4, c->d_fc4_posr.p, c->d_qpnt.p, c->ph_grid.evec.p, c->d_mass_rs.p,
                                 c->ph_grid.omega.p, c->d_v4_ph.p, c->d_v4_etab.p, c->d_v4_wf.p);
     SPRING_CHECK(launch_check(c, "k4_grid_tabs"));
+    if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v4tc tables: injected launch failure");
     k4_modes<<<(int)std::min<long long>(((long long)nq * NM * rs + threads - 1) / threads, 148LL * 16), threads, 0,
                c->stream>>>(nq, c->nT, rs, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->ph_grid.nbe.p, c->d_v4_rec.p);
     SPRING_CHECK(launch_check(c, "k4_modes"));
@@ -760,9 +761,11 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
         k4_total<<<1, 1, 0, c->stream>>>(nq, c->d_v4_toff.p, c->d_v4_ntl.p, c->d_v4_stat.p);
         SPRING_CHECK(launch_check(c, "k4_total"));
         // C of q0 and the operand images of every q1 that starts a quartet (while the count is read)
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v4tc tables: injected launch failure");
         k4_c0<<<std::min((2 * NM * KA * KA * KA + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
             c->na4, c->d_fc4.p, c->ph_irr.evec.p + (size_t)q0 * 36, c->d_mass_rs.p, c->d_v4_c.p);
         SPRING_CHECK(launch_check(c, "k4_c0"));
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v4tc tables: injected launch failure");
         k4_bimg<<<nq * NM, 256, bimg_smem, c->stream>>>(
             nq, c->na4, H, mask, bk, c->d_v4_cnt.p, c->d_v4_map.p, c->d_v4_c.p, c->d_v4_ph.p, c->d_v4_etab.p,
             c->d_fc4_btyp.p, reinterpret_cast<__nv_bfloat16*>(c->d_v4_img.p));
