@@ -501,6 +501,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
 #pragma unroll
                 for (int T = 0; T < 9; ++T) acc[T] = 0.0;
                 const uint32_t tb = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(buf * 256);
+#pragma unroll 1
                 for (int j = 0; j < 3; ++j) {
                     const int s1 = s1b + j;
                     const bool act = valid && s0 >= pol_lo0 && !(gam1 && s1 < 3);
@@ -568,57 +569,66 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                     const double2 m1 = *reinterpret_cast<const double2*>(r1);
                     const float u = S.w0f[s0] - w1f[s1], v = S.w0f[s0] + w1f[s1];
                     const float au = fabsf(u), av = fabsf(v);
+                    // FP32 screen of the 18 (s2, s3) of this thread (unrolled: registers only), then
+                    // one copy of the FP64 code for the quads inside a window (a rolled loop keeps the
+                    // kernel's code within the instruction cache)
+                    unsigned am = 0u;
+                    float a2s[NM * 3];
 #pragma unroll
-                    for (int s2 = 0; s2 < NM; ++s2) {
-                        if (gam2 && s2 < 3) continue;
+                    for (int s2 = 0; s2 < NM; ++s2)
 #pragma unroll
                         for (int y = 0; y < 3; ++y) {
-                            const int s3 = 3 * h + y;
-                            if (gam3 && s3 < 3) continue;
+                            a2s[3 * s2 + y] = phi[s2][y].x * phi[s2][y].x + phi[s2][y].y * phi[s2][y].y;
+                            if ((gam2 && s2 < 3) || (gam3 && 3 * h + y < 3)) continue;
                             const float P = w2f[s2] + w3f[y], M = w2f[s2] - w3f[y];
                             const float aM = fabsf(M);
                             const bool any = fabsf(au - fabsf(P)) < a.rf || fabsf(v - P) < a.rf ||
                                              fabsf(au - aM) < a.rf || fabsf(av - aM) < a.rf;
-                            if (!any) continue;
-                            const float a2 = phi[s2][y].x * phi[s2][y].x + phi[s2][y].y * phi[s2][y].y;
-                            // FP64: W and the seven terms, from the mode records (omega, 1/omega, n(T))
-                            // of q2 and q3, one load each; the q1 record was read for this s1
-                            const double* r2 = rec + ((size_t)g2 * NM + s2) * a.rs;
-                            const double* r3 = rec + ((size_t)g3 * NM + s3) * a.rs;
-                            const double2 m2 = *reinterpret_cast<const double2*>(r2);
-                            const double2 m3 = *reinterpret_cast<const double2*>(r3);
-                            const double W0 = S.w0[s0], W1 = m1.x, W2 = m2.x, W3 = m3.x;
-                            const double Wv = (double)a2 * S.ob0[s0] * m1.y * m2.y * m3.y * a.mfac;
-                            const double dd[7] = {W0 - W1 - W2 - W3, W0 + W1 - W2 - W3, W0 + W2 - W1 - W3,
-                                                  W0 + W3 - W1 - W2, W0 + W2 + W3 - W1, W0 + W1 + W3 - W2,
-                                                  W0 + W1 + W2 - W3};
-                            const int cw[7] = {c1, c2[0], c2[1], c2[2], c3[0], c3[1], c3[2]};
-                            double gm[7];
-                            bool anyg = false;
+                            if (any) am |= 1u << (3 * s2 + y);
+                        }
+#pragma unroll 1
+                    while (am != 0u) {
+                        const int bq = __ffs(am) - 1;
+                        am &= am - 1u;
+                        const int s2 = bq / 3, s3 = 3 * h + bq % 3;
+                        const float a2 = a2s[bq];
+                        // FP64: W and the seven terms, from the mode records (omega, 1/omega, n(T))
+                        // of q2 and q3, one load each; the q1 record was read for this s1
+                        const double* r2 = rec + ((size_t)g2 * NM + s2) * a.rs;
+                        const double* r3 = rec + ((size_t)g3 * NM + s3) * a.rs;
+                        const double2 m2 = *reinterpret_cast<const double2*>(r2);
+                        const double2 m3 = *reinterpret_cast<const double2*>(r3);
+                        const double W0 = S.w0[s0], W1 = m1.x, W2 = m2.x, W3 = m3.x;
+                        const double Wv = (double)a2 * S.ob0[s0] * m1.y * m2.y * m3.y * a.mfac;
+                        const double dd[7] = {W0 - W1 - W2 - W3, W0 + W1 - W2 - W3, W0 + W2 - W1 - W3,
+                                              W0 + W3 - W1 - W2, W0 + W2 + W3 - W1, W0 + W1 + W3 - W2,
+                                              W0 + W1 + W2 - W3};
+                        const int cw[7] = {c1, c2[0], c2[1], c2[2], c3[0], c3[1], c3[2]};
+                        double gm[7];
+                        bool anyg = false;
 #pragma unroll
-                            for (int m = 0; m < 7; ++m) {
-                                gm[m] = 0.0;
-                                if (cw[m] == 0) continue;
-                                const double x = a.half_os2 * (dd[m] * dd[m]);
-                                if (!(x < EXP_CUT)) continue;
-                                const double wt = m == 0 ? cw[m] * ONEBYSIX : cw[m] * 0.5;
-                                gm[m] = (a.pre * exp(-x)) * wt * Wv;
-                                anyg = true;
-                            }
-                            if (!anyg) continue;
-                            // occupation factors of the seven terms, per temperature:
-                            // n1 n2 n3, (1+n1) n2 n3, (1+n2) n1 n3, (1+n3) n1 n2, (1+n2)(1+n3) n1,
-                            // (1+n1)(1+n3) n2, (1+n1)(1+n2) n3, over n0
+                        for (int m = 0; m < 7; ++m) {
+                            gm[m] = 0.0;
+                            if (cw[m] == 0) continue;
+                            const double x = a.half_os2 * (dd[m] * dd[m]);
+                            if (!(x < EXP_CUT)) continue;
+                            const double wt = m == 0 ? cw[m] * ONEBYSIX : cw[m] * 0.5;
+                            gm[m] = (a.pre * exp(-x)) * wt * Wv;
+                            anyg = true;
+                        }
+                        if (!anyg) continue;
+                        // occupation factors of the seven terms, per temperature:
+                        // n1 n2 n3, (1+n1) n2 n3, (1+n2) n1 n3, (1+n3) n1 n2, (1+n2)(1+n3) n1,
+                        // (1+n1)(1+n3) n2, (1+n1)(1+n2) n3, over n0
 #pragma unroll
-                            for (int T = 0; T < 9; ++T) {
-                                if (T >= a.nT) break;
-                                const double n1 = r1[2 + T], n2 = r2[2 + T], n3 = r3[2 + T];
-                                const double p1 = 1.0 + n1, p2 = 1.0 + n2, p3 = 1.0 + n3;
-                                const double f = gm[0] * (n1 * n2 * n3) + gm[1] * (p1 * n2 * n3) + gm[2] * (p2 * n1 * n3) +
-                                                 gm[3] * (p3 * n1 * n2) + gm[4] * (p2 * p3 * n1) + gm[5] * (p1 * p3 * n2) +
-                                                 gm[6] * (p1 * p2 * n3);
-                                acc[T] += f * S.n0inv[T][s0];
-                            }
+                        for (int T = 0; T < 9; ++T) {
+                            if (T >= a.nT) break;
+                            const double n1 = r1[2 + T], n2 = r2[2 + T], n3 = r3[2 + T];
+                            const double p1 = 1.0 + n1, p2 = 1.0 + n2, p3 = 1.0 + n3;
+                            const double f = gm[0] * (n1 * n2 * n3) + gm[1] * (p1 * n2 * n3) + gm[2] * (p2 * n1 * n3) +
+                                             gm[3] * (p3 * n1 * n2) + gm[4] * (p2 * p3 * n1) + gm[5] * (p1 * p3 * n2) +
+                                             gm[6] * (p1 * p2 * n3);
+                            acc[T] += f * S.n0inv[T][s0];
                         }
                     }
                 }
