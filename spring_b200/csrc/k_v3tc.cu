@@ -331,7 +331,6 @@ struct OpStage {
 };
 struct EpStage {
     alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: tc_window_vals of the FP32 omegas
-    alignas(16) float2 e0[EPT][NMODE][NMODE];  // per pair, s0: m^-1/2 e0(mu a, s0) of the pair's q0 (FP32)
     alignas(8) float w1s[NMODE];               // omega of q1 in FP32, s1 in slot order 0 3 1 4 2 5
     int4 ent[EPT];                             // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
@@ -350,14 +349,14 @@ constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int TC_THREADS = EPI_THREADS + 96;  // warp 12: TMA copies; warp 13: MMA issue; warp 14: frequencies
 constexpr int TC_COLS = NEP * 128;
 
-// An active mode triple, written by k_v3tc for k_v3tc_eval: |Phi|^2 (FP32, Phi = sum_k e0'(k, s0)
-// Y_k formed in the epilogue), k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29, k1 = q1 * 6 + s1,
-// k2 = q2 * 6 + s2.
-struct alignas(16) TcItem {
-    float a2;
-    int k0, k1, k2;
+// An active mode triple, written by k_v3tc for k_v3tc_eval: the row (pair, s2) of Y for its s1,
+// (Re, Im) Y[mu][a] with k = mu * 3 + a, and k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29,
+// k1 = q1 * 6 + s1, k2 = q2 * 6 + s2.
+struct TcItem {
+    float yr[6], yi[6];
+    int k0, k1, k2, pad;
 };
-static_assert(sizeof(TcItem) == 16, "item");
+static_assert(sizeof(TcItem) == 64, "item");
 
 // Warp-specialised tensor-core pass.  For tile j the copy warp loads operand stage j % 2 (TMA
 // gathers of the A images, four pairs' table rows per request, hi and lo parts as separate
@@ -372,7 +371,7 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict__ tiles, const int4* __restrict__ entrec,
        const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ om0, const double* __restrict__ omg,
-       const Q0Rec* __restrict__ q0rec, TcItem* __restrict__ items, int* __restrict__ counts, int* __restrict__ err) {
+       TcItem* __restrict__ items, int* __restrict__ counts, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -525,19 +524,6 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     }
                 }
             }
-            {  // e0' of each pair's q0: lane (pw, hw) copies s0 = 3 hw .. 3 hw + 2 (48 bytes each)
-                const int q0p = __shfl_sync(0xffffffffu, entA.x, pw);
-                if (pw < ne)
-#pragma unroll
-                    for (int i = 0; i < 3; ++i) {
-                        const float4* src = reinterpret_cast<const float4*>(q0rec[(size_t)q0p * NMODE + 3 * hw + i].e0);
-                        float4* dst = reinterpret_cast<float4*>(&E.e0[pw][3 * hw + i][0]);
-                        const float4 x0 = src[0], x1 = src[1], x2 = src[2];
-                        dst[0] = x0;
-                        dst[1] = x1;
-                        dst[2] = x2;
-                    }
-            }
             tc::mbar_arrive(tc::smem_u32(&S.ready[es]));  // each lane releases its own stores
             // loads for later fills
             if (j + 1 < nt) load_w(entB, recB);
@@ -666,6 +652,9 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
             int pos = base + pre;
             base += tot;
+            tc::fence_before_sync();
+            __syncwarp();
+            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
             if (cnt > 0) {
                 const int kw = en.z == 2 ? (1 << 30) : 0;
                 const int k2 = en.y * NMODE + s2;
@@ -674,34 +663,25 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     unsigned m = (act >> (6 * sl)) & 0x3fu;
                     if (m == 0u) continue;
                     const int b = 8 * sl, k1 = q1 * NMODE + g + 3 * sl;
-                    // Y_k = (Re, Im) Y[mu][a] of this row for s1, k = mu * 3 + a
-                    const float yr[6] = {y[0][b], y[0][b + 1], y[0][b + 2], y[1][b], y[1][b + 1], y[1][b + 2]};
-                    const float yi[6] = {y[0][b + 3], y[0][b + 4], y[0][b + 5], y[1][b + 3], y[1][b + 4], y[1][b + 5]};
+                    // item (Re, Im) Y[mu][a], k = mu * 3 + a
+                    const float4 v0 = make_float4(y[0][b], y[0][b + 1], y[0][b + 2], y[1][b]);
+                    const float4 v1 = make_float4(y[1][b + 1], y[1][b + 2], y[0][b + 3], y[0][b + 4]);
+                    const float4 v2 = make_float4(y[0][b + 5], y[1][b + 3], y[1][b + 4], y[1][b + 5]);
                     do {
                         const int s0 = __ffs(m) - 1;
                         m &= m - 1u;
                         if (pos < a.cap) {
-                            // Phi = sum_k e0'(k, s0) Y_k (the same FP32 products the evaluation pass formed)
-                            const float2* c0 = E.e0[e][s0];
-                            float pr = 0.0f, pim = 0.0f;
-#pragma unroll
-                            for (int k = 0; k < 6; ++k) {
-                                const float2 cv = c0[k];
-                                pr = fmaf(cv.x, yr[k], fmaf(-cv.y, yi[k], pr));
-                                pim = fmaf(cv.x, yi[k], fmaf(cv.y, yr[k], pim));
-                            }
+                            float4* dst = reinterpret_cast<float4*>(region + pos);
+                            dst[0] = v0;
+                            dst[1] = v1;
+                            dst[2] = v2;
                             const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
-                            reinterpret_cast<int4*>(region)[pos] =
-                                make_int4(__float_as_int(pr * pr + pim * pim), k0, k1, k2);
+                            reinterpret_cast<int4*>(dst)[3] = make_int4(k0, k1, k2, 0);
                         }
                         ++pos;
                     } while (m != 0u);
                 }
             }
-            // every read of the stage (shared memory and accumulator) is done: release it
-            tc::fence_before_sync();
-            __syncwarp();
-            if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
         }
         if (lane == 0) counts[blockIdx.x * EPI_WARPS + warp] = base;
     }
@@ -732,9 +712,9 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
 // needs a single round trip to memory after its own load.
 constexpr int NT_FAST = 4;
 struct EvalIn {
-    float a2;
+    float4 v0, v1, v2;
     int4 kk;
-    double w0, ob0;
+    Q0Rec q0;
     double w1, ob1, w2, ob2;
     double n1[NT_FAST], n2[NT_FAST];
 };
@@ -742,12 +722,12 @@ struct EvalIn {
 template <bool FAST>
 __device__ __forceinline__ void eval_load(EvalIn& x, const TcItem* item, const Q0Rec* __restrict__ q0rec,
                                           const double* __restrict__ modes, int rs) {
-    const int4 raw = *reinterpret_cast<const int4*>(item);
-    x.a2 = __int_as_float(raw.x);
-    x.kk = make_int4(raw.y, raw.z, raw.w, 0);
-    const Q0Rec& r0 = q0rec[x.kk.x & 0x1fffffff];
-    x.w0 = r0.w;
-    x.ob0 = r0.ob;
+    const float4* src = reinterpret_cast<const float4*>(item);
+    x.v0 = src[0];
+    x.v1 = src[1];
+    x.v2 = src[2];
+    x.kk = reinterpret_cast<const int4*>(src)[3];
+    x.q0 = q0rec[x.kk.x & 0x1fffffff];
     const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)x.kk.y * rs);
     const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)x.kk.z * rs);
     const double2 a = pa[0], b = pb[0];
@@ -773,7 +753,7 @@ __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int 
                                           double mfac, const double* __restrict__ modes, double* out_lw,
                                           double* out_p3) {
     const int o = x.kk.x & 0x1fffffff;
-    const double w0 = x.w0, w1 = x.w1, w2 = x.w2;
+    const double w0 = x.q0.w, w1 = x.w1, w2 = x.w2;
     const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
     const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
     const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
@@ -783,7 +763,16 @@ __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int 
     const double p3 = e1 + e2 + e3;
     if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
     if ((x.kk.x >> 29) & 1) return;  // W = 0 for the Gamma acoustic modes of q0
-    const double W = (double)x.a2 * (x.ob0 * x.ob2 * x.ob1) * mfac * wt;
+    const float yr[6] = {x.v0.x, x.v0.y, x.v0.z, x.v0.w, x.v1.x, x.v1.y};
+    const float yi[6] = {x.v1.z, x.v1.w, x.v2.x, x.v2.y, x.v2.z, x.v2.w};
+    float pr = 0.0f, pim = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float2 c = x.q0.e0[k];
+        pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
+        pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
+    }
+    const double W = (double)(pr * pr + pim * pim) * (x.q0.ob * x.ob2 * x.ob1) * mfac * wt;
     const double we1 = W * e1, wf2 = W * (e2 - e3);
     if (FAST) {
 #pragma unroll
@@ -804,7 +793,7 @@ __device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int 
     }
 }
 
-// FP64 part of the active triples: W = wt mfac |Phi|^2 /
+// FP64 part of the active triples: Phi = sum_k e0'(k, s0) Y_k (FP32), W = wt mfac |Phi|^2 /
 // (omega0 omega1 omega2), the three Gaussian delta weights, then the phase-space and linewidth
 // sums with atomics: P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].
 // Block (r, y) walks region r of the item list, two items per thread at a time with both items'
@@ -864,9 +853,8 @@ int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
     cudaFuncSetAttribute(k_v3tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
     k_v3tc<SPLIT><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
-        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p,
-        c->ph_grid.omega.p, reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), items, c->d_tc_cnt_cta.p,
-        c->d_tc_cnt_cta.p + c->tc_grid * EPI_WARPS);
+        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p, c->ph_grid.omega.p, items,
+        c->d_tc_cnt_cta.p, c->d_tc_cnt_cta.p + c->tc_grid * EPI_WARPS);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
