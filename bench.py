@@ -18,6 +18,13 @@ step; the three temperatures reuse the same V3).
 --impl reference times the CPU restatement of the reference (the oracle; the
 Fortran reference cannot be built on this image) on a bounded sample of the
 same workload, with all host threads.
+
+Extra legs on the other configurations (--legs, default c2,c3,c4): c2 iterative
+kappa at 24^3 (T = 100/300/700 K, tolerance 1e-6); c3 three- plus four-phonon
+plus isotope kappa at 16^3 with the tensor-core V4 (FP64 four-phonon time from
+sampled q0 unless --c3-fp64 full); c4 the batched uneven workload and 200 path
+points; c5 the surrogate-screened four-phonon run (trained at 12^3, screened at
+20^3, T = 300 and 900 K).  Each reports its own times and errors in the line.
 """
 from __future__ import annotations
 
