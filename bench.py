@@ -19,7 +19,7 @@ step; the three temperatures reuse the same V3).
 Fortran reference cannot be built on this image) on a bounded sample of the
 same workload, with all host threads.
 
-Extra legs on the other configurations (--legs, default c2,c3,c4): c2 iterative
+Extra legs on the other configurations (--legs, default all four): c2 iterative
 kappa at 24^3 (T = 100/300/700 K, tolerance 1e-6); c3 three- plus four-phonon
 plus isotope kappa at 16^3 with the tensor-core V4 (FP64 four-phonon time from
 sampled q0 unless --c3-fp64 full); c4 the batched uneven workload and 200 path
@@ -59,10 +59,10 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mesh", type=int, default=MESH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--legs", default="c2,c3,c4",
+    ap.add_argument("--legs", default="c2,c3,c4,c5",
                     help="extra legs on their own configurations: c2 iterative kappa (24^3), c3 four-phonon + "
-                         "isotope (16^3), c4 batched workloads + path points, c5 surrogate screening (12^3 -> 20^3; "
-                         "about 20 minutes, so not in the default run); 'none' for the main leg alone")
+                         "isotope (16^3), c4 batched workloads + path points, c5 surrogate screening (12^3 -> 20^3); "
+                         "'none' for the main leg alone (all four take about two minutes on one B200)")
     ap.add_argument("--mesh4", type=int, default=16, help="mesh of the four-phonon leg")
     ap.add_argument("--c3-fp64", default="sample", choices=["sample", "full", "off"],
                     help="FP64 comparison of the four-phonon leg: 'sample' times 8 evenly spaced q0 and "
