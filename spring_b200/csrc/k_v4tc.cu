@@ -428,6 +428,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                     const uint32_t sbo = (uint32_t)(bk.kpad[b] / 8) * 128u;
                     __nv_bfloat16* Ah = reinterpret_cast<__nv_bfloat16*>(sA) + QT * bk.koff[b];
                     __nv_bfloat16* Al = Ah + QT * bk.ktot;
+#pragma unroll 4
                     for (int j = 0; j < bk.kb[b]; ++j) {
                         const int e = bk.klist[b][j];
                         const int mu = e >> 8, N2 = (e >> 4) & 15, N3 = e & 15;
@@ -445,6 +446,7 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                         if (H == 2) Al[oim] = ll;
                     }
                 }
+#pragma unroll 6
                 for (int j = 0; j < 36; ++j) myE2[j] = etab[(size_t)g2 * 36 + j];
             }
             tc::fence_async_smem();
@@ -598,6 +600,16 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                         const double* r3 = rec + ((size_t)g3 * NM + s3) * a.rs;
                         const double2 m2 = *reinterpret_cast<const double2*>(r2);
                         const double2 m3 = *reinterpret_cast<const double2*>(r3);
+                        // occupations of up to four temperatures, loaded with the records (rs >= 6)
+                        double2 n2a = make_double2(0.0, 0.0), n2b = n2a, n3a = n2a, n3b = n2a;
+                        if (a.nT <= 4) {
+                            n2a = *reinterpret_cast<const double2*>(r2 + 2);
+                            n3a = *reinterpret_cast<const double2*>(r3 + 2);
+                            if (a.nT > 2) {
+                                n2b = *reinterpret_cast<const double2*>(r2 + 4);
+                                n3b = *reinterpret_cast<const double2*>(r3 + 4);
+                            }
+                        }
                         const double W0 = S.w0[s0], W1 = m1.x, W2 = m2.x, W3 = m3.x;
                         const double Wv = (double)a2 * S.ob0[s0] * m1.y * m2.y * m3.y * a.mfac;
                         const double dd[7] = {W0 - W1 - W2 - W3, W0 + W1 - W2 - W3, W0 + W2 - W1 - W3,
@@ -623,7 +635,15 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
 #pragma unroll
                         for (int T = 0; T < 9; ++T) {
                             if (T >= a.nT) break;
-                            const double n1 = r1[2 + T], n2 = r2[2 + T], n3 = r3[2 + T];
+                            double n2, n3;
+                            if (a.nT <= 4 && T < 4) {
+                                n2 = T == 0 ? n2a.x : T == 1 ? n2a.y : T == 2 ? n2b.x : n2b.y;
+                                n3 = T == 0 ? n3a.x : T == 1 ? n3a.y : T == 2 ? n3b.x : n3b.y;
+                            } else {
+                                n2 = r2[2 + T];
+                                n3 = r3[2 + T];
+                            }
+                            const double n1 = r1[2 + T];
                             const double p1 = 1.0 + n1, p2 = 1.0 + n2, p3 = 1.0 + n3;
                             const double f = gm[0] * (n1 * n2 * n3) + gm[1] * (p1 * n2 * n3) + gm[2] * (p2 * n1 * n3) +
                                              gm[3] * (p3 * n1 * n2) + gm[4] * (p2 * p3 * n1) + gm[5] * (p1 * p3 * n2) +
