@@ -143,56 +143,59 @@ __global__ void __launch_bounds__(128) k_tc_tab_b(int nq, int na, const double* 
     __shared__ double2 sU[24 * NMODE];                   // [N b][s]
     __shared__ __align__(16) __nv_bfloat16 img[2][BIMG];  // hi, lo images of this (q1, mu), built here
     __shared__ double2 ph[8];
-    __shared__ double sF[8 * 8 * 27];  // FC3 of mu
-    const int q = blockIdx.x / 2, mu = blockIdx.x % 2;
+    __shared__ double sF[8 * 8 * 27];  // FC3 of mu, staged once: the CTA loops over grid points
+    const int mu = blockIdx.x % 2;
     const int KR = 3 * na;
-    q_phases(q, mu, na, posr, qpnt, ph);
     for (int i = threadIdx.x; i < na * na * 27; i += blockDim.x) sF[i] = fc3[(size_t)mu * na * na * 27 + i];
-    __syncthreads();
-    for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
-        sU[i] = u_value(ph, q, mu, i / NMODE, i % NMODE, na, btyp, mrs, evg);
-    for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // padding rows and K stay zero
-        reinterpret_cast<uint4*>(&img[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
-    __syncthreads();
-    // Z[(a, s1)][(N2, c)] = sum_{N1, b} FC3[mu][N1][N2][a b c] U[N1 b][s1]: one thread per
-    // (a, N2, c, s1 half), each FC3 value (staged in shared memory) used for three s1.
-    for (int i = threadIdx.x; i < 3 * KR * 2; i += blockDim.x) {
-        const int half = i % 2, t = i / 2, al = t / KR, k2 = t % KR;  // k2 = N2*3 + c
-        const int N2 = k2 / 3, ga = k2 % 3;
-        double zr[3] = {0.0, 0.0, 0.0}, zi[3] = {0.0, 0.0, 0.0};
-        for (int N1 = 0; N1 < na; ++N1) {  // k1 = N1*3 + b in order
-            const double* f = sF + (N1 * na + N2) * 27 + al * 9 + ga;
-            const double2* u1 = sU + N1 * 3 * NMODE + half * 3;
+    for (int q = blockIdx.x / 2; q < nq; q += gridDim.x / 2) {
+        __syncthreads();  // the previous point's image has been written out
+        q_phases(q, mu, na, posr, qpnt, ph);
+        for (int i = threadIdx.x; i < (int)(sizeof(img) / 16); i += blockDim.x)  // padding rows and K stay zero
+            reinterpret_cast<uint4*>(&img[0][0])[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncthreads();
+        for (int i = threadIdx.x; i < KR * NMODE; i += blockDim.x)
+            sU[i] = u_value(ph, q, mu, i / NMODE, i % NMODE, na, btyp, mrs, evg);
+        __syncthreads();
+        // Z[(a, s1)][(N2, c)] = sum_{N1, b} FC3[mu][N1][N2][a b c] U[N1 b][s1]: one thread per
+        // (a, N2, c, s1 half), each FC3 value (staged in shared memory) used for three s1.
+        for (int i = threadIdx.x; i < 3 * KR * 2; i += blockDim.x) {
+            const int half = i % 2, t = i / 2, al = t / KR, k2 = t % KR;  // k2 = N2*3 + c
+            const int N2 = k2 / 3, ga = k2 % 3;
+            double zr[3] = {0.0, 0.0, 0.0}, zi[3] = {0.0, 0.0, 0.0};
+            for (int N1 = 0; N1 < na; ++N1) {  // k1 = N1*3 + b in order
+                const double* f = sF + (N1 * na + N2) * 27 + al * 9 + ga;
+                const double2* u1 = sU + N1 * 3 * NMODE + half * 3;
 #pragma unroll
-            for (int be = 0; be < 3; ++be) {
-                const double fv = f[be * 3];
+                for (int be = 0; be < 3; ++be) {
+                    const double fv = f[be * 3];
 #pragma unroll
-                for (int j = 0; j < 3; ++j) {
-                    const double2 u = u1[be * NMODE + j];
-                    zr[j] = fma(fv, u.x, zr[j]);
-                    zi[j] = fma(fv, u.y, zi[j]);
+                    for (int j = 0; j < 3; ++j) {
+                        const double2 u = u1[be * NMODE + j];
+                        zr[j] = fma(fv, u.x, zr[j]);
+                        zi[j] = fma(fv, u.y, zi[j]);
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            const int r = 8 * b_slot(half * 3 + j) + al, ri = r + 3;  // Re and Im output rows of (a, s1)
-            __nv_bfloat16 h, l;
-            // row r (Re output): [Re Z | -Im Z];  row ri (Im output): [Im Z | Re Z]
-            split_bf16(zr[j], h, l);
-            img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
-            img[0][bimg(ri, KR + k2)] = h;         img[1][bimg(ri, KR + k2)] = l;
-            split_bf16(-zi[j], h, l);
-            img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
-            split_bf16(zi[j], h, l);
-            img[0][bimg(ri, k2)] = h;              img[1][bimg(ri, k2)] = l;
+            for (int j = 0; j < 3; ++j) {
+                const int r = 8 * b_slot(half * 3 + j) + al, ri = r + 3;  // Re and Im output rows of (a, s1)
+                __nv_bfloat16 h, l;
+                // row r (Re output): [Re Z | -Im Z];  row ri (Im output): [Im Z | Re Z]
+                split_bf16(zr[j], h, l);
+                img[0][bimg(r, k2)] = h;               img[1][bimg(r, k2)] = l;
+                img[0][bimg(ri, KR + k2)] = h;         img[1][bimg(ri, KR + k2)] = l;
+                split_bf16(-zi[j], h, l);
+                img[0][bimg(r, KR + k2)] = h;          img[1][bimg(r, KR + k2)] = l;
+                split_bf16(zi[j], h, l);
+                img[0][bimg(ri, k2)] = h;              img[1][bimg(ri, k2)] = l;
+            }
         }
+        __syncthreads();
+        constexpr int V = BIMG * 2 / 16;  // 16-byte vectors per image
+        uint4* out = reinterpret_cast<uint4*>(tab + (size_t)q * 4 * BIMG + mu * BIMG);
+        for (int i = threadIdx.x; i < 2 * V; i += blockDim.x)
+            out[(i / V) * 2 * V + i % V] = reinterpret_cast<const uint4*>(&img[0][0])[i];
     }
-    __syncthreads();
-    constexpr int V = BIMG * 2 / 16;  // 16-byte vectors per image
-    uint4* out = reinterpret_cast<uint4*>(tab + (size_t)q * 4 * BIMG + mu * BIMG);
-    for (int i = threadIdx.x; i < 2 * V; i += blockDim.x)
-        out[(i / V) * 2 * V + i % V] = reinterpret_cast<const uint4*>(&img[0][0])[i];
 }
 
 // q0 mode records, 64 bytes per (q0, s0): e0' = m_mu^-1/2 e0(mu a, s0) as float2[6], omega0, 1/omega0.
@@ -1022,7 +1025,7 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
                                                    reinterpret_cast<__nv_bfloat16*>(c->d_tc_a.p));
         SPRING_CHECK(launch_check(c, "k_tc_tab_a"));
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-        k_tc_tab_b<<<nq * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
+        k_tc_tab_b<<<std::min(nq, 148 * 6) * 2, 128, 0, c->stream>>>(nq, c->na3, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
                                                    c->d_qpnt.p, c->ph_grid.evec.p,
                                                    reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
         SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
