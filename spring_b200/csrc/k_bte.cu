@@ -332,28 +332,17 @@ __global__ void __launch_bounds__(256) k_bteg_rows(int rows, const int* __restri
     const int lane = threadIdx.x & 31;
     for (int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += (gridDim.x * blockDim.x) >> 5) {
         double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-        const int beg = rowoff[r], end = rowoff[r + 1];
-        if (MODE == 0) {
-            for (int i = beg + lane; i < end; i += 32) a0 += cf[i];
-        } else {
-            // four entries per lane in flight: their (k1, k2) and coefficients first, then the gathers of F
-            for (int i = beg + lane; i < end; i += 128) {
-                int2 k[4];
-                double c[4];
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int j = i + 32 * u;
-                    k[u] = j < end ? kk[j] : make_int2(0, 0);
-                    c[u] = j < end ? cf[j] : 0.0;
-                }
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const double* f1 = Fg + 3 * (size_t)k[u].x;
-                    const double* f2 = Fg + 3 * (size_t)k[u].y;
-                    a0 -= c[u] * (f1[0] + f2[0]);
-                    a1 -= c[u] * (f1[1] + f2[1]);
-                    a2 -= c[u] * (f1[2] + f2[2]);
-                }
+        for (int i = rowoff[r] + lane; i < rowoff[r + 1]; i += 32) {
+            const double c = cf[i];
+            if (MODE == 0) {
+                a0 += c;
+            } else {
+                const int2 k = kk[i];
+                const double* f1 = Fg + 3 * (size_t)k.x;
+                const double* f2 = Fg + 3 * (size_t)k.y;
+                a0 -= c * (f1[0] + f2[0]);
+                a1 -= c * (f1[1] + f2[1]);
+                a2 -= c * (f1[2] + f2[2]);
             }
         }
         a0 = tet::warp_sum(a0);

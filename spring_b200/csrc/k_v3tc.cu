@@ -18,15 +18,15 @@
 // into hi + lo BF16 parts and accumulates hi*hi + hi*lo + lo*hi (compensated).
 // Frequencies, occupations, the delta weights and every sum stay FP64.  Pairs with
 // no mode triple inside the delta window are dropped before the tiles are cut
-// (k_tc_keys, about half of them).  Two
-// passes: k_v3tc computes Y on the tensor cores and screens each mode triple in
-// FP32 against the window where a delta weight can exceed exp(-40) of its peak
-// (4e-18), writing the ~1-2 % inside it (with their Y values) to an item list;
-// k_v3tc_eval forms Phi, W and the FP64 delta weights of those and accumulates
-// the phase space and the linewidths.
+// (k_tc_keys, about half of them).  One pass: k_v3tc computes Y on the tensor
+// cores and screens each mode triple in FP32 against the window where a delta
+// weight can exceed exp(-40) of its peak (4e-18); for the ~1-3 % inside it the
+// epilogue warp forms |Phi|^2 (FP32), stages it in shared memory and, 32 at a
+// time, evaluates W, the FP64 delta weights and the phase-space and linewidth
+// sums.
 // Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass);
-// in practice the per-tile pipeline (TMA requests, FP32 screening issue) and, for
-// k_v3tc_eval, L2 latency of the scattered per-item loads.
+// in practice the per-tile pipeline (TMA requests, FP32 screening issue) and the
+// L2 latency of the mode records read by the staged evaluations.
 #include <algorithm>
 #include <vector>
 #include <cub/cub.cuh>
@@ -316,9 +316,9 @@ __global__ void k_tc_entrec(int n, int nq, const int* __restrict__ entries, cons
 
 // ------------------------------------------------------------------ main kernels
 struct TcArgs {
-    int nq, nq0, nT, ntiles, tiles_per_cta, cap;
+    int nq, nq0, nT, ntiles, tiles_per_cta, rs;
     int lo[3], hi[3];
-    double half_os2;
+    double half_os2, pre, mfac;
     float rf;             // delta window of the FP32 screen (tc_window)
     long long max_spins;  // poll limit of every wait of one warp on another (the pipeline waits)
 };
@@ -327,54 +327,116 @@ constexpr int NOP = 2;  // operand stages (A and B images; free once the tile's 
 constexpr int NEP = 4;  // epilogue stages (frequencies and one 128-column accumulator each)
 static_assert(NOP <= NEP, "a fill of ready[j % NEP] must follow the completion of its previous phase");
 
+// An active mode triple, staged in shared memory by the epilogue warp that found it: |Phi|^2 in
+// FP32, k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29, k1 = q1 * 6 + s1, k2 = q2 * 6 + s2.
+struct TcStage {
+    float phi2;
+    int k0, k1, k2;
+};
+constexpr int STG_CAP = 128;  // staged triples per epilogue warp: 32 + up to 96 from one chunk
+
 struct OpStage {
     alignas(128) uint8_t A[2][EPT * 1536];    // [hi, lo]: per pair its two mu images (pair stride 1536)
     alignas(128) uint8_t B[2 * 2 * B_BYTES];  // [hi, lo][mu]: rows (re/im, a, s1)
     int q1;                                   // q1 whose B images are resident
 };
 struct EpStage {
+    alignas(128) Q0Rec q0r[EPT][NMODE];        // per pair its six q0 records (bulk copies)
     alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: tc_window_vals of the FP32 omegas
     alignas(8) float w1s[NMODE];               // omega of q1 in FP32, s1 in slot order 0 3 1 4 2 5
     int4 ent[EPT];                             // (q0, q2, weight, q0 is Gamma)
     int q1, ne;
 };
+constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s1 each
 struct TcSmem {
     OpStage op[NOP];
     EpStage ep[NEP];
+    alignas(16) TcStage stg[EPI_WARPS][STG_CAP];
     alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP];
     uint32_t tslot;
     int abort;  // set by any warp whose pipeline wait ran out
     int fdone;  // tiles the frequency warp arrived on ready for (written when it leaves its loop)
 };
+static_assert(sizeof(TcSmem) <= 227 * 1024, "tensor-core V3 shared memory");
 
-constexpr int EPI_WARPS = 12;      // warps 0-11: epilogue; warps w, w+4, w+8 share TMEM lanes, two s1 each
 constexpr int EPI_THREADS = EPI_WARPS * 32;
 constexpr int TC_THREADS = EPI_THREADS + 96;  // warp 12: TMA copies; warp 13: MMA issue; warp 14: frequencies
 constexpr int TC_COLS = NEP * 128;
+constexpr int NT_FAST = 4;  // mode records of 8 doubles carry the occupations of up to 4 temperatures
 
-// An active mode triple, written by k_v3tc for k_v3tc_eval: the row (pair, s2) of Y for its s1,
-// (Re, Im) Y[mu][a] with k = mu * 3 + a, and k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29,
-// k1 = q1 * 6 + s1, k2 = q2 * 6 + s2.
-struct TcItem {
-    float yr[6], yi[6];
-    int k0, k1, k2, pad;
-};
-static_assert(sizeof(TcItem) == 64, "item");
+// FP64 part of n <= 32 staged triples, one per lane: W = wt mfac |Phi|^2 / (omega0 omega1 omega2),
+// the three Gaussian delta weights, then the phase-space and linewidth sums with atomics:
+// P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].  The q0 record
+// (omega, 1/omega) and the mode records (omega, 1/omega, nBE[T]) of q1 and q2 are read whole, so
+// a triple needs one memory round trip.  FAST: records of 8 doubles, n_temps <= 4.
+template <bool FAST>
+__device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
+                                      double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
+                                      double* out_lw, double* out_p3) {
+    const int lane = threadIdx.x & 31;
+    if (lane < n) {
+        const TcStage s = st[lane];
+        const int o = s.k0 & 0x1fffffff;
+        const double2 r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
+        const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
+        const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
+        const double2 a = pa[0], b = pb[0];
+        double2 a1 = make_double2(0.0, 0.0), a2 = a1, b1 = a1, b2 = a1;
+        if (FAST) {
+            a1 = pa[1];
+            a2 = pa[2];
+            b1 = pb[1];
+            b2 = pb[2];
+        }
+        const double w0 = r0.x, w1 = a.x, w2 = b.x;
+        const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
+        const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
+        const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
+        const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
+        const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
+        const double wt = (s.k0 >> 30) & 1 ? 2.0 : 1.0;
+        const double p3 = e1 + e2 + e3;
+        if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
+        if (!((s.k0 >> 29) & 1)) {  // W = 0 for the Gamma acoustic modes of q0
+            const double W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac * wt;
+            const double we1 = W * e1, wf2 = W * (e2 - e3);
+            if (FAST) {
+                const double n1[NT_FAST] = {a1.x, a1.y, a2.x, a2.y}, n2[NT_FAST] = {b1.x, b1.y, b2.x, b2.y};
+#pragma unroll
+                for (int T = 0; T < NT_FAST; ++T)
+                    if (T < nT) {
+                        const double v = ((n1[T] + n2[T] + 1.0) * we1) + ((n1[T] - n2[T]) * wf2);
+                        if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
+                    }
+            } else {
+                const double* m1 = modes + (size_t)s.k1 * rs + 2;
+                const double* m2 = modes + (size_t)s.k2 * rs + 2;
+                for (int T = 0; T < nT; ++T) {
+                    const double v = ((m1[T] + m2[T] + 1.0) * we1) + ((m1[T] - m2[T]) * wf2);
+                    if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
+                }
+            }
+        }
+    }
+    __syncwarp();  // every lane has read its entry before the warp stages new ones over it
+}
 
 // Warp-specialised tensor-core pass.  For tile j the copy warp loads operand stage j % 2 (TMA
 // gathers of the A images, four pairs' table rows per request, hi and lo parts as separate
 // requests; one bulk copy of the B images when q1 changed) and the frequency warp epilogue stage
-// j % 4 (entry records and the tile's omegas, plain loads issued one tile ahead); both complete on
-// ready[j % 4].  The MMA warp issues tile j's MMAs into the accumulator of epilogue stage j % 4 and
-// commits them to full[j % 4] and opfree[j % 2].  Each epilogue warp works on its own: it reads its
-// 32 accumulator rows, screens its 12 mode triples per row in FP32 against the delta window,
-// releases the stage, and appends the active triples (with their Y values) to its own region of
-// the item list.  The FP64 part runs in k_v3tc_eval.
-template <bool SPLIT>
+// j % 4 (entry records and the tile's omegas, plain loads issued one tile ahead; the pairs' q0
+// records as bulk copies); both complete on ready[j % 4].  The MMA warp issues tile j's MMAs into
+// the accumulator of epilogue stage j % 4 and commits them to full[j % 4] and opfree[j % 2].  Each
+// epilogue warp works on its own: it reads its 32 accumulator rows, screens its 12 mode triples per
+// row in FP32 against the delta window, forms |Phi|^2 of the active ones (about 1-3 %) from the
+// stage's q0 records, stages them in its shared-memory buffer, releases the stage, and evaluates
+// the FP64 delta weights and sums of the staged triples 32 at a time, one per lane (tc_drain).
+template <bool SPLIT, bool FAST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict__ tiles, const int4* __restrict__ entrec,
        const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ om0, const double* __restrict__ omg,
-       TcItem* __restrict__ items, int* __restrict__ counts, int* __restrict__ err) {
+       const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes, double* __restrict__ out_lw,
+       double* __restrict__ out_p3, int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -459,10 +521,12 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     } else if (warp == EPI_WARPS + 2) {
         // ------------------------------------------------------------ frequency warp
         // Epilogue stage j % 4 for tile j, after the epilogue of tile j-4 released it: entry
-        // records, the q1 omegas and, per pair, s2 and s0, the window values (w0 - w2, w0 + w2)
-        // of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16) .. 3 (l / 16) + 2 from
-        // omegas loaded during the fill of tile j-1; no warp barrier follows a load: each lane
-        // arrives on ready itself, after its own stores and before it issues new loads.
+        // records, the pairs' q0 records (lane l < 16 copies pair l's six, 384 bytes, adding its
+        // bytes to ready first), the q1 omegas and, per pair, s2 and s0, the window values
+        // (w0 - w2, w0 + w2) of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16)
+        // .. 3 (l / 16) + 2 from omegas loaded during the fill of tile j-1; no warp barrier follows
+        // a load: each lane arrives on ready itself, after its own stores and before it issues new
+        // loads.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
@@ -505,6 +569,11 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             }
             EpStage& E = S.ep[es];
             const int q1 = recA.x, ne = recA.z;
+            const uint32_t rb = tc::smem_u32(&S.ready[es]);
+            if (lane < ne) {
+                tc::mbar_expect_tx(rb, (uint32_t)sizeof(E.q0r[0]));
+                tc::bulk_g2s(tc::smem_u32(&E.q0r[lane][0]), q0rec + (size_t)entA.x * NMODE, (uint32_t)sizeof(E.q0r[0]), rb);
+            }
             if (lane == 0) {
                 E.ne = ne;
                 E.q1 = q1;
@@ -527,7 +596,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     }
                 }
             }
-            tc::mbar_arrive(tc::smem_u32(&S.ready[es]));  // each lane releases its own stores
+            tc::mbar_arrive(rb);  // each lane releases its own stores
             // loads for later fills
             if (j + 1 < nt) load_w(entB, recB);
             const int4 entC = (j + 2 < nt && lane < recC.z) ? entrec[recC.y + lane] : z4;
@@ -590,9 +659,8 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         // per warp keeps the active triples even across the three warps of a lane quarter.
         const int wq = warp & 3, g = warp >> 2;
         const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
-        // this warp's region of the item list and its fill
-        TcItem* region = items + ((size_t)blockIdx.x * EPI_WARPS + warp) * a.cap;
-        int base = 0;
+        TcStage* stg = S.stg[warp];
+        int count = 0;  // staged triples (warp-uniform); fewer than 32 between tiles
         // slots allowed by the mode ranges, and by the Gamma acoustic rule when q1 = Gamma (amask_g:
         // s1 = g < 3 drops out)
         unsigned amask_n = 0u;
@@ -604,6 +672,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 if (s1 >= a.lo[1] && s1 <= a.hi[1] && s0 >= a.lo[0] && s0 <= a.hi[0]) amask_n |= 1u << (6 * sl + s0);
         }
         const unsigned amask_g = amask_n & ~0x3fu;
+        const unsigned lt = (1u << lane) - 1u;
         for (int j = 0; j < nt; ++j) {
             const int es = j % NEP, u = j / NEP;
             const EpStage& E = S.ep[es];
@@ -641,184 +710,82 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 }
                 act &= amask;
             }
-            // Positions in this warp's region (exclusive prefix of the lanes' counts), release the
-            // stage (every read of it is done), then each lane writes its own active triples.
-            // counts are at most 12: four bit-plane ballots give the exclusive prefix and the total
-            const int cnt = __popc(act);
-            const unsigned lt = (1u << lane) - 1u;
-            int pre = 0, tot = 0;
+            // Stage the active triples in four chunks (s1 slot, s0 half; at most 3 per lane, 96 per
+            // warp): positions from two bit-plane ballots, |Phi|^2 = |sum_k e0'(k, s0) Y_k|^2 in FP32
+            // from the stage's q0 record of the lane's pair.  A chunk that would not fit first
+            // evaluates full rounds (rare: fewer than 32 are left between tiles).
+            const int kw = en.z == 2 ? (1 << 30) : 0;
+            const int k0b = en.x * NMODE, k2 = en.y * NMODE + s2;
+            const bool g0 = en.w != 0;
+            const Q0Rec* qr = E.q0r[e];
 #pragma unroll
-            for (int bp = 0; bp < 4; ++bp) {
-                const unsigned bal = __ballot_sync(0xffffffffu, (cnt >> bp) & 1);
-                pre += __popc(bal & lt) << bp;
-                tot += __popc(bal) << bp;
+            for (int c = 0; c < 4; ++c) {
+                const int sl = c >> 1;
+                unsigned m = (act >> (3 * c)) & 7u;
+                const int cm = __popc(m);
+                const unsigned b0 = __ballot_sync(0xffffffffu, cm & 1), b1 = __ballot_sync(0xffffffffu, cm & 2);
+                const int tot = __popc(b0) + 2 * __popc(b1);
+                if (tot == 0) continue;
+                while (count + tot > STG_CAP) {
+                    count -= 32;
+                    tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
+                                   out_p3);
+                }
+                int pos = count + __popc(b0 & lt) + 2 * __popc(b1 & lt);
+                count += tot;
+                while (m != 0u) {
+                    const int s0 = 3 * (c & 1) + __ffs(m) - 1;  // bit 3 c + t of act is s0 = 3 (c & 1) + t
+                    m &= m - 1u;
+                    const float2* c0 = qr[s0].e0;
+                    float pr = 0.0f, pim = 0.0f;
+#pragma unroll
+                    for (int k = 0; k < NMODE; ++k) {
+                        const float yr = y[k / 3][8 * sl + k % 3], yi = y[k / 3][8 * sl + 3 + k % 3];
+                        const float2 cv = c0[k];
+                        pr = fmaf(cv.x, yr, fmaf(-cv.y, yi, pr));
+                        pim = fmaf(cv.x, yi, fmaf(cv.y, yr, pim));
+                    }
+                    const int k0 = (k0b + s0) | kw | (g0 && s0 < 3 ? (1 << 29) : 0);
+                    stg[pos++] = TcStage{pr * pr + pim * pim, k0, q1 * NMODE + g + 3 * sl, k2};
+                }
+                __syncwarp();
             }
-            int pos = base + pre;
-            base += tot;
+            // every read of the stage is done: release it, then evaluate full rounds
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
-            if (cnt > 0) {
-                const int kw = en.z == 2 ? (1 << 30) : 0;
-                const int k2 = en.y * NMODE + s2;
-#pragma unroll
-                for (int sl = 0; sl < 2; ++sl) {
-                    unsigned m = (act >> (6 * sl)) & 0x3fu;
-                    if (m == 0u) continue;
-                    const int b = 8 * sl, k1 = q1 * NMODE + g + 3 * sl;
-                    // item (Re, Im) Y[mu][a], k = mu * 3 + a
-                    const float4 v0 = make_float4(y[0][b], y[0][b + 1], y[0][b + 2], y[1][b]);
-                    const float4 v1 = make_float4(y[1][b + 1], y[1][b + 2], y[0][b + 3], y[0][b + 4]);
-                    const float4 v2 = make_float4(y[0][b + 5], y[1][b + 3], y[1][b + 4], y[1][b + 5]);
-                    do {
-                        const int s0 = __ffs(m) - 1;
-                        m &= m - 1u;
-                        if (pos < a.cap) {
-                            float4* dst = reinterpret_cast<float4*>(region + pos);
-                            dst[0] = v0;
-                            dst[1] = v1;
-                            dst[2] = v2;
-                            const int k0 = (en.x * NMODE + s0) | kw | (en.w != 0 && s0 < 3 ? (1 << 29) : 0);
-                            reinterpret_cast<int4*>(dst)[3] = make_int4(k0, k1, k2, 0);
-                        }
-                        ++pos;
-                    } while (m != 0u);
-                }
+            while (count >= 32) {
+                count -= 32;
+                tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
+                               out_p3);
             }
         }
-        if (lane == 0) counts[blockIdx.x * EPI_WARPS + warp] = base;
+        if (count > 0)
+            tc_drain<FAST>(stg, count, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw, out_p3);
     }
-    // Every role has left its loop (each of its waits is bounded).  After a time-out the operand
-    // copies of up to NOP tiles may be in flight, unconsumed by the MMA warp: a copy of tile t is
-    // only issued once the MMAs of tile t - NOP completed, so those tiles are filled - NOP + 1 ..
-    // filled, and each of their ready phases completes once the copy lands (the frequency warp
-    // arrived for them: it runs NEP >= NOP tiles ahead without waiting).  The copy warp waits for
-    // them before the CTA releases its shared memory.  The MMA warp already waited for its last
+    // Every role has left its loop (each of its waits is bounded).  After a time-out copies may be
+    // in flight into shared memory, unconsumed: the copy warp's operand copies of up to NOP tiles
+    // (a copy of tile t is only issued once the MMAs of tile t - NOP completed, so those tiles are
+    // filled - NOP + 1 .. filled), and the frequency warp's q0-record copies of the tiles it filled
+    // beyond `filled` (at most NEP: it runs at most NEP tiles ahead of the epilogue, which cannot
+    // pass `filled`).  Each such ready phase completes once its copies land and both filling warps
+    // arrived: the copy warp arrives in place of the warp that did not fill the tile and waits for
+    // the phase before the CTA releases its shared memory.  The MMA warp already waited for its last
     // commit, so no MMA writes tensor memory after the release below.
-    // Where the frequency warp stopped before tile t, the copy warp arrives in its place, so that
-    // the phase completes on the copies' bytes alone.
     tc::fence_before_sync();
     __syncthreads();
-    if (warp == EPI_WARPS && lane == 0 && *(volatile int*)&S.abort)
-        for (int t = max(0, filled - NOP + 1); t <= filled; ++t) {
+    if (warp == EPI_WARPS && lane == 0 && *(volatile int*)&S.abort) {
+        const int fd = S.fdone;
+        for (int t = max(0, filled - NOP + 1); t <= max(filled, fd - 1); ++t) {
             const uint32_t rb = tc::smem_u32(&S.ready[t % NEP]);
-            if (t >= S.fdone) tc::mbar_arrive_cnt(rb, 32);
+            if (t >= fd) tc::mbar_arrive_cnt(rb, 32);
+            if (t > filled) tc::mbar_arrive_cnt(rb, 32);
             tc::mbar_wait(rb, (uint32_t)((t / NEP) & 1), MAX_SPINS);
         }
+    }
     __syncthreads();
     tc::fence_after_sync();
     if (warp == 0) tc::tmem_dealloc(tm, TC_COLS);
-}
-
-// One active triple whose item and records are already in registers.  FAST (mode records of 8
-// doubles, n_temps <= 4): the occupations come with omega and 1/omega in the same load, so an item
-// needs a single round trip to memory after its own load.
-constexpr int NT_FAST = 4;
-struct EvalIn {
-    float4 v0, v1, v2;
-    int4 kk;
-    Q0Rec q0;
-    double w1, ob1, w2, ob2;
-    double n1[NT_FAST], n2[NT_FAST];
-};
-
-template <bool FAST>
-__device__ __forceinline__ void eval_load(EvalIn& x, const TcItem* item, const Q0Rec* __restrict__ q0rec,
-                                          const double* __restrict__ modes, int rs) {
-    const float4* src = reinterpret_cast<const float4*>(item);
-    x.v0 = src[0];
-    x.v1 = src[1];
-    x.v2 = src[2];
-    x.kk = reinterpret_cast<const int4*>(src)[3];
-    x.q0 = q0rec[x.kk.x & 0x1fffffff];
-    const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)x.kk.y * rs);
-    const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)x.kk.z * rs);
-    const double2 a = pa[0], b = pb[0];
-    x.w1 = a.x;
-    x.ob1 = a.y;
-    x.w2 = b.x;
-    x.ob2 = b.y;
-    if (FAST) {
-        const double2 a1 = pa[1], a2 = pa[2], b1 = pb[1], b2 = pb[2];
-        x.n1[0] = a1.x;
-        x.n1[1] = a1.y;
-        x.n1[2] = a2.x;
-        x.n1[3] = a2.y;
-        x.n2[0] = b1.x;
-        x.n2[1] = b1.y;
-        x.n2[2] = b2.x;
-        x.n2[3] = b2.y;
-    }
-}
-
-template <bool FAST>
-__device__ __forceinline__ void eval_item(const EvalIn& x, int nq0, int nT, int rs, double half_os2, double pre,
-                                          double mfac, const double* __restrict__ modes, double* out_lw,
-                                          double* out_p3) {
-    const int o = x.kk.x & 0x1fffffff;
-    const double w0 = x.q0.w, w1 = x.w1, w2 = x.w2;
-    const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
-    const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
-    const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
-    const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
-    const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
-    const double wt = (x.kk.x >> 30) & 1 ? 2.0 : 1.0;
-    const double p3 = e1 + e2 + e3;
-    if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
-    if ((x.kk.x >> 29) & 1) return;  // W = 0 for the Gamma acoustic modes of q0
-    const float yr[6] = {x.v0.x, x.v0.y, x.v0.z, x.v0.w, x.v1.x, x.v1.y};
-    const float yi[6] = {x.v1.z, x.v1.w, x.v2.x, x.v2.y, x.v2.z, x.v2.w};
-    float pr = 0.0f, pim = 0.0f;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        const float2 c = x.q0.e0[k];
-        pr = fmaf(c.x, yr[k], fmaf(-c.y, yi[k], pr));
-        pim = fmaf(c.x, yi[k], fmaf(c.y, yr[k], pim));
-    }
-    const double W = (double)(pr * pr + pim * pim) * (x.q0.ob * x.ob2 * x.ob1) * mfac * wt;
-    const double we1 = W * e1, wf2 = W * (e2 - e3);
-    if (FAST) {
-#pragma unroll
-        for (int T = 0; T < NT_FAST; ++T)
-            if (T < nT) {
-                const double n1 = x.n1[T], n2 = x.n2[T];
-                const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
-                if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
-            }
-        return;
-    }
-    const double* m1 = modes + (size_t)x.kk.y * rs + 2;
-    const double* m2 = modes + (size_t)x.kk.z * rs + 2;
-    for (int T = 0; T < nT; ++T) {
-        const double n1 = m1[T], n2 = m2[T];
-        const double v = ((n1 + n2 + 1.0) * we1) + ((n1 - n2) * wf2);
-        if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
-    }
-}
-
-// FP64 part of the active triples: Phi = sum_k e0'(k, s0) Y_k (FP32), W = wt mfac |Phi|^2 /
-// (omega0 omega1 omega2), the three Gaussian delta weights, then the phase-space and linewidth
-// sums with atomics: P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].
-// Block (r, y) walks region r of the item list, two items per thread at a time with both items'
-// loads issued first.
-template <bool FAST>
-__global__ void __launch_bounds__(256, 2) k_v3tc_eval(const TcItem* __restrict__ items, const int* __restrict__ counts,
-                                                   int cap, int nq0, int nT, int rs, double half_os2, double pre,
-                                                   double mfac, const Q0Rec* __restrict__ q0rec,
-                                                   const double* __restrict__ modes, double* __restrict__ out_lw,
-                                                   double* __restrict__ out_p3) {
-    const int r = blockIdx.x;
-    const int n = min(counts[r], cap);
-    const TcItem* reg = items + (size_t)r * cap;
-    const int stride = gridDim.y * blockDim.x;
-    for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < n; i += 2 * stride) {
-        const int j = i + stride;
-        EvalIn a, b;
-        eval_load<FAST>(a, reg + i, q0rec, modes, rs);
-        if (j < n) eval_load<FAST>(b, reg + j, q0rec, modes, rs);
-        eval_item<FAST>(a, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
-        if (j < n) eval_item<FAST>(b, nq0, nT, rs, half_os2, pre, mfac, modes, out_lw, out_p3);
-    }
 }
 
 // Tensor map of the A table as a 2-D array of 8-byte elements: rows = grid points, 384 columns
@@ -847,17 +814,17 @@ int make_tmap_a(spring_ctx* c, CUtensorMap* tm) {
     return SPRING_OK;
 }
 
-template <bool SPLIT>
-int launch_tc(spring_ctx* c, TcArgs& a, TcItem* items) {
+template <bool SPLIT, bool FAST>
+int launch_tc(spring_ctx* c, TcArgs& a, double* d_lw, double* d_p3) {
     const size_t smem = sizeof(TcSmem);
     alignas(64) CUtensorMap tmA;
     SPRING_CHECK(make_tmap_a(c, &tmA));
     if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "tensor-core V3 needs %zu bytes of shared memory", smem);
-    cudaFuncSetAttribute(k_v3tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_v3tc<SPLIT, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
-    k_v3tc<SPLIT><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
-        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p, c->ph_grid.omega.p, items,
-        c->d_tc_cnt_cta.p, c->d_tc_cnt_cta.p + c->tc_grid * EPI_WARPS);
+    k_v3tc<SPLIT, FAST><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
+        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p,
+        c->ph_grid.omega.p, reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p, d_lw, d_p3, c->d_tc_cnt_cta.p);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -1079,52 +1046,19 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     const int ctas = std::max(1, std::min(a.ntiles, sms));
     a.tiles_per_cta = (a.ntiles + ctas - 1) / ctas;
     c->tc_grid = (a.ntiles + a.tiles_per_cta - 1) / a.tiles_per_cta;
-    const int nreg = c->tc_grid * EPI_WARPS;  // item regions: one per epilogue warp
-    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, nreg + 1, "V3 item counts"));  // + the status word
-    // Item list: one region per epilogue warp, first sized for 8 % of its share of the CTA's mode
-    // triples (about 3 % of the triples of the pairs left after the pre-screen pass the screen on
-    // meshes from 8^3 to 24^3), regrown to what the pass reports if that overflows.
-    const long long triples = (long long)a.tiles_per_cta * EPT * NMODE * NMODE * NMODE / EPI_WARPS;
-    long long cap = std::max<long long>(c->tc_cap_frac > 0.0 ? (long long)(c->tc_cap_frac * triples) : triples / 12, 256);
-    const bool split = c->precision == SPRING_BF16X3;
-    int maxcnt = 0;
-    for (int attempt = 0; attempt < 2; ++attempt) {
-        cap = std::min<long long>(cap, triples);
-        a.cap = (int)cap;
-        SPRING_CHECK(dalloc(c, c->d_tc_items, (size_t)nreg * cap * (sizeof(TcItem) / sizeof(float4)), "V3 items"));
-        TcItem* items = reinterpret_cast<TcItem*>(c->d_tc_items.p);
-        SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p + nreg, sizeof(int), "V3 status"));
-        SPRING_CHECK(split ? launch_tc<true>(c, a, items) : launch_tc<false>(c, a, items));
-        SPRING_CHECK(d2h_pin_async(c, c->d_tc_cnt_cta.p, sizeof(int) * (nreg + 1), "V3 item counts"));
-        // The evaluation pass is queued at once: it reads the item counts on the device and clamps
-        // them to the region size, so the host checks them while it runs.
-        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc eval: injected launch failure");
-        const int gy = c->tc_eval_y > 0 ? c->tc_eval_y : (int)std::min<long long>(1024, (cap + 2 * threads - 1) / (2 * threads));
-        auto eval = (rs == 8 && c->nT <= NT_FAST) ? k_v3tc_eval<true> : k_v3tc_eval<false>;
-        eval<<<dim3(nreg, gy), threads, 0, c->stream>>>(
-            items, c->d_tc_cnt_cta.p, (int)cap, c->nq0, c->nT, rs, a.half_os2, os * ONEBYSQRT2PI,
-            host_constants().Sctr3THz2 / double(nq), reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p,
-            d_lw, d_p3);
-        SPRING_CHECK(launch_check(c, "k_v3tc_eval"));
-        SPRING_CHECK(pin_wait(c, "V3 item counts"));
-        const int* cnt = c->h_pin;
-        const int herr = cnt[nreg];
-        if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
-        if (herr) return fail(c, SPRING_ERR_TIMEOUT, "tensor-core V3: a pipeline wait ran out after %lld polls",
-                              a.max_spins);
-        maxcnt = *std::max_element(cnt, cnt + nreg);
-        if (maxcnt <= cap) break;
-        // The pass wrote only what fit and the evaluation summed that part: clear this block's sums
-        // and run both again with regions sized from the counts.
-        for (int T = 0; T < c->nT; ++T)
-            SPRING_CHECK(zero(c, d_lw + ((size_t)T * c->nq0 + q0_first) * NMODE, sizeof(double) * n_q0 * NMODE,
-                              "linewidths"));
-        SPRING_CHECK(zero(c, d_p3 + (size_t)q0_first * NMODE, sizeof(double) * n_q0 * NMODE, "phase space"));
-        cap = (long long)(maxcnt * 1.25) + 256;
-    }
-    if (maxcnt > cap) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: item list overflow");
-    c->tc_cap_frac = std::max(c->tc_cap_frac, 1.25 * maxcnt / (double)triples);
-    c->tc_eval_y = std::max(1, std::min(1024, (maxcnt + 2 * threads - 1) / (2 * threads)));
+    a.rs = rs;
+    a.pre = os * ONEBYSQRT2PI;
+    a.mfac = host_constants().Sctr3THz2 / double(nq);
+    SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, 1, "V3 status"));
+    SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p, sizeof(int), "V3 status"));
+    const bool split = c->precision == SPRING_BF16X3, fast = rs == 8 && c->nT <= NT_FAST;
+    SPRING_CHECK(split ? (fast ? launch_tc<true, true>(c, a, d_lw, d_p3) : launch_tc<true, false>(c, a, d_lw, d_p3))
+                       : (fast ? launch_tc<false, true>(c, a, d_lw, d_p3) : launch_tc<false, false>(c, a, d_lw, d_p3)));
+    SPRING_CHECK(d2h_pin_async(c, c->d_tc_cnt_cta.p, sizeof(int), "V3 status"));
+    SPRING_CHECK(pin_wait(c, "V3 status"));
+    const int herr = c->h_pin[0];
+    if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
+    if (herr) return fail(c, SPRING_ERR_TIMEOUT, "tensor-core V3: a pipeline wait ran out after %lld polls", a.max_spins);
     return SPRING_OK;
 }
 

@@ -243,19 +243,16 @@ struct spring_ctx {
     spring::DBuf<uint16_t> d_tc_b;     // bf16 B operand images [q1][hi, lo][mu]
     spring::DBuf<double> d_tc_q0;      // q0 mode records: e0' float2[6], omega, 1/omega (64 bytes each)
     spring::DBuf<double> d_tc_modes;   // grid mode records: omega, 1/omega, nBE[T] (padded to 4 doubles)
-    spring::DBuf<float4> d_tc_items;   // active mode triples, one region per CTA (64 bytes each)
-    spring::DBuf<int> d_tc_cnt_cta;    // triples written per CTA, then the status word
+    spring::DBuf<int> d_tc_cnt_cta;    // status word of the tensor-core pass
     spring::DBuf<int> d_scr_sum;       // one-int readback scratch
     spring::DBuf<int> d_scr_rot, d_scr_map;  // spring_find_irr_q scratch: rotations, orbit map
     int tc_grid = 0;
-    double tc_cap_frac = 0.0;          // item region size as a fraction of its share of the triples
     spring::DBuf<int> d_tc_entries;    // pair indices sorted by q1
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
     int tc_ntiles = 0, tc_gen = -1, tc_q0 = -1, tc_n0 = -1, tc_nmax = 0, tc_ph_gen = -1;  // tile cache key
     int tc_npairs = 0;                 // pairs in those tiles
     float tc_rf = 0.0f;                // delta window the cached tiles were screened with
-    int tc_eval_y = 0;                 // blocks per item region of the last evaluation pass
     bool tc_pending = false;           // tile count read back asynchronously, tiles not cut yet
     int ph_gen = 0;                    // bumped whenever the grid or irreducible phonons change
     // scratch kept between calls (the enumeration and the tile sort run every step)

@@ -39,7 +39,7 @@ def main() -> int:
             ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6)
         total_ms, total_n = ctx.kernel_time("")  # waits for the stream
         wall = time.time() - t
-    names = {"v3": ("k_v3tc<", "k_v3tc_eval", "k_v3s", "k_tc_"), "v4": ("k_v4tc", "k4_", "k_enum4"),
+    names = {"v3": ("k_v3tc<", "k_v3s", "k_tc_"), "v4": ("k_v4tc", "k4_", "k_enum4"),
              "bte": ("k_v3s", "k_bteg_", "k_bte_")}[a.case]
     print(f"{a.case} mesh {a.mesh}^3, {n} q0, {a.precision}: wall {wall * 1e3:.1f} ms, "
           f"{total_n} profiled launches {total_ms:.3f} ms")
