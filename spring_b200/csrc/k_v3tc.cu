@@ -325,7 +325,7 @@ struct TcArgs {
 
 constexpr int NOP = 2;  // operand stages (A and B images; free once the tile's MMAs completed)
 constexpr int NEP = 4;  // epilogue stages (frequencies and one 128-column accumulator each)
-static_assert(NOP <= NEP, "a fill of ready[j % NEP] must follow the completion of its previous phase");
+static_assert(NOP <= NEP, "operand stages beyond the accumulator stages would wait on the epilogue anyway");
 
 // An active mode triple, staged in shared memory by the epilogue warp that found it: |Phi|^2 in
 // FP32, k0 = (q0 * 6 + s0) | (wt == 2) << 30 | (W = 0) << 29, k1 = q1 * 6 + s1, k2 = q2 * 6 + s2.
@@ -341,7 +341,7 @@ struct OpStage {
     int q1;                                   // q1 whose B images are resident
 };
 struct EpStage {
-    alignas(128) Q0Rec q0r[EPT][NMODE];        // per pair its six q0 records (bulk copies)
+    alignas(128) Q0Rec q0r[EPT][NMODE];        // per pair its six q0 records (e0' only: 16-byte async copies)
     alignas(16) float2 cb[EPT][NMODE][NMODE];  // per pair, s2, s0: tc_window_vals of the FP32 omegas
     alignas(8) float w1s[NMODE];               // omega of q1 in FP32, s1 in slot order 0 3 1 4 2 5
     int4 ent[EPT];                             // (q0, q2, weight, q0 is Gamma)
@@ -352,10 +352,10 @@ struct TcSmem {
     OpStage op[NOP];
     EpStage ep[NEP];
     alignas(16) TcStage stg[EPI_WARPS][STG_CAP];
-    alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP];
+    alignas(8) uint64_t ready[NEP], full[NEP], empty[NEP], opfree[NOP], opready[NOP];
     uint32_t tslot;
     int abort;  // set by any warp whose pipeline wait ran out
-    int fdone;  // tiles the frequency warp arrived on ready for (written when it leaves its loop)
+    int fdone;  // tiles the frequency warp filled (written when it leaves its loop)
 };
 static_assert(sizeof(TcSmem) <= 227 * 1024, "tensor-core V3 shared memory");
 
@@ -391,9 +391,11 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
         const double w0 = r0.x, w1 = a.x, w2 = b.x;
         const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
         const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
-        const double e1 = x1 < EXP_CUT ? pre * exp(-x1) : 0.0;
-        const double e2 = x2 < EXP_CUT ? pre * exp(-x2) : 0.0;
-        const double e3 = x3 < EXP_CUT ? pre * exp(-x3) : 0.0;
+        // three independent exponentials of clamped arguments (no branch between them), then the cut
+        const double g1 = exp(-fmin(x1, EXP_CUT)), g2 = exp(-fmin(x2, EXP_CUT)), g3 = exp(-fmin(x3, EXP_CUT));
+        const double e1 = x1 < EXP_CUT ? pre * g1 : 0.0;
+        const double e2 = x2 < EXP_CUT ? pre * g2 : 0.0;
+        const double e3 = x3 < EXP_CUT ? pre * g3 : 0.0;
         const double wt = (s.k0 >> 30) & 1 ? 2.0 : 1.0;
         const double p3 = e1 + e2 + e3;
         if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
@@ -423,10 +425,12 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
 
 // Warp-specialised tensor-core pass.  For tile j the copy warp loads operand stage j % 2 (TMA
 // gathers of the A images, four pairs' table rows per request, hi and lo parts as separate
-// requests; one bulk copy of the B images when q1 changed) and the frequency warp epilogue stage
-// j % 4 (entry records and the tile's omegas, plain loads issued one tile ahead; the pairs' q0
-// records as bulk copies); both complete on ready[j % 4].  The MMA warp issues tile j's MMAs into
-// the accumulator of epilogue stage j % 4 and commits them to full[j % 4] and opfree[j % 2].  Each
+// requests; one bulk copy of the B images when q1 changed), completing on opready[j % 2], and the
+// frequency warp epilogue stage j % 4 (entry records and the tile's omegas, plain loads issued one
+// tile ahead; the pairs' e0' as asynchronous copies), completing on ready[j % 4].  The MMA warp
+// issues tile j's MMAs once its operands landed and the epilogue released accumulator j % 4
+// (empty), and commits them to full[j % 4] and opfree[j % 2]: the frequency warp's fill is off the
+// operand loop (copy -> MMA -> opfree -> copy), which runs two tiles deep.  Each
 // epilogue warp works on its own: it reads its 32 accumulator rows, screens its 12 mode triples per
 // row in FP32 against the delta window, forms |Phi|^2 of the active ones (about 1-3 %) from the
 // stage's q0 records, stages them in its shared-memory buffer, releases the stage, and evaluates
@@ -456,9 +460,10 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         for (int k = 0; k < NOP; ++k) {
             S.op[k].q1 = -1;
             tc::mbar_init(tc::smem_u32(&S.opfree[k]), 1);
+            tc::mbar_init(tc::smem_u32(&S.opready[k]), 32);  // copy-warp lanes (and the copies' bytes)
         }
         for (int k = 0; k < NEP; ++k) {
-            tc::mbar_init(tc::smem_u32(&S.ready[k]), 64);  // copy-warp and frequency-warp lanes
+            tc::mbar_init(tc::smem_u32(&S.ready[k]), 64);  // frequency-warp lanes and their copies
             tc::mbar_init(tc::smem_u32(&S.full[k]), 1);
             tc::mbar_init(tc::smem_u32(&S.empty[k]), EPI_WARPS);
         }
@@ -473,15 +478,15 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
 
     if (warp == EPI_WARPS) {
         // ------------------------------------------------------------ copy warp
-        // Operand stage j % 2 for tile j, after the MMAs of tile j-2 released it (so every earlier
-        // phase of ready[j % 4] has completed, NOP <= NEP): TMA gathers of the A images and, when q1 changed,
-        // the B images; each issuing lane adds its own bytes to ready before its copy, then every
+        // Operand stage j % 2 for tile j, after the MMAs of tile j-2 released it (so the previous
+        // phase of opready[j % 2] has completed): TMA gathers of the A images and, when q1 changed,
+        // the B images; each issuing lane adds its own bytes to opready before its copy, then every
         // lane arrives.  Tile and entry records are loaded ahead into registers.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
         for (int j = 0; j < nt; ++j) {
-            const int es = j % NEP, os = j % NOP;
+            const int os = j % NOP;
             const bool ok = j < NOP || tc::mbar_wait(tc::smem_u32(&S.opfree[os]), (uint32_t)(((j - NOP) / NOP) & 1),
                                                      a.max_spins);
             if (__any_sync(0xffffffffu, !ok)) {
@@ -499,7 +504,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             int rows[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) rows[k] = __shfl_sync(0xffffffffu, entA.y, 4 * g + k < ne ? 4 * g + k : 0);
-            const uint32_t rb = tc::smem_u32(&S.ready[es]);
+            const uint32_t rb = tc::smem_u32(&S.opready[os]);
             if (lane < 4 * H && 4 * g < ne) {
                 tc::mbar_expect_tx(rb, 4u * PB);
                 tc::gather4_g2s(tc::smem_u32(&O.A[part][g * 4 * PB]), &tmA, part * (PB / 8), rows[0], rows[1], rows[2],
@@ -521,12 +526,12 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     } else if (warp == EPI_WARPS + 2) {
         // ------------------------------------------------------------ frequency warp
         // Epilogue stage j % 4 for tile j, after the epilogue of tile j-4 released it: entry
-        // records, the pairs' q0 records (lane l < 16 copies pair l's six, 384 bytes, adding its
-        // bytes to ready first), the q1 omegas and, per pair, s2 and s0, the window values
-        // (w0 - w2, w0 + w2) of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16)
+        // records, the pairs' e0' (lane l copies those of pair l % 16 for s0 = 3 (l / 16) .. + 2 as
+        // nine 16-byte asynchronous copies), the q1 omegas and, per pair, s2 and s0, the window
+        // values (w0 - w2, w0 + w2) of the FP32 screen.  Lane l prepares pair l % 16 for s2 = 3 (l / 16)
         // .. 3 (l / 16) + 2 from omegas loaded during the fill of tile j-1; no warp barrier follows
         // a load: each lane arrives on ready itself, after its own stores and before it issues new
-        // loads.
+        // loads, and once more when its copies have landed.
         const int4 z4 = make_int4(0, 0, 0, 0);
         int4 recA = nt > 0 ? tiles[t0] : z4, recB = nt > 1 ? tiles[t0 + 1] : z4, recC = nt > 2 ? tiles[t0 + 2] : z4;
         int4 entA = lane < recA.z ? entrec[recA.y + lane] : z4;
@@ -570,9 +575,15 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             EpStage& E = S.ep[es];
             const int q1 = recA.x, ne = recA.z;
             const uint32_t rb = tc::smem_u32(&S.ready[es]);
-            if (lane < ne) {
-                tc::mbar_expect_tx(rb, (uint32_t)sizeof(E.q0r[0]));
-                tc::bulk_g2s(tc::smem_u32(&E.q0r[lane][0]), q0rec + (size_t)entA.x * NMODE, (uint32_t)sizeof(E.q0r[0]), rb);
+            {
+                const int q0p = __shfl_sync(0xffffffffu, entA.x, pw);
+                if (pw < ne) {
+                    const char* src = reinterpret_cast<const char*>(q0rec + (size_t)q0p * NMODE + 3 * hw);
+                    const uint32_t dst = tc::smem_u32(&E.q0r[pw][3 * hw]);
+#pragma unroll
+                    for (int k = 0; k < 9; ++k)  // e0' of three s0: 48 of each record's 64 bytes
+                        tc::cp_async16(dst + (k / 3) * 64 + (k % 3) * 16, src + (k / 3) * 64 + (k % 3) * 16);
+                }
             }
             if (lane == 0) {
                 E.ne = ne;
@@ -596,7 +607,8 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     }
                 }
             }
-            tc::mbar_arrive(rb);  // each lane releases its own stores
+            tc::mbar_arrive(rb);           // each lane releases its own stores
+            tc::cp_async_mbar_arrive(rb);  // and, once they land, its copies
             // loads for later fills
             if (j + 1 < nt) load_w(entB, recB);
             const int4 entC = (j + 2 < nt && lane < recC.z) ? entrec[recC.y + lane] : z4;
@@ -610,13 +622,15 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         if (lane == 0) S.fdone = j;
     } else if (warp == EPI_WARPS + 1) {
         // ------------------------------------------------------------ MMA warp
-        // Tile j's MMAs once its operands have landed (ready); its accumulator was drained before the
-        // fill of j (which waited for empty), its operands stay until the commit to opfree.
+        // Tile j's MMAs once the epilogue has drained its accumulator (tile j-4, empty) and its
+        // operands have landed (opready); its operands stay until the commit to opfree.
         int issued = -1;
         if (lane == 0) {
             for (int j = 0; j < nt; ++j) {
                 const int es = j % NEP, os = j % NOP;
-                if (!tc::mbar_wait(tc::smem_u32(&S.ready[es]), (uint32_t)((j / NEP) & 1), a.max_spins)) {
+                const bool acc_free = j < NEP || tc::mbar_wait(tc::smem_u32(&S.empty[es]),
+                                                               (uint32_t)(((j - NEP) / NEP) & 1), a.max_spins);
+                if (!acc_free || !tc::mbar_wait(tc::smem_u32(&S.opready[os]), (uint32_t)((j / NOP) & 1), a.max_spins)) {
                     atomicExch(err, 1);
                     *(volatile int*)&S.abort = 1;
                     break;
@@ -690,13 +704,13 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             const uint32_t ta = tm + ((uint32_t)(wq * 32) << 16) + (uint32_t)(es * 128 + 16 * g);
             tc::tmem_ld16(ta, y[0]);
             tc::tmem_ld16(ta + 64, y[1]);
-            // shared-memory reads that do not depend on the accumulator, issued before its wait
+            // The window screen and the item positions need only the stage's shared-memory records:
+            // they run while the accumulator loads are in flight.
             const int ne = E.ne, q1 = E.q1;
             const int4 en = E.ent[e];
             const float4* cbp = reinterpret_cast<const float4*>(&E.cb[e][s2c][0]);
             const float4 c01 = cbp[0], c23 = cbp[1], c45 = cbp[2];
             const float2 w1 = *reinterpret_cast<const float2*>(&E.w1s[2 * g]);
-            tc::tmem_ld_wait();
             const bool row_on = s2 < NMODE && e < ne && s2 >= a.lo[2] && s2 <= a.hi[2] && !(en.y == 0 && s2 < 3);
             const unsigned amask = q1 == 0 ? amask_g : amask_n;
             unsigned act = 0u;
@@ -710,45 +724,68 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                 }
                 act &= amask;
             }
-            // Stage the active triples in four chunks (s1 slot, s0 half; at most 3 per lane, 96 per
-            // warp): positions from two bit-plane ballots, |Phi|^2 = |sum_k e0'(k, s0) Y_k|^2 in FP32
-            // from the stage's q0 record of the lane's pair.  A chunk that would not fit first
-            // evaluates full rounds (rare: fewer than 32 are left between tiles).
+            // Stage the active triples: positions from four bit-plane ballots of the lanes' counts
+            // (at most 12), then each lane writes its own, |Phi|^2 = |sum_k e0'(k, s0) Y_k|^2 in FP32
+            // from the stage's q0 record of the lane's pair (the two basis atoms' terms summed
+            // separately).  When the tile's triples would not fit beside those left from earlier
+            // tiles (fewer than 32; rare), they go in four chunks of at most 3 per lane, each after
+            // full rounds are evaluated to make room.
             const int kw = en.z == 2 ? (1 << 30) : 0;
             const int k0b = en.x * NMODE, k2 = en.y * NMODE + s2;
             const bool g0 = en.w != 0;
             const Q0Rec* qr = E.q0r[e];
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const int sl = c >> 1;
-                unsigned m = (act >> (3 * c)) & 7u;
-                const int cm = __popc(m);
-                const unsigned b0 = __ballot_sync(0xffffffffu, cm & 1), b1 = __ballot_sync(0xffffffffu, cm & 2);
-                const int tot = __popc(b0) + 2 * __popc(b1);
-                if (tot == 0) continue;
-                while (count + tot > STG_CAP) {
-                    count -= 32;
-                    tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
-                                   out_p3);
-                }
-                int pos = count + __popc(b0 & lt) + 2 * __popc(b1 & lt);
-                count += tot;
+            auto stage_bits = [&](unsigned m, int pos) {
                 while (m != 0u) {
-                    const int s0 = 3 * (c & 1) + __ffs(m) - 1;  // bit 3 c + t of act is s0 = 3 (c & 1) + t
+                    const int bit = __ffs(m) - 1;  // bit 6 sl + s0
                     m &= m - 1u;
-                    const float2* c0 = qr[s0].e0;
-                    float pr = 0.0f, pim = 0.0f;
+                    const int sl = bit >= NMODE ? 1 : 0, s0 = bit - NMODE * sl;
+                    const float4* cq = reinterpret_cast<const float4*>(qr[s0].e0);
+                    const float4 c01 = cq[0], c23 = cq[1], c45 = cq[2];
+                    const float cx[NMODE] = {c01.x, c01.z, c23.x, c23.z, c45.x, c45.z};
+                    const float cy[NMODE] = {c01.y, c01.w, c23.y, c23.w, c45.y, c45.w};
+                    float pr[2] = {0.0f, 0.0f}, pim[2] = {0.0f, 0.0f};
 #pragma unroll
                     for (int k = 0; k < NMODE; ++k) {
-                        const float yr = y[k / 3][8 * sl + k % 3], yi = y[k / 3][8 * sl + 3 + k % 3];
-                        const float2 cv = c0[k];
-                        pr = fmaf(cv.x, yr, fmaf(-cv.y, yi, pr));
-                        pim = fmaf(cv.x, yi, fmaf(cv.y, yr, pim));
+                        const int mu = k / 3, al = k % 3;
+                        const float yr = sl ? y[mu][8 + al] : y[mu][al], yi = sl ? y[mu][11 + al] : y[mu][3 + al];
+                        pr[mu] = fmaf(cx[k], yr, fmaf(-cy[k], yi, pr[mu]));
+                        pim[mu] = fmaf(cx[k], yi, fmaf(cy[k], yr, pim[mu]));
                     }
+                    const float p = pr[0] + pr[1], q = pim[0] + pim[1];
                     const int k0 = (k0b + s0) | kw | (g0 && s0 < 3 ? (1 << 29) : 0);
-                    stg[pos++] = TcStage{pr * pr + pim * pim, k0, q1 * NMODE + g + 3 * sl, k2};
+                    stg[pos++] = TcStage{p * p + q * q, k0, q1 * NMODE + g + 3 * sl, k2};
                 }
-                __syncwarp();
+            };
+            const int cnt = __popc(act);
+            int pre = 0, tot = 0;
+#pragma unroll
+            for (int bp = 0; bp < 4; ++bp) {
+                const unsigned bal = __ballot_sync(0xffffffffu, (cnt >> bp) & 1);
+                pre += __popc(bal & lt) << bp;
+                tot += __popc(bal) << bp;
+            }
+            tc::tmem_ld_wait();
+            tc::tmem_regs_ready<16>(y[0]);
+            tc::tmem_regs_ready<16>(y[1]);
+            if (count + tot <= STG_CAP) {
+                stage_bits(act, count + pre);
+                count += tot;
+            } else {
+#pragma unroll 1
+                for (int c = 0; c < 4; ++c) {
+                    const unsigned m = act & (7u << (3 * c));
+                    const int cm = __popc(m);
+                    const unsigned b0 = __ballot_sync(0xffffffffu, cm & 1), b1 = __ballot_sync(0xffffffffu, cm & 2);
+                    const int nc = __popc(b0) + 2 * __popc(b1);
+                    while (count + nc > STG_CAP) {
+                        count -= 32;
+                        tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes,
+                                       out_lw, out_p3);
+                    }
+                    stage_bits(m, count + __popc(b0 & lt) + 2 * __popc(b1 & lt));
+                    count += nc;
+                    __syncwarp();
+                }
             }
             // every read of the stage is done: release it, then evaluate full rounds
             tc::fence_before_sync();
@@ -766,22 +803,20 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
     // Every role has left its loop (each of its waits is bounded).  After a time-out copies may be
     // in flight into shared memory, unconsumed: the copy warp's operand copies of up to NOP tiles
     // (a copy of tile t is only issued once the MMAs of tile t - NOP completed, so those tiles are
-    // filled - NOP + 1 .. filled), and the frequency warp's q0-record copies of the tiles it filled
-    // beyond `filled` (at most NEP: it runs at most NEP tiles ahead of the epilogue, which cannot
-    // pass `filled`).  Each such ready phase completes once its copies land and both filling warps
-    // arrived: the copy warp arrives in place of the warp that did not fill the tile and waits for
-    // the phase before the CTA releases its shared memory.  The MMA warp already waited for its last
-    // commit, so no MMA writes tensor memory after the release below.
+    // filled - NOP + 1 .. filled) and the frequency warp's e0' copies of up to NEP tiles (a fill of
+    // tile t follows the epilogue of tile t - NEP, so those tiles are fdone - NEP .. fdone - 1).
+    // Every such phase completes by itself once its copies land (each filling lane arrived, its
+    // copies' arrivals are asynchronous): the copy warp waits for them before the CTA releases its
+    // shared memory.  The MMA warp already waited for its last commit, so no MMA writes tensor memory
+    // after the release below.
     tc::fence_before_sync();
     __syncthreads();
     if (warp == EPI_WARPS && lane == 0 && *(volatile int*)&S.abort) {
+        for (int t = max(0, filled - NOP + 1); t <= filled; ++t)
+            tc::mbar_wait(tc::smem_u32(&S.opready[t % NOP]), (uint32_t)((t / NOP) & 1), MAX_SPINS);
         const int fd = S.fdone;
-        for (int t = max(0, filled - NOP + 1); t <= max(filled, fd - 1); ++t) {
-            const uint32_t rb = tc::smem_u32(&S.ready[t % NEP]);
-            if (t >= fd) tc::mbar_arrive_cnt(rb, 32);
-            if (t > filled) tc::mbar_arrive_cnt(rb, 32);
-            tc::mbar_wait(rb, (uint32_t)((t / NEP) & 1), MAX_SPINS);
-        }
+        for (int t = max(0, fd - NEP); t < fd; ++t)
+            tc::mbar_wait(tc::smem_u32(&S.ready[t % NEP]), (uint32_t)((t / NEP) & 1), MAX_SPINS);
     }
     __syncthreads();
     tc::fence_after_sync();

@@ -127,6 +127,13 @@ static __device__ __forceinline__ void tmem_ld2(uint32_t taddr, float* v) {
 static __device__ __forceinline__ void tmem_ld_wait() {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+// After tmem_ld_wait: ties n registers written by earlier tcgen05.ld to this point, so that no use
+// of them is scheduled before the wait.
+template <int N>
+static __device__ __forceinline__ void tmem_regs_ready(float* v) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) asm volatile("" : "+f"(v[i]));
+}
 
 // Plain arrive on an mbarrier (release semantics at CTA scope).
 static __device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
@@ -145,6 +152,11 @@ static __device__ __forceinline__ void named_bar(uint32_t id, uint32_t count) {
 // 16-byte global -> shared asynchronous copy and the wait for all of this thread's copies.
 static __device__ __forceinline__ void cp_async16(uint32_t saddr, const void* g) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr), "l"(g) : "memory");
+}
+// Arrive on an mbarrier once every cp.async this thread issued so far has landed; the arrival counts
+// toward the barrier's expected count (.noinc).
+static __device__ __forceinline__ void cp_async_mbar_arrive(uint32_t mbar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(mbar) : "memory");
 }
 static __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.wait_all;" ::: "memory");
