@@ -582,8 +582,44 @@ def batched_leg(torch, steps=3):
     ctx12.linewidth_path(q, z, delta="gauss", sigma=SIGMA)
     path_ms = min(ev_ms(lambda: ctx12.linewidth_path(q, z, delta="gauss", sigma=SIGMA)) for _ in range(steps))
     b.close()
+    # Mixed precision: the two-atom contexts on BF16x3 (tensor-core pass), the 8-atom ones on FP64;
+    # single calls plus the path call, against one batch holding all of it (path points in its graph).
+    for name, _, ctx, _ in cells:
+        if name == "rocksalt2":
+            ctx.set_precision("bf16x3")
+    path_lw = [None]
+
+    def separate_mixed():
+        for _, _, ctx, _ in cells:
+            ctx.reset_linewidths()
+            ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA, want=False)
+        path_lw[0] = ctx12.linewidth_path(q, z, delta="gauss", sigma=SIGMA)[0]
+        for _, _, ctx, _ in cells:
+            ctx.synchronize()
+
+    separate_mixed()
+    sep_mixed = min(ev_ms(separate_mixed) for _ in range(steps))
+    ref_m = [ctx.get_linewidths() for _, _, ctx, _ in cells]
+    bm = Batch()
+    for _, _, ctx, _ in cells:
+        bm.add_linewidth3(ctx, 1, ctx.nq0, SIGMA)
+    ip = bm.add_path(ctx12, q, z, SIGMA)
+    bm.set_config(*cfg)
+    runs_m = []
+    for _ in range(steps + 1):
+        for _, _, ctx, _ in cells:
+            ctx.reset_linewidths()
+        bm.run()
+        runs_m.append(bm.result(0)[2])
+    batch_mixed = min(runs_m[1:])
+    err_m = max(float(np.abs(bm.result(k)[0] - ref_m[k]).max() / np.abs(ref_m[k]).max()) for k in range(len(cells)))
+    lwp = bm.path_result(ip)[0]
+    err_p = float(np.abs(lwp - path_lw[0]).max() / np.abs(path_lw[0]).max())
+    bm.close()
     for _, _, ctx, _ in cells:
         ctx.close()
+    nq12 = 12 ** 3
+    path_evals = int(len(q)) * nq12 * 6 ** 3
     return {"workloads": [f"{n}-{N}^3" for n, N, _, _ in cells], "temperatures": temps,
             "pairs": [int(p) for *_, p in cells], "evals_per_T": int(evals),
             "batch_ms": batch_ms, "separate_calls_ms": sep, "separate_over_batch": sep / batch_ms,
@@ -594,7 +630,17 @@ def batched_leg(torch, steps=3):
             "tuning": {"configs_tried": tried, "best_trial_ms": tuned_ms},
             "path_points": int(len(q)), "path_ms": path_ms, "path_mesh": [12, 12, 12],
             "what": "one persistent FP64 launch over all five workloads' (pair, s0-block) items, heaviest "
-                    "first, replayed from a CUDA graph; path points on the 12^3 context afterwards"}
+                    "first, replayed from a CUDA graph; path points on the 12^3 context afterwards",
+            "mixed": {"batch_ms": batch_mixed, "separate_calls_ms": sep_mixed,
+                      "separate_over_batch": sep_mixed / batch_mixed,
+                      "evals_per_s_batch": (evals + path_evals) / (batch_mixed * 1e-3),
+                      "evals_per_s_separate": (evals + path_evals) / (sep_mixed * 1e-3),
+                      "path_evals_per_T": path_evals,
+                      "max_rel_diff_vs_separate": err_m, "path_max_rel_diff_vs_separate": err_p,
+                      "what": "two-atom workloads on BF16x3 through the tensor-core pass (the kernel of "
+                              "spring_linewidth3), 8-atom workloads in the persistent FP64 kernel, the 200 "
+                              "path points inside the batch's CUDA graph; against each context's own call "
+                              "with the same precision plus the path call, one after the other"}}
 
 
 def run_ours(args):

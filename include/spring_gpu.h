@@ -330,7 +330,11 @@ int spring_kappa_iter_gauss(spring_ctx* ctx, double sigma, double eps_k, int max
  * meaning of spring_linewidth3(ctx, i0_first, n_q0, SPRING_DELTA_GAUSS, sigma,
  * pol3, ...) on its context (the q0 loop body of main.f90:552-715 for many
  * inputs at once); no counterpart in the reference, which runs one input per
- * process.  Requests on one context must not overlap in q0. */
+ * process.  Requests on one context must not overlap in q0.  A request on a
+ * two-atom context set to SPRING_BF16 / SPRING_BF16X3 runs through the
+ * tensor-core pass of spring_linewidth3 (same kernel, same results) right
+ * after the graph, inside the same spring_batch_run; path requests
+ * (spring_batch_add_path) are launched inside the graph. */
 typedef struct spring_batch spring_batch;
 int spring_batch_create(spring_batch** batch);
 int spring_batch_destroy(spring_batch* batch);
@@ -359,6 +363,17 @@ int spring_batch_run(spring_batch* batch);
  * P3_q0(Ndof,n_q0) of its context (either may be NULL); device time of the last
  * run in *ms (may be NULL). */
 int spring_batch_result(spring_batch* batch, int index, double* lw, double* p3_q0, double* ms);
+/* Gaussian linewidths at n_path off-grid points of a context, as
+ * spring_linewidth_path(ctx, n_path, q_path, zero_centered, SPRING_DELTA_GAUSS,
+ * sigma, ...) computes them (LineWidth.x path mode, src/LineWidth/Src/main.f90:293-379),
+ * queued in the batch's graph after the persistent kernel.  Its buffers are
+ * allocated at the first spring_batch_run; add a linewidth request first (it
+ * binds the batch's device).  Returns its index among the path requests. */
+int spring_batch_add_path(spring_batch* batch, spring_ctx* ctx, int n_path, const double* q_path,
+                          const int* zero_centered, double sigma, int* index);
+/* lw(Ndof,n_path,n_temps) and omega(Ndof,n_path) of path request `index` after the last run
+ * (either may be NULL). */
+int spring_batch_path_result(spring_batch* batch, int index, double* lw, double* omega);
 
 /* ---- options ----------------------------------------------------------- */
 /* SPRING_OPT_GENERIC_V3 = 1: always use the any-cell V3 kernel (default 0 picks the

@@ -99,6 +99,8 @@ SIGNATURES = {
     "spring_batch_tune": [P, P, P, P],
     "spring_batch_run": [P],
     "spring_batch_result": [P, I, P, P, P],
+    "spring_batch_add_path": [P, P, I, P, P, D, P],
+    "spring_batch_path_result": [P, I, P, P],
 }
 _RESTYPE = {"spring_last_error": ct.c_char_p, "spring_batch_last_error": ct.c_char_p}
 

@@ -463,6 +463,7 @@ class Batch:
             raise SpringError(rc, "spring_batch_create failed")
         self._h = h
         self._reqs = []
+        self._paths = []
 
     def _call(self, name, *args):
         rc = getattr(self._lib, name)(self._h, *args)
@@ -478,6 +479,26 @@ class Batch:
                    ct.byref(idx))
         self._reqs.append((ctx, int(n_q0)))
         return idx.value
+
+    def add_path(self, ctx: Context, q0, zero_centered, sigma: float) -> int:
+        """Queue Gaussian linewidths at off-grid points q0 (n, 3) of ``ctx`` (the path mode of
+        spring_linewidth_path); they run inside the batch's graph.  Returns the path request's index."""
+        q = _c(q0, np.float64).reshape(-1, 3)
+        z = _c(zero_centered, np.int32)
+        idx = ct.c_int()
+        self._call("spring_batch_add_path", ctx._h, int(q.shape[0]), _ptr(q), _ptr(z), float(sigma), ct.byref(idx))
+        self._paths.append((ctx, int(q.shape[0]), q, z))
+        return idx.value
+
+    def path_result(self, index: int):
+        """(lw[T][n][Ndof], omega[n][Ndof]) of path request ``index`` after the last run."""
+        if not 0 <= index < len(self._paths):
+            self._call("spring_batch_path_result", int(index), None, None)  # raises: no such request
+        ctx, n, _, _ = self._paths[index]
+        lw = np.zeros((ctx.n_temps, n, ctx.ndof))
+        om = np.zeros((n, ctx.ndof))
+        self._call("spring_batch_path_result", int(index), _ptr(lw), _ptr(om))
+        return lw, om
 
     def set_config(self, two_atom=1, ctas_per_sm=0, s0_block=0, chunk=1):
         """two_atom: run two-atom cells in the specialised 8-pair layout; ctas_per_sm (0: as many as

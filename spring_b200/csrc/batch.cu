@@ -130,10 +130,22 @@ struct spring_batch {
         double sigma;
         spring::Pol pol;
         long long pairs = 0, items = 0;
-        int kind = 1;
+        int kind = 1;       // 0: two-atom groups, 1: any cell, 2: tensor-core pass (outside the kernel)
         double cost = 0.0;  // per item, for the heaviest-first order
     };
     std::vector<Work> work;
+    // Gaussian linewidths at path points of a context (LineWidth.x path mode), queued in the graph
+    // after the persistent kernel; the plan holds every buffer, allocated at the first run.
+    struct PathReq {
+        spring_ctx* c;
+        int n_path;
+        std::vector<double> q;
+        std::vector<int> zc;
+        double sigma;
+        spring::PathPlan plan;
+        bool ready = false;
+    };
+    std::vector<PathReq> paths;
     std::string err;
     // two-atom group path (1: where the cell fits), CTAs per SM (0: occupancy limit), s0 block for
     // Ndof > 12 (0: 6), work items per scheduler step
@@ -191,6 +203,11 @@ std::string shape_key(const spring_batch* b) {
     return k;
 }
 
+// Requests that the tensor-core pass takes (two-atom cells with at most 8-atom FC3 clusters on a
+// context set to BF16 or BF16x3, as in spring_linewidth3): they run through it, not as items of the
+// persistent FP64 kernel.
+bool tc_request(const spring_ctx* c) { return c->precision != SPRING_FP64 && c->nb == 2 && c->na3 <= 8; }
+
 // Device descriptors of every request for the configuration in b->cfg, in heaviest-first order;
 // returns the shared-memory size, the item offsets and the fold total on the host too.
 int build_desc(spring_batch* b, std::vector<BatchDesc>& D, std::vector<long long>& off, size_t* smem,
@@ -206,7 +223,11 @@ int build_desc(spring_batch* b, std::vector<BatchDesc>& D, std::vector<long long
         if (spring::pairoff_host(c, ps) != SPRING_OK) return bfail(b, SPRING_ERR_CUDA, "%s", c->err.c_str());
         w.pairs = ps.h_pairoff[w.q0 + w.n_q0] - ps.h_pairoff[w.q0];
         w.kind = (b->cfg[0] && c->nb == spring::s3::NB && c->na3 == spring::s3::NA && c->nT <= spring::s3::MAXT) ? 0 : 1;
-        if (w.kind == 0) {
+        if (tc_request(c)) w.kind = 2;
+        if (w.kind == 2) {
+            w.items = 0;  // the tensor-core pass runs it, beside the persistent kernel
+            w.cost = 0.0;
+        } else if (w.kind == 0) {
             w.items = (w.pairs + spring::s3::PP - 1) / spring::s3::PP;
             w.cost = spring::s3::PP * (27.0 * 4 * c->na3 * c->na3 + 8.0 * n * n * n * n);
         } else {
@@ -274,7 +295,7 @@ int build_desc(spring_batch* b, std::vector<BatchDesc>& D, std::vector<long long
         }
         D[k].lw_all = c->d_lw_all.p;
         D[k].fold0 = fold;
-        D[k].fold_n = (long long)c->nT * w.n_q0 * n;
+        D[k].fold_n = w.kind == 2 ? 0 : (long long)c->nT * w.n_q0 * n;  // kind 2 folds after its own pass
         fold += D[k].fold_n;
         off[k + 1] = off[k] + w.items;
     }
@@ -357,18 +378,68 @@ int upload(spring_batch* b, const std::vector<BatchDesc>& D, const std::vector<l
 }
 
 // Order the batch stream after the contexts' streams (and, at the end, the contexts after it).
+int join_ctx_in(spring_batch* b, spring_ctx* c) {
+    if (c->stream == b->stream) return SPRING_OK;
+    BCHECK(bcuda(b, cudaEventRecord(b->ev_sync, c->stream), "batch join"));
+    return bcuda(b, cudaStreamWaitEvent(b->stream, b->ev_sync, 0), "batch join");
+}
+int join_ctx_out(spring_batch* b, spring_ctx* c) {
+    if (c->stream == b->stream) return SPRING_OK;
+    BCHECK(bcuda(b, cudaEventRecord(b->ev_sync, b->stream), "batch join"));
+    return bcuda(b, cudaStreamWaitEvent(c->stream, b->ev_sync, 0), "batch join");
+}
 int join_in(spring_batch* b) {
-    for (const auto& w : b->work)
-        if (w.c->stream != b->stream) {
-            BCHECK(bcuda(b, cudaEventRecord(b->ev_sync, w.c->stream), "batch join"));
-            BCHECK(bcuda(b, cudaStreamWaitEvent(b->stream, b->ev_sync, 0), "batch join"));
-        }
+    for (const auto& w : b->work) BCHECK(join_ctx_in(b, w.c));
+    for (const auto& p : b->paths) BCHECK(join_ctx_in(b, p.c));
     return SPRING_OK;
 }
 int join_out(spring_batch* b) {
-    BCHECK(bcuda(b, cudaEventRecord(b->ev_sync, b->stream), "batch join"));
-    for (const auto& w : b->work)
-        if (w.c->stream != b->stream) BCHECK(bcuda(b, cudaStreamWaitEvent(w.c->stream, b->ev_sync, 0), "batch join"));
+    for (const auto& w : b->work) BCHECK(join_ctx_out(b, w.c));
+    for (const auto& p : b->paths) BCHECK(join_ctx_out(b, p.c));
+    return SPRING_OK;
+}
+
+// Buffers of every path request (once) and the upload of its points.
+int prepare_paths(spring_batch* b) {
+    for (auto& p : b->paths) {
+        if (p.ready) continue;
+        spring::Guard g(p.c->device);
+        const int rc = spring::path_prepare(p.c, p.plan, p.n_path, p.q.data(), p.zc.data());
+        if (rc != SPRING_OK) return bfail(b, rc, "path request: %s", p.c->err.c_str());
+        p.ready = true;
+    }
+    return SPRING_OK;
+}
+
+// The launches of every path request on the batch stream (captured into the graph).
+int enqueue_paths(spring_batch* b) {
+    for (auto& p : b->paths) {
+        spring_ctx* c = p.c;
+        cudaStream_t own = c->stream;
+        const bool prof = c->profiling;
+        c->stream = b->stream;
+        c->profiling = false;  // no per-launch timing events inside the graph
+        const int rc = spring::path_enqueue(c, p.plan, SPRING_DELTA_GAUSS, p.sigma);
+        c->stream = own;
+        c->profiling = prof;
+        if (rc != SPRING_OK) return bfail(b, rc, "path request: %s", c->err.c_str());
+    }
+    return SPRING_OK;
+}
+
+// The tensor-core requests after the graph (which zeroed their scratch): the pass of
+// spring_linewidth3 on each context's stream, then its LW_Allq0 update; the batch stream waits for
+// them.
+int run_tc_requests(spring_batch* b) {
+    for (const auto& w : b->work) {
+        if (w.kind != 2) continue;
+        spring_ctx* c = w.c;
+        BCHECK(join_ctx_out(b, c));
+        int rc = spring::run_v3_gauss(c, w.q0, w.n_q0, w.sigma, w.pol, c->d_lw_tmp.p, c->d_p3.p);
+        if (rc == SPRING_OK) rc = spring::run_axpy_lw(c, 1.0, c->d_lw_tmp.p, c->d_lw_all.p, w.q0, w.n_q0);
+        if (rc != SPRING_OK) return bfail(b, rc, "tensor-core request: %s", c->err.c_str());
+        BCHECK(join_ctx_in(b, c));
+    }
     return SPRING_OK;
 }
 
@@ -412,6 +483,7 @@ int spring_batch_destroy(spring_batch* b) {
         if (b->ev0) cudaEventDestroy(b->ev0);
         if (b->ev1) cudaEventDestroy(b->ev1);
         if (b->ev_sync) cudaEventDestroy(b->ev_sync);
+        for (auto& p : b->paths) spring::path_release(p.plan);
     }
     delete b;
     return SPRING_OK;
@@ -452,6 +524,44 @@ int spring_batch_add_linewidth3(spring_batch* b, spring_ctx* c, int i0_first, in
     drop_graph(b);
     if (index) *index = (int)b->work.size() - 1;
     return SPRING_OK;
+}
+
+int spring_batch_add_path(spring_batch* b, spring_ctx* c, int n_path, const double* q_path, const int* zero_centered,
+                          double sigma, int* index) {
+    if (!b) return SPRING_ERR_ARG;
+    b->err.clear();
+    if (!c) return bfail(b, SPRING_ERR_ARG, "context is NULL");
+    if (b->device < 0) return bfail(b, SPRING_ERR_STATE, "add a linewidth request first (it binds the batch's device)");
+    if (c->device != b->device)
+        return bfail(b, SPRING_ERR_ARG, "context on device %d, batch on device %d", c->device, b->device);
+    if (n_path < 1 || !q_path || !zero_centered) return bfail(b, SPRING_ERR_ARG, "n_path < 1 or NULL points / flags");
+    if (!(sigma > 0.0)) return bfail(b, SPRING_ERR_ARG, "sigma must be > 0");
+    if (!c->fc2_set || !c->fc3_set || !c->mesh_set || !c->ph_grid.set)
+        return bfail(b, SPRING_ERR_STATE, "the context needs FC2, FC3, the mesh and the grid phonons");
+    if (!c->mesh_zc) return bfail(b, SPRING_ERR_STATE, "the path mode needs the zero-centred mesh");
+    if (c->nT > 9) return bfail(b, SPRING_ERR_UNSUPPORTED, "the path mode handles at most 9 temperatures");
+    spring_batch::PathReq r;
+    r.c = c;
+    r.n_path = n_path;
+    r.q.assign(q_path, q_path + 3 * (size_t)n_path);
+    r.zc.assign(zero_centered, zero_centered + n_path);
+    r.sigma = sigma;
+    b->paths.push_back(std::move(r));
+    drop_graph(b);
+    if (index) *index = (int)b->paths.size() - 1;
+    return SPRING_OK;
+}
+
+int spring_batch_path_result(spring_batch* b, int index, double* lw, double* omega) {
+    if (!b) return SPRING_ERR_ARG;
+    b->err.clear();
+    if (index < 0 || index >= (int)b->paths.size()) return bfail(b, SPRING_ERR_ARG, "no path request %d", index);
+    auto& p = b->paths[index];
+    if (!p.ready || !b->exec) return bfail(b, SPRING_ERR_STATE, "the batch has not run");
+    spring::Guard g(b->device);
+    BCHECK(join_ctx_out(b, p.c));  // the context's stream follows the batch's last run
+    const int rc = spring::path_fetch(p.c, p.plan, lw, omega);
+    return rc == SPRING_OK ? SPRING_OK : bfail(b, rc, "%s", p.c->err.c_str());
 }
 
 int spring_batch_set_config(spring_batch* b, const int* config) {
@@ -533,6 +643,7 @@ int spring_batch_run(spring_batch* b) {
     if (b->work.empty()) return bfail(b, SPRING_ERR_STATE, "the batch holds no requests");
     spring::Guard g(b->device);
     BCHECK(prepare(b));
+    BCHECK(prepare_paths(b));
     // a tuned configuration of the same shape, if this batch has not been configured otherwise
     if (b->cfg[0] == 1 && b->cfg[1] == 0 && b->cfg[2] == 0 && b->cfg[3] == 1) {
         std::vector<BatchDesc> D0;
@@ -559,10 +670,15 @@ int spring_batch_run(spring_batch* b) {
     key.push_back(fold_total);
     key.push_back((long long)reinterpret_cast<uintptr_t>(b->d_desc));
     key.insert(key.end(), off.begin(), off.end());
+    for (const auto& p : b->paths) key.push_back((long long)reinterpret_cast<uintptr_t>(p.plan.lw.p));
     if (!b->exec || key != b->graph_key) {
         drop_graph(b);
+        // one run of the path launches outside the capture, so that whatever they allocate or set
+        // on first use is in place before it
+        if (!b->paths.empty()) BCHECK(enqueue_paths(b));
         BCHECK(bcuda(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal), "batch capture"));
-        const int rc = enqueue(b, D, off, smem, fold_total, true);
+        int rc = enqueue(b, D, off, smem, fold_total, true);
+        if (rc == SPRING_OK) rc = enqueue_paths(b);
         cudaGraph_t graph = nullptr;
         const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
         if (rc != SPRING_OK) {
@@ -576,8 +692,9 @@ int spring_batch_run(spring_batch* b) {
     }
     BCHECK(bcuda(b, cudaEventRecord(b->ev0, b->stream), "batch timing"));
     BCHECK(bcuda(b, cudaGraphLaunch(b->exec, b->stream), "batch graph launch"));
-    BCHECK(bcuda(b, cudaEventRecord(b->ev1, b->stream), "batch timing"));
     b->work[0].c->launches += 2;
+    BCHECK(run_tc_requests(b));
+    BCHECK(bcuda(b, cudaEventRecord(b->ev1, b->stream), "batch timing"));
     BCHECK(join_out(b));
     BCHECK(bcuda(b, cudaEventSynchronize(b->ev1), "batch run"));
     float t = 0.0f;

@@ -399,19 +399,10 @@ int path_points(const double* G, int n_nodes, const double* qhs, double* qpoints
     return sp;
 }
 
-int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
-             double* h_lw, double* h_omega) {
-    const int n = c->ndof, nq = c->nq;
-    const size_t n3 = (size_t)n * n * n;
-    // slots: path points per batch (W grid + q2 phonons of a slot)
-    const size_t per_slot = (size_t)nq * (n3 * sizeof(double) + (size_t)n * n * sizeof(double2) +
-                                          (size_t)n * sizeof(double) * (6 + c->nT) + 8 * sizeof(double));
-    const size_t budget = (size_t)512 << 20;
-    const int slots = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_path, budget / per_slot));
-    const long long rows_max = (long long)slots * nq;
-
+namespace {
+PathQ2Args path_q2_args(spring_ctx* c) {
     PathQ2Args qa{};
-    qa.nq = nq;
+    qa.nq = c->nq;
     qa.n0 = c->mesh[0];
     qa.n1 = c->mesh[1];
     qa.n2 = c->mesh[2];
@@ -422,27 +413,52 @@ int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int
         }
     for (int k = 0; k < 3; ++k) qa.shift[k] = (double)c->mesh_shift[k] * 0.5;
     lu3(c->G, qa.lu, qa.piv);
+    return qa;
+}
+}  // namespace
 
-    DBuf<double> q0v, q1v, q2v, w, lw, p3;
-    DBuf<int> zc, ex;
-    Phonons php, ph2;
-    int rc = SPRING_OK;
-    auto step = [&](int r) { if (rc == SPRING_OK) rc = r; };
-    step(dalloc(c, q0v, (size_t)3 * n_path, "path q0"));
-    step(dalloc(c, zc, (size_t)n_path, "path flags"));
-    step(dalloc(c, q1v, (size_t)3 * rows_max, "path q1"));
-    step(dalloc(c, q2v, (size_t)3 * rows_max, "path q2"));
-    step(dalloc(c, ex, (size_t)rows_max, "path q2 flags"));
-    step(dalloc(c, w, (size_t)rows_max * n3, "path W"));
-    step(dalloc(c, lw, (size_t)c->nT * n_path * n, "path linewidth"));
-    step(dalloc(c, p3, (size_t)n_path * n, "path scratch"));
-    step(alloc_phonons(c, php, n_path));
-    step(alloc_phonons(c, ph2, (int)rows_max));
-    if (rc == SPRING_OK) rc = h2d(c, q0v.p, h_q0, sizeof(double) * 3 * n_path, "path q0");
-    if (rc == SPRING_OK) rc = h2d(c, zc.p, h_zc, sizeof(int) * n_path, "path flags");
-    if (rc == SPRING_OK) rc = zero(c, lw.p, sizeof(double) * c->nT * n_path * n, "path linewidth");
-    if (rc == SPRING_OK) rc = run_phonons(c, php, q0v.p, n_path);
+void path_release(PathPlan& p) {
+    dfree(p.q0v); dfree(p.q1v); dfree(p.q2v); dfree(p.w); dfree(p.lw); dfree(p.p3); dfree(p.zc); dfree(p.ex);
+    free_phonons(p.php);
+    free_phonons(p.ph2);
+    p.n_path = 0;
+    p.slots = 0;
+}
 
+int path_prepare(spring_ctx* c, PathPlan& p, int n_path, const double* h_q0, const int* h_zc) {
+    const int n = c->ndof, nq = c->nq;
+    const size_t n3 = (size_t)n * n * n;
+    // slots: path points per batch (W grid + q2 phonons of a slot)
+    const size_t per_slot = (size_t)nq * (n3 * sizeof(double) + (size_t)n * n * sizeof(double2) +
+                                          (size_t)n * sizeof(double) * (6 + c->nT) + 8 * sizeof(double));
+    const size_t budget = (size_t)512 << 20;
+    p.n_path = n_path;
+    p.slots = (int)std::max<size_t>(1, std::min<size_t>((size_t)n_path, budget / per_slot));
+    const long long rows_max = (long long)p.slots * nq;
+    SPRING_CHECK(dalloc(c, p.q0v, (size_t)3 * n_path, "path q0"));
+    SPRING_CHECK(dalloc(c, p.zc, (size_t)n_path, "path flags"));
+    SPRING_CHECK(dalloc(c, p.q1v, (size_t)3 * rows_max, "path q1"));
+    SPRING_CHECK(dalloc(c, p.q2v, (size_t)3 * rows_max, "path q2"));
+    SPRING_CHECK(dalloc(c, p.ex, (size_t)rows_max, "path q2 flags"));
+    SPRING_CHECK(dalloc(c, p.w, (size_t)rows_max * n3, "path W"));
+    SPRING_CHECK(dalloc(c, p.lw, (size_t)c->nT * n_path * n, "path linewidth"));
+    SPRING_CHECK(dalloc(c, p.p3, (size_t)n_path * n, "path scratch"));
+    SPRING_CHECK(alloc_phonons(c, p.php, n_path));
+    SPRING_CHECK(alloc_phonons(c, p.ph2, (int)rows_max));
+    SPRING_CHECK(h2d(c, p.q0v.p, h_q0, sizeof(double) * 3 * n_path, "path q0"));
+    SPRING_CHECK(h2d(c, p.zc.p, h_zc, sizeof(int) * n_path, "path flags"));
+    const size_t smem = v3p_smem(n, c->na3, n <= 12 ? n : 6);
+    if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "path V3 tile needs %zu bytes of shared memory", smem);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_v3_path, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return SPRING_OK;
+}
+
+int path_enqueue(spring_ctx* c, PathPlan& p, int delta_mode, double sigma) {
+    const int n = c->ndof, nq = c->nq, n_path = p.n_path;
+    const size_t n3 = (size_t)n * n * n;
+    const PathQ2Args qa0 = path_q2_args(c);
+    SPRING_CHECK(zero(c, p.lw.p, sizeof(double) * c->nT * n_path * n, "path linewidth"));
+    SPRING_CHECK(run_phonons(c, p.php, p.q0v.p, n_path));
     V3PArgs va{};
     va.nb = c->nb;
     va.n = n;
@@ -453,54 +469,63 @@ int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int
     va.nqd = double(nq);
     va.sctr = host_constants().Sctr3THz2;
     const size_t smem = v3p_smem(n, c->na3, va.sb);
-    if (rc == SPRING_OK && smem > 227 * 1024)
-        rc = fail(c, SPRING_ERR_UNSUPPORTED, "path V3 tile needs %zu bytes of shared memory", smem);
-    if (rc == SPRING_OK && smem > 48 * 1024)
-        cudaFuncSetAttribute(k_v3_path, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-
-    for (int p0 = 0; rc == SPRING_OK && p0 < n_path; p0 += slots) {
-        const int ns = std::min(slots, n_path - p0);
+    for (int p0 = 0; p0 < n_path; p0 += p.slots) {
+        const int ns = std::min(p.slots, n_path - p0);
         const long long rows = (long long)ns * nq;
+        PathQ2Args qa = qa0;
         qa.p_first = p0;
         const int threads = 128;
         const int blocks = (int)std::min<long long>((rows + threads - 1) / threads, 148LL * 32);
-        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
-        k_path_q2<<<blocks, threads, 0, c->stream>>>(qa, ns, q0v.p, zc.p, c->d_qpnt.p, q1v.p, q2v.p, ex.p);
-        if ((rc = launch_check(c, "k_path_q2")) != SPRING_OK) break;
-        if ((rc = run_phonons(c, ph2, q2v.p, (int)rows, 1)) != SPRING_OK) break;  // single points (get_phonon_singleq)
-        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
-        k_path_clear_missing<<<blocks, threads, 0, c->stream>>>(rows, n, c->nT, ex.p, ph2.omega.p, ph2.nbe.p);
-        if ((rc = launch_check(c, "k_path_clear_missing")) != SPRING_OK) break;
-        if ((rc = zero(c, w.p, sizeof(double) * rows * n3, "path W")) != SPRING_OK) break;
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "path: injected launch failure");
+        k_path_q2<<<blocks, threads, 0, c->stream>>>(qa, ns, p.q0v.p, p.zc.p, c->d_qpnt.p, p.q1v.p, p.q2v.p, p.ex.p);
+        SPRING_CHECK(launch_check(c, "k_path_q2"));
+        SPRING_CHECK(run_phonons(c, p.ph2, p.q2v.p, (int)rows, 1));  // single points (get_phonon_singleq)
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "path: injected launch failure");
+        k_path_clear_missing<<<blocks, threads, 0, c->stream>>>(rows, n, c->nT, p.ex.p, p.ph2.omega.p, p.ph2.nbe.p);
+        SPRING_CHECK(launch_check(c, "k_path_clear_missing"));
+        SPRING_CHECK(zero(c, p.w.p, sizeof(double) * rows * n3, "path W"));
         va.p_first = p0;
-        if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "path: injected launch failure");
         k_v3_path<<<dim3((unsigned)(nq * va.nsb), ns), 128, smem, c->stream>>>(
-            va, ex.p, q0v.p, q1v.p, q2v.p, c->d_qint.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p, c->d_mass_rs.p,
-            php.evec.p, php.omega.p, c->ph_grid.evec.p, c->ph_grid.omega.p, ph2.evec.p, ph2.omega.p, w.p);
-        if ((rc = launch_check(c, "k_v3_path")) != SPRING_OK) break;
+            va, p.ex.p, p.q0v.p, p.q1v.p, p.q2v.p, c->d_qint.p, c->d_fc3.p, c->d_fc3_posr.p, c->d_fc3_btyp.p,
+            c->d_mass_rs.p, p.php.evec.p, p.php.omega.p, c->ph_grid.evec.p, c->ph_grid.omega.p, p.ph2.evec.p,
+            p.ph2.omega.p, p.w.p);
+        SPRING_CHECK(launch_check(c, "k_v3_path"));
         if (delta_mode == SPRING_DELTA_TETRA) {
-            rc = run_tetra3_path(c, p0, ns, n_path, w.p, php.omega.p, ph2.omega.p, ph2.nbe.p, rows, lw.p, p3.p);
+            SPRING_CHECK(run_tetra3_path(c, p0, ns, n_path, p.w.p, p.php.omega.p, p.ph2.omega.p, p.ph2.nbe.p, rows,
+                                         p.lw.p, p.p3.p));
         } else {
             const double os = 1.0 / sigma;
             dim3 grid((unsigned)std::max(1, std::min((nq + 127) / 128, 64)), n, ns);
-            if (launch_injected(c)) { rc = fail(c, SPRING_ERR_INJECTED, "path: injected launch failure"); break; }
+            if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "path: injected launch failure");
 #define SPRING_GAUSS_PATH(NTM)                                                                                    \
-    k_gauss_path<NTM><<<grid, 128, 0, c->stream>>>(n, nq, n_path, p0, c->nT, rows, os, os * os, ex.p, c->d_qint.p, \
-                                                   w.p, php.omega.p, c->ph_grid.omega.p, c->ph_grid.nbe.p,       \
-                                                   ph2.omega.p, ph2.nbe.p, lw.p)
+    k_gauss_path<NTM><<<grid, 128, 0, c->stream>>>(n, nq, n_path, p0, c->nT, rows, os, os * os, p.ex.p, c->d_qint.p, \
+                                                   p.w.p, p.php.omega.p, c->ph_grid.omega.p, c->ph_grid.nbe.p,   \
+                                                   p.ph2.omega.p, p.ph2.nbe.p, p.lw.p)
             if (c->nT == 1) SPRING_GAUSS_PATH(1);
             else if (c->nT <= 3) SPRING_GAUSS_PATH(3);
             else SPRING_GAUSS_PATH(9);
 #undef SPRING_GAUSS_PATH
-            rc = launch_check(c, "k_gauss_path");
+            SPRING_CHECK(launch_check(c, "k_gauss_path"));
         }
     }
-    if (rc == SPRING_OK && h_lw) rc = d2h(c, h_lw, lw.p, sizeof(double) * c->nT * n_path * n, "path linewidth");
-    if (rc == SPRING_OK && h_omega) rc = d2h(c, h_omega, php.omega.p, sizeof(double) * n_path * n, "path omega");
+    return SPRING_OK;
+}
+
+int path_fetch(spring_ctx* c, PathPlan& p, double* h_lw, double* h_omega) {
+    if (h_lw) SPRING_CHECK(d2h(c, h_lw, p.lw.p, sizeof(double) * c->nT * p.n_path * c->ndof, "path linewidth"));
+    if (h_omega) SPRING_CHECK(d2h(c, h_omega, p.php.omega.p, sizeof(double) * p.n_path * c->ndof, "path omega"));
+    return SPRING_OK;
+}
+
+int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
+             double* h_lw, double* h_omega) {
+    PathPlan p;
+    int rc = path_prepare(c, p, n_path, h_q0, h_zc);
+    if (rc == SPRING_OK) rc = path_enqueue(c, p, delta_mode, sigma);
+    if (rc == SPRING_OK) rc = path_fetch(c, p, h_lw, h_omega);
     cudaStreamSynchronize(c->stream);
-    dfree(q0v); dfree(q1v); dfree(q2v); dfree(w); dfree(lw); dfree(p3); dfree(zc); dfree(ex);
-    free_phonons(php);
-    free_phonons(ph2);
+    path_release(p);
     return rc;
 }
 

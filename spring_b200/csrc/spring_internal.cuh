@@ -365,6 +365,19 @@ int run_v4tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const in
 // k_path.cu: LineWidth.x path mode; h_q0 (3, n_path) Cartesian, h_lw [T][p][s], h_omega [p][s]
 int run_path(spring_ctx* c, int n_path, const double* h_q0, const int* h_zc, int delta_mode, double sigma,
              double* h_lw, double* h_omega);
+// The same in three steps: path_prepare allocates every buffer of the run and uploads the points;
+// path_enqueue queues its launches and memsets on c->stream (no allocation, copy from the host or
+// wait on the host, so a stream capture may record it); path_fetch copies the results back.
+struct PathPlan {
+    int n_path = 0, slots = 0;
+    DBuf<double> q0v, q1v, q2v, w, lw, p3;
+    DBuf<int> zc, ex;
+    Phonons php, ph2;
+};
+int path_prepare(spring_ctx* c, PathPlan& p, int n_path, const double* h_q0, const int* h_zc);
+int path_enqueue(spring_ctx* c, PathPlan& p, int delta_mode, double sigma);
+int path_fetch(spring_ctx* c, PathPlan& p, double* h_lw, double* h_omega);
+void path_release(PathPlan& p);
 int path_points(const double* G, int n_nodes, const double* q_high_sym, double* qpoints, double* dist, int* zc);
 // k_mlp.cu: the surrogate network (row-major X[n][SPRING_MLP_INPUTS], y[n])
 int mlp_num_params();

@@ -132,3 +132,58 @@ def test_batch_argument_errors():
     b.close()
     ctx8.close()
     ctx.close()
+
+
+def test_batch_tensor_core_requests_and_path_points():
+    """A batch mixing a two-atom context set to BF16x3 (run through the tensor-core pass), an FP64
+    8-atom context (persistent kernel) and Gaussian path points (launched inside the graph): every
+    result equals the context's own single call, on the first run and on a graph replay."""
+    cr2, cr8 = S.build("rocksalt2"), S.build("rocksalt8")
+    st2 = D.Setup(cr2, (6, 6, 6), [100.0, 300.0, 700.0])
+    ctx2, _ = from_crystal(cr2, (6, 6, 6), st2.temps, phonons={"grid": st2.ph, "irr": st2.ph0})
+    st8 = D.Setup(cr8, (2, 2, 2), [300.0])
+    ctx8, _ = from_crystal(cr8, (2, 2, 2), st8.temps, phonons={"grid": st8.ph, "irr": st8.ph0})
+    ctx2.set_precision("bf16x3")
+    path = np.array([[0.11, 0.23, 0.37, 0], [0.31, 0.17, 0.05, 5]])
+    q, _, z = ctx2.path_qpoints(path)
+    singles = []
+    for ctx in (ctx2, ctx8):
+        ctx.reset_linewidths()
+        singles.append(ctx.linewidth3(1, ctx.nq0, "gauss", SIGMA))
+    lw_path, om_path = ctx2.linewidth_path(q, z, delta="gauss", sigma=SIGMA)
+    b = Batch()
+    i2 = b.add_linewidth3(ctx2, 1, ctx2.nq0, SIGMA)
+    i8 = b.add_linewidth3(ctx8, 1, ctx8.nq0, SIGMA)
+    ip = b.add_path(ctx2, q, z, SIGMA)
+    for rep in range(2):
+        for ctx in (ctx2, ctx8):
+            ctx.reset_linewidths()
+        b.run()
+        for i, ctx, (lw_ref, p3_ref) in ((i2, ctx2, singles[0]), (i8, ctx8, singles[1])):
+            lw, p3, _ = b.result(i)
+            _close(lw, lw_ref, 1e-11)
+            _close(p3, p3_ref, 1e-11)
+            _close(ctx.get_linewidths(), lw_ref, 1e-11)
+        lwp, omp = b.path_result(ip)
+        _close(lwp, lw_path, 1e-11)
+        np.testing.assert_array_equal(omp, om_path)
+    b.close()
+    ctx2.close()
+    ctx8.close()
+
+
+def test_batch_path_request_errors():
+    cr = S.build("rocksalt2")
+    ctx, _ = from_crystal(cr, (3, 3, 3), [300.0])
+    q = np.zeros((1, 3))
+    z = np.ones(1, dtype=np.int32)
+    b = Batch()
+    with pytest.raises(SpringError):
+        b.add_path(ctx, q, z, SIGMA)  # no linewidth request has bound the device yet
+    b.add_linewidth3(ctx, 1, 1, SIGMA)
+    with pytest.raises(SpringError):
+        b.add_path(ctx, q, z, -1.0)
+    with pytest.raises(SpringError):
+        b.path_result(0)  # no such request
+    b.close()
+    ctx.close()
