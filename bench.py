@@ -115,8 +115,8 @@ def measured_peaks():
 
 # DRAM bytes per tiled pair of the tensor-core pass (read + write), from one ncu capture of the
 # 16^3 rocksalt launch (140,383 of its 297,076 pairs have a mode triple inside the delta window and
-# are tiled; 61.7 MB read, 17.9 MB written)
-TC_DRAM_BYTES_PER_TILED_PAIR = (61.688320e6 + 17.917696e6) / 140383
+# are tiled; 61.0 MB read, 0.68 MB written: the operand tables and mode records in, the sums out)
+TC_DRAM_BYTES_PER_TILED_PAIR = (60.978176e6 + 0.677120e6) / 140383
 
 
 def tc_issued_flops_per_tile(passes):
