@@ -488,10 +488,14 @@ def surrogate_c5_leg(torch, train_mesh=12, mesh=20, frac=0.25, members=3):
 
 def bte_c2_leg(torch, ctx, mesh):
     """Iterative (non-RTA) kappa of the benchmark context (mesh^3, T = 100/300/700 K) to the
-    tolerance 1e-6, in the Gaussian operator form (delta weights of width SIGMA, FP64 throughout).
-    First call: time-reversal pairs, operator build (FP64 V3 of every pair, the entries inside the
-    delta window, row sort) and the iterations; then the iterations alone on the kept operator,
-    and the operator pass's achieved HBM bandwidth."""
+    tolerance 1e-6, in the Gaussian operator form (delta weights of width SIGMA).  FP64 operator:
+    first call (time-reversal pairs, operator build with the FP64 V3 of every pair, the entries
+    inside the delta window, row sort, iterations), then the iterations alone on the kept operator,
+    and the operator pass's achieved HBM bandwidth.  Then the same with the operator entries from
+    the BF16x3 tensor-core pass (the iterations, deltas and occupations stay FP64), against the
+    FP64 operator's kappa."""
+    prec = ctx.precision
+    ctx.set_precision("fp64")
     r1, first_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
     r2, iter_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
     ctx.set_profiling(True)
@@ -505,7 +509,20 @@ def bte_c2_leg(torch, ctx, mesh):
     bytes_pass = E * (8 + 8) + ntr_rows * (4 + 24)
     per_ms = rows_ms / rows_n if rows_n else None
     peaks = measured_peaks()
+    ctx.set_precision("bf16x3")
+    t1, tc_first_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
+    t2, tc_iter_ms = _ev_ms(torch, lambda: ctx.kappa_iter_gauss(SIGMA, eps_k=1e-6))
+    ctx.set_precision(prec)
+    kerr = float(np.abs(t1["kappa"] - r2["kappa"]).max() / np.abs(r2["kappa"]).max())
+    kerr0 = float(np.abs(t1["kappa_rta"] - r2["kappa_rta"]).max() / np.abs(r2["kappa_rta"]).max())
+    tc = {"first_call_ms": tc_first_ms, "iterations_only_ms": tc_iter_ms, "operator_entries": t1["entries"],
+          "iterations": t1["iters"].tolist(), "first_call_fp64_over_this": first_ms / tc_first_ms,
+          "kappa_max_rel_diff_vs_fp64_operator": kerr, "kappa_rta_max_rel_diff_vs_fp64_operator": kerr0,
+          "kappa_diag": [_kdiag(k).tolist() for k in t1["kappa"]],
+          "what": "operator entries from the tensor-core V3 pass (BF16x3) over the time-reversal pairs, "
+                  "window and cuts as in FP64; the same FP64 iterations"}
     return {"mesh": [mesh] * 3, "temperatures": TEMPS, "sigma_rad_ps": SIGMA, "eps_k": 1e-6,
+            "tensor_core_operator": tc,
             "operator_entries": E, "pairs": r2["pairs"], "iterations": r2["iters"].tolist(),
             "converged": bool((r2["iters"] <= 1000).all()),
             "first_call_ms": first_ms, "iterations_only_ms": iter_ms,

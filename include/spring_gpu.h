@@ -317,6 +317,9 @@ int spring_kappa_iter(spring_ctx* ctx, double eps_k, int max_iter, double* kappa
  * operator (one entry per pair and mode triple inside the exp(-40) window) is built once
  * on the device, sorted by row and kept until sigma, FC3 or the phonons change; every
  * iteration is then one pass over it.  Two-atom cells with 7-atom FC3 clusters.
+ * On a context set to SPRING_BF16 / SPRING_BF16X3 the operator entries come
+ * from the tensor-core V3 pass (same window and cuts; |Phi|^2 in compensated
+ * BF16), the iterations stay FP64.
  * stats(2) optional: number of operator entries, number of enumerated pairs. */
 int spring_kappa_iter_gauss(spring_ctx* ctx, double sigma, double eps_k, int max_iter, double* kappa,
                             double* kappa_rta, int* iters, double* stats);

@@ -98,6 +98,12 @@ class Context:
         """"fp64" (default), "bf16" or "bf16x3": arithmetic of the Gaussian V3 and V4 contractions."""
         code = {"fp64": L.SPRING_FP64, "bf16": L.SPRING_BF16, "bf16x3": L.SPRING_BF16X3}[precision]
         self._call("spring_set_precision", code)
+        self._precision = precision
+
+    @property
+    def precision(self) -> str:
+        """The arithmetic last set with set_precision ("fp64" until then)."""
+        return getattr(self, "_precision", "fp64")
 
     # -- surrogate network (no counterpart in the reference)
     def mlp_init(self, seed: int = 0):

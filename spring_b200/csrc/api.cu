@@ -332,7 +332,7 @@ int spring_ctx_destroy(spring_ctx* c) {
         dfree(c->pd.vfc); dfree(c->pd.vm); dfree(c->pd.qpnt); dfree(c->pd.w2); dfree(c->pd.qint); dfree(c->pd.tet);
         dfree(c->pd.inc); dfree(c->pd.gamma0); dfree(c->pd.wgt); dfree(c->pd.G); dfree(c->pd.te0);
         free_phonons(c->pd.ph);
-        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries);
+        dfree(c->d_tc_a); dfree(c->d_tc_b); dfree(c->d_tc_q0); dfree(c->d_tc_modes); dfree(c->d_tc_cnt_cta); dfree(c->d_scr_sum); dfree(c->d_kap_part); dfree(c->d_scr_rot); dfree(c->d_scr_map); dfree(c->d_tc_entries); dfree(c->d_tr_ev); dfree(c->d_tr_om); dfree(c->d_tr_ob);
         dfree(c->d_tc_rec); dfree(c->d_tc_tiles);
         free_mlp(c->mlp);
         dfree(c->d_scr_rep); dfree(c->d_tc_keys); dfree(c->d_tc_keys_s); dfree(c->d_tc_vals); dfree(c->d_tc_cnt);

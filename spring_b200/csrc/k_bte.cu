@@ -376,7 +376,8 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
     const int threads = 256;
     auto blocks_for = [&](long long m) { return (int)std::max<long long>(1, std::min<long long>((m + threads - 1) / threads, 148LL * 16)); };
     // ---- the operator: entries, sorted by row (kept until sigma, the phonons or the pairs change)
-    if (!(c->bteg_sigma == sigma && c->bteg_gen == c->ph_gen && c->bteg_pairs == c->ps_tr.gen && c->bteg_n > 0)) {
+    if (!(c->bteg_sigma == sigma && c->bteg_gen == c->ph_gen && c->bteg_pairs == c->ps_tr.gen && c->bteg_n > 0 &&
+          c->bteg_prec == c->precision)) {
         c->bteg_n = 0;
         DBuf<s3::BteEntry> ent;
         DBuf<unsigned long long> ctr;
@@ -387,7 +388,10 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
             int rc = dalloc(c, ent, (size_t)cap, "BTE operator entries");
             if (rc == SPRING_OK) rc = zero(c, ctr.p, sizeof(unsigned long long), "operator count");
             bool handled = false;
-            if (rc == SPRING_OK) rc = launch_v3s_bte(c, c->ps_tr, view, 0, ntr, sigma, ent.p, ctr.p, cap, &handled);
+            // BF16 / BF16x3 contexts: the tensor-core pass writes the entries; FP64: the FP64 pass
+            if (rc == SPRING_OK) rc = run_v3tc_bte(c, 0, ntr, sigma, ent.p, ctr.p, cap, &handled);
+            if (rc == SPRING_OK && !handled)
+                rc = launch_v3s_bte(c, c->ps_tr, view, 0, ntr, sigma, ent.p, ctr.p, cap, &handled);
             unsigned long long h = 0;
             if (rc == SPRING_OK) rc = d2h(c, &h, ctr.p, sizeof h, "operator count");
             if (rc != SPRING_OK) { dfree(ent); dfree(ctr); return rc; }
@@ -441,6 +445,7 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
         c->bteg_sigma = sigma;
         c->bteg_gen = c->ph_gen;
         c->bteg_pairs = c->ps_tr.gen;
+        c->bteg_prec = c->precision;
     }
     const long long cnt = c->bteg_n;
     if (h_stats) {

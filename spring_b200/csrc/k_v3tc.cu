@@ -317,6 +317,8 @@ __global__ void k_tc_entrec(int n, int nq, const int* __restrict__ entries, cons
 // ------------------------------------------------------------------ main kernels
 struct TcArgs {
     int nq, nq0, nT, ntiles, tiles_per_cta, rs;
+    int q0_first;            // first q0 of the block (operator rows are counted from it)
+    long long bte_cap;       // operator entries the output holds (entry mode)
     int lo[3], hi[3];
     double half_os2, pre, mfac;
     float rf;             // delta window of the FP32 screen (tc_window)
@@ -334,6 +336,14 @@ struct TcStage {
     int k0, k1, k2;
 };
 constexpr int STG_CAP = 128;  // staged triples per epilogue warp: 32 + up to 96 from one chunk
+
+// One entry of the Gaussian iterative-BTE operator (row r0 = (q0 - q0_first) * 6 + s0, grid modes
+// k1, k2; c = (n1 - n2) P + (1 + n1 + n2) Q), in the layout the operator sort reads.
+struct TcBteEntry {
+    int r0, k1, k2, pad;
+    double P, Q;
+};
+static_assert(sizeof(TcBteEntry) == 32, "operator entry");
 
 struct OpStage {
     alignas(128) uint8_t A[2][EPT * 1536];    // [hi, lo]: per pair its two mu images (pair stride 1536)
@@ -369,11 +379,58 @@ constexpr int NT_FAST = 4;  // mode records of 8 doubles carry the occupations o
 // P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].  The q0 record
 // (omega, 1/omega) and the mode records (omega, 1/omega, nBE[T]) of q1 and q2 are read whole, so
 // a triple needs one memory round trip.  FAST: records of 8 doubles, n_temps <= 4.
-template <bool FAST>
+template <bool FAST, int MODE>
 __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
                                       double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
-                                      double* out_lw, double* out_p3) {
+                                      double* out_lw, double* out_p3, TcBteEntry* bte, unsigned long long* bte_ctr,
+                                      long long bte_cap, int q0_first) {
     const int lane = threadIdx.x & 31;
+    if (MODE == 1) {
+        // operator entries: P = 4 W (g(w0 + w1 - w2) - g(w0 + w2 - w1)), Q = 4 W g(w0 - w1 - w2), the
+        // second term of P dropped and Q halved when q1 = q2; one entry per triple with P or Q nonzero
+        double Pv = 0.0, Qv = 0.0;
+        TcStage s{};
+        if (lane < n) {
+            s = st[lane];
+            const int o = s.k0 & 0x1fffffff;
+            const double2 r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
+            const double2 a = *reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
+            const double2 b = *reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
+            if (!((s.k0 >> 29) & 1)) {
+                const double w0 = r0.x, w1 = a.x, w2 = b.x;
+                const double dm = w0 - w1 - w2, da = w0 + w1 - w2, db = w0 - w1 + w2;
+                const double xm = half_os2 * (dm * dm), xa = half_os2 * (da * da), xb = half_os2 * (db * db);
+                const double gm = exp(-fmin(xm, EXP_CUT)), ga = exp(-fmin(xa, EXP_CUT)), gb = exp(-fmin(xb, EXP_CUT));
+                const bool self = !((s.k0 >> 30) & 1);
+                const double em = xm < EXP_CUT ? pre * gm : 0.0;
+                const double ea = xa < EXP_CUT ? pre * ga : 0.0;
+                const double eb = (!self && xb < EXP_CUT) ? pre * gb : 0.0;
+                const double W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac;
+                Pv = 4.0 * W * (ea - eb);
+                Qv = 4.0 * W * (self ? 0.5 : 1.0) * em;
+            }
+        }
+        const bool has = Pv != 0.0 || Qv != 0.0;
+        const unsigned bal = __ballot_sync(0xffffffffu, has);
+        unsigned long long base = 0;
+        if (lane == 0 && bal != 0u) base = atomicAdd(bte_ctr, (unsigned long long)__popc(bal));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (has) {
+            const unsigned long long pos = base + (unsigned long long)__popc(bal & ((1u << lane) - 1u));
+            if ((long long)pos < bte_cap) {
+                TcBteEntry e;
+                e.r0 = (s.k0 & 0x1fffffff) - q0_first * NMODE;
+                e.k1 = s.k1;
+                e.k2 = s.k2;
+                e.pad = 0;
+                e.P = Pv;
+                e.Q = Qv;
+                bte[pos] = e;
+            }
+        }
+        __syncwarp();
+        return;
+    }
     if (lane < n) {
         const TcStage s = st[lane];
         const int o = s.k0 & 0x1fffffff;
@@ -435,12 +492,14 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
 // row in FP32 against the delta window, forms |Phi|^2 of the active ones (about 1-3 %) from the
 // stage's q0 records, stages them in its shared-memory buffer, releases the stage, and evaluates
 // the FP64 delta weights and sums of the staged triples 32 at a time, one per lane (tc_drain).
-template <bool SPLIT, bool FAST>
+// MODE 0: linewidth and phase-space sums; MODE 1: entries of the iterative-BTE operator.
+template <bool SPLIT, bool FAST, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict__ tiles, const int4* __restrict__ entrec,
        const __nv_bfloat16* __restrict__ tabB, const double* __restrict__ om0, const double* __restrict__ omg,
        const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes, double* __restrict__ out_lw,
-       double* __restrict__ out_p3, int* __restrict__ err) {
+       double* __restrict__ out_p3, TcBteEntry* __restrict__ bte, unsigned long long* __restrict__ bte_ctr,
+       int* __restrict__ err) {
     extern __shared__ __align__(128) uint8_t smraw[];
     TcSmem& S = *reinterpret_cast<TcSmem*>(smraw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -779,8 +838,8 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
                     const int nc = __popc(b0) + 2 * __popc(b1);
                     while (count + nc > STG_CAP) {
                         count -= 32;
-                        tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes,
-                                       out_lw, out_p3);
+                        tc_drain<FAST, MODE>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes,
+                                       out_lw, out_p3, bte, bte_ctr, a.bte_cap, a.q0_first);
                     }
                     stage_bits(m, count + __popc(b0 & lt) + 2 * __popc(b1 & lt));
                     count += nc;
@@ -793,12 +852,12 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
             while (count >= 32) {
                 count -= 32;
-                tc_drain<FAST>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
-                               out_p3);
+                tc_drain<FAST, MODE>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
+                               out_p3, bte, bte_ctr, a.bte_cap, a.q0_first);
             }
         }
         if (count > 0)
-            tc_drain<FAST>(stg, count, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw, out_p3);
+            tc_drain<FAST, MODE>(stg, count, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw, out_p3, bte, bte_ctr, a.bte_cap, a.q0_first);
     }
     // Every role has left its loop (each of its waits is bounded).  After a time-out copies may be
     // in flight into shared memory, unconsumed: the copy warp's operand copies of up to NOP tiles
@@ -849,17 +908,33 @@ int make_tmap_a(spring_ctx* c, CUtensorMap* tm) {
     return SPRING_OK;
 }
 
-template <bool SPLIT, bool FAST>
-int launch_tc(spring_ctx* c, TcArgs& a, double* d_lw, double* d_p3) {
+// The q0 set a pass runs over: its pairs, its q0 phonons ([q0][s] and [q0][s][row]) and integer
+// coordinates, and a tag for the tile cache (0: the irreducible set, 1: the time-reversal set).
+struct TcQ0 {
+    const PairSet* ps;
+    const double2* ev0;
+    const double* om0;
+    const double* ob0;
+    const int* q0_int;
+    int nq0, set;
+};
+TcQ0 irr_src(spring_ctx* c) {
+    return TcQ0{&c->ps_irr, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_irr_int.p, c->nq0, 0};
+}
+
+template <bool SPLIT, bool FAST, int MODE>
+int launch_tc(spring_ctx* c, TcArgs& a, const TcQ0& src, double* d_lw, double* d_p3, TcBteEntry* bte,
+              unsigned long long* bte_ctr) {
     const size_t smem = sizeof(TcSmem);
     alignas(64) CUtensorMap tmA;
     SPRING_CHECK(make_tmap_a(c, &tmA));
     if (smem > 227 * 1024) return fail(c, SPRING_ERR_UNSUPPORTED, "tensor-core V3 needs %zu bytes of shared memory", smem);
-    cudaFuncSetAttribute(k_v3tc<SPLIT, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_v3tc<SPLIT, FAST, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
-    k_v3tc<SPLIT, FAST><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
-        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), c->ph_irr.omega.p,
-        c->ph_grid.omega.p, reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p, d_lw, d_p3, c->d_tc_cnt_cta.p);
+    k_v3tc<SPLIT, FAST, MODE><<<c->tc_grid, TC_THREADS, smem, c->stream>>>(
+        a, tmA, c->d_tc_tiles.p, c->d_tc_rec.p, reinterpret_cast<const __nv_bfloat16*>(c->d_tc_b.p), src.om0,
+        c->ph_grid.omega.p, reinterpret_cast<const Q0Rec*>(c->d_tc_q0.p), c->d_tc_modes.p, d_lw, d_p3, bte, bte_ctr,
+        c->d_tc_cnt_cta.p);
     return launch_check(c, SPLIT ? "k_v3tc<bf16x3>" : "k_v3tc<bf16>");
 }
 
@@ -870,10 +945,11 @@ int launch_tc(spring_ctx* c, TcArgs& a, double* d_lw, double* d_p3) {
 // the sort, the tile counts and an asynchronous readback of their total (c->tc_pending);
 // build_tiles_end waits for it and cuts the tiles, so that work queued between the two (the
 // operand tables) runs while the host waits.
-int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
-    const PairSet& ps = c->ps_irr;
+int build_tiles_begin(spring_ctx* c, const TcQ0& src, int q0, int n0, int nmax, float rf) {
+    const PairSet& ps = *src.ps;
     c->tc_pending = false;
-    if (c->tc_gen == ps.gen && c->tc_q0 == q0 && c->tc_n0 == n0 && c->tc_ph_gen == c->ph_gen && c->tc_rf == rf)
+    if (c->tc_set == src.set && c->tc_gen == ps.gen && c->tc_q0 == q0 && c->tc_n0 == n0 && c->tc_ph_gen == c->ph_gen &&
+        c->tc_rf == rf)
         return SPRING_OK;
     c->tc_gen = -1;  // no valid tiles until build_tiles_end has cut them
     const int n = nmax, nq = c->nq;
@@ -898,7 +974,7 @@ int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
         else {
             k_tc_keys<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
-                n, ps.cap, q0, n0, nq, ps.pairoff.p, ps.pairs.p, ps.pair_q0.p, c->ph_irr.omega.p, c->ph_grid.omega.p,
+                n, ps.cap, q0, n0, nq, ps.pairoff.p, ps.pairs.p, ps.pair_q0.p, src.om0, c->ph_grid.omega.p,
                 rf, keys.p, vals.p, cnt.p, c->d_scr_sum.p + 1);
             rc = launch_check(c, "k_tc_keys");
         }
@@ -933,6 +1009,7 @@ int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
     if (rc == SPRING_OK) rc = d2h_pin_async(c, c->d_scr_sum.p, 3 * sizeof(int), "tile and pair counts");
     if (rc != SPRING_OK) return rc;
     c->tc_pending = true;
+    c->tc_set = src.set;
     c->tc_q0 = q0;
     c->tc_n0 = n0;
     c->tc_nmax = nmax;
@@ -940,10 +1017,10 @@ int build_tiles_begin(spring_ctx* c, int q0, int n0, int nmax, float rf) {
     return SPRING_OK;
 }
 
-int build_tiles_end(spring_ctx* c) {
+int build_tiles_end(spring_ctx* c, const TcQ0& src) {
     if (!c->tc_pending) return SPRING_OK;
     c->tc_pending = false;
-    const PairSet& ps = c->ps_irr;
+    const PairSet& ps = *src.ps;
     const int n = c->tc_nmax, nq = c->nq;
     DBuf<int>&cnt = c->d_tc_cnt, &seg = c->d_tc_seg, &toff = c->d_tc_toff;
     const int threads = 256;
@@ -963,7 +1040,7 @@ int build_tiles_end(spring_ctx* c) {
         if (launch_injected(c)) rc = fail(c, SPRING_ERR_INJECTED, "tiles: injected launch failure");
         else {
             k_tc_entrec<<<std::min((n + threads - 1) / threads, 148 * 8), threads, 0, c->stream>>>(
-                n, nq, c->d_tc_entries.p, c->d_tc_keys_s.p, ps.pairs.p, ps.pair_q0.p, c->d_irr_int.p, c->d_tc_rec.p);
+                n, nq, c->d_tc_entries.p, c->d_tc_keys_s.p, ps.pairs.p, ps.pair_q0.p, src.q0_int, c->d_tc_rec.p);
             rc = launch_check(c, "k_tc_entrec");
         }
     }
@@ -982,25 +1059,61 @@ int run_v3_prescreen(spring_ctx* c, int q0_first, int n_q0, double sigma, const 
     const int nmax = (int)std::min<long long>(ps.cap, (long long)n_q0 * (c->nq / 2 + 8));
     const double os = 1.0 / sigma;
     const float rf = (float)(sqrt(EXP_CUT / (0.5 * (os * os))) * 1.0001 + 1e-3);
-    SPRING_CHECK(build_tiles_begin(c, q0_first, n_q0, nmax, rf));
-    SPRING_CHECK(build_tiles_end(c));
+    const TcQ0 src = irr_src(c);
+    SPRING_CHECK(build_tiles_begin(c, src, q0_first, n_q0, nmax, rf));
+    SPRING_CHECK(build_tiles_end(c, src));
     *d_list = c->d_tc_entries.p;  // sorted by q1; the pairs with a triple in the window come first
     *n = c->tc_npairs;
     return SPRING_OK;
 }
 
-int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
-                   bool* handled) {
-    *handled = false;
-    if (c->nb != 2 || c->na3 > 8) return SPRING_OK;
-    const PairSet& ps = c->ps_irr;
-    *handled = true;
+namespace {
+
+// q0 phonons of the time-reversal set, gathered from the grid phonons
+__global__ void k_tc_gather_q0(int n0, const int* __restrict__ grid, const double2* __restrict__ evg,
+                               const double* __restrict__ omg, const double* __restrict__ obg, double2* __restrict__ ev0,
+                               double* __restrict__ om0, double* __restrict__ ob0) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n0 * NMODE * NMODE; i += gridDim.x * blockDim.x) {
+        const int q = i / (NMODE * NMODE), r = i % (NMODE * NMODE);
+        const size_t g = (size_t)grid[q];
+        ev0[i] = evg[g * NMODE * NMODE + r];
+        if (r < NMODE) {
+            om0[q * NMODE + r] = omg[g * NMODE + r];
+            ob0[q * NMODE + r] = obg[g * NMODE + r];
+        }
+    }
+}
+
+int tr_src(spring_ctx* c, TcQ0* out) {
+    const int n0 = c->ntr;
+    if (c->tr_ph_gen != c->ph_gen || c->d_tr_ev.n < (size_t)n0 * NMODE * NMODE) {
+        SPRING_CHECK(dalloc(c, c->d_tr_ev, (size_t)n0 * NMODE * NMODE, "time-reversal q0 phonons"));
+        SPRING_CHECK(dalloc(c, c->d_tr_om, (size_t)n0 * NMODE, "time-reversal q0 phonons"));
+        SPRING_CHECK(dalloc(c, c->d_tr_ob, (size_t)n0 * NMODE, "time-reversal q0 phonons"));
+        if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc: injected launch failure");
+        k_tc_gather_q0<<<std::max(1, std::min((n0 * NMODE * NMODE + 255) / 256, 148 * 8)), 256, 0, c->stream>>>(
+            n0, c->d_tr_grid.p, c->ph_grid.evec.p, c->ph_grid.omega.p, c->ph_grid.oneby.p, c->d_tr_ev.p, c->d_tr_om.p,
+            c->d_tr_ob.p);
+        SPRING_CHECK(launch_check(c, "k_tc_gather_q0"));
+        c->tr_ph_gen = c->ph_gen;
+    }
+    *out = TcQ0{&c->ps_tr, c->d_tr_ev.p, c->d_tr_om.p, c->d_tr_ob.p, c->d_tr_int.p, n0, 1};
+    return SPRING_OK;
+}
+
+// The tensor-core pass over q0 block [q0_first, q0_first + n_q0) of `src`: MODE 0 adds the
+// linewidths and phase space into d_lw / d_p3, MODE 1 appends operator entries to bte (its count
+// in *bte_ctr, which may exceed bte_cap: then only bte_cap were written).
+template <int MODE>
+int run_v3tc_core(spring_ctx* c, const TcQ0& src, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw,
+                  double* d_p3, TcBteEntry* bte, unsigned long long* bte_ctr, long long bte_cap) {
+    const PairSet& ps = *src.ps;
     const int nq = c->nq;
     // slots for the block's pairs without reading their count: at most Nq/2 + 8 per q0
     const int nmax = (int)std::min<long long>(ps.cap, (long long)n_q0 * (nq / 2 + 8));
     SPRING_CHECK(dalloc(c, c->d_tc_a, (size_t)nq * 4 * AIMG, "V3 A table"));
     SPRING_CHECK(dalloc(c, c->d_tc_b, (size_t)nq * 4 * BIMG, "V3 B table"));
-    SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)c->nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
+    SPRING_CHECK(dalloc(c, c->d_tc_q0, (size_t)src.nq0 * NMODE * sizeof(Q0Rec) / sizeof(double), "V3 q0 records"));
     const int rs = (2 + c->nT + 3) / 4 * 4;
     SPRING_CHECK(dalloc(c, c->d_tc_modes, (size_t)nq * NMODE * rs, "V3 mode records"));
     const double os = 1.0 / sigma;
@@ -1032,9 +1145,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
                                                    reinterpret_cast<__nv_bfloat16*>(c->d_tc_b.p));
         SPRING_CHECK(launch_check(c, "k_tc_tab_b"));
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
-        k_tc_q0tab<<<std::max(1, std::min((c->nq0 * NMODE + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
-            c->nq0, c->ph_irr.evec.p, c->ph_irr.omega.p, c->ph_irr.oneby.p, c->d_mass_rs.p,
-            reinterpret_cast<Q0Rec*>(c->d_tc_q0.p));
+        k_tc_q0tab<<<std::max(1, std::min((src.nq0 * NMODE + threads - 1) / threads, 148 * 4)), threads, 0, c->stream>>>(
+            src.nq0, src.ev0, src.om0, src.ob0, c->d_mass_rs.p, reinterpret_cast<Q0Rec*>(c->d_tc_q0.p));
         SPRING_CHECK(launch_check(c, "k_tc_q0tab"));
         if (launch_injected(c)) return fail(c, SPRING_ERR_INJECTED, "v3tc tables: injected launch failure");
         k_tc_modes<<<(int)std::min<long long>(((long long)nq * NMODE * rs + threads - 1) / threads, 148LL * 8), threads, 0,
@@ -1055,8 +1167,8 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
         }
         if (e != cudaSuccess) return cuda_fail(c, e, "side stream join");
     }
-    int brc = build_tiles_begin(c, q0_first, n_q0, nmax, rf);
-    if (brc == SPRING_OK) brc = build_tiles_end(c);  // the tile count was read while the tables ran
+    int brc = build_tiles_begin(c, src, q0_first, n_q0, nmax, rf);
+    if (brc == SPRING_OK) brc = build_tiles_end(c, src);  // the tile count was read while the tables ran
     {
         const cudaError_t e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);  // join the tables
         if (brc != SPRING_OK) return brc;
@@ -1066,9 +1178,11 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
 
     TcArgs a{};
     a.nq = nq;
-    a.nq0 = c->nq0;
+    a.nq0 = src.nq0;
     a.nT = c->nT;
     a.ntiles = c->tc_ntiles;
+    a.q0_first = q0_first;
+    a.bte_cap = bte_cap;
     for (int k = 0; k < 3; ++k) {
         a.lo[k] = pol.lo[k];
         a.hi[k] = pol.hi[k];
@@ -1087,14 +1201,49 @@ int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Po
     SPRING_CHECK(dalloc(c, c->d_tc_cnt_cta, 1, "V3 status"));
     SPRING_CHECK(zero(c, c->d_tc_cnt_cta.p, sizeof(int), "V3 status"));
     const bool split = c->precision == SPRING_BF16X3, fast = rs == 8 && c->nT <= NT_FAST;
-    SPRING_CHECK(split ? (fast ? launch_tc<true, true>(c, a, d_lw, d_p3) : launch_tc<true, false>(c, a, d_lw, d_p3))
-                       : (fast ? launch_tc<false, true>(c, a, d_lw, d_p3) : launch_tc<false, false>(c, a, d_lw, d_p3)));
+    int lrc;
+    if (MODE == 1)
+        lrc = split ? launch_tc<true, false, 1>(c, a, src, d_lw, d_p3, bte, bte_ctr)
+                    : launch_tc<false, false, 1>(c, a, src, d_lw, d_p3, bte, bte_ctr);
+    else if (split)
+        lrc = fast ? launch_tc<true, true, 0>(c, a, src, d_lw, d_p3, bte, bte_ctr)
+                   : launch_tc<true, false, 0>(c, a, src, d_lw, d_p3, bte, bte_ctr);
+    else
+        lrc = fast ? launch_tc<false, true, 0>(c, a, src, d_lw, d_p3, bte, bte_ctr)
+                   : launch_tc<false, false, 0>(c, a, src, d_lw, d_p3, bte, bte_ctr);
+    SPRING_CHECK(lrc);
     SPRING_CHECK(d2h_pin_async(c, c->d_tc_cnt_cta.p, sizeof(int), "V3 status"));
     SPRING_CHECK(pin_wait(c, "V3 status"));
     const int herr = c->h_pin[0];
     if (herr == 2) return fail(c, SPRING_ERR_CUDA, "tensor-core V3: shared memory base not 128-byte aligned");
     if (herr) return fail(c, SPRING_ERR_TIMEOUT, "tensor-core V3: a pipeline wait ran out after %lld polls", a.max_spins);
     return SPRING_OK;
+}
+
+}  // namespace
+
+int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
+                   bool* handled) {
+    *handled = false;
+    if (c->nb != 2 || c->na3 > 8) return SPRING_OK;
+    *handled = true;
+    return run_v3tc_core<0>(c, irr_src(c), q0_first, n_q0, sigma, pol, d_lw, d_p3, nullptr, nullptr, 0);
+}
+
+int run_v3tc_bte(spring_ctx* c, int q0_first, int n_q0, double sigma, void* entries, unsigned long long* ctr,
+                 long long cap, bool* handled) {
+    *handled = false;
+    if (c->nb != 2 || c->na3 > 8 || c->precision == SPRING_FP64) return SPRING_OK;
+    *handled = true;
+    TcQ0 src;
+    SPRING_CHECK(tr_src(c, &src));
+    Pol all;
+    for (int k = 0; k < 3; ++k) {
+        all.lo[k] = 0;
+        all.hi[k] = NMODE - 1;
+    }
+    return run_v3tc_core<1>(c, src, q0_first, n_q0, sigma, all, nullptr, nullptr, static_cast<TcBteEntry*>(entries),
+                            ctr, cap);
 }
 
 }  // namespace spring

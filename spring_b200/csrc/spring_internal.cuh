@@ -213,7 +213,7 @@ struct spring_ctx {
     spring::DBuf<double2> d_bteg_pq;
     long long bteg_n = 0;
     double bteg_sigma = 0.0;
-    int bteg_gen = -1, bteg_pairs = -1;
+    int bteg_gen = -1, bteg_pairs = -1, bteg_prec = -1;
 
     // four-phonon quartet lists (k_4ph.cu, opaque) and the tensor-core V4 buffers (k_v4tc.cu)
     void* e4 = nullptr;
@@ -251,6 +251,10 @@ struct spring_ctx {
     spring::DBuf<int4> d_tc_rec;       // (q0, q2, weight, q0 is Gamma) in that order
     spring::DBuf<int4> d_tc_tiles;     // (q1, first entry, count)
     int tc_ntiles = 0, tc_gen = -1, tc_q0 = -1, tc_n0 = -1, tc_nmax = 0, tc_ph_gen = -1;  // tile cache key
+    int tc_set = -1;                   // q0 set of the cached tiles (0 irreducible, 1 time-reversal)
+    spring::DBuf<double2> d_tr_ev;     // time-reversal q0 phonons gathered from the grid (tensor-core operator)
+    spring::DBuf<double> d_tr_om, d_tr_ob;
+    int tr_ph_gen = -1;
     int tc_npairs = 0;                 // pairs in those tiles
     float tc_rf = 0.0f;                // delta window the cached tiles were screened with
     bool tc_pending = false;           // tile count read back asynchronously, tiles not cut yet
@@ -350,6 +354,11 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
 // tensor-core path's pre-screen), as a device list of pair indices and its length
 int run_v3_prescreen(spring_ctx* c, int q0_first, int n_q0, double sigma, const int** d_list, int* n);
 // k_v3tc.cu: tensor-core V3 + Gaussian sum (BF16 / BF16x3) for two-atom cells; *handled false otherwise
+// k_v3tc.cu: entries of the Gaussian iterative-BTE operator (s3::BteEntry layout) over time-reversal
+// q0 block [q0_first, q0_first + n_q0) on the tensor cores; *handled false when the cell or the
+// precision (FP64) does not take it.  *ctr receives the entry count, which may exceed cap.
+int run_v3tc_bte(spring_ctx* c, int q0_first, int n_q0, double sigma, void* entries, unsigned long long* ctr,
+                 long long cap, bool* handled);
 int run_v3tc_gauss(spring_ctx* c, int q0_first, int n_q0, double sigma, const Pol& pol, double* d_lw, double* d_p3,
                    bool* handled);
 // k_4ph.cu

@@ -24,6 +24,30 @@ def test_kappa_iter_matches_oracle(N):
     ctx.close()
 
 
+@pytest.mark.parametrize("N,sigma", [(5, 1.5), (6, 0.8)])
+def test_kappa_iter_gauss_tensor_core_operator(N, sigma):
+    """On a BF16x3 context the operator entries come from the tensor-core pass: the same entries
+    (the window and the cuts are the FP64 ones, only |Phi|^2 is compensated BF16), kappa and the RTA
+    start within 1e-5 of the FP64 operator's; switching back to FP64 rebuilds the FP64 operator."""
+    cr = S.build("rocksalt2")
+    st = D.Setup(cr, (N, N, N), [300.0, 700.0])
+    ctx, _ = from_crystal(cr, (N, N, N), st.temps, phonons={"grid": st.ph, "irr": st.ph0})
+    ref = ctx.kappa_iter_gauss(sigma, eps_k=1e-6)
+    ctx.set_precision("bf16x3")
+    out = ctx.kappa_iter_gauss(sigma, eps_k=1e-6)
+    assert out["entries"] == ref["entries"] and out["pairs"] == ref["pairs"]
+    for it in range(2):
+        for key in ("kappa_rta", "kappa"):
+            scale = np.abs(ref[key][it]).max()
+            # within 1e-5 of the tensor's largest component (the small off-diagonal terms included)
+            np.testing.assert_allclose(out[key][it], ref[key][it], rtol=1e-5, atol=1e-5 * scale)
+        assert abs(int(out["iters"][it]) - int(ref["iters"][it])) <= 1
+    ctx.set_precision("fp64")
+    back = ctx.kappa_iter_gauss(sigma, eps_k=1e-6)
+    np.testing.assert_allclose(back["kappa"], ref["kappa"], rtol=1e-12, atol=0.0)
+    ctx.close()
+
+
 def test_kappa_iter_rta_equals_kappa_x_full_grid():
     """Iteration 0 of the BTE is kappa.x's RTA on the full grid (identity symmetry)."""
     cr = S.build("rocksalt2")
