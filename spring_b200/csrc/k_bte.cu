@@ -312,19 +312,21 @@ __global__ void k_bteg_coef(long long n, const int2* __restrict__ kk, const doub
         cf[i] = (n1 - n2) * v.x + (1.0 + n1 + n2) * v.y;
     }
 }
-// F at every grid mode from the time-reversal slots: Fg[g][s] = sgn(g) F[pos(g)][s]
+// F at every grid mode from the time-reversal slots: Fg[g][s] = sgn(g) F[pos(g)][s], padded to four
+// doubles (32 bytes, one L2 sector) per mode for the row pass's gathers.
 __global__ void k_bteg_expand(int nq, int n, const int* __restrict__ pos, const int* __restrict__ sgn,
                               const double* __restrict__ F, double* __restrict__ Fg) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nq * n; i += gridDim.x * blockDim.x) {
         const int g = i / n, sx = i % n;
         const double sg = sgn[g];
         const double* f = F + ((size_t)pos[g] * n + sx) * 3;
-        Fg[3 * (size_t)i] = sg * f[0];
-        Fg[3 * (size_t)i + 1] = sg * f[1];
-        Fg[3 * (size_t)i + 2] = sg * f[2];
+        double2* o = reinterpret_cast<double2*>(Fg + 4 * (size_t)i);
+        o[0] = make_double2(sg * f[0], sg * f[1]);
+        o[1] = make_double2(sg * f[2], 0.0);
     }
 }
-// One warp per row: MODE 0 inv_tau[r] = sum c; MODE 1 dF[r] = -sum c (Fg[k1] + Fg[k2]).
+// One warp per row: MODE 0 inv_tau[r] = sum c; MODE 1 dF[r] = -sum c (Fg[k1] + Fg[k2]) (Fg: four
+// doubles per mode, the fourth zero).
 template <int MODE>
 __global__ void __launch_bounds__(256) k_bteg_rows(int rows, const int* __restrict__ rowoff, const int2* __restrict__ kk,
                                                   const double* __restrict__ cf, const double* __restrict__ Fg,
@@ -338,11 +340,12 @@ __global__ void __launch_bounds__(256) k_bteg_rows(int rows, const int* __restri
                 a0 += c;
             } else {
                 const int2 k = kk[i];
-                const double* f1 = Fg + 3 * (size_t)k.x;
-                const double* f2 = Fg + 3 * (size_t)k.y;
-                a0 -= c * (f1[0] + f2[0]);
-                a1 -= c * (f1[1] + f2[1]);
-                a2 -= c * (f1[2] + f2[2]);
+                const double2* f1 = reinterpret_cast<const double2*>(Fg + 4 * (size_t)k.x);
+                const double2* f2 = reinterpret_cast<const double2*>(Fg + 4 * (size_t)k.y);
+                const double2 u1 = f1[0], v1 = f1[1], u2 = f2[0], v2 = f2[1];
+                a0 -= c * (u1.x + u2.x);
+                a1 -= c * (u1.y + u2.y);
+                a2 -= c * (v1.x + v2.x);
             }
         }
         a0 = tet::warp_sum(a0);
@@ -460,7 +463,7 @@ int run_bte_gauss(spring_ctx* c, double sigma, double eps_k, int max_iter, doubl
     if (rc == SPRING_OK) rc = dalloc(c, dF, (size_t)rows * 3, "dF");
     if (rc == SPRING_OK) rc = dalloc(c, kap, 9, "kappa");
     if (rc == SPRING_OK) rc = dalloc(c, cf, std::max<long long>(cnt, 1), "operator coefficients");
-    if (rc == SPRING_OK) rc = dalloc(c, Fg, (size_t)nq * n * 3, "F on the grid");
+    if (rc == SPRING_OK) rc = dalloc(c, Fg, (size_t)nq * n * 4, "F on the grid");
     const int rblocks = std::max(1, std::min((rows + 7) / 8, 148 * 16));
     const int eblocks = std::max(1, std::min((rows + threads - 1) / threads, 148 * 8));
     auto kappa_of = [&](int T, const double* Fv, double* out9) -> int {
