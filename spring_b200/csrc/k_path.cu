@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(128) k_v3_path(V3PArgs a, const int* __restric
     for (int i = tid; i < nn; i += nt) {
         sE0[i] = ev0[(size_t)p * nn + i];
         sE1[i] = evg[(size_t)q1 * nn + i];
-        sE2[i] = ev2[row * nn + i];
+        sE2[(i % n) * n + i / n] = ev2[row * nn + i];  // [row][s]: read along s2 below
     }
     for (int i = tid; i < nphi; i += nt) sPhi[i] = make_double2(0.0, 0.0);
 
@@ -225,9 +225,9 @@ __global__ void __launch_bounds__(128) k_v3_path(V3PArgs a, const int* __restric
         for (int o = tid; o < 3 * nn; o += nt) {
             const int ar = o / n, s2 = o % n;
             const double2* drow = sD + ar * n;
-            const double2* e2 = sE2 + s2 * n;
+            const double2* e2 = sE2 + s2;
             double2 acc = make_double2(0.0, 0.0);
-            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k]);
+            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k * n]);
             sT1[o] = acc;
         }
         __syncthreads();

@@ -82,7 +82,7 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
     const int sb = a.sb;
     double2* sE0 = smem2;              // [s][row]
     double2* sE1 = sE0 + nn;
-    double2* sE2 = sE1 + nn;
+    double2* sE2 = sE1 + nn;           // [row][s] (transposed: stage (d) reads it along s2)
     double2* sD = sE2 + nn;            // [a][nu b][eta c]
     double2* sT1 = sD + 3 * nn;        // [a][nu b][s2]
     double2* sT2 = sD;                 // [a][s1][s2]: D is dead once T1 is formed
@@ -103,7 +103,7 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
     for (int i = tid; i < nn; i += nt) {
         sE0[i] = ev0[(size_t)p0 * nn + i];
         sE1[i] = evg[(size_t)g1 * nn + i];
-        sE2[i] = evg[(size_t)g2 * nn + i];
+        sE2[(i % n) * n + i / n] = evg[(size_t)g2 * nn + i];
     }
     for (int i = tid; i < nphi; i += nt) sPhi[i] = make_double2(0.0, 0.0);
 
@@ -153,9 +153,9 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
         for (int o = tid; o < 3 * nn; o += nt) {
             const int ar = o / n, s2 = o % n;
             const double2* drow = sD + ar * n;
-            const double2* e2 = sE2 + s2 * n;
+            const double2* e2 = sE2 + s2;  // consecutive threads read consecutive s2: no bank conflict
             double2 acc = make_double2(0.0, 0.0);
-            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k]);
+            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k * n]);
             sT1[o] = acc;
         }
         __syncthreads();
