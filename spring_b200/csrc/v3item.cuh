@@ -92,6 +92,8 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
     double* sFC = reinterpret_cast<double*>(sP + 2 * na);  // [N1][N2][27]
     double* sLw = sFC + ((na * na * 27 + 1) & ~1);         // [nT + 1][sb]
     int* sBt = reinterpret_cast<int*>(sLw + (a.nT + 1) * sb + 1);  // [na]
+    int* sCnt = sBt + na;              // [nb] slots of each basis type
+    int* sIdx = sCnt + a.nb;           // [nb][na] those slots, ascending
 
     const int tid = threadIdx.x, nt = blockDim.x;
     const int2 pq = pairs[pr];
@@ -122,6 +124,13 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
             sP[i] = make_double2(cs, sn);
         }
         __syncthreads();
+        // the slots of each basis type (the D sums below visit only these, in the same order)
+        if (tid < a.nb) {
+            int cnt = 0;
+            for (int N = 0; N < na; ++N)
+                if (sBt[N] == tid) sIdx[tid * na + cnt++] = N;
+            sCnt[tid] = cnt;
+        }
         // (b) phase products with the neighbour masses
         for (int i = tid; i < na * na; i += nt) {
             const int N1 = i / na, N2 = i % na;
@@ -136,10 +145,11 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
             const int nu = r / 3, be = r % 3, eta = cidx / 3, ga = cidx % 3;
             const int abc = (al * 3 + be) * 3 + ga;
             double2 acc = make_double2(0.0, 0.0);
-            for (int N1 = 0; N1 < na; ++N1) {
-                if (sBt[N1] != nu) continue;
-                for (int N2 = 0; N2 < na; ++N2) {
-                    if (sBt[N2] != eta) continue;
+            const int c1 = sCnt[nu], c2 = sCnt[eta];
+            for (int i1 = 0; i1 < c1; ++i1) {
+                const int N1 = sIdx[nu * na + i1];
+                for (int i2 = 0; i2 < c2; ++i2) {
+                    const int N2 = sIdx[eta * na + i2];
                     const double fv = sFC[(N1 * na + N2) * 27 + abc];
                     const double2 pp = sPP[N1 * na + N2];
                     acc.x = fma(fv, pp.x, acc.x);
@@ -149,24 +159,40 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
             sD[o] = acc;
         }
         __syncthreads();
-        // (d) T1[a][r][s2] = sum_c D[a][r][c] e2(c, s2)
-        for (int o = tid; o < 3 * nn; o += nt) {
-            const int ar = o / n, s2 = o % n;
-            const double2* drow = sD + ar * n;
-            const double2* e2 = sE2 + s2;  // consecutive threads read consecutive s2: no bank conflict
-            double2 acc = make_double2(0.0, 0.0);
-            for (int k = 0; k < n; ++k) cfma(acc, drow[k], e2[k * n]);
-            sT1[o] = acc;
+        // (d) T1[a][r][s2] = sum_c D[a][r][c] e2(c, s2); one thread per (r, s2), all three a, so each
+        // e2 value read serves three products (consecutive threads read consecutive s2: no bank
+        // conflict)
+        for (int o = tid; o < nn; o += nt) {
+            const int r = o / n, s2 = o % n;
+            const double2* d0 = sD + r * n;
+            const double2* e2 = sE2 + s2;
+            double2 acc0 = make_double2(0.0, 0.0), acc1 = acc0, acc2 = acc0;
+            for (int k = 0; k < n; ++k) {
+                const double2 e = e2[k * n];
+                cfma(acc0, d0[k], e);
+                cfma(acc1, d0[nn + k], e);
+                cfma(acc2, d0[2 * nn + k], e);
+            }
+            sT1[o] = acc0;
+            sT1[nn + o] = acc1;
+            sT1[2 * nn + o] = acc2;
         }
         __syncthreads();
-        // (e) T2[a][s1][s2] = sum_r e1(r, s1) T1[a][r][s2]
-        for (int o = tid; o < 3 * nn; o += nt) {
-            const int al = o / nn, s1 = (o / n) % n, s2 = o % n;
+        // (e) T2[a][s1][s2] = sum_r e1(r, s1) T1[a][r][s2]; one thread per (s1, s2), all three a
+        for (int o = tid; o < nn; o += nt) {
+            const int s1 = o / n, s2 = o % n;
             const double2* e1 = sE1 + s1 * n;
-            const double2* t1 = sT1 + al * nn + s2;
-            double2 acc = make_double2(0.0, 0.0);
-            for (int k = 0; k < n; ++k) cfma(acc, e1[k], t1[k * n]);
-            sT2[o] = acc;
+            const double2* t1 = sT1 + s2;
+            double2 acc0 = make_double2(0.0, 0.0), acc1 = acc0, acc2 = acc0;
+            for (int k = 0; k < n; ++k) {
+                const double2 w = e1[k];
+                cfma(acc0, w, t1[k * n]);
+                cfma(acc1, w, t1[nn + k * n]);
+                cfma(acc2, w, t1[2 * nn + k * n]);
+            }
+            sT2[o] = acc0;
+            sT2[nn + o] = acc1;
+            sT2[2 * nn + o] = acc2;
         }
         __syncthreads();
         // (f) Phi[s0][s1][s2] += sum_a m_mu^-1/2 e0(mu a, s0) T2[a][s1][s2]
@@ -250,7 +276,8 @@ __device__ __forceinline__ void v3_item(const V3Args& a, const V3Ptrs& P, int pr
 inline size_t v3_smem(int n, int na, int sb, int nT) {
     const int nn = n * n;
     return sizeof(double2) * (3 * nn + 6 * nn + sb * nn + na * na + 2 * na) +
-           sizeof(double) * (((na * na * 27 + 1) & ~1) + (nT + 1) * sb + 1) + sizeof(int) * na + 16;
+           sizeof(double) * (((na * na * 27 + 1) & ~1) + (nT + 1) * sb + 1) + sizeof(int) * (na + n / 3 * (na + 1)) +
+           16;
 }
 
 inline int v3_block(int n) {
