@@ -379,6 +379,24 @@ constexpr int NT_FAST = 4;  // mode records of 8 doubles carry the occupations o
 // P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 + (n1 - n2)(g2 - g3)].  The q0 record
 // (omega, 1/omega) and the mode records (omega, 1/omega, nBE[T]) of q1 and q2 are read whole, so
 // a triple needs one memory round trip.  FAST: records of 8 doubles, n_temps <= 4.
+// exp(-x) of the arguments below the cut (g = 0 for the others), each lane computing only its own:
+// the warp runs as many exponentials as the lane that needs most (usually one of the three, the
+// deltas of a triple being 2 omega1 or 2 omega2 apart).  One call site of exp.
+__device__ __forceinline__ void tc_gauss3(double x1, double x2, double x3, double& g1, double& g2, double& g3) {
+    unsigned need = (x1 < EXP_CUT ? 1u : 0u) | (x2 < EXP_CUT ? 2u : 0u) | (x3 < EXP_CUT ? 4u : 0u);
+    g1 = g2 = g3 = 0.0;
+    while (__any_sync(0xffffffffu, need != 0u)) {
+        if (need != 0u) {
+            const int k = __ffs(need) - 1;
+            need &= need - 1u;
+            const double g = exp(-(k == 0 ? x1 : (k == 1 ? x2 : x3)));
+            if (k == 0) g1 = g;
+            else if (k == 1) g2 = g;
+            else g3 = g;
+        }
+    }
+}
+
 template <bool FAST, int MODE>
 __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
                                       double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
@@ -390,6 +408,8 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
         // second term of P dropped and Q halved when q1 = q2; one entry per triple with P or Q nonzero
         double Pv = 0.0, Qv = 0.0;
         TcStage s{};
+        double xm = EXP_CUT, xa = EXP_CUT, xb = EXP_CUT, W = 0.0;  // EXP_CUT: no weight
+        bool self = true;
         if (lane < n) {
             s = st[lane];
             const int o = s.k0 & 0x1fffffff;
@@ -399,16 +419,22 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
             if (!((s.k0 >> 29) & 1)) {
                 const double w0 = r0.x, w1 = a.x, w2 = b.x;
                 const double dm = w0 - w1 - w2, da = w0 + w1 - w2, db = w0 - w1 + w2;
-                const double xm = half_os2 * (dm * dm), xa = half_os2 * (da * da), xb = half_os2 * (db * db);
-                const double gm = exp(-fmin(xm, EXP_CUT)), ga = exp(-fmin(xa, EXP_CUT)), gb = exp(-fmin(xb, EXP_CUT));
-                const bool self = !((s.k0 >> 30) & 1);
-                const double em = xm < EXP_CUT ? pre * gm : 0.0;
-                const double ea = xa < EXP_CUT ? pre * ga : 0.0;
-                const double eb = (!self && xb < EXP_CUT) ? pre * gb : 0.0;
-                const double W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac;
-                Pv = 4.0 * W * (ea - eb);
-                Qv = 4.0 * W * (self ? 0.5 : 1.0) * em;
+                xm = half_os2 * (dm * dm);
+                xa = half_os2 * (da * da);
+                xb = half_os2 * (db * db);
+                self = !((s.k0 >> 30) & 1);
+                if (self) xb = EXP_CUT;  // the second term of P is dropped when q1 = q2
+                W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac;
             }
+        }
+        double gm, ga, gb;
+        tc_gauss3(xm, xa, xb, gm, ga, gb);
+        if (W != 0.0) {
+            const double em = xm < EXP_CUT ? pre * gm : 0.0;
+            const double ea = xa < EXP_CUT ? pre * ga : 0.0;
+            const double eb = xb < EXP_CUT ? pre * gb : 0.0;
+            Pv = 4.0 * W * (ea - eb);
+            Qv = 4.0 * W * (self ? 0.5 : 1.0) * em;
         }
         const bool has = Pv != 0.0 || Qv != 0.0;
         const unsigned bal = __ballot_sync(0xffffffffu, has);
@@ -431,14 +457,17 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
         __syncwarp();
         return;
     }
+    TcStage s{};
+    double2 r0 = make_double2(0.0, 0.0), a = r0, b = r0, a1 = r0, a2 = r0, b1 = r0, b2 = r0;
+    double x1 = EXP_CUT, x2 = EXP_CUT, x3 = EXP_CUT;  // EXP_CUT: no weight (lanes past n)
     if (lane < n) {
-        const TcStage s = st[lane];
+        s = st[lane];
         const int o = s.k0 & 0x1fffffff;
-        const double2 r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
+        r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
         const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
         const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
-        const double2 a = pa[0], b = pb[0];
-        double2 a1 = make_double2(0.0, 0.0), a2 = a1, b1 = a1, b2 = a1;
+        a = pa[0];
+        b = pb[0];
         if (FAST) {
             a1 = pa[1];
             a2 = pa[2];
@@ -447,9 +476,14 @@ __device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT,
         }
         const double w0 = r0.x, w1 = a.x, w2 = b.x;
         const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
-        const double x1 = half_os2 * (d1 * d1), x2 = half_os2 * (d2 * d2), x3 = half_os2 * (d3 * d3);
-        // three independent exponentials of clamped arguments (no branch between them), then the cut
-        const double g1 = exp(-fmin(x1, EXP_CUT)), g2 = exp(-fmin(x2, EXP_CUT)), g3 = exp(-fmin(x3, EXP_CUT));
+        x1 = half_os2 * (d1 * d1);
+        x2 = half_os2 * (d2 * d2);
+        x3 = half_os2 * (d3 * d3);
+    }
+    double g1, g2, g3;
+    tc_gauss3(x1, x2, x3, g1, g2, g3);
+    if (lane < n) {
+        const int o = s.k0 & 0x1fffffff;
         const double e1 = x1 < EXP_CUT ? pre * g1 : 0.0;
         const double e2 = x2 < EXP_CUT ? pre * g2 : 0.0;
         const double e3 = x3 < EXP_CUT ? pre * g3 : 0.0;
