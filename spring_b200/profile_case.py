@@ -19,7 +19,9 @@ def main() -> int:
     ap.add_argument("--mesh", type=int, default=8)
     ap.add_argument("--q0", type=int, default=0, help="irreducible points (0: all)")
     ap.add_argument("--precision", default="bf16x3", choices=["fp64", "bf16", "bf16x3"])
-    ap.add_argument("--repeat", type=int, default=2, help="calls (the first one warms up)")
+    ap.add_argument("--repeat", type=int, default=2, help="calls (only the last is profiled)")
+    ap.add_argument("--warm", type=int, default=0,
+                    help="extra calls before them: a few cold calls run below full clocks, so use ~30 for timings")
     a = ap.parse_args()
     from . import synthetic as S
     from .api import from_crystal
@@ -27,8 +29,8 @@ def main() -> int:
     ctx, _ = from_crystal(cr, (a.mesh,) * 3, [300.0], with_fc4=a.case == "v4")
     ctx.set_precision(a.precision)
     n = ctx.nq0 if a.q0 <= 0 else min(a.q0, ctx.nq0)
-    for r in range(a.repeat):
-        ctx.set_profiling(r == a.repeat - 1)
+    for r in range(a.warm + a.repeat):
+        ctx.set_profiling(r == a.warm + a.repeat - 1)
         t = time.time()
         if a.case == "v3":
             ctx.reset_linewidths()
