@@ -616,19 +616,34 @@ k_v4tc(V4Args a, Blk4 bk, const int4* __restrict__ tiles, const int4* __restrict
                                               W0 + W3 - W1 - W2, W0 + W2 + W3 - W1, W0 + W1 + W3 - W2,
                                               W0 + W1 + W2 - W3};
                         const int cw[7] = {c1, c2[0], c2[1], c2[2], c3[0], c3[1], c3[2]};
-                        double gm[7];
-                        bool anyg = false;
+                        double gm[7], xs[7];
+                        unsigned need = 0u;  // the terms of this quad inside the cut
 #pragma unroll
                         for (int m = 0; m < 7; ++m) {
                             gm[m] = 0.0;
-                            if (cw[m] == 0) continue;
-                            const double x = a.half_os2 * (dd[m] * dd[m]);
-                            if (!(x < EXP_CUT)) continue;
-                            const double wt = m == 0 ? cw[m] * ONEBYSIX : cw[m] * 0.5;
-                            gm[m] = (a.pre * exp(-x)) * wt * Wv;
-                            anyg = true;
+                            xs[m] = a.half_os2 * (dd[m] * dd[m]);
+                            if (cw[m] != 0 && xs[m] < EXP_CUT) need |= 1u << m;
                         }
-                        if (!anyg) continue;
+                        if (need == 0u) continue;
+                        // one exp call site for whichever terms a lane needs (lanes needing different
+                        // terms run it together); the values are those of the term-by-term form
+                        while (need != 0u) {
+                            const int m = __ffs(need) - 1;
+                            need &= need - 1u;
+                            double x = xs[0];
+                            int c = cw[0];
+#pragma unroll
+                            for (int k = 1; k < 7; ++k)
+                                if (m == k) {
+                                    x = xs[k];
+                                    c = cw[k];
+                                }
+                            const double wt = m == 0 ? c * ONEBYSIX : c * 0.5;
+                            const double g = (a.pre * exp(-x)) * wt * Wv;
+#pragma unroll
+                            for (int k = 0; k < 7; ++k)
+                                if (m == k) gm[k] = g;
+                        }
                         // occupation factors of the seven terms, per temperature:
                         // n1 n2 n3, (1+n1) n2 n3, (1+n2) n1 n3, (1+n3) n1 n2, (1+n2)(1+n3) n1,
                         // (1+n1)(1+n3) n2, (1+n1)(1+n2) n3, over n0
