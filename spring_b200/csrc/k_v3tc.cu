@@ -398,7 +398,7 @@ __device__ __forceinline__ void tc_gauss3(double x1, double x2, double x3, doubl
 }
 
 template <bool FAST, int MODE>
-__device__ __noinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
+__device__ __forceinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
                                       double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
                                       double* out_lw, double* out_p3, TcBteEntry* bte, unsigned long long* bte_ctr,
                                       long long bte_cap, int q0_first) {
