@@ -335,7 +335,7 @@ struct TcStage {
     float phi2;
     int k0, k1, k2;
 };
-constexpr int STG_CAP = 128;  // staged triples per epilogue warp: 32 + up to 96 from one chunk
+constexpr int STG_CAP = 160;  // staged triples per epilogue warp: fewer than 64 left + up to 96 from one chunk
 
 // One entry of the Gaussian iterative-BTE operator (row r0 = (q0 - q0_first) * 6 + s0, grid modes
 // k1, k2; c = (n1 - n2) P + (1 + n1 + n2) Q), in the layout the operator sort reads.
@@ -397,121 +397,163 @@ __device__ __forceinline__ void tc_gauss3(double x1, double x2, double x3, doubl
     }
 }
 
-template <bool FAST, int MODE>
-__device__ __forceinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
-                                      double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
-                                      double* out_lw, double* out_p3, TcBteEntry* bte, unsigned long long* bte_ctr,
-                                      long long bte_cap, int q0_first) {
+// One round of operator entries (iterative BTE): n <= 32 staged triples, one per lane.
+__device__ __forceinline__ void tc_bte_round(const TcStage* st, int n, int rs, double half_os2, double pre, double mfac,
+                                             const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
+                                             TcBteEntry* bte, unsigned long long* bte_ctr, long long bte_cap,
+                                             int q0_first) {
     const int lane = threadIdx.x & 31;
-    if (MODE == 1) {
-        // operator entries: P = 4 W (g(w0 + w1 - w2) - g(w0 + w2 - w1)), Q = 4 W g(w0 - w1 - w2), the
-        // second term of P dropped and Q halved when q1 = q2; one entry per triple with P or Q nonzero
-        double Pv = 0.0, Qv = 0.0;
-        TcStage s{};
-        double xm = EXP_CUT, xa = EXP_CUT, xb = EXP_CUT, W = 0.0;  // EXP_CUT: no weight
-        bool self = true;
-        if (lane < n) {
-            s = st[lane];
-            const int o = s.k0 & 0x1fffffff;
-            const double2 r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
-            const double2 a = *reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
-            const double2 b = *reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
-            if (!((s.k0 >> 29) & 1)) {
-                const double w0 = r0.x, w1 = a.x, w2 = b.x;
-                const double dm = w0 - w1 - w2, da = w0 + w1 - w2, db = w0 - w1 + w2;
-                xm = half_os2 * (dm * dm);
-                xa = half_os2 * (da * da);
-                xb = half_os2 * (db * db);
-                self = !((s.k0 >> 30) & 1);
-                if (self) xb = EXP_CUT;  // the second term of P is dropped when q1 = q2
-                W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac;
-            }
-        }
-        double gm, ga, gb;
-        tc_gauss3(xm, xa, xb, gm, ga, gb);
-        if (W != 0.0) {
-            const double em = xm < EXP_CUT ? pre * gm : 0.0;
-            const double ea = xa < EXP_CUT ? pre * ga : 0.0;
-            const double eb = xb < EXP_CUT ? pre * gb : 0.0;
-            Pv = 4.0 * W * (ea - eb);
-            Qv = 4.0 * W * (self ? 0.5 : 1.0) * em;
-        }
-        const bool has = Pv != 0.0 || Qv != 0.0;
-        const unsigned bal = __ballot_sync(0xffffffffu, has);
-        unsigned long long base = 0;
-        if (lane == 0 && bal != 0u) base = atomicAdd(bte_ctr, (unsigned long long)__popc(bal));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (has) {
-            const unsigned long long pos = base + (unsigned long long)__popc(bal & ((1u << lane) - 1u));
-            if ((long long)pos < bte_cap) {
-                TcBteEntry e;
-                e.r0 = (s.k0 & 0x1fffffff) - q0_first * NMODE;
-                e.k1 = s.k1;
-                e.k2 = s.k2;
-                e.pad = 0;
-                e.P = Pv;
-                e.Q = Qv;
-                bte[pos] = e;
-            }
-        }
-        __syncwarp();
-        return;
-    }
+    // operator entries: P = 4 W (g(w0 + w1 - w2) - g(w0 + w2 - w1)), Q = 4 W g(w0 - w1 - w2), the
+    // second term of P dropped and Q halved when q1 = q2; one entry per triple with P or Q nonzero
+    double Pv = 0.0, Qv = 0.0;
     TcStage s{};
-    double2 r0 = make_double2(0.0, 0.0), a = r0, b = r0, a1 = r0, a2 = r0, b1 = r0, b2 = r0;
-    double x1 = EXP_CUT, x2 = EXP_CUT, x3 = EXP_CUT;  // EXP_CUT: no weight (lanes past n)
+    double xm = EXP_CUT, xa = EXP_CUT, xb = EXP_CUT, W = 0.0;  // EXP_CUT: no weight
+    bool self = true;
     if (lane < n) {
         s = st[lane];
         const int o = s.k0 & 0x1fffffff;
-        r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
-        const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
-        const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
-        a = pa[0];
-        b = pb[0];
-        if (FAST) {
-            a1 = pa[1];
-            a2 = pa[2];
-            b1 = pb[1];
-            b2 = pb[2];
+        const double2 r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
+        const double2 a = *reinterpret_cast<const double2*>(modes + (size_t)s.k1 * rs);
+        const double2 b = *reinterpret_cast<const double2*>(modes + (size_t)s.k2 * rs);
+        if (!((s.k0 >> 29) & 1)) {
+            const double w0 = r0.x, w1 = a.x, w2 = b.x;
+            const double dm = w0 - w1 - w2, da = w0 + w1 - w2, db = w0 - w1 + w2;
+            xm = half_os2 * (dm * dm);
+            xa = half_os2 * (da * da);
+            xb = half_os2 * (db * db);
+            self = !((s.k0 >> 30) & 1);
+            if (self) xb = EXP_CUT;  // the second term of P is dropped when q1 = q2
+            W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac;
         }
-        const double w0 = r0.x, w1 = a.x, w2 = b.x;
-        const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
-        x1 = half_os2 * (d1 * d1);
-        x2 = half_os2 * (d2 * d2);
-        x3 = half_os2 * (d3 * d3);
     }
-    double g1, g2, g3;
-    tc_gauss3(x1, x2, x3, g1, g2, g3);
-    if (lane < n) {
-        const int o = s.k0 & 0x1fffffff;
-        const double e1 = x1 < EXP_CUT ? pre * g1 : 0.0;
-        const double e2 = x2 < EXP_CUT ? pre * g2 : 0.0;
-        const double e3 = x3 < EXP_CUT ? pre * g3 : 0.0;
-        const double wt = (s.k0 >> 30) & 1 ? 2.0 : 1.0;
-        const double p3 = e1 + e2 + e3;
-        if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
-        if (!((s.k0 >> 29) & 1)) {  // W = 0 for the Gamma acoustic modes of q0
-            const double W = (double)s.phi2 * (r0.y * b.y * a.y) * mfac * wt;
-            const double we1 = W * e1, wf2 = W * (e2 - e3);
-            if (FAST) {
-                const double n1[NT_FAST] = {a1.x, a1.y, a2.x, a2.y}, n2[NT_FAST] = {b1.x, b1.y, b2.x, b2.y};
+    double gm, ga, gb;
+    tc_gauss3(xm, xa, xb, gm, ga, gb);
+    if (W != 0.0) {
+        const double em = xm < EXP_CUT ? pre * gm : 0.0;
+        const double ea = xa < EXP_CUT ? pre * ga : 0.0;
+        const double eb = xb < EXP_CUT ? pre * gb : 0.0;
+        Pv = 4.0 * W * (ea - eb);
+        Qv = 4.0 * W * (self ? 0.5 : 1.0) * em;
+    }
+    const bool has = Pv != 0.0 || Qv != 0.0;
+    const unsigned bal = __ballot_sync(0xffffffffu, has);
+    unsigned long long base = 0;
+    if (lane == 0 && bal != 0u) base = atomicAdd(bte_ctr, (unsigned long long)__popc(bal));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (has) {
+        const unsigned long long pos = base + (unsigned long long)__popc(bal & ((1u << lane) - 1u));
+        if ((long long)pos < bte_cap) {
+            TcBteEntry e;
+            e.r0 = (s.k0 & 0x1fffffff) - q0_first * NMODE;
+            e.k1 = s.k1;
+            e.k2 = s.k2;
+            e.pad = 0;
+            e.P = Pv;
+            e.Q = Qv;
+            bte[pos] = e;
+        }
+    }
+    __syncwarp();
+}
+
+// One staged triple of the linewidth sums, loaded: its entry, the q0 record (omega, 1/omega), the mode
+// records of q1 and q2 (omega, 1/omega, up to four occupations when FAST) and the three Gaussian
+// arguments (EXP_CUT, no weight, for an empty slot).
+struct TcEv {
+    TcStage s;
+    double2 r0, a, b, a1, a2, b1, b2;
+    double x1, x2, x3;
+};
+template <bool FAST>
+__device__ __forceinline__ void tc_ev_load(TcEv& v, const TcStage* st, int i, int n, int rs,
+                                           const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes) {
+    v.x1 = v.x2 = v.x3 = EXP_CUT;
+    if (i >= n) return;
+    v.s = st[i];
+    const int o = v.s.k0 & 0x1fffffff;
+    v.r0 = *reinterpret_cast<const double2*>(&q0rec[o].w);
+    const double2* pa = reinterpret_cast<const double2*>(modes + (size_t)v.s.k1 * rs);
+    const double2* pb = reinterpret_cast<const double2*>(modes + (size_t)v.s.k2 * rs);
+    v.a = pa[0];
+    v.b = pb[0];
+    if (FAST) {
+        v.a1 = pa[1];
+        v.a2 = pa[2];
+        v.b1 = pb[1];
+        v.b2 = pb[2];
+    }
+}
+__device__ __forceinline__ void tc_ev_args(TcEv& v, int i, int n, double half_os2) {
+    if (i >= n) return;
+    const double w0 = v.r0.x, w1 = v.a.x, w2 = v.b.x;
+    const double d1 = w0 - w1 - w2, d2 = w0 + w1 - w2, d3 = w0 - w1 + w2;
+    v.x1 = half_os2 * (d1 * d1);
+    v.x2 = half_os2 * (d2 * d2);
+    v.x3 = half_os2 * (d3 * d3);
+}
+template <bool FAST>
+__device__ __forceinline__ void tc_ev_sum(const TcEv& v, double g1, double g2, double g3, int nq0, int nT, int rs,
+                                          double pre, double mfac, const double* __restrict__ modes, double* out_lw,
+                                          double* out_p3) {
+    const TcStage& s = v.s;
+    const int o = s.k0 & 0x1fffffff;
+    const double e1 = v.x1 < EXP_CUT ? pre * g1 : 0.0;
+    const double e2 = v.x2 < EXP_CUT ? pre * g2 : 0.0;
+    const double e3 = v.x3 < EXP_CUT ? pre * g3 : 0.0;
+    const double wt = (s.k0 >> 30) & 1 ? 2.0 : 1.0;
+    const double p3 = e1 + e2 + e3;
+    if (p3 != 0.0) atomicAdd(&out_p3[o], wt * p3);
+    if ((s.k0 >> 29) & 1) return;  // W = 0 for the Gamma acoustic modes of q0
+    const double W = (double)s.phi2 * (v.r0.y * v.b.y * v.a.y) * mfac * wt;
+    const double we1 = W * e1, wf2 = W * (e2 - e3);
+    if (FAST) {
+        const double n1[NT_FAST] = {v.a1.x, v.a1.y, v.a2.x, v.a2.y}, n2[NT_FAST] = {v.b1.x, v.b1.y, v.b2.x, v.b2.y};
 #pragma unroll
-                for (int T = 0; T < NT_FAST; ++T)
-                    if (T < nT) {
-                        const double v = ((n1[T] + n2[T] + 1.0) * we1) + ((n1[T] - n2[T]) * wf2);
-                        if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
-                    }
-            } else {
-                const double* m1 = modes + (size_t)s.k1 * rs + 2;
-                const double* m2 = modes + (size_t)s.k2 * rs + 2;
-                for (int T = 0; T < nT; ++T) {
-                    const double v = ((m1[T] + m2[T] + 1.0) * we1) + ((m1[T] - m2[T]) * wf2);
-                    if (v != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], v);
-                }
+        for (int T = 0; T < NT_FAST; ++T)
+            if (T < nT) {
+                const double x = ((n1[T] + n2[T] + 1.0) * we1) + ((n1[T] - n2[T]) * wf2);
+                if (x != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], x);
             }
+    } else {
+        const double* m1 = modes + (size_t)s.k1 * rs + 2;
+        const double* m2 = modes + (size_t)s.k2 * rs + 2;
+        for (int T = 0; T < nT; ++T) {
+            const double x = ((m1[T] + m2[T] + 1.0) * we1) + ((m1[T] - m2[T]) * wf2);
+            if (x != 0.0) atomicAdd(&out_lw[(size_t)T * nq0 * NMODE + o], x);
         }
     }
-    __syncwarp();  // every lane has read its entry before the warp stages new ones over it
+}
+
+// FP64 part of n <= 64 staged triples, entries lane and lane + 32 of each lane (the loads of both
+// issued before either is evaluated): MODE 0 the linewidth and phase-space sums, W = wt mfac
+// |Phi|^2 / (omega0 omega1 omega2), P3 += wt (g1 + g2 + g3), Gamma_T += W [(n1 + n2 + 1) g1 +
+// (n1 - n2)(g2 - g3)] with atomics; MODE 1 operator entries.  FAST: mode records of 8 doubles,
+// n_temps <= 4.
+template <bool FAST, int MODE>
+__device__ __forceinline__ void tc_drain(const TcStage* st, int n, int nq0, int nT, int rs, double half_os2, double pre,
+                                         double mfac, const Q0Rec* __restrict__ q0rec, const double* __restrict__ modes,
+                                         double* out_lw, double* out_p3, TcBteEntry* bte, unsigned long long* bte_ctr,
+                                         long long bte_cap, int q0_first) {
+    const int lane = threadIdx.x & 31;
+    if (MODE == 1) {
+        tc_bte_round(st, min(n, 32), rs, half_os2, pre, mfac, q0rec, modes, bte, bte_ctr, bte_cap, q0_first);
+        if (n > 32)
+            tc_bte_round(st + 32, n - 32, rs, half_os2, pre, mfac, q0rec, modes, bte, bte_ctr, bte_cap, q0_first);
+        return;
+    }
+    TcEv v0, v1;
+    tc_ev_load<FAST>(v0, st, lane, n, rs, q0rec, modes);
+    tc_ev_load<FAST>(v1, st, lane + 32, n, rs, q0rec, modes);
+    tc_ev_args(v0, lane, n, half_os2);
+    tc_ev_args(v1, lane + 32, n, half_os2);
+    double g1, g2, g3;
+    tc_gauss3(v0.x1, v0.x2, v0.x3, g1, g2, g3);
+    if (lane < n) tc_ev_sum<FAST>(v0, g1, g2, g3, nq0, nT, rs, pre, mfac, modes, out_lw, out_p3);
+    if (__any_sync(0xffffffffu, lane + 32 < n)) {
+        tc_gauss3(v1.x1, v1.x2, v1.x3, g1, g2, g3);
+        if (lane + 32 < n) tc_ev_sum<FAST>(v1, g1, g2, g3, nq0, nT, rs, pre, mfac, modes, out_lw, out_p3);
+    }
+    __syncwarp();  // every lane has read its entries before the warp stages new ones over them
 }
 
 // Warp-specialised tensor-core pass.  For tile j the copy warp loads operand stage j % 2 (TMA
@@ -767,7 +809,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
         const int wq = warp & 3, g = warp >> 2;
         const int e = 4 * wq + lane / 8, s2 = lane % 8, s2c = s2 < NMODE ? s2 : 0;
         TcStage* stg = S.stg[warp];
-        int count = 0;  // staged triples (warp-uniform); fewer than 32 between tiles
+        int count = 0;  // staged triples (warp-uniform); fewer than 64 between tiles
         // slots allowed by the mode ranges, and by the Gamma acoustic rule when q1 = Gamma (amask_g:
         // s1 = g < 3 drops out)
         unsigned amask_n = 0u;
@@ -821,7 +863,7 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             // (at most 12), then each lane writes its own, |Phi|^2 = |sum_k e0'(k, s0) Y_k|^2 in FP32
             // from the stage's q0 record of the lane's pair (the two basis atoms' terms summed
             // separately).  When the tile's triples would not fit beside those left from earlier
-            // tiles (fewer than 32; rare), they go in four chunks of at most 3 per lane, each after
+            // tiles (fewer than 64; rare), they go in four chunks of at most 3 per lane, each after
             // full rounds are evaluated to make room.
             const int kw = en.z == 2 ? (1 << 30) : 0;
             const int k0b = en.x * NMODE, k2 = en.y * NMODE + s2;
@@ -884,9 +926,9 @@ k_v3tc(TcArgs a, const __grid_constant__ CUtensorMap tmA, const int4* __restrict
             tc::fence_before_sync();
             __syncwarp();
             if (lane == 0) tc::mbar_arrive(tc::smem_u32(&S.empty[es]));
-            while (count >= 32) {
-                count -= 32;
-                tc_drain<FAST, MODE>(stg + count, 32, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
+            while (count >= 64) {
+                count -= 64;
+                tc_drain<FAST, MODE>(stg + count, 64, a.nq0, a.nT, a.rs, a.half_os2, a.pre, a.mfac, q0rec, modes, out_lw,
                                out_p3, bte, bte_ctr, a.bte_cap, a.q0_first);
             }
         }
