@@ -21,9 +21,9 @@
 // (k_tc_keys, about half of them).  One pass: k_v3tc computes Y on the tensor
 // cores and screens each mode triple in FP32 against the window where a delta
 // weight can exceed exp(-40) of its peak (4e-18); for the ~1-3 % inside it the
-// epilogue warp forms |Phi|^2 (FP32), stages it in shared memory and, 32 at a
-// time, evaluates W, the FP64 delta weights and the phase-space and linewidth
-// sums.
+// epilogue warp forms |Phi|^2 (FP32), stages it in shared memory and, 64 at a
+// time (two per lane), evaluates W, the FP64 delta weights and the phase-space
+// and linewidth sums (or, for the iterative BTE, the operator entries).
 // Roofline: tensor pipe for Y (about 74 kflop issued per pair per split pass);
 // in practice the per-tile pipeline (TMA requests, FP32 screening issue) and the
 // L2 latency of the mode records read by the staged evaluations.
@@ -567,7 +567,7 @@ __device__ __forceinline__ void tc_drain(const TcStage* st, int n, int nq0, int 
 // epilogue warp works on its own: it reads its 32 accumulator rows, screens its 12 mode triples per
 // row in FP32 against the delta window, forms |Phi|^2 of the active ones (about 1-3 %) from the
 // stage's q0 records, stages them in its shared-memory buffer, releases the stage, and evaluates
-// the FP64 delta weights and sums of the staged triples 32 at a time, one per lane (tc_drain).
+// the FP64 delta weights and sums of the staged triples 64 at a time, two per lane (tc_drain).
 // MODE 0: linewidth and phase-space sums; MODE 1: entries of the iterative-BTE operator.
 template <bool SPLIT, bool FAST, int MODE>
 __global__ void __launch_bounds__(TC_THREADS, 1)
